@@ -1,0 +1,402 @@
+#!/usr/bin/env python
+"""Benchmark of the CompLB3D hot path on B200.
+
+Headline: coupled-step MLUPS of the 256x256x512 sphere-pack workload (porosity
+0.35): one transport step (fused D3Q7 ADR of 8 mobile solutes with dual-Monod
+kinetics, surface-gated CaCO3 precipitation and a 3-component Newton
+speciation in every pore voxel) plus the amortised flow re-solve (500 D3Q19
+steps every 200 transport steps = 2.5 flow steps per step) and the node
+conversion every 200 steps.  Inputs are resident in HBM; the state (~13 GB) is
+far larger than L2, so no flush is needed between steps.
+
+The same line reports the learned-vs-cold Newton speciation batch (2^21
+solves of a 5-component x 14-species tableau at a 1e-10 relative residual,
+network trained on 2^20 Newton-produced pairs), the roofline of the dominant
+kernel from CUDA events on its own stream, an end-to-end figure through the
+C ABI with host buffers, and the FP64 CPU oracle timed on the host cores.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+Under torchrun each rank runs its own domain (weak scaling, no collective on
+the data path); the timed region is bracketed by a barrier and the max over
+ranks is reported.
+"""
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(ROOT, "complb3d-lattice-boltzmann-fba-surrogate-cobrapy-glpk_b200")
+METRIC = "coupled-step MLUPS on 1 B200; learned vs cold Newton speciation at 1e-10 residual"
+FULL = (512, 256, 256)          # nx (flow direction, incl. the two boundary planes), ny, nz
+CPU_SAMPLE = (128, 64, 64)      # bounded sample of the same workload for the CPU legs
+ADE_BYTES_PER_FLUID_SITE = 8 * 56 + 12 + 8 + 8   # 8 solutes x (7 f32 read + write), u, mineral, biomass
+FLOW_BYTES_PER_BGK_SITE = 19 * 4 * 2
+
+
+def load_pkg():
+    if "complab_b200" in sys.modules:
+        return sys.modules["complab_b200"]
+    spec = importlib.util.spec_from_file_location("complab_b200", os.path.join(PKG_DIR, "__init__.py"),
+                                                  submodule_search_locations=[PKG_DIR])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["complab_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def load_workloads():
+    load_pkg()
+    import importlib
+    return importlib.import_module("complab_b200.workloads")
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_from_profile(kernel):
+    """DRAM bytes per fluid site from the committed ncu summary, or None."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        parts = line.split()
+        if len(parts) >= 2 and parts[0] == kernel:
+            return float(parts[1])
+    return None
+
+
+class Clocks:
+    """nvidia-smi clock sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev):
+        self.dev = dev
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.Q,
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = [l.strip().split(",") for l in open(self.f.name) if l.strip()]
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            try:
+                sm.append(float(r[1])); mx = float(r[2])
+            except (ValueError, IndexError):
+                continue
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def coupled_setup(pkg, wl, shape, seed, stream=None):
+    nx, ny, nz = shape
+    mask = wl.sphere_pack(nx, ny, nz, 0.35, 5.0, 10.0, seed=seed)
+    cfg = wl.coupled_config(pkg, nx, ny, nz)
+    bio = wl.seed_biomass(mask, seed + 1)
+    return cfg, mask, bio
+
+
+def fluid_counts(cfg, mask):
+    fluid = np.isin(mask, list(cfg.pore_codes)[:cfg.n_pore_codes] + list(cfg.bio_codes)[:cfg.n_bio_codes])
+    return int(fluid[1:-1].sum()), int(fluid.sum())
+
+
+def coupled_step(lat, i):
+    """One coupled step: transport, the amortised flow re-solve, and every 200
+    steps the node conversion with its dynamics switch and velocity coupling."""
+    lat.step(1)
+    lat.flow_steps(2 if i % 2 == 0 else 3)
+    if i % 200 == 199:
+        lat.precip_convert()
+        lat.update_dynamics()
+        lat.couple_velocity()
+
+
+# ----------------------------------------------------------------- CPU legs
+def cpu_coupled(steps, seed=5):
+    """The FP64 oracle (OpenMP, all host cores) on a bounded sample of the
+    coupled workload: returns (MLUPS, seconds, threads, sample text)."""
+    pkg, wl = load_pkg(), load_workloads()
+    from oracle import oracle as o
+    cfg, mask, bio = coupled_setup(pkg, wl, CPU_SAMPLE, seed)
+    fl = o.Flow(cfg, mask)
+    fl.step(50)
+    _, u = fl.macro()
+    tr = o.Transport(cfg, mask, u=u)
+    tr.set_biomass(0, bio)
+    tr.step(1)
+    t0 = time.perf_counter()
+    for i in range(steps):
+        tr.step(1)
+        fl.step(2 if i % 2 == 0 else 3)
+    dt = time.perf_counter() - t0
+    N = int(np.prod(CPU_SAMPLE))
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    sample = "%dx%dx%d sites (same chemistry, porosity, step schedule), %d coupled steps" % (
+        CPU_SAMPLE[0], CPU_SAMPLE[1], CPU_SAMPLE[2], steps)
+    return N * steps / dt / 1e6, dt, threads, sample
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    steps = max(args.steps, 1)
+    mlups, dt, threads, sample = cpu_coupled(steps)
+    line = {"impl": "reference", "metric": METRIC, "value": mlups, "unit": "MLUPS", "n_gpus": args.gpus,
+            "steps": steps, "warmup": args.warmup, "ms_per_step": dt / steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_block(),
+            "cpu_baseline": {"value": mlups, "unit": "MLUPS", "cores": threads, "kind": "port",
+                             "sample": sample + "; the reference's own LBM path needs Palabos v2.3.0, which is "
+                                                "not vendored, so its CPU restatement runs instead"},
+            "e2e": {"value": mlups, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def config_block():
+    return {"workload": "coupled sphere pack %dx%dx%d (nx incl. 2 boundary planes), porosity 0.35, radii 5-10; "
+                        "D3Q19 flow (2.5 steps amortised) + D3Q7 ADR of 8 mobile solutes + 1 mineral, dual-Monod "
+                        "kinetics, surface precipitation, 3-component Newton speciation per pore voxel"
+                        % FULL,
+            "nx": FULL[0], "ny": FULL[1], "nz": FULL[2], "sites": int(np.prod(FULL)),
+            "l2": "inputs larger than L2 (about 13 GB of state), no flush",
+            "parallelism": "one domain per GPU (weak scaling, no data-path collective)"}
+
+
+# ----------------------------------------------------------------- speciation
+def speciation_bench(pkg, wl, stream, n_train=1 << 20, n_test=1 << 21):
+    import torch
+    S, logk, cs = wl.tableau(5, 9, seed=4)
+    sys_ = pkg.EqSystem()
+    pkg.set_eq_system(sys_, S, logk, cs, max_iter=200, tol=1e-10, warm_iter=6)
+    eq = pkg.EqSolver(sys_, stream=stream)
+    dev = torch.device("cuda")
+    Ttr, _, _, _ = wl.speciation_batch(S, logk, n_train, seed=301)
+    Tte, _, _, acc = wl.speciation_batch(S, logk, n_test, seed=302)
+    f64 = dict(dtype=torch.float64, device=dev)
+    dT = torch.tensor(Ttr, **f64)
+    dC = torch.tensor(wl.cold_species(S, Ttr, cs), **f64)
+    dX = torch.zeros((n_train, 5), **f64)
+    dI = torch.zeros(n_train, dtype=torch.int32, device=dev)
+    dS = torch.zeros(n_train, dtype=torch.uint8, device=dev)
+    t0 = time.perf_counter()
+    eq.solve_device(dT.data_ptr(), dC.data_ptr(), dX.data_ptr(), dI.data_ptr(), dS.data_ptr(), n_train,
+                    pkg.EQ_START_COLD)
+    ok = (dS == 0)
+    Tk, Xk = dT[ok].contiguous(), dX[ok].contiguous()
+    loss = eq.train_device(Tk.data_ptr(), Xk.data_ptr(), int(Tk.shape[0]), epochs=8, batch=4096, lr=2e-3, seed=7)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    eT = torch.tensor(Tte, **f64)
+    eC = torch.tensor(wl.cold_species(S, Tte, cs), **f64)
+    res = {}
+    for name, start in (("cold", pkg.EQ_START_COLD), ("learned", pkg.EQ_START_LEARNED)):
+        X = torch.zeros((n_test, 5), **f64)
+        I = torch.zeros(n_test, dtype=torch.int32, device=dev)
+        St = torch.zeros(n_test, dtype=torch.uint8, device=dev)
+        eq.solve_device(eT.data_ptr(), eC.data_ptr(), X.data_ptr(), I.data_ptr(), St.data_ptr(), n_test, start)
+        times = []
+        for _ in range(3):
+            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            s0.record()
+            eq.solve_device(eT.data_ptr(), eC.data_ptr(), X.data_ptr(), I.data_ptr(), St.data_ptr(), n_test, start)
+            s1.record()
+            torch.cuda.synchronize()
+            times.append(s0.elapsed_time(s1))
+        ms = min(times)
+        st = St.cpu().numpy()
+        res[name] = {"ms": ms, "solves_per_s": n_test / (ms * 1e-3), "mean_iters": float(I.float().mean().item()),
+                     "converged": float((st <= 1).mean()), "fell_back": float((st == 1).mean()),
+                     "x": X}
+    # same roots and residuals where both converged
+    from_cold, from_learned = res["cold"].pop("x"), res["learned"].pop("x")
+    diff = (from_cold - from_learned).abs().max(dim=1).values
+    res["max_abs_logdiff_both_converged"] = float(diff.max().item())
+    res["speedup_learned_vs_cold"] = res["cold"]["ms"] / res["learned"]["ms"]
+    res.update({"n_solves": n_test, "n_train_pairs": int(Tk.shape[0]), "train_s": train_s, "final_loss": loss,
+                "tableau": "5 components x 14 species, logK U[-14,14], stoichiometry in [-2,2] (negative only on "
+                           "the pH-like component), totals 1e-6..1e-1, free H 1e-9..1e-5; acceptance %.3f" % acc,
+                "residual": "max_j |S^T c - T|_j / (|S|^T c)_j <= 1e-10"})
+    eq.close()
+    return res
+
+
+# ----------------------------------------------------------------- main arm
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-speciation", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--shape", default=None, help="override nx,ny,nz (development only)")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    args.warmup = max(args.warmup, 3)
+    global FULL
+    if args.shape:
+        FULL = tuple(int(v) for v in args.shape.split(","))
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    pkg, wl = load_pkg(), load_workloads()
+    stream = torch.cuda.current_stream().cuda_stream
+    cfg, mask, bio = coupled_setup(pkg, wl, FULL, seed=5 + rank)
+    n_fluid_int, n_fluid = fluid_counts(cfg, mask)
+    N = int(np.prod(FULL))
+    lat = pkg.Lattice(cfg, stream=stream)
+    lat.upload_mask(mask)
+    lat.flow_init()
+    lat.flow_steps(200)
+    lat.couple_velocity()
+    lat.ade_init()
+    lat.set_field(pkg.FIELD_BIOMASS, 0, bio)
+    for i in range(args.warmup):
+        coupled_step(lat, i)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = Clocks(local)
+    clocks.start()
+    lat.timing(True)
+    lat.timing_read(pkg.KERNEL_ADE_MAIN)
+    lat.timing_read(pkg.KERNEL_FLOW_STEP)
+    l0 = lat.launch_count()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for i in range(args.steps):
+        coupled_step(lat, args.warmup + i)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = lat.launch_count() - l0
+    ade_ms, ade_n = lat.timing_read(pkg.KERNEL_ADE_MAIN)
+    flow_ms, flow_n = lat.timing_read(pkg.KERNEL_FLOW_STEP)
+    lat.timing(False)
+    clk = clocks.stop()
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    ms_per_step = ms / args.steps
+    value = N * world * args.steps / (ms * 1e-3) / 1e6
+    out = {"metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32 populations, f64 speciation", "data": "synthetic (seeded sphere pack)",
+           "config": config_block(), "fluid_mlups": n_fluid * world * args.steps / (ms * 1e-3) / 1e6,
+           "gpu_launches": int(launches), "clocks": clk}
+    # roofline of the dominant kernel: the fused transport step
+    peak, peak_kind = peaks()
+    ade_bytes = n_fluid_int * ADE_BYTES_PER_FLUID_SITE + (N - 2 * FULL[1] * FULL[2])
+    if ade_n:
+        achieved = ade_bytes / (ade_ms / ade_n * 1e-3) / 1e9
+        tps = traffic_from_profile("ade_main_kernel")
+        out["roofline"] = {"kernel": "ade_main_kernel", "bound": "hbm", "achieved": achieved, "peak": peak,
+                           "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind + " (hbm_gbs)",
+                           "algorithmic_bytes_per_launch": ade_bytes, "avg_launch_ms": ade_ms / ade_n,
+                           "traffic": (tps * n_fluid_int) if tps else None,
+                           "share_of_step": ade_ms / ms if ms else None}
+    if flow_n:
+        n_bgk = n_fluid
+        fb = n_bgk * FLOW_BYTES_PER_BGK_SITE + N
+        out["flow_kernel"] = {"achieved_gbs": fb / (flow_ms / flow_n * 1e-3) / 1e9, "avg_launch_ms": flow_ms / flow_n,
+                              "launches": flow_n, "share_of_step": flow_ms / ms if ms else None}
+    # end to end through the C ABI with pinned host buffers
+    out["e2e"] = e2e_run(pkg, torch, cfg, mask, bio, args.steps, stream, world)
+    lat.close()
+    if rank == 0 and world == 1 and not args.no_speciation:
+        out["speciation"] = speciation_bench(pkg, wl, stream)
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cm, cdt, threads, sample = cpu_coupled(40)
+        out["cpu_baseline"] = {"value": cm, "unit": "MLUPS", "cores": threads, "kind": "port", "sample": sample}
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def e2e_run(pkg, torch, cfg, mask, bio, steps, stream, world):
+    """The same job through the public C ABI with pinned host buffers: upload
+    the geometry and the biomass, initialise, run the steps, read every solute
+    field back; the copies are inside the timed region."""
+    N = mask.size
+    h_mask = torch.from_numpy(np.ascontiguousarray(mask.reshape(-1))).pin_memory().numpy()
+    h_bio = torch.from_numpy(np.ascontiguousarray(bio.reshape(-1))).pin_memory().numpy()
+    h_out = torch.empty((cfg.n_solutes, N), dtype=torch.float64).pin_memory().numpy()
+    lat = pkg.Lattice(cfg, stream=stream)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    lat.upload_mask(h_mask)
+    lat.flow_init()
+    lat.couple_velocity()
+    lat.ade_init()
+    lat.set_field(pkg.FIELD_BIOMASS, 0, h_bio)
+    for i in range(steps):
+        coupled_step(lat, i)
+    for s in range(cfg.n_solutes):
+        lat._c(lat.lib.cl_get_field(lat.h, pkg.FIELD_CONC, s, pkg._ptr(h_out[s])), "cl_get_field")
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    lat.close()
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([dt], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dt = float(t.item())
+    h2d = h_mask.nbytes + h_bio.nbytes
+    d2h = h_out.nbytes
+    return {"value": N * world * steps / dt / 1e6, "unit": "MLUPS", "h2d_bytes_per_step": h2d // steps,
+            "d2h_bytes_per_step": d2h // steps,
+            "includes": "geometry and biomass upload, initialisation, the steps (flow develops inside the "
+                        "amortised re-solve), and the read-back of every solute field, amortised over the steps"}
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,359 @@
+// ade.cu -- fused multi-solute D3Q7 advection-diffusion-reaction step (rows a5-a12).
+//
+// One launch does, for every interior site and every mobile solute, what the
+// reference does in separate whole-lattice passes (src/complab.cpp:1252-1374,
+// 1849-1857): AdvectionDiffusionBGKdynamics collide, run_kinetics +
+// update_rxnLattices, the dC reset + run_abiotic_kinetics /
+// surfaceAbioticKinetics3D + update_abiotic_rxnLattices, run_equilibrium_biotic
+// (Newton), and stream.  The increment lattices dC/dB of the reference
+// (whole-lattice copies every step, complab.cpp:1264) never exist: increments
+// stay in shared memory of the thread that owns the voxel.
+//
+// Per site the reaction chain only needs the solute densities, and every
+// reference processor adds t_i*dC to the post-collision populations, so:
+//   pass 1  gathers the populations and sums the densities,
+//   chain   runs kinetics -> abiotic -> equilibrium on the densities (FP64),
+//   pass 2  re-gathers (L1/L2 hit), collides, adds t_i*dC_total, streams.
+// HBM traffic stays at one read and one write of 7 FP32 populations per
+// solute; the FP64 Newton state never shares registers with the populations.
+//
+// Boundary planes x = 0 and x = nx-1 run in a second, small launch after the
+// interior one: a zero-gradient face needs the pre-collision density of its
+// neighbour plane, which the interior launch records (FlatAdiabaticBoundary-
+// Functional3D sets the boundary density to that value after each stream).
+#pragma once
+#include "internal.h"
+#include "newton.cuh"
+
+namespace cl {
+
+#define THRD 1e-12
+
+struct AdeK {
+    Geo g;
+    float* pop;               // n_mob * 7 * N
+    const uint8_t* cls;
+    const float* u;           // 3*N
+    double* imm;              // S*N
+    double* bio;              // M*N
+    float* rho_adj;           // n_mob * 2 * plane
+    int32_t* eq_iters;        // N (may be null)
+    unsigned long long* counters;
+    int nodyn_coupled;
+    int parity;
+    AdeParams p;
+    EqDev e;
+};
+
+template <int PARITY>
+__device__ __forceinline__ void gather7(const float* pop, const Geo& g, int64_t n, int x, int y, int z, float* f) {
+#pragma unroll
+    for (int i = 0; i < 7; ++i) {
+        if (PARITY == 0) f[i] = pop[i * g.N + n];
+        else {
+            const int64_t m = nbr(g, n, x, y, z, -c7x(i), -c7y(i), -c7z(i));
+            f[i] = (m < 0) ? pop[i * g.N + n] : pop[opp7(i) * g.N + m];
+        }
+    }
+}
+
+template <int PARITY>
+__device__ __forceinline__ void scatter7(float* pop, const Geo& g, int64_t n, int x, int y, int z, const float* f) {
+#pragma unroll
+    for (int i = 0; i < 7; ++i) {
+        if (PARITY == 0) pop[opp7(i) * g.N + n] = f[i];
+        else {
+            const int64_t m = nbr(g, n, x, y, z, c7x(i), c7y(i), c7z(i));
+            if (m < 0) pop[opp7(i) * g.N + n] = f[i];
+            else pop[i * g.N + m] = f[i];
+        }
+    }
+}
+
+// AdvectionDiffusionBGKdynamics: geq_i = t_i rho (1 + c_i.u / cs2), cs2 = 1/4
+__device__ __forceinline__ void collide7(float* f, float om, float ux, float uy, float uz, float& rho) {
+    float r = 0.f;
+#pragma unroll
+    for (int i = 0; i < 7; ++i) r += f[i];
+    rho = r;
+#pragma unroll
+    for (int i = 0; i < 7; ++i) {
+        const float cu = c7x(i) * ux + c7y(i) * uy + c7z(i) * uz;
+        const float geq = t7(i) * r * (1.f + 4.f * cu);
+        f[i] = f[i] - om * (f[i] - geq);
+    }
+}
+
+// Table-driven rate law (defineRxnKinetics / defineAbioticRxnKinetics ABI).
+// C, R, B, BR are shared-memory columns with stride bd.
+static __device__ void rates_dev(const AdeParams& p, int abiotic, const double* C, const double* B,
+                          double* R, double* BR, int bd) {
+    for (int s = 0; s < p.S; ++s) R[s * bd] = 0.0;
+    if (!abiotic) for (int m = 0; m < p.M; ++m) BR[m * bd] = 0.0;
+    for (int k = 0; k < p.n_rxn; ++k) {
+        const cl_rxn& r = p.rxn[k];
+        if ((r.microbe < 0) != (abiotic != 0)) continue;
+        double rate = r.k;
+        if (r.microbe >= 0) {
+            const double b = B[r.microbe * bd];
+            if (!(b > 0.0)) continue;
+            rate *= b;
+        }
+        for (int j = 0; j < r.n_monod; ++j) {
+            const double c = fmax(C[r.monod_s[j] * bd], 0.0);
+            rate *= c / (r.monod_ks[j] + c);
+        }
+        for (int j = 0; j < r.n_mass; ++j) rate *= fmax(C[r.mass_s[j] * bd], 0.0);
+        for (int s = 0; s < p.S; ++s) R[s * bd] = fma(r.nu[s], rate, R[s * bd]);
+        if (!abiotic) BR[r.microbe * bd] = fma(r.yield, rate, BR[r.microbe * bd]);
+    }
+    if (!abiotic)
+        for (int m = 0; m < p.M; ++m) BR[m * bd] -= p.decay[m] * fmax(B[m * bd], 0.0);
+    for (int s = 0; s < p.S; ++s) if (!isfinite(R[s * bd])) R[s * bd] = 0.0;
+    if (!abiotic) for (int m = 0; m < p.M; ++m) if (!isfinite(BR[m * bd])) BR[m * bd] = 0.0;
+}
+
+// The reaction chain of one voxel.  Cur holds the current densities (updated
+// as each processor applies its increments), App the total increment per
+// solute.  Returns 1 if the equilibrium solve did not converge.
+template <int NC>
+__device__ int reaction_chain(const AdeK& k, int64_t n, uint8_t cls, double* Cur, double* App,
+                              double* Ct, double* R, double* B, double* BR, int bd) {
+    const AdeParams& p = k.p;
+    const int64_t N = k.g.N;
+    int nonconv = 0;
+    // run_kinetics (part1.hh:63-146) + update_rxnLattices (:338-429)
+    if (p.do_kin) {
+        for (int s = 0; s < p.S; ++s) { const double c = Cur[s * bd]; Ct[s * bd] = c < THRD ? 0.0 : c; }
+        for (int m = 0; m < p.M; ++m) { const double b = k.bio[m * N + n]; B[m * bd] = b < THRD ? 0.0 : b; }
+        rates_dev(p, 0, Ct, B, R, BR, bd);
+        for (int s = 0; s < p.S; ++s) {
+            const double d = R[s * bd] * p.dt;
+            if (d > THRD || d < -THRD) { Cur[s * bd] += d; App[s * bd] += d; }
+        }
+        for (int m = 0; m < p.M; ++m) {
+            const double d = BR[m * bd] * p.dt;
+            if (d > THRD || d < -THRD) k.bio[m * N + n] += d;
+        }
+    }
+    // dC = dC0; run_abiotic_kinetics | surfaceAbioticKinetics3D; update_abiotic_rxnLattices
+    if (p.do_abio && (!p.surface_only || (cls & F_SURFACE))) {
+        for (int s = 0; s < p.S; ++s) { const double c = Cur[s * bd]; Ct[s * bd] = c < THRD ? 0.0 : c; }
+        rates_dev(p, 1, Ct, nullptr, R, nullptr, bd);
+        for (int s = 0; s < p.S; ++s) {
+            const double d = R[s * bd] * p.dt;
+            if (d > THRD || d < -THRD) { Cur[s * bd] += d; App[s * bd] += d; }
+        }
+    }
+    // run_equilibrium_biotic (part4_eqsolver.hh:1355-1494), Newton applied only
+    // when converged (run_equilibrium_NR, NR_reserve.hh:734)
+    if constexpr (NC > 0) {
+        const EqDev& e = k.e;
+        double x[NC], T[NC];
+        for (int s = 0; s < p.S; ++s) Ct[s * bd] = fmax(Cur[s * bd], 1e-30);
+        // totals and cold start read the floored species column
+#pragma unroll
+        for (int j = 0; j < NC; ++j) T[j] = 0.0;
+        for (int i = 0; i < e.ns; ++i) {
+            if (!e.active[i]) continue;
+            const double c = fmin(fmax(Ct[i * bd], 1e-30), 10.0);
+#pragma unroll
+            for (int j = 0; j < NC; ++j) T[j] = fma(e.stoich[i][j], c, T[j]);
+        }
+#pragma unroll
+        for (int j = 0; j < NC; ++j) {
+            T[j] = fmax(T[j], 1e-30);
+            double c = 1e-7;
+            const int idx = e.comp_species[j];
+            if (idx >= 0) c = Ct[idx * bd];
+            x[j] = log10(fmin(fmax(c, 1e-30), 10.0));
+        }
+        int conv = 0;
+        const int it = eq_newton<NC>(e, T, x, p.eq.max_iter, p.eq.tol, &conv);
+        if (k.eq_iters) k.eq_iters[n] = it;
+        if (!conv) nonconv = 1;
+        else {
+            for (int s = 0; s < p.S && s < e.ns; ++s) {
+                const double conc = Ct[s * bd];
+                double eqc = e.active[s] ? species_c<NC>(e, s, x) : fmin(conc, 10.0);
+                eqc = fmin(fmax(eqc, 1e-30), 10.0);
+                double d = eqc - conc;
+                const double mx = fmax(1e-9, 0.1 * fabs(conc));
+                if (fabs(d) > mx) d = d > 0 ? mx : -mx;
+                if (conc + d < 1e-20) d = 1e-20 - conc;
+                if (fabs(d) > THRD) { Cur[s * bd] += d; App[s * bd] += d; }
+            }
+        }
+    }
+    return nonconv;
+}
+
+template <int NMOB, int NC, int PARITY>
+__global__ void __launch_bounds__(256) ade_main_kernel(AdeK k) {
+    extern __shared__ double sm[];
+    const int bd = blockDim.x;
+    const AdeParams& p = k.p;
+    double* Cur = sm + threadIdx.x;
+    double* App = Cur + p.S * bd;
+    double* Ct  = App + p.S * bd;
+    double* R   = Ct + p.S * bd;
+    double* B   = R + p.S * bd;
+    double* BR  = B + (p.M > 0 ? p.M : 1) * bd;
+    const int64_t N = k.g.N, plane = k.g.plane;
+    const int64_t lo = plane, hi = N - plane;                 // interior x = 1 .. nx-2
+    const int64_t stride = (int64_t)gridDim.x * bd;
+    const bool any_rxn = p.do_kin || p.do_abio || NC > 0;
+    unsigned long long nonconv = 0;
+    for (int64_t n = lo + (int64_t)blockIdx.x * bd + threadIdx.x; n < hi; n += stride) {
+        const uint8_t cls = k.cls[n];
+        const uint8_t dyn = cls & 3;
+        if (dyn == BB) continue;
+        if (dyn == NODYN && !k.nodyn_coupled) continue;
+        int x, y, z;
+        decode(k.g, n, x, y, z);
+        float dC[NMOB];
+#pragma unroll
+        for (int m = 0; m < NMOB; ++m) dC[m] = 0.f;
+        if (dyn != NODYN && (cls & F_REACTIVE) && any_rxn) {
+            // pass 1: densities
+            for (int s = 0; s < p.S; ++s) { App[s * bd] = 0.0; }
+#pragma unroll
+            for (int m = 0; m < NMOB; ++m) {
+                float f[7];
+                gather7<PARITY>(k.pop + (int64_t)m * 7 * N, k.g, n, x, y, z, f);
+                float r = 0.f;
+#pragma unroll
+                for (int i = 0; i < 7; ++i) r += f[i];
+                Cur[p.mob_index[m] * bd] = (double)r;
+            }
+            for (int s = 0; s < p.S; ++s)
+                if (p.mob_slot[s] < 0) Cur[s * bd] = k.imm[(int64_t)s * N + n];
+            nonconv += reaction_chain<NC>(k, n, cls, Cur, App, Ct, R, B, BR, bd);
+#pragma unroll
+            for (int m = 0; m < NMOB; ++m) dC[m] = (float)App[p.mob_index[m] * bd];
+            for (int s = 0; s < p.S; ++s)
+                if (p.mob_slot[s] < 0 && App[s * bd] != 0.0) k.imm[(int64_t)s * N + n] += App[s * bd];
+        }
+        // pass 2: collide, add t_i*dC, stream
+        const float ux = k.u[n], uy = k.u[N + n], uz = k.u[2 * N + n];
+        const bool adj = (x == 1 || x == k.g.nx - 2);
+#pragma unroll
+        for (int m = 0; m < NMOB; ++m) {
+            float* pm = k.pop + (int64_t)m * 7 * N;
+            float f[7];
+            gather7<PARITY>(pm, k.g, n, x, y, z, f);
+            float rho = 0.f;
+            if (dyn != NODYN) {
+                const float om = (dyn == BIO) ? p.omega_bio[m] : p.omega_pore[m];
+                collide7(f, om, ux, uy, uz, rho);
+                const float d = dC[m];
+                if (d != 0.f) {
+#pragma unroll
+                    for (int i = 0; i < 7; ++i) f[i] += t7(i) * d;
+                }
+            } else if (adj) {
+#pragma unroll
+                for (int i = 0; i < 7; ++i) rho += f[i];
+            }
+            if (adj) {
+                const int side = (x == 1) ? 0 : 1;
+                k.rho_adj[((int64_t)m * 2 + side) * plane + (n - (int64_t)x * plane)] = rho;
+            }
+            scatter7<PARITY>(pm, k.g, n, x, y, z, f);
+        }
+    }
+    if (nonconv) atomicAdd(&k.counters[0], nonconv);
+}
+
+// x = 0 and x = nx-1: AdvectionDiffusionBoundaryDynamics (the one unknown
+// population = prescribed density - the six known ones) then BGK collide.
+template <int NMOB, int PARITY>
+__global__ void __launch_bounds__(256) ade_boundary_kernel(AdeK k) {
+    const AdeParams& p = k.p;
+    const int64_t N = k.g.N, plane = k.g.plane;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < 2 * plane; q += stride) {
+        const int side = q >= plane ? 1 : 0;
+        const int64_t p2 = q - side * plane;
+        const int64_t n = side ? (N - plane + p2) : p2;
+        const uint8_t dyn = k.cls[n] & 3;
+        if (dyn == BB) continue;
+        if (dyn == NODYN && !k.nodyn_coupled) continue;
+        int x, y, z;
+        decode(k.g, n, x, y, z);
+        const float ux = k.u[n], uy = k.u[N + n], uz = k.u[2 * N + n];
+#pragma unroll
+        for (int m = 0; m < NMOB; ++m) {
+            float* pm = k.pop + (int64_t)m * 7 * N;
+            float f[7];
+            gather7<PARITY>(pm, k.g, n, x, y, z, f);
+            if (dyn != NODYN) {
+                const int unk = side == 0 ? 4 : 1;
+                const int neu = side == 0 ? p.left_neu[m] : p.right_neu[m];
+                const float rb = neu ? k.rho_adj[((int64_t)m * 2 + side) * plane + p2]
+                                     : (side == 0 ? p.left_val[m] : p.right_val[m]);
+                float s = 0.f;
+#pragma unroll
+                for (int i = 0; i < 7; ++i) if (i != unk) s += f[i];
+                f[unk] = rb - s;
+                const float om = (dyn == BIO) ? p.omega_bio[m] : p.omega_pore[m];
+                float rho;
+                collide7(f, om, ux, uy, uz, rho);
+            }
+            scatter7<PARITY>(pm, k.g, n, x, y, z, f);
+        }
+    }
+}
+
+inline AdeK make_adek(Ctx* c) {
+    AdeK k;
+    k.g = c->geo;
+    k.pop = c->d_g;
+    k.cls = c->d_ade_cls;
+    k.u = c->d_u;
+    k.imm = c->d_imm;
+    k.bio = c->d_bio;
+    k.rho_adj = c->d_rho_adj;
+    k.eq_iters = c->d_eq_iters;
+    k.counters = c->d_counters;
+    k.nodyn_coupled = c->ade_nodyn_coupled ? 1 : 0;
+    k.parity = c->ade_parity;
+    k.p = c->ap;
+    eqdev_from_system(c->cfg.eq, k.e);
+    return k;
+}
+
+template <int NMOB, int NC>
+inline int launch_step(Ctx* c, const AdeK& k) {
+    const int bd = 256;
+    const int S = c->ap.S, M = c->ap.M > 0 ? c->ap.M : 1;
+    const size_t smem = (size_t)(4 * S + 2 * M) * bd * sizeof(double);
+    const int64_t interior = c->geo.N - 2 * c->geo.plane;
+    const int blocks = grid_for(interior, bd, 148 * 8);
+    int r = timing_begin(c, CL_KERNEL_ADE_MAIN);
+    if (r) return r;
+    if (c->ade_parity == 0) {
+        auto kern = ade_main_kernel<NMOB, NC, 0>;
+        CL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kern<<<blocks, bd, smem, c->stream>>>(k);
+    } else {
+        auto kern = ade_main_kernel<NMOB, NC, 1>;
+        CL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kern<<<blocks, bd, smem, c->stream>>>(k);
+    }
+    CL_LAUNCH_CHECK("ade_main_kernel");
+    if ((r = timing_end(c, CL_KERNEL_ADE_MAIN))) return r;
+    c->launches += 2;
+    const int bblocks = grid_for(2 * c->geo.plane, bd, 148 * 4);
+    if (c->ade_parity == 0) ade_boundary_kernel<NMOB, 0><<<bblocks, bd, 0, c->stream>>>(k);
+    else ade_boundary_kernel<NMOB, 1><<<bblocks, bd, 0, c->stream>>>(k);
+    CL_LAUNCH_CHECK("ade_boundary_kernel");
+    c->ade_parity ^= 1;
+    return CL_OK;
+}
+
+// one translation unit per component count instantiates these
+int ade_step_nc0(Ctx* c); int ade_step_nc1(Ctx* c); int ade_step_nc2(Ctx* c);
+int ade_step_nc3(Ctx* c); int ade_step_nc4(Ctx* c); int ade_step_nc5(Ctx* c);
+
+}  // namespace cl

@@ -1,0 +1,23 @@
+// ade_nc4.cu -- instantiations of the fused transport step with 4 equilibrium
+// components (0: no equilibrium), one translation unit per count so they build in parallel.
+#include "ade_kernels.cuh"
+
+namespace cl {
+
+int ade_step_nc4(Ctx* c) {
+    AdeK k = make_adek(c);
+    switch (c->ap.n_mob) {
+        case 1: return launch_step<1, 4>(c, k);
+        case 2: return launch_step<2, 4>(c, k);
+        case 3: return launch_step<3, 4>(c, k);
+        case 4: return launch_step<4, 4>(c, k);
+        case 5: return launch_step<5, 4>(c, k);
+        case 6: return launch_step<6, 4>(c, k);
+        case 7: return launch_step<7, 4>(c, k);
+        case 8: return launch_step<8, 4>(c, k);
+        default: set_error("the fused transport step supports 1..8 mobile solutes");
+                 return CL_ERR_ARG;
+    }
+}
+
+}  // namespace cl

@@ -1,0 +1,556 @@
+// capi.cu -- the C ABI of include/complab_gpu.h over the device context.
+#include "internal.h"
+#include <cstring>
+#include <cstdio>
+#include <vector>
+
+namespace cl {
+
+static thread_local std::string g_err;
+void set_error(const std::string& msg) { g_err = msg; }
+
+// sum the elapsed time of the recorded pairs of one kernel and free the pool
+static int fold_events(Ctx* c, int k) {
+    for (int i = 0; i < c->ev_used[k]; ++i) {
+        float ms = 0.f;
+        cudaError_t e = cudaEventSynchronize(c->ev[k][i][1]);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, c->ev[k][i][0], c->ev[k][i][1]);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaEventElapsedTime");
+        c->ev_ms[k] += ms;
+        c->ev_launches[k] += 1;
+    }
+    c->ev_used[k] = 0;
+    return CL_OK;
+}
+
+int timing_begin(Ctx* c, int k) {
+    if (!c->timing) return CL_OK;
+    if (c->ev_used[k] == Ctx::kEventPool) { int r = fold_events(c, k); if (r) return r; }
+    CL_CUDA(cudaEventRecord(c->ev[k][c->ev_used[k]][0], c->stream));
+    return CL_OK;
+}
+
+// k >= 0: close the pair opened by timing_begin; k < 0: fold kernel -1-k
+int timing_end(Ctx* c, int k) {
+    if (k < 0) return fold_events(c, -1 - k);
+    if (!c->timing) return CL_OK;
+    CL_CUDA(cudaEventRecord(c->ev[k][c->ev_used[k]][1], c->stream));
+    c->ev_used[k] += 1;
+    return CL_OK;
+}
+int cuda_fail(cudaError_t e, const char* where) {
+    g_err = std::string(where) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? CL_ERR_NOMEM : CL_ERR_CUDA;
+}
+
+static int validate(const cl_config* c) {
+    if (!c) { set_error("null config"); return CL_ERR_ARG; }
+    if (c->nx < 3 || c->ny < 1 || c->nz < 1) { set_error("lattice needs nx >= 3, ny >= 1, nz >= 1"); return CL_ERR_ARG; }
+    if (c->n_solutes < 0 || c->n_solutes > CL_MAX_SOLUTES) { set_error("n_solutes out of range"); return CL_ERR_ARG; }
+    if (c->n_microbes < 0 || c->n_microbes > CL_MAX_MICROBES) { set_error("n_microbes out of range"); return CL_ERR_ARG; }
+    if (c->n_rxn < 0 || c->n_rxn > CL_MAX_RXN) { set_error("n_rxn out of range"); return CL_ERR_ARG; }
+    if (c->n_pore_codes < 0 || c->n_pore_codes > CL_MAX_CODES || c->n_bio_codes < 0 || c->n_bio_codes > CL_MAX_CODES) {
+        set_error("material code lists out of range"); return CL_ERR_ARG;
+    }
+    if (!(c->tau_ns > 0.5)) { set_error("tau_ns must exceed 0.5"); return CL_ERR_ARG; }
+    for (int k = 0; k < c->n_rxn; ++k) {
+        const cl_rxn& r = c->rxn[k];
+        if (r.microbe >= c->n_microbes || r.n_monod < 0 || r.n_monod > CL_MAX_MONOD || r.n_mass < 0 || r.n_mass > 2) {
+            set_error("rate table entry out of range"); return CL_ERR_ARG;
+        }
+        for (int j = 0; j < r.n_monod; ++j) if (r.monod_s[j] < 0 || r.monod_s[j] >= c->n_solutes) { set_error("monod solute index"); return CL_ERR_ARG; }
+        for (int j = 0; j < r.n_mass; ++j) if (r.mass_s[j] < 0 || r.mass_s[j] >= c->n_solutes) { set_error("mass-action solute index"); return CL_ERR_ARG; }
+    }
+    if (c->use_equilibrium) {
+        const cl_eq_system& e = c->eq;
+        if (e.n_comp < 1 || e.n_comp > 5 || e.n_species != c->n_solutes) {
+            set_error("equilibrium in the transport step needs 1..5 components and one species per solute");
+            return CL_ERR_ARG;
+        }
+    }
+    return CL_OK;
+}
+
+}  // namespace cl
+
+using namespace cl;
+
+struct cl_ctx { Ctx c; };
+
+extern "C" {
+
+const char* cl_last_error(void) { return g_err.c_str(); }
+
+int cl_abi_sizes(int32_t* sizes, int32_t n) {
+    const int32_t v[5] = {(int32_t)sizeof(cl_config), (int32_t)sizeof(cl_rxn), (int32_t)sizeof(cl_eq_system),
+                          (int32_t)sizeof(cl_phase), (int32_t)sizeof(cl_surrogate_net)};
+    int k = 0;
+    for (; k < n && k < 5; ++k) sizes[k] = v[k];
+    return k;
+}
+
+cl_ctx* cl_create(const cl_config* cfg, void* stream, int* status) {
+    int st = validate(cfg);
+    if (st != CL_OK) { if (status) *status = st; return nullptr; }
+    cl_ctx* h = new cl_ctx();
+    Ctx* c = &h->c;
+    c->cfg = *cfg;
+    c->geo.nx = cfg->nx; c->geo.ny = cfg->ny; c->geo.nz = cfg->nz;
+    c->geo.plane = (int64_t)cfg->ny * cfg->nz;
+    c->geo.N = c->geo.plane * cfg->nx;
+    const int64_t N = c->geo.N;
+    auto fail = [&](int s) { if (status) *status = s; cl_destroy(h); return (cl_ctx*)nullptr; };
+    if (stream) { c->stream = (cudaStream_t)stream; c->own_stream = false; }
+    else {
+        cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return fail(cuda_fail(e, "cudaStreamCreate"));
+        c->own_stream = true;
+    }
+    // transport parameters
+    AdeParams& p = c->ap;
+    std::memset(&p, 0, sizeof p);
+    p.S = cfg->n_solutes;
+    p.n_mob = 0;
+    for (int s = 0; s < CL_MAX_SOLUTES; ++s) p.mob_slot[s] = -1;
+    for (int s = 0; s < cfg->n_solutes; ++s) {
+        if (cfg->immobile[s]) continue;
+        const int m = p.n_mob++;
+        p.mob_index[m] = s;
+        p.mob_slot[s] = m;
+        p.omega_pore[m] = (float)cfg->omega_pore[s];
+        p.omega_bio[m] = (float)cfg->omega_bio[s];
+        p.left_neu[m] = cfg->left_type[s] == CL_BC_NEUMANN;
+        p.right_neu[m] = cfg->right_type[s] == CL_BC_NEUMANN;
+        p.left_val[m] = (float)cfg->left_value[s];
+        p.right_val[m] = (float)cfg->right_value[s];
+    }
+    p.M = cfg->n_microbes;
+    p.dt = cfg->dt;
+    int n_bio = 0, n_abio = 0;
+    for (int k = 0; k < cfg->n_rxn; ++k) (cfg->rxn[k].microbe >= 0 ? n_bio : n_abio)++;
+    p.do_kin = cfg->enable_kinetics && (n_bio > 0 || cfg->n_microbes > 0);
+    p.do_abio = cfg->enable_abiotic && n_abio > 0 && cfg->n_solutes > 0;
+    p.surface_only = cfg->precip_enabled && cfg->abiotic_surface_only;
+    p.do_eq = cfg->use_equilibrium;
+    p.n_rxn = cfg->n_rxn;
+    for (int k = 0; k < cfg->n_rxn; ++k) p.rxn[k] = cfg->rxn[k];
+    for (int m = 0; m < CL_MAX_MICROBES; ++m) p.decay[m] = cfg->decay[m];
+    p.eq = cfg->eq;
+    p.solid_code = cfg->solid_code;
+    p.bb_code = cfg->bb_code;
+    // device memory
+    int r = CL_OK;
+    if ((r = dalloc(c, &c->d_mask, N)) || (r = dalloc(c, &c->d_ns_cls, N)) || (r = dalloc(c, &c->d_ade_cls, N)) ||
+        (r = dalloc(c, &c->d_f, 19 * N)) || (r = dalloc(c, &c->d_u, 3 * N)) ||
+        (r = dalloc(c, &c->d_g, (size_t)p.n_mob * 7 * N)) ||
+        (r = dalloc(c, &c->d_imm, (size_t)(p.S - p.n_mob > 0 ? p.S : 0) * N)) ||
+        (r = dalloc(c, &c->d_bio, (size_t)p.M * N)) ||
+        (r = dalloc(c, &c->d_rho_adj, (size_t)p.n_mob * 2 * c->geo.plane)) ||
+        (r = dalloc(c, &c->d_eq_iters, (size_t)(cfg->use_equilibrium ? N : 0))) ||
+        (r = dalloc(c, &c->d_counters, 8)) || (r = dalloc(c, &c->d_tracer, 1)))
+        return fail(r);
+    c->energy_blocks = grid_for(N, 256, 148 * 8);
+    if ((r = dalloc(c, &c->d_energy_part, c->energy_blocks))) return fail(r);
+    c->scratch_bytes = sizeof(double) * ((size_t)N + 65536);
+    if ((r = dalloc(c, &c->d_scratch, c->scratch_bytes / sizeof(double)))) return fail(r);
+    cudaMemsetAsync(c->d_u, 0, sizeof(float) * 3 * N, c->stream);
+    if (c->d_bio) cudaMemsetAsync(c->d_bio, 0, sizeof(double) * p.M * N, c->stream);
+    cudaMemsetAsync(c->d_counters, 0, 8 * sizeof(unsigned long long), c->stream);
+    if (c->d_eq_iters) cudaMemsetAsync(c->d_eq_iters, 0, sizeof(int32_t) * N, c->stream);
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return fail(cuda_fail(e, "cl_create"));
+    if (status) *status = CL_OK;
+    return h;
+}
+
+int cl_destroy(cl_ctx* h) {
+    if (!h) return CL_OK;
+    Ctx* c = &h->c;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    void* ptrs[] = {c->d_mask, c->d_ns_cls, c->d_ade_cls, c->d_f, c->d_u, c->d_g, c->d_imm, c->d_bio,
+                    c->d_rho_adj, c->d_eq_iters, c->d_counters, c->d_tracer, c->d_energy_part, c->d_scratch};
+    for (void* p : ptrs) if (p) cudaFree(p);
+    for (int k = 0; k < Ctx::kTimedKernels; ++k)
+        for (int i = 0; i < Ctx::kEventPool; ++i)
+            for (int j = 0; j < 2; ++j) if (c->ev[k][i][j]) cudaEventDestroy(c->ev[k][i][j]);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    delete h;
+    return CL_OK;
+}
+
+int cl_device_bytes(const cl_ctx* h, uint64_t* bytes) {
+    if (!h || !bytes) return CL_ERR_ARG;
+    *bytes = h->c.device_bytes;
+    return CL_OK;
+}
+
+int cl_upload_mask(cl_ctx* h, const uint8_t* mask) {
+    if (!h || !mask) { set_error("null argument"); return CL_ERR_ARG; }
+    Ctx* c = &h->c;
+    CL_CUDA(cudaMemcpyAsync(c->d_mask, mask, c->geo.N, cudaMemcpyHostToDevice, c->stream));
+    int r = classes_from_mask(c);
+    if (r) return r;
+    c->mask_ready = true;
+    return CL_OK;
+}
+
+int cl_download_mask(cl_ctx* h, uint8_t* mask) {
+    if (!h || !mask) { set_error("null argument"); return CL_ERR_ARG; }
+    Ctx* c = &h->c;
+    CL_CUDA(cudaMemcpyAsync(mask, c->d_mask, c->geo.N, cudaMemcpyDeviceToHost, c->stream));
+    CL_CUDA(cudaStreamSynchronize(c->stream));
+    return CL_OK;
+}
+
+int cl_flow_init(cl_ctx* h) {
+    if (!h) return CL_ERR_ARG;
+    Ctx* c = &h->c;
+    if (!c->mask_ready) { set_error("upload the mask first"); return CL_ERR_STATE; }
+    int r = flow_init(c);
+    if (r) return r;
+    c->flow_ready = true;
+    CL_CUDA(cudaStreamSynchronize(c->stream));
+    return CL_OK;
+}
+
+static int run_flow(Ctx* c, int32_t n, int use_tracer) {
+    for (int32_t i = 0; i < n; ++i) {
+        int r = flow_step(c, use_tracer);
+        if (r) return r;
+    }
+    return CL_OK;
+}
+
+int cl_flow_steps(cl_ctx* h, int32_t n) {
+    if (!h || n < 0) return CL_ERR_ARG;
+    Ctx* c = &h->c;
+    if (!c->flow_ready) { set_error("call cl_flow_init first"); return CL_ERR_STATE; }
+    int r = flow_arm_tracer(c, 0.0);
+    if (r) return r;
+    if ((r = run_flow(c, n, 0))) return r;
+    CL_CUDA(cudaStreamSynchronize(c->stream));
+    return CL_OK;
+}
+
+int cl_flow_solve(cl_ctx* h, int32_t max_it, double eps, int32_t* iters) {
+    if (!h || max_it < 0) return CL_ERR_ARG;
+    Ctx* c = &h->c;
+    if (!c->flow_ready) { set_error("call cl_flow_init first"); return CL_ERR_STATE; }
+    int r = flow_arm_tracer(c, eps);
+    if (r) return r;
+    const int chunk = 200;
+    int done = 0;
+    FlowTracer tr;
+    while (done < max_it) {
+        const int n = (max_it - done) < chunk ? (max_it - done) : chunk;
+        // launch n steps; once converged the remaining launches exit at once
+        if ((r = run_flow(c, n, 1))) return r;
+        CL_CUDA(cudaMemcpyAsync(&tr, c->d_tracer, sizeof tr, cudaMemcpyDeviceToHost, c->stream));
+        CL_CUDA(cudaStreamSynchronize(c->stream));
+        done += n;
+        if (tr.converged) break;
+    }
+    CL_CUDA(cudaMemcpyAsync(&tr, c->d_tracer, sizeof tr, cudaMemcpyDeviceToHost, c->stream));
+    CL_CUDA(cudaStreamSynchronize(c->stream));
+    // parity follows the steps actually executed
+    c->flow_parity = tr.steps_done & 1;
+    // the reference's loop counter at exit: the index of the converging step, or max_it
+    if (iters) *iters = tr.converged ? (tr.converged_at - 1) : max_it;
+    if (tr.diverged) { set_error("flow diverged (NaN energy)"); return CL_ERR_DIVERGED; }
+    return tr.converged ? CL_OK : CL_WARN_NOT_CONVERGED;
+}
+
+int cl_flow_energy(cl_ctx* h, double* energy) {
+    if (!h || !energy) return CL_ERR_ARG;
+    Ctx* c = &h->c;
+    FlowTracer tr;
+    CL_CUDA(cudaMemcpyAsync(&tr, c->d_tracer, sizeof tr, cudaMemcpyDeviceToHost, c->stream));
+    CL_CUDA(cudaStreamSynchronize(c->stream));
+    *energy = tr.last_energy;
+    return CL_OK;
+}
+
+int cl_couple_velocity(cl_ctx* h) {
+    if (!h) return CL_ERR_ARG;
+    Ctx* c = &h->c;
+    if (!c->flow_ready) { set_error("no flow field"); return CL_ERR_STATE; }
+    int r = flow_macro(c, nullptr, c->d_u, 1);
+    if (r) return r;
+    CL_CUDA(cudaStreamSynchronize(c->stream));
+    return CL_OK;
+}
+
+int cl_update_dynamics(cl_ctx* h) {
+    if (!h) return CL_ERR_ARG;
+    return update_dynamics(&h->c);
+}
+
+int cl_ade_init(cl_ctx* h) {
+    if (!h) return CL_ERR_ARG;
+    Ctx* c = &h->c;
+    if (!c->mask_ready) { set_error("upload the mask first"); return CL_ERR_STATE; }
+    int r = ade_init(c);
+    if (r) return r;
+    c->ade_ready = true;
+    CL_CUDA(cudaStreamSynchronize(c->stream));
+    return CL_OK;
+}
+
+int cl_step(cl_ctx* h, int32_t n) {
+    if (!h || n < 0) return CL_ERR_ARG;
+    Ctx* c = &h->c;
+    if (!c->ade_ready) { set_error("call cl_ade_init first"); return CL_ERR_STATE; }
+    if (c->ap.n_mob == 0) { set_error("no mobile solute"); return CL_ERR_STATE; }
+    for (int32_t i = 0; i < n; ++i) {
+        int r = ade_step(c);
+        if (r) return r;
+    }
+    unsigned long long cnt = 0;
+    CL_CUDA(cudaMemcpyAsync(&cnt, c->d_counters, sizeof cnt, cudaMemcpyDeviceToHost, c->stream));
+    CL_CUDA(cudaMemsetAsync(c->d_counters, 0, sizeof cnt, c->stream));
+    CL_CUDA(cudaStreamSynchronize(c->stream));
+    return cnt ? CL_WARN_NOT_CONVERGED : CL_OK;
+}
+
+}  // extern "C"
+
+namespace cl {
+
+__global__ void f2d_kernel(const float* a, double* b, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) b[i] = a[i];
+}
+__global__ void d2f_kernel(const double* a, float* b, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) b[i] = (float)a[i];
+}
+__global__ void i2d_kernel(const int32_t* a, double* b, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) b[i] = a[i];
+}
+// set solute populations to t_i * c at the slots that hold each site's
+// pre-collision populations for the current parity
+template <int PARITY>
+__global__ void ade_set_kernel(Geo g, float* pm, const double* c) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < g.N; n += stride) {
+        int x, y, z;
+        decode(g, n, x, y, z);
+        const float v = (float)c[n];
+#pragma unroll
+        for (int i = 0; i < 7; ++i) {
+            if (PARITY == 0) pm[i * g.N + n] = t7(i) * v;
+            else {
+                const int64_t m = nbr(g, n, x, y, z, -c7x(i), -c7y(i), -c7z(i));
+                if (m < 0) pm[i * g.N + n] = t7(i) * v;
+                else pm[opp7(i) * g.N + m] = t7(i) * v;
+            }
+        }
+    }
+}
+
+}  // namespace cl
+
+extern "C" {
+
+int cl_get_field(cl_ctx* h, int32_t field, int32_t index, double* out) {
+    if (!h || !out) { set_error("null argument"); return CL_ERR_ARG; }
+    Ctx* c = &h->c;
+    const int64_t N = c->geo.N;
+    double* d = c->d_scratch;
+    const int blocks = grid_for(N, 256, 148 * 16);
+    int r = CL_OK;
+    switch (field) {
+        case CL_FIELD_CONC:
+            if (index < 0 || index >= c->ap.S || !c->ade_ready) { set_error("bad solute / not initialised"); return CL_ERR_ARG; }
+            r = ade_density(c, index, d); break;
+        case CL_FIELD_BIOMASS:
+            if (index < 0 || index >= c->ap.M) { set_error("bad microbe"); return CL_ERR_ARG; }
+            CL_CUDA(cudaMemcpyAsync(d, c->d_bio + (int64_t)index * N, sizeof(double) * N, cudaMemcpyDeviceToDevice, c->stream));
+            break;
+        case CL_FIELD_VELOCITY:
+            if (index < 0 || index > 2) return CL_ERR_ARG;
+            f2d_kernel<<<blocks, 256, 0, c->stream>>>(c->d_u + index * N, d, N);
+            break;
+        case CL_FIELD_FLOW_RHO:
+            if (!c->flow_ready) return CL_ERR_STATE;
+            r = flow_macro(c, d, nullptr, 1); break;
+        case CL_FIELD_FLOW_U: {
+            if (index < 0 || index > 2 || !c->flow_ready) return CL_ERR_ARG;
+            // computes all three into the velocity buffer's shape in scratch (floats)
+            float* fu = reinterpret_cast<float*>(d + N / 2 + 1);
+            if (3 * N * sizeof(float) > (N / 2) * sizeof(double)) {
+                // not enough room after the output: go through the coupled-velocity buffer copy
+                float* tmp = nullptr;
+                CL_CUDA(cudaMalloc(&tmp, sizeof(float) * 3 * N));
+                r = flow_macro(c, nullptr, tmp, 1);
+                if (!r) f2d_kernel<<<blocks, 256, 0, c->stream>>>(tmp + index * N, d, N);
+                cudaStreamSynchronize(c->stream);
+                cudaFree(tmp);
+            } else {
+                r = flow_macro(c, nullptr, fu, 1);
+                if (!r) f2d_kernel<<<blocks, 256, 0, c->stream>>>(fu + index * N, d, N);
+            }
+            break;
+        }
+        case CL_FIELD_EQ_ITERS:
+            if (!c->d_eq_iters) return CL_ERR_STATE;
+            i2d_kernel<<<blocks, 256, 0, c->stream>>>(c->d_eq_iters, d, N);
+            break;
+        default: set_error("unknown field"); return CL_ERR_ARG;
+    }
+    if (r) return r;
+    CL_LAUNCH_CHECK("cl_get_field");
+    CL_CUDA(cudaMemcpyAsync(out, d, sizeof(double) * N, cudaMemcpyDeviceToHost, c->stream));
+    CL_CUDA(cudaStreamSynchronize(c->stream));
+    return CL_OK;
+}
+
+int cl_set_field(cl_ctx* h, int32_t field, int32_t index, const double* in) {
+    if (!h || !in) { set_error("null argument"); return CL_ERR_ARG; }
+    Ctx* c = &h->c;
+    const int64_t N = c->geo.N;
+    double* d = c->d_scratch;
+    const int blocks = grid_for(N, 256, 148 * 16);
+    CL_CUDA(cudaMemcpyAsync(d, in, sizeof(double) * N, cudaMemcpyHostToDevice, c->stream));
+    switch (field) {
+        case CL_FIELD_CONC: {
+            if (index < 0 || index >= c->ap.S || !c->ade_ready) { set_error("bad solute / not initialised"); return CL_ERR_ARG; }
+            const int slot = c->ap.mob_slot[index];
+            if (slot < 0) {
+                CL_CUDA(cudaMemcpyAsync(c->d_imm + (int64_t)index * N, d, sizeof(double) * N, cudaMemcpyDeviceToDevice, c->stream));
+            } else {
+                float* pm = c->d_g + (int64_t)slot * 7 * N;
+                if (c->ade_parity == 0) ade_set_kernel<0><<<blocks, 256, 0, c->stream>>>(c->geo, pm, d);
+                else ade_set_kernel<1><<<blocks, 256, 0, c->stream>>>(c->geo, pm, d);
+            }
+            break;
+        }
+        case CL_FIELD_BIOMASS:
+            if (index < 0 || index >= c->ap.M) { set_error("bad microbe"); return CL_ERR_ARG; }
+            CL_CUDA(cudaMemcpyAsync(c->d_bio + (int64_t)index * N, d, sizeof(double) * N, cudaMemcpyDeviceToDevice, c->stream));
+            break;
+        case CL_FIELD_VELOCITY:
+            if (index < 0 || index > 2) return CL_ERR_ARG;
+            d2f_kernel<<<blocks, 256, 0, c->stream>>>(d, c->d_u + index * N, N);
+            break;
+        default: set_error("field is read-only or unknown"); return CL_ERR_ARG;
+    }
+    CL_LAUNCH_CHECK("cl_set_field");
+    CL_CUDA(cudaStreamSynchronize(c->stream));
+    return CL_OK;
+}
+
+int cl_get_flow_populations(cl_ctx* h, float* out) {
+    if (!h || !out) return CL_ERR_ARG;
+    Ctx* c = &h->c;
+    const int64_t N = c->geo.N;
+    float* tmp = nullptr;
+    CL_CUDA(cudaMalloc(&tmp, sizeof(float) * 19 * N));
+    int r = flow_population_io(c, tmp, 1);
+    if (!r) {
+        cudaError_t e = cudaMemcpyAsync(out, tmp, sizeof(float) * 19 * N, cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) r = cuda_fail(e, "cl_get_flow_populations");
+    }
+    cudaFree(tmp);
+    return r;
+}
+
+int cl_set_flow_populations(cl_ctx* h, const float* in) {
+    if (!h || !in) return CL_ERR_ARG;
+    Ctx* c = &h->c;
+    const int64_t N = c->geo.N;
+    float* tmp = nullptr;
+    CL_CUDA(cudaMalloc(&tmp, sizeof(float) * 19 * N));
+    cudaError_t e = cudaMemcpyAsync(tmp, in, sizeof(float) * 19 * N, cudaMemcpyHostToDevice, c->stream);
+    int r = e == cudaSuccess ? flow_population_io(c, tmp, 0) : cuda_fail(e, "cl_set_flow_populations");
+    if (!r) { e = cudaStreamSynchronize(c->stream); if (e != cudaSuccess) r = cuda_fail(e, "sync"); }
+    cudaFree(tmp);
+    if (!r) c->flow_ready = true;
+    return r;
+}
+
+int cl_get_solute_populations(cl_ctx* h, int32_t s, float* out) {
+    if (!h || !out) return CL_ERR_ARG;
+    Ctx* c = &h->c;
+    if (s < 0 || s >= c->ap.S || c->ap.mob_slot[s] < 0) { set_error("not a mobile solute"); return CL_ERR_ARG; }
+    const int64_t N = c->geo.N;
+    float* tmp = nullptr;
+    CL_CUDA(cudaMalloc(&tmp, sizeof(float) * 7 * N));
+    int r = ade_population_io(c, c->ap.mob_slot[s], tmp);
+    if (!r) {
+        cudaError_t e = cudaMemcpyAsync(out, tmp, sizeof(float) * 7 * N, cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) r = cuda_fail(e, "cl_get_solute_populations");
+    }
+    cudaFree(tmp);
+    return r;
+}
+
+int cl_reduce(cl_ctx* h, int32_t field, int32_t index, int32_t op, double arg, double* out) {
+    if (!h || !out) { set_error("null argument"); return CL_ERR_ARG; }
+    Ctx* c = &h->c;
+    if (op == CL_RED_COUNT_EQ) return reduce_field(c, nullptr, op, arg, c->d_mask, out);
+    if (op < 0 || op > 2) return CL_ERR_ARG;
+    // materialise the field into the first N doubles of scratch, reduce from a copy region
+    double* tmp = nullptr;
+    const int64_t N = c->geo.N;
+    CL_CUDA(cudaMalloc(&tmp, sizeof(double) * N));
+    int r = CL_OK;
+    switch (field) {
+        case CL_FIELD_CONC: r = (index >= 0 && index < c->ap.S) ? ade_density(c, index, tmp) : CL_ERR_ARG; break;
+        case CL_FIELD_BIOMASS:
+            if (index < 0 || index >= c->ap.M) r = CL_ERR_ARG;
+            else { cudaError_t e = cudaMemcpyAsync(tmp, c->d_bio + (int64_t)index * N, sizeof(double) * N, cudaMemcpyDeviceToDevice, c->stream);
+                   if (e != cudaSuccess) r = cuda_fail(e, "copy"); }
+            break;
+        case CL_FIELD_FLOW_RHO: r = flow_macro(c, tmp, nullptr, 1); break;
+        default: r = CL_ERR_ARG; set_error("field not reducible");
+    }
+    if (!r) r = reduce_field(c, tmp, op, arg, nullptr, out);
+    cudaStreamSynchronize(c->stream);
+    cudaFree(tmp);
+    return r;
+}
+
+int cl_timing_enable(cl_ctx* h, int32_t on) {
+    if (!h) return CL_ERR_ARG;
+    Ctx* c = &h->c;
+    if (on && !c->ev[0][0][0]) {
+        for (int k = 0; k < Ctx::kTimedKernels; ++k)
+            for (int i = 0; i < Ctx::kEventPool; ++i)
+                for (int j = 0; j < 2; ++j) CL_CUDA(cudaEventCreate(&c->ev[k][i][j]));
+    }
+    c->timing = on != 0;
+    return CL_OK;
+}
+
+int cl_timing_read(cl_ctx* h, int32_t kernel, double* total_ms, int64_t* launches) {
+    if (!h || kernel < 0 || kernel >= Ctx::kTimedKernels) return CL_ERR_ARG;
+    Ctx* c = &h->c;
+    CL_CUDA(cudaStreamSynchronize(c->stream));
+    int r = timing_end(c, -1 - kernel);   // fold the pending pairs
+    if (r) return r;
+    if (total_ms) *total_ms = c->ev_ms[kernel];
+    if (launches) *launches = c->ev_launches[kernel];
+    c->ev_ms[kernel] = 0.0;
+    c->ev_launches[kernel] = 0;
+    return CL_OK;
+}
+
+int cl_launch_count(const cl_ctx* h, int64_t* launches) {
+    if (!h || !launches) return CL_ERR_ARG;
+    *launches = h->c.launches;
+    return CL_OK;
+}
+
+int cl_precip_convert(cl_ctx* h, int64_t* changed) {
+    if (!h || !changed) return CL_ERR_ARG;
+    return precip_convert(&h->c, changed);
+}
+
+int cl_dissol_convert(cl_ctx* h, int64_t* changed) {
+    (void)h; (void)changed;
+    set_error("dissolution node conversion is not built in this library version");
+    return CL_ERR_STATE;
+}
+
+}  // extern "C"

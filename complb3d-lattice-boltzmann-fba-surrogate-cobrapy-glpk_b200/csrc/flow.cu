@@ -1,0 +1,310 @@
+// flow.cu -- D3Q19 incompressible BGK flow on the AA pattern (rows a1-a4).
+//
+// Replaces Palabos IncBGKdynamics + collideAndStream as the reference drives it
+// (NSdomainSetup, src/complab_functions.hh:245-294; loops src/complab.cpp:596-695).
+// Populations are FP32 deviations fbar_i = f_i - t_i (the rho-1 storage the
+// reference's processors assume), one 4-byte slot per population per site:
+// 76 B read + 76 B write per fluid site per step.  The pressure boundaries on
+// the x faces (regularized density boundary) and the energy reduction that
+// drives the convergence tracer are fused into the same kernel.
+#include "internal.h"
+#include <cmath>
+
+namespace cl {
+
+struct FlowK {
+    Geo g;
+    float* f;
+    const uint8_t* cls;
+    float omega, omega_bio;
+    float rb_in, rb_out;        // rhoBar at x = 0 and x = nx-1
+    int nodyn_coupled;
+    double* part;               // per-block energy partial sums
+    const FlowTracer* tracer;   // early exit once converged (may be null)
+};
+
+// Palabos bgk_ma2_equilibrium with invRho = 1, deviation form
+__device__ __forceinline__ float feq19(int i, float rb, float jx, float jy, float jz, float jsq) {
+    float cj = c19x(i) * jx + c19y(i) * jy + c19z(i) * jz;
+    return t19(i) * (rb + 3.f * cj + 4.5f * cj * cj - 1.5f * jsq);
+}
+
+// Regularized density boundary on an x face (side -1: x = 0, +1: x = nx-1).
+// Normal momentum from the known populations, tangential momentum zero,
+// PiNeq from the known populations counting the bounce-back of the unknown
+// non-equilibrium parts, populations rebuilt as feq + t_i*9/2*Q_i:PiNeq.
+template <int SIDE>
+__device__ __forceinline__ void regularize(float* f, float rb, float& jx) {
+    float s0 = 0.f, sn = 0.f;
+#pragma unroll
+    for (int i = 0; i < 19; ++i) {
+        if (c19x(i) == 0) s0 += f[i];
+        else if (c19x(i) == SIDE) sn += f[i];
+    }
+    jx = (SIDE < 0) ? (rb - s0 - 2.f * sn) : (s0 + 2.f * sn - rb);
+    const float jsq = jx * jx;
+    float pxx = 0, pyy = 0, pzz = 0, pxy = 0, pxz = 0, pyz = 0;
+#pragma unroll
+    for (int i = 0; i < 19; ++i) {
+        if (c19x(i) == -SIDE) continue;
+        const float w = (c19x(i) == 0) ? 1.f : 2.f;
+        const float fn = w * (f[i] - feq19(i, rb, jx, 0.f, 0.f, jsq));
+        const float cx = c19x(i), cy = c19y(i), cz = c19z(i);
+        pxx += cx * cx * fn; pyy += cy * cy * fn; pzz += cz * cz * fn;
+        pxy += cx * cy * fn; pxz += cx * cz * fn; pyz += cy * cz * fn;
+    }
+#pragma unroll
+    for (int i = 0; i < 19; ++i) {
+        const float cx = c19x(i), cy = c19y(i), cz = c19z(i);
+        const float cs2 = 1.f / 3.f;
+        const float q = (cx * cx - cs2) * pxx + (cy * cy - cs2) * pyy + (cz * cz - cs2) * pzz
+                      + 2.f * (cx * cy * pxy + cx * cz * pxz + cy * cz * pyz);
+        f[i] = feq19(i, rb, jx, 0.f, 0.f, jsq) + t19(i) * 4.5f * q;
+    }
+}
+
+template <int PARITY>
+__device__ __forceinline__ void gather19(const FlowK& k, int64_t n, int x, int y, int z, float* f) {
+    const int64_t N = k.g.N;
+#pragma unroll
+    for (int i = 0; i < 19; ++i) {
+        if (PARITY == 0) {
+            f[i] = k.f[i * N + n];
+        } else {
+            int64_t m = nbr(k.g, n, x, y, z, -c19x(i), -c19y(i), -c19z(i));
+            f[i] = (m < 0) ? k.f[i * N + n] : k.f[opp19(i) * N + m];
+        }
+    }
+}
+
+template <int PARITY>
+__device__ __forceinline__ void scatter19(const FlowK& k, int64_t n, int x, int y, int z, const float* f) {
+    const int64_t N = k.g.N;
+#pragma unroll
+    for (int i = 0; i < 19; ++i) {
+        if (PARITY == 0) {
+            k.f[opp19(i) * N + n] = f[i];
+        } else {
+            int64_t m = nbr(k.g, n, x, y, z, c19x(i), c19y(i), c19z(i));
+            if (m < 0) k.f[opp19(i) * N + n] = f[i];
+            else k.f[i * N + m] = f[i];
+        }
+    }
+}
+
+template <int PARITY>
+__global__ void __launch_bounds__(256) flow_aa_kernel(FlowK k) {
+    if (k.tracer && k.tracer->converged) return;
+    double esum = 0.0;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < k.g.N; n += stride) {
+        const uint8_t cls = k.cls[n];
+        if (cls == BB) continue;                 // AA bounce-back is a no-op
+        if (cls == NODYN && !k.nodyn_coupled) continue;
+        int x, y, z;
+        decode(k.g, n, x, y, z);
+        float f[19];
+        gather19<PARITY>(k, n, x, y, z, f);
+        if (cls != NODYN) {
+            const float om = (cls == BIO) ? k.omega_bio : k.omega;
+            float rb, jx, jy = 0.f, jz = 0.f;
+            if (x == 0) { rb = k.rb_in; regularize<-1>(f, rb, jx); }
+            else if (x == k.g.nx - 1) { rb = k.rb_out; regularize<1>(f, rb, jx); }
+            else {
+                rb = 0.f; jx = 0.f;
+#pragma unroll
+                for (int i = 0; i < 19; ++i) {
+                    rb += f[i];
+                    jx += c19x(i) * f[i]; jy += c19y(i) * f[i]; jz += c19z(i) * f[i];
+                }
+            }
+            const float jsq = jx * jx + jy * jy + jz * jz;
+#pragma unroll
+            for (int i = 0; i < 19; ++i) f[i] = f[i] * (1.f - om) + om * feq19(i, rb, jx, jy, jz, jsq);
+            esum += 0.5 * (double)jsq;
+        }
+        scatter19<PARITY>(k, n, x, y, z, f);
+    }
+    // deterministic block reduction of the energy
+    __shared__ double red[8];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) esum += __shfl_down_sync(0xffffffffu, esum, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = esum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+        k.part[blockIdx.x] = s;
+    }
+}
+
+// Sum the per-block partials in a fixed order and advance the ValueTracer.
+__global__ void flow_finalize_kernel(const double* part, int nblocks, double inv_count,
+                                     FlowTracer* tr, int use_tracer) {
+    __shared__ double red[512];
+    if (tr->converged) return;
+    double s = 0.0;
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) s += part[b];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x != 0) return;
+    const double e = red[0] * inv_count;
+    tr->last_energy = e;
+    tr->steps_done += 1;
+    if (!use_tracer) return;
+    tr->window[tr->head] = e;
+    tr->head = (tr->head + 1) % 500;
+    if (tr->count < 500) tr->count += 1;
+    if (tr->count >= 500) {
+        double avg = 0.0;
+        for (int i = 0; i < 500; ++i) avg += tr->window[i];
+        avg /= 500.0;
+        double sq = 0.0;
+        for (int i = 0; i < 500; ++i) { double d = tr->window[i] - avg; sq += d * d; }
+        const double ratio = sqrt(sq / 499.0) / avg;
+        if (isnan(ratio)) { tr->diverged = 1; tr->converged = 1; tr->converged_at = tr->steps_done; }
+        else if (ratio < tr->eps) { tr->converged = 1; tr->converged_at = tr->steps_done; }
+    }
+}
+
+static FlowK make_flowk(Ctx* c) {
+    FlowK k;
+    k.g = c->geo;
+    k.f = c->d_f;
+    k.cls = c->d_ns_cls;
+    const double om = 1.0 / c->cfg.tau_ns;
+    k.omega = (float)om;
+    k.omega_bio = (float)(1.0 / (c->cfg.perm_ratio * (1.0 / om - 0.5) + 0.5));
+    k.rb_in = (float)(c->cfg.rho_in - 1.0);
+    k.rb_out = (float)(c->cfg.rho_out - 1.0);
+    k.nodyn_coupled = c->flow_nodyn_coupled ? 1 : 0;
+    k.part = c->d_energy_part;
+    k.tracer = c->d_tracer;
+    return k;
+}
+
+// initializeAtEquilibrium with the linear density profile; non-BGK sites hold 0.
+__global__ void flow_init_kernel(Geo g, float* f, const uint8_t* cls, double rho_in, double rho_out) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < g.N; n += stride) {
+        int x, y, z;
+        decode(g, n, x, y, z);
+        const uint8_t c = cls[n];
+        const bool bgk = (c == FLUID || c == BIO);
+        const double rho = rho_in + (rho_out - rho_in) * (double)x / (double)(g.nx - 1);
+        const float rb = bgk ? (float)(rho - 1.0) : 0.f;
+#pragma unroll
+        for (int i = 0; i < 19; ++i) f[i * g.N + n] = t19(i) * rb;
+    }
+}
+
+__global__ void tracer_reset_kernel(FlowTracer* tr, double eps) {
+    tr->count = 0; tr->head = 0; tr->converged = 0; tr->diverged = 0;
+    tr->steps_done = 0; tr->converged_at = -1; tr->eps = eps; tr->last_energy = 0.0;
+}
+
+int flow_arm_tracer(Ctx* c, double eps) {
+    tracer_reset_kernel<<<1, 1, 0, c->stream>>>(c->d_tracer, eps);
+    CL_LAUNCH_CHECK("tracer_reset_kernel");
+    return CL_OK;
+}
+
+int flow_init(Ctx* c) {
+    flow_init_kernel<<<grid_for(c->geo.N, 256, 148 * 16), 256, 0, c->stream>>>(
+        c->geo, c->d_f, c->d_ns_cls, c->cfg.rho_in, c->cfg.rho_out);
+    CL_LAUNCH_CHECK("flow_init_kernel");
+    c->flow_parity = 0;
+    return flow_arm_tracer(c, 0.0);
+}
+
+// One collideAndStream (two launches: the step, then the tracer update).
+int flow_step(Ctx* c, int use_tracer) {
+    FlowK k = make_flowk(c);
+    if (!use_tracer) k.tracer = nullptr;
+    const int blocks = c->energy_blocks;
+    int r = timing_begin(c, CL_KERNEL_FLOW_STEP);
+    if (r) return r;
+    if (c->flow_parity == 0) flow_aa_kernel<0><<<blocks, 256, 0, c->stream>>>(k);
+    else flow_aa_kernel<1><<<blocks, 256, 0, c->stream>>>(k);
+    CL_LAUNCH_CHECK("flow_aa_kernel");
+    if ((r = timing_end(c, CL_KERNEL_FLOW_STEP))) return r;
+    c->launches += 2;
+    const double inv = c->n_bgk > 0 ? 1.0 / (double)c->n_bgk : 0.0;
+    flow_finalize_kernel<<<1, 512, 0, c->stream>>>(c->d_energy_part, blocks, inv, c->d_tracer, use_tracer);
+    CL_LAUNCH_CHECK("flow_finalize_kernel");
+    c->flow_parity ^= 1;
+    return CL_OK;
+}
+
+// Density and momentum of every site from the current AA state
+// (Palabos computeDensity / computeVelocity; IncBGK: velocity is j).
+template <int PARITY>
+__global__ void flow_macro_kernel(FlowK k, double* rho, float* u) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < k.g.N; n += stride) {
+        int x, y, z;
+        decode(k.g, n, x, y, z);
+        const uint8_t cls = k.cls[n];
+        float f[19];
+        gather19<PARITY>(k, n, x, y, z, f);
+        float rb = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
+        const bool bgk = (cls == FLUID || cls == BIO);
+        if (bgk && x == 0) { rb = k.rb_in; regularize<-1>(f, rb, jx); }
+        else if (bgk && x == k.g.nx - 1) { rb = k.rb_out; regularize<1>(f, rb, jx); }
+        else {
+#pragma unroll
+            for (int i = 0; i < 19; ++i) {
+                rb += f[i];
+                jx += c19x(i) * f[i]; jy += c19y(i) * f[i]; jz += c19z(i) * f[i];
+            }
+            if (!bgk) { jx = jy = jz = 0.f; }
+        }
+        if (rho) rho[n] = 1.0 + (double)rb;
+        if (u) { u[n] = jx; u[k.g.N + n] = jy; u[2 * k.g.N + n] = jz; }
+    }
+}
+
+int flow_macro(Ctx* c, double* d_rho, float* d_u3, int) {
+    FlowK k = make_flowk(c);
+    const int blocks = grid_for(c->geo.N, 256, 148 * 16);
+    if (c->flow_parity == 0) flow_macro_kernel<0><<<blocks, 256, 0, c->stream>>>(k, d_rho, d_u3);
+    else flow_macro_kernel<1><<<blocks, 256, 0, c->stream>>>(k, d_rho, d_u3);
+    CL_LAUNCH_CHECK("flow_macro_kernel");
+    return CL_OK;
+}
+
+// natural-order copy of the populations (to_natural) or upload from natural
+// order (requires parity 0 afterwards).
+template <int PARITY>
+__global__ void flow_io_kernel(FlowK k, float* nat, int to_natural) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < k.g.N; n += stride) {
+        if (to_natural) {
+            int x, y, z;
+            decode(k.g, n, x, y, z);
+            float f[19];
+            gather19<PARITY>(k, n, x, y, z, f);
+#pragma unroll
+            for (int i = 0; i < 19; ++i) nat[i * k.g.N + n] = f[i];
+        } else {
+#pragma unroll
+            for (int i = 0; i < 19; ++i) k.f[i * k.g.N + n] = nat[i * k.g.N + n];
+        }
+    }
+}
+
+int flow_population_io(Ctx* c, float* d_nat, int to_natural) {
+    FlowK k = make_flowk(c);
+    const int blocks = grid_for(c->geo.N, 256, 148 * 16);
+    if (!to_natural || c->flow_parity == 0) flow_io_kernel<0><<<blocks, 256, 0, c->stream>>>(k, d_nat, to_natural);
+    else flow_io_kernel<1><<<blocks, 256, 0, c->stream>>>(k, d_nat, to_natural);
+    CL_LAUNCH_CHECK("flow_io_kernel");
+    if (!to_natural) c->flow_parity = 0;
+    return CL_OK;
+}
+
+}  // namespace cl

@@ -1,0 +1,257 @@
+// geometry.cu -- node classes from the mask, the dynamics switch after a mask
+// change, precipitation node conversion and the global reductions (rows a14,
+// a17).  All integer/byte work: results are bit-exact against the oracle.
+#include "internal.h"
+
+namespace cl {
+
+struct ClassK {
+    Geo g;
+    const uint8_t* mask;
+    uint8_t* ns;
+    uint8_t* ade;
+    int solid, bb;
+    int n_pore, pore[CL_MAX_CODES];
+    int n_bio, bio[CL_MAX_CODES];
+    int bio_is_bb;                 // perm_ratio <= 1e-14: biofilm is BounceBack for the flow
+    unsigned long long* counts;    // [0] BGK flow sites, [1] coupled flow NoDyn, [2] coupled ade NoDyn
+};
+
+__device__ __forceinline__ bool in_codes(int v, const int* list, int n) {
+    for (int i = 0; i < n; ++i) if (list[i] == v) return true;
+    return false;
+}
+
+__device__ __forceinline__ bool is_wall(const ClassK& k, int m) { return m == k.solid || m == k.bb; }
+
+// reactive: interior in x and not solid / bounce-back (processor guards of
+// run_kinetics etc.); surface: a face neighbour is solid or bounce-back
+// (surfaceAbioticKinetics3D, precipitationVOP.hh:79-90; y,z periodic here).
+__device__ uint8_t flags_for(const ClassK& k, int64_t n, int x, int y, int z) {
+    const int m = k.mask[n];
+    uint8_t fl = 0;
+    if (x > 0 && x < k.g.nx - 1 && !is_wall(k, m)) fl |= F_REACTIVE;
+    const int d6[6][3] = {{1,0,0},{-1,0,0},{0,1,0},{0,-1,0},{0,0,1},{0,0,-1}};
+    for (int d = 0; d < 6; ++d) {
+        const int64_t q = nbr(k.g, n, x, y, z, d6[d][0], d6[d][1], d6[d][2]);
+        if (q < 0) continue;
+        if (is_wall(k, k.mask[q])) { fl |= F_SURFACE; break; }
+    }
+    return fl;
+}
+
+// NSdomainSetup / soluteDomainSetup dynamics assignment (complab_functions.hh:245-340)
+__global__ void classes_kernel(ClassK k) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < k.g.N; n += stride) {
+        int x, y, z;
+        decode(k.g, n, x, y, z);
+        const int m = k.mask[n];
+        uint8_t ns = FLUID, ad = FLUID;
+        if (in_codes(m, k.pore, k.n_pore)) { ns = FLUID; ad = FLUID; }
+        if (k.bb > 0 && m == k.bb) { ns = BB; ad = BB; }
+        if (k.solid >= 0 && m == k.solid) { ns = NODYN; ad = NODYN; }
+        if (in_codes(m, k.bio, k.n_bio)) { ns = k.bio_is_bb ? BB : BIO; ad = BIO; }
+        k.ns[n] = ns;
+        k.ade[n] = ad | flags_for(k, n, x, y, z);
+    }
+}
+
+// updateNsLatticesDynamics3D (part2.hh:630-695): a site whose flow dynamics is
+// the pore IncBGK and whose mask is no longer a pore code becomes BounceBack
+// (impermeable biofilm / precipitate) or IncBGK(omega_bio); a pore-coded site
+// with any other dynamics returns to the pore IncBGK.
+// updateSoluteDynamics3D (:461-529): non-wall sites switch their solute omega
+// between pore and biofilm; wall-coded sites keep their solute dynamics.
+__global__ void update_dynamics_kernel(ClassK k) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < k.g.N; n += stride) {
+        int x, y, z;
+        decode(k.g, n, x, y, z);
+        const int m = k.mask[n];
+        const bool pore = in_codes(m, k.pore, k.n_pore);
+        uint8_t ns = k.ns[n];
+        if (!pore && ns == FLUID) ns = k.bio_is_bb ? BB : BIO;
+        else if (pore && ns != FLUID) ns = FLUID;
+        k.ns[n] = ns;
+        uint8_t ad = k.ade[n] & 3;
+        if (!is_wall(k, m) && (ad == FLUID || ad == BIO)) ad = pore ? FLUID : BIO;
+        k.ade[n] = ad | flags_for(k, n, x, y, z);
+    }
+}
+
+// Counts that steer the step kernels: BGK flow sites (energy average) and
+// whether any NoDynamics site is linked to a dynamic site (otherwise NoDynamics
+// regions are sealed behind bounce-back and need no streaming at all).
+__global__ void class_counts_kernel(ClassK k) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    unsigned long long nb = 0, cf = 0, ca = 0;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < k.g.N; n += stride) {
+        const uint8_t ns = k.ns[n], ad = k.ade[n] & 3;
+        if (ns == FLUID || ns == BIO) ++nb;
+        if (ns != NODYN && ad != NODYN) continue;
+        int x, y, z;
+        decode(k.g, n, x, y, z);
+        if (ns == NODYN) {
+            for (int i = 1; i < 19; ++i) {
+                const int64_t q = nbr(k.g, n, x, y, z, c19x(i), c19y(i), c19z(i));
+                if (q < 0) continue;
+                const uint8_t c = k.ns[q];
+                if (c == FLUID || c == BIO) { ++cf; break; }
+            }
+        }
+        if (ad == NODYN) {
+            for (int i = 1; i < 7; ++i) {
+                const int64_t q = nbr(k.g, n, x, y, z, c7x(i), c7y(i), c7z(i));
+                if (q < 0) continue;
+                const uint8_t c = k.ade[q] & 3;
+                if (c == FLUID || c == BIO) { ++ca; break; }
+            }
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        nb += __shfl_down_sync(0xffffffffu, nb, o);
+        cf += __shfl_down_sync(0xffffffffu, cf, o);
+        ca += __shfl_down_sync(0xffffffffu, ca, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (nb) atomicAdd(&k.counts[0], nb);
+        if (cf) atomicAdd(&k.counts[1], cf);
+        if (ca) atomicAdd(&k.counts[2], ca);
+    }
+}
+
+static ClassK make_classk(Ctx* c) {
+    ClassK k;
+    k.g = c->geo;
+    k.mask = c->d_mask;
+    k.ns = c->d_ns_cls;
+    k.ade = c->d_ade_cls;
+    k.solid = c->cfg.solid_code;
+    k.bb = c->cfg.bb_code;
+    k.n_pore = c->cfg.n_pore_codes;
+    k.n_bio = c->cfg.n_bio_codes;
+    for (int i = 0; i < CL_MAX_CODES; ++i) { k.pore[i] = c->cfg.pore_codes[i]; k.bio[i] = c->cfg.bio_codes[i]; }
+    k.bio_is_bb = c->cfg.perm_ratio > 1e-14 ? 0 : 1;
+    k.counts = reinterpret_cast<unsigned long long*>(c->d_scratch);
+    return k;
+}
+
+static int refresh_counts(Ctx* c, ClassK& k) {
+    CL_CUDA(cudaMemsetAsync(k.counts, 0, 3 * sizeof(unsigned long long), c->stream));
+    class_counts_kernel<<<grid_for(c->geo.N, 256, 148 * 16), 256, 0, c->stream>>>(k);
+    CL_LAUNCH_CHECK("class_counts_kernel");
+    unsigned long long h[3];
+    CL_CUDA(cudaMemcpyAsync(h, k.counts, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+    CL_CUDA(cudaStreamSynchronize(c->stream));
+    c->n_bgk = (int64_t)h[0];
+    c->flow_nodyn_coupled = h[1] > 0;
+    c->ade_nodyn_coupled = h[2] > 0;
+    return CL_OK;
+}
+
+int classes_from_mask(Ctx* c) {
+    ClassK k = make_classk(c);
+    classes_kernel<<<grid_for(c->geo.N, 256, 148 * 16), 256, 0, c->stream>>>(k);
+    CL_LAUNCH_CHECK("classes_kernel");
+    return refresh_counts(c, k);
+}
+
+int update_dynamics(Ctx* c) {
+    ClassK k = make_classk(c);
+    update_dynamics_kernel<<<grid_for(c->geo.N, 256, 148 * 16), 256, 0, c->stream>>>(k);
+    CL_LAUNCH_CHECK("update_dynamics_kernel");
+    return refresh_counts(c, k);
+}
+
+// precipNodeConversion3D (precipitationVOP.hh:158-219): a non-wall site whose
+// precipitate inventory reached max_precipRho takes the precipitate code.
+__global__ void precip_kernel(Geo g, uint8_t* mask, const double* inv, double thr, int solid, int bb,
+                              int code, unsigned long long* changed) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    unsigned long long cnt = 0;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < g.N; n += stride) {
+        const int m = mask[n];
+        if (m == solid || m == bb) continue;
+        if (inv[n] >= thr) {
+            if (m != code) ++cnt;
+            mask[n] = (uint8_t)code;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, o);
+    if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(changed, cnt);
+}
+
+int precip_convert(Ctx* c, int64_t* changed) {
+    const int s = c->cfg.precip_substrate;
+    if (s < 0 || s >= c->ap.S || c->ap.mob_slot[s] >= 0) {
+        set_error("precipitation needs an immobile precipitate substrate");
+        return CL_ERR_ARG;
+    }
+    unsigned long long* d_cnt = reinterpret_cast<unsigned long long*>(c->d_scratch);
+    CL_CUDA(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long), c->stream));
+    precip_kernel<<<grid_for(c->geo.N, 256, 148 * 16), 256, 0, c->stream>>>(
+        c->geo, c->d_mask, c->d_imm + (int64_t)s * c->geo.N, c->cfg.max_precip_rho,
+        c->cfg.solid_code, c->cfg.bb_code, c->cfg.precip_code, d_cnt);
+    CL_LAUNCH_CHECK("precip_kernel");
+    unsigned long long h = 0;
+    CL_CUDA(cudaMemcpyAsync(&h, d_cnt, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+    CL_CUDA(cudaStreamSynchronize(c->stream));
+    *changed = (int64_t)h;
+    return CL_OK;
+}
+
+// Deterministic FP64 reduction: fixed-size grid, per-block partials, one final
+// block summing them in index order.
+__global__ void reduce_part_kernel(const double* v, int64_t n, int op, double* part) {
+    __shared__ double red[256];
+    double acc = (op == CL_RED_SUM) ? 0.0 : (op == CL_RED_MIN ? 1.0 / 0.0 : -1.0 / 0.0);
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const double x = v[i];
+        acc = (op == CL_RED_SUM) ? acc + x : (op == CL_RED_MIN ? fmin(acc, x) : fmax(acc, x));
+    }
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) {
+            const double a = red[threadIdx.x], b = red[threadIdx.x + o];
+            red[threadIdx.x] = (op == CL_RED_SUM) ? a + b : (op == CL_RED_MIN ? fmin(a, b) : fmax(a, b));
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+__global__ void count_eq_kernel(const uint8_t* mask, int64_t n, int code, unsigned long long* out) {
+    unsigned long long cnt = 0;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        cnt += (mask[i] == code);
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, o);
+    if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(out, cnt);
+}
+
+int reduce_field(Ctx* c, const double* d_field, int op, double arg, const uint8_t* d_mask, double* out) {
+    if (op == CL_RED_COUNT_EQ) {
+        unsigned long long* d_cnt = reinterpret_cast<unsigned long long*>(c->d_scratch);
+        CL_CUDA(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long), c->stream));
+        count_eq_kernel<<<grid_for(c->geo.N, 256, 148 * 8), 256, 0, c->stream>>>(d_mask, c->geo.N, (int)arg, d_cnt);
+        CL_LAUNCH_CHECK("count_eq_kernel");
+        unsigned long long h = 0;
+        CL_CUDA(cudaMemcpyAsync(&h, d_cnt, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+        CL_CUDA(cudaStreamSynchronize(c->stream));
+        *out = (double)h;
+        return CL_OK;
+    }
+    const int blocks = 148 * 4;
+    double* part = c->d_scratch;
+    reduce_part_kernel<<<blocks, 256, 0, c->stream>>>(d_field, c->geo.N, op, part);
+    reduce_part_kernel<<<1, 256, 0, c->stream>>>(part, blocks, op, part + blocks);
+    CL_LAUNCH_CHECK("reduce_part_kernel");
+    CL_CUDA(cudaMemcpyAsync(out, part + blocks, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CL_CUDA(cudaStreamSynchronize(c->stream));
+    return CL_OK;
+}
+
+}  // namespace cl

@@ -1,0 +1,130 @@
+// internal.h -- context layout and kernel-launch declarations shared by the
+// translation units of libcomplab_gpu.so.  Not part of the C ABI.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include "../../include/complab_gpu.h"
+#include "lattice.cuh"
+
+namespace cl {
+
+void set_error(const std::string& msg);
+int  cuda_fail(cudaError_t e, const char* where);
+
+#define CL_CUDA(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) return ::cl::cuda_fail(e_, #call); } while (0)
+#define CL_LAUNCH_CHECK(where) do { cudaError_t e_ = cudaGetLastError(); if (e_ != cudaSuccess) return ::cl::cuda_fail(e_, where); } while (0)
+
+// Flow-convergence tracer state on the device (Palabos util::ValueTracer, window 500).
+struct FlowTracer {
+    double window[500];
+    int    count, head;
+    int    converged;      // 1 once stddev/avg < eps (or NaN)
+    int    diverged;       // NaN ratio
+    int    steps_done;     // steps executed since the tracer was armed
+    int    converged_at;   // steps_done value when it converged
+    double last_energy;
+    double eps;
+};
+
+// Per-solute transport parameters passed by value to the transport kernels.
+struct AdeParams {
+    int    S;                          // all solutes
+    int    n_mob;                      // mobile solutes
+    int    mob_index[CL_MAX_SOLUTES];  // solute index of mobile slot k
+    int    mob_slot[CL_MAX_SOLUTES];   // mobile slot of solute s, or -1 if immobile
+    float  omega_pore[CL_MAX_SOLUTES]; // per mobile slot
+    float  omega_bio[CL_MAX_SOLUTES];
+    int    left_neu[CL_MAX_SOLUTES], right_neu[CL_MAX_SOLUTES];   // per mobile slot
+    float  left_val[CL_MAX_SOLUTES], right_val[CL_MAX_SOLUTES];
+    int    M;                          // microbes
+    double dt;
+    int    do_kin, do_abio, surface_only, do_eq;
+    int    n_rxn;
+    cl_rxn rxn[CL_MAX_RXN];
+    double decay[CL_MAX_MICROBES];
+    cl_eq_system eq;
+    int    solid_code, bb_code;
+};
+
+struct Ctx {
+    cl_config cfg;
+    Geo geo;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    bool mask_ready = false, flow_ready = false, ade_ready = false;
+    // geometry
+    uint8_t* d_mask = nullptr;       // material numbers
+    uint8_t* d_ns_cls = nullptr;     // flow node class
+    uint8_t* d_ade_cls = nullptr;    // transport node class | F_REACTIVE | F_SURFACE
+    int64_t  n_bgk = 0;              // flow BGK sites (energy average denominator)
+    bool     flow_nodyn_coupled = true;   // some NoDynamics site touches a flow site
+    bool     ade_nodyn_coupled = true;
+    // flow
+    float*   d_f = nullptr;          // 19*N deviations
+    int      flow_parity = 0;        // steps done mod 2
+    double*  d_energy_part = nullptr;
+    int      energy_blocks = 0;
+    FlowTracer* d_tracer = nullptr;
+    // transport
+    AdeParams ap;
+    float*   d_g = nullptr;          // n_mob*7*N
+    int      ade_parity = 0;
+    double*  d_imm = nullptr;        // S*N (only immobile slots used)
+    double*  d_bio = nullptr;        // M*N
+    float*   d_u = nullptr;          // 3*N
+    float*   d_rho_adj = nullptr;    // n_mob*2*plane : pre-collision density next to each x face
+    int32_t* d_eq_iters = nullptr;   // N
+    unsigned long long* d_counters = nullptr;  // [0] non-converged Newton solves
+    // scratch for reductions / field IO
+    double*  d_scratch = nullptr;
+    size_t   scratch_bytes = 0;
+    uint64_t device_bytes = 0;
+    // measurement: event pairs around timed kernels, launch counter
+    static constexpr int kTimedKernels = 2, kEventPool = 512;
+    bool     timing = false;
+    cudaEvent_t ev[kTimedKernels][kEventPool][2] = {};
+    int      ev_used[kTimedKernels] = {0, 0};
+    double   ev_ms[kTimedKernels] = {0.0, 0.0};
+    int64_t  ev_launches[kTimedKernels] = {0, 0};
+    int64_t  launches = 0;
+};
+
+// event bracket around one launch of a timed kernel (no-op when timing is off)
+int timing_begin(Ctx* c, int kernel);
+int timing_end(Ctx* c, int kernel);
+
+// kernels (launchers return a CL_* status)
+int flow_init(Ctx* c);
+int flow_step(Ctx* c, int arm_tracer_flag);
+int flow_arm_tracer(Ctx* c, double eps);
+int flow_macro(Ctx* c, double* d_rho, float* d_u3, int want_bc_velocity);
+int classes_from_mask(Ctx* c);
+int ade_init(Ctx* c);
+int ade_step(Ctx* c);
+int ade_density(Ctx* c, int s, double* d_out);
+int flow_population_io(Ctx* c, float* d_natural, int to_natural);
+int ade_population_io(Ctx* c, int slot, float* d_natural);
+int precip_convert(Ctx* c, int64_t* changed);
+int update_dynamics(Ctx* c);
+int reduce_field(Ctx* c, const double* d_field, int op, double arg, const uint8_t* d_mask, double* out);
+
+// alloc helper with accounting
+template <typename T>
+inline int dalloc(Ctx* c, T** p, size_t count) {
+    size_t bytes = count * sizeof(T);
+    if (bytes == 0) { *p = nullptr; return CL_OK; }
+    cudaError_t e = cudaMalloc((void**)p, bytes);
+    if (e != cudaSuccess) { *p = nullptr; return cuda_fail(e, "cudaMalloc"); }
+    c->device_bytes += bytes;
+    return CL_OK;
+}
+
+inline int grid_for(int64_t work, int block, int max_blocks) {
+    int64_t b = (work + block - 1) / block;
+    if (b > max_blocks) b = max_blocks;
+    if (b < 1) b = 1;
+    return (int)b;
+}
+
+}  // namespace cl

@@ -1,0 +1,218 @@
+// newton.cuh -- FP64 Newton speciation for one voxel per thread (rows a10-a12).
+//
+// Restates the Newton-Raphson reserve solver of the reference
+// (src/complab3d_processors_part4_eqsolver_NR_reserve.hh:512-615):
+//   unknowns x_j = log10 of the free component concentrations,
+//   c_i = 10^(logK_i + sum_j S_ij x_j) clamped to [1e-30, 10]   (calc_species, :442-496 of the live solver)
+//   F_j = sum_i S_ij c_i - T_j                                  (calc_residual, :309-328)
+//   J   = ln10 * S^T diag(c) S                                  (calc_jacobian, :356-377)
+//   J d = -F, Armijo backtracking on ||F||_2, alpha halving, <= 40 trials (:577-598)
+// The linear solve is a Cholesky factorisation (J is symmetric positive
+// definite); the reserve uses Gaussian elimination with partial pivoting, which
+// gives the same step up to rounding.  Deviations from the reserve, shared with
+// the FP64 oracle (without them the reserve stalls on most cold starts of the
+// 5x14 random tableaux):
+//   - convergence: relative mass-balance residual max_j |F_j| / sum_i |S_ij| c_i <= tol;
+//   - species at a clamp bound contribute nothing to J;
+//   - the step is scaled so that no component moves more than 2 decades;
+//   - the Armijo merit is ||F_j / sum_i |S_ij| c_i||_2 with the current weights.
+// Species are evaluated on the fly (no per-species storage), the component
+// count NC is a template parameter so every array lives in registers.
+#pragma once
+#include "../../include/complab_gpu.h"
+
+namespace cl {
+
+struct EqDev {
+    int ns;
+    double stoich[CL_MAX_SPECIES][CL_MAX_COMP];
+    double absS[CL_MAX_SPECIES][CL_MAX_COMP];
+    double logk[CL_MAX_SPECIES];
+    int active[CL_MAX_SPECIES];
+    int comp_species[CL_MAX_COMP];
+};
+
+inline void eqdev_from_system(const cl_eq_system& s, EqDev& d) {
+    d.ns = s.n_species;
+    for (int i = 0; i < CL_MAX_SPECIES; ++i) {
+        int act = 0;
+        for (int j = 0; j < CL_MAX_COMP; ++j) {
+            double v = (i < s.n_species && j < s.n_comp) ? s.stoich[i][j] : 0.0;
+            d.stoich[i][j] = v;
+            d.absS[i][j] = v < 0 ? -v : v;
+            if (v > 1e-10 || v < -1e-10) act = 1;
+        }
+        d.active[i] = act;
+        d.logk[i] = i < s.n_species ? s.logk[i] : 0.0;
+    }
+    for (int j = 0; j < CL_MAX_COMP; ++j) d.comp_species[j] = j < s.n_comp ? s.comp_species[j] : -1;
+}
+
+// species concentration from the component logs, clamped as calc_species
+template <int NC>
+__device__ __forceinline__ double species_c(const EqDev& e, int i, const double* x) {
+    double lc = e.logk[i];
+#pragma unroll
+    for (int j = 0; j < NC; ++j) lc = fma(e.stoich[i][j], x[j], lc);
+    lc = fmin(fmax(lc, -30.0), 1.0);
+    return exp10(lc);
+}
+
+// F, and the relative residual
+template <int NC>
+__device__ __forceinline__ double eq_residual(const EqDev& e, const double* T, const double* x, double* F) {
+    double sc[NC];
+#pragma unroll
+    for (int j = 0; j < NC; ++j) { F[j] = -T[j]; sc[j] = 0.0; }
+    for (int i = 0; i < e.ns; ++i) {
+        if (!e.active[i]) continue;
+        const double c = species_c<NC>(e, i, x);
+#pragma unroll
+        for (int j = 0; j < NC; ++j) { F[j] = fma(e.stoich[i][j], c, F[j]); sc[j] = fma(e.absS[i][j], c, sc[j]); }
+    }
+    double rel = 0.0;
+#pragma unroll
+    for (int j = 0; j < NC; ++j) {
+        const double r = fabs(F[j]) / fmax(sc[j], 1e-300);
+        rel = (r > rel || r != r) ? r : rel;
+    }
+    return rel;
+}
+
+// reference cold start (solve_equilibrium_anderson, part4_eqsolver.hh:977-994)
+template <int NC>
+__device__ __forceinline__ void eq_cold_start(const EqDev& e, const double* species, double* x) {
+#pragma unroll
+    for (int j = 0; j < NC; ++j) {
+        double c = 1e-7;
+        const int idx = e.comp_species[j];
+        if (idx >= 0) c = species[idx];
+        c = fmin(fmax(c, 1e-30), 10.0);
+        x[j] = log10(c);
+    }
+}
+
+// Runs at most max_iter Newton iterations from x.  Returns the iterations
+// taken; *conv = 1 when the residual test passed.
+template <int NC>
+__device__ int eq_newton(const EqDev& e, const double* T, double* x, int max_iter, double tol, int* conv) {
+    const double ln10 = 2.302585092994046;
+    *conv = 0;
+    for (int it = 0; it < max_iter; ++it) {
+        // residual and Jacobian in one pass over the species
+        double F[NC], sc[NC], J[NC][NC];
+#pragma unroll
+        for (int a = 0; a < NC; ++a) {
+            F[a] = -T[a]; sc[a] = 0.0;
+#pragma unroll
+            for (int b = 0; b < NC; ++b) J[a][b] = 0.0;
+        }
+        for (int i = 0; i < e.ns; ++i) {
+            if (!e.active[i]) continue;
+            double lc = e.logk[i];
+#pragma unroll
+            for (int j = 0; j < NC; ++j) lc = fma(e.stoich[i][j], x[j], lc);
+            const bool clamped = (lc > 1.0) || (lc < -30.0);
+            const double c = exp10(fmin(fmax(lc, -30.0), 1.0));
+            const double cj = clamped ? 0.0 : c;
+#pragma unroll
+            for (int a = 0; a < NC; ++a) {
+                const double sa = e.stoich[i][a];
+                F[a] = fma(sa, c, F[a]);
+                sc[a] = fma(e.absS[i][a], c, sc[a]);
+                const double sac = sa * cj;
+#pragma unroll
+                for (int b = 0; b <= a; ++b) J[a][b] = fma(sac, e.stoich[i][b], J[a][b]);
+            }
+        }
+        double rel = 0.0, fn = 0.0, w[NC];
+#pragma unroll
+        for (int a = 0; a < NC; ++a) {
+            w[a] = 1.0 / fmax(sc[a], 1e-300);
+            const double r = fabs(F[a]) * w[a];
+            rel = (r > rel || r != r) ? r : rel;
+            fn = fma(r, r, fn);
+        }
+        if (rel <= tol) { *conv = 1; return it; }
+        if (!(rel < 1e300)) return it;       // NaN / inf
+        fn = sqrt(fn);
+        // Cholesky of ln10*J (lower triangle), solve L L^T d = -F
+        double L[NC][NC];
+        bool ok = true;
+#pragma unroll
+        for (int a = 0; a < NC; ++a) {
+#pragma unroll
+            for (int b = 0; b <= a; ++b) {
+                double s = ln10 * J[a][b];
+#pragma unroll
+                for (int k = 0; k < b; ++k) s -= L[a][k] * L[b][k];
+                if (a == b) {
+                    if (!(s > 1e-300)) { ok = false; s = 1.0; }
+                    L[a][a] = sqrt(s);
+                } else {
+                    L[a][b] = s / L[b][b];
+                }
+            }
+        }
+        if (!ok) return it + 1;
+        double d[NC];
+#pragma unroll
+        for (int a = 0; a < NC; ++a) {
+            double s = -F[a];
+#pragma unroll
+            for (int k = 0; k < a; ++k) s -= L[a][k] * d[k];
+            d[a] = s / L[a][a];
+        }
+#pragma unroll
+        for (int a = NC - 1; a >= 0; --a) {
+            double s = d[a];
+#pragma unroll
+            for (int k = a + 1; k < NC; ++k) s -= L[k][a] * d[k];
+            d[a] = s / L[a][a];
+        }
+        // step cap (2 decades), then Armijo backtracking on the weighted residual
+        double dmax = 0.0;
+#pragma unroll
+        for (int a = 0; a < NC; ++a) dmax = fmax(dmax, fabs(d[a]));
+        if (dmax > 2.0) {
+            const double sfac = 2.0 / dmax;
+#pragma unroll
+            for (int a = 0; a < NC; ++a) d[a] *= sfac;
+        }
+        double alpha = 1.0, xt[NC];
+        for (int ls = 0; ls < 40; ++ls) {
+#pragma unroll
+            for (int a = 0; a < NC; ++a) xt[a] = fmin(fmax(fma(alpha, d[a], x[a]), -30.0), 1.0);
+            double Ft[NC];
+            eq_residual<NC>(e, T, xt, Ft);
+            double fnt = 0.0;
+#pragma unroll
+            for (int a = 0; a < NC; ++a) { const double r = Ft[a] * w[a]; fnt = fma(r, r, fnt); }
+            fnt = sqrt(fnt);
+            if (fnt < fn * (1.0 - 1e-4 * alpha) || alpha < 1e-15) break;
+            alpha *= 0.5;
+        }
+#pragma unroll
+        for (int a = 0; a < NC; ++a) x[a] = xt[a];
+    }
+    double Fe[NC];
+    if (eq_residual<NC>(e, T, x, Fe) <= tol) *conv = 1;
+    return max_iter;
+}
+
+// component totals (calc_component_totals, part4_eqsolver.hh:520-538)
+template <int NC>
+__device__ __forceinline__ void eq_totals(const EqDev& e, const double* species, double* T) {
+#pragma unroll
+    for (int j = 0; j < NC; ++j) T[j] = 0.0;
+    for (int i = 0; i < e.ns; ++i) {
+        if (!e.active[i]) continue;
+        const double c = fmin(fmax(species[i], 1e-30), 10.0);
+#pragma unroll
+        for (int j = 0; j < NC; ++j) T[j] = fma(e.stoich[i][j], c, T[j]);
+    }
+#pragma unroll
+    for (int j = 0; j < NC; ++j) T[j] = fmax(T[j], 1e-30);
+}
+
+}  // namespace cl

@@ -1,0 +1,222 @@
+"""Seeded synthetic inputs with the shapes and value distributions of the five
+benchmark workloads (the reference ships no dataset; all inputs are generated).
+
+- sphere_pack: random overlapping spheres until the porosity target, y/z
+  periodic; solid voxels linked to a pore voxel by any D3Q19 direction become
+  bounce-back (material 1), other solids NoDynamics (material 0), pores 2.  The
+  x planes 0 and nx-1 copy planes 1 and nx-2, as readGeometry does
+  (src/complab_functions.hh:127-156).
+- tableau / speciation_batch: components-and-species systems with integer
+  stoichiometry in [-2, 2] and log10 K uniform in [-14, 14], and well-posed
+  component totals drawn by sampling the free-component logs first.
+- the configuration builders of the 64^3 flow+transport case, the 128^3
+  biotic case, and the 256x256x512 coupled case.
+"""
+import numpy as np
+
+MAT_SOLID, MAT_BB, MAT_PORE, MAT_BIO = 0, 1, 2, 3
+
+D3Q19 = [(0, 0, 0), (-1, 0, 0), (0, -1, 0), (0, 0, -1), (-1, -1, 0), (-1, 1, 0), (-1, 0, -1), (-1, 0, 1),
+         (0, -1, -1), (0, -1, 1), (1, 0, 0), (0, 1, 0), (0, 0, 1), (1, 1, 0), (1, -1, 0), (1, 0, 1), (1, 0, -1),
+         (0, 1, 1), (0, 1, -1)]
+
+
+def sphere_pack(nx, ny, nz, porosity, rmin, rmax, seed, max_spheres=10_000_000):
+    """Material numbers (uint8, shape (nx, ny, nz)).  nx includes the two x
+    boundary planes; spheres are placed in the interior planes 1..nx-2."""
+    rng = np.random.default_rng(seed)
+    nxi = nx - 2
+    solid = np.zeros((nxi, ny, nz), bool)
+    total = solid.size
+    n_solid = 0
+    target = (1.0 - porosity) * total
+    placed = 0
+    while n_solid < target and placed < max_spheres:
+        cx, cy, cz = rng.uniform(0, nxi), rng.uniform(0, ny), rng.uniform(0, nz)
+        r = rng.uniform(rmin, rmax)
+        ir = int(np.ceil(r))
+        xs = np.arange(int(np.floor(cx - ir)), int(np.ceil(cx + ir)) + 1)
+        xs = xs[(xs >= 0) & (xs < nxi)]
+        ys = np.arange(int(np.floor(cy - ir)), int(np.ceil(cy + ir)) + 1)
+        zs = np.arange(int(np.floor(cz - ir)), int(np.ceil(cz + ir)) + 1)
+        if xs.size == 0:
+            placed += 1
+            continue
+        X, Y, Z = np.meshgrid(xs, ys, zs, indexing="ij")
+        inside = (X + 0.5 - cx) ** 2 + (Y + 0.5 - cy) ** 2 + (Z + 0.5 - cz) ** 2 <= r * r
+        Xi, Yi, Zi = X[inside], Y[inside] % ny, Z[inside] % nz
+        before = solid[Xi, Yi, Zi]
+        n_solid += int((~before).sum())
+        solid[Xi, Yi, Zi] = True
+        placed += 1
+    mat = np.full((nx, ny, nz), MAT_PORE, np.uint8)
+    mat[1:nx - 1][solid] = MAT_SOLID
+    mat[0] = mat[1]
+    mat[nx - 1] = mat[nx - 2]
+    return mark_bounce_back(mat)
+
+
+def mark_bounce_back(mat):
+    """Solids with a pore/biofilm neighbour along any D3Q19 link become bounce-back."""
+    fluid = (mat != MAT_SOLID) & (mat != MAT_BB)
+    near = np.zeros_like(fluid)
+    nx = mat.shape[0]
+    for (dx, dy, dz) in D3Q19[1:]:
+        sh = np.roll(np.roll(fluid, dy, axis=1), dz, axis=2)
+        if dx == 1:
+            near[1:] |= sh[:-1]
+        elif dx == -1:
+            near[:-1] |= sh[1:]
+        else:
+            near |= sh
+    out = mat.copy()
+    out[(mat == MAT_SOLID) & near] = MAT_BB
+    return out
+
+
+def channel(nx, ny, nz):
+    """Plane channel: walls at y = 0 and y = ny-1 (bounce-back), pore between."""
+    mat = np.full((nx, ny, nz), MAT_PORE, np.uint8)
+    mat[:, 0, :] = MAT_BB
+    mat[:, ny - 1, :] = MAT_BB
+    return mat
+
+
+# ---------------------------------------------------------------- speciation
+def tableau(n_comp=5, n_secondary=9, seed=4, stoich_range=2, logk_range=14.0, ph_comp=None):
+    """(stoich (ns x nc), logk (ns,), comp_species) with the components first as
+    identity rows (logK 0), then secondary species with integer stoichiometry
+    and logK ~ U[-logk_range, logk_range].  The pH-like component (the last one
+    by default) takes coefficients in [-stoich_range, stoich_range]; the others
+    in [0, stoich_range], as in real tableaux where only the proton carries
+    negative coefficients.  With negative coefficients on every column almost
+    no draw has all component totals positive, which the reference requires
+    (totals are floored at 1e-30, part4_eqsolver.hh:535)."""
+    rng = np.random.default_rng(seed)
+    if ph_comp is None:
+        ph_comp = n_comp - 1
+    ns = n_comp + n_secondary
+    S = np.zeros((ns, n_comp))
+    S[:n_comp] = np.eye(n_comp)
+    for i in range(n_comp, ns):
+        while True:
+            row = rng.integers(0, stoich_range + 1, n_comp).astype(float)
+            row[ph_comp] = rng.integers(-stoich_range, stoich_range + 1)
+            others = np.delete(row, ph_comp)
+            if np.count_nonzero(others) >= 1 and np.abs(row).sum() >= 2:
+                break
+        S[i] = row
+    logk = np.zeros(ns)
+    logk[n_comp:] = rng.uniform(-logk_range, logk_range, n_secondary)
+    return S, logk, list(range(n_comp))
+
+
+def speciation_batch(S, logk, n, seed, ph_comp=None, tot_lo=1e-6, tot_hi=1e-1, h_lo=1e-9, h_hi=1e-5,
+                     max_log_c=0.5):
+    """Well-posed batch: sample free-component logs x*, form c* = 10^(logK + S x*)
+    and totals T = S^T c*; keep samples with no clamp active (all species in
+    [1e-30, 10^max_log_c]) and every total positive, non-pH totals within
+    [tot_lo, tot_hi].  Returns (totals (n x nc), x* (n x nc), species c* (n x ns),
+    acceptance rate)."""
+    rng = np.random.default_rng(seed)
+    ns, nc = S.shape
+    if ph_comp is None:
+        ph_comp = nc - 1
+    keep_T, keep_x, keep_c = [], [], []
+    got, drawn = 0, 0
+    while got < n:
+        m = max(4 * (n - got), 4096)
+        x = rng.uniform(np.log10(tot_lo) - 1.0, np.log10(tot_hi), (m, nc))
+        x[:, ph_comp] = rng.uniform(np.log10(h_lo), np.log10(h_hi), m)
+        lc = logk[None, :] + x @ S.T
+        ok = (lc <= max_log_c).all(1) & (lc >= -30).all(1)
+        c = 10.0 ** np.clip(lc, -30, 1)
+        T = c @ S
+        ok &= (T > 0).all(1)
+        others = [j for j in range(nc) if j != ph_comp]
+        ok &= ((T[:, others] >= tot_lo) & (T[:, others] <= tot_hi)).all(1)
+        drawn += m
+        idx = np.nonzero(ok)[0][: n - got]
+        keep_T.append(T[idx]); keep_x.append(x[idx]); keep_c.append(c[idx])
+        got += idx.size
+        if drawn > 200 * n + 10_000_000:
+            raise RuntimeError("tableau gives too few well-posed samples")
+    return (np.concatenate(keep_T), np.concatenate(keep_x), np.concatenate(keep_c), got / drawn)
+
+
+def seed_biomass(mask, seed, frac=0.02, lo=10.0, hi=50.0):
+    """Biomass density U[lo, hi] on `frac` of the pore voxels that touch a wall."""
+    rng = np.random.default_rng(seed)
+    pore = mask == MAT_PORE
+    wall = (mask == MAT_SOLID) | (mask == MAT_BB)
+    near = np.zeros_like(pore)
+    for ax in range(3):
+        for sh in (1, -1):
+            near |= np.roll(wall, sh, axis=ax)
+    cand = pore & near
+    cand[0] = False
+    cand[-1] = False
+    pick = cand & (rng.random(mask.shape) < frac)
+    b = np.zeros(mask.shape)
+    b[pick] = rng.uniform(lo, hi, int(pick.sum()))
+    return b
+
+
+# solutes of the coupled workload
+COUPLED_SOLUTES = ["DOC", "O2", "NO3-", "HCO3-", "Ca2+", "H+", "CO3--", "CaCO3(aq)", "CaCO3(s)"]
+
+
+def coupled_config(pkg, nx, ny, nz, seed=5):
+    """Flow + 8 mobile solutes + 1 immobile mineral:
+      kinetics   dual-Monod oxidation of DOC by O2 and by NO3- (one sessile
+                 microbe), Vmax ~ U[1e-5, 1e-4], Ks ~ U[1e-3, 1e-1] per step;
+      speciation components HCO3-, Ca2+, H+ with CO3-- (logK -10.33) and
+                 CaCO3(aq) (logK -7.13) as secondary species, Newton to a 1e-10
+                 relative residual every step in every pore voxel;
+      precipitation Ca2+ + CO3-- -> CaCO3(s), rate 1e-6 [Ca][CO3], on wall-
+                 adjacent voxels only; a voxel whose inventory reaches 1.0
+                 becomes solid (node conversion every 200 steps)."""
+    rng = np.random.default_rng(seed)
+    taus = rng.uniform(0.6, 0.9, 8)
+    inlet = [2e-3, 2.5e-4, 5e-4, 2e-3, 1e-3, 1e-7, 1e-30, 1e-30]
+    c0 = [1e-3, 2.5e-4, 1e-4, 2e-3, 1e-3, 1e-7, 1e-30, 1e-30]
+    sol = [{"tau": float(taus[s]), "c0": c0[s], "left": "D", "left_value": inlet[s], "right": "N"} for s in range(8)]
+    sol.append({"immobile": True, "c0": 0.0})
+    cfg = pkg.make_config(nx, ny, nz, tau_ns=0.8, rho_in=1.0005, rho_out=1.0, solutes=sol, microbes=1, dt=1.0)
+    vmax = rng.uniform(1e-5, 1e-4, 2)
+    ks = rng.uniform(1e-3, 1e-1, 3)
+    cfg.enable_kinetics = 1
+    pkg.add_rxn(cfg, microbe=0, k=float(vmax[0]), monod=[(0, float(ks[0])), (1, float(ks[1]))],
+                nu={0: -1.0, 1: -1.0, 3: 1.0}, yield_=0.3)
+    pkg.add_rxn(cfg, microbe=0, k=float(vmax[1]), monod=[(0, float(ks[0])), (2, float(ks[2]))],
+                nu={0: -1.0, 2: -0.8, 3: 1.0}, yield_=0.2)
+    cfg.decay[0] = 1e-7
+    cfg.enable_abiotic = 1
+    cfg.precip_enabled = 1
+    cfg.abiotic_surface_only = 1
+    cfg.precip_substrate = 8
+    cfg.max_precip_rho = 1.0
+    cfg.precip_code = MAT_SOLID
+    pkg.add_rxn(cfg, k=1e-6, mass=[4, 6], nu={4: -1.0, 6: -1.0, 8: 1.0})
+    cfg.use_equilibrium = 1
+    S = np.zeros((9, 3))
+    S[3, 0] = 1; S[4, 1] = 1; S[5, 2] = 1
+    S[6] = [1, 0, -1]
+    S[7] = [1, 1, -1]
+    logk = [0, 0, 0, 0, 0, 0, -10.33, -7.13, 0]
+    pkg.set_eq_system(cfg.eq, S, logk, [3, 4, 5], max_iter=100, tol=1e-10, warm_iter=8)
+    return cfg
+
+
+def cold_species(S, T, comp_species=None):
+    """Species vector a voxel would hold before equilibration: each component's
+    own species at its total (the reference's cold start reads these), every
+    other species at the floor."""
+    n = T.shape[0]
+    ns, nc = S.shape
+    c = np.full((n, ns), 1e-30)
+    cs = comp_species if comp_species is not None else list(range(nc))
+    for j in range(nc):
+        if cs[j] >= 0:
+            c[:, cs[j]] = T[:, j]
+    return c

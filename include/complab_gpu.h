@@ -1,0 +1,308 @@
+/*
+ * complab_gpu.h -- C ABI of the B200 (sm_100a) implementation of CompLB3D's
+ * per-timestep hot path.
+ *
+ * The reference drives its hot path through Palabos data processors
+ * (`applyProcessingFunctional(new X(...), box, latticeVector)`,
+ * src/complab.cpp:1152-1860) over FP64 AoS lattices.  This header replaces
+ * that processor surface with plain C entry points over a device-resident
+ * context: plain pointers and sizes, no C++ or torch types, an int status on
+ * every call (0 = ok, < 0 = error, > 0 = soft warning such as "some Newton
+ * solves fell back or did not converge").  Nothing traps on the device; every
+ * device loop is bounded and reports through a status word.
+ *
+ * Data conventions
+ *   - Site index n = (x*ny + y)*nz + z   (x slowest, z fastest).  This is the
+ *     reader order of the reference's geometry file (x-slices, each slice
+ *     y-major then z; src/complab_functions.hh:127-156).
+ *   - nx INCLUDES the inlet (x=0) and outlet (x=nx-1) planes, as the reference
+ *     does after `nx += 2` (src/complab_functions.hh:769).
+ *   - y and z are periodic.
+ *   - Host buffers are owned by the caller, device memory by the context.
+ *   - All calls are synchronous on the context's stream unless they say
+ *     otherwise.  One context per GPU; a context is not thread-safe.
+ */
+#ifndef COMPLAB_GPU_H
+#define COMPLAB_GPU_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CL_MAX_SOLUTES   16
+#define CL_MAX_MICROBES  4
+#define CL_MAX_RXN       16
+#define CL_MAX_MONOD     3
+#define CL_MAX_COMP      8
+#define CL_MAX_SPECIES   16
+#define CL_MAX_CODES     8
+#define CL_MAX_PHASES    4
+
+/* status codes */
+#define CL_OK                 0
+#define CL_WARN_NOT_CONVERGED 1   /* soft: a bounded loop ended before its tolerance */
+#define CL_ERR_ARG          (-1)  /* bad argument (null pointer, size out of range) */
+#define CL_ERR_CUDA         (-2)  /* a CUDA runtime call failed */
+#define CL_ERR_STATE        (-3)  /* call out of order (e.g. step before mask upload) */
+#define CL_ERR_NOMEM        (-4)  /* device allocation failed */
+#define CL_ERR_DIVERGED     (-5)  /* NaN in a convergence tracer (reference: "simulation diverged") */
+
+/* boundary types of a solute on an x face (reference <left_boundary_type>) */
+#define CL_BC_DIRICHLET   0
+#define CL_BC_NEUMANN     1       /* zero gradient: FlatAdiabaticBoundaryFunctional3D */
+
+/* One table-driven rate expression.  It covers the shipped example rate laws
+ * (e.g. examples/05_biotic_cellular_automaton/defineKinetics.hh:57-86,
+ *  examples/13_precipitation/defineAbioticKinetics.hh:39-58) and the dual-Monod
+ * law of the 128^3 biotic workload:
+ *   r = k * (B_m if microbe >= 0) * prod_j C[monod_s[j]]/(Ks[j] + C[monod_s[j]])
+ *         * prod_j C[mass_s[j]]
+ *   subsR[s] += nu[s] * r ;  bioR[microbe] += yield * r                      */
+typedef struct {
+    int32_t microbe;                   /* -1 = abiotic */
+    int32_t n_monod;
+    int32_t monod_s[CL_MAX_MONOD];
+    double  monod_ks[CL_MAX_MONOD];
+    int32_t n_mass;
+    int32_t mass_s[2];
+    double  k;
+    double  nu[CL_MAX_SOLUTES];
+    double  yield;
+} cl_rxn;
+
+/* Components-and-species tableau (reference EquilibriumChemistry<T>,
+ * src/complab3d_processors_part4_eqsolver.hh:186-1271).  Species are the
+ * solutes in order; rows of all zeros are non-equilibrium species. */
+typedef struct {
+    int32_t n_comp;
+    int32_t n_species;                 /* == number of solutes it acts on */
+    int32_t comp_species[CL_MAX_COMP]; /* species index named like component j, or -1 */
+    double  stoich[CL_MAX_SPECIES][CL_MAX_COMP];
+    double  logk[CL_MAX_SPECIES];
+    int32_t max_iter;                  /* Newton iterations (cold) */
+    double  tol;                       /* relative mass-balance residual */
+    int32_t warm_iter;                 /* k: Newton iterations allowed from the learned start */
+} cl_eq_system;
+
+/* Dissolvable solid phase (reference SolidPhase, src/dissolutionVOP.hh:142-154) */
+typedef struct {
+    int32_t id;
+    int32_t material;
+    int32_t substrate;                 /* immobile solute holding its inventory */
+    double  full_density;
+    /* first-order dissolution law: rate = -k_dis * mineral * (1 - C[sat_s]/c_sat),
+     * products nu_prod[s] * (-rate) scattered to open faces */
+    double  k_dis;
+    int32_t sat_s;
+    double  c_sat;
+    double  nu_prod[CL_MAX_SOLUTES];
+} cl_phase;
+
+typedef struct {
+    /* lattice */
+    int32_t nx, ny, nz;
+    /* material numbers (reference <material_numbers>) */
+    int32_t solid_code;                /* NoDynamics (<solid>) */
+    int32_t bb_code;                   /* BounceBack (<bounce_back>) */
+    int32_t n_pore_codes;
+    int32_t pore_codes[CL_MAX_CODES];
+    int32_t n_bio_codes;
+    int32_t bio_codes[CL_MAX_CODES];
+    /* flow (D3Q19 incompressible BGK) */
+    double  tau_ns;
+    double  perm_ratio;                /* biofilm permeability ratio X (<= 1e-14: biofilm is bounce-back) */
+    double  rho_in, rho_out;           /* densities at x=0 and x=nx-1 */
+    /* solutes (D3Q7 advection-diffusion BGK) */
+    int32_t n_solutes;
+    double  omega_pore[CL_MAX_SOLUTES];
+    double  omega_bio[CL_MAX_SOLUTES];
+    int32_t immobile[CL_MAX_SOLUTES];
+    int32_t left_type[CL_MAX_SOLUTES], right_type[CL_MAX_SOLUTES];
+    double  left_value[CL_MAX_SOLUTES], right_value[CL_MAX_SOLUTES];
+    double  c0[CL_MAX_SOLUTES];
+    /* sessile biomass, one scalar field per microbe */
+    int32_t n_microbes;
+    double  b_max;                     /* <max_biomass_density> (CA trigger) */
+    double  thrd_bfilm_frac;           /* <thrd_biofilm_fraction> */
+    double  dt;                        /* ade_dt, seconds per transport step */
+    /* reactions */
+    int32_t enable_kinetics;
+    int32_t enable_abiotic;
+    int32_t abiotic_surface_only;      /* <precipitation><surface_only> */
+    int32_t n_rxn;
+    cl_rxn  rxn[CL_MAX_RXN];
+    double  decay[CL_MAX_MICROBES];    /* kd, 1/s */
+    int32_t use_equilibrium;
+    cl_eq_system eq;
+    /* precipitation / dissolution (reference src/precipitationVOP.hh, src/dissolutionVOP.hh) */
+    int32_t precip_enabled;
+    int32_t precip_substrate;          /* immobile solute holding the precipitate */
+    double  max_precip_rho;
+    int32_t precip_code;               /* mask code a full voxel becomes */
+    int32_t precip_phase_id;
+    int32_t dissol_enabled;
+    double  reopen_fraction;
+    int32_t dissol_surface_only;
+    int32_t n_phases;
+    cl_phase phases[CL_MAX_PHASES];
+} cl_config;
+
+typedef struct cl_ctx cl_ctx;
+
+/* ---- context ---------------------------------------------------------------
+ * Replaces the lattice construction of src/complab.cpp:588-884 and the dynamics
+ * assignment of NSdomainSetup / soluteDomainSetup (src/complab_functions.hh:245-340).
+ * `stream` is a cudaStream_t (may be NULL: the context creates its own). */
+cl_ctx* cl_create(const cl_config* cfg, void* stream, int* status);
+int     cl_destroy(cl_ctx* ctx);
+const char* cl_last_error(void);
+int     cl_device_bytes(const cl_ctx* ctx, uint64_t* bytes);
+/* sizeof of the ABI structs, for binding checks: [cl_config, cl_rxn,
+ * cl_eq_system, cl_phase, cl_surrogate_net]; returns how many were written */
+int     cl_abi_sizes(int32_t* sizes, int32_t n);
+
+/* geometry: one material number per site, 0..255 (readGeometry, src/complab_functions.hh:127-156) */
+int cl_upload_mask(cl_ctx* ctx, const uint8_t* mask);
+int cl_download_mask(cl_ctx* ctx, uint8_t* mask);
+
+/* ---- flow (rows a1-a4) -------------------------------------------------------
+ * cl_flow_init:  initializeAtEquilibrium with the linear PressureGradient profile
+ *                (src/complab_functions.hh:72-84,285-290).
+ * cl_flow_steps: n collideAndStream steps (src/complab.cpp:607-620).
+ * cl_flow_solve: collideAndStream until the ValueTracer(1, 1000, eps) on the
+ *                average energy converges, at most max_it steps
+ *                (src/complab.cpp:593,607-611).  *iters = the step index at
+ *                which it converged (reference's iT), or max_it.
+ * cl_couple_velocity: latticeToPassiveAdvDiff (src/complab.cpp:1097-1109). */
+int cl_flow_init(cl_ctx* ctx);
+int cl_flow_steps(cl_ctx* ctx, int32_t n);
+int cl_flow_solve(cl_ctx* ctx, int32_t max_it, double eps, int32_t* iters);
+int cl_flow_energy(cl_ctx* ctx, double* energy);
+int cl_couple_velocity(cl_ctx* ctx);
+/* NS dynamics switch after a mask change (updateNsLatticesDynamics3D,
+ * src/complab3d_processors_part2.hh:630-695) and the solute omega switch
+ * (updateSoluteDynamics3D, :461-529). */
+int cl_update_dynamics(cl_ctx* ctx);
+
+/* ---- transport step (rows a5-a12) ---------------------------------------------
+ * cl_ade_init: initializeAtEquilibrium(c0, u=0) for every solute
+ *              (src/complab_functions.hh:334-336).
+ * cl_step:     n transport steps in the reference's order (src/complab.cpp:1252-1374,
+ *              1849-1857): collide -> kinetics -> update_rxnLattices -> abiotic
+ *              (+ dissolution) -> update_abiotic_rxnLattices -> equilibrium -> stream.
+ *              Every step ends with geometry updates only when the caller asks
+ *              (cl_precip_convert / cl_dissol_convert), as the reference gates them
+ *              on an interval. */
+int cl_ade_init(cl_ctx* ctx);
+int cl_step(cl_ctx* ctx, int32_t n);
+
+/* field access (host FP64 buffers of nx*ny*nz values) */
+#define CL_FIELD_CONC      0   /* solute density (index = solute) */
+#define CL_FIELD_BIOMASS   1   /* sessile biomass (index = microbe) */
+#define CL_FIELD_VELOCITY  2   /* coupled velocity component (index = 0,1,2) */
+#define CL_FIELD_FLOW_RHO  3   /* flow density rho */
+#define CL_FIELD_FLOW_U    4   /* flow velocity j computed from the populations (index = 0,1,2) */
+#define CL_FIELD_PHASE     5   /* phase id */
+#define CL_FIELD_EQ_ITERS  6   /* Newton iterations of the last equilibrium step */
+int cl_get_field(cl_ctx* ctx, int32_t field, int32_t index, double* host_out);
+int cl_set_field(cl_ctx* ctx, int32_t field, int32_t index, const double* host_in);
+
+/* raw populations (debug/parity): flow 19*N floats as deviations f-t_i in the
+ * natural (post-stream) order; solute s: 7*N floats of g_i. */
+int cl_get_flow_populations(cl_ctx* ctx, float* host_out);
+int cl_set_flow_populations(cl_ctx* ctx, const float* host_in);
+int cl_get_solute_populations(cl_ctx* ctx, int32_t s, float* host_out);
+
+/* ---- measurement ----------------------------------------------------------------
+ * CUDA events recorded on the context's stream around every launch of the
+ * named kernel while timing is on; cl_timing_read synchronises and returns the
+ * summed device time and the number of timed launches since the last read.
+ * cl_launch_count: kernels this context launched since it was created. */
+#define CL_KERNEL_ADE_MAIN  0   /* fused transport + reaction step, interior sites */
+#define CL_KERNEL_FLOW_STEP 1   /* D3Q19 collide-stream */
+int cl_timing_enable(cl_ctx* ctx, int32_t on);
+int cl_timing_read(cl_ctx* ctx, int32_t kernel, double* total_ms, int64_t* launches);
+int cl_launch_count(const cl_ctx* ctx, int64_t* launches);
+
+/* ---- reductions (row a17) ----------------------------------------------------- */
+#define CL_RED_SUM   0
+#define CL_RED_MIN   1
+#define CL_RED_MAX   2
+#define CL_RED_COUNT_EQ 3          /* count of sites whose mask == (int)arg */
+int cl_reduce(cl_ctx* ctx, int32_t field, int32_t index, int32_t op, double arg, double* out);
+
+/* ---- geometry updates (rows a14-a15) --------------------------------------------
+ * precipNodeConversion3D (src/precipitationVOP.hh:158-219) and
+ * dissolNodeConversion3D (src/dissolutionVOP.hh:459-527).  *changed = number of
+ * sites whose mask changed. */
+int cl_precip_convert(cl_ctx* ctx, int64_t* changed);
+int cl_dissol_convert(cl_ctx* ctx, int64_t* changed);
+
+/* ---- speciation batch (rows a10-a11, a18) ------------------------------------
+ * One FP64 Newton solve per entry.  totals: n*n_comp component totals T_j.
+ * logfree_io: n*n_comp log10 free component concentrations; on input the start
+ *   used by CL_EQ_START_GIVEN, on output the solution.
+ * iters: Newton iterations used (may be NULL).  status: 0 converged from the
+ *   first start, 1 converged after the cold fallback, 2 not converged (may be NULL).
+ * Residual: max_j |sum_i S_ij c_i - T_j| / sum_i |S_ij| c_i <= eq->tol. */
+#define CL_EQ_START_COLD    0   /* reference rule: log10 of the component's own species, else 1e-7 */
+#define CL_EQ_START_GIVEN   1   /* start from logfree_io */
+#define CL_EQ_START_LEARNED 2   /* start from the context's trained network */
+typedef struct cl_eq_solver cl_eq_solver;
+cl_eq_solver* cl_eq_create(const cl_eq_system* sys, void* stream, int* status);
+int cl_eq_destroy(cl_eq_solver* s);
+/* device-pointer variant (inputs already in HBM) */
+int cl_eq_solve_device(cl_eq_solver* s, const double* d_totals, const double* d_cold_species,
+                       double* d_logfree, int32_t* d_iters, uint8_t* d_status,
+                       int64_t n, int32_t start);
+/* host-buffer variant (copies inside) */
+int cl_eq_solve_host(cl_eq_solver* s, const double* totals, const double* cold_species,
+                     double* logfree, int32_t* iters, uint8_t* status,
+                     int64_t n, int32_t start);
+
+/* ---- learned warm start: MLP n_comp -> 64 -> 64 -> n_comp, GELU, BF16 weights,
+ *      FP32 accumulate, trained on the device by the library's own forward and
+ *      backward kernels on pairs (log10 T -> log10 free) that Newton produced. */
+int cl_eq_train(cl_eq_solver* s, const double* d_totals, const double* d_logfree,
+                int64_t n_pairs, int32_t epochs, int32_t batch, float lr, uint64_t seed,
+                float* final_loss);
+/* one forward+backward of a batch, for gradient checks: x n*n_comp inputs
+ * (log10 T), y n*n_comp targets; writes the loss and the FP32 gradients in the
+ * layout of cl_eq_get_params.  Host buffers. */
+int cl_eq_grad_host(cl_eq_solver* s, const float* x, const float* y, int32_t n,
+                    float* loss, float* grads);
+#define CL_MLP_HIDDEN 64
+int cl_eq_param_count(const cl_eq_solver* s, int32_t* count);
+int cl_eq_get_params(cl_eq_solver* s, float* host_params);
+int cl_eq_set_params(cl_eq_solver* s, const float* host_params);
+int cl_eq_predict_host(cl_eq_solver* s, const float* x, float* y, int32_t n);
+
+/* ---- surrogate reaction type (row a13) ----------------------------------------
+ * Feed-forward network with mapminmax scaling (reference defineSurrogateModel,
+ * surrogateModel.hh:252-501).  Layers: widths[0] inputs ... widths[n_layers]
+ * outputs; tanh on hidden layers, linear output. */
+#define CL_SRG_MAX_LAYERS 5
+#define CL_SRG_MAX_WIDTH  32
+typedef struct {
+    int32_t n_layers;
+    int32_t widths[CL_SRG_MAX_LAYERS + 1];
+    double  x_offset[CL_SRG_MAX_WIDTH], x_gain[CL_SRG_MAX_WIDTH], x_ymin;
+    double  y_offset[CL_SRG_MAX_WIDTH], y_gain[CL_SRG_MAX_WIDTH], y_ymin;
+    double  x_lo[CL_SRG_MAX_WIDTH], x_hi[CL_SRG_MAX_WIDTH];   /* input clamp box */
+    /* weights, row-major W[l][out][in] then bias b[l][out], packed layer by layer */
+    double  params[4096];
+} cl_surrogate_net;
+#define CL_SRG_TENSOR 0   /* BF16 tensor-core inference, FP32 accumulate */
+#define CL_SRG_FP32   1   /* FP32 CUDA-core reference kernel */
+int cl_surrogate_batch_device(const cl_surrogate_net* net, const float* d_x, float* d_y,
+                              int64_t n, int32_t mode, void* stream);
+int cl_surrogate_batch_host(const cl_surrogate_net* net, const float* x, float* y,
+                            int64_t n, int32_t mode);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* COMPLAB_GPU_H */

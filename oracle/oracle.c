@@ -1,0 +1,789 @@
+/*
+ * oracle.c -- FP64 CPU oracle (test infrastructure only; see oracle.h).
+ *
+ * Every function restates one reference processor or one Palabos algorithm
+ * the reference calls; the citation sits above each.  Parity with Palabos
+ * itself is unpinned (Palabos v2.3.0 is not vendored with the reference).
+ */
+#include "oracle.h"
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include <float.h>
+
+#define THRD 1e-12                 /* src/complab3d_processors.hh: thrd */
+#define COMPLAB_THRD 1e-14         /* src/complab_functions.hh:64 */
+
+/* ---------------------------------------------------------------- lattices */
+/* D3Q19 in Palabos order: the first nine have a negative leading component,
+ * opp(i) = i +/- 9. */
+static const int C19[19][3] = {
+    {0,0,0},
+    {-1,0,0},{0,-1,0},{0,0,-1},{-1,-1,0},{-1,1,0},{-1,0,-1},{-1,0,1},{0,-1,-1},{0,-1,1},
+    {1,0,0},{0,1,0},{0,0,1},{1,1,0},{1,-1,0},{1,0,1},{1,0,-1},{0,1,1},{0,1,-1}};
+static const double T19[19] = {
+    1.0/3,
+    1.0/18,1.0/18,1.0/18,1.0/36,1.0/36,1.0/36,1.0/36,1.0/36,1.0/36,
+    1.0/18,1.0/18,1.0/18,1.0/36,1.0/36,1.0/36,1.0/36,1.0/36,1.0/36};
+static int opp19(int i) { return i == 0 ? 0 : (i <= 9 ? i + 9 : i - 9); }
+
+/* D3Q7 (Palabos AdvectionDiffusionD3Q7Descriptor): t0 = 1/4, ti = 1/8, cs2 = 1/4.
+ * The reference's increment code adds dC/4 to g[0] and dC/8 to the others
+ * (src/complab3d_processors_part1.hh:108), consistent with these weights. */
+static const int C7[7][3] = {{0,0,0},{-1,0,0},{0,-1,0},{0,0,-1},{1,0,0},{0,1,0},{0,0,1}};
+static const double T7[7] = {0.25,0.125,0.125,0.125,0.125,0.125,0.125};
+static int opp7(int i) { return i == 0 ? 0 : (i <= 3 ? i + 3 : i - 3); }
+
+static inline int64_t site(const cl_config* c, int x, int y, int z) {
+    return ((int64_t)x * c->ny + y) * c->nz + z;
+}
+static inline int wrap(int a, int n) { return a < 0 ? a + n : (a >= n ? a - n : a); }
+
+static int in_list(int v, const int32_t* list, int n) {
+    for (int i = 0; i < n; ++i) if (list[i] == v) return 1;
+    return 0;
+}
+
+/* Dynamics assignment of NSdomainSetup (src/complab_functions.hh:245-294) and
+ * soluteDomainSetup (:296-340): default BGK everywhere, then pore codes, then
+ * bounce_back, then solid (NoDynamics), then biofilm codes, later wins. */
+void orc_classes_from_mask(const cl_config* cfg, const uint8_t* mask,
+                           uint8_t* ns_class, uint8_t* ade_class) {
+    int64_t N = (int64_t)cfg->nx * cfg->ny * cfg->nz;
+    for (int64_t n = 0; n < N; ++n) {
+        int m = mask[n];
+        uint8_t ns = ORC_FLUID, ad = ORC_FLUID;
+        if (in_list(m, cfg->pore_codes, cfg->n_pore_codes)) { ns = ORC_FLUID; ad = ORC_FLUID; }
+        if (cfg->bb_code > 0 && m == cfg->bb_code) { ns = ORC_BB; ad = ORC_BB; }
+        if (cfg->solid_code >= 0 && m == cfg->solid_code) { ns = ORC_NODYN; ad = ORC_NODYN; }
+        if (in_list(m, cfg->bio_codes, cfg->n_bio_codes)) {
+            ns = (cfg->perm_ratio > COMPLAB_THRD) ? ORC_BIO : ORC_BB;
+            ad = ORC_BIO;
+        }
+        ns_class[n] = ns; ade_class[n] = ad;
+    }
+}
+
+/* ------------------------------------------------------------------- flow */
+/* Palabos bgk_ma2_equilibrium with invRho = 1 (IncBGKdynamics): deviation form */
+static inline double feq_inc(int i, double rhoBar, const double j[3], double jSqr) {
+    double cj = C19[i][0]*j[0] + C19[i][1]*j[1] + C19[i][2]*j[2];
+    return T19[i] * (rhoBar + 3.0*cj + 4.5*cj*cj - 1.5*jSqr);
+}
+
+static double omega_ns(const cl_config* cfg, int cls) {
+    double om = 1.0 / cfg->tau_ns;
+    if (cls == ORC_BIO) om = 1.0 / (cfg->perm_ratio * (1.0/om - 0.5) + 0.5);  /* complab_functions.hh:271 */
+    return om;
+}
+
+/* PressureGradient (src/complab_functions.hh:72-84) generalised to given end
+ * densities: rho(x) linear from rho_in at x=0 to rho_out at x=nx-1; u = 0.
+ * Non-BGK cells hold their dynamics' zero equilibrium (fbar = 0). */
+void orc_flow_init(const cl_config* cfg, const uint8_t* ns_class, double* f) {
+    int64_t N = (int64_t)cfg->nx * cfg->ny * cfg->nz;
+    for (int x = 0; x < cfg->nx; ++x)
+        for (int y = 0; y < cfg->ny; ++y)
+            for (int z = 0; z < cfg->nz; ++z) {
+                int64_t n = site(cfg, x, y, z);
+                double rho = cfg->rho_in + (cfg->rho_out - cfg->rho_in) * (double)x / (double)(cfg->nx - 1);
+                int bgk = ns_class[n] == ORC_FLUID || ns_class[n] == ORC_BIO;
+                for (int i = 0; i < 19; ++i) f[i*N + n] = bgk ? T19[i] * (rho - 1.0) : 0.0;
+            }
+}
+
+/* Regularized density boundary (Latt et al. 2008), as Palabos
+ * RegularizedDensityBoundaryDynamics over IncBGK: the normal momentum from the
+ * known populations, tangential momentum zero, PiNeq from the known
+ * populations with bounce-back of the non-equilibrium part, populations rebuilt
+ * as feq + t_i/(2 cs^4) Q_i:PiNeq.  side = -1 west (x=0), +1 east (x=nx-1). */
+static void regularize_pressure(double* fb, double rhoBar, int side, double j[3]) {
+    double s0 = 0, sn = 0;
+    for (int i = 0; i < 19; ++i) {
+        if (C19[i][0] == 0) s0 += fb[i];
+        else if (C19[i][0] == side) sn += fb[i];          /* known: leaving through this face */
+    }
+    /* west: j_x = rhoBar - s0 - 2*s_minus ; east: j_x = s0 + 2*s_plus - rhoBar */
+    j[0] = (side < 0) ? (rhoBar - s0 - 2.0*sn) : (s0 + 2.0*sn - rhoBar);
+    j[1] = 0.0; j[2] = 0.0;
+    double jSqr = j[0]*j[0];
+    double pi[6] = {0,0,0,0,0,0};   /* xx yy zz xy xz yz */
+    for (int i = 0; i < 19; ++i) {
+        double w;
+        if (C19[i][0] == 0) w = 1.0;
+        else if (C19[i][0] == side) w = 2.0;
+        else continue;
+        double fneq = fb[i] - feq_inc(i, rhoBar, j, jSqr);
+        const int* c = C19[i];
+        pi[0] += w*c[0]*c[0]*fneq; pi[1] += w*c[1]*c[1]*fneq; pi[2] += w*c[2]*c[2]*fneq;
+        pi[3] += w*c[0]*c[1]*fneq; pi[4] += w*c[0]*c[2]*fneq; pi[5] += w*c[1]*c[2]*fneq;
+    }
+    for (int i = 0; i < 19; ++i) {
+        const int* c = C19[i];
+        const double cs2 = 1.0/3.0;
+        double qpi = (c[0]*c[0]-cs2)*pi[0] + (c[1]*c[1]-cs2)*pi[1] + (c[2]*c[2]-cs2)*pi[2]
+                   + 2.0*(c[0]*c[1]*pi[3] + c[0]*c[2]*pi[4] + c[1]*c[2]*pi[5]);
+        fb[i] = feq_inc(i, rhoBar, j, jSqr) + T19[i] * 4.5 * qpi;
+    }
+}
+
+/* One collideAndStream.  Collide per class (IncBGK, BounceBack swap, NoDynamics
+ * identity), then push streaming; y,z periodic; a population leaving through an
+ * x face is reflected into its own site's opposite slot (what Palabos's
+ * swap-based streaming leaves in a slot with no upstream neighbour). */
+double orc_flow_step(const cl_config* cfg, const uint8_t* ns_class,
+                     const double* f_in, double* f_out) {
+    const int nx = cfg->nx, ny = cfg->ny, nz = cfg->nz;
+    const int64_t N = (int64_t)nx * ny * nz;
+    double esum = 0.0; int64_t ecount = 0;
+    #pragma omp parallel for collapse(2) reduction(+:esum,ecount) schedule(static)
+    for (int x = 0; x < nx; ++x)
+        for (int y = 0; y < ny; ++y)
+            for (int z = 0; z < nz; ++z) {
+                int64_t n = site(cfg, x, y, z);
+                double fb[19], fo[19];
+                for (int i = 0; i < 19; ++i) fb[i] = f_in[i*N + n];
+                int cls = ns_class[n];
+                if (cls == ORC_NODYN) {
+                    for (int i = 0; i < 19; ++i) fo[i] = fb[i];
+                } else if (cls == ORC_BB) {
+                    for (int i = 0; i < 19; ++i) fo[i] = fb[opp19(i)];
+                } else {
+                    double om = omega_ns(cfg, cls);
+                    double rhoBar = 0, j[3] = {0,0,0};
+                    if (x == 0 || x == nx - 1) {
+                        rhoBar = (x == 0 ? cfg->rho_in : cfg->rho_out) - 1.0;
+                        regularize_pressure(fb, rhoBar, x == 0 ? -1 : 1, j);
+                    } else {
+                        for (int i = 0; i < 19; ++i) {
+                            rhoBar += fb[i];
+                            j[0] += C19[i][0]*fb[i]; j[1] += C19[i][1]*fb[i]; j[2] += C19[i][2]*fb[i];
+                        }
+                    }
+                    double jSqr = j[0]*j[0] + j[1]*j[1] + j[2]*j[2];
+                    for (int i = 0; i < 19; ++i)
+                        fo[i] = fb[i]*(1.0 - om) + om*feq_inc(i, rhoBar, j, jSqr);
+                    esum += 0.5*jSqr; ecount += 1;
+                }
+                for (int i = 0; i < 19; ++i) {
+                    int xd = x + C19[i][0];
+                    if (xd < 0 || xd >= nx) { f_out[opp19(i)*N + n] = fo[i]; continue; }
+                    int yd = wrap(y + C19[i][1], ny), zd = wrap(z + C19[i][2], nz);
+                    f_out[i*N + site(cfg, xd, yd, zd)] = fo[i];
+                }
+            }
+    return ecount ? esum / (double)ecount : 0.0;
+}
+
+/* util::ValueTracer(u=1, L=1000, eps) of Palabos: window deltaT = L/u/2 = 500
+ * values; converged when the window is full and stddev/average < eps (sample
+ * stddev, n-1); a NaN ratio counts as "diverged" and also stops the loop.
+ * Loop shape of src/complab.cpp:607-611. */
+int orc_flow_solve(const cl_config* cfg, const uint8_t* ns_class, double* f,
+                   double* f_tmp, int max_it, double eps, double* energy_hist) {
+    const int W = 500;
+    const int64_t N = (int64_t)cfg->nx * cfg->ny * cfg->nz;
+    double* win = (double*)malloc(sizeof(double) * W);
+    int count = 0, head = 0, it = 0, diverged = 0;
+    for (it = 0; it < max_it; ++it) {
+        double e = orc_flow_step(cfg, ns_class, f, f_tmp);
+        memcpy(f, f_tmp, sizeof(double) * 19 * N);
+        if (energy_hist) energy_hist[it] = e;
+        win[head] = e; head = (head + 1) % W; if (count < W) ++count;
+        if (count >= W) {
+            double avg = 0; for (int k = 0; k < W; ++k) avg += win[k];
+            avg /= W;
+            double sq = 0; for (int k = 0; k < W; ++k) sq += (win[k]-avg)*(win[k]-avg);
+            double ratio = sqrt(sq / (W - 1)) / avg;
+            if (isnan(ratio)) { diverged = 1; break; }
+            if (ratio < eps) break;
+        }
+    }
+    free(win);
+    return diverged ? -1 : it;
+}
+
+/* computeDensity / computeVelocity per site.  BGK cells: rho = 1 + sum fbar,
+ * u = j (IncBGK: velocity is j).  Pressure-boundary cells: the prescribed rho
+ * and the boundary's j.  BounceBack / NoDynamics: rho as stored, u = 0. */
+void orc_flow_macro(const cl_config* cfg, const uint8_t* ns_class, const double* f,
+                    double* rho, double* u) {
+    const int nx = cfg->nx, ny = cfg->ny, nz = cfg->nz;
+    const int64_t N = (int64_t)nx * ny * nz;
+    #pragma omp parallel for collapse(2) schedule(static)
+    for (int x = 0; x < nx; ++x)
+        for (int y = 0; y < ny; ++y)
+            for (int z = 0; z < nz; ++z) {
+                int64_t n = site(cfg, x, y, z);
+                double fb[19], rb = 0, j[3] = {0,0,0};
+                for (int i = 0; i < 19; ++i) fb[i] = f[i*N + n];
+                int cls = ns_class[n];
+                if ((cls == ORC_FLUID || cls == ORC_BIO) && (x == 0 || x == nx - 1)) {
+                    rb = (x == 0 ? cfg->rho_in : cfg->rho_out) - 1.0;
+                    double tmp[19]; memcpy(tmp, fb, sizeof tmp);
+                    regularize_pressure(tmp, rb, x == 0 ? -1 : 1, j);
+                } else {
+                    for (int i = 0; i < 19; ++i) {
+                        rb += fb[i];
+                        j[0] += C19[i][0]*fb[i]; j[1] += C19[i][1]*fb[i]; j[2] += C19[i][2]*fb[i];
+                    }
+                    if (!(cls == ORC_FLUID || cls == ORC_BIO)) { j[0] = j[1] = j[2] = 0; }
+                }
+                if (rho) rho[n] = 1.0 + rb;
+                if (u) { u[n] = j[0]; u[N + n] = j[1]; u[2*N + n] = j[2]; }
+            }
+}
+
+/* -------------------------------------------------------------- transport */
+static int is_reactive(const cl_config* cfg, int x, int m) {
+    return x > 0 && x < cfg->nx - 1 && m != cfg->solid_code && m != cfg->bb_code;
+}
+
+/* initializeAtEquilibrium(c0, u=0) of every solute lattice
+ * (src/complab_functions.hh:334-336); the prescribed boundary densities are
+ * the Dirichlet values, or for a zero-gradient face the density next to it
+ * (FlatAdiabaticBoundaryFunctional3D run by lattice.initialize()). */
+void orc_ade_init(const cl_config* cfg, orc_state* st) {
+    const int64_t N = (int64_t)cfg->nx * cfg->ny * cfg->nz;
+    const int64_t P = (int64_t)cfg->ny * cfg->nz;
+    for (int s = 0; s < cfg->n_solutes; ++s) {
+        if (cfg->immobile[s]) {
+            for (int64_t n = 0; n < N; ++n) st->imm[s*N + n] = cfg->c0[s];
+        } else {
+            for (int i = 0; i < 7; ++i)
+                for (int64_t n = 0; n < N; ++n) st->g[(s*7 + i)*N + n] = T7[i] * cfg->c0[s];
+        }
+        for (int64_t p = 0; p < P; ++p) {
+            st->rho_bc[(s*2 + 0)*P + p] = cfg->left_type[s] == CL_BC_DIRICHLET ? cfg->left_value[s] : cfg->c0[s];
+            st->rho_bc[(s*2 + 1)*P + p] = cfg->right_type[s] == CL_BC_DIRICHLET ? cfg->right_value[s] : cfg->c0[s];
+        }
+    }
+}
+
+/* computeDensity of every site.  A dynamic cell on an x face answers with its
+ * prescribed density (the boundary dynamics stores it: the Dirichlet value, or
+ * for a zero-gradient face the value FlatAdiabaticBoundaryFunctional3D copied
+ * from the neighbour plane after the last stream). */
+void orc_solute_density(const cl_config* cfg, const orc_state* st, int s, double* out) {
+    const int64_t N = (int64_t)cfg->nx * cfg->ny * cfg->nz, P = (int64_t)cfg->ny * cfg->nz;
+    if (cfg->immobile[s]) { memcpy(out, st->imm + s*N, sizeof(double)*N); return; }
+    for (int64_t n = 0; n < N; ++n) {
+        double r = 0; for (int i = 0; i < 7; ++i) r += st->g[(s*7 + i)*N + n];
+        out[n] = r;
+    }
+    for (int side = 0; side < 2; ++side) {
+        int64_t base = side == 0 ? 0 : N - P;
+        for (int64_t p = 0; p < P; ++p) {
+            int cls = st->ade_class[base + p];
+            if (cls == ORC_FLUID || cls == ORC_BIO) out[base + p] = st->rho_bc[(s*2 + side)*P + p];
+        }
+    }
+}
+
+/* Table-driven rate law (defineRxnKinetics / defineAbioticRxnKinetics ABI:
+ * defineKinetics.hh:223-229, defineAbioticKinetics.hh:130).  abiotic selects
+ * the reactions with microbe < 0, biotic those with microbe >= 0 plus decay. */
+void orc_rates(const cl_config* cfg, int abiotic, const double* C, const double* B,
+               double* subsR, double* bioR) {
+    for (int s = 0; s < cfg->n_solutes; ++s) subsR[s] = 0.0;
+    if (bioR) for (int m = 0; m < cfg->n_microbes; ++m) bioR[m] = 0.0;
+    for (int k = 0; k < cfg->n_rxn; ++k) {
+        const cl_rxn* r = &cfg->rxn[k];
+        if ((r->microbe < 0) != (abiotic != 0)) continue;
+        double rate = r->k;
+        if (r->microbe >= 0) {
+            double b = B[r->microbe];
+            if (!(b > 0.0)) continue;
+            rate *= b;
+        }
+        for (int j = 0; j < r->n_monod; ++j) {
+            double c = C[r->monod_s[j]]; if (c < 0) c = 0;
+            rate *= c / (r->monod_ks[j] + c);
+        }
+        for (int j = 0; j < r->n_mass; ++j) {
+            double c = C[r->mass_s[j]]; if (c < 0) c = 0;
+            rate *= c;
+        }
+        for (int s = 0; s < cfg->n_solutes; ++s) subsR[s] += r->nu[s] * rate;
+        if (r->microbe >= 0 && bioR) bioR[r->microbe] += r->yield * rate;
+    }
+    if (!abiotic && bioR)
+        for (int m = 0; m < cfg->n_microbes; ++m) {
+            double b = B[m] > 0 ? B[m] : 0.0;
+            bioR[m] -= cfg->decay[m] * b;
+        }
+    for (int s = 0; s < cfg->n_solutes; ++s) if (!isfinite(subsR[s])) subsR[s] = 0.0;
+    if (bioR) for (int m = 0; m < cfg->n_microbes; ++m) if (!isfinite(bioR[m])) bioR[m] = 0.0;
+}
+
+/* Speciation --------------------------------------------------------------- */
+#define MIN_CONC 1e-30
+#define MAX_CONC 10.0
+#define MIN_LOG_C (-30.0)
+#define MAX_LOG_C 1.0
+
+static int eq_species_active(const cl_eq_system* sys, int i) {
+    for (int j = 0; j < sys->n_comp; ++j) if (fabs(sys->stoich[i][j]) > 1e-10) return 1;
+    return 0;
+}
+
+/* calc_species (part4_eqsolver.hh:442-496) for equilibrium species */
+void orc_eq_species(const cl_eq_system* sys, const double* x, double* c) {
+    for (int i = 0; i < sys->n_species; ++i) {
+        if (!eq_species_active(sys, i)) { c[i] = 0.0; continue; }
+        double lc = sys->logk[i];
+        for (int j = 0; j < sys->n_comp; ++j) lc += sys->stoich[i][j] * x[j];
+        if (lc > MAX_LOG_C) lc = MAX_LOG_C;
+        if (lc < MIN_LOG_C) lc = MIN_LOG_C;
+        c[i] = pow(10.0, lc);
+    }
+}
+
+/* calc_component_totals (part4_eqsolver.hh:520-538) */
+void orc_eq_totals(const cl_eq_system* sys, const double* species, double* totals) {
+    for (int j = 0; j < sys->n_comp; ++j) {
+        double t = 0.0;
+        for (int i = 0; i < sys->n_species; ++i) {
+            if (!eq_species_active(sys, i)) continue;
+            double c = species[i];
+            if (c > MAX_CONC) c = MAX_CONC;
+            if (c < MIN_CONC) c = MIN_CONC;
+            t += sys->stoich[i][j] * c;
+        }
+        totals[j] = t > MIN_CONC ? t : MIN_CONC;
+    }
+}
+
+/* initial guess of solve_equilibrium_anderson (part4_eqsolver.hh:977-994),
+ * identical in the Newton reserve (NR_reserve.hh:527-540) */
+void orc_eq_cold_start(const cl_eq_system* sys, const double* species, double* x0) {
+    for (int j = 0; j < sys->n_comp; ++j) {
+        double c = 1e-7;
+        int idx = sys->comp_species[j];
+        if (idx >= 0 && idx < sys->n_species) c = species[idx];
+        if (c > MAX_CONC) c = MAX_CONC;
+        if (c < MIN_CONC) c = MIN_CONC;
+        x0[j] = log10(c);
+    }
+}
+
+/* relative mass-balance residual max_j |sum_i S_ij c_i - T_j| / sum_i |S_ij| c_i */
+static double eq_eval(const cl_eq_system* sys, const double* T, const double* x,
+                      double* F, double* c) {
+    orc_eq_species(sys, x, c);
+    double rel = 0.0;
+    for (int j = 0; j < sys->n_comp; ++j) {
+        double f = -T[j], sc = 0.0;
+        for (int i = 0; i < sys->n_species; ++i) {
+            f += sys->stoich[i][j] * c[i];
+            sc += fabs(sys->stoich[i][j]) * c[i];
+        }
+        F[j] = f;
+        double r = fabs(f) / (sc > 1e-300 ? sc : 1e-300);
+        if (!(r <= rel)) rel = r;   /* NaN-propagating max */
+    }
+    return rel;
+}
+
+double orc_eq_residual(const cl_eq_system* sys, const double* totals, const double* x) {
+    double F[CL_MAX_COMP], c[CL_MAX_SPECIES];
+    return eq_eval(sys, totals, x, F, c);
+}
+
+/* Newton-Raphson in log10 free components, restating solve_equilibrium_NR
+ * (src/complab3d_processors_part4_eqsolver_NR_reserve.hh:512-615): residual
+ * F = S^T c - T (:309-328), Jacobian J = ln10 S^T diag(c) S (:356-377),
+ * Gaussian elimination with partial pivoting (:414-481), Armijo backtracking
+ * with alpha halving, at most 40 trials (:577-598).  Four documented
+ * deviations make it converge on the 5x14 random tableaux, where the reserve
+ * as written stalls on 83% of cold starts (its line search on the unweighted
+ * ||F||_2 accepts only vanishing steps when totals span decades):
+ *   - stopping test: relative mass-balance residual <= tol (reserve: absolute
+ *     ||F||_2 < 1e-12);
+ *   - species held at a clamp bound contribute nothing to J (the derivative of
+ *     the clamped value), so J matches F;
+ *   - the Newton step is scaled so that no component moves more than 2 decades;
+ *   - the Armijo merit is ||F_j / sum_i |S_ij| c_i||_2 with the weights of the
+ *     current iterate. */
+int orc_eq_newton(const cl_eq_system* sys, const double* totals, double* x,
+                  int max_iter, double tol, int* converged) {
+    const int nc = sys->n_comp, ns = sys->n_species;
+    double F[CL_MAX_COMP], c[CL_MAX_SPECIES], Ft[CL_MAX_COMP], ct[CL_MAX_SPECIES];
+    double xt[CL_MAX_COMP];
+    *converged = 0;
+    if (nc == 0) { *converged = 1; return 0; }
+    for (int it = 0; it < max_iter; ++it) {
+        double rel = eq_eval(sys, totals, x, F, c);
+        if (rel <= tol) { *converged = 1; return it; }
+        if (!isfinite(rel)) return it;
+        /* J = ln10 * S^T diag(c) S ; A = [J | -F] */
+        double A[CL_MAX_COMP][CL_MAX_COMP + 1], cj[CL_MAX_SPECIES], w[CL_MAX_COMP];
+        const double ln10 = 2.302585092994046;
+        for (int i = 0; i < ns; ++i) {
+            double lc = sys->logk[i];
+            for (int j = 0; j < nc; ++j) lc += sys->stoich[i][j] * x[j];
+            cj[i] = (lc > MAX_LOG_C || lc < MIN_LOG_C) ? 0.0 : c[i];
+        }
+        for (int a = 0; a < nc; ++a) {
+            for (int b = 0; b < nc; ++b) {
+                double s = 0;
+                for (int i = 0; i < ns; ++i) s += sys->stoich[i][a] * sys->stoich[i][b] * cj[i];
+                A[a][b] = ln10 * s;
+            }
+            A[a][nc] = -F[a];
+            double sc = 0;
+            for (int i = 0; i < ns; ++i) sc += fabs(sys->stoich[i][a]) * c[i];
+            w[a] = 1.0 / (sc > 1e-300 ? sc : 1e-300);
+        }
+        int ok = 1;
+        for (int k = 0; k < nc; ++k) {
+            int p = k; double mx = fabs(A[k][k]);
+            for (int r = k + 1; r < nc; ++r) if (fabs(A[r][k]) > mx) { mx = fabs(A[r][k]); p = r; }
+            if (!(mx > 1e-300)) { ok = 0; break; }
+            if (p != k) for (int q = 0; q <= nc; ++q) { double t = A[k][q]; A[k][q] = A[p][q]; A[p][q] = t; }
+            for (int r = k + 1; r < nc; ++r) {
+                double fct = A[r][k] / A[k][k];
+                for (int q = k; q <= nc; ++q) A[r][q] -= fct * A[k][q];
+            }
+        }
+        if (!ok) return it + 1;
+        double d[CL_MAX_COMP];
+        for (int k = nc - 1; k >= 0; --k) {
+            double s = A[k][nc];
+            for (int q = k + 1; q < nc; ++q) s -= A[k][q] * d[q];
+            d[k] = s / A[k][k];
+        }
+        double dmax = 0; for (int j = 0; j < nc; ++j) if (fabs(d[j]) > dmax) dmax = fabs(d[j]);
+        if (dmax > 2.0) for (int j = 0; j < nc; ++j) d[j] *= 2.0 / dmax;
+        double fn = 0; for (int j = 0; j < nc; ++j) fn += (F[j]*w[j])*(F[j]*w[j]);
+        fn = sqrt(fn);
+        double alpha = 1.0;
+        for (int ls = 0; ls < 40; ++ls) {
+            for (int j = 0; j < nc; ++j) {
+                double v = x[j] + alpha * d[j];
+                if (v > MAX_LOG_C) v = MAX_LOG_C;
+                if (v < MIN_LOG_C) v = MIN_LOG_C;
+                xt[j] = v;
+            }
+            eq_eval(sys, totals, xt, Ft, ct);
+            double fnt = 0; for (int j = 0; j < nc; ++j) fnt += (Ft[j]*w[j])*(Ft[j]*w[j]);
+            fnt = sqrt(fnt);
+            if (fnt < fn * (1.0 - 1e-4 * alpha) || alpha < 1e-15) break;
+            alpha *= 0.5;
+        }
+        for (int j = 0; j < nc; ++j) x[j] = xt[j];
+    }
+    double F2[CL_MAX_COMP], c2[CL_MAX_SPECIES];
+    if (eq_eval(sys, totals, x, F2, c2) <= tol) *converged = 1;
+    return max_iter;
+}
+
+void orc_eq_batch(const cl_eq_system* sys, const double* totals, const double* cold_species,
+                  double* x_io, int32_t* iters, uint8_t* status, int64_t n, int start) {
+    const int nc = sys->n_comp, ns = sys->n_species;
+    #pragma omp parallel for schedule(dynamic, 256)
+    for (int64_t k = 0; k < n; ++k) {
+        double x[CL_MAX_COMP];
+        if (start == CL_EQ_START_COLD) orc_eq_cold_start(sys, cold_species + k*ns, x);
+        else for (int j = 0; j < nc; ++j) x[j] = x_io[k*nc + j];
+        int conv = 0;
+        int limit = (start == CL_EQ_START_COLD) ? sys->max_iter : sys->warm_iter;
+        int it = orc_eq_newton(sys, totals + k*nc, x, limit, sys->tol, &conv);
+        uint8_t stt = 0;
+        if (!conv && start != CL_EQ_START_COLD) {
+            orc_eq_cold_start(sys, cold_species + k*ns, x);
+            it += orc_eq_newton(sys, totals + k*nc, x, sys->max_iter, sys->tol, &conv);
+            stt = 1;
+        }
+        if (!conv) stt = 2;
+        for (int j = 0; j < nc; ++j) x_io[k*nc + j] = x[j];
+        if (iters) iters[k] = it;
+        if (status) status[k] = stt;
+    }
+}
+
+/* One transport step in the order of src/complab.cpp:1252-1374,1849-1857:
+ *   collide (mobile solutes; boundary cells complete their unknown population
+ *   from the prescribed density first) -> run_kinetics -> update_rxnLattices ->
+ *   dC reset -> run_abiotic_kinetics | surfaceAbioticKinetics3D ->
+ *   update_abiotic_rxnLattices -> run_equilibrium_biotic -> stream ->
+ *   FlatAdiabaticBoundaryFunctional3D on zero-gradient faces. */
+int64_t orc_transport_step(const cl_config* cfg, orc_state* st) {
+    const int nx = cfg->nx, ny = cfg->ny, nz = cfg->nz, S = cfg->n_solutes, M = cfg->n_microbes;
+    const int64_t N = (int64_t)nx * ny * nz, P = (int64_t)ny * nz;
+    int64_t nonconv = 0;
+    double* g = st->g;
+
+    /* ---- collide (AdvectionDiffusionBGKdynamics, BounceBack, NoDynamics) ---- */
+    #pragma omp parallel for collapse(2) schedule(static)
+    for (int x = 0; x < nx; ++x)
+        for (int y = 0; y < ny; ++y)
+            for (int z = 0; z < nz; ++z) {
+                int64_t n = site(cfg, x, y, z);
+                int cls = st->ade_class[n];
+                for (int s = 0; s < S; ++s) {
+                    if (cfg->immobile[s]) continue;
+                    double gi[7];
+                    for (int i = 0; i < 7; ++i) gi[i] = g[(s*7 + i)*N + n];
+                    if (cls == ORC_NODYN) continue;
+                    if (cls == ORC_BB) {
+                        for (int i = 0; i < 7; ++i) g[(s*7 + i)*N + n] = gi[opp7(i)];
+                        continue;
+                    }
+                    if (x == 0 || x == nx - 1) {
+                        /* AdvectionDiffusionBoundaryDynamics: the one unknown population
+                         * (entering through the face) = prescribed rho - sum of the others */
+                        int unk = (x == 0) ? 4 : 1;
+                        double rb = st->rho_bc[(s*2 + (x == 0 ? 0 : 1))*P + (int64_t)y*nz + z];
+                        double sum = 0; for (int i = 0; i < 7; ++i) if (i != unk) sum += gi[i];
+                        gi[unk] = rb - sum;
+                    }
+                    double om = (cls == ORC_BIO) ? cfg->omega_bio[s] : cfg->omega_pore[s];
+                    double rho = 0; for (int i = 0; i < 7; ++i) rho += gi[i];
+                    double ux = st->u[n], uy = st->u[N + n], uz = st->u[2*N + n];
+                    for (int i = 0; i < 7; ++i) {
+                        double cu = C7[i][0]*ux + C7[i][1]*uy + C7[i][2]*uz;
+                        double geq = T7[i] * rho * (1.0 + 4.0*cu);
+                        g[(s*7 + i)*N + n] = gi[i] - om*(gi[i] - geq);
+                    }
+                }
+            }
+
+    /* ---- reactions (per voxel; processors run over the whole lattice in turn,
+     *      and each one reads only its own voxel, so per-voxel order is exact) ---- */
+    int n_bio = 0, n_abio = 0;
+    for (int k = 0; k < cfg->n_rxn; ++k) { if (cfg->rxn[k].microbe >= 0) ++n_bio; else ++n_abio; }
+    int any_bio = cfg->enable_kinetics && (n_bio > 0 || M > 0);
+    int any_abio = cfg->enable_abiotic && S > 0;
+    #pragma omp parallel for collapse(2) reduction(+:nonconv) schedule(dynamic, 4)
+    for (int x = 1; x < nx - 1; ++x)
+        for (int y = 0; y < ny; ++y)
+            for (int z = 0; z < nz; ++z) {
+                int64_t n = site(cfg, x, y, z);
+                int m = st->mask[n];
+                if (!is_reactive(cfg, x, m)) continue;
+                double C[CL_MAX_SOLUTES], Bm[CL_MAX_MICROBES], R[CL_MAX_SOLUTES], BR[CL_MAX_MICROBES];
+                double dC[CL_MAX_SOLUTES];
+                #define DENS(s) (cfg->immobile[s] ? st->imm[(s)*N + n] : \
+                    (g[((s)*7+0)*N+n]+g[((s)*7+1)*N+n]+g[((s)*7+2)*N+n]+g[((s)*7+3)*N+n]+ \
+                     g[((s)*7+4)*N+n]+g[((s)*7+5)*N+n]+g[((s)*7+6)*N+n]))
+                #define APPLY(s, d) do { if (cfg->immobile[s]) st->imm[(s)*N + n] += (d); \
+                    else for (int i_ = 0; i_ < 7; ++i_) g[((s)*7+i_)*N + n] += T7[i_]*(d); } while (0)
+                /* run_kinetics (part1.hh:63-146) + update_rxnLattices (:338-429) */
+                if (any_bio) {
+                    for (int s = 0; s < S; ++s) { double c = DENS(s); C[s] = c < THRD ? 0.0 : c; }
+                    for (int b = 0; b < M; ++b) { double v = st->bio[b*N + n]; Bm[b] = v < THRD ? 0.0 : v; }
+                    orc_rates(cfg, 0, C, Bm, R, BR);
+                    for (int s = 0; s < S; ++s) {
+                        double d = R[s] * cfg->dt;
+                        dC[s] = (d > THRD || d < -THRD) ? d : 0.0;
+                    }
+                    for (int s = 0; s < S; ++s) if (dC[s] > THRD || dC[s] < -THRD) APPLY(s, dC[s]);
+                    for (int b = 0; b < M; ++b) {
+                        double d = BR[b] * cfg->dt;
+                        if (d > THRD || d < -THRD) st->bio[b*N + n] += d;
+                    }
+                }
+                /* dC = dC0; run_abiotic_kinetics (part1.hh:158-249) or
+                 * surfaceAbioticKinetics3D (precipitationVOP.hh:53-145);
+                 * update_abiotic_rxnLattices (part1.hh:258-336) */
+                if (any_abio && n_abio > 0) {
+                    int fire = 1;
+                    if (cfg->precip_enabled && cfg->abiotic_surface_only) {
+                        static const int d6[6][3] = {{1,0,0},{-1,0,0},{0,1,0},{0,-1,0},{0,0,1},{0,0,-1}};
+                        fire = 0;
+                        for (int d = 0; d < 6 && !fire; ++d) {
+                            int xa = x + d6[d][0];
+                            if (xa < 0 || xa > nx - 1) continue;
+                            int nb = st->mask[site(cfg, xa, wrap(y + d6[d][1], ny), wrap(z + d6[d][2], nz))];
+                            if (nb == cfg->solid_code || nb == cfg->bb_code) fire = 1;
+                        }
+                    }
+                    if (fire) {
+                        for (int s = 0; s < S; ++s) { double c = DENS(s); C[s] = c < THRD ? 0.0 : c; }
+                        orc_rates(cfg, 1, C, NULL, R, NULL);
+                        for (int s = 0; s < S; ++s) {
+                            double d = R[s] * cfg->dt;
+                            if (d > THRD || d < -THRD) APPLY(s, d);
+                        }
+                    }
+                }
+                /* run_equilibrium_biotic (part4_eqsolver.hh:1355-1494), Newton solve */
+                if (cfg->use_equilibrium) {
+                    const cl_eq_system* sys = &cfg->eq;
+                    double conc[CL_MAX_SPECIES], T[CL_MAX_COMP], xx[CL_MAX_COMP], eqc[CL_MAX_SPECIES];
+                    for (int s = 0; s < S; ++s) { double c = DENS(s); conc[s] = c > MIN_CONC ? c : MIN_CONC; }
+                    orc_eq_totals(sys, conc, T);
+                    orc_eq_cold_start(sys, conc, xx);
+                    int conv = 0;
+                    int it = orc_eq_newton(sys, T, xx, sys->max_iter, sys->tol, &conv);
+                    if (st->eq_iters) st->eq_iters[n] = it;
+                    if (!conv) { nonconv += 1; }
+                    else {
+                        orc_eq_species(sys, xx, eqc);
+                        for (int s = 0; s < S && s < sys->n_species; ++s) {
+                            double e = eq_species_active(sys, s) ? eqc[s]
+                                     : (conc[s] > MIN_CONC ? (conc[s] < MAX_CONC ? conc[s] : MAX_CONC) : MIN_CONC);
+                            if (e > MAX_CONC) e = MAX_CONC;
+                            if (e < MIN_CONC) e = MIN_CONC;
+                            double d = e - conc[s];
+                            double mx = 0.1 * fabs(conc[s]); if (mx < 1e-9) mx = 1e-9;
+                            if (fabs(d) > mx) d = d > 0 ? mx : -mx;
+                            if (conc[s] + d < 1e-20) d = 1e-20 - conc[s];
+                            if (fabs(d) > THRD) APPLY(s, d);
+                        }
+                    }
+                }
+                #undef DENS
+                #undef APPLY
+            }
+
+    /* ---- stream (push, periodic y/z, reflect at x faces) ---- */
+    for (int s = 0; s < S; ++s) {
+        if (cfg->immobile[s]) continue;
+        double* gs = g + (int64_t)s*7*N;
+        double* go = st->g_tmp + (int64_t)s*7*N;
+        #pragma omp parallel for collapse(2) schedule(static)
+        for (int x = 0; x < nx; ++x)
+            for (int y = 0; y < ny; ++y)
+                for (int z = 0; z < nz; ++z) {
+                    int64_t n = site(cfg, x, y, z);
+                    for (int i = 0; i < 7; ++i) {
+                        int xd = x + C7[i][0];
+                        if (xd < 0 || xd >= nx) { go[opp7(i)*N + n] = gs[i*N + n]; continue; }
+                        go[i*N + site(cfg, xd, wrap(y + C7[i][1], ny), wrap(z + C7[i][2], nz))] = gs[i*N + n];
+                    }
+                }
+        memcpy(gs, go, sizeof(double) * 7 * N);
+        /* FlatAdiabaticBoundaryFunctional3D<0,-1/+1>: boundary density := neighbour's */
+        for (int side = 0; side < 2; ++side) {
+            int bt = side == 0 ? cfg->left_type[s] : cfg->right_type[s];
+            if (bt != CL_BC_NEUMANN) continue;
+            int xn = side == 0 ? 1 : nx - 2;
+            for (int y = 0; y < ny; ++y)
+                for (int z = 0; z < nz; ++z) {
+                    int64_t n = site(cfg, xn, y, z);
+                    double r = 0; for (int i = 0; i < 7; ++i) r += gs[i*N + n];
+                    st->rho_bc[(s*2 + side)*P + (int64_t)y*nz + z] = r;
+                }
+        }
+    }
+    return nonconv;
+}
+
+/* precipNodeConversion3D (src/precipitationVOP.hh:158-219) */
+int64_t orc_precip_convert(const cl_config* cfg, orc_state* st) {
+    const int64_t N = (int64_t)cfg->nx * cfg->ny * cfg->nz;
+    int64_t changed = 0;
+    int s = cfg->precip_substrate;
+    for (int64_t n = 0; n < N; ++n) {
+        int m = st->mask[n];
+        if (m == cfg->solid_code || m == cfg->bb_code) continue;
+        double p = cfg->immobile[s] ? st->imm[s*N + n] : 0.0;
+        if (!cfg->immobile[s]) for (int i = 0; i < 7; ++i) p += st->g[(s*7 + i)*N + n];
+        if (p >= cfg->max_precip_rho) {
+            if (m != cfg->precip_code) ++changed;
+            st->mask[n] = (uint8_t)cfg->precip_code;
+        }
+    }
+    return changed;
+}
+
+/* ---------------------------------------------------------------- MLP (FP64) */
+static double gelu(double v) { return 0.5 * v * (1.0 + erf(v / sqrt(2.0))); }
+static double gelu_d(double v) {
+    return 0.5 * (1.0 + erf(v / sqrt(2.0))) + v * exp(-0.5 * v * v) / sqrt(2.0 * M_PI);
+}
+
+/* Forward and analytic backward of a 2-hidden-layer GELU MLP with MSE loss,
+ * following the structure of surrogate_training/trainSurrogate.py:132-166
+ * (tanh hidden layers there, GELU here). */
+double orc_mlp_forward_backward(int n_in, int H, int n_out, const double* p,
+                                const double* xin, const double* yin, int n,
+                                double* grads, double* y_hat) {
+    const double* W1 = p;               const double* b1 = W1 + H*n_in;
+    const double* W2 = b1 + H;          const double* b2 = W2 + H*H;
+    const double* W3 = b2 + H;          const double* b3 = W3 + n_out*H;
+    int np = H*n_in + H + H*H + H + n_out*H + n_out;
+    if (grads) memset(grads, 0, sizeof(double) * np);
+    double* gW1 = grads; double* gb1 = grads ? gW1 + H*n_in : NULL;
+    double* gW2 = grads ? gb1 + H : NULL; double* gb2 = grads ? gW2 + H*H : NULL;
+    double* gW3 = grads ? gb2 + H : NULL; double* gb3 = grads ? gW3 + n_out*H : NULL;
+    double loss = 0.0;
+    double z1[256], a1[256], z2[256], a2[256], yo[64], dy[64], d2[256], d1[256];
+    for (int k = 0; k < n; ++k) {
+        const double* x = xin + (int64_t)k*n_in;
+        for (int h = 0; h < H; ++h) {
+            double s = b1[h]; for (int i = 0; i < n_in; ++i) s += W1[h*n_in + i]*x[i];
+            z1[h] = s; a1[h] = gelu(s);
+        }
+        for (int h = 0; h < H; ++h) {
+            double s = b2[h]; for (int i = 0; i < H; ++i) s += W2[h*H + i]*a1[i];
+            z2[h] = s; a2[h] = gelu(s);
+        }
+        for (int o = 0; o < n_out; ++o) {
+            double s = b3[o]; for (int i = 0; i < H; ++i) s += W3[o*H + i]*a2[i];
+            yo[o] = s;
+            if (y_hat) y_hat[(int64_t)k*n_out + o] = s;
+            double e = s - yin[(int64_t)k*n_out + o];
+            loss += e*e;
+            dy[o] = 2.0 * e / ((double)n * n_out);
+        }
+        if (!grads) continue;
+        for (int o = 0; o < n_out; ++o) {
+            gb3[o] += dy[o];
+            for (int i = 0; i < H; ++i) gW3[o*H + i] += dy[o]*a2[i];
+        }
+        for (int h = 0; h < H; ++h) {
+            double s = 0; for (int o = 0; o < n_out; ++o) s += W3[o*H + h]*dy[o];
+            d2[h] = s * gelu_d(z2[h]);
+        }
+        for (int h = 0; h < H; ++h) {
+            gb2[h] += d2[h];
+            for (int i = 0; i < H; ++i) gW2[h*H + i] += d2[h]*a1[i];
+        }
+        for (int h = 0; h < H; ++h) {
+            double s = 0; for (int o = 0; o < H; ++o) s += W2[o*H + h]*d2[o];
+            d1[h] = s * gelu_d(z1[h]);
+        }
+        for (int h = 0; h < H; ++h) {
+            gb1[h] += d1[h];
+            for (int i = 0; i < n_in; ++i) gW1[h*n_in + i] += d1[h]*x[i];
+        }
+    }
+    return loss / ((double)n * n_out);
+}
+
+/* --------------------------------------------------------- surrogate (FP64) */
+/* defineSurrogateModel (surrogateModel.hh:390-430): mapminmax input
+ * xs = (x - offset)*gain + ymin, tansig hidden layers, linear output, reverse
+ * map y = (a - ymin)/gain + offset.  Inputs are first clamped to [x_lo, x_hi]. */
+void orc_surrogate_forward(const cl_surrogate_net* net, const double* xin, double* yout, int64_t n) {
+    int L = net->n_layers;
+    for (int64_t k = 0; k < n; ++k) {
+        double a[CL_SRG_MAX_WIDTH], b[CL_SRG_MAX_WIDTH];
+        int w0 = net->widths[0];
+        for (int i = 0; i < w0; ++i) {
+            double v = xin[k*w0 + i];
+            if (v < net->x_lo[i]) v = net->x_lo[i];
+            if (v > net->x_hi[i]) v = net->x_hi[i];
+            a[i] = (v - net->x_offset[i]) * net->x_gain[i] + net->x_ymin;
+        }
+        const double* p = net->params;
+        for (int l = 0; l < L; ++l) {
+            int wi = net->widths[l], wo = net->widths[l + 1];
+            const double* W = p; const double* bb = p + wo*wi;
+            for (int o = 0; o < wo; ++o) {
+                double s = 0.0;
+                for (int i = 0; i < wi; ++i) s += W[o*wi + i] * a[i];
+                s += bb[o];
+                b[o] = (l < L - 1) ? (2.0 / (1.0 + exp(-2.0 * s)) - 1.0) : s;
+            }
+            for (int o = 0; o < wo; ++o) a[o] = b[o];
+            p += wo*wi + wo;
+        }
+        int wl = net->widths[L];
+        for (int o = 0; o < wl; ++o)
+            yout[k*wl + o] = (a[o] - net->y_ymin) / net->y_gain[o] + net->y_offset[o];
+    }
+}

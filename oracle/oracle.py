@@ -1,0 +1,244 @@
+"""ctypes binding of the FP64 CPU oracle (liboracle.so) and of the reference's
+own Palabos-free code compiled from its sources (_ref/libref.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() and
+by the CPU legs of bench.py, always as the checker or the timed CPU baseline,
+never as the product path.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libref.so")
+
+_orc = None
+_ref = None
+
+
+def build():
+    """Compile liboracle.so (and _ref/libref.so when the reference tree exists)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def _p(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else None
+
+
+def lib():
+    global _orc
+    if _orc is None:
+        if not os.path.exists(LIB):
+            build()
+        _orc = ctypes.CDLL(LIB)
+        vp, d, i = ctypes.c_void_p, ctypes.c_double, ctypes.c_int
+        _orc.orc_flow_step.restype = d
+        _orc.orc_flow_step.argtypes = [vp, vp, vp, vp]
+        _orc.orc_flow_solve.restype = i
+        _orc.orc_flow_solve.argtypes = [vp, vp, vp, vp, i, d, vp]
+        _orc.orc_transport_step.restype = ctypes.c_int64
+        _orc.orc_transport_step.argtypes = [vp, vp]
+        _orc.orc_precip_convert.restype = ctypes.c_int64
+        _orc.orc_precip_convert.argtypes = [vp, vp]
+        _orc.orc_eq_newton.restype = i
+        _orc.orc_eq_newton.argtypes = [vp, vp, vp, i, d, vp]
+        _orc.orc_eq_residual.restype = d
+        _orc.orc_eq_residual.argtypes = [vp, vp, vp]
+        _orc.orc_eq_batch.restype = None
+        _orc.orc_eq_batch.argtypes = [vp, vp, vp, vp, vp, vp, ctypes.c_int64, i]
+        _orc.orc_mlp_forward_backward.restype = d
+        _orc.orc_mlp_forward_backward.argtypes = [i, i, i, vp, vp, vp, i, vp, vp]
+        _orc.orc_surrogate_forward.restype = None
+        _orc.orc_surrogate_forward.argtypes = [vp, vp, vp, ctypes.c_int64]
+        _orc.orc_rates.restype = None
+        _orc.orc_rates.argtypes = [vp, i, vp, vp, vp, vp]
+    return _orc
+
+
+def ref_lib():
+    """The reference's own code; None when it was not built (no reference tree)."""
+    global _ref
+    if _ref is None and os.path.exists(REF_LIB):
+        _ref = ctypes.CDLL(REF_LIB)
+    return _ref
+
+
+class OrcState(ctypes.Structure):
+    _fields_ = [("g", ctypes.c_void_p), ("g_tmp", ctypes.c_void_p), ("imm", ctypes.c_void_p),
+                ("bio", ctypes.c_void_p), ("u", ctypes.c_void_p), ("mask", ctypes.c_void_p),
+                ("ade_class", ctypes.c_void_p), ("rho_bc", ctypes.c_void_p), ("eq_iters", ctypes.c_void_p)]
+
+
+def classes(cfg, mask):
+    N = mask.size
+    ns = np.empty(N, np.uint8)
+    ad = np.empty(N, np.uint8)
+    lib().orc_classes_from_mask(ctypes.byref(cfg), _p(np.ascontiguousarray(mask, np.uint8).reshape(-1)), _p(ns), _p(ad))
+    return ns, ad
+
+
+class Flow:
+    """FP64 flow lattice (deviation populations, natural order)."""
+
+    def __init__(self, cfg, mask):
+        self.cfg = cfg
+        self.N = cfg.nx * cfg.ny * cfg.nz
+        self.mask = np.ascontiguousarray(mask, np.uint8).reshape(-1)
+        self.ns, self.ade = classes(cfg, self.mask)
+        self.f = np.zeros(19 * self.N)
+        self.tmp = np.zeros(19 * self.N)
+        lib().orc_flow_init(ctypes.byref(cfg), _p(self.ns), _p(self.f))
+
+    def step(self, n=1):
+        e = 0.0
+        for _ in range(n):
+            e = lib().orc_flow_step(ctypes.byref(self.cfg), _p(self.ns), _p(self.f), _p(self.tmp))
+            self.f, self.tmp = self.tmp, self.f
+        return e
+
+    def solve(self, max_it, eps):
+        hist = np.zeros(max(max_it, 1))
+        it = lib().orc_flow_solve(ctypes.byref(self.cfg), _p(self.ns), _p(self.f), _p(self.tmp), max_it, eps, _p(hist))
+        return it, hist
+
+    def macro(self):
+        rho = np.zeros(self.N)
+        u = np.zeros(3 * self.N)
+        lib().orc_flow_macro(ctypes.byref(self.cfg), _p(self.ns), _p(self.f), _p(rho), _p(u))
+        return rho, u.reshape(3, self.N)
+
+
+class Transport:
+    """FP64 solute lattices stepped in the reference's processor order."""
+
+    def __init__(self, cfg, mask, u=None):
+        self.cfg = cfg
+        N = self.N = cfg.nx * cfg.ny * cfg.nz
+        S, M = cfg.n_solutes, max(cfg.n_microbes, 1)
+        self.mask = np.ascontiguousarray(mask, np.uint8).reshape(-1).copy()
+        self.ns, self.ade = classes(cfg, self.mask)
+        self.g = np.zeros(S * 7 * N)
+        self.g_tmp = np.zeros(S * 7 * N)
+        self.imm = np.zeros(S * N)
+        self.bio = np.zeros(M * N)
+        self.u = np.zeros(3 * N) if u is None else np.ascontiguousarray(u, np.float64).reshape(-1).copy()
+        self.rho_bc = np.zeros(S * 2 * cfg.ny * cfg.nz)
+        self.eq_iters = np.zeros(N, np.int32)
+        self.st = OrcState(_p(self.g).value, _p(self.g_tmp).value, _p(self.imm).value, _p(self.bio).value,
+                           _p(self.u).value, _p(self.mask).value, _p(self.ade).value, _p(self.rho_bc).value,
+                           _p(self.eq_iters).value)
+        lib().orc_ade_init(ctypes.byref(cfg), ctypes.byref(self.st))
+
+    def step(self, n=1):
+        nc = 0
+        for _ in range(n):
+            nc += lib().orc_transport_step(ctypes.byref(self.cfg), ctypes.byref(self.st))
+        return nc
+
+    def density(self, s):
+        out = np.zeros(self.N)
+        lib().orc_solute_density(ctypes.byref(self.cfg), ctypes.byref(self.st), s, _p(out))
+        return out
+
+    def set_conc(self, s, values):
+        v = np.asarray(values, np.float64).reshape(-1)
+        if self.cfg.immobile[s]:
+            self.imm[s * self.N:(s + 1) * self.N] = v
+        else:
+            t = np.array([0.25] + [0.125] * 6)
+            for i in range(7):
+                self.g[(s * 7 + i) * self.N:(s * 7 + i + 1) * self.N] = t[i] * v
+
+    def set_biomass(self, m, values):
+        self.bio[m * self.N:(m + 1) * self.N] = np.asarray(values, np.float64).reshape(-1)
+
+    def biomass(self, m):
+        return self.bio[m * self.N:(m + 1) * self.N].copy()
+
+    def precip_convert(self):
+        return lib().orc_precip_convert(ctypes.byref(self.cfg), ctypes.byref(self.st))
+
+
+def eq_batch(sys, totals, cold_species, x0=None, start=0):
+    n = totals.shape[0]
+    nc = sys.n_comp
+    x = np.zeros((n, nc)) if x0 is None else np.array(x0, np.float64, copy=True)
+    it = np.zeros(n, np.int32)
+    stt = np.zeros(n, np.uint8)
+    lib().orc_eq_batch(ctypes.byref(sys), _p(np.ascontiguousarray(totals, np.float64)),
+                       _p(np.ascontiguousarray(cold_species, np.float64)), _p(x), _p(it), _p(stt),
+                       ctypes.c_int64(n), start)
+    return x, it, stt
+
+
+def eq_residual(sys, totals, x):
+    t = np.ascontiguousarray(totals, np.float64)
+    xx = np.ascontiguousarray(x, np.float64)
+    return np.array([lib().orc_eq_residual(ctypes.byref(sys), _p(t[k]), _p(xx[k])) for k in range(t.shape[0])])
+
+
+def mlp_forward_backward(n_in, H, n_out, params, x, y, want_grad=True):
+    p = np.ascontiguousarray(params, np.float64)
+    x = np.ascontiguousarray(x, np.float64)
+    y = np.ascontiguousarray(y, np.float64)
+    g = np.zeros_like(p) if want_grad else None
+    yh = np.zeros((x.shape[0], n_out))
+    loss = lib().orc_mlp_forward_backward(n_in, H, n_out, _p(p), _p(x), _p(y), x.shape[0], _p(g), _p(yh))
+    return loss, g, yh
+
+
+def surrogate_forward(net, x):
+    x = np.ascontiguousarray(x, np.float64)
+    n = x.shape[0]
+    y = np.zeros((n, net.widths[net.n_layers]))
+    lib().orc_surrogate_forward(ctypes.byref(net), _p(x), _p(y), ctypes.c_int64(n))
+    return y
+
+
+def rates(cfg, abiotic, C, B=None):
+    S, M = cfg.n_solutes, max(cfg.n_microbes, 1)
+    R = np.zeros(S)
+    BR = np.zeros(M)
+    Bv = np.zeros(M) if B is None else np.asarray(B, np.float64)
+    lib().orc_rates(ctypes.byref(cfg), abiotic, _p(np.asarray(C, np.float64)), _p(Bv), _p(R), _p(BR))
+    return R, BR
+
+
+# ---- reference's own code -------------------------------------------------
+def ref_pcf_solve(stoich, logk, comp_species, species, max_iter=200, tol=1e-10, depth=4):
+    r = ref_lib()
+    stoich = np.ascontiguousarray(stoich, np.float64)
+    ns, nc = stoich.shape
+    species = np.ascontiguousarray(species, np.float64).reshape(-1, ns)
+    n = species.shape[0]
+    out = np.zeros_like(species)
+    it = np.zeros(n, np.int32)
+    cv = np.zeros(n, np.uint8)
+    cs = np.ascontiguousarray(comp_species, np.int32)
+    r.ref_pcf_solve(nc, ns, _p(stoich), _p(np.ascontiguousarray(logk, np.float64)), _p(cs), _p(species),
+                    _p(out), _p(it), _p(cv), ctypes.c_int64(n), max_iter, ctypes.c_double(tol), depth)
+    return out, it, cv
+
+
+def ref_surrogate(fin):
+    fin = np.ascontiguousarray(fin, np.float64).reshape(-1, 2)
+    out = np.zeros(fin.shape[0])
+    ref_lib().ref_surrogate(_p(fin), _p(out), ctypes.c_int64(fin.shape[0]))
+    return out
+
+
+def ref_kinetics_ex05(B, C, mask=2):
+    B = np.asarray(B, np.float64); C = np.asarray(C, np.float64)
+    sr = np.zeros(C.size); br = np.zeros(B.size)
+    ref_lib().ref_kinetics_ex05(_p(B), B.size, _p(C), C.size, mask, _p(sr), _p(br))
+    return sr, br
+
+
+def ref_abiotic_ex13(C, mask=2):
+    C = np.asarray(C, np.float64)
+    sr = np.zeros(C.size)
+    ref_lib().ref_abiotic_ex13(_p(C), C.size, mask, _p(sr))
+    return sr
