@@ -715,15 +715,19 @@ extern "C" int cl_eq_train(cl_eq_solver* s, const double* d_totals, const double
     std::mt19937_64 rng(seed);
     std::vector<int64_t> order(nb);
     for (int64_t i = 0; i < nb; ++i) order[i] = i;
+    const double total_steps = (double)epochs * (double)nb;
+    int64_t step = 0;
     for (int ep = 0; ep < epochs && !r; ++ep) {
         std::shuffle(order.begin(), order.end(), rng);
-        for (int64_t bi = 0; bi < nb; ++bi) {
+        for (int64_t bi = 0; bi < nb; ++bi, ++step) {
             ++s->adam_t;
             const float b1c = 1.f - std::pow(0.9f, (float)s->adam_t), b2c = 1.f - std::pow(0.999f, (float)s->adam_t);
+            // cosine decay of the learning rate over the whole run, floor 5% of lr
+            const float lr_t = lr * (float)(0.05 + 0.95 * 0.5 * (1.0 + std::cos(3.141592653589793 * step / total_steps)));
             mlp_grad_kernel<<<blocks, MLP_THREADS, mlp_smem_bytes(), s->stream>>>(
                 s->w, nc, Xn, Yn, order[bi] * batch, batch, 1.f / ((float)batch * nc), s->part, np);
             mlp_update_kernel<<<64, 256, 0, s->stream>>>(s->w, nc, s->master, s->m1, s->m2, s->part, blocks, np,
-                                                         (bi == nb - 1) ? s->grad : nullptr, lr, b1c, b2c, 1);
+                                                         (bi == nb - 1) ? s->grad : nullptr, lr_t, b1c, b2c, 1);
         }
         e = cudaGetLastError();
         if (e != cudaSuccess) r = cuda_fail(e, "mlp training");

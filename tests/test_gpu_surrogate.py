@@ -42,6 +42,6 @@ def test_tensor_core_matches_fp32(gpu_lib, pkg, n):
     y32 = pkg.surrogate_batch(net, x, mode=pkg.SRG_FP32)
     ytc = pkg.surrogate_batch(net, x, mode=pkg.SRG_TENSOR)
     yo = o.surrogate_forward(net, x.astype(np.float64))
-    rng_out = yo.max(0) - yo.min(0) + 1e-12
+    rng_out = np.maximum(yo.max(0) - yo.min(0), np.abs(yo).max(0)) + 1e-12
     assert np.max(np.abs(y32 - yo) / rng_out) < 1e-5
     assert np.max(np.abs(ytc - y32) / rng_out) < 2e-2
