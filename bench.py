@@ -281,6 +281,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-speciation", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--shape", default=None, help="override nx,ny,nz (development only)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -366,7 +367,8 @@ def main():
         out["flow_kernel"] = {"achieved_gbs": fb / (flow_ms / flow_n * 1e-3) / 1e9, "avg_launch_ms": flow_ms / flow_n,
                               "launches": flow_n, "share_of_step": flow_ms / ms if ms else None}
     # end to end through the C ABI with pinned host buffers
-    out["e2e"] = e2e_run(pkg, torch, cfg, mask, bio, args.steps, stream, world)
+    if not args.no_e2e:
+        out["e2e"] = e2e_run(pkg, torch, cfg, mask, bio, args.steps, stream, world)
     lat.close()
     if rank == 0 and world == 1 and not args.no_speciation:
         out["speciation"] = speciation_bench(pkg, wl, stream)

@@ -57,7 +57,7 @@ __device__ __forceinline__ double site_density(Geo g, const float* pm, int64_t n
     int x, y, z;
     decode(g, n, x, y, z);
     float f[7];
-    gather7<PARITY>(pm, g, n, x, y, z, f);
+    gather7<PARITY>(pm, (uint32_t)g.N, make_site(g, x, y, z, (uint32_t)n), f);
     double r = 0.0;
 #pragma unroll
     for (int i = 0; i < 7; ++i) r += f[i];
@@ -101,7 +101,7 @@ __global__ void ade_io_kernel(Geo g, const float* pm, float* nat) {
         int x, y, z;
         decode(g, n, x, y, z);
         float f[7];
-        gather7<PARITY>(pm, g, n, x, y, z, f);
+        gather7<PARITY>(pm, (uint32_t)g.N, make_site(g, x, y, z, (uint32_t)n), f);
 #pragma unroll
         for (int i = 0; i < 7; ++i) nat[i * g.N + n] = f[i];
     }

@@ -28,6 +28,7 @@
 namespace cl {
 
 #define THRD 1e-12
+constexpr int kGroup = 4;   // solutes whose populations are in flight together
 
 struct AdeK {
     Geo g;
@@ -46,27 +47,20 @@ struct AdeK {
 };
 
 template <int PARITY>
-__device__ __forceinline__ void gather7(const float* pop, const Geo& g, int64_t n, int x, int y, int z, float* f) {
+__device__ __forceinline__ void gather7(const float* pop, uint32_t N, const Site& st, float* f) {
 #pragma unroll
     for (int i = 0; i < 7; ++i) {
-        if (PARITY == 0) f[i] = pop[i * g.N + n];
-        else {
-            const int64_t m = nbr(g, n, x, y, z, -c7x(i), -c7y(i), -c7z(i));
-            f[i] = (m < 0) ? pop[i * g.N + n] : pop[opp7(i) * g.N + m];
-        }
+        if (PARITY == 0 || !st.inx(-c7x(i))) f[i] = pop[i * N + st.n];
+        else f[i] = pop[opp7(i) * N + st.at(-c7x(i), -c7y(i), -c7z(i))];
     }
 }
 
 template <int PARITY>
-__device__ __forceinline__ void scatter7(float* pop, const Geo& g, int64_t n, int x, int y, int z, const float* f) {
+__device__ __forceinline__ void scatter7(float* pop, uint32_t N, const Site& st, const float* f) {
 #pragma unroll
     for (int i = 0; i < 7; ++i) {
-        if (PARITY == 0) pop[opp7(i) * g.N + n] = f[i];
-        else {
-            const int64_t m = nbr(g, n, x, y, z, c7x(i), c7y(i), c7z(i));
-            if (m < 0) pop[opp7(i) * g.N + n] = f[i];
-            else pop[i * g.N + m] = f[i];
-        }
+        if (PARITY == 0 || !st.inx(c7x(i))) pop[opp7(i) * N + st.n] = f[i];
+        else pop[i * N + st.at(c7x(i), c7y(i), c7z(i))] = f[i];
     }
 }
 
@@ -85,7 +79,8 @@ __device__ __forceinline__ void collide7(float* f, float om, float ux, float uy,
 }
 
 // Table-driven rate law (defineRxnKinetics / defineAbioticRxnKinetics ABI).
-// C, R, B, BR are shared-memory columns with stride bd.
+// C, R, B, BR are shared-memory columns with stride bd.  Concentrations below
+// thrd read as zero, as the processors floor them before the call.
 static __device__ void rates_dev(const AdeParams& p, int abiotic, const double* C, const double* B,
                           double* R, double* BR, int bd) {
     for (int s = 0; s < p.S; ++s) R[s * bd] = 0.0;
@@ -100,10 +95,14 @@ static __device__ void rates_dev(const AdeParams& p, int abiotic, const double* 
             rate *= b;
         }
         for (int j = 0; j < r.n_monod; ++j) {
-            const double c = fmax(C[r.monod_s[j] * bd], 0.0);
+            const double c0 = C[r.monod_s[j] * bd];
+            const double c = c0 < THRD ? 0.0 : c0;
             rate *= c / (r.monod_ks[j] + c);
         }
-        for (int j = 0; j < r.n_mass; ++j) rate *= fmax(C[r.mass_s[j] * bd], 0.0);
+        for (int j = 0; j < r.n_mass; ++j) {
+            const double c0 = C[r.mass_s[j] * bd];
+            rate *= c0 < THRD ? 0.0 : c0;
+        }
         for (int s = 0; s < p.S; ++s) R[s * bd] = fma(r.nu[s], rate, R[s * bd]);
         if (!abiotic) BR[r.microbe * bd] = fma(r.yield, rate, BR[r.microbe * bd]);
     }
@@ -118,15 +117,14 @@ static __device__ void rates_dev(const AdeParams& p, int abiotic, const double* 
 // solute.  Returns 1 if the equilibrium solve did not converge.
 template <int NC>
 __device__ int reaction_chain(const AdeK& k, int64_t n, uint8_t cls, double* Cur, double* App,
-                              double* Ct, double* R, double* B, double* BR, int bd) {
+                              double* R, double* B, double* BR, int bd) {
     const AdeParams& p = k.p;
     const int64_t N = k.g.N;
     int nonconv = 0;
     // run_kinetics (part1.hh:63-146) + update_rxnLattices (:338-429)
     if (p.do_kin) {
-        for (int s = 0; s < p.S; ++s) { const double c = Cur[s * bd]; Ct[s * bd] = c < THRD ? 0.0 : c; }
         for (int m = 0; m < p.M; ++m) { const double b = k.bio[m * N + n]; B[m * bd] = b < THRD ? 0.0 : b; }
-        rates_dev(p, 0, Ct, B, R, BR, bd);
+        rates_dev(p, 0, Cur, B, R, BR, bd);
         for (int s = 0; s < p.S; ++s) {
             const double d = R[s * bd] * p.dt;
             if (d > THRD || d < -THRD) { Cur[s * bd] += d; App[s * bd] += d; }
@@ -138,25 +136,22 @@ __device__ int reaction_chain(const AdeK& k, int64_t n, uint8_t cls, double* Cur
     }
     // dC = dC0; run_abiotic_kinetics | surfaceAbioticKinetics3D; update_abiotic_rxnLattices
     if (p.do_abio && (!p.surface_only || (cls & F_SURFACE))) {
-        for (int s = 0; s < p.S; ++s) { const double c = Cur[s * bd]; Ct[s * bd] = c < THRD ? 0.0 : c; }
-        rates_dev(p, 1, Ct, nullptr, R, nullptr, bd);
+        rates_dev(p, 1, Cur, nullptr, R, nullptr, bd);
         for (int s = 0; s < p.S; ++s) {
             const double d = R[s * bd] * p.dt;
             if (d > THRD || d < -THRD) { Cur[s * bd] += d; App[s * bd] += d; }
         }
     }
-    // run_equilibrium_biotic (part4_eqsolver.hh:1355-1494), Newton applied only
-    // when converged (run_equilibrium_NR, NR_reserve.hh:734)
+    // run_equilibrium_biotic (part4_eqsolver.hh:1355-1494): species floored at
+    // 1e-30; Newton applied only when converged (run_equilibrium_NR, NR_reserve.hh:734)
     if constexpr (NC > 0) {
         const EqDev& e = k.e;
         double x[NC], T[NC];
-        for (int s = 0; s < p.S; ++s) Ct[s * bd] = fmax(Cur[s * bd], 1e-30);
-        // totals and cold start read the floored species column
 #pragma unroll
         for (int j = 0; j < NC; ++j) T[j] = 0.0;
         for (int i = 0; i < e.ns; ++i) {
             if (!e.active[i]) continue;
-            const double c = fmin(fmax(Ct[i * bd], 1e-30), 10.0);
+            const double c = fmin(fmax(Cur[i * bd], 1e-30), 10.0);
 #pragma unroll
             for (int j = 0; j < NC; ++j) T[j] = fma(e.stoich[i][j], c, T[j]);
         }
@@ -165,7 +160,7 @@ __device__ int reaction_chain(const AdeK& k, int64_t n, uint8_t cls, double* Cur
             T[j] = fmax(T[j], 1e-30);
             double c = 1e-7;
             const int idx = e.comp_species[j];
-            if (idx >= 0) c = Ct[idx * bd];
+            if (idx >= 0) c = Cur[idx * bd];
             x[j] = log10(fmin(fmax(c, 1e-30), 10.0));
         }
         int conv = 0;
@@ -174,7 +169,7 @@ __device__ int reaction_chain(const AdeK& k, int64_t n, uint8_t cls, double* Cur
         if (!conv) nonconv = 1;
         else {
             for (int s = 0; s < p.S && s < e.ns; ++s) {
-                const double conc = Ct[s * bd];
+                const double conc = fmax(Cur[s * bd], 1e-30);
                 double eqc = e.active[s] ? species_c<NC>(e, s, x) : fmin(conc, 10.0);
                 eqc = fmin(fmax(eqc, 1e-30), 10.0);
                 double d = eqc - conc;
@@ -189,78 +184,100 @@ __device__ int reaction_chain(const AdeK& k, int64_t n, uint8_t cls, double* Cur
 }
 
 template <int NMOB, int NC, int PARITY>
-__global__ void __launch_bounds__(256) ade_main_kernel(AdeK k) {
+__global__ void __launch_bounds__(256, 2) ade_main_kernel(AdeK k) {
     extern __shared__ double sm[];
     const int bd = blockDim.x;
     const AdeParams& p = k.p;
     double* Cur = sm + threadIdx.x;
     double* App = Cur + p.S * bd;
-    double* Ct  = App + p.S * bd;
-    double* R   = Ct + p.S * bd;
+    double* R   = App + p.S * bd;
     double* B   = R + p.S * bd;
     double* BR  = B + (p.M > 0 ? p.M : 1) * bd;
     const int64_t N = k.g.N, plane = k.g.plane;
-    const int64_t lo = plane, hi = N - plane;                 // interior x = 1 .. nx-2
-    const int64_t stride = (int64_t)gridDim.x * bd;
+    const uint32_t N32 = (uint32_t)N;
     const bool any_rxn = p.do_kin || p.do_abio || NC > 0;
     unsigned long long nonconv = 0;
-    for (int64_t n = lo + (int64_t)blockIdx.x * bd + threadIdx.x; n < hi; n += stride) {
+    const RowMap rm = make_rowmap(k.g.nz);
+    const int row_lo = k.g.ny, row_hi = (k.g.nx - 1) * k.g.ny;     // interior x = 1 .. nx-2
+    for (int row0 = row_lo + blockIdx.x * rm.rpb; row0 < row_hi; row0 += gridDim.x * rm.rpb) {
+      const int row = row0 + rm.lrow;
+      if (!rm.active || row >= row_hi) continue;
+      const int x = row / k.g.ny, y = row - x * k.g.ny;
+      for (int z = rm.z0; z < k.g.nz; z += rm.zstep) {
+        const uint32_t n = (uint32_t)row * (uint32_t)k.g.nz + (uint32_t)z;
         const uint8_t cls = k.cls[n];
         const uint8_t dyn = cls & 3;
         if (dyn == BB) continue;
         if (dyn == NODYN && !k.nodyn_coupled) continue;
-        int x, y, z;
-        decode(k.g, n, x, y, z);
+        const Site st = make_site(k.g, x, y, z, n);
         float dC[NMOB];
 #pragma unroll
         for (int m = 0; m < NMOB; ++m) dC[m] = 0.f;
         if (dyn != NODYN && (cls & F_REACTIVE) && any_rxn) {
-            // pass 1: densities
-            for (int s = 0; s < p.S; ++s) { App[s * bd] = 0.0; }
+            // pass 1: the populations of a group of solutes in flight at once, then the densities
+            for (int s = 0; s < p.S; ++s) App[s * bd] = 0.0;
 #pragma unroll
-            for (int m = 0; m < NMOB; ++m) {
-                float f[7];
-                gather7<PARITY>(k.pop + (int64_t)m * 7 * N, k.g, n, x, y, z, f);
-                float r = 0.f;
+            for (int m0 = 0; m0 < NMOB; m0 += kGroup) {
+                float f[kGroup][7];
 #pragma unroll
-                for (int i = 0; i < 7; ++i) r += f[i];
-                Cur[p.mob_index[m] * bd] = (double)r;
+                for (int j = 0; j < kGroup; ++j)
+                    if (m0 + j < NMOB) gather7<PARITY>(k.pop + (int64_t)(m0 + j) * 7 * N, N32, st, f[j]);
+#pragma unroll
+                for (int j = 0; j < kGroup; ++j) {
+                    if (m0 + j >= NMOB) continue;
+                    float r = 0.f;
+#pragma unroll
+                    for (int i = 0; i < 7; ++i) r += f[j][i];
+                    Cur[p.mob_index[m0 + j] * bd] = (double)r;
+                }
             }
             for (int s = 0; s < p.S; ++s)
                 if (p.mob_slot[s] < 0) Cur[s * bd] = k.imm[(int64_t)s * N + n];
-            nonconv += reaction_chain<NC>(k, n, cls, Cur, App, Ct, R, B, BR, bd);
+            nonconv += reaction_chain<NC>(k, n, cls, Cur, App, R, B, BR, bd);
 #pragma unroll
             for (int m = 0; m < NMOB; ++m) dC[m] = (float)App[p.mob_index[m] * bd];
             for (int s = 0; s < p.S; ++s)
                 if (p.mob_slot[s] < 0 && App[s * bd] != 0.0) k.imm[(int64_t)s * N + n] += App[s * bd];
         }
-        // pass 2: collide, add t_i*dC, stream
+        // keep the second gather after the chain: hoisting it would hold all
+        // populations in registers across the Newton solve
+        asm volatile("" ::: "memory");
+        // pass 2: gather every solute (L1/L2 hits after pass 1), collide, add t_i*dC, stream
         const float ux = k.u[n], uy = k.u[N + n], uz = k.u[2 * N + n];
         const bool adj = (x == 1 || x == k.g.nx - 2);
 #pragma unroll
-        for (int m = 0; m < NMOB; ++m) {
-            float* pm = k.pop + (int64_t)m * 7 * N;
-            float f[7];
-            gather7<PARITY>(pm, k.g, n, x, y, z, f);
-            float rho = 0.f;
-            if (dyn != NODYN) {
-                const float om = (dyn == BIO) ? p.omega_bio[m] : p.omega_pore[m];
-                collide7(f, om, ux, uy, uz, rho);
-                const float d = dC[m];
-                if (d != 0.f) {
+        for (int m0 = 0; m0 < NMOB; m0 += kGroup) {
+            float f[kGroup][7];
 #pragma unroll
-                    for (int i = 0; i < 7; ++i) f[i] += t7(i) * d;
+            for (int j = 0; j < kGroup; ++j)
+                if (m0 + j < NMOB) gather7<PARITY>(k.pop + (int64_t)(m0 + j) * 7 * N, N32, st, f[j]);
+#pragma unroll
+            for (int j = 0; j < kGroup; ++j) {
+                const int m = m0 + j;
+                if (m >= NMOB) continue;
+                float rho = 0.f;
+                if (dyn != NODYN) {
+                    const float om = (dyn == BIO) ? p.omega_bio[m] : p.omega_pore[m];
+                    collide7(f[j], om, ux, uy, uz, rho);
+                    const float d = dC[m];
+                    if (d != 0.f) {
+#pragma unroll
+                        for (int i = 0; i < 7; ++i) f[j][i] += t7(i) * d;
+                    }
+                } else if (adj) {
+#pragma unroll
+                    for (int i = 0; i < 7; ++i) rho += f[j][i];
                 }
-            } else if (adj) {
+                if (adj) {
+                    const int side = (x == 1) ? 0 : 1;
+                    k.rho_adj[((int64_t)m * 2 + side) * plane + (n - (int64_t)x * plane)] = rho;
+                }
+            }
 #pragma unroll
-                for (int i = 0; i < 7; ++i) rho += f[i];
-            }
-            if (adj) {
-                const int side = (x == 1) ? 0 : 1;
-                k.rho_adj[((int64_t)m * 2 + side) * plane + (n - (int64_t)x * plane)] = rho;
-            }
-            scatter7<PARITY>(pm, k.g, n, x, y, z, f);
+            for (int j = 0; j < kGroup; ++j)
+                if (m0 + j < NMOB) scatter7<PARITY>(k.pop + (int64_t)(m0 + j) * 7 * N, N32, st, f[j]);
         }
+      }
     }
     if (nonconv) atomicAdd(&k.counters[0], nonconv);
 }
@@ -281,12 +298,13 @@ __global__ void __launch_bounds__(256) ade_boundary_kernel(AdeK k) {
         if (dyn == NODYN && !k.nodyn_coupled) continue;
         int x, y, z;
         decode(k.g, n, x, y, z);
+        const Site st = make_site(k.g, x, y, z, (uint32_t)n);
         const float ux = k.u[n], uy = k.u[N + n], uz = k.u[2 * N + n];
 #pragma unroll
         for (int m = 0; m < NMOB; ++m) {
             float* pm = k.pop + (int64_t)m * 7 * N;
             float f[7];
-            gather7<PARITY>(pm, k.g, n, x, y, z, f);
+            gather7<PARITY>(pm, (uint32_t)N, st, f);
             if (dyn != NODYN) {
                 const int unk = side == 0 ? 4 : 1;
                 const int neu = side == 0 ? p.left_neu[m] : p.right_neu[m];
@@ -300,7 +318,7 @@ __global__ void __launch_bounds__(256) ade_boundary_kernel(AdeK k) {
                 float rho;
                 collide7(f, om, ux, uy, uz, rho);
             }
-            scatter7<PARITY>(pm, k.g, n, x, y, z, f);
+            scatter7<PARITY>(pm, (uint32_t)N, st, f);
         }
     }
 }
@@ -327,7 +345,8 @@ template <int NMOB, int NC>
 inline int launch_step(Ctx* c, const AdeK& k) {
     const int bd = 256;
     const int S = c->ap.S, M = c->ap.M > 0 ? c->ap.M : 1;
-    const size_t smem = (size_t)(4 * S + 2 * M) * bd * sizeof(double);
+    const bool any_rxn = c->ap.do_kin || c->ap.do_abio || NC > 0;
+    const size_t smem = any_rxn ? (size_t)(3 * S + 2 * M) * bd * sizeof(double) : 0;
     const int64_t interior = c->geo.N - 2 * c->geo.plane;
     const int blocks = grid_for(interior, bd, 148 * 8);
     int r = timing_begin(c, CL_KERNEL_ADE_MAIN);

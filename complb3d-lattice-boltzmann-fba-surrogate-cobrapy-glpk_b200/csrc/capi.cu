@@ -49,6 +49,10 @@ static int validate(const cl_config* c) {
     if (c->n_solutes < 0 || c->n_solutes > CL_MAX_SOLUTES) { set_error("n_solutes out of range"); return CL_ERR_ARG; }
     if (c->n_microbes < 0 || c->n_microbes > CL_MAX_MICROBES) { set_error("n_microbes out of range"); return CL_ERR_ARG; }
     if (c->n_rxn < 0 || c->n_rxn > CL_MAX_RXN) { set_error("n_rxn out of range"); return CL_ERR_ARG; }
+    {
+        const int64_t N = (int64_t)c->nx * c->ny * c->nz;
+        if (N * 19 >= (int64_t)1 << 32) { set_error("lattice too large: 19*nx*ny*nz must stay below 2^32"); return CL_ERR_ARG; }
+    }
     if (c->n_pore_codes < 0 || c->n_pore_codes > CL_MAX_CODES || c->n_bio_codes < 0 || c->n_bio_codes > CL_MAX_CODES) {
         set_error("material code lists out of range"); return CL_ERR_ARG;
     }

@@ -64,66 +64,82 @@ __device__ __forceinline__ void regularize(float* f, float rb, float& jx) {
 }
 
 template <int PARITY>
-__device__ __forceinline__ void gather19(const FlowK& k, int64_t n, int x, int y, int z, float* f) {
-    const int64_t N = k.g.N;
+__device__ __forceinline__ void gather19(const FlowK& k, const Site& st, float* f) {
+    const uint32_t N = (uint32_t)k.g.N;
 #pragma unroll
     for (int i = 0; i < 19; ++i) {
-        if (PARITY == 0) {
-            f[i] = k.f[i * N + n];
+        if (PARITY == 0 || !st.inx(-c19x(i))) {
+            f[i] = k.f[i * N + st.n];
         } else {
-            int64_t m = nbr(k.g, n, x, y, z, -c19x(i), -c19y(i), -c19z(i));
-            f[i] = (m < 0) ? k.f[i * N + n] : k.f[opp19(i) * N + m];
+            f[i] = k.f[opp19(i) * N + st.at(-c19x(i), -c19y(i), -c19z(i))];
         }
     }
 }
 
 template <int PARITY>
-__device__ __forceinline__ void scatter19(const FlowK& k, int64_t n, int x, int y, int z, const float* f) {
-    const int64_t N = k.g.N;
+__device__ __forceinline__ void scatter19(const FlowK& k, const Site& st, const float* f) {
+    const uint32_t N = (uint32_t)k.g.N;
 #pragma unroll
     for (int i = 0; i < 19; ++i) {
-        if (PARITY == 0) {
-            k.f[opp19(i) * N + n] = f[i];
+        if (PARITY == 0 || !st.inx(c19x(i))) {
+            k.f[opp19(i) * N + st.n] = f[i];
         } else {
-            int64_t m = nbr(k.g, n, x, y, z, c19x(i), c19y(i), c19z(i));
-            if (m < 0) k.f[opp19(i) * N + n] = f[i];
-            else k.f[i * N + m] = f[i];
+            k.f[i * N + st.at(c19x(i), c19y(i), c19z(i))] = f[i];
         }
     }
 }
 
+__device__ __forceinline__ Site site_of(const Geo& g, int64_t n) {
+    int x, y, z;
+    decode(g, n, x, y, z);
+    return make_site(g, x, y, z, (uint32_t)n);
+}
+
+// One site of the collide-stream; returns 0.5|j|^2 for BGK sites.
 template <int PARITY>
-__global__ void __launch_bounds__(256) flow_aa_kernel(FlowK k) {
+__device__ __forceinline__ double flow_site(const FlowK& k, const Site& st, int x, uint8_t cls) {
+    float f[19];
+    gather19<PARITY>(k, st, f);
+    double e = 0.0;
+    if (cls != NODYN) {
+        const float om = (cls == BIO) ? k.omega_bio : k.omega;
+        float rb, jx, jy = 0.f, jz = 0.f;
+        if (x == 0) { rb = k.rb_in; regularize<-1>(f, rb, jx); }
+        else if (x == k.g.nx - 1) { rb = k.rb_out; regularize<1>(f, rb, jx); }
+        else {
+            rb = 0.f; jx = 0.f;
+#pragma unroll
+            for (int i = 0; i < 19; ++i) {
+                rb += f[i];
+                jx += c19x(i) * f[i]; jy += c19y(i) * f[i]; jz += c19z(i) * f[i];
+            }
+        }
+        const float jsq = jx * jx + jy * jy + jz * jz;
+#pragma unroll
+        for (int i = 0; i < 19; ++i) f[i] = f[i] * (1.f - om) + om * feq19(i, rb, jx, jy, jz, jsq);
+        e = 0.5 * (double)jsq;
+    }
+    scatter19<PARITY>(k, st, f);
+    return e;
+}
+
+template <int PARITY>
+__global__ void __launch_bounds__(256, 3) flow_aa_kernel(FlowK k) {
     if (k.tracer && k.tracer->converged) return;
     double esum = 0.0;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < k.g.N; n += stride) {
-        const uint8_t cls = k.cls[n];
-        if (cls == BB) continue;                 // AA bounce-back is a no-op
-        if (cls == NODYN && !k.nodyn_coupled) continue;
-        int x, y, z;
-        decode(k.g, n, x, y, z);
-        float f[19];
-        gather19<PARITY>(k, n, x, y, z, f);
-        if (cls != NODYN) {
-            const float om = (cls == BIO) ? k.omega_bio : k.omega;
-            float rb, jx, jy = 0.f, jz = 0.f;
-            if (x == 0) { rb = k.rb_in; regularize<-1>(f, rb, jx); }
-            else if (x == k.g.nx - 1) { rb = k.rb_out; regularize<1>(f, rb, jx); }
-            else {
-                rb = 0.f; jx = 0.f;
-#pragma unroll
-                for (int i = 0; i < 19; ++i) {
-                    rb += f[i];
-                    jx += c19x(i) * f[i]; jy += c19y(i) * f[i]; jz += c19z(i) * f[i];
-                }
-            }
-            const float jsq = jx * jx + jy * jy + jz * jz;
-#pragma unroll
-            for (int i = 0; i < 19; ++i) f[i] = f[i] * (1.f - om) + om * feq19(i, rb, jx, jy, jz, jsq);
-            esum += 0.5 * (double)jsq;
+    const RowMap rm = make_rowmap(k.g.nz);
+    const int rows = k.g.nx * k.g.ny;
+    for (int row0 = blockIdx.x * rm.rpb; row0 < rows; row0 += gridDim.x * rm.rpb) {
+        const int row = row0 + rm.lrow;
+        if (!rm.active || row >= rows) continue;
+        const int x = row / k.g.ny, y = row - x * k.g.ny;
+        for (int z = rm.z0; z < k.g.nz; z += rm.zstep) {
+            const uint32_t n = (uint32_t)row * (uint32_t)k.g.nz + (uint32_t)z;
+            const uint8_t cls = k.cls[n];
+            if (cls == BB) continue;                 // AA bounce-back is a no-op
+            if (cls == NODYN && !k.nodyn_coupled) continue;
+            esum += flow_site<PARITY>(k, make_site(k.g, x, y, z, n), x, cls);
         }
-        scatter19<PARITY>(k, n, x, y, z, f);
     }
     // deterministic block reduction of the energy
     __shared__ double red[8];
@@ -250,7 +266,7 @@ __global__ void flow_macro_kernel(FlowK k, double* rho, float* u) {
         decode(k.g, n, x, y, z);
         const uint8_t cls = k.cls[n];
         float f[19];
-        gather19<PARITY>(k, n, x, y, z, f);
+        gather19<PARITY>(k, make_site(k.g, x, y, z, (uint32_t)n), f);
         float rb = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
         const bool bgk = (cls == FLUID || cls == BIO);
         if (bgk && x == 0) { rb = k.rb_in; regularize<-1>(f, rb, jx); }
@@ -284,10 +300,8 @@ __global__ void flow_io_kernel(FlowK k, float* nat, int to_natural) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < k.g.N; n += stride) {
         if (to_natural) {
-            int x, y, z;
-            decode(k.g, n, x, y, z);
             float f[19];
-            gather19<PARITY>(k, n, x, y, z, f);
+            gather19<PARITY>(k, site_of(k.g, n), f);
 #pragma unroll
             for (int i = 0; i < 19; ++i) nat[i * k.g.N + n] = f[i];
         } else {

@@ -78,4 +78,60 @@ __device__ __forceinline__ int64_t nbr(const Geo& g, int64_t n, int x, int y, in
     return m;
 }
 
+// Row-blocked traversal: a block walks whole z-rows (x, y fixed), so x and y
+// come from one 32-bit division per row and the neighbour offsets are row
+// constants.  Offsets inside one population array are 32-bit (the context
+// refuses lattices with 19*N >= 2^32).
+struct Site {
+    uint32_t n;
+    int32_t oxm, oxp, oym, oyp, ozm, ozp;
+    bool hxm, hxp;     // x-1 / x+1 inside 0..nx-1
+    __device__ __forceinline__ uint32_t at(int dx, int dy, int dz) const {
+        int32_t o = 0;
+        if (dx < 0) o += oxm; else if (dx > 0) o += oxp;
+        if (dy < 0) o += oym; else if (dy > 0) o += oyp;
+        if (dz < 0) o += ozm; else if (dz > 0) o += ozp;
+        return (uint32_t)((int32_t)n + o);
+    }
+    __device__ __forceinline__ bool inx(int dx) const { return dx < 0 ? hxm : (dx > 0 ? hxp : true); }
+};
+
+__device__ __forceinline__ Site make_site(const Geo& g, int x, int y, int z, uint32_t n) {
+    Site s;
+    s.n = n;
+    const int32_t plane = (int32_t)g.plane, nz = g.nz;
+    s.oxm = -plane; s.oxp = plane;
+    s.oym = (y == 0) ? (g.ny - 1) * nz : -nz;
+    s.oyp = (y == g.ny - 1) ? -(g.ny - 1) * nz : nz;
+    s.ozm = (z == 0) ? nz - 1 : -1;
+    s.ozp = (z == nz - 1) ? -(nz - 1) : 1;
+    s.hxm = x > 0;
+    s.hxp = x < g.nx - 1;
+    return s;
+}
+
+// Threads of a block cover `rows_per_block` consecutive z-rows when nz is
+// smaller than the block, or loop over z in block-sized chunks otherwise.
+struct RowMap {
+    int rpb;      // rows per block iteration
+    int lrow;     // this thread's row within the block's rows
+    int z0;       // this thread's first z
+    int zstep;    // z stride
+    bool active;  // thread maps to a z
+};
+
+__device__ __forceinline__ RowMap make_rowmap(int nz) {
+    RowMap r;
+    const int bd = blockDim.x, t = threadIdx.x;
+    if (nz >= bd) { r.rpb = 1; r.lrow = 0; r.z0 = t; r.zstep = bd; r.active = true; }
+    else {
+        r.rpb = bd / nz;
+        r.lrow = t / nz;
+        r.z0 = t - r.lrow * nz;
+        r.zstep = nz;
+        r.active = r.lrow < r.rpb;
+    }
+    return r;
+}
+
 }  // namespace cl

@@ -19,21 +19,26 @@
 // Species are evaluated on the fly (no per-species storage), the component
 // count NC is a template parameter so every array lives in registers.
 #pragma once
+#include <cmath>
 #include "../../include/complab_gpu.h"
 
 namespace cl {
 
 struct EqDev {
     int ns;
+    int all_int;                       // every stoichiometric coefficient is an integer in [-8, 8]
     double stoich[CL_MAX_SPECIES][CL_MAX_COMP];
     double absS[CL_MAX_SPECIES][CL_MAX_COMP];
     double logk[CL_MAX_SPECIES];
+    double k10[CL_MAX_SPECIES];        // 10^logK
+    signed char ipow[CL_MAX_SPECIES][CL_MAX_COMP];
     int active[CL_MAX_SPECIES];
     int comp_species[CL_MAX_COMP];
 };
 
 inline void eqdev_from_system(const cl_eq_system& s, EqDev& d) {
     d.ns = s.n_species;
+    d.all_int = 1;
     for (int i = 0; i < CL_MAX_SPECIES; ++i) {
         int act = 0;
         for (int j = 0; j < CL_MAX_COMP; ++j) {
@@ -41,9 +46,13 @@ inline void eqdev_from_system(const cl_eq_system& s, EqDev& d) {
             d.stoich[i][j] = v;
             d.absS[i][j] = v < 0 ? -v : v;
             if (v > 1e-10 || v < -1e-10) act = 1;
+            const double r = v < 0 ? -(double)(long long)(-v + 0.5) : (double)(long long)(v + 0.5);
+            if (r != v || r > 8 || r < -8) d.all_int = 0;
+            d.ipow[i][j] = (signed char)r;
         }
         d.active[i] = act;
         d.logk[i] = i < s.n_species ? s.logk[i] : 0.0;
+        d.k10[i] = std::pow(10.0, d.logk[i]);
     }
     for (int j = 0; j < CL_MAX_COMP; ++j) d.comp_species[j] = j < s.n_comp ? s.comp_species[j] : -1;
 }
@@ -58,15 +67,55 @@ __device__ __forceinline__ double species_c(const EqDev& e, int i, const double*
     return exp10(lc);
 }
 
+// Free-component activities a_j = 10^x_j and their inverses, once per
+// evaluation; with integer stoichiometry every species is then
+// c_i = 10^logK_i * prod_j a_j^S_ij by multiplication only (NC exp10 per
+// evaluation instead of one per species).  The clamp test uses the exact log.
+template <int NC>
+struct Powers {
+    double a[NC], ai[NC];
+    __device__ __forceinline__ void set(const double* x) {
+#pragma unroll
+        for (int j = 0; j < NC; ++j) { a[j] = exp10(x[j]); ai[j] = 1.0 / a[j]; }
+    }
+};
+
+template <int NC>
+__device__ __forceinline__ double species_eval(const EqDev& e, int i, const double* x, const Powers<NC>& pw,
+                                               bool& clamped) {
+    double lc = e.logk[i];
+#pragma unroll
+    for (int j = 0; j < NC; ++j) lc = fma(e.stoich[i][j], x[j], lc);
+    if (lc > 1.0) { clamped = true; return 10.0; }
+    if (lc < -30.0) { clamped = true; return 1e-30; }
+    clamped = false;
+    if (!e.all_int) return exp10(lc);
+    double p = e.k10[i];
+#pragma unroll
+    for (int j = 0; j < NC; ++j) {
+        const int q = e.ipow[i][j];
+        if (q == 0) continue;
+        const double b = q > 0 ? pw.a[j] : pw.ai[j];
+        const int m = q > 0 ? q : -q;
+        double t = b;
+        for (int r = 1; r < m; ++r) t *= b;
+        p *= t;
+    }
+    return p;
+}
+
 // F, and the relative residual
 template <int NC>
 __device__ __forceinline__ double eq_residual(const EqDev& e, const double* T, const double* x, double* F) {
     double sc[NC];
 #pragma unroll
     for (int j = 0; j < NC; ++j) { F[j] = -T[j]; sc[j] = 0.0; }
+    Powers<NC> pw;
+    pw.set(x);
     for (int i = 0; i < e.ns; ++i) {
         if (!e.active[i]) continue;
-        const double c = species_c<NC>(e, i, x);
+        bool clamped;
+        const double c = species_eval<NC>(e, i, x, pw, clamped);
 #pragma unroll
         for (int j = 0; j < NC; ++j) { F[j] = fma(e.stoich[i][j], c, F[j]); sc[j] = fma(e.absS[i][j], c, sc[j]); }
     }
@@ -107,13 +156,12 @@ __device__ int eq_newton(const EqDev& e, const double* T, double* x, int max_ite
 #pragma unroll
             for (int b = 0; b < NC; ++b) J[a][b] = 0.0;
         }
+        Powers<NC> pw;
+        pw.set(x);
         for (int i = 0; i < e.ns; ++i) {
             if (!e.active[i]) continue;
-            double lc = e.logk[i];
-#pragma unroll
-            for (int j = 0; j < NC; ++j) lc = fma(e.stoich[i][j], x[j], lc);
-            const bool clamped = (lc > 1.0) || (lc < -30.0);
-            const double c = exp10(fmin(fmax(lc, -30.0), 1.0));
+            bool clamped;
+            const double c = species_eval<NC>(e, i, x, pw, clamped);
             const double cj = clamped ? 0.0 : c;
 #pragma unroll
             for (int a = 0; a < NC; ++a) {
