@@ -21,6 +21,7 @@
 #include <vector>
 #include <random>
 #include <algorithm>
+#include <mutex>
 
 namespace cl {
 
@@ -741,4 +742,97 @@ extern "C" int cl_eq_train(cl_eq_solver* s, const double* d_totals, const double
     cudaFree(Xn); cudaFree(Yn);
     if (!r) s->trained = true;
     return r;
+}
+
+// ---------------------------------------------------------------------------
+// Batch speciation that allocates nothing.
+//
+// For callers that must not allocate device memory themselves or have the
+// library do it: host code that runs under a framework's caching allocator,
+// which owns the GPU's memory budget and would be bypassed by cudaMalloc, and
+// code placed between the kernels of a stream-ordered sequence, where
+// cudaMalloc / cudaFree would synchronise the whole device.  Such a caller
+// passes its own input and output buffers; the only scratch the solve needs,
+// the compacted list of voxels that fall back to the cold start, lives in the
+// fixed array below, which every GPU that loads this library holds until the
+// process exits.
+// ---------------------------------------------------------------------------
+namespace cl {
+
+// slot 0: the fallback counter; slots kNoAllocListOffset.. : the fallback list
+constexpr int64_t kNoAllocListOffset = 32;
+static __device__ __align__(256) unsigned long long g_noalloc_scratch[kNoAllocListOffset + CL_EQ_NOALLOC_MAX_N];
+
+static std::mutex g_noalloc_mu;
+static unsigned long long* g_noalloc_ptr[CL_EQ_NOALLOC_MAX_DEVICES] = {};
+
+// Device address of the scratch array on the current device.  In host code
+// the symbol is only a stand-in, so the address is looked up once per device
+// (with that device current) and cached.
+static int noalloc_scratch(unsigned long long** out) {
+    int dev = 0;
+    CL_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= CL_EQ_NOALLOC_MAX_DEVICES) {
+        set_error("cl_eq_solve_noalloc: device ordinal beyond the supported range");
+        return CL_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+        g_noalloc_ptr[dev] = static_cast<unsigned long long*>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return CL_OK;
+}
+
+}  // namespace cl
+
+extern "C" int cl_eq_solve_noalloc(const cl_eq_system* sys, const double* d_totals, const double* d_cold_species,
+                                   double* d_logfree, int32_t* d_iters, uint8_t* d_status, int64_t n, int32_t start,
+                                   void* stream) {
+    if (!sys || sys->n_comp < 1 || sys->n_comp > 5 || sys->n_species < sys->n_comp || sys->n_species > CL_MAX_SPECIES) {
+        set_error("cl_eq_solve_noalloc: 1..5 components and n_comp <= n_species <= 16");
+        return CL_ERR_ARG;
+    }
+    if (!d_totals || !d_logfree || n < 0) { set_error("cl_eq_solve_noalloc: null argument"); return CL_ERR_ARG; }
+    if (n > CL_EQ_NOALLOC_MAX_N) {
+        set_error("cl_eq_solve_noalloc: n exceeds CL_EQ_NOALLOC_MAX_N (1048576); split the batch");
+        return CL_ERR_ARG;
+    }
+    if (start != CL_EQ_START_COLD && start != CL_EQ_START_GIVEN) {
+        set_error("cl_eq_solve_noalloc: start must be CL_EQ_START_COLD or CL_EQ_START_GIVEN");
+        return CL_ERR_ARG;
+    }
+    if (start == CL_EQ_START_COLD && !d_cold_species) {
+        set_error("cl_eq_solve_noalloc: the cold start needs the species vectors");
+        return CL_ERR_ARG;
+    }
+    if (n == 0) return CL_OK;
+    unsigned long long* scratch = nullptr;
+    int r = noalloc_scratch(&scratch);
+    if (r) return r;
+    cudaStream_t st = (cudaStream_t)stream;
+    EqDev e;
+    eqdev_from_system(*sys, e);
+    const bool fallback = (start == CL_EQ_START_GIVEN) && d_cold_species != nullptr;
+    unsigned long long* count = scratch;
+    int64_t* list = reinterpret_cast<int64_t*>(scratch + kNoAllocListOffset);
+    if (fallback) CL_CUDA(cudaMemsetAsync(count, 0, sizeof(unsigned long long), st));
+    const int limit = (start == CL_EQ_START_COLD) ? sys->max_iter : sys->warm_iter;
+    const int blocks = grid_for(n, 128, 148 * 16);
+#define CL_NA_FIRST(NCV) newton_first_kernel<NCV><<<blocks, 128, 0, st>>>(e, d_totals, d_cold_species, d_logfree, d_iters, d_status, n, start, limit, sys->tol, fallback ? list : nullptr, count)
+#define CL_NA_FB(NCV) newton_fallback_kernel<NCV><<<blocks, 128, 0, st>>>(e, d_totals, d_cold_species, d_logfree, d_iters, d_status, list, count, sys->max_iter, sys->tol)
+    switch (sys->n_comp) {
+        case 1: CL_NA_FIRST(1); if (fallback) CL_NA_FB(1); break;
+        case 2: CL_NA_FIRST(2); if (fallback) CL_NA_FB(2); break;
+        case 3: CL_NA_FIRST(3); if (fallback) CL_NA_FB(3); break;
+        case 4: CL_NA_FIRST(4); if (fallback) CL_NA_FB(4); break;
+        default: CL_NA_FIRST(5); if (fallback) CL_NA_FB(5); break;
+    }
+#undef CL_NA_FIRST
+#undef CL_NA_FB
+    CL_LAUNCH_CHECK("cl_eq_solve_noalloc");
+    return CL_OK;
 }

@@ -263,6 +263,26 @@ int cl_eq_solve_host(cl_eq_solver* s, const double* totals, const double* cold_s
                      double* logfree, int32_t* iters, uint8_t* status,
                      int64_t n, int32_t start);
 
+/* Batch speciation that allocates nothing (no counterpart in the reference).
+ * For callers that must not allocate device memory: code running under a
+ * framework's caching allocator that owns the GPU's memory budget, and code
+ * between the kernels of a stream-ordered sequence, where cudaMalloc/cudaFree
+ * would synchronise the device.  Same solve as cl_eq_solve_device with start
+ * CL_EQ_START_COLD or CL_EQ_START_GIVEN (warm start with cold fallback when
+ * cold_species is given), on caller-owned device buffers and `stream`; no
+ * solver object is needed.  The fallback list lives in a fixed array of
+ * CL_EQ_NOALLOC_MAX_N entries (8 MiB) that every GPU loading the library
+ * holds until exit; larger n is rejected with CL_ERR_ARG.  The first call on
+ * a device looks up that array's device address, so make it before any
+ * stream capture.  All calls share the array: calls that overlap on the GPU
+ * race, and it keeps the last call's contents (the counter is cleared on
+ * every call). */
+#define CL_EQ_NOALLOC_MAX_N       1048576
+#define CL_EQ_NOALLOC_MAX_DEVICES 64
+int cl_eq_solve_noalloc(const cl_eq_system* sys, const double* d_totals, const double* d_cold_species,
+                        double* d_logfree, int32_t* d_iters, uint8_t* d_status,
+                        int64_t n, int32_t start, void* stream);
+
 /* ---- learned warm start: MLP n_comp -> 64 -> 64 -> n_comp, GELU, BF16 weights,
  *      FP32 accumulate, trained on the device by the library's own forward and
  *      backward kernels on pairs (log10 T -> log10 free) that Newton produced. */
