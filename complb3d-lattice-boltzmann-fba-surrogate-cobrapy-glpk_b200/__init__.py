@@ -27,6 +27,9 @@ FIELD_CONC, FIELD_BIOMASS, FIELD_VELOCITY, FIELD_FLOW_RHO, FIELD_FLOW_U, FIELD_P
 RED_SUM, RED_MIN, RED_MAX, RED_COUNT_EQ = range(4)
 EQ_START_COLD, EQ_START_GIVEN, EQ_START_LEARNED = range(3)
 SRG_TENSOR, SRG_FP32 = 0, 1
+MAX_SRG_ORG = 2
+SRG_IN_FIN, SRG_IN_CONC, SRG_IN_BIOMASS = 0, 1, 2
+SRG_OUT_GROWTH, SRG_OUT_FOUT = 0, 1
 KERNEL_ADE_MAIN, KERNEL_FLOW_STEP = 0, 1
 
 c_int32, c_double, c_int64 = ctypes.c_int32, ctypes.c_double, ctypes.c_int64
@@ -45,8 +48,24 @@ class EqSystem(ctypes.Structure):
 
 
 class Phase(ctypes.Structure):
-    _fields_ = [("id", c_int32), ("material", c_int32), ("substrate", c_int32), ("full_density", c_double),
-                ("k_dis", c_double), ("sat_s", c_int32), ("c_sat", c_double), ("nu_prod", c_double * MAX_SOLUTES)]
+    _fields_ = [("id", c_int32), ("material", c_int32), ("substrate", c_int32), ("is_precipitate", c_int32),
+                ("full_density", c_double), ("initial_fill", c_double), ("k", c_double), ("n_mass", c_int32),
+                ("mass_s", c_int32 * 2), ("nu", c_double * MAX_SOLUTES)]
+
+
+class SurrogateNet(ctypes.Structure):
+    _fields_ = [("n_layers", c_int32), ("widths", c_int32 * (SRG_MAX_LAYERS + 1)),
+                ("x_offset", c_double * SRG_MAX_WIDTH), ("x_gain", c_double * SRG_MAX_WIDTH), ("x_ymin", c_double),
+                ("y_offset", c_double * SRG_MAX_WIDTH), ("y_gain", c_double * SRG_MAX_WIDTH), ("y_ymin", c_double),
+                ("x_lo", c_double * SRG_MAX_WIDTH), ("x_hi", c_double * SRG_MAX_WIDTH),
+                ("params", c_double * 4096)]
+
+
+class SrgOrganism(ctypes.Structure):
+    _fields_ = [("microbe", c_int32), ("net", c_int32),
+                ("in_kind", c_int32 * SRG_MAX_WIDTH), ("in_index", c_int32 * SRG_MAX_WIDTH),
+                ("out_kind", c_int32 * SRG_MAX_WIDTH), ("out_index", c_int32 * SRG_MAX_WIDTH),
+                ("kc", c_double * MAX_SOLUTES), ("vmax", c_double * MAX_SOLUTES), ("mw", c_double), ("kd", c_double)]
 
 
 class Config(ctypes.Structure):
@@ -65,20 +84,14 @@ class Config(ctypes.Structure):
         ("n_microbes", c_int32), ("b_max", c_double), ("thrd_bfilm_frac", c_double), ("dt", c_double),
         ("enable_kinetics", c_int32), ("enable_abiotic", c_int32), ("abiotic_surface_only", c_int32),
         ("n_rxn", c_int32), ("rxn", Rxn * MAX_RXN), ("decay", c_double * MAX_MICROBES),
-        ("use_equilibrium", c_int32), ("eq", EqSystem),
+        ("use_equilibrium", c_int32), ("eq", EqSystem), ("eq_warm_previous", c_int32),
         ("precip_enabled", c_int32), ("precip_substrate", c_int32), ("max_precip_rho", c_double),
         ("precip_code", c_int32), ("precip_phase_id", c_int32),
         ("dissol_enabled", c_int32), ("reopen_fraction", c_double), ("dissol_surface_only", c_int32),
+        ("dissol_apply_at_walls", c_int32),
         ("n_phases", c_int32), ("phases", Phase * MAX_PHASES),
+        ("n_srg", c_int32), ("srg", SrgOrganism * MAX_SRG_ORG),
     ]
-
-
-class SurrogateNet(ctypes.Structure):
-    _fields_ = [("n_layers", c_int32), ("widths", c_int32 * (SRG_MAX_LAYERS + 1)),
-                ("x_offset", c_double * SRG_MAX_WIDTH), ("x_gain", c_double * SRG_MAX_WIDTH), ("x_ymin", c_double),
-                ("y_offset", c_double * SRG_MAX_WIDTH), ("y_gain", c_double * SRG_MAX_WIDTH), ("y_ymin", c_double),
-                ("x_lo", c_double * SRG_MAX_WIDTH), ("x_hi", c_double * SRG_MAX_WIDTH),
-                ("params", c_double * 4096)]
 
 
 _lib = None
@@ -108,7 +121,7 @@ def load_library(path=LIB_PATH):
         ("cl_precip_convert", [vp, P(c_int64)]), ("cl_dissol_convert", [vp, P(c_int64)]),
         ("cl_device_bytes", [vp, P(ctypes.c_uint64)]), ("cl_abi_sizes", [vp, c_int32]),
         ("cl_timing_enable", [vp, c_int32]), ("cl_timing_read", [vp, c_int32, P(c_double), P(c_int64)]),
-        ("cl_launch_count", [vp, P(c_int64)]),
+        ("cl_launch_count", [vp, P(c_int64)]), ("cl_set_surrogate", [vp, c_int32, vp]),
     ]:
         fn = getattr(lib, name)
         fn.restype = ctypes.c_int
@@ -194,6 +207,26 @@ def add_rxn(cfg, microbe=-1, k=0.0, monod=(), mass=(), nu=None, yield_=0.0):
         r.nu[s] = v
     cfg.n_rxn += 1
     return r
+
+
+def add_phase(cfg, substrate, full_density, material=0, initial_fill=0.0, is_precipitate=False,
+              k=0.0, mass=(), nu=None):
+    """Append one dissolvable phase (id = its position + 1) with its rate law
+    rate = k * mineral * prod water[mass]; products nu[s] * rate.  A phase
+    marked is_precipitate becomes the one precipitation stamps."""
+    ph = cfg.phases[cfg.n_phases]
+    ph.id = cfg.n_phases + 1
+    ph.material, ph.substrate, ph.is_precipitate = material, substrate, 1 if is_precipitate else 0
+    ph.full_density, ph.initial_fill, ph.k = full_density, initial_fill, k
+    ph.n_mass = len(mass)
+    for j, sidx in enumerate(mass):
+        ph.mass_s[j] = sidx
+    for sidx, v in (nu or {}).items():
+        ph.nu[sidx] = v
+    cfg.n_phases += 1
+    if is_precipitate:
+        cfg.precip_phase_id = ph.id
+    return ph
 
 
 def set_eq_system(sys, stoich, logk, comp_species, max_iter=100, tol=1e-10, warm_iter=8):
@@ -314,6 +347,11 @@ class Lattice:
         self._c(self.lib.cl_precip_convert(self.h, ctypes.byref(ch)), "cl_precip_convert")
         return ch.value
 
+    def dissol_convert(self):
+        ch = c_int64(0)
+        self._c(self.lib.cl_dissol_convert(self.h, ctypes.byref(ch)), "cl_dissol_convert")
+        return ch.value
+
     def timing(self, on=True):
         self._c(self.lib.cl_timing_enable(self.h, 1 if on else 0), "cl_timing_enable")
 
@@ -326,6 +364,9 @@ class Lattice:
         n = c_int64(0)
         self._c(self.lib.cl_launch_count(self.h, ctypes.byref(n)), "cl_launch_count")
         return n.value
+
+    def set_surrogate(self, slot, net):
+        self._c(self.lib.cl_set_surrogate(self.h, slot, ctypes.byref(net)), "cl_set_surrogate")
 
     def device_bytes(self):
         b = ctypes.c_uint64(0)

@@ -21,6 +21,14 @@
 // interior one: a zero-gradient face needs the pre-collision density of its
 // neighbour plane, which the interior launch records (FlatAdiabaticBoundary-
 // Functional3D sets the boundary density to that value after each stream).
+//
+// Dissolution (surfaceDissolutionKinetics3D) is the one processor that writes
+// other voxels' increments.  A small launch before the fused one evaluates
+// every phase voxel's release from the water of its open neighbours (their
+// densities after this step's kinetics, recomputed there) and records it per
+// phase voxel; the fused kernel then gathers, at each voxel flagged as next to
+// a phase, its neighbours' records into the abiotic increment, in the order
+// the reference's serial scatter adds them.
 #pragma once
 #include "internal.h"
 #include "newton.cuh"
@@ -39,6 +47,10 @@ struct AdeK {
     double* bio;              // M*N
     float* rho_adj;           // n_mob * 2 * plane
     int32_t* eq_iters;        // N (may be null)
+    double* eq_x;             // NC*N previous solutions (null: cold start only)
+    const uint8_t* mask;      // N material numbers
+    const uint8_t* phase;     // N phase ids (null without dissolution)
+    double* rel;              // S*N releases of the phase voxels (null without dissolution)
     unsigned long long* counters;
     int nodyn_coupled;
     int parity;
@@ -112,33 +124,172 @@ static __device__ void rates_dev(const AdeParams& p, int abiotic, const double* 
     if (!abiotic) for (int m = 0; m < p.M; ++m) if (!isfinite(BR[m * bd])) BR[m * bd] = 0.0;
 }
 
+// Surrogate reaction type of one voxel (run_surrogate3D,
+// src/complab3d_processors_surrogate.hh:94-295).  Reads the densities the
+// kinetics read (before update_rxnLattices), adds its thresholded increments
+// into D (solutes) and DB (biomass), which the caller applies together with
+// the kinetics increments, as the shared dC/dB lattices of the reference do.
+static __device__ __noinline__ void surrogate_chain(const AdeParams& p, const double* Cur, const double* B,
+                                             double* D, double* DB, int bd) {
+    double conc[CL_MAX_SOLUTES], draw[CL_MAX_SOLUTES];
+    bool any = false;
+    for (int o = 0; o < p.n_srg; ++o) any = any || B[p.srg[o].microbe * bd] > THRD;
+    if (!any) return;
+    for (int s = 0; s < p.S; ++s) {
+        const double c = Cur[s * bd];
+        conc[s] = c > THRD ? c : 0.0;
+        draw[s] = 0.0;
+    }
+    for (int o = 0; o < p.n_srg; ++o) {
+        const cl_srg_organism& org = p.srg[o];
+        const SrgNetDev& net = p.net[org.net];
+        const double b = B[org.microbe * bd];
+        if (!(b > THRD)) continue;
+        // Michaelis-Menten uptake estimates, capped by the exhaustion flux
+        // (MetabolicConfig::exhaustionFlux, complab3d_metabolic.hh:504-519)
+        double fin[CL_MAX_SOLUTES];
+        const double denom = b * org.mw * p.dt;
+        for (int s = 0; s < p.S; ++s) {
+            const double av = conc[s];
+            const double mm = (org.kc[s] + av > 0.0) ? av / (org.kc[s] + av) : 0.0;
+            double exh = 0.0;
+            if (denom > 1e-30) { exh = -av * 3.6e6 / denom; if (exh < -1e4) exh = -1e4; }
+            double v = org.vmax[s] > THRD ? org.vmax[s] * mm : -exh * mm;
+            const double cap = -exh;
+            if (cap > 0.0 && v > cap) v = cap;
+            fin[s] = v;
+        }
+        // the network: mapminmax inputs, tanh hidden layers, linear output
+        float a[CL_SRG_MAX_WIDTH], t[CL_SRG_MAX_WIDTH];
+        const int win = net.w[0];
+        for (int i = 0; i < win; ++i) {
+            const int kind = org.in_kind[i], idx = org.in_index[i];
+            float v = kind == CL_SRG_IN_FIN ? (float)fin[idx] : kind == CL_SRG_IN_CONC ? (float)conc[idx] : (float)b;
+            v = fminf(fmaxf(v, net.xlo[i]), net.xhi[i]);
+            a[i] = (v - net.xo[i]) * net.xg[i] + net.xymin;
+        }
+        for (int l = 0; l < net.L; ++l) {
+            const int wi = net.w[l], wo = net.w[l + 1];
+            const float* W = net.params + net.poff[l];
+            for (int q = 0; q < wo; ++q) {
+                float acc = __ldg(W + wo * wi + q);
+                for (int i = 0; i < wi; ++i) acc = fmaf(__ldg(W + q * wi + i), a[i], acc);
+                t[q] = (l < net.L - 1) ? tanhf(acc) : acc;
+            }
+            for (int q = 0; q < wo; ++q) a[q] = t[q];
+        }
+        double mu = 0.0;
+        double fout[CL_MAX_SOLUTES];
+        for (int s = 0; s < p.S; ++s) fout[s] = fin[s];
+        for (int q = 0; q < net.w[net.L]; ++q) {
+            const double y = ((double)a[q] - net.yymin) / net.yg[q] + net.yo[q];
+            if (org.out_kind[q] == CL_SRG_OUT_GROWTH) mu = y;
+            else fout[org.out_index[q]] = y;
+        }
+        if (mu < 1e-8 || !isfinite(mu)) mu = 0.0;     // the exported model's dust / NaN guard
+        // growthToDeltaB / decayToDeltaB (complab3d_metabolic.hh:487-500)
+        double dB = (fabs(mu) < THRD) ? -org.kd * b * p.dt : mu * b * p.dt / 3600.0;
+        if (dB + b < 0.0) dB = -b;
+        if (fabs(dB) > THRD) DB[org.microbe * bd] += dB;
+        // fluxToDeltaC: positive Fout is consumed
+        for (int s = 0; s < p.S; ++s) draw[s] += -fout[s] * b * org.mw * p.dt / 3.6e6;
+    }
+    for (int s = 0; s < p.S; ++s) {
+        double d = draw[s];
+        if (fabs(d) <= THRD) continue;
+        if (d + conc[s] < 0.0) d = -conc[s];
+        if (d > 0.0) d = 0.0;
+        if (fabs(d) > THRD) D[s * bd] += d;
+    }
+}
+
+// run_kinetics (part1.hh:63-146) and run_surrogate3D deposit into the same
+// dC/dB lattices, each contribution only if above thrd: the increments of one
+// voxel into R (solutes) and BR (biomass), B its floored biomass.  Not applied.
+__device__ __forceinline__ void kinetics_increments(const AdeParams& p, const double* bio, int64_t N, int64_t n,
+                                                    const double* Cur, double* R, double* B, double* BR, int bd) {
+    for (int m = 0; m < p.M; ++m) { const double b = bio[m * N + n]; B[m * bd] = b < THRD ? 0.0 : b; }
+    if (p.do_kin) {
+        rates_dev(p, 0, Cur, B, R, BR, bd);
+        for (int s = 0; s < p.S; ++s) {
+            const double d = R[s * bd] * p.dt;
+            R[s * bd] = (d > THRD || d < -THRD) ? d : 0.0;
+        }
+        for (int m = 0; m < p.M; ++m) {
+            const double d = BR[m * bd] * p.dt;
+            BR[m * bd] = (d > THRD || d < -THRD) ? d : 0.0;
+        }
+    } else {
+        for (int s = 0; s < p.S; ++s) R[s * bd] = 0.0;
+        for (int m = 0; m < p.M; ++m) BR[m * bd] = 0.0;
+    }
+    if (p.n_srg > 0) surrogate_chain(p, Cur, B, R, BR, bd);
+}
+
+// The dissolution increments that reach voxel n (surfaceDissolutionKinetics3D,
+// dissolutionVOP.hh:392-425): the products of each face neighbour that carries
+// a phase, and the voxel's own mineral decrement.  Neighbours are visited in
+// increasing site order with the voxel itself between -z and +z, the order in
+// which the reference's serial scatter adds into this voxel's dC.
+__device__ __forceinline__ void dissol_gather(const AdeK& k, int64_t n, int x, int y, int z, uint8_t cls,
+                                              double* D, int bd) {
+    const AdeParams& p = k.p;
+    const int64_t N = k.g.N, plane = k.g.plane, nz = k.g.nz;
+    const int64_t q[7] = {n - plane, n - nz, n - 1, n, n + 1, n + nz, n + plane};
+    const bool ok[7] = {x - 1 >= 1, y > 0, z > 0, (cls & F_PHASE_SELF) != 0,
+                        z < k.g.nz - 1, y < k.g.ny - 1, x + 1 <= k.g.nx - 2};
+#pragma unroll
+    for (int j = 0; j < 7; ++j) {
+        if (!ok[j]) continue;
+        const int pid = k.phase[q[j]];
+        if (pid == 0) continue;
+        const int sM = p.phase[pid - 1].substrate;
+        if (j == 3) { D[sM * bd] += k.rel[(int64_t)sM * N + n]; continue; }
+        for (int s = 0; s < p.S; ++s)
+            if (s != sM) D[s * bd] += k.rel[(int64_t)s * N + q[j]];
+    }
+}
+
 // The reaction chain of one voxel.  Cur holds the current densities (updated
 // as each processor applies its increments), App the total increment per
 // solute.  Returns 1 if the equilibrium solve did not converge.
 template <int NC>
-__device__ int reaction_chain(const AdeK& k, int64_t n, uint8_t cls, double* Cur, double* App,
+__device__ int reaction_chain(const AdeK& k, int64_t n, int x, int y, int z, uint8_t cls, double* Cur, double* App,
                               double* R, double* B, double* BR, int bd) {
     const AdeParams& p = k.p;
     const int64_t N = k.g.N;
     int nonconv = 0;
-    // run_kinetics (part1.hh:63-146) + update_rxnLattices (:338-429)
-    if (p.do_kin) {
-        for (int m = 0; m < p.M; ++m) { const double b = k.bio[m * N + n]; B[m * bd] = b < THRD ? 0.0 : b; }
-        rates_dev(p, 0, Cur, B, R, BR, bd);
+    // kinetics and surrogate increments; update_rxnLattices (:338-429) applies
+    // the sums that exceed thrd
+    if (p.do_kin || p.n_srg > 0) {
+        kinetics_increments(p, k.bio, N, n, Cur, R, B, BR, bd);
         for (int s = 0; s < p.S; ++s) {
-            const double d = R[s * bd] * p.dt;
+            const double d = R[s * bd];
             if (d > THRD || d < -THRD) { Cur[s * bd] += d; App[s * bd] += d; }
         }
         for (int m = 0; m < p.M; ++m) {
-            const double d = BR[m * bd] * p.dt;
+            const double d = BR[m * bd];
             if (d > THRD || d < -THRD) k.bio[m * N + n] += d;
         }
     }
-    // dC = dC0; run_abiotic_kinetics | surfaceAbioticKinetics3D; update_abiotic_rxnLattices
-    if (p.do_abio && (!p.surface_only || (cls & F_SURFACE))) {
-        rates_dev(p, 1, Cur, nullptr, R, nullptr, bd);
+    // dC = dC0; run_abiotic_kinetics | surfaceAbioticKinetics3D (thresholded);
+    // + surfaceDissolutionKinetics3D; update_abiotic_rxnLattices applies the
+    // sums that exceed thrd
+    const bool abio = p.do_abio && (!p.surface_only || (cls & F_SURFACE));
+    const bool dis = p.do_dissol && (cls & (F_PHASE_NBR | F_PHASE_SELF));
+    if (abio || dis) {
+        if (abio) {
+            rates_dev(p, 1, Cur, nullptr, R, nullptr, bd);
+            for (int s = 0; s < p.S; ++s) {
+                const double d = R[s * bd] * p.dt;
+                R[s * bd] = (d > THRD || d < -THRD) ? d : 0.0;
+            }
+        } else {
+            for (int s = 0; s < p.S; ++s) R[s * bd] = 0.0;
+        }
+        if (dis) dissol_gather(k, n, x, y, z, cls, R, bd);
         for (int s = 0; s < p.S; ++s) {
-            const double d = R[s * bd] * p.dt;
+            const double d = R[s * bd];
             if (d > THRD || d < -THRD) { Cur[s * bd] += d; App[s * bd] += d; }
         }
     }
@@ -155,16 +306,35 @@ __device__ int reaction_chain(const AdeK& k, int64_t n, uint8_t cls, double* Cur
 #pragma unroll
             for (int j = 0; j < NC; ++j) T[j] = fma(e.stoich[i][j], c, T[j]);
         }
+        auto cold = [&](double* xs) {
 #pragma unroll
-        for (int j = 0; j < NC; ++j) {
-            T[j] = fmax(T[j], 1e-30);
-            double c = 1e-7;
-            const int idx = e.comp_species[j];
-            if (idx >= 0) c = Cur[idx * bd];
-            x[j] = log10(fmin(fmax(c, 1e-30), 10.0));
+            for (int j = 0; j < NC; ++j) {
+                double c = 1e-7;
+                const int idx = e.comp_species[j];
+                if (idx >= 0) c = Cur[idx * bd];
+                xs[j] = log10(fmin(fmax(c, 1e-30), 10.0));
+            }
+        };
+#pragma unroll
+        for (int j = 0; j < NC; ++j) T[j] = fmax(T[j], 1e-30);
+        int conv = 0, it = 0;
+        bool warm = false;
+        if (k.eq_x) {
+            warm = true;
+#pragma unroll
+            for (int j = 0; j < NC; ++j) { x[j] = k.eq_x[(int64_t)j * N + n]; warm = warm && (x[j] == x[j]); }
         }
-        int conv = 0;
-        const int it = eq_newton<NC>(e, T, x, p.eq.max_iter, p.eq.tol, &conv);
+        if (warm) {
+            it = eq_newton<NC>(e, T, x, p.eq.warm_iter, p.eq.tol, &conv);
+            if (!conv) { cold(x); int it2 = eq_newton<NC>(e, T, x, p.eq.max_iter, p.eq.tol, &conv); it += it2; }
+        } else {
+            cold(x);
+            it = eq_newton<NC>(e, T, x, p.eq.max_iter, p.eq.tol, &conv);
+        }
+        if (k.eq_x && conv) {
+#pragma unroll
+            for (int j = 0; j < NC; ++j) k.eq_x[(int64_t)j * N + n] = x[j];
+        }
         if (k.eq_iters) k.eq_iters[n] = it;
         if (!conv) nonconv = 1;
         else {
@@ -184,7 +354,7 @@ __device__ int reaction_chain(const AdeK& k, int64_t n, uint8_t cls, double* Cur
 }
 
 template <int NMOB, int NC, int PARITY>
-__global__ void __launch_bounds__(256, 2) ade_main_kernel(AdeK k) {
+__global__ void __launch_bounds__(256, 2) ade_main_kernel(const __grid_constant__ AdeK k) {
     extern __shared__ double sm[];
     const int bd = blockDim.x;
     const AdeParams& p = k.p;
@@ -195,7 +365,7 @@ __global__ void __launch_bounds__(256, 2) ade_main_kernel(AdeK k) {
     double* BR  = B + (p.M > 0 ? p.M : 1) * bd;
     const int64_t N = k.g.N, plane = k.g.plane;
     const uint32_t N32 = (uint32_t)N;
-    const bool any_rxn = p.do_kin || p.do_abio || NC > 0;
+    const bool any_rxn = p.do_kin || p.do_abio || p.n_srg > 0 || p.do_dissol || NC > 0;
     unsigned long long nonconv = 0;
     const RowMap rm = make_rowmap(k.g.nz);
     const int row_lo = k.g.ny, row_hi = (k.g.nx - 1) * k.g.ny;     // interior x = 1 .. nx-2
@@ -213,7 +383,9 @@ __global__ void __launch_bounds__(256, 2) ade_main_kernel(AdeK k) {
         float dC[NMOB];
 #pragma unroll
         for (int m = 0; m < NMOB; ++m) dC[m] = 0.f;
-        if (dyn != NODYN && (cls & F_REACTIVE) && any_rxn) {
+        // the processors test the mask, not the dynamics: a NoDynamics site
+        // whose mask reopened to pore reacts too
+        if ((cls & F_REACTIVE) && any_rxn) {
             // pass 1: the populations of a group of solutes in flight at once, then the densities
             for (int s = 0; s < p.S; ++s) App[s * bd] = 0.0;
 #pragma unroll
@@ -233,7 +405,7 @@ __global__ void __launch_bounds__(256, 2) ade_main_kernel(AdeK k) {
             }
             for (int s = 0; s < p.S; ++s)
                 if (p.mob_slot[s] < 0) Cur[s * bd] = k.imm[(int64_t)s * N + n];
-            nonconv += reaction_chain<NC>(k, n, cls, Cur, App, R, B, BR, bd);
+            nonconv += reaction_chain<NC>(k, n, x, y, z, cls, Cur, App, R, B, BR, bd);
 #pragma unroll
             for (int m = 0; m < NMOB; ++m) dC[m] = (float)App[p.mob_index[m] * bd];
             for (int s = 0; s < p.S; ++s)
@@ -259,14 +431,14 @@ __global__ void __launch_bounds__(256, 2) ade_main_kernel(AdeK k) {
                 if (dyn != NODYN) {
                     const float om = (dyn == BIO) ? p.omega_bio[m] : p.omega_pore[m];
                     collide7(f[j], om, ux, uy, uz, rho);
-                    const float d = dC[m];
-                    if (d != 0.f) {
-#pragma unroll
-                        for (int i = 0; i < 7; ++i) f[j][i] += t7(i) * d;
-                    }
                 } else if (adj) {
 #pragma unroll
                     for (int i = 0; i < 7; ++i) rho += f[j][i];
+                }
+                const float d = dC[m];
+                if (d != 0.f) {
+#pragma unroll
+                    for (int i = 0; i < 7; ++i) f[j][i] += t7(i) * d;
                 }
                 if (adj) {
                     const int side = (x == 1) ? 0 : 1;
@@ -285,7 +457,7 @@ __global__ void __launch_bounds__(256, 2) ade_main_kernel(AdeK k) {
 // x = 0 and x = nx-1: AdvectionDiffusionBoundaryDynamics (the one unknown
 // population = prescribed density - the six known ones) then BGK collide.
 template <int NMOB, int PARITY>
-__global__ void __launch_bounds__(256) ade_boundary_kernel(AdeK k) {
+__global__ void __launch_bounds__(256) ade_boundary_kernel(const __grid_constant__ AdeK k) {
     const AdeParams& p = k.p;
     const int64_t N = k.g.N, plane = k.g.plane;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -333,6 +505,10 @@ inline AdeK make_adek(Ctx* c) {
     k.bio = c->d_bio;
     k.rho_adj = c->d_rho_adj;
     k.eq_iters = c->d_eq_iters;
+    k.eq_x = c->d_eq_x;
+    k.mask = c->d_mask;
+    k.phase = c->d_phase;
+    k.rel = c->d_rel;
     k.counters = c->d_counters;
     k.nodyn_coupled = c->ade_nodyn_coupled ? 1 : 0;
     k.parity = c->ade_parity;
@@ -341,16 +517,20 @@ inline AdeK make_adek(Ctx* c) {
     return k;
 }
 
+// the phase voxels' releases of this step (dissolution.cu), before the fused launch
+int dissol_release(Ctx* c, const AdeK& k);
+
 template <int NMOB, int NC>
 inline int launch_step(Ctx* c, const AdeK& k) {
     const int bd = 256;
     const int S = c->ap.S, M = c->ap.M > 0 ? c->ap.M : 1;
-    const bool any_rxn = c->ap.do_kin || c->ap.do_abio || NC > 0;
+    const bool any_rxn = c->ap.do_kin || c->ap.do_abio || c->ap.n_srg > 0 || c->ap.do_dissol || NC > 0;
     const size_t smem = any_rxn ? (size_t)(3 * S + 2 * M) * bd * sizeof(double) : 0;
     const int64_t interior = c->geo.N - 2 * c->geo.plane;
     const int blocks = grid_for(interior, bd, 148 * 8);
-    int r = timing_begin(c, CL_KERNEL_ADE_MAIN);
-    if (r) return r;
+    int r = CL_OK;
+    if (c->ap.do_dissol && (r = dissol_release(c, k))) return r;
+    if ((r = timing_begin(c, CL_KERNEL_ADE_MAIN))) return r;
     if (c->ade_parity == 0) {
         auto kern = ade_main_kernel<NMOB, NC, 0>;
         CL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

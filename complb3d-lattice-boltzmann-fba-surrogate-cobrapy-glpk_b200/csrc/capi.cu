@@ -3,6 +3,7 @@
 #include <cstring>
 #include <cstdio>
 #include <vector>
+#include <algorithm>
 
 namespace cl {
 
@@ -64,6 +65,41 @@ static int validate(const cl_config* c) {
         }
         for (int j = 0; j < r.n_monod; ++j) if (r.monod_s[j] < 0 || r.monod_s[j] >= c->n_solutes) { set_error("monod solute index"); return CL_ERR_ARG; }
         for (int j = 0; j < r.n_mass; ++j) if (r.mass_s[j] < 0 || r.mass_s[j] >= c->n_solutes) { set_error("mass-action solute index"); return CL_ERR_ARG; }
+    }
+    if (c->n_srg < 0 || c->n_srg > CL_MAX_SRG_ORG) { set_error("n_srg out of range"); return CL_ERR_ARG; }
+    for (int o = 0; o < c->n_srg; ++o) {
+        const cl_srg_organism& g = c->srg[o];
+        if (g.microbe < 0 || g.microbe >= c->n_microbes || g.net < 0 || g.net >= CL_MAX_SRG_ORG) {
+            set_error("surrogate organism: microbe or network slot out of range"); return CL_ERR_ARG;
+        }
+        for (int i = 0; i < CL_SRG_MAX_WIDTH; ++i) {
+            if ((g.in_kind[i] == CL_SRG_IN_FIN || g.in_kind[i] == CL_SRG_IN_CONC) &&
+                (g.in_index[i] < 0 || g.in_index[i] >= c->n_solutes)) { set_error("surrogate input index"); return CL_ERR_ARG; }
+            if (g.out_kind[i] == CL_SRG_OUT_FOUT && (g.out_index[i] < 0 || g.out_index[i] >= c->n_solutes)) {
+                set_error("surrogate output index"); return CL_ERR_ARG;
+            }
+        }
+    }
+    if (c->n_phases < 0 || c->n_phases > CL_MAX_PHASES) { set_error("n_phases out of range"); return CL_ERR_ARG; }
+    if (c->dissol_enabled) {
+        // complab.cpp:336-368: at least one phase, reopen_fraction in (0,1),
+        // a substrate and a positive full density per phase
+        if (c->n_phases < 1) { set_error("dissolution is enabled but no phase is declared"); return CL_ERR_ARG; }
+        if (!(c->reopen_fraction > 0.0) || c->reopen_fraction >= 1.0) {
+            set_error("reopen_fraction must lie in (0, 1)"); return CL_ERR_ARG;
+        }
+        for (int k = 0; k < c->n_phases; ++k) {
+            const cl_phase& ph = c->phases[k];
+            if (ph.id != k + 1) { set_error("phase ids must be 1..n_phases in declaration order"); return CL_ERR_ARG; }
+            if (ph.substrate < 0 || ph.substrate >= c->n_solutes || !c->immobile[ph.substrate]) {
+                set_error("a phase needs an immobile substrate for its inventory"); return CL_ERR_ARG;
+            }
+            if (!(ph.full_density > 0.0)) { set_error("phase full_density must be positive"); return CL_ERR_ARG; }
+            if (ph.n_mass < 0 || ph.n_mass > 2) { set_error("phase rate law: 0..2 mass-action solutes"); return CL_ERR_ARG; }
+            for (int j = 0; j < ph.n_mass; ++j)
+                if (ph.mass_s[j] < 0 || ph.mass_s[j] >= c->n_solutes) { set_error("phase rate law solute index"); return CL_ERR_ARG; }
+        }
+        if (c->precip_phase_id < 0 || c->precip_phase_id > c->n_phases) { set_error("precip_phase_id out of range"); return CL_ERR_ARG; }
     }
     if (c->use_equilibrium) {
         const cl_eq_system& e = c->eq;
@@ -136,12 +172,20 @@ cl_ctx* cl_create(const cl_config* cfg, void* stream, int* status) {
     p.do_abio = cfg->enable_abiotic && n_abio > 0 && cfg->n_solutes > 0;
     p.surface_only = cfg->precip_enabled && cfg->abiotic_surface_only;
     p.do_eq = cfg->use_equilibrium;
+    p.eq_warm = cfg->use_equilibrium && cfg->eq_warm_previous;
     p.n_rxn = cfg->n_rxn;
     for (int k = 0; k < cfg->n_rxn; ++k) p.rxn[k] = cfg->rxn[k];
     for (int m = 0; m < CL_MAX_MICROBES; ++m) p.decay[m] = cfg->decay[m];
     p.eq = cfg->eq;
     p.solid_code = cfg->solid_code;
     p.bb_code = cfg->bb_code;
+    p.n_srg = cfg->n_srg;
+    for (int o = 0; o < CL_MAX_SRG_ORG; ++o) { p.srg[o] = cfg->srg[o]; p.net[o] = SrgNetDev{}; }
+    p.do_dissol = cfg->dissol_enabled && cfg->n_phases > 0;
+    p.dissol_surface_only = cfg->dissol_surface_only;
+    p.dissol_walls = cfg->dissol_apply_at_walls;
+    p.n_phases = cfg->n_phases;
+    for (int k = 0; k < cfg->n_phases; ++k) p.phase[k] = cfg->phases[k];
     // device memory
     int r = CL_OK;
     if ((r = dalloc(c, &c->d_mask, N)) || (r = dalloc(c, &c->d_ns_cls, N)) || (r = dalloc(c, &c->d_ade_cls, N)) ||
@@ -151,8 +195,12 @@ cl_ctx* cl_create(const cl_config* cfg, void* stream, int* status) {
         (r = dalloc(c, &c->d_bio, (size_t)p.M * N)) ||
         (r = dalloc(c, &c->d_rho_adj, (size_t)p.n_mob * 2 * c->geo.plane)) ||
         (r = dalloc(c, &c->d_eq_iters, (size_t)(cfg->use_equilibrium ? N : 0))) ||
+        (r = dalloc(c, &c->d_eq_x, (size_t)(p.eq_warm ? cfg->eq.n_comp : 0) * N)) ||
+        (r = dalloc(c, &c->d_phase, (size_t)(p.do_dissol ? N : 0))) ||
+        (r = dalloc(c, &c->d_rel, (size_t)(p.do_dissol ? p.S : 0) * N)) ||
         (r = dalloc(c, &c->d_counters, 8)) || (r = dalloc(c, &c->d_tracer, 1)))
         return fail(r);
+    if (c->d_eq_x) cudaMemsetAsync(c->d_eq_x, 0xff, sizeof(double) * cfg->eq.n_comp * N, c->stream);  // NaN
     c->energy_blocks = grid_for(N, 256, 148 * 8);
     if ((r = dalloc(c, &c->d_energy_part, c->energy_blocks))) return fail(r);
     c->scratch_bytes = sizeof(double) * ((size_t)N + 65536);
@@ -161,6 +209,8 @@ cl_ctx* cl_create(const cl_config* cfg, void* stream, int* status) {
     if (c->d_bio) cudaMemsetAsync(c->d_bio, 0, sizeof(double) * p.M * N, c->stream);
     cudaMemsetAsync(c->d_counters, 0, 8 * sizeof(unsigned long long), c->stream);
     if (c->d_eq_iters) cudaMemsetAsync(c->d_eq_iters, 0, sizeof(int32_t) * N, c->stream);
+    if (c->d_phase) cudaMemsetAsync(c->d_phase, 0, N, c->stream);
+    if (c->d_rel) cudaMemsetAsync(c->d_rel, 0, sizeof(double) * p.S * N, c->stream);
     cudaError_t e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) return fail(cuda_fail(e, "cl_create"));
     if (status) *status = CL_OK;
@@ -172,8 +222,10 @@ int cl_destroy(cl_ctx* h) {
     Ctx* c = &h->c;
     if (c->stream) cudaStreamSynchronize(c->stream);
     void* ptrs[] = {c->d_mask, c->d_ns_cls, c->d_ade_cls, c->d_f, c->d_u, c->d_g, c->d_imm, c->d_bio,
-                    c->d_rho_adj, c->d_eq_iters, c->d_counters, c->d_tracer, c->d_energy_part, c->d_scratch};
+                    c->d_rho_adj, c->d_eq_iters, c->d_eq_x, c->d_phase, c->d_rel, c->d_counters, c->d_tracer,
+                    c->d_energy_part, c->d_scratch};
     for (void* p : ptrs) if (p) cudaFree(p);
+    for (int o = 0; o < CL_MAX_SRG_ORG; ++o) if (c->d_srg_params[o]) cudaFree(c->d_srg_params[o]);
     for (int k = 0; k < Ctx::kTimedKernels; ++k)
         for (int i = 0; i < Ctx::kEventPool; ++i)
             for (int j = 0; j < 2; ++j) if (c->ev[k][i][j]) cudaEventDestroy(c->ev[k][i][j]);
@@ -192,7 +244,9 @@ int cl_upload_mask(cl_ctx* h, const uint8_t* mask) {
     if (!h || !mask) { set_error("null argument"); return CL_ERR_ARG; }
     Ctx* c = &h->c;
     CL_CUDA(cudaMemcpyAsync(c->d_mask, mask, c->geo.N, cudaMemcpyHostToDevice, c->stream));
-    int r = classes_from_mask(c);
+    int r = phase_seed(c);
+    if (r) return r;
+    r = classes_from_mask(c);
     if (r) return r;
     c->mask_ready = true;
     return CL_OK;
@@ -295,8 +349,40 @@ int cl_ade_init(cl_ctx* h) {
     if (!c->mask_ready) { set_error("upload the mask first"); return CL_ERR_STATE; }
     int r = ade_init(c);
     if (r) return r;
+    if ((r = phase_fill(c))) return r;
     c->ade_ready = true;
     CL_CUDA(cudaStreamSynchronize(c->stream));
+    return CL_OK;
+}
+
+int cl_set_surrogate(cl_ctx* h, int32_t slot, const cl_surrogate_net* net) {
+    if (!h || !net || slot < 0 || slot >= CL_MAX_SRG_ORG) { set_error("cl_set_surrogate: bad argument"); return CL_ERR_ARG; }
+    Ctx* c = &h->c;
+    SrgNetDev d{};
+    d.L = net->n_layers;
+    if (d.L < 1 || d.L > CL_SRG_MAX_LAYERS) { set_error("surrogate: 1..5 layers"); return CL_ERR_ARG; }
+    int off = 0;
+    for (int l = 0; l <= d.L; ++l) {
+        d.w[l] = net->widths[l];
+        if (d.w[l] < 1 || d.w[l] > CL_SRG_MAX_WIDTH) { set_error("surrogate: widths 1..32"); return CL_ERR_ARG; }
+    }
+    for (int l = 0; l < d.L; ++l) { d.poff[l] = off; off += d.w[l + 1] * d.w[l] + d.w[l + 1]; }
+    if (off > 4096) { set_error("surrogate: too many parameters"); return CL_ERR_ARG; }
+    for (int i = 0; i < CL_SRG_MAX_WIDTH; ++i) {
+        d.xo[i] = (float)net->x_offset[i]; d.xg[i] = (float)net->x_gain[i];
+        d.xlo[i] = (float)std::max(net->x_lo[i], -3.0e38); d.xhi[i] = (float)std::min(net->x_hi[i], 3.0e38);
+        d.yo[i] = (float)net->y_offset[i]; d.yg[i] = (float)net->y_gain[i];
+    }
+    d.xymin = (float)net->x_ymin; d.yymin = (float)net->y_ymin;
+    std::vector<float> hp(off);
+    for (int i = 0; i < off; ++i) hp[i] = (float)net->params[i];
+    if (c->d_srg_params[slot]) { cudaFree(c->d_srg_params[slot]); c->d_srg_params[slot] = nullptr; }
+    int r = dalloc(c, &c->d_srg_params[slot], (size_t)off);
+    if (r) return r;
+    CL_CUDA(cudaMemcpyAsync(c->d_srg_params[slot], hp.data(), sizeof(float) * off, cudaMemcpyHostToDevice, c->stream));
+    CL_CUDA(cudaStreamSynchronize(c->stream));
+    d.params = c->d_srg_params[slot];
+    c->ap.net[slot] = d;
     return CL_OK;
 }
 
@@ -304,6 +390,8 @@ int cl_step(cl_ctx* h, int32_t n) {
     if (!h || n < 0) return CL_ERR_ARG;
     Ctx* c = &h->c;
     if (!c->ade_ready) { set_error("call cl_ade_init first"); return CL_ERR_STATE; }
+    for (int o = 0; o < c->ap.n_srg; ++o)
+        if (!c->ap.net[c->ap.srg[o].net].params) { set_error("surrogate network slot not set"); return CL_ERR_STATE; }
     if (c->ap.n_mob == 0) { set_error("no mobile solute"); return CL_ERR_STATE; }
     for (int32_t i = 0; i < n; ++i) {
         int r = ade_step(c);
@@ -328,6 +416,17 @@ __global__ void d2f_kernel(const double* a, float* b, int64_t n) {
 }
 __global__ void i2d_kernel(const int32_t* a, double* b, int64_t n) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) b[i] = a[i];
+}
+__global__ void u2d_kernel(const uint8_t* a, double* b, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) b[i] = a[i];
+}
+// phase ids from doubles; any value that is not an id 0..n_phases sets *bad
+__global__ void d2phase_kernel(const double* a, uint8_t* b, int64_t n, int n_phases, int* bad) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double v = a[i];
+        if (v >= 0.0 && v <= (double)n_phases && v == (double)(int)v) b[i] = (uint8_t)(int)v;
+        else { b[i] = 0; *bad = 1; }
+    }
 }
 // set solute populations to t_i * c at the slots that hold each site's
 // pre-collision populations for the current parity
@@ -398,6 +497,10 @@ int cl_get_field(cl_ctx* h, int32_t field, int32_t index, double* out) {
             if (!c->d_eq_iters) return CL_ERR_STATE;
             i2d_kernel<<<blocks, 256, 0, c->stream>>>(c->d_eq_iters, d, N);
             break;
+        case CL_FIELD_PHASE:
+            if (!c->d_phase) { set_error("dissolution is not enabled in this context"); return CL_ERR_STATE; }
+            u2d_kernel<<<blocks, 256, 0, c->stream>>>(c->d_phase, d, N);
+            break;
         default: set_error("unknown field"); return CL_ERR_ARG;
     }
     if (r) return r;
@@ -435,6 +538,20 @@ int cl_set_field(cl_ctx* h, int32_t field, int32_t index, const double* in) {
             if (index < 0 || index > 2) return CL_ERR_ARG;
             d2f_kernel<<<blocks, 256, 0, c->stream>>>(d, c->d_u + index * N, N);
             break;
+        case CL_FIELD_PHASE: {
+            if (!c->d_phase) { set_error("dissolution is not enabled in this context"); return CL_ERR_STATE; }
+            int* d_bad = reinterpret_cast<int*>(c->d_scratch + N);
+            CL_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(int), c->stream));
+            d2phase_kernel<<<blocks, 256, 0, c->stream>>>(d, c->d_phase, N, c->cfg.n_phases, d_bad);
+            CL_LAUNCH_CHECK("d2phase_kernel");
+            int bad = 0;
+            CL_CUDA(cudaMemcpyAsync(&bad, d_bad, sizeof bad, cudaMemcpyDeviceToHost, c->stream));
+            CL_CUDA(cudaStreamSynchronize(c->stream));
+            int r = refresh_flags(c);
+            if (r) return r;
+            if (bad) { set_error("phase ids must be integers 0..n_phases (others were set to 0)"); return CL_ERR_ARG; }
+            break;
+        }
         default: set_error("field is read-only or unknown"); return CL_ERR_ARG;
     }
     CL_LAUNCH_CHECK("cl_set_field");
@@ -552,9 +669,8 @@ int cl_precip_convert(cl_ctx* h, int64_t* changed) {
 }
 
 int cl_dissol_convert(cl_ctx* h, int64_t* changed) {
-    (void)h; (void)changed;
-    set_error("dissolution node conversion is not built in this library version");
-    return CL_ERR_STATE;
+    if (!h || !changed) return CL_ERR_ARG;
+    return dissol_convert(&h->c, changed);
 }
 
 }  // extern "C"

@@ -14,6 +14,7 @@ struct ClassK {
     int n_pore, pore[CL_MAX_CODES];
     int n_bio, bio[CL_MAX_CODES];
     int bio_is_bb;                 // perm_ratio <= 1e-14: biofilm is BounceBack for the flow
+    const uint8_t* phase;          // dissolvable phase ids (null without dissolution)
     unsigned long long* counts;    // [0] BGK flow sites, [1] coupled flow NoDyn, [2] coupled ade NoDyn
 };
 
@@ -27,6 +28,9 @@ __device__ __forceinline__ bool is_wall(const ClassK& k, int m) { return m == k.
 // reactive: interior in x and not solid / bounce-back (processor guards of
 // run_kinetics etc.); surface: a face neighbour is solid or bounce-back
 // (surfaceAbioticKinetics3D, precipitationVOP.hh:79-90; y,z periodic here).
+// Phase flags: the voxel carries a phase, or a face neighbour inside
+// x = 1..nx-2 and inside y, z (no wrap: surfaceDissolutionKinetics3D,
+// dissolutionVOP.hh:323-325) does.
 __device__ uint8_t flags_for(const ClassK& k, int64_t n, int x, int y, int z) {
     const int m = k.mask[n];
     uint8_t fl = 0;
@@ -36,6 +40,14 @@ __device__ uint8_t flags_for(const ClassK& k, int64_t n, int x, int y, int z) {
         const int64_t q = nbr(k.g, n, x, y, z, d6[d][0], d6[d][1], d6[d][2]);
         if (q < 0) continue;
         if (is_wall(k, k.mask[q])) { fl |= F_SURFACE; break; }
+    }
+    if (k.phase) {
+        if (k.phase[n]) fl |= F_PHASE_SELF;
+        for (int d = 0; d < 6; ++d) {
+            const int ax = x + d6[d][0], ay = y + d6[d][1], az = z + d6[d][2];
+            if (ax < 1 || ax > k.g.nx - 2 || ay < 0 || ay >= k.g.ny || az < 0 || az >= k.g.nz) continue;
+            if (k.phase[((int64_t)ax * k.g.ny + ay) * k.g.nz + az]) { fl |= F_PHASE_NBR; break; }
+        }
     }
     return fl;
 }
@@ -80,9 +92,22 @@ __global__ void update_dynamics_kernel(ClassK k) {
     }
 }
 
+// class flags only, after a mask or phase change that does not switch dynamics
+// (the reaction processors read the mask every step)
+__global__ void flags_kernel(ClassK k) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < k.g.N; n += stride) {
+        int x, y, z;
+        decode(k.g, n, x, y, z);
+        k.ade[n] = (uint8_t)((k.ade[n] & 3) | flags_for(k, n, x, y, z));
+    }
+}
+
 // Counts that steer the step kernels: BGK flow sites (energy average) and
 // whether any NoDynamics site is linked to a dynamic site (otherwise NoDynamics
-// regions are sealed behind bounce-back and need no streaming at all).
+// regions are sealed behind bounce-back and need no streaming at all).  A
+// NoDynamics solute site whose mask reopened to pore reacts, so it counts as
+// linked too.
 __global__ void class_counts_kernel(ClassK k) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     unsigned long long nb = 0, cf = 0, ca = 0;
@@ -100,7 +125,8 @@ __global__ void class_counts_kernel(ClassK k) {
                 if (c == FLUID || c == BIO) { ++cf; break; }
             }
         }
-        if (ad == NODYN) {
+        if (ad == NODYN && (k.ade[n] & F_REACTIVE)) ++ca;
+        else if (ad == NODYN) {
             for (int i = 1; i < 7; ++i) {
                 const int64_t q = nbr(k.g, n, x, y, z, c7x(i), c7y(i), c7z(i));
                 if (q < 0) continue;
@@ -133,6 +159,7 @@ static ClassK make_classk(Ctx* c) {
     k.n_bio = c->cfg.n_bio_codes;
     for (int i = 0; i < CL_MAX_CODES; ++i) { k.pore[i] = c->cfg.pore_codes[i]; k.bio[i] = c->cfg.bio_codes[i]; }
     k.bio_is_bb = c->cfg.perm_ratio > 1e-14 ? 0 : 1;
+    k.phase = c->d_phase;
     k.counts = reinterpret_cast<unsigned long long*>(c->d_scratch);
     return k;
 }
@@ -157,6 +184,13 @@ int classes_from_mask(Ctx* c) {
     return refresh_counts(c, k);
 }
 
+int refresh_flags(Ctx* c) {
+    ClassK k = make_classk(c);
+    flags_kernel<<<grid_for(c->geo.N, 256, 148 * 16), 256, 0, c->stream>>>(k);
+    CL_LAUNCH_CHECK("flags_kernel");
+    return refresh_counts(c, k);
+}
+
 int update_dynamics(Ctx* c) {
     ClassK k = make_classk(c);
     update_dynamics_kernel<<<grid_for(c->geo.N, 256, 148 * 16), 256, 0, c->stream>>>(k);
@@ -165,9 +199,10 @@ int update_dynamics(Ctx* c) {
 }
 
 // precipNodeConversion3D (precipitationVOP.hh:158-219): a non-wall site whose
-// precipitate inventory reached max_precipRho takes the precipitate code.
+// precipitate inventory reached max_precipRho takes the precipitate code, and
+// the precipitate phase id when one is declared (so it can dissolve later).
 __global__ void precip_kernel(Geo g, uint8_t* mask, const double* inv, double thr, int solid, int bb,
-                              int code, unsigned long long* changed) {
+                              int code, uint8_t* phase, int phase_id, unsigned long long* changed) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     unsigned long long cnt = 0;
     for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < g.N; n += stride) {
@@ -176,6 +211,7 @@ __global__ void precip_kernel(Geo g, uint8_t* mask, const double* inv, double th
         if (inv[n] >= thr) {
             if (m != code) ++cnt;
             mask[n] = (uint8_t)code;
+            if (phase && phase_id > 0) phase[n] = (uint8_t)phase_id;
         }
     }
     for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, o);
@@ -192,13 +228,107 @@ int precip_convert(Ctx* c, int64_t* changed) {
     CL_CUDA(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long), c->stream));
     precip_kernel<<<grid_for(c->geo.N, 256, 148 * 16), 256, 0, c->stream>>>(
         c->geo, c->d_mask, c->d_imm + (int64_t)s * c->geo.N, c->cfg.max_precip_rho,
-        c->cfg.solid_code, c->cfg.bb_code, c->cfg.precip_code, d_cnt);
+        c->cfg.solid_code, c->cfg.bb_code, c->cfg.precip_code, c->d_phase, c->cfg.precip_phase_id, d_cnt);
     CL_LAUNCH_CHECK("precip_kernel");
     unsigned long long h = 0;
     CL_CUDA(cudaMemcpyAsync(&h, d_cnt, sizeof h, cudaMemcpyDeviceToHost, c->stream));
     CL_CUDA(cudaStreamSynchronize(c->stream));
     *changed = (int64_t)h;
+    return h ? refresh_flags(c) : CL_OK;
+}
+
+// initPhaseLattice3D (dissolutionVOP.hh:195-229): a site takes the id of the
+// first grain (not precipitate) phase whose material is its mask code.
+struct PhaseTab {
+    int n;
+    int material[CL_MAX_PHASES], substrate[CL_MAX_PHASES], is_precip[CL_MAX_PHASES];
+    double full[CL_MAX_PHASES], fill[CL_MAX_PHASES];
+};
+
+static PhaseTab make_phasetab(const Ctx* c) {
+    PhaseTab t{};
+    t.n = c->cfg.n_phases;
+    for (int k = 0; k < t.n; ++k) {
+        const cl_phase& ph = c->cfg.phases[k];
+        t.material[k] = ph.material; t.substrate[k] = ph.substrate; t.is_precip[k] = ph.is_precipitate;
+        t.full[k] = ph.full_density; t.fill[k] = ph.initial_fill;
+    }
+    return t;
+}
+
+__global__ void phase_seed_kernel(Geo g, const uint8_t* mask, uint8_t* phase, PhaseTab t) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < g.N; n += stride) {
+        const int m = mask[n];
+        uint8_t pid = 0;
+        for (int k = 0; k < t.n; ++k)
+            if (!t.is_precip[k] && t.material[k] == m) { pid = (uint8_t)(k + 1); break; }
+        phase[n] = pid;
+    }
+}
+
+int phase_seed(Ctx* c) {
+    if (!c->d_phase) return CL_OK;
+    phase_seed_kernel<<<grid_for(c->geo.N, 256, 148 * 16), 256, 0, c->stream>>>(c->geo, c->d_mask, c->d_phase, make_phasetab(c));
+    CL_LAUNCH_CHECK("phase_seed_kernel");
     return CL_OK;
+}
+
+// each grain phase with initial_fill > 0 seeds that inventory on its material
+// (initializeScalarLattice3D, complab.cpp:858-871), phases in declaration order
+__global__ void phase_fill_kernel(Geo g, const uint8_t* mask, double* imm, PhaseTab t) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < g.N; n += stride) {
+        const int m = mask[n];
+        for (int k = 0; k < t.n; ++k)
+            if (!t.is_precip[k] && t.fill[k] > 0.0 && t.material[k] == m) imm[(int64_t)t.substrate[k] * g.N + n] = t.fill[k];
+    }
+}
+
+int phase_fill(Ctx* c) {
+    if (!c->d_phase) return CL_OK;
+    phase_fill_kernel<<<grid_for(c->geo.N, 256, 148 * 16), 256, 0, c->stream>>>(c->geo, c->d_mask, c->d_imm, make_phasetab(c));
+    CL_LAUNCH_CHECK("phase_fill_kernel");
+    return CL_OK;
+}
+
+// dissolNodeConversion3D (dissolutionVOP.hh:459-527): a phase site whose
+// mineral fell below reopen_fraction * full_density takes the pore code and
+// loses its phase id.
+__global__ void dissol_convert_kernel(Geo g, uint8_t* mask, uint8_t* phase, const double* imm, PhaseTab t,
+                                      double reopen, int pore, unsigned long long* changed) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    unsigned long long cnt = 0;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < g.N; n += stride) {
+        const int pid = phase[n];
+        if (pid <= 0 || pid > t.n) continue;
+        const int k = pid - 1;
+        if (!(t.full[k] > 0.0)) continue;
+        const double mineral = imm[(int64_t)t.substrate[k] * g.N + n];
+        if (mineral < reopen * t.full[k]) {
+            if (mask[n] != pore) ++cnt;
+            mask[n] = (uint8_t)pore;
+            phase[n] = 0;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, o);
+    if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(changed, cnt);
+}
+
+int dissol_convert(Ctx* c, int64_t* changed) {
+    *changed = 0;
+    if (!c->d_phase) { set_error("dissolution is not enabled in this context"); return CL_ERR_STATE; }
+    const int pore = c->cfg.n_pore_codes > 0 ? c->cfg.pore_codes[0] : 2;
+    unsigned long long* d_cnt = reinterpret_cast<unsigned long long*>(c->d_scratch);
+    CL_CUDA(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long), c->stream));
+    dissol_convert_kernel<<<grid_for(c->geo.N, 256, 148 * 16), 256, 0, c->stream>>>(
+        c->geo, c->d_mask, c->d_phase, c->d_imm, make_phasetab(c), c->cfg.reopen_fraction, pore, d_cnt);
+    CL_LAUNCH_CHECK("dissol_convert_kernel");
+    unsigned long long h = 0;
+    CL_CUDA(cudaMemcpyAsync(&h, d_cnt, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+    CL_CUDA(cudaStreamSynchronize(c->stream));
+    *changed = (int64_t)h;
+    return h ? refresh_flags(c) : CL_OK;
 }
 
 // Deterministic FP64 reduction: fixed-size grid, per-block partials, one final

@@ -27,6 +27,18 @@ struct FlowTracer {
     double eps;
 };
 
+// A surrogate network as the transport kernel reads it: FP32 parameters in
+// device memory (W then b, layer by layer) and the mapminmax settings.
+struct SrgNetDev {
+    int L;
+    int w[CL_SRG_MAX_LAYERS + 1];
+    int poff[CL_SRG_MAX_LAYERS];
+    float xo[CL_SRG_MAX_WIDTH], xg[CL_SRG_MAX_WIDTH], xlo[CL_SRG_MAX_WIDTH], xhi[CL_SRG_MAX_WIDTH];
+    float yo[CL_SRG_MAX_WIDTH], yg[CL_SRG_MAX_WIDTH];
+    float xymin, yymin;
+    const float* params;
+};
+
 // Per-solute transport parameters passed by value to the transport kernels.
 struct AdeParams {
     int    S;                          // all solutes
@@ -39,12 +51,18 @@ struct AdeParams {
     float  left_val[CL_MAX_SOLUTES], right_val[CL_MAX_SOLUTES];
     int    M;                          // microbes
     double dt;
-    int    do_kin, do_abio, surface_only, do_eq;
+    int    do_kin, do_abio, surface_only, do_eq, eq_warm;
     int    n_rxn;
     cl_rxn rxn[CL_MAX_RXN];
     double decay[CL_MAX_MICROBES];
     cl_eq_system eq;
     int    solid_code, bb_code;
+    int    n_srg;
+    cl_srg_organism srg[CL_MAX_SRG_ORG];
+    SrgNetDev net[CL_MAX_SRG_ORG];
+    // dissolution: phase id k+1 is phase[k] (ids are checked to be 1..n_phases)
+    int    do_dissol, dissol_surface_only, dissol_walls, n_phases;
+    cl_phase phase[CL_MAX_PHASES];
 };
 
 struct Ctx {
@@ -75,6 +93,11 @@ struct Ctx {
     float*   d_u = nullptr;          // 3*N
     float*   d_rho_adj = nullptr;    // n_mob*2*plane : pre-collision density next to each x face
     int32_t* d_eq_iters = nullptr;   // N
+    float*   d_srg_params[CL_MAX_SRG_ORG] = {nullptr, nullptr};
+    double*  d_eq_x = nullptr;       // n_comp*N previous converged log10 free components (NaN: none)
+    uint8_t* d_phase = nullptr;      // N dissolvable phase id, 0 = none (dissolution only)
+    double*  d_rel = nullptr;        // S*N this step's release of each phase voxel: products per open
+                                     // face, and at the phase substrate the voxel's own decrement
     unsigned long long* d_counters = nullptr;  // [0] non-converged Newton solves
     // scratch for reductions / field IO
     double*  d_scratch = nullptr;
@@ -106,6 +129,10 @@ int ade_density(Ctx* c, int s, double* d_out);
 int flow_population_io(Ctx* c, float* d_natural, int to_natural);
 int ade_population_io(Ctx* c, int slot, float* d_natural);
 int precip_convert(Ctx* c, int64_t* changed);
+int dissol_convert(Ctx* c, int64_t* changed);
+int phase_seed(Ctx* c);          // grain phases from the mask (initPhaseLattice3D)
+int phase_fill(Ctx* c);          // grain inventories (initial_fill) after ade_init
+int refresh_flags(Ctx* c);       // class flags after a mask / phase change, dynamics kept
 int update_dynamics(Ctx* c);
 int reduce_field(Ctx* c, const double* d_field, int op, double arg, const uint8_t* d_mask, double* out);
 

@@ -43,8 +43,10 @@ __host__ __device__ constexpr float t7(int i) { return i == 0 ? 0.25f : 0.125f; 
 
 // node classes (low two bits of a class byte)
 enum : uint8_t { NODYN = 0, BB = 1, FLUID = 2, BIO = 3 };
-// class-byte flags
-enum : uint8_t { F_REACTIVE = 4, F_SURFACE = 8 };
+// class-byte flags: reactive (interior x, not solid / bounce-back), surface (a
+// face neighbour is solid / bounce-back), phase-neighbour (a face neighbour in
+// x = 1..nx-2 carries a dissolvable phase), phase-self (carries one itself)
+enum : uint8_t { F_REACTIVE = 4, F_SURFACE = 8, F_PHASE_NBR = 16, F_PHASE_SELF = 32 };
 
 struct Geo {
     int nx, ny, nz;

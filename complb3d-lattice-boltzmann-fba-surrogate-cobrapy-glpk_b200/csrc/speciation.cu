@@ -379,6 +379,40 @@ __global__ void newton_fallback_kernel(EqDev e, const double* totals, const doub
     }
 }
 
+// One pass of the bucketed solve: every listed voxel (all n when `in_list` is
+// null) runs at most `budget` Newton iterations from its stored x (mode 0), the
+// reference's cold start (mode 1) or the given start (mode 2); converged voxels
+// get status `ok_status`, the others are appended to `out_list` for the next
+// pass, or get status 2 when this is the last pass.  Newton keeps no state
+// besides x, so a solve split over passes is the same solve.
+template <int NC>
+__global__ void newton_pass_kernel(EqDev e, const double* totals, const double* cold_species, double* logfree,
+                                   int32_t* iters, uint8_t* status, const int64_t* in_list,
+                                   const unsigned long long* in_count, int64_t n, int mode, int budget, double tol,
+                                   int ok_status, int last, int64_t* out_list, unsigned long long* out_count) {
+    const int64_t cnt = in_list ? (int64_t)*in_count : n;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < cnt; q += stride) {
+        const int64_t k = in_list ? in_list[q] : q;
+        double T[NC], x[NC];
+#pragma unroll
+        for (int j = 0; j < NC; ++j) T[j] = totals[k * NC + j];
+        if (mode == 1) eq_cold_start<NC>(e, cold_species + k * e.ns, x);
+        else {
+#pragma unroll
+            for (int j = 0; j < NC; ++j) x[j] = logfree[k * NC + j];
+        }
+        int conv = 0;
+        const int it = eq_newton<NC>(e, T, x, budget, tol, &conv);
+#pragma unroll
+        for (int j = 0; j < NC; ++j) logfree[k * NC + j] = x[j];
+        if (iters) iters[k] = (mode == 0 ? iters[k] : (mode == 1 && in_list ? iters[k] : 0)) + it;
+        if (conv) { if (status) status[k] = (uint8_t)ok_status; }
+        else if (last) { if (status) status[k] = 2; }
+        else out_list[atomicAdd(out_count, 1ull)] = k;
+    }
+}
+
 }  // namespace cl
 
 using namespace cl;
@@ -397,9 +431,10 @@ struct cl_eq_solver {
     int part_blocks = 0;
     float* grad = nullptr;     // n_params + 1 (loss)
     bool trained = false;
-    int64_t* fail_list = nullptr;
+    int64_t* fail_list = nullptr;     // ping-pong lists of the bucketed solve
+    int64_t* fail_list2 = nullptr;
     int64_t fail_cap = 0;
-    unsigned long long* fail_count = nullptr;
+    unsigned long long* fail_count = nullptr;   // two counters
     uint64_t adam_t = 0;
 };
 
@@ -408,9 +443,61 @@ static size_t mlp_smem_bytes() { return sizeof(MlpSmem); }
 static int eq_ensure_fail(cl_eq_solver* s, int64_t n) {
     if (s->fail_cap >= n) return CL_OK;
     if (s->fail_list) cudaFree(s->fail_list);
-    s->fail_list = nullptr;
+    if (s->fail_list2) cudaFree(s->fail_list2);
+    s->fail_list = s->fail_list2 = nullptr;
     CL_CUDA(cudaMalloc(&s->fail_list, sizeof(int64_t) * (size_t)std::max<int64_t>(n, 1)));
+    CL_CUDA(cudaMalloc(&s->fail_list2, sizeof(int64_t) * (size_t)std::max<int64_t>(n, 1)));
     s->fail_cap = n;
+    return CL_OK;
+}
+
+// Iteration budgets of the bucketed passes: short passes first (most solves
+// finish there), then doubling, summing to `total`.
+static std::vector<int> bucket_budgets(int total, int first) {
+    std::vector<int> b;
+    int used = 0, next = std::max(1, first);
+    while (used < total) {
+        const int take = std::min(next, total - used);
+        b.push_back(take);
+        used += take;
+        if (b.size() >= 2) next *= 2;
+    }
+    return b;
+}
+
+template <int NC>
+static int bucketed_solve(cl_eq_solver* s, const double* T, const double* cold, double* x, int32_t* it,
+                          uint8_t* st, int64_t n, int start) {
+    const int blocks = grid_for(n, 128, 148 * 16);
+    unsigned long long* cnt[2] = {s->fail_count, s->fail_count + 1};
+    int64_t* lists[2] = {s->fail_list, s->fail_list2};
+    int cur = -1;   // list holding the voxels still to solve (-1: all n)
+    auto pass = [&](int mode, int budget, int ok_status, bool last) -> int {
+        const int out = (cur == 0) ? 1 : 0;
+        CL_CUDA(cudaMemsetAsync(cnt[out], 0, sizeof(unsigned long long), s->stream));
+        newton_pass_kernel<NC><<<blocks, 128, 0, s->stream>>>(
+            s->e, T, cold, x, it, st, cur < 0 ? nullptr : lists[cur], cur < 0 ? nullptr : cnt[cur], n, mode, budget,
+            s->sys.tol, ok_status, last ? 1 : 0, lists[out], cnt[out]);
+        CL_LAUNCH_CHECK("newton_pass_kernel");
+        cur = out;
+        return CL_OK;
+    };
+    int r = CL_OK;
+    std::vector<int> cold_b = bucket_budgets(s->sys.max_iter, 3);
+    if (start == CL_EQ_START_COLD) {
+        for (size_t i = 0; i < cold_b.size(); ++i)
+            if ((r = pass(i == 0 ? 1 : 0, cold_b[i], 0, i + 1 == cold_b.size()))) return r;
+        return CL_OK;
+    }
+    // warm start with warm_iter iterations in short passes, then the cold
+    // restart for the misses
+    const bool fallback = cold != nullptr;
+    std::vector<int> warm_b = bucket_budgets(s->sys.warm_iter, 2);
+    for (size_t i = 0; i < warm_b.size(); ++i)
+        if ((r = pass(i == 0 ? 2 : 0, warm_b[i], 0, !fallback && i + 1 == warm_b.size()))) return r;
+    if (!fallback) return CL_OK;
+    for (size_t i = 0; i < cold_b.size(); ++i)
+        if ((r = pass(i == 0 ? 1 : 0, cold_b[i], 1, i + 1 == cold_b.size()))) return r;
     return CL_OK;
 }
 
@@ -464,7 +551,7 @@ cl_eq_solver* cl_eq_create(const cl_eq_system* sys, void* stream, int* status) {
     A((void**)&s->m2, sizeof(float) * np);
     A((void**)&s->part, sizeof(float) * (size_t)s->part_blocks * (np + 1));
     A((void**)&s->grad, sizeof(float) * (np + 1));
-    A((void**)&s->fail_count, sizeof(unsigned long long));
+    A((void**)&s->fail_count, 2 * sizeof(unsigned long long));
     if (e != cudaSuccess) return fail(cuda_fail(e, "cl_eq_create"), s);
     if (cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mlp_smem_bytes()) != cudaSuccess ||
         cudaFuncSetAttribute(mlp_predict_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mlp_smem_bytes()) != cudaSuccess)
@@ -495,7 +582,7 @@ int cl_eq_destroy(cl_eq_solver* s) {
     if (!s) return CL_OK;
     if (s->stream) cudaStreamSynchronize(s->stream);
     void* ptrs[] = {s->w.W1, s->w.W2, s->w.W2T, s->w.W3, s->w.W3T, s->w.b, s->w.norm, s->master, s->m1, s->m2,
-                    s->part, s->grad, s->fail_list, s->fail_count};
+                    s->part, s->grad, s->fail_list, s->fail_list2, s->fail_count};
     for (void* p : ptrs) if (p) cudaFree(p);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     delete s;
@@ -523,59 +610,25 @@ int cl_eq_set_params(cl_eq_solver* s, const float* host) {
     return CL_OK;
 }
 
-static int launch_first(cl_eq_solver* s, const double* T, const double* cold, double* x, int32_t* it, uint8_t* st,
-                        int64_t n, int start, int limit, bool list) {
-    const int blocks = grid_for(n, 128, 148 * 16);
-    int64_t* fl = list ? s->fail_list : nullptr;
-#define CL_EQ_FIRST(NCV) newton_first_kernel<NCV><<<blocks, 128, 0, s->stream>>>(s->e, T, cold, x, it, st, n, start, limit, s->sys.tol, fl, s->fail_count)
-    switch (s->nc) {
-        case 1: CL_EQ_FIRST(1); break;
-        case 2: CL_EQ_FIRST(2); break;
-        case 3: CL_EQ_FIRST(3); break;
-        case 4: CL_EQ_FIRST(4); break;
-        default: CL_EQ_FIRST(5); break;
-    }
-#undef CL_EQ_FIRST
-    CL_LAUNCH_CHECK("newton_first_kernel");
-    return CL_OK;
-}
-
-static int launch_fallback(cl_eq_solver* s, const double* T, const double* cold, double* x, int32_t* it, uint8_t* st,
-                           int64_t n) {
-    const int blocks = grid_for(n, 128, 148 * 16);
-#define CL_EQ_FB(NCV) newton_fallback_kernel<NCV><<<blocks, 128, 0, s->stream>>>(s->e, T, cold, x, it, st, s->fail_list, s->fail_count, s->sys.max_iter, s->sys.tol)
-    switch (s->nc) {
-        case 1: CL_EQ_FB(1); break;
-        case 2: CL_EQ_FB(2); break;
-        case 3: CL_EQ_FB(3); break;
-        case 4: CL_EQ_FB(4); break;
-        default: CL_EQ_FB(5); break;
-    }
-#undef CL_EQ_FB
-    CL_LAUNCH_CHECK("newton_fallback_kernel");
-    return CL_OK;
-}
-
 int cl_eq_solve_device(cl_eq_solver* s, const double* d_totals, const double* d_cold_species, double* d_logfree,
                        int32_t* d_iters, uint8_t* d_status, int64_t n, int32_t start) {
     if (!s || !d_totals || !d_logfree || n < 0) { set_error("null argument"); return CL_ERR_ARG; }
     if (n == 0) return CL_OK;
-    if (start == CL_EQ_START_COLD) {
-        if (!d_cold_species) { set_error("cold start needs the species vectors"); return CL_ERR_ARG; }
-        return launch_first(s, d_totals, d_cold_species, d_logfree, d_iters, d_status, n, start, s->sys.max_iter, false);
-    }
+    if (start == CL_EQ_START_COLD && !d_cold_species) { set_error("cold start needs the species vectors"); return CL_ERR_ARG; }
     if (start == CL_EQ_START_LEARNED) {
         mlp_predict_kernel<<<grid_for((n + TS - 1) / TS, 1, 148 * 2), MLP_THREADS, mlp_smem_bytes(), s->stream>>>(
             s->w, s->nc, d_totals, d_logfree, nullptr, nullptr, n);
         CL_LAUNCH_CHECK("mlp_predict_kernel");
-    } else if (start != CL_EQ_START_GIVEN) { set_error("unknown start mode"); return CL_ERR_ARG; }
-    const bool fallback = d_cold_species != nullptr;
-    int r = CL_OK;
-    if (fallback && (r = eq_ensure_fail(s, n))) return r;
-    if (fallback) CL_CUDA(cudaMemsetAsync(s->fail_count, 0, sizeof(unsigned long long), s->stream));
-    if ((r = launch_first(s, d_totals, d_cold_species, d_logfree, d_iters, d_status, n, start, s->sys.warm_iter, fallback))) return r;
-    if (fallback && (r = launch_fallback(s, d_totals, d_cold_species, d_logfree, d_iters, d_status, n))) return r;
-    return CL_OK;
+    } else if (start != CL_EQ_START_GIVEN && start != CL_EQ_START_COLD) { set_error("unknown start mode"); return CL_ERR_ARG; }
+    int r = eq_ensure_fail(s, n);
+    if (r) return r;
+    switch (s->nc) {
+        case 1: return bucketed_solve<1>(s, d_totals, d_cold_species, d_logfree, d_iters, d_status, n, start);
+        case 2: return bucketed_solve<2>(s, d_totals, d_cold_species, d_logfree, d_iters, d_status, n, start);
+        case 3: return bucketed_solve<3>(s, d_totals, d_cold_species, d_logfree, d_iters, d_status, n, start);
+        case 4: return bucketed_solve<4>(s, d_totals, d_cold_species, d_logfree, d_iters, d_status, n, start);
+        default: return bucketed_solve<5>(s, d_totals, d_cold_species, d_logfree, d_iters, d_status, n, start);
+    }
 }
 
 int cl_eq_solve_host(cl_eq_solver* s, const double* totals, const double* cold_species, double* logfree,

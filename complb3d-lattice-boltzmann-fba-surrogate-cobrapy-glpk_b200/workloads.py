@@ -166,13 +166,14 @@ def seed_biomass(mask, seed, frac=0.02, lo=10.0, hi=50.0):
 COUPLED_SOLUTES = ["DOC", "O2", "NO3-", "HCO3-", "Ca2+", "H+", "CO3--", "CaCO3(aq)", "CaCO3(s)"]
 
 
-def coupled_config(pkg, nx, ny, nz, seed=5):
+def coupled_config(pkg, nx, ny, nz, seed=5, warm_previous=True):
     """Flow + 8 mobile solutes + 1 immobile mineral:
       kinetics   dual-Monod oxidation of DOC by O2 and by NO3- (one sessile
                  microbe), Vmax ~ U[1e-5, 1e-4], Ks ~ U[1e-3, 1e-1] per step;
       speciation components HCO3-, Ca2+, H+ with CO3-- (logK -10.33) and
                  CaCO3(aq) (logK -7.13) as secondary species, Newton to a 1e-10
-                 relative residual every step in every pore voxel;
+                 relative residual every step in every pore voxel, started
+                 from the voxel's previous solution (cold start after 4 misses);
       precipitation Ca2+ + CO3-- -> CaCO3(s), rate 1e-6 [Ca][CO3], on wall-
                  adjacent voxels only; a voxel whose inventory reaches 1.0
                  becomes solid (node conversion every 200 steps)."""
@@ -204,7 +205,8 @@ def coupled_config(pkg, nx, ny, nz, seed=5):
     S[6] = [1, 0, -1]
     S[7] = [1, 1, -1]
     logk = [0, 0, 0, 0, 0, 0, -10.33, -7.13, 0]
-    pkg.set_eq_system(cfg.eq, S, logk, [3, 4, 5], max_iter=100, tol=1e-10, warm_iter=8)
+    pkg.set_eq_system(cfg.eq, S, logk, [3, 4, 5], max_iter=100, tol=1e-10, warm_iter=4)
+    cfg.eq_warm_previous = 1 if warm_previous else 0
     return cfg
 
 
@@ -220,3 +222,52 @@ def cold_species(S, T, comp_species=None):
         if cs[j] >= 0:
             c[:, cs[j]] = T[:, j]
     return c
+
+
+def surrogate_nets(pkg, seed=0):
+    """Two organism networks, 3 -> 20 tanh -> 20 tanh -> 4 linear, weights
+    ~N(0, 0.3); inputs (donor, acceptor, biomass) clamped to their mapminmax
+    box; outputs (growth 1/h, donor uptake, acceptor uptake, product uptake),
+    uptakes in mmol/gDW/h (positive = consumed, so the product's is negative)."""
+    rng = np.random.default_rng(seed)
+    nets = []
+    for o in range(2):
+        widths = [3, 20, 20, 4]
+        W = [rng.normal(0, 0.3, (widths[l + 1], widths[l])) for l in range(3)]
+        b = [rng.normal(0, 0.3, widths[l + 1]) for l in range(3)]
+        lo = np.array([0.0, 0.0, 0.0])
+        hi = np.array([2e-3, 1e-3, 60.0])
+        gain = 2.0 / (hi - lo)
+        # output box: growth 0..0.4 1/h, uptakes 0..8, product -8..0
+        y_lo = np.array([0.0, 0.0, 0.0, -8.0])
+        y_hi = np.array([0.4, 8.0, 8.0, 0.0])
+        nets.append(pkg.make_surrogate_net(widths, W, b, lo, gain, y_lo, 2.0 / (y_hi - y_lo), x_lo=lo, x_hi=hi))
+    return nets
+
+
+def surrogate_config(pkg, nx, ny, nz, seed=6):
+    """Six solutes (donor, acceptor, product of each of two organisms) fed by
+    the surrogate reaction type of two organisms on sessile biomass."""
+    rng = np.random.default_rng(seed)
+    taus = rng.uniform(0.6, 0.9, 6)
+    inlet = [1e-3, 5e-4, 0.0, 1e-3, 5e-4, 0.0]
+    sol = [{"tau": float(taus[s]), "c0": inlet[s] * 0.5, "left": "D", "left_value": inlet[s], "right": "N"}
+           for s in range(6)]
+    cfg = pkg.make_config(nx, ny, nz, tau_ns=0.8, rho_in=1.0005, rho_out=1.0, solutes=sol, microbes=2, dt=360.0)
+    cfg.n_srg = 2
+    for o in range(2):
+        g = cfg.srg[o]
+        g.microbe, g.net = o, o
+        base = 3 * o
+        for i, (kind, idx) in enumerate([(pkg.SRG_IN_CONC, base), (pkg.SRG_IN_CONC, base + 1),
+                                         (pkg.SRG_IN_BIOMASS, 0)]):
+            g.in_kind[i], g.in_index[i] = kind, idx
+        for q, (kind, idx) in enumerate([(pkg.SRG_OUT_GROWTH, 0), (pkg.SRG_OUT_FOUT, base),
+                                         (pkg.SRG_OUT_FOUT, base + 1), (pkg.SRG_OUT_FOUT, base + 2)]):
+            g.out_kind[q], g.out_index[q] = kind, idx
+        for s in range(6):
+            g.kc[s] = 1e-4
+            g.vmax[s] = 5.0 if s in (base, base + 1) else 0.0
+        g.mw = 24.6
+        g.kd = 1e-7
+    return cfg

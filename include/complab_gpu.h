@@ -87,19 +87,65 @@ typedef struct {
     int32_t warm_iter;                 /* k: Newton iterations allowed from the learned start */
 } cl_eq_system;
 
-/* Dissolvable solid phase (reference SolidPhase, src/dissolutionVOP.hh:142-154) */
+/* Dissolvable solid phase (reference SolidPhase, src/dissolutionVOP.hh:142-154)
+ * and its rate law (the defineDissolutionRate hook, defineAbioticKinetics.hh:292):
+ *   rate = k * mineral * prod_j water[mass_s[j]]   (water: mean over open faces)
+ *   mineralR = -rate ;  subsR[s] = nu[s] * rate
+ * as examples/14_dissolution and 15_precip_and_dissolution write it (calcite or
+ * FeS + H+).  phases[k].id must be k+1 (the reference numbers them so,
+ * complab.cpp:329); the substrate must be an immobile solute. */
 typedef struct {
-    int32_t id;
-    int32_t material;
+    int32_t id;                        /* 1-based */
+    int32_t material;                  /* material number the phase occupies (grain phases) */
     int32_t substrate;                 /* immobile solute holding its inventory */
-    double  full_density;
-    /* first-order dissolution law: rate = -k_dis * mineral * (1 - C[sat_s]/c_sat),
-     * products nu_prod[s] * (-rate) scattered to open faces */
-    double  k_dis;
-    int32_t sat_s;
-    double  c_sat;
-    double  nu_prod[CL_MAX_SOLUTES];
+    int32_t is_precipitate;            /* stamped by precipitation instead of seeded from the geometry */
+    double  full_density;              /* mol/L in a full voxel */
+    double  initial_fill;              /* mol/L seeded on `material` at start */
+    double  k;
+    int32_t n_mass;
+    int32_t mass_s[2];
+    double  nu[CL_MAX_SOLUTES];
 } cl_phase;
+
+/* ---- surrogate reaction type (row a13) ----------------------------------------
+ * Feed-forward network with mapminmax scaling (reference defineSurrogateModel,
+ * surrogateModel.hh:252-501).  Layers: widths[0] inputs ... widths[n_layers]
+ * outputs; tanh on hidden layers, linear output. */
+#define CL_SRG_MAX_LAYERS 5
+#define CL_SRG_MAX_WIDTH  32
+typedef struct {
+    int32_t n_layers;
+    int32_t widths[CL_SRG_MAX_LAYERS + 1];
+    double  x_offset[CL_SRG_MAX_WIDTH], x_gain[CL_SRG_MAX_WIDTH], x_ymin;
+    double  y_offset[CL_SRG_MAX_WIDTH], y_gain[CL_SRG_MAX_WIDTH], y_ymin;
+    double  x_lo[CL_SRG_MAX_WIDTH], x_hi[CL_SRG_MAX_WIDTH];   /* input clamp box */
+    /* weights, row-major W[l][out][in] then bias b[l][out], packed layer by layer */
+    double  params[4096];
+} cl_surrogate_net;
+/* One organism of the surrogate reaction type (run_surrogate3D,
+ * src/complab3d_processors_surrogate.hh:74-295).  Per voxel where its biomass
+ * exceeds 1e-12: Michaelis-Menten uptake estimates Fin[s] = Vmax*C/(Kc+C) (or,
+ * with no Vmax, the flux that would exhaust C in one step), capped by that
+ * exhaustion flux; the network maps its inputs to a growth rate (1/h) and,
+ * optionally, uptake fluxes Fout[s] (default Fout = Fin); biomass grows by
+ * mu*B*dt/3600 or decays by kd*B*dt; the substrate draw summed over organisms is
+ * clamped to what the voxel holds.  Fluxes are mmol/gDW/h, B mol/L. */
+#define CL_MAX_SRG_ORG     2
+#define CL_SRG_IN_FIN      0     /* input: Fin of solute in_index */
+#define CL_SRG_IN_CONC     1     /* input: concentration of solute in_index */
+#define CL_SRG_IN_BIOMASS  2     /* input: this organism's biomass */
+#define CL_SRG_OUT_GROWTH  0     /* output: specific growth rate, 1/h */
+#define CL_SRG_OUT_FOUT    1     /* output: uptake flux of solute out_index (positive = consumed) */
+typedef struct {
+    int32_t microbe;                       /* biomass field of this organism */
+    int32_t net;                           /* network slot set by cl_set_surrogate */
+    int32_t in_kind[CL_SRG_MAX_WIDTH], in_index[CL_SRG_MAX_WIDTH];
+    int32_t out_kind[CL_SRG_MAX_WIDTH], out_index[CL_SRG_MAX_WIDTH];
+    double  kc[CL_MAX_SOLUTES];            /* half-saturation per solute */
+    double  vmax[CL_MAX_SOLUTES];          /* <maximum_uptake_flux>; <= 1e-12: exhaustion flux */
+    double  mw;                            /* <biomass_molar_mass>, gDW/mol */
+    double  kd;                            /* decay, 1/s */
+} cl_srg_organism;
 
 typedef struct {
     /* lattice */
@@ -137,6 +183,8 @@ typedef struct {
     double  decay[CL_MAX_MICROBES];    /* kd, 1/s */
     int32_t use_equilibrium;
     cl_eq_system eq;
+    int32_t eq_warm_previous;          /* 1: start each voxel's Newton from its previous converged solution
+                                          (cold start after eq.warm_iter misses); 0: the reference's cold start */
     /* precipitation / dissolution (reference src/precipitationVOP.hh, src/dissolutionVOP.hh) */
     int32_t precip_enabled;
     int32_t precip_substrate;          /* immobile solute holding the precipitate */
@@ -146,8 +194,14 @@ typedef struct {
     int32_t dissol_enabled;
     double  reopen_fraction;
     int32_t dissol_surface_only;
+    int32_t dissol_apply_at_walls;     /* 0: as the reference, a mineral decrement on a solid/bounce-back
+                                          voxel is dropped (update_abiotic_rxnLattices skips walls);
+                                          1: it is applied, so grains can dissolve and reopen */
     int32_t n_phases;
     cl_phase phases[CL_MAX_PHASES];
+    /* surrogate reaction type: organisms, networks uploaded by cl_set_surrogate */
+    int32_t n_srg;
+    cl_srg_organism srg[CL_MAX_SRG_ORG];
 } cl_config;
 
 typedef struct cl_ctx cl_ctx;
@@ -227,6 +281,9 @@ int cl_timing_enable(cl_ctx* ctx, int32_t on);
 int cl_timing_read(cl_ctx* ctx, int32_t kernel, double* total_ms, int64_t* launches);
 int cl_launch_count(const cl_ctx* ctx, int64_t* launches);
 
+/* network of the surrogate reaction type, slot 0..CL_MAX_SRG_ORG-1 (before cl_step) */
+int cl_set_surrogate(cl_ctx* ctx, int32_t slot, const cl_surrogate_net* net);
+
 /* ---- reductions (row a17) ----------------------------------------------------- */
 #define CL_RED_SUM   0
 #define CL_RED_MIN   1
@@ -235,9 +292,16 @@ int cl_launch_count(const cl_ctx* ctx, int64_t* launches);
 int cl_reduce(cl_ctx* ctx, int32_t field, int32_t index, int32_t op, double arg, double* out);
 
 /* ---- geometry updates (rows a14-a15) --------------------------------------------
- * precipNodeConversion3D (src/precipitationVOP.hh:158-219) and
- * dissolNodeConversion3D (src/dissolutionVOP.hh:459-527).  *changed = number of
- * sites whose mask changed. */
+ * precipNodeConversion3D (src/precipitationVOP.hh:158-219; stamps
+ * precip_phase_id on the voxels it seals) and dissolNodeConversion3D
+ * (src/dissolutionVOP.hh:459-527; reopens to the first pore code).  *changed =
+ * number of sites whose mask changed; the reaction gates follow the new mask at
+ * once, the flow / solute dynamics only after cl_update_dynamics, as in the
+ * reference's loop (complab.cpp:1783-1845).  Mineral release
+ * (surfaceDissolutionKinetics3D, :265-435) runs inside cl_step when
+ * dissol_enabled; the phase lattice is seeded from the mask by cl_upload_mask
+ * (initPhaseLattice3D) and the grain inventories by cl_ade_init.
+ * CL_FIELD_PHASE reads and writes the phase ids (0 = none). */
 int cl_precip_convert(cl_ctx* ctx, int64_t* changed);
 int cl_dissol_convert(cl_ctx* ctx, int64_t* changed);
 
@@ -300,21 +364,6 @@ int cl_eq_get_params(cl_eq_solver* s, float* host_params);
 int cl_eq_set_params(cl_eq_solver* s, const float* host_params);
 int cl_eq_predict_host(cl_eq_solver* s, const float* x, float* y, int32_t n);
 
-/* ---- surrogate reaction type (row a13) ----------------------------------------
- * Feed-forward network with mapminmax scaling (reference defineSurrogateModel,
- * surrogateModel.hh:252-501).  Layers: widths[0] inputs ... widths[n_layers]
- * outputs; tanh on hidden layers, linear output. */
-#define CL_SRG_MAX_LAYERS 5
-#define CL_SRG_MAX_WIDTH  32
-typedef struct {
-    int32_t n_layers;
-    int32_t widths[CL_SRG_MAX_LAYERS + 1];
-    double  x_offset[CL_SRG_MAX_WIDTH], x_gain[CL_SRG_MAX_WIDTH], x_ymin;
-    double  y_offset[CL_SRG_MAX_WIDTH], y_gain[CL_SRG_MAX_WIDTH], y_ymin;
-    double  x_lo[CL_SRG_MAX_WIDTH], x_hi[CL_SRG_MAX_WIDTH];   /* input clamp box */
-    /* weights, row-major W[l][out][in] then bias b[l][out], packed layer by layer */
-    double  params[4096];
-} cl_surrogate_net;
 #define CL_SRG_TENSOR 0   /* BF16 tensor-core inference, FP32 accumulate */
 #define CL_SRG_FP32   1   /* FP32 CUDA-core reference kernel */
 int cl_surrogate_batch_device(const cl_surrogate_net* net, const float* d_x, float* d_y,

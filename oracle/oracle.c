@@ -12,6 +12,9 @@
 #include <float.h>
 
 #define THRD 1e-12                 /* src/complab3d_processors.hh: thrd */
+
+/* sizeof(cl_config) as this library was compiled, for binding checks */
+int orc_config_size(void) { return (int)sizeof(cl_config); }
 #define COMPLAB_THRD 1e-14         /* src/complab_functions.hh:64 */
 
 /* ---------------------------------------------------------------- lattices */
@@ -258,6 +261,30 @@ void orc_ade_init(const cl_config* cfg, orc_state* st) {
             st->rho_bc[(s*2 + 1)*P + p] = cfg->right_type[s] == CL_BC_DIRICHLET ? cfg->right_value[s] : cfg->c0[s];
         }
     }
+    /* initPhaseLattice3D (dissolutionVOP.hh:195-229): grain phases take their
+     * id where the geometry holds their material; then each grain phase with
+     * initial_fill > 0 seeds that inventory there (initializeScalarLattice3D,
+     * complab.cpp:858-871) */
+    if (cfg->dissol_enabled && st->phase) {
+        for (int64_t n = 0; n < N; ++n) {
+            uint8_t pid = 0;
+            for (int k = 0; k < cfg->n_phases; ++k) {
+                if (cfg->phases[k].is_precipitate) continue;
+                if (cfg->phases[k].material == st->mask[n]) { pid = (uint8_t)cfg->phases[k].id; break; }
+            }
+            st->phase[n] = pid;
+        }
+        for (int k = 0; k < cfg->n_phases; ++k) {
+            const cl_phase* ph = &cfg->phases[k];
+            if (ph->is_precipitate || !(ph->initial_fill > 0.0)) continue;
+            const int s = ph->substrate;
+            for (int64_t n = 0; n < N; ++n) {
+                if (st->mask[n] != ph->material) continue;
+                if (cfg->immobile[s]) st->imm[s*N + n] = ph->initial_fill;
+                else for (int i = 0; i < 7; ++i) st->g[(s*7 + i)*N + n] = T7[i] * ph->initial_fill;
+            }
+        }
+    }
 }
 
 /* computeDensity of every site.  A dynamic cell on an x face answers with its
@@ -314,6 +341,62 @@ void orc_rates(const cl_config* cfg, int abiotic, const double* C, const double*
         }
     for (int s = 0; s < cfg->n_solutes; ++s) if (!isfinite(subsR[s])) subsR[s] = 0.0;
     if (bioR) for (int m = 0; m < cfg->n_microbes; ++m) if (!isfinite(bioR[m])) bioR[m] = 0.0;
+}
+
+/* Surrogate reaction type at one voxel (run_surrogate3D,
+ * src/complab3d_processors_surrogate.hh:94-295, with MetabolicConfig's
+ * conversions, complab3d_metabolic.hh:481-519).  C: densities before
+ * update_rxnLattices; B: floored biomass.  Adds thresholded increments to
+ * D (solutes) and DB (biomass). */
+static void orc_surrogate_voxel(const cl_config* cfg, const cl_surrogate_net* nets, const double* C,
+                                const double* B, double* D, double* DB) {
+    const int S = cfg->n_solutes;
+    double conc[CL_MAX_SOLUTES], draw[CL_MAX_SOLUTES];
+    int any = 0;
+    for (int o = 0; o < cfg->n_srg; ++o) if (B[cfg->srg[o].microbe] > THRD) any = 1;
+    if (!any) return;
+    for (int s = 0; s < S; ++s) { conc[s] = C[s] > THRD ? C[s] : 0.0; draw[s] = 0.0; }
+    for (int o = 0; o < cfg->n_srg; ++o) {
+        const cl_srg_organism* g = &cfg->srg[o];
+        const cl_surrogate_net* net = &nets[g->net];
+        const double b = B[g->microbe];
+        if (!(b > THRD)) continue;
+        double fin[CL_MAX_SOLUTES], fout[CL_MAX_SOLUTES];
+        const double denom = b * g->mw * cfg->dt;
+        for (int s = 0; s < S; ++s) {
+            const double av = conc[s];
+            const double mm = (g->kc[s] + av > 0.0) ? av / (g->kc[s] + av) : 0.0;
+            double exh = 0.0;                                  /* exhaustionFlux */
+            if (denom > 1e-30) { exh = -av * 3.6e6 / denom; if (exh < -1e4) exh = -1e4; }
+            double v = g->vmax[s] > THRD ? g->vmax[s] * mm : -exh * mm;
+            const double cap = -exh;
+            if (cap > 0.0 && v > cap) v = cap;
+            fin[s] = v; fout[s] = v;
+        }
+        double xin[CL_SRG_MAX_WIDTH], y[CL_SRG_MAX_WIDTH];
+        for (int i = 0; i < net->widths[0]; ++i) {
+            int kind = g->in_kind[i], idx = g->in_index[i];
+            xin[i] = kind == CL_SRG_IN_FIN ? fin[idx] : kind == CL_SRG_IN_CONC ? conc[idx] : b;
+        }
+        orc_surrogate_forward(net, xin, y, 1);
+        double mu = 0.0;
+        for (int q = 0; q < net->widths[net->n_layers]; ++q) {
+            if (g->out_kind[q] == CL_SRG_OUT_GROWTH) mu = y[q];
+            else fout[g->out_index[q]] = y[q];
+        }
+        if (mu < 1e-8 || !isfinite(mu)) mu = 0.0;
+        double dB = (fabs(mu) < THRD) ? -g->kd * b * cfg->dt : mu * b * cfg->dt / 3600.0;
+        if (dB + b < 0.0) dB = -b;
+        if (fabs(dB) > THRD) DB[g->microbe] += dB;
+        for (int s = 0; s < S; ++s) draw[s] += -fout[s] * b * g->mw * cfg->dt / 3.6e6;
+    }
+    for (int s = 0; s < S; ++s) {
+        double d = draw[s];
+        if (fabs(d) <= THRD) continue;
+        if (d + conc[s] < 0.0) d = -conc[s];
+        if (d > 0.0) d = 0.0;
+        if (fabs(d) > THRD) D[s] += d;
+    }
 }
 
 /* Speciation --------------------------------------------------------------- */
@@ -502,6 +585,183 @@ void orc_eq_batch(const cl_eq_system* sys, const double* totals, const double* c
     }
 }
 
+/* ---- per-voxel reaction processors (shared by both pass structures) ---- */
+typedef struct {
+    const cl_config* cfg;
+    orc_state* st;
+    int64_t N;
+    int any_bio, any_srg, any_abio;
+} rx_ctx;
+
+static double vox_dens(const rx_ctx* r, int s, int64_t n) {
+    const int64_t N = r->N;
+    if (r->cfg->immobile[s]) return r->st->imm[s*N + n];
+    const double* g = r->st->g;
+    return g[(s*7+0)*N+n] + g[(s*7+1)*N+n] + g[(s*7+2)*N+n] + g[(s*7+3)*N+n] +
+           g[(s*7+4)*N+n] + g[(s*7+5)*N+n] + g[(s*7+6)*N+n];
+}
+
+/* g_i += t_i * d (the reference's g[0] += d/4, g[1..6] += d/8) */
+static void vox_apply(const rx_ctx* r, int s, int64_t n, double d) {
+    const int64_t N = r->N;
+    if (r->cfg->immobile[s]) { r->st->imm[s*N + n] += d; return; }
+    for (int i = 0; i < 7; ++i) r->st->g[(s*7 + i)*N + n] += T7[i] * d;
+}
+
+/* run_kinetics (part1.hh:63-146) and run_surrogate3D deposit into the same
+ * dC/dB lattices, each contribution only above thrd; update_rxnLattices
+ * (:338-429) applies the sums above thrd */
+static void vox_kinetics(const rx_ctx* r, int64_t n) {
+    const cl_config* cfg = r->cfg;
+    const int S = cfg->n_solutes, M = cfg->n_microbes;
+    const int64_t N = r->N;
+    double C[CL_MAX_SOLUTES], Bm[CL_MAX_MICROBES], R[CL_MAX_SOLUTES], BR[CL_MAX_MICROBES];
+    double dC[CL_MAX_SOLUTES], dB[CL_MAX_MICROBES];
+    for (int s = 0; s < S; ++s) { double c = vox_dens(r, s, n); C[s] = c < THRD ? 0.0 : c; dC[s] = 0.0; }
+    for (int b = 0; b < M; ++b) { double v = r->st->bio[b*N + n]; Bm[b] = v < THRD ? 0.0 : v; dB[b] = 0.0; }
+    if (r->any_bio) {
+        orc_rates(cfg, 0, C, Bm, R, BR);
+        for (int s = 0; s < S; ++s) {
+            double d = R[s] * cfg->dt;
+            dC[s] = (d > THRD || d < -THRD) ? d : 0.0;
+        }
+        for (int b = 0; b < M; ++b) {
+            double d = BR[b] * cfg->dt;
+            dB[b] = (d > THRD || d < -THRD) ? d : 0.0;
+        }
+    }
+    if (r->any_srg) orc_surrogate_voxel(cfg, r->st->srg_nets, C, Bm, dC, dB);
+    for (int s = 0; s < S; ++s) if (dC[s] > THRD || dC[s] < -THRD) vox_apply(r, s, n, dC[s]);
+    for (int b = 0; b < M; ++b) if (dB[b] > THRD || dB[b] < -THRD) r->st->bio[b*N + n] += dB[b];
+}
+
+/* run_abiotic_kinetics (part1.hh:158-249) or surfaceAbioticKinetics3D
+ * (precipitationVOP.hh:53-145): the thresholded increments of one voxel
+ * (zero where the surface gate does not fire) */
+static void vox_abiotic(const rx_ctx* r, int x, int y, int z, int64_t n, double* dC) {
+    const cl_config* cfg = r->cfg;
+    const orc_state* st = r->st;
+    const int S = cfg->n_solutes;
+    for (int s = 0; s < S; ++s) dC[s] = 0.0;
+    int fire = 1;
+    if (cfg->precip_enabled && cfg->abiotic_surface_only) {
+        static const int d6[6][3] = {{1,0,0},{-1,0,0},{0,1,0},{0,-1,0},{0,0,1},{0,0,-1}};
+        fire = 0;
+        for (int d = 0; d < 6 && !fire; ++d) {
+            int xa = x + d6[d][0];
+            if (xa < 0 || xa > cfg->nx - 1) continue;
+            int nb = st->mask[site(cfg, xa, wrap(y + d6[d][1], cfg->ny), wrap(z + d6[d][2], cfg->nz))];
+            if (nb == cfg->solid_code || nb == cfg->bb_code) fire = 1;
+        }
+    }
+    if (!fire) return;
+    double C[CL_MAX_SOLUTES], R[CL_MAX_SOLUTES];
+    for (int s = 0; s < S; ++s) { double c = vox_dens(r, s, n); C[s] = c < THRD ? 0.0 : c; }
+    orc_rates(cfg, 1, C, NULL, R, NULL);
+    for (int s = 0; s < S; ++s) {
+        double d = R[s] * cfg->dt;
+        dC[s] = (d > THRD || d < -THRD) ? d : 0.0;
+    }
+}
+
+/* SolidPhase by id (DissolutionConfig::byId, dissolutionVOP.hh:176-180) */
+static const cl_phase* phase_by_id(const cl_config* cfg, int pid) {
+    for (int k = 0; k < cfg->n_phases; ++k) if (cfg->phases[k].id == pid) return &cfg->phases[k];
+    return NULL;
+}
+
+/* surfaceDissolutionKinetics3D (dissolutionVOP.hh:265-435) at one voxel:
+ * water = mean solute density over the open face neighbours (x in 1..nx-2,
+ * y/z inside the domain, not solid or bounce-back), the phase's rate law,
+ * at most half the mineral per step, the mineral decrement into the voxel's
+ * own dC and the products split evenly into the open neighbours' dC. */
+static void vox_dissolve(const rx_ctx* r, int x, int y, int z, double* dab) {
+    const cl_config* cfg = r->cfg;
+    const orc_state* st = r->st;
+    const int S = cfg->n_solutes, nx = cfg->nx, ny = cfg->ny, nz = cfg->nz;
+    const int64_t N = r->N, n = site(cfg, x, y, z);
+    const int pid = st->phase[n];
+    if (pid <= 0) return;
+    const cl_phase* ph = phase_by_id(cfg, pid);
+    if (!ph || ph->substrate < 0 || ph->substrate >= S) return;
+    const int sM = ph->substrate;
+    const double mineral = vox_dens(r, sM, n);
+    if (!(mineral > THRD)) return;
+    static const int d6[6][3] = {{1,0,0},{-1,0,0},{0,1,0},{0,-1,0},{0,0,1},{0,0,-1}};
+    int64_t open[6];
+    int nOpen = 0;
+    for (int d = 0; d < 6; ++d) {
+        int ax = x + d6[d][0], ay = y + d6[d][1], az = z + d6[d][2];
+        if (ax < 1 || ax > nx - 2 || ay < 0 || ay > ny - 1 || az < 0 || az > nz - 1) continue;
+        int64_t q = site(cfg, ax, ay, az);
+        int m = st->mask[q];
+        if (m == cfg->solid_code || m == cfg->bb_code) continue;
+        open[nOpen++] = q;
+    }
+    if (nOpen == 0 && cfg->dissol_surface_only) return;
+    double water[CL_MAX_SOLUTES];
+    for (int s = 0; s < S; ++s) water[s] = 0.0;
+    if (nOpen > 0) {
+        for (int k = 0; k < nOpen; ++k)
+            for (int s = 0; s < S; ++s) water[s] += vox_dens(r, s, open[k]);
+        for (int s = 0; s < S; ++s) water[s] /= (double)nOpen;
+    }
+    for (int s = 0; s < S; ++s) if (water[s] < 0.0) water[s] = 0.0;
+    /* defineDissolutionRate as a table: rate = k * mineral * prod water[mass_s] */
+    double rate = ph->k * (mineral > 0.0 ? mineral : 0.0);
+    for (int j = 0; j < ph->n_mass; ++j) rate *= water[ph->mass_s[j]];
+    double mineralR = -rate, subsR[CL_MAX_SOLUTES];
+    for (int s = 0; s < S; ++s) subsR[s] = ph->nu[s] * rate;
+    if (isnan(mineralR) || isinf(mineralR)) mineralR = 0.0;
+    for (int s = 0; s < S; ++s) if (isnan(subsR[s]) || isinf(subsR[s])) subsR[s] = 0.0;
+    if (!(mineralR < 0.0)) return;
+    double dM = mineralR * cfg->dt;
+    double scale = 1.0;
+    const double maxRemove = 0.5 * mineral;
+    if (-dM > maxRemove) scale = maxRemove / (-dM);
+    dM *= scale;
+    if (!(-dM > THRD)) return;
+    dab[sM*N + n] += dM;
+    if (nOpen > 0) {
+        for (int s = 0; s < S; ++s) {
+            if (s == sM) continue;
+            const double released = subsR[s] * cfg->dt * scale;
+            if (fabs(released) <= THRD) continue;
+            const double perFace = released / (double)nOpen;
+            for (int k = 0; k < nOpen; ++k) dab[s*N + open[k]] += perFace;
+        }
+    }
+}
+
+/* run_equilibrium_biotic (part4_eqsolver.hh:1355-1494), Newton solve;
+ * returns 1 if it did not converge */
+static int vox_equilibrium(const rx_ctx* r, int64_t n) {
+    const cl_config* cfg = r->cfg;
+    const int S = cfg->n_solutes;
+    const cl_eq_system* sys = &cfg->eq;
+    double conc[CL_MAX_SPECIES], T[CL_MAX_COMP], xx[CL_MAX_COMP], eqc[CL_MAX_SPECIES];
+    for (int s = 0; s < S; ++s) { double c = vox_dens(r, s, n); conc[s] = c > MIN_CONC ? c : MIN_CONC; }
+    orc_eq_totals(sys, conc, T);
+    orc_eq_cold_start(sys, conc, xx);
+    int conv = 0;
+    int it = orc_eq_newton(sys, T, xx, sys->max_iter, sys->tol, &conv);
+    if (r->st->eq_iters) r->st->eq_iters[n] = it;
+    if (!conv) return 1;
+    orc_eq_species(sys, xx, eqc);
+    for (int s = 0; s < S && s < sys->n_species; ++s) {
+        double e = eq_species_active(sys, s) ? eqc[s]
+                 : (conc[s] > MIN_CONC ? (conc[s] < MAX_CONC ? conc[s] : MAX_CONC) : MIN_CONC);
+        if (e > MAX_CONC) e = MAX_CONC;
+        if (e < MIN_CONC) e = MIN_CONC;
+        double d = e - conc[s];
+        double mx = 0.1 * fabs(conc[s]); if (mx < 1e-9) mx = 1e-9;
+        if (fabs(d) > mx) d = d > 0 ? mx : -mx;
+        if (conc[s] + d < 1e-20) d = 1e-20 - conc[s];
+        if (fabs(d) > THRD) vox_apply(r, s, n, d);
+    }
+    return 0;
+}
+
 /* One transport step in the order of src/complab.cpp:1252-1374,1849-1857:
  *   collide (mobile solutes; boundary cells complete their unknown population
  *   from the prescribed density first) -> run_kinetics -> update_rxnLattices ->
@@ -549,94 +809,86 @@ int64_t orc_transport_step(const cl_config* cfg, orc_state* st) {
                 }
             }
 
-    /* ---- reactions (per voxel; processors run over the whole lattice in turn,
-     *      and each one reads only its own voxel, so per-voxel order is exact) ---- */
+    /* ---- reactions ---- */
     int n_bio = 0, n_abio = 0;
     for (int k = 0; k < cfg->n_rxn; ++k) { if (cfg->rxn[k].microbe >= 0) ++n_bio; else ++n_abio; }
-    int any_bio = cfg->enable_kinetics && (n_bio > 0 || M > 0);
-    int any_abio = cfg->enable_abiotic && S > 0;
-    #pragma omp parallel for collapse(2) reduction(+:nonconv) schedule(dynamic, 4)
-    for (int x = 1; x < nx - 1; ++x)
-        for (int y = 0; y < ny; ++y)
-            for (int z = 0; z < nz; ++z) {
-                int64_t n = site(cfg, x, y, z);
-                int m = st->mask[n];
-                if (!is_reactive(cfg, x, m)) continue;
-                double C[CL_MAX_SOLUTES], Bm[CL_MAX_MICROBES], R[CL_MAX_SOLUTES], BR[CL_MAX_MICROBES];
-                double dC[CL_MAX_SOLUTES];
-                #define DENS(s) (cfg->immobile[s] ? st->imm[(s)*N + n] : \
-                    (g[((s)*7+0)*N+n]+g[((s)*7+1)*N+n]+g[((s)*7+2)*N+n]+g[((s)*7+3)*N+n]+ \
-                     g[((s)*7+4)*N+n]+g[((s)*7+5)*N+n]+g[((s)*7+6)*N+n]))
-                #define APPLY(s, d) do { if (cfg->immobile[s]) st->imm[(s)*N + n] += (d); \
-                    else for (int i_ = 0; i_ < 7; ++i_) g[((s)*7+i_)*N + n] += T7[i_]*(d); } while (0)
-                /* run_kinetics (part1.hh:63-146) + update_rxnLattices (:338-429) */
-                if (any_bio) {
-                    for (int s = 0; s < S; ++s) { double c = DENS(s); C[s] = c < THRD ? 0.0 : c; }
-                    for (int b = 0; b < M; ++b) { double v = st->bio[b*N + n]; Bm[b] = v < THRD ? 0.0 : v; }
-                    orc_rates(cfg, 0, C, Bm, R, BR);
+    rx_ctx rc;
+    rc.cfg = cfg; rc.st = st; rc.N = N;
+    rc.any_bio = cfg->enable_kinetics && (n_bio > 0 || M > 0);
+    rc.any_srg = cfg->n_srg > 0 && st->srg_nets;
+    rc.any_abio = cfg->enable_abiotic && S > 0 && n_abio > 0;
+    const int dissol = cfg->dissol_enabled && cfg->n_phases > 0 && st->phase;
+    if (!dissol) {
+        /* processors run over the whole lattice in turn, and each reads only
+         * its own voxel, so one pass per voxel is exact */
+        #pragma omp parallel for collapse(2) reduction(+:nonconv) schedule(dynamic, 4)
+        for (int x = 1; x < nx - 1; ++x)
+            for (int y = 0; y < ny; ++y)
+                for (int z = 0; z < nz; ++z) {
+                    int64_t n = site(cfg, x, y, z);
+                    if (!is_reactive(cfg, x, st->mask[n])) continue;
+                    double dC[CL_MAX_SOLUTES];
+                    if (rc.any_bio || rc.any_srg) vox_kinetics(&rc, n);
+                    if (rc.any_abio) {
+                        vox_abiotic(&rc, x, y, z, n, dC);
+                        for (int s = 0; s < S; ++s) if (dC[s] > THRD || dC[s] < -THRD) vox_apply(&rc, s, n, dC[s]);
+                    }
+                    if (cfg->use_equilibrium) nonconv += vox_equilibrium(&rc, n);
+                }
+    } else {
+        /* surfaceDissolutionKinetics3D writes the dC of face neighbours, so the
+         * processors run as separate whole-lattice passes, as the reference does */
+        #pragma omp parallel for collapse(2) schedule(dynamic, 4)
+        for (int x = 1; x < nx - 1; ++x)
+            for (int y = 0; y < ny; ++y)
+                for (int z = 0; z < nz; ++z) {
+                    int64_t n = site(cfg, x, y, z);
+                    if (!is_reactive(cfg, x, st->mask[n])) continue;
+                    if (rc.any_bio || rc.any_srg) vox_kinetics(&rc, n);
+                }
+        /* dC = dC0 (complab.cpp:1328 / :1359) */
+        double* dab = (double*)calloc((size_t)S * N, sizeof(double));
+        if (rc.any_abio) {
+            #pragma omp parallel for collapse(2) schedule(dynamic, 4)
+            for (int x = 1; x < nx - 1; ++x)
+                for (int y = 0; y < ny; ++y)
+                    for (int z = 0; z < nz; ++z) {
+                        int64_t n = site(cfg, x, y, z);
+                        if (!is_reactive(cfg, x, st->mask[n])) continue;
+                        double dC[CL_MAX_SOLUTES];
+                        vox_abiotic(&rc, x, y, z, n, dC);
+                        for (int s = 0; s < S; ++s) dab[s*N + n] = dC[s];
+                    }
+        }
+        /* the scatter into neighbours runs serially in the reference's voxel order */
+        for (int x = 1; x < nx - 1; ++x)
+            for (int y = 0; y < ny; ++y)
+                for (int z = 0; z < nz; ++z) vox_dissolve(&rc, x, y, z, dab);
+        /* update_abiotic_rxnLattices (part1.hh:258-336): interior x, not solid or
+         * bounce-back; with dissol_apply_at_walls the walls' mineral decrement too */
+        #pragma omp parallel for collapse(2) schedule(static)
+        for (int x = 1; x < nx - 1; ++x)
+            for (int y = 0; y < ny; ++y)
+                for (int z = 0; z < nz; ++z) {
+                    int64_t n = site(cfg, x, y, z);
+                    if (!is_reactive(cfg, x, st->mask[n]) && !cfg->dissol_apply_at_walls) continue;
                     for (int s = 0; s < S; ++s) {
-                        double d = R[s] * cfg->dt;
-                        dC[s] = (d > THRD || d < -THRD) ? d : 0.0;
-                    }
-                    for (int s = 0; s < S; ++s) if (dC[s] > THRD || dC[s] < -THRD) APPLY(s, dC[s]);
-                    for (int b = 0; b < M; ++b) {
-                        double d = BR[b] * cfg->dt;
-                        if (d > THRD || d < -THRD) st->bio[b*N + n] += d;
+                        double d = dab[s*N + n];
+                        if (d > THRD || d < -THRD) vox_apply(&rc, s, n, d);
                     }
                 }
-                /* dC = dC0; run_abiotic_kinetics (part1.hh:158-249) or
-                 * surfaceAbioticKinetics3D (precipitationVOP.hh:53-145);
-                 * update_abiotic_rxnLattices (part1.hh:258-336) */
-                if (any_abio && n_abio > 0) {
-                    int fire = 1;
-                    if (cfg->precip_enabled && cfg->abiotic_surface_only) {
-                        static const int d6[6][3] = {{1,0,0},{-1,0,0},{0,1,0},{0,-1,0},{0,0,1},{0,0,-1}};
-                        fire = 0;
-                        for (int d = 0; d < 6 && !fire; ++d) {
-                            int xa = x + d6[d][0];
-                            if (xa < 0 || xa > nx - 1) continue;
-                            int nb = st->mask[site(cfg, xa, wrap(y + d6[d][1], ny), wrap(z + d6[d][2], nz))];
-                            if (nb == cfg->solid_code || nb == cfg->bb_code) fire = 1;
-                        }
+        free(dab);
+        if (cfg->use_equilibrium) {
+            #pragma omp parallel for collapse(2) reduction(+:nonconv) schedule(dynamic, 4)
+            for (int x = 1; x < nx - 1; ++x)
+                for (int y = 0; y < ny; ++y)
+                    for (int z = 0; z < nz; ++z) {
+                        int64_t n = site(cfg, x, y, z);
+                        if (!is_reactive(cfg, x, st->mask[n])) continue;
+                        nonconv += vox_equilibrium(&rc, n);
                     }
-                    if (fire) {
-                        for (int s = 0; s < S; ++s) { double c = DENS(s); C[s] = c < THRD ? 0.0 : c; }
-                        orc_rates(cfg, 1, C, NULL, R, NULL);
-                        for (int s = 0; s < S; ++s) {
-                            double d = R[s] * cfg->dt;
-                            if (d > THRD || d < -THRD) APPLY(s, d);
-                        }
-                    }
-                }
-                /* run_equilibrium_biotic (part4_eqsolver.hh:1355-1494), Newton solve */
-                if (cfg->use_equilibrium) {
-                    const cl_eq_system* sys = &cfg->eq;
-                    double conc[CL_MAX_SPECIES], T[CL_MAX_COMP], xx[CL_MAX_COMP], eqc[CL_MAX_SPECIES];
-                    for (int s = 0; s < S; ++s) { double c = DENS(s); conc[s] = c > MIN_CONC ? c : MIN_CONC; }
-                    orc_eq_totals(sys, conc, T);
-                    orc_eq_cold_start(sys, conc, xx);
-                    int conv = 0;
-                    int it = orc_eq_newton(sys, T, xx, sys->max_iter, sys->tol, &conv);
-                    if (st->eq_iters) st->eq_iters[n] = it;
-                    if (!conv) { nonconv += 1; }
-                    else {
-                        orc_eq_species(sys, xx, eqc);
-                        for (int s = 0; s < S && s < sys->n_species; ++s) {
-                            double e = eq_species_active(sys, s) ? eqc[s]
-                                     : (conc[s] > MIN_CONC ? (conc[s] < MAX_CONC ? conc[s] : MAX_CONC) : MIN_CONC);
-                            if (e > MAX_CONC) e = MAX_CONC;
-                            if (e < MIN_CONC) e = MIN_CONC;
-                            double d = e - conc[s];
-                            double mx = 0.1 * fabs(conc[s]); if (mx < 1e-9) mx = 1e-9;
-                            if (fabs(d) > mx) d = d > 0 ? mx : -mx;
-                            if (conc[s] + d < 1e-20) d = 1e-20 - conc[s];
-                            if (fabs(d) > THRD) APPLY(s, d);
-                        }
-                    }
-                }
-                #undef DENS
-                #undef APPLY
-            }
+        }
+    }
 
     /* ---- stream (push, periodic y/z, reflect at x faces) ---- */
     for (int s = 0; s < S; ++s) {
@@ -684,6 +936,34 @@ int64_t orc_precip_convert(const cl_config* cfg, orc_state* st) {
         if (p >= cfg->max_precip_rho) {
             if (m != cfg->precip_code) ++changed;
             st->mask[n] = (uint8_t)cfg->precip_code;
+            /* stamp the precipitate phase so dissolution can find the voxel */
+            if (cfg->precip_phase_id > 0 && st->phase) st->phase[n] = (uint8_t)cfg->precip_phase_id;
+        }
+    }
+    return changed;
+}
+
+/* dissolNodeConversion3D (src/dissolutionVOP.hh:459-527): a phase voxel whose
+ * mineral fell below reopen_fraction * full_density becomes the first pore
+ * code (2 when none is declared) and loses its phase id. */
+int64_t orc_dissol_convert(const cl_config* cfg, orc_state* st) {
+    const int64_t N = (int64_t)cfg->nx * cfg->ny * cfg->nz;
+    const int pore = cfg->n_pore_codes > 0 ? cfg->pore_codes[0] : 2;
+    int64_t changed = 0;
+    if (!st->phase) return 0;
+    for (int64_t n = 0; n < N; ++n) {
+        const int pid = st->phase[n];
+        if (pid <= 0) continue;
+        const cl_phase* ph = phase_by_id(cfg, pid);
+        if (!ph || ph->substrate < 0 || ph->substrate >= cfg->n_solutes) continue;
+        if (!(ph->full_density > 0.0)) continue;
+        const int s = ph->substrate;
+        double mineral = cfg->immobile[s] ? st->imm[s*N + n] : 0.0;
+        if (!cfg->immobile[s]) for (int i = 0; i < 7; ++i) mineral += st->g[(s*7 + i)*N + n];
+        if (mineral < cfg->reopen_fraction * ph->full_density) {
+            if (st->mask[n] != pore) ++changed;
+            st->mask[n] = (uint8_t)pore;
+            st->phase[n] = 0;
         }
     }
     return changed;

@@ -37,6 +37,7 @@ extern "C" {
 #define ORC_FLUID 2   /* NS: IncBGK(omega); ADE: omega_pore */
 #define ORC_BIO   3   /* NS: IncBGK(omega_bio); ADE: omega_bio */
 
+int  orc_config_size(void);
 void orc_classes_from_mask(const cl_config* cfg, const uint8_t* mask,
                            uint8_t* ns_class, uint8_t* ade_class);
 
@@ -64,6 +65,8 @@ typedef struct {
     uint8_t* ade_class;/* [N] */
     double*  rho_bc;   /* [S][2][ny*nz] prescribed boundary density (0: x=0, 1: x=nx-1) */
     int32_t* eq_iters; /* [N] Newton iterations of the last equilibrium step (may be NULL) */
+    const cl_surrogate_net* srg_nets;  /* [CL_MAX_SRG_ORG] networks of the surrogate organisms (may be NULL) */
+    uint8_t* phase;    /* [N] dissolvable phase id, 0 = none (may be NULL without dissolution) */
 } orc_state;
 
 void orc_ade_init(const cl_config* cfg, orc_state* st);
@@ -76,8 +79,10 @@ void orc_solute_density(const cl_config* cfg, const orc_state* st, int s, double
 void orc_rates(const cl_config* cfg, int abiotic, const double* C, const double* B,
                double* subsR, double* bioR);
 
-/* geometry updates (precipNodeConversion3D); returns the number of changed sites */
+/* geometry updates (precipNodeConversion3D, dissolNodeConversion3D);
+ * return the number of sites whose mask changed */
 int64_t orc_precip_convert(const cl_config* cfg, orc_state* st);
+int64_t orc_dissol_convert(const cl_config* cfg, orc_state* st);
 
 /* ---- speciation ------------------------------------------------------------ */
 /* totals from species (calc_component_totals) */

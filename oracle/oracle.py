@@ -31,8 +31,9 @@ def _p(a):
 def lib():
     global _orc
     if _orc is None:
-        if not os.path.exists(LIB):
-            build()
+        # make is a no-op when liboracle.so is newer than its sources and the
+        # public header whose structs it reads
+        build()
         _orc = ctypes.CDLL(LIB)
         vp, d, i = ctypes.c_void_p, ctypes.c_double, ctypes.c_int
         _orc.orc_flow_step.restype = d
@@ -43,6 +44,8 @@ def lib():
         _orc.orc_transport_step.argtypes = [vp, vp]
         _orc.orc_precip_convert.restype = ctypes.c_int64
         _orc.orc_precip_convert.argtypes = [vp, vp]
+        _orc.orc_dissol_convert.restype = ctypes.c_int64
+        _orc.orc_dissol_convert.argtypes = [vp, vp]
         _orc.orc_eq_newton.restype = i
         _orc.orc_eq_newton.argtypes = [vp, vp, vp, i, d, vp]
         _orc.orc_eq_residual.restype = d
@@ -69,7 +72,17 @@ def ref_lib():
 class OrcState(ctypes.Structure):
     _fields_ = [("g", ctypes.c_void_p), ("g_tmp", ctypes.c_void_p), ("imm", ctypes.c_void_p),
                 ("bio", ctypes.c_void_p), ("u", ctypes.c_void_p), ("mask", ctypes.c_void_p),
-                ("ade_class", ctypes.c_void_p), ("rho_bc", ctypes.c_void_p), ("eq_iters", ctypes.c_void_p)]
+                ("ade_class", ctypes.c_void_p), ("rho_bc", ctypes.c_void_p), ("eq_iters", ctypes.c_void_p),
+                ("srg_nets", ctypes.c_void_p), ("phase", ctypes.c_void_p)]
+
+
+def check_config_layout(cfg):
+    """The oracle reads cl_config through the public header: its sizeof must
+    match the ctypes mirror, or every field after the change is misread."""
+    got = lib().orc_config_size()
+    if got != ctypes.sizeof(cfg):
+        raise RuntimeError("liboracle.so was built against another cl_config (%d vs %d bytes): rebuild it"
+                           % (got, ctypes.sizeof(cfg)))
 
 
 def classes(cfg, mask):
@@ -84,6 +97,7 @@ class Flow:
     """FP64 flow lattice (deviation populations, natural order)."""
 
     def __init__(self, cfg, mask):
+        check_config_layout(cfg)
         self.cfg = cfg
         self.N = cfg.nx * cfg.ny * cfg.nz
         self.mask = np.ascontiguousarray(mask, np.uint8).reshape(-1)
@@ -115,6 +129,7 @@ class Transport:
     """FP64 solute lattices stepped in the reference's processor order."""
 
     def __init__(self, cfg, mask, u=None):
+        check_config_layout(cfg)
         self.cfg = cfg
         N = self.N = cfg.nx * cfg.ny * cfg.nz
         S, M = cfg.n_solutes, max(cfg.n_microbes, 1)
@@ -127,9 +142,11 @@ class Transport:
         self.u = np.zeros(3 * N) if u is None else np.ascontiguousarray(u, np.float64).reshape(-1).copy()
         self.rho_bc = np.zeros(S * 2 * cfg.ny * cfg.nz)
         self.eq_iters = np.zeros(N, np.int32)
+        self.phase = np.zeros(N, np.uint8)
         self.st = OrcState(_p(self.g).value, _p(self.g_tmp).value, _p(self.imm).value, _p(self.bio).value,
                            _p(self.u).value, _p(self.mask).value, _p(self.ade).value, _p(self.rho_bc).value,
-                           _p(self.eq_iters).value)
+                           _p(self.eq_iters).value, None, _p(self.phase).value)
+        self._nets = None
         lib().orc_ade_init(ctypes.byref(cfg), ctypes.byref(self.st))
 
     def step(self, n=1):
@@ -152,6 +169,12 @@ class Transport:
             for i in range(7):
                 self.g[(s * 7 + i) * self.N:(s * 7 + i + 1) * self.N] = t[i] * v
 
+    def set_surrogates(self, nets):
+        """Networks of the surrogate organisms (a sequence of SurrogateNet, one per slot)."""
+        arr = (type(nets[0]) * len(nets))(*nets)
+        self._nets = arr
+        self.st.srg_nets = ctypes.addressof(arr)
+
     def set_biomass(self, m, values):
         self.bio[m * self.N:(m + 1) * self.N] = np.asarray(values, np.float64).reshape(-1)
 
@@ -160,6 +183,9 @@ class Transport:
 
     def precip_convert(self):
         return lib().orc_precip_convert(ctypes.byref(self.cfg), ctypes.byref(self.st))
+
+    def dissol_convert(self):
+        return lib().orc_dissol_convert(ctypes.byref(self.cfg), ctypes.byref(self.st))
 
 
 def eq_batch(sys, totals, cold_species, x0=None, start=0):

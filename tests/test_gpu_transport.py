@@ -181,3 +181,63 @@ def test_equilibrium_in_transport_carbonate(gpu_lib, pkg, wl):
         co = ref.density(s)
         assert rel_l2(cg, co) < 1e-4, s
     lat.close()
+
+
+def test_coupled_warm_previous_matches_cold(gpu_lib, pkg, wl):
+    """The coupled chemistry with Newton started from each voxel's previous
+    solution gives the same fields as the reference's cold start (both stop
+    at the 1e-10 relative residual) and needs fewer iterations."""
+    mask = wl.sphere_pack(24, 16, 16, 0.5, 2.0, 4.0, seed=17)
+    nx, ny, nz = mask.shape
+    bio = wl.seed_biomass(mask, 3, frac=0.2)
+    out = {}
+    for warm in (False, True):
+        cfg = wl.coupled_config(pkg, nx, ny, nz, warm_previous=warm)
+        lat = pkg.Lattice(cfg)
+        lat.upload_mask(mask)
+        lat.flow_init()
+        lat.flow_steps(50)
+        lat.couple_velocity()
+        lat.ade_init()
+        lat.set_field(pkg.FIELD_BIOMASS, 0, bio)
+        st = lat.step(30)
+        assert st == pkg.OK
+        it = lat.field(pkg.FIELD_EQ_ITERS).reshape(-1)[(mask == 2).reshape(-1)]
+        out[warm] = ([lat.field(pkg.FIELD_CONC, s).reshape(-1) for s in range(cfg.n_solutes)], it.mean())
+        lat.close()
+    for s in range(len(out[False][0])):
+        assert rel_l2(out[True][0][s], out[False][0][s]) < 1e-6, s
+    assert out[True][1] < out[False][1]
+
+
+def test_surrogate_reaction_type(gpu_lib, pkg, wl):
+    """Two surrogate organisms (3->20->20->4 networks) on sessile biomass feed
+    six transported solutes; the fused step against the FP64 oracle (the
+    network runs in FP32 on the GPU)."""
+    mask = wl.sphere_pack(22, 14, 14, 0.5, 2.0, 3.0, seed=23)
+    nx, ny, nz = mask.shape
+    cfg = wl.surrogate_config(pkg, nx, ny, nz)
+    nets = wl.surrogate_nets(pkg)
+    rng = np.random.default_rng(8)
+    b0 = wl.seed_biomass(mask, 4, frac=0.3, lo=0.005, hi=0.05)
+    b1 = wl.seed_biomass(mask, 5, frac=0.3, lo=0.005, hi=0.05)
+    lat, u = flow_field(pkg, cfg, mask, steps=100)
+    for slot in range(2):
+        lat.set_surrogate(slot, nets[slot])
+    lat.ade_init()
+    lat.set_field(pkg.FIELD_BIOMASS, 0, b0)
+    lat.set_field(pkg.FIELD_BIOMASS, 1, b1)
+    ref = o.Transport(cfg, mask, u=u)
+    ref.set_surrogates(nets)
+    ref.set_biomass(0, b0)
+    ref.set_biomass(1, b1)
+    for n in (1, 4, 20):
+        lat.step(n)
+        ref.step(n)
+    for s in range(6):
+        assert rel_l2(lat.field(pkg.FIELD_CONC, s).reshape(-1), ref.density(s)) < 1e-4, s
+    for m in range(2):
+        bg, bo = lat.field(pkg.FIELD_BIOMASS, m).reshape(-1), ref.biomass(m)
+        assert rel_l2(bg, bo) < 1e-5, m
+        assert not np.allclose(bo, (b0, b1)[m].reshape(-1))      # the organisms did something
+    lat.close()
