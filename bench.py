@@ -258,6 +258,31 @@ def speciation_bench(pkg, wl, stream, n_train=1 << 20, n_test=1 << 21):
         res[name] = {"ms": ms, "solves_per_s": n_test / (ms * 1e-3), "mean_iters": float(I.float().mean().item()),
                      "converged": float((st <= 1).mean()), "fell_back": float((st == 1).mean()),
                      "x": X, "ok": St <= 1}
+    # where the learned time goes: the network alone, and Newton from its
+    # start and from the converged roots (the cost floor of one check)
+    def timed(fn, reps=3):
+        ts = []
+        for _ in range(reps):
+            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            s0.record()
+            fn()
+            s1.record()
+            torch.cuda.synchronize()
+            ts.append(s0.elapsed_time(s1))
+        return min(ts)
+    Xp = torch.zeros((n_test, 5), **f64)
+    X = torch.zeros((n_test, 5), **f64)
+    I = torch.zeros(n_test, dtype=torch.int32, device=dev)
+    St = torch.zeros(n_test, dtype=torch.uint8, device=dev)
+    res["breakdown_ms"] = {"network": timed(lambda: eq.predict_device(eT.data_ptr(), Xp.data_ptr(), n_test))}
+    for name, start_x in (("newton_from_network", Xp), ("newton_from_root", res["cold"]["x"])):
+        def run(start_x=start_x):
+            X.copy_(start_x)
+            eq.solve_device(eT.data_ptr(), eC.data_ptr(), X.data_ptr(), I.data_ptr(), St.data_ptr(), n_test,
+                            pkg.EQ_START_GIVEN)
+        res["breakdown_ms"][name] = timed(run)
+        res["breakdown_ms"][name + "_mean_iters"] = float(I.float().mean().item())
     # same roots and residuals where both converged
     from_cold, from_learned = res["cold"].pop("x"), res["learned"].pop("x")
     both = res["cold"].pop("ok") & res["learned"].pop("ok")
@@ -329,10 +354,12 @@ def main():
     l0 = lat.launch_count()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push("timed")       # lets a profiler select the timed launches
     e0.record()
     for i in range(args.steps):
         coupled_step(lat, args.warmup + i)
     e1.record()
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     launches = lat.launch_count() - l0

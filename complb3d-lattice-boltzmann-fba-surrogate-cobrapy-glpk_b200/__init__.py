@@ -390,6 +390,7 @@ def _bind_eq(lib):
         ("cl_eq_grad_host", [vp, vp, vp, c_int32, P(ctypes.c_float), vp]),
         ("cl_eq_param_count", [vp, P(c_int32)]), ("cl_eq_get_params", [vp, vp]),
         ("cl_eq_set_params", [vp, vp]), ("cl_eq_predict_host", [vp, vp, vp, c_int32]),
+        ("cl_eq_predict_device", [vp, vp, vp, c_int64]),
         ("cl_surrogate_batch_device", [P(SurrogateNet), vp, vp, c_int64, c_int32, vp]),
         ("cl_surrogate_batch_host", [P(SurrogateNet), vp, vp, c_int64, c_int32]),
     ]:
@@ -444,6 +445,10 @@ class EqSolver:
         """Device-pointer variant (ints from torch.Tensor.data_ptr())."""
         return _check(self.lib, self.lib.cl_eq_solve_device(self.h, d_totals, d_cold, d_x, d_iters, d_status, n,
                                                             start), "cl_eq_solve_device")
+
+    def predict_device(self, d_totals, d_x, n):
+        """The network's Newton start for n device totals (device pointers)."""
+        return _check(self.lib, self.lib.cl_eq_predict_device(self.h, d_totals, d_x, n), "cl_eq_predict_device")
 
     def train_device(self, d_totals, d_logfree, n, epochs=10, batch=1024, lr=2e-3, seed=0):
         loss = ctypes.c_float(0)

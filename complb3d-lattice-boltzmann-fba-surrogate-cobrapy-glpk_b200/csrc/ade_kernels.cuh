@@ -91,9 +91,10 @@ __device__ __forceinline__ void collide7(float* f, float om, float ux, float uy,
 }
 
 // Table-driven rate law (defineRxnKinetics / defineAbioticRxnKinetics ABI).
-// C, R, B, BR are shared-memory columns with stride bd.  Concentrations below
-// thrd read as zero, as the processors floor them before the call.
-static __device__ void rates_dev(const AdeParams& p, int abiotic, const double* C, const double* B,
+// C is a column with stride cs; R, B, BR columns with stride bd.
+// Concentrations below thrd read as zero, as the processors floor them
+// before the call.
+static __device__ void rates_dev(const AdeParams& p, int abiotic, const double* C, int cs, const double* B,
                           double* R, double* BR, int bd) {
     for (int s = 0; s < p.S; ++s) R[s * bd] = 0.0;
     if (!abiotic) for (int m = 0; m < p.M; ++m) BR[m * bd] = 0.0;
@@ -107,12 +108,12 @@ static __device__ void rates_dev(const AdeParams& p, int abiotic, const double* 
             rate *= b;
         }
         for (int j = 0; j < r.n_monod; ++j) {
-            const double c0 = C[r.monod_s[j] * bd];
+            const double c0 = C[r.monod_s[j] * cs];
             const double c = c0 < THRD ? 0.0 : c0;
             rate *= c / (r.monod_ks[j] + c);
         }
         for (int j = 0; j < r.n_mass; ++j) {
-            const double c0 = C[r.mass_s[j] * bd];
+            const double c0 = C[r.mass_s[j] * cs];
             rate *= c0 < THRD ? 0.0 : c0;
         }
         for (int s = 0; s < p.S; ++s) R[s * bd] = fma(r.nu[s], rate, R[s * bd]);
@@ -129,14 +130,14 @@ static __device__ void rates_dev(const AdeParams& p, int abiotic, const double* 
 // kinetics read (before update_rxnLattices), adds its thresholded increments
 // into D (solutes) and DB (biomass), which the caller applies together with
 // the kinetics increments, as the shared dC/dB lattices of the reference do.
-static __device__ __noinline__ void surrogate_chain(const AdeParams& p, const double* Cur, const double* B,
+static __device__ __noinline__ void surrogate_chain(const AdeParams& p, const double* Cur, int cs, const double* B,
                                              double* D, double* DB, int bd) {
     double conc[CL_MAX_SOLUTES], draw[CL_MAX_SOLUTES];
     bool any = false;
     for (int o = 0; o < p.n_srg; ++o) any = any || B[p.srg[o].microbe * bd] > THRD;
     if (!any) return;
     for (int s = 0; s < p.S; ++s) {
-        const double c = Cur[s * bd];
+        const double c = Cur[s * cs];
         conc[s] = c > THRD ? c : 0.0;
         draw[s] = 0.0;
     }
@@ -207,10 +208,11 @@ static __device__ __noinline__ void surrogate_chain(const AdeParams& p, const do
 // dC/dB lattices, each contribution only if above thrd: the increments of one
 // voxel into R (solutes) and BR (biomass), B its floored biomass.  Not applied.
 __device__ __forceinline__ void kinetics_increments(const AdeParams& p, const double* bio, int64_t N, int64_t n,
-                                                    const double* Cur, double* R, double* B, double* BR, int bd) {
+                                                    const double* Cur, int cs, double* R, double* B, double* BR,
+                                                    int bd) {
     for (int m = 0; m < p.M; ++m) { const double b = bio[m * N + n]; B[m * bd] = b < THRD ? 0.0 : b; }
     if (p.do_kin) {
-        rates_dev(p, 0, Cur, B, R, BR, bd);
+        rates_dev(p, 0, Cur, cs, B, R, BR, bd);
         for (int s = 0; s < p.S; ++s) {
             const double d = R[s * bd] * p.dt;
             R[s * bd] = (d > THRD || d < -THRD) ? d : 0.0;
@@ -223,7 +225,7 @@ __device__ __forceinline__ void kinetics_increments(const AdeParams& p, const do
         for (int s = 0; s < p.S; ++s) R[s * bd] = 0.0;
         for (int m = 0; m < p.M; ++m) BR[m * bd] = 0.0;
     }
-    if (p.n_srg > 0) surrogate_chain(p, Cur, B, R, BR, bd);
+    if (p.n_srg > 0) surrogate_chain(p, Cur, cs, B, R, BR, bd);
 }
 
 // The dissolution increments that reach voxel n (surfaceDissolutionKinetics3D,
@@ -255,17 +257,17 @@ __device__ __forceinline__ void dissol_gather(const AdeK& k, int64_t n, int x, i
 // solute.  Returns 1 if the equilibrium solve did not converge.
 template <int NC>
 __device__ int reaction_chain(const AdeK& k, int64_t n, int x, int y, int z, uint8_t cls, double* Cur, double* App,
-                              double* R, double* B, double* BR, int bd) {
+                              int cs, double* R, double* B, double* BR, int bd) {
     const AdeParams& p = k.p;
     const int64_t N = k.g.N;
     int nonconv = 0;
     // kinetics and surrogate increments; update_rxnLattices (:338-429) applies
     // the sums that exceed thrd
     if (p.do_kin || p.n_srg > 0) {
-        kinetics_increments(p, k.bio, N, n, Cur, R, B, BR, bd);
+        kinetics_increments(p, k.bio, N, n, Cur, cs, R, B, BR, bd);
         for (int s = 0; s < p.S; ++s) {
             const double d = R[s * bd];
-            if (d > THRD || d < -THRD) { Cur[s * bd] += d; App[s * bd] += d; }
+            if (d > THRD || d < -THRD) { Cur[s * cs] += d; App[s * cs] += d; }
         }
         for (int m = 0; m < p.M; ++m) {
             const double d = BR[m * bd];
@@ -279,7 +281,7 @@ __device__ int reaction_chain(const AdeK& k, int64_t n, int x, int y, int z, uin
     const bool dis = p.do_dissol && (cls & (F_PHASE_NBR | F_PHASE_SELF));
     if (abio || dis) {
         if (abio) {
-            rates_dev(p, 1, Cur, nullptr, R, nullptr, bd);
+            rates_dev(p, 1, Cur, cs, nullptr, R, nullptr, bd);
             for (int s = 0; s < p.S; ++s) {
                 const double d = R[s * bd] * p.dt;
                 R[s * bd] = (d > THRD || d < -THRD) ? d : 0.0;
@@ -290,7 +292,7 @@ __device__ int reaction_chain(const AdeK& k, int64_t n, int x, int y, int z, uin
         if (dis) dissol_gather(k, n, x, y, z, cls, R, bd);
         for (int s = 0; s < p.S; ++s) {
             const double d = R[s * bd];
-            if (d > THRD || d < -THRD) { Cur[s * bd] += d; App[s * bd] += d; }
+            if (d > THRD || d < -THRD) { Cur[s * cs] += d; App[s * cs] += d; }
         }
     }
     // run_equilibrium_biotic (part4_eqsolver.hh:1355-1494): species floored at
@@ -302,7 +304,7 @@ __device__ int reaction_chain(const AdeK& k, int64_t n, int x, int y, int z, uin
         for (int j = 0; j < NC; ++j) T[j] = 0.0;
         for (int i = 0; i < e.ns; ++i) {
             if (!e.active[i]) continue;
-            const double c = fmin(fmax(Cur[i * bd], 1e-30), 10.0);
+            const double c = fmin(fmax(Cur[i * cs], 1e-30), 10.0);
 #pragma unroll
             for (int j = 0; j < NC; ++j) T[j] = fma(e.stoich[i][j], c, T[j]);
         }
@@ -311,7 +313,7 @@ __device__ int reaction_chain(const AdeK& k, int64_t n, int x, int y, int z, uin
             for (int j = 0; j < NC; ++j) {
                 double c = 1e-7;
                 const int idx = e.comp_species[j];
-                if (idx >= 0) c = Cur[idx * bd];
+                if (idx >= 0) c = Cur[idx * cs];
                 xs[j] = log10(fmin(fmax(c, 1e-30), 10.0));
             }
         };
@@ -324,12 +326,12 @@ __device__ int reaction_chain(const AdeK& k, int64_t n, int x, int y, int z, uin
 #pragma unroll
             for (int j = 0; j < NC; ++j) { x[j] = k.eq_x[(int64_t)j * N + n]; warm = warm && (x[j] == x[j]); }
         }
-        if (warm) {
-            it = eq_newton<NC>(e, T, x, p.eq.warm_iter, p.eq.tol, &conv);
-            if (!conv) { cold(x); int it2 = eq_newton<NC>(e, T, x, p.eq.max_iter, p.eq.tol, &conv); it += it2; }
-        } else {
-            cold(x);
-            it = eq_newton<NC>(e, T, x, p.eq.max_iter, p.eq.tol, &conv);
+        // the warm attempt (previous solution, warm_iter iterations), then the
+        // cold start; one call site keeps one copy of the solver in the kernel
+        for (int phase = warm ? 0 : 1; phase < 2; ++phase) {
+            if (phase == 1) cold(x);
+            it += eq_newton<NC>(e, T, x, phase == 0 ? p.eq.warm_iter : p.eq.max_iter, p.eq.tol, &conv);
+            if (conv) break;
         }
         if (k.eq_x && conv) {
 #pragma unroll
@@ -339,116 +341,203 @@ __device__ int reaction_chain(const AdeK& k, int64_t n, int x, int y, int z, uin
         if (!conv) nonconv = 1;
         else {
             for (int s = 0; s < p.S && s < e.ns; ++s) {
-                const double conc = fmax(Cur[s * bd], 1e-30);
+                const double conc = fmax(Cur[s * cs], 1e-30);
                 double eqc = e.active[s] ? species_c<NC>(e, s, x) : fmin(conc, 10.0);
                 eqc = fmin(fmax(eqc, 1e-30), 10.0);
                 double d = eqc - conc;
                 const double mx = fmax(1e-9, 0.1 * fabs(conc));
                 if (fabs(d) > mx) d = d > 0 ? mx : -mx;
                 if (conc + d < 1e-20) d = 1e-20 - conc;
-                if (fabs(d) > THRD) { Cur[s * bd] += d; App[s * bd] += d; }
+                if (fabs(d) > THRD) { Cur[s * cs] += d; App[s * cs] += d; }
             }
         }
     }
     return nonconv;
 }
 
+// A tile of kTile = 2 x kBlock sites of whole z-rows is one block iteration;
+// each thread owns two sites of it.  Only the reactive sites (about the
+// porosity's share) run the reaction chain, so after pass 1 the block
+// compacts them into a list and its threads work through that list, each on
+// the shared-memory columns of the site it took and on its own scratch
+// columns: the FP64 chain then runs on full warps, and a tile of two sites
+// per thread keeps about two thirds of the block busy in it.
+constexpr int kBlock = 256;
+constexpr int kSitesPerThread = 2;
+constexpr int kTile = kBlock * kSitesPerThread;
+
+// virtual thread v of a tile -> (row offset, z, stride) as RowMap does for threads
+struct TileMap {
+    int rpb, zstep;
+    __device__ __forceinline__ void at(int nz, int v, int& lrow, int& z0, bool& active) const {
+        if (nz >= kTile) { lrow = 0; z0 = v; active = true; }
+        else { lrow = v / nz; z0 = v - lrow * nz; active = lrow < rpb; }
+    }
+};
+
+__device__ __forceinline__ TileMap make_tilemap(int nz) {
+    TileMap m;
+    if (nz >= kTile) { m.rpb = 1; m.zstep = kTile; }
+    else { m.rpb = kTile / nz; m.zstep = nz; }
+    return m;
+}
+
 template <int NMOB, int NC, int PARITY>
-__global__ void __launch_bounds__(256, 2) ade_main_kernel(const __grid_constant__ AdeK k) {
+__global__ void __launch_bounds__(kBlock, 2) ade_main_kernel(const __grid_constant__ AdeK k) {
     extern __shared__ double sm[];
-    const int bd = blockDim.x;
+    __shared__ uint32_t s_n[kTile];        // site of each tile column
+    __shared__ int s_xyz[kTile][3];
+    __shared__ uint8_t s_cls[kTile];
+    __shared__ short s_list[kTile];        // compacted reactive columns
+    __shared__ int s_count;
+    const int t = threadIdx.x;
     const AdeParams& p = k.p;
-    double* Cur = sm + threadIdx.x;
-    double* App = Cur + p.S * bd;
-    double* R   = App + p.S * bd;
-    double* B   = R + p.S * bd;
-    double* BR  = B + (p.M > 0 ? p.M : 1) * bd;
+    const int Mw = p.M > 0 ? p.M : 1;
+    double* CurT = sm;                       // [S][kTile] densities of the tile's sites
+    double* AppT = CurT + p.S * kTile;       // [S][kTile] their total increments
+    double* Rw = AppT + p.S * kTile;         // [S][kBlock] per-thread scratch
+    double* Bw = Rw + p.S * kBlock;          // [M][kBlock]
+    double* BRw = Bw + Mw * kBlock;          // [M][kBlock]
     const int64_t N = k.g.N, plane = k.g.plane;
     const uint32_t N32 = (uint32_t)N;
     const bool any_rxn = p.do_kin || p.do_abio || p.n_srg > 0 || p.do_dissol || NC > 0;
     unsigned long long nonconv = 0;
-    const RowMap rm = make_rowmap(k.g.nz);
+    const TileMap tm = make_tilemap(k.g.nz);
     const int row_lo = k.g.ny, row_hi = (k.g.nx - 1) * k.g.ny;     // interior x = 1 .. nx-2
-    for (int row0 = row_lo + blockIdx.x * rm.rpb; row0 < row_hi; row0 += gridDim.x * rm.rpb) {
-      const int row = row0 + rm.lrow;
-      if (!rm.active || row >= row_hi) continue;
-      const int x = row / k.g.ny, y = row - x * k.g.ny;
-      for (int z = rm.z0; z < k.g.nz; z += rm.zstep) {
-        const uint32_t n = (uint32_t)row * (uint32_t)k.g.nz + (uint32_t)z;
-        const uint8_t cls = k.cls[n];
-        const uint8_t dyn = cls & 3;
-        if (dyn == BB) continue;
-        if (dyn == NODYN && !k.nodyn_coupled) continue;
-        const Site st = make_site(k.g, x, y, z, n);
-        float dC[NMOB];
+    // every thread of a block runs the same iterations (the barriers below)
+    for (int row0 = row_lo + blockIdx.x * tm.rpb; row0 < row_hi; row0 += gridDim.x * tm.rpb) {
+      for (int zb = 0; zb < k.g.nz; zb += tm.zstep) {
+        // the tile's sites: live (streams) and reactive masks, site data in shared memory
+        unsigned lvm = 0, rcm = 0;
 #pragma unroll
-        for (int m = 0; m < NMOB; ++m) dC[m] = 0.f;
-        // the processors test the mask, not the dynamics: a NoDynamics site
-        // whose mask reopened to pore reacts too
-        if ((cls & F_REACTIVE) && any_rxn) {
+        for (int j = 0; j < kSitesPerThread; ++j) {
+            const int v = t + j * kBlock;
+            int lrow, z0; bool act;
+            tm.at(k.g.nz, v, lrow, z0, act);
+            const int row = row0 + lrow, z = zb + z0;
+            if (!(act && row < row_hi && z < k.g.nz)) continue;
+            const int x = row / k.g.ny, y = row - x * k.g.ny;
+            const uint32_t n = (uint32_t)row * (uint32_t)k.g.nz + (uint32_t)z;
+            const uint8_t cls = k.cls[n];
+            const uint8_t dyn = cls & 3;
+            // bounce-back sites are a no-op of the AA step, unless their mask
+            // reopened to pore: then they react (the processors test the mask)
+            if ((dyn == BB && !(cls & F_REACTIVE)) || (dyn == NODYN && !k.nodyn_coupled)) continue;
+            lvm |= 1u << j;
+            // the processors test the mask, not the dynamics: a NoDynamics
+            // site whose mask reopened to pore reacts too
+            if (any_rxn && (cls & F_REACTIVE)) rcm |= 1u << j;
+            s_n[v] = n; s_xyz[v][0] = x; s_xyz[v][1] = y; s_xyz[v][2] = z; s_cls[v] = cls;
+        }
+        if (any_rxn) {
             // pass 1: the populations of a group of solutes in flight at once, then the densities
-            for (int s = 0; s < p.S; ++s) App[s * bd] = 0.0;
+#pragma unroll 1
+            for (int j = 0; j < kSitesPerThread; ++j) {
+                if (!((rcm >> j) & 1u)) continue;
+                const int v = t + j * kBlock;
+                const uint32_t n = s_n[v];
+                const Site st = make_site(k.g, s_xyz[v][0], s_xyz[v][1], s_xyz[v][2], n);
+                for (int s = 0; s < p.S; ++s) AppT[s * kTile + v] = 0.0;
 #pragma unroll
-            for (int m0 = 0; m0 < NMOB; m0 += kGroup) {
-                float f[kGroup][7];
+                for (int m0 = 0; m0 < NMOB; m0 += kGroup) {
+                    float f[kGroup][7];
 #pragma unroll
-                for (int j = 0; j < kGroup; ++j)
-                    if (m0 + j < NMOB) gather7<PARITY>(k.pop + (int64_t)(m0 + j) * 7 * N, N32, st, f[j]);
+                    for (int q = 0; q < kGroup; ++q)
+                        if (m0 + q < NMOB) gather7<PARITY>(k.pop + (int64_t)(m0 + q) * 7 * N, N32, st, f[q]);
 #pragma unroll
-                for (int j = 0; j < kGroup; ++j) {
-                    if (m0 + j >= NMOB) continue;
-                    float r = 0.f;
+                    for (int q = 0; q < kGroup; ++q) {
+                        if (m0 + q >= NMOB) continue;
+                        float r = 0.f;
 #pragma unroll
-                    for (int i = 0; i < 7; ++i) r += f[j][i];
-                    Cur[p.mob_index[m0 + j] * bd] = (double)r;
+                        for (int i = 0; i < 7; ++i) r += f[q][i];
+                        CurT[p.mob_index[m0 + q] * kTile + v] = (double)r;
+                    }
                 }
+                for (int s = 0; s < p.S; ++s)
+                    if (p.mob_slot[s] < 0) CurT[s * kTile + v] = k.imm[(int64_t)s * N + n];
             }
-            for (int s = 0; s < p.S; ++s)
-                if (p.mob_slot[s] < 0) Cur[s * bd] = k.imm[(int64_t)s * N + n];
-            nonconv += reaction_chain<NC>(k, n, x, y, z, cls, Cur, App, R, B, BR, bd);
+            if (t == 0) s_count = 0;
+            __syncthreads();
+            // compact the reactive columns (warp-aggregated slots)
 #pragma unroll
-            for (int m = 0; m < NMOB; ++m) dC[m] = (float)App[p.mob_index[m] * bd];
-            for (int s = 0; s < p.S; ++s)
-                if (p.mob_slot[s] < 0 && App[s * bd] != 0.0) k.imm[(int64_t)s * N + n] += App[s * bd];
+            for (int j = 0; j < kSitesPerThread; ++j) {
+                const bool rc = (rcm >> j) & 1u;
+                const unsigned ball = __ballot_sync(0xffffffffu, rc);
+                int base = 0;
+                if ((t & 31) == 0 && ball) base = atomicAdd(&s_count, __popc(ball));
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if (rc) s_list[base + __popc(ball & ((1u << (t & 31)) - 1u))] = (short)(t + j * kBlock);
+            }
+            __syncthreads();
+            const int cnt = s_count;
+            for (int r = t; r < cnt; r += kBlock) {
+                const int c = s_list[r];
+                double* cCur = CurT + c;
+                double* cApp = AppT + c;
+                const uint32_t cn = s_n[c];
+                nonconv += reaction_chain<NC>(k, cn, s_xyz[c][0], s_xyz[c][1], s_xyz[c][2], s_cls[c],
+                                              cCur, cApp, kTile, Rw + t, Bw + t, BRw + t, kBlock);
+                for (int s = 0; s < p.S; ++s)
+                    if (p.mob_slot[s] < 0 && cApp[s * kTile] != 0.0) k.imm[(int64_t)s * N + cn] += cApp[s * kTile];
+            }
+            __syncthreads();
         }
         // keep the second gather after the chain: hoisting it would hold all
         // populations in registers across the Newton solve
         asm volatile("" ::: "memory");
         // pass 2: gather every solute (L1/L2 hits after pass 1), collide, add t_i*dC, stream
-        const float ux = k.u[n], uy = k.u[N + n], uz = k.u[2 * N + n];
-        const bool adj = (x == 1 || x == k.g.nx - 2);
+#pragma unroll 1
+        for (int j = 0; j < kSitesPerThread; ++j) {
+            if (!((lvm >> j) & 1u)) continue;
+            const int v = t + j * kBlock;
+            const bool rc = (rcm >> j) & 1u;
+            const uint32_t n = s_n[v];
+            const int x = s_xyz[v][0];
+            const uint8_t dyn = s_cls[v] & 3;
+            const Site st = make_site(k.g, x, s_xyz[v][1], s_xyz[v][2], n);
+            const float ux = k.u[n], uy = k.u[N + n], uz = k.u[2 * N + n];
+            const bool adj = (x == 1 || x == k.g.nx - 2);
 #pragma unroll
-        for (int m0 = 0; m0 < NMOB; m0 += kGroup) {
-            float f[kGroup][7];
+            for (int m0 = 0; m0 < NMOB; m0 += kGroup) {
+                float f[kGroup][7];
 #pragma unroll
-            for (int j = 0; j < kGroup; ++j)
-                if (m0 + j < NMOB) gather7<PARITY>(k.pop + (int64_t)(m0 + j) * 7 * N, N32, st, f[j]);
+                for (int q = 0; q < kGroup; ++q)
+                    if (m0 + q < NMOB) gather7<PARITY>(k.pop + (int64_t)(m0 + q) * 7 * N, N32, st, f[q]);
 #pragma unroll
-            for (int j = 0; j < kGroup; ++j) {
-                const int m = m0 + j;
-                if (m >= NMOB) continue;
-                float rho = 0.f;
-                if (dyn != NODYN) {
-                    const float om = (dyn == BIO) ? p.omega_bio[m] : p.omega_pore[m];
-                    collide7(f[j], om, ux, uy, uz, rho);
-                } else if (adj) {
+                for (int q = 0; q < kGroup; ++q) {
+                    const int m = m0 + q;
+                    if (m >= NMOB) continue;
+                    float rho = 0.f;
+                    if (dyn == BB) {
+                        // BounceBack's collision swaps opposite populations; in the
+                        // AA layout swap + scatter leaves every slot as it was, so
+                        // only the reaction increment moves anything
 #pragma unroll
-                    for (int i = 0; i < 7; ++i) rho += f[j][i];
+                        for (int i = 1; i < 4; ++i) { const float tmp = f[q][i]; f[q][i] = f[q][i + 3]; f[q][i + 3] = tmp; }
+                    } else if (dyn != NODYN) {
+                        const float om = (dyn == BIO) ? p.omega_bio[m] : p.omega_pore[m];
+                        collide7(f[q], om, ux, uy, uz, rho);
+                    } else if (adj) {
+#pragma unroll
+                        for (int i = 0; i < 7; ++i) rho += f[q][i];
+                    }
+                    const float d = rc ? (float)AppT[p.mob_index[m] * kTile + v] : 0.f;
+                    if (d != 0.f) {
+#pragma unroll
+                        for (int i = 0; i < 7; ++i) f[q][i] += t7(i) * d;
+                    }
+                    if (adj && dyn != BB) {
+                        const int side = (x == 1) ? 0 : 1;
+                        k.rho_adj[((int64_t)m * 2 + side) * plane + (n - (int64_t)x * plane)] = rho;
+                    }
                 }
-                const float d = dC[m];
-                if (d != 0.f) {
 #pragma unroll
-                    for (int i = 0; i < 7; ++i) f[j][i] += t7(i) * d;
-                }
-                if (adj) {
-                    const int side = (x == 1) ? 0 : 1;
-                    k.rho_adj[((int64_t)m * 2 + side) * plane + (n - (int64_t)x * plane)] = rho;
-                }
+                for (int q = 0; q < kGroup; ++q)
+                    if (m0 + q < NMOB) scatter7<PARITY>(k.pop + (int64_t)(m0 + q) * 7 * N, N32, st, f[q]);
             }
-#pragma unroll
-            for (int j = 0; j < kGroup; ++j)
-                if (m0 + j < NMOB) scatter7<PARITY>(k.pop + (int64_t)(m0 + j) * 7 * N, N32, st, f[j]);
         }
+        // no barrier needed before the next tile: after the chain's barrier
+        // every thread reads only its own columns
       }
     }
     if (nonconv) atomicAdd(&k.counters[0], nonconv);
@@ -522,10 +611,10 @@ int dissol_release(Ctx* c, const AdeK& k);
 
 template <int NMOB, int NC>
 inline int launch_step(Ctx* c, const AdeK& k) {
-    const int bd = 256;
+    const int bd = kBlock;
     const int S = c->ap.S, M = c->ap.M > 0 ? c->ap.M : 1;
     const bool any_rxn = c->ap.do_kin || c->ap.do_abio || c->ap.n_srg > 0 || c->ap.do_dissol || NC > 0;
-    const size_t smem = any_rxn ? (size_t)(3 * S + 2 * M) * bd * sizeof(double) : 0;
+    const size_t smem = any_rxn ? ((size_t)2 * S * kTile + (size_t)(S + 2 * M) * kBlock) * sizeof(double) : 0;
     const int64_t interior = c->geo.N - 2 * c->geo.plane;
     const int blocks = grid_for(interior, bd, 148 * 8);
     int r = CL_OK;

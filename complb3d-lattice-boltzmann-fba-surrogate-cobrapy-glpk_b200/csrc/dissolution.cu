@@ -44,7 +44,7 @@ __device__ __forceinline__ void post_kinetics(const AdeK& k, int x, int y, int z
     voxel_densities<NMOB, PARITY>(k, x, y, z, n, C);
     if (p.do_kin || p.n_srg > 0) {
         double R[CL_MAX_SOLUTES], B[CL_MAX_MICROBES], BR[CL_MAX_MICROBES];
-        kinetics_increments(p, k.bio, k.g.N, n, C, R, B, BR, 1);
+        kinetics_increments(p, k.bio, k.g.N, n, C, 1, R, B, BR, 1);
         for (int s = 0; s < p.S; ++s) {
             const double d = R[s];
             if (d > THRD || d < -THRD) C[s] += d;

@@ -106,14 +106,18 @@ __global__ void flags_kernel(ClassK k) {
 // Counts that steer the step kernels: BGK flow sites (energy average) and
 // whether any NoDynamics site is linked to a dynamic site (otherwise NoDynamics
 // regions are sealed behind bounce-back and need no streaming at all).  A
-// NoDynamics solute site whose mask reopened to pore reacts, so it counts as
-// linked too.
+// NoDynamics or bounce-back solute site whose mask reopened to pore reacts,
+// and what it adds reaches NoDynamics neighbours too, so it counts as a link.
 __global__ void class_counts_kernel(ClassK k) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     unsigned long long nb = 0, cf = 0, ca = 0;
     for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < k.g.N; n += stride) {
         const uint8_t ns = k.ns[n], ad = k.ade[n] & 3;
         if (ns == FLUID || ns == BIO) ++nb;
+        // a wall-class solute site whose mask reopened reacts, and its
+        // increments stream into NoDynamics neighbours as well
+        const bool reopened = (ad == NODYN || ad == BB) && (k.ade[n] & F_REACTIVE);
+        if (reopened) ++ca;
         if (ns != NODYN && ad != NODYN) continue;
         int x, y, z;
         decode(k.g, n, x, y, z);
@@ -125,8 +129,7 @@ __global__ void class_counts_kernel(ClassK k) {
                 if (c == FLUID || c == BIO) { ++cf; break; }
             }
         }
-        if (ad == NODYN && (k.ade[n] & F_REACTIVE)) ++ca;
-        else if (ad == NODYN) {
+        if (ad == NODYN && !reopened) {
             for (int i = 1; i < 7; ++i) {
                 const int64_t q = nbr(k.g, n, x, y, z, c7x(i), c7y(i), c7z(i));
                 if (q < 0) continue;

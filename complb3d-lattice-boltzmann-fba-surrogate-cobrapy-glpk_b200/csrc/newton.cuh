@@ -15,7 +15,9 @@
 //   - convergence: relative mass-balance residual max_j |F_j| / sum_i |S_ij| c_i <= tol;
 //   - species at a clamp bound contribute nothing to J;
 //   - the step is scaled so that no component moves more than 2 decades;
-//   - the Armijo merit is ||F_j / sum_i |S_ij| c_i||_2 with the current weights.
+//   - the Armijo merit is ||F_j / sum_i |S_ij| c_i||_2 with the current weights;
+//   - a solve whose 40 backtracking trials all fail stops (the next iterate
+//     would be the same point to ~1e-12 of a step).
 // Species are evaluated on the fly (no per-species storage), the component
 // count NC is a template parameter so every array lives in registers.
 #pragma once
@@ -143,10 +145,166 @@ __device__ __forceinline__ void eq_cold_start(const EqDev& e, const double* spec
 
 // Runs at most max_iter Newton iterations from x.  Returns the iterations
 // taken; *conv = 1 when the residual test passed.
+// F = S^T c - T, sc = |S|^T c and the lower triangle of S^T diag(c) S
+// (clamped species excluded) in one pass over the species
 template <int NC>
-__device__ int eq_newton(const EqDev& e, const double* T, double* x, int max_iter, double tol, int* conv) {
+__device__ __forceinline__ void eq_eval_full(const EqDev& e, const double* T, const double* x,
+                                             double* F, double* sc, double (*J)[NC]) {
+#pragma unroll
+    for (int a = 0; a < NC; ++a) {
+        F[a] = -T[a]; sc[a] = 0.0;
+#pragma unroll
+        for (int b = 0; b < NC; ++b) J[a][b] = 0.0;
+    }
+    Powers<NC> pw;
+    pw.set(x);
+    for (int i = 0; i < e.ns; ++i) {
+        if (!e.active[i]) continue;
+        bool clamped;
+        const double c = species_eval<NC>(e, i, x, pw, clamped);
+        const double cj = clamped ? 0.0 : c;
+#pragma unroll
+        for (int a = 0; a < NC; ++a) {
+            const double sa = e.stoich[i][a];
+            F[a] = fma(sa, c, F[a]);
+            sc[a] = fma(e.absS[i][a], c, sc[a]);
+            const double sac = sa * cj;
+#pragma unroll
+            for (int b = 0; b <= a; ++b) J[a][b] = fma(sac, e.stoich[i][b], J[a][b]);
+        }
+    }
+}
+
+// Newton in log10 free components.  The first line-search trial (the full
+// step) is evaluated with the Jacobian, which becomes the next iteration's
+// when the full step is accepted (the usual case near the root); after a
+// shorter step the point is evaluated again.  The iterates are the same as
+// evaluating residual and Jacobian afresh at every iterate.  Returns the
+// number of steps taken; *conv = 1 at the relative residual tolerance.
+template <int NC>
+__device__ int eq_newton_reuse(const EqDev& e, const double* T, double* x, int max_iter, double tol, int* conv,
+                               int* stopped) {
     const double ln10 = 2.302585092994046;
     *conv = 0;
+    double F[NC], sc[NC], J[NC][NC];
+    eq_eval_full<NC>(e, T, x, F, sc, J);
+    for (int it = 0; it < max_iter; ++it) {
+        double rel = 0.0, fn = 0.0, w[NC];
+#pragma unroll
+        for (int a = 0; a < NC; ++a) {
+            w[a] = 1.0 / fmax(sc[a], 1e-300);
+            const double r = fabs(F[a]) * w[a];
+            rel = (r > rel || r != r) ? r : rel;
+            fn = fma(r, r, fn);
+        }
+        if (rel <= tol) { *conv = 1; return it; }
+        if (!(rel < 1e300)) { if (stopped) *stopped = 1; return it; }      // NaN / inf
+        fn = sqrt(fn);
+        // Cholesky of ln10*J (lower triangle), solve L L^T d = -F
+        double L[NC][NC];
+        bool ok = true;
+#pragma unroll
+        for (int a = 0; a < NC; ++a) {
+#pragma unroll
+            for (int b = 0; b <= a; ++b) {
+                double s = ln10 * J[a][b];
+#pragma unroll
+                for (int k = 0; k < b; ++k) s -= L[a][k] * L[b][k];
+                if (a == b) {
+                    if (!(s > 1e-300)) { ok = false; s = 1.0; }
+                    L[a][a] = sqrt(s);
+                } else {
+                    L[a][b] = s / L[b][b];
+                }
+            }
+        }
+        if (!ok) { if (stopped) *stopped = 1; return it + 1; }
+        double d[NC];
+#pragma unroll
+        for (int a = 0; a < NC; ++a) {
+            double s = -F[a];
+#pragma unroll
+            for (int k = 0; k < a; ++k) s -= L[a][k] * d[k];
+            d[a] = s / L[a][a];
+        }
+#pragma unroll
+        for (int a = NC - 1; a >= 0; --a) {
+            double s = d[a];
+#pragma unroll
+            for (int k = a + 1; k < NC; ++k) s -= L[k][a] * d[k];
+            d[a] = s / L[a][a];
+        }
+        // step cap (2 decades), then Armijo backtracking on the weighted residual
+        double dmax = 0.0;
+#pragma unroll
+        for (int a = 0; a < NC; ++a) dmax = fmax(dmax, fabs(d[a]));
+        if (dmax > 2.0) {
+            const double sfac = 2.0 / dmax;
+#pragma unroll
+            for (int a = 0; a < NC; ++a) d[a] *= sfac;
+        }
+        double xt[NC], Ft[NC], sct[NC];
+#pragma unroll
+        for (int a = 0; a < NC; ++a) xt[a] = fmin(fmax(d[a] + x[a], -30.0), 1.0);
+        eq_eval_full<NC>(e, T, xt, Ft, sct, J);      // J is free once L is formed
+        double fnt = 0.0;
+#pragma unroll
+        for (int a = 0; a < NC; ++a) { const double r = Ft[a] * w[a]; fnt = fma(r, r, fnt); }
+        fnt = sqrt(fnt);
+        if (fnt < fn * (1.0 - 1e-4)) {
+#pragma unroll
+            for (int a = 0; a < NC; ++a) { x[a] = xt[a]; F[a] = Ft[a]; sc[a] = sct[a]; }
+            continue;
+        }
+        double alpha = 0.5;
+        bool accepted = false;
+        for (int ls = 1; ls < 40; ++ls) {
+#pragma unroll
+            for (int a = 0; a < NC; ++a) xt[a] = fmin(fmax(fma(alpha, d[a], x[a]), -30.0), 1.0);
+            eq_residual<NC>(e, T, xt, Ft);
+            fnt = 0.0;
+#pragma unroll
+            for (int a = 0; a < NC; ++a) { const double r = Ft[a] * w[a]; fnt = fma(r, r, fnt); }
+            fnt = sqrt(fnt);
+            if (fnt < fn * (1.0 - 1e-4 * alpha)) { accepted = true; break; }
+            if (alpha < 1e-15) break;
+            alpha *= 0.5;
+        }
+#pragma unroll
+        for (int a = 0; a < NC; ++a) x[a] = xt[a];
+        eq_eval_full<NC>(e, T, x, F, sc, J);
+        if (!accepted) {
+            // every trial failed: the next iterate is this point to ~1e-12 of
+            // a step and fails the same way, so the solve stops here
+            double rel2 = 0.0;
+#pragma unroll
+            for (int a = 0; a < NC; ++a) {
+                const double r = fabs(F[a]) / fmax(sc[a], 1e-300);
+                rel2 = (r > rel2 || r != r) ? r : rel2;
+            }
+            if (rel2 <= tol) *conv = 1;
+            if (stopped) *stopped = 1;
+            return it + 1;
+        }
+    }
+    double rel = 0.0;
+#pragma unroll
+    for (int a = 0; a < NC; ++a) {
+        const double r = fabs(F[a]) / fmax(sc[a], 1e-300);
+        rel = (r > rel || r != r) ? r : rel;
+    }
+    if (rel <= tol) *conv = 1;
+    return max_iter;
+}
+
+// The same iteration with residual and Jacobian evaluated afresh at every
+// iterate (fewer live registers; used above three components).
+template <int NC>
+__device__ int eq_newton_plain(const EqDev& e, const double* T, double* x, int max_iter, double tol, int* conv,
+                               int* stopped) {
+    const double ln10 = 2.302585092994046;
+    *conv = 0;
+    bool stuck = false;
     for (int it = 0; it < max_iter; ++it) {
         // residual and Jacobian in one pass over the species
         double F[NC], sc[NC], J[NC][NC];
@@ -182,7 +340,7 @@ __device__ int eq_newton(const EqDev& e, const double* T, double* x, int max_ite
             fn = fma(r, r, fn);
         }
         if (rel <= tol) { *conv = 1; return it; }
-        if (!(rel < 1e300)) return it;       // NaN / inf
+        if (!(rel < 1e300) || stuck) { if (stopped) *stopped = 1; return it; }      // NaN / inf, or stuck
         fn = sqrt(fn);
         // Cholesky of ln10*J (lower triangle), solve L L^T d = -F
         double L[NC][NC];
@@ -202,7 +360,7 @@ __device__ int eq_newton(const EqDev& e, const double* T, double* x, int max_ite
                 }
             }
         }
-        if (!ok) return it + 1;
+        if (!ok) { if (stopped) *stopped = 1; return it + 1; }
         double d[NC];
 #pragma unroll
         for (int a = 0; a < NC; ++a) {
@@ -228,6 +386,7 @@ __device__ int eq_newton(const EqDev& e, const double* T, double* x, int max_ite
             for (int a = 0; a < NC; ++a) d[a] *= sfac;
         }
         double alpha = 1.0, xt[NC];
+        bool accepted = false;
         for (int ls = 0; ls < 40; ++ls) {
 #pragma unroll
             for (int a = 0; a < NC; ++a) xt[a] = fmin(fmax(fma(alpha, d[a], x[a]), -30.0), 1.0);
@@ -237,15 +396,168 @@ __device__ int eq_newton(const EqDev& e, const double* T, double* x, int max_ite
 #pragma unroll
             for (int a = 0; a < NC; ++a) { const double r = Ft[a] * w[a]; fnt = fma(r, r, fnt); }
             fnt = sqrt(fnt);
-            if (fnt < fn * (1.0 - 1e-4 * alpha) || alpha < 1e-15) break;
+            if (fnt < fn * (1.0 - 1e-4 * alpha)) { accepted = true; break; }
+            if (alpha < 1e-15) break;
             alpha *= 0.5;
         }
 #pragma unroll
         for (int a = 0; a < NC; ++a) x[a] = xt[a];
+        // every trial failed: the next iterate is this point to ~1e-12 of a
+        // step and fails the same way, so the solve stops after the
+        // convergence test at this point
+        stuck = !accepted;
     }
     double Fe[NC];
     if (eq_residual<NC>(e, T, x, Fe) <= tol) *conv = 1;
+    else if (stuck && stopped) *stopped = 1;
     return max_iter;
+}
+
+// The same Newton solve run by a whole warp on one system: every lane holds
+// the same iterate and does the same arithmetic, except that the
+// backtracking trials of an iteration are spread over the lanes.  Iterates,
+// counts and results are those of eq_newton_plain; an iteration that needs
+// many trials costs one or two residual evaluations of latency instead of
+// up to forty.  For the few slow solves that set the time of the last passes.
+template <int NC>
+__device__ int eq_newton_warp(const EqDev& e, const double* T, double* x, int max_iter, double tol, int* conv,
+                               int* stopped) {
+    const double ln10 = 2.302585092994046;
+    *conv = 0;
+    bool stuck = false;
+    for (int it = 0; it < max_iter; ++it) {
+        // residual and Jacobian in one pass over the species
+        double F[NC], sc[NC], J[NC][NC];
+#pragma unroll
+        for (int a = 0; a < NC; ++a) {
+            F[a] = -T[a]; sc[a] = 0.0;
+#pragma unroll
+            for (int b = 0; b < NC; ++b) J[a][b] = 0.0;
+        }
+        Powers<NC> pw;
+        pw.set(x);
+        for (int i = 0; i < e.ns; ++i) {
+            if (!e.active[i]) continue;
+            bool clamped;
+            const double c = species_eval<NC>(e, i, x, pw, clamped);
+            const double cj = clamped ? 0.0 : c;
+#pragma unroll
+            for (int a = 0; a < NC; ++a) {
+                const double sa = e.stoich[i][a];
+                F[a] = fma(sa, c, F[a]);
+                sc[a] = fma(e.absS[i][a], c, sc[a]);
+                const double sac = sa * cj;
+#pragma unroll
+                for (int b = 0; b <= a; ++b) J[a][b] = fma(sac, e.stoich[i][b], J[a][b]);
+            }
+        }
+        double rel = 0.0, fn = 0.0, w[NC];
+#pragma unroll
+        for (int a = 0; a < NC; ++a) {
+            w[a] = 1.0 / fmax(sc[a], 1e-300);
+            const double r = fabs(F[a]) * w[a];
+            rel = (r > rel || r != r) ? r : rel;
+            fn = fma(r, r, fn);
+        }
+        if (rel <= tol) { *conv = 1; return it; }
+        if (!(rel < 1e300) || stuck) { if (stopped) *stopped = 1; return it; }      // NaN / inf, or stuck
+        fn = sqrt(fn);
+        // Cholesky of ln10*J (lower triangle), solve L L^T d = -F
+        double L[NC][NC];
+        bool ok = true;
+#pragma unroll
+        for (int a = 0; a < NC; ++a) {
+#pragma unroll
+            for (int b = 0; b <= a; ++b) {
+                double s = ln10 * J[a][b];
+#pragma unroll
+                for (int k = 0; k < b; ++k) s -= L[a][k] * L[b][k];
+                if (a == b) {
+                    if (!(s > 1e-300)) { ok = false; s = 1.0; }
+                    L[a][a] = sqrt(s);
+                } else {
+                    L[a][b] = s / L[b][b];
+                }
+            }
+        }
+        if (!ok) { if (stopped) *stopped = 1; return it + 1; }
+        double d[NC];
+#pragma unroll
+        for (int a = 0; a < NC; ++a) {
+            double s = -F[a];
+#pragma unroll
+            for (int k = 0; k < a; ++k) s -= L[a][k] * d[k];
+            d[a] = s / L[a][a];
+        }
+#pragma unroll
+        for (int a = NC - 1; a >= 0; --a) {
+            double s = d[a];
+#pragma unroll
+            for (int k = a + 1; k < NC; ++k) s -= L[k][a] * d[k];
+            d[a] = s / L[a][a];
+        }
+        // step cap (2 decades), then Armijo backtracking on the weighted residual
+        double dmax = 0.0;
+#pragma unroll
+        for (int a = 0; a < NC; ++a) dmax = fmax(dmax, fabs(d[a]));
+        if (dmax > 2.0) {
+            const double sfac = 2.0 / dmax;
+#pragma unroll
+            for (int a = 0; a < NC; ++a) d[a] *= sfac;
+        }
+        // the backtracking trials alpha = 2^-k, k = 0..39, one per lane, 32 at
+        // a time; the first k that passes is the one the serial search takes
+        const int lane = threadIdx.x & 31;
+        double xt[NC];
+        bool accepted = false;
+        for (int base = 0; base < 40; base += 32) {
+            const int kk = base + lane;
+            double xk[NC];
+#pragma unroll
+            for (int a = 0; a < NC; ++a) xk[a] = x[a];
+            bool pass = false;
+            if (kk < 40) {
+                const double alpha = ldexp(1.0, -kk);
+#pragma unroll
+                for (int a = 0; a < NC; ++a) xk[a] = fmin(fmax(fma(alpha, d[a], x[a]), -30.0), 1.0);
+                double Ft[NC];
+                eq_residual<NC>(e, T, xk, Ft);
+                double fnt = 0.0;
+#pragma unroll
+                for (int a = 0; a < NC; ++a) { const double r = Ft[a] * w[a]; fnt = fma(r, r, fnt); }
+                fnt = sqrt(fnt);
+                pass = fnt < fn * (1.0 - 1e-4 * alpha);
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, pass);
+            const int src = bal ? __ffs(bal) - 1 : 39 - base;     // else the last trial (k = 39)
+#pragma unroll
+            for (int a = 0; a < NC; ++a) xt[a] = __shfl_sync(0xffffffffu, xk[a], src);
+            if (bal) { accepted = true; break; }
+        }
+#pragma unroll
+        for (int a = 0; a < NC; ++a) x[a] = xt[a];
+        // every trial failed: the next iterate is this point to ~1e-12 of a
+        // step and fails the same way, so the solve stops after the
+        // convergence test at this point
+        stuck = !accepted;
+    }
+    double Fe[NC];
+    if (eq_residual<NC>(e, T, x, Fe) <= tol) *conv = 1;
+    else if (stuck && stopped) *stopped = 1;
+    return max_iter;
+}
+
+// Both variants take the same iterates; above three components the second
+// set of residual registers of the reuse variant costs more occupancy than
+// the evaluation it saves.
+// *stopped (optional) is set when the solve ended before max_iter without
+// converging (NaN, singular Jacobian, or every backtracking trial failed):
+// continuing from x would repeat the same failure.
+template <int NC>
+__device__ __forceinline__ int eq_newton(const EqDev& e, const double* T, double* x, int max_iter, double tol,
+                                         int* conv, int* stopped = nullptr) {
+    if constexpr (NC <= 3) return eq_newton_reuse<NC>(e, T, x, max_iter, tol, conv, stopped);
+    else return eq_newton_plain<NC>(e, T, x, max_iter, tol, conv, stopped);
 }
 
 // component totals (calc_component_totals, part4_eqsolver.hh:520-538)

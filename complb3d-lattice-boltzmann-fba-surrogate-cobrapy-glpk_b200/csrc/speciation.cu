@@ -384,16 +384,28 @@ __global__ void newton_fallback_kernel(EqDev e, const double* totals, const doub
 // reference's cold start (mode 1) or the given start (mode 2); converged voxels
 // get status `ok_status`, the others are appended to `out_list` for the next
 // pass, or get status 2 when this is the last pass.  Newton keeps no state
-// besides x, so a solve split over passes is the same solve.
+// besides x, so a solve split over passes is the same solve; a solve that
+// stopped early (stop_mark) is carried through the remaining passes of its
+// phase without running, as the unsplit solve would have ended there.
+// lists at most this long are solved one warp per system (newton_pass_warp_kernel)
+constexpr int64_t kWarpPassMax = 4096;
+
 template <int NC>
-__global__ void newton_pass_kernel(EqDev e, const double* totals, const double* cold_species, double* logfree,
+__global__ void __launch_bounds__(128, 4) newton_pass_kernel(EqDev e, const double* totals, const double* cold_species, double* logfree,
                                    int32_t* iters, uint8_t* status, const int64_t* in_list,
                                    const unsigned long long* in_count, int64_t n, int mode, int budget, double tol,
-                                   int ok_status, int last, int64_t* out_list, unsigned long long* out_count) {
+                                   int ok_status, int last, int64_t* out_list, unsigned long long* out_count,
+                                   uint8_t* stop_mark) {
     const int64_t cnt = in_list ? (int64_t)*in_count : n;
+    if (cnt <= kWarpPassMax) return;           // the warp-per-solve pass takes short lists
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < cnt; q += stride) {
         const int64_t k = in_list ? in_list[q] : q;
+        if (mode == 0 && stop_mark[k]) {
+            if (last) { if (status) status[k] = 2; }
+            else out_list[atomicAdd(out_count, 1ull)] = k;
+            continue;
+        }
         double T[NC], x[NC];
 #pragma unroll
         for (int j = 0; j < NC; ++j) T[j] = totals[k * NC + j];
@@ -402,10 +414,52 @@ __global__ void newton_pass_kernel(EqDev e, const double* totals, const double* 
 #pragma unroll
             for (int j = 0; j < NC; ++j) x[j] = logfree[k * NC + j];
         }
-        int conv = 0;
-        const int it = eq_newton<NC>(e, T, x, budget, tol, &conv);
+        int conv = 0, stopped = 0;
+        const int it = eq_newton<NC>(e, T, x, budget, tol, &conv, &stopped);
 #pragma unroll
         for (int j = 0; j < NC; ++j) logfree[k * NC + j] = x[j];
+        stop_mark[k] = (uint8_t)(stopped && !conv);
+        if (iters) iters[k] = (mode == 0 ? iters[k] : (mode == 1 && in_list ? iters[k] : 0)) + it;
+        if (conv) { if (status) status[k] = (uint8_t)ok_status; }
+        else if (last) { if (status) status[k] = 2; }
+        else out_list[atomicAdd(out_count, 1ull)] = k;
+    }
+}
+
+template <int NC>
+__global__ void newton_pass_warp_kernel(EqDev e, const double* totals, const double* cold_species, double* logfree,
+                                   int32_t* iters, uint8_t* status, const int64_t* in_list,
+                                   const unsigned long long* in_count, int64_t n, int mode, int budget, double tol,
+                                   int ok_status, int last, int64_t* out_list, unsigned long long* out_count,
+                                   uint8_t* stop_mark) {
+    const int64_t cnt = in_list ? (int64_t)*in_count : n;
+    if (cnt > kWarpPassMax) return;            // long lists: newton_pass_kernel
+    const bool lead = (threadIdx.x & 31) == 0;
+    const int64_t stride = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t q = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < cnt; q += stride) {
+        const int64_t k = in_list ? in_list[q] : q;
+        if (mode == 0 && stop_mark[k]) {
+            if (lead) {
+                if (last) { if (status) status[k] = 2; }
+                else out_list[atomicAdd(out_count, 1ull)] = k;
+            }
+            continue;
+        }
+        double T[NC], x[NC];
+#pragma unroll
+        for (int j = 0; j < NC; ++j) T[j] = totals[k * NC + j];
+        if (mode == 1) eq_cold_start<NC>(e, cold_species + k * e.ns, x);
+        else {
+#pragma unroll
+            for (int j = 0; j < NC; ++j) x[j] = logfree[k * NC + j];
+        }
+        int conv = 0, stopped = 0;
+        const int it = eq_newton_warp<NC>(e, T, x, budget, tol, &conv, &stopped);
+        __syncwarp();                          // every lane has read iters[k] / stop_mark[k]
+        if (!lead) continue;
+#pragma unroll
+        for (int j = 0; j < NC; ++j) logfree[k * NC + j] = x[j];
+        stop_mark[k] = (uint8_t)(stopped && !conv);
         if (iters) iters[k] = (mode == 0 ? iters[k] : (mode == 1 && in_list ? iters[k] : 0)) + it;
         if (conv) { if (status) status[k] = (uint8_t)ok_status; }
         else if (last) { if (status) status[k] = 2; }
@@ -433,6 +487,7 @@ struct cl_eq_solver {
     bool trained = false;
     int64_t* fail_list = nullptr;     // ping-pong lists of the bucketed solve
     int64_t* fail_list2 = nullptr;
+    uint8_t* stop_mark = nullptr;     // solves that stopped early in the current phase
     int64_t fail_cap = 0;
     unsigned long long* fail_count = nullptr;   // two counters
     uint64_t adam_t = 0;
@@ -444,9 +499,12 @@ static int eq_ensure_fail(cl_eq_solver* s, int64_t n) {
     if (s->fail_cap >= n) return CL_OK;
     if (s->fail_list) cudaFree(s->fail_list);
     if (s->fail_list2) cudaFree(s->fail_list2);
+    if (s->stop_mark) cudaFree(s->stop_mark);
     s->fail_list = s->fail_list2 = nullptr;
+    s->stop_mark = nullptr;
     CL_CUDA(cudaMalloc(&s->fail_list, sizeof(int64_t) * (size_t)std::max<int64_t>(n, 1)));
     CL_CUDA(cudaMalloc(&s->fail_list2, sizeof(int64_t) * (size_t)std::max<int64_t>(n, 1)));
+    CL_CUDA(cudaMalloc(&s->stop_mark, (size_t)std::max<int64_t>(n, 1)));
     s->fail_cap = n;
     return CL_OK;
 }
@@ -475,10 +533,19 @@ static int bucketed_solve(cl_eq_solver* s, const double* T, const double* cold, 
     auto pass = [&](int mode, int budget, int ok_status, bool last) -> int {
         const int out = (cur == 0) ? 1 : 0;
         CL_CUDA(cudaMemsetAsync(cnt[out], 0, sizeof(unsigned long long), s->stream));
-        newton_pass_kernel<NC><<<blocks, 128, 0, s->stream>>>(
-            s->e, T, cold, x, it, st, cur < 0 ? nullptr : lists[cur], cur < 0 ? nullptr : cnt[cur], n, mode, budget,
-            s->sys.tol, ok_status, last ? 1 : 0, lists[out], cnt[out]);
-        CL_LAUNCH_CHECK("newton_pass_kernel");
+        // both kernels read the list length on the device and only one works
+        if (cur >= 0 || n > kWarpPassMax) {
+            newton_pass_kernel<NC><<<blocks, 128, 0, s->stream>>>(
+                s->e, T, cold, x, it, st, cur < 0 ? nullptr : lists[cur], cur < 0 ? nullptr : cnt[cur], n, mode,
+                budget, s->sys.tol, ok_status, last ? 1 : 0, lists[out], cnt[out], s->stop_mark);
+            CL_LAUNCH_CHECK("newton_pass_kernel");
+        }
+        if (cur >= 0 || n <= kWarpPassMax) {
+            newton_pass_warp_kernel<NC><<<(int)(kWarpPassMax * 32 / 128), 128, 0, s->stream>>>(
+                s->e, T, cold, x, it, st, cur < 0 ? nullptr : lists[cur], cur < 0 ? nullptr : cnt[cur], n, mode,
+                budget, s->sys.tol, ok_status, last ? 1 : 0, lists[out], cnt[out], s->stop_mark);
+            CL_LAUNCH_CHECK("newton_pass_warp_kernel");
+        }
         cur = out;
         return CL_OK;
     };
@@ -582,7 +649,7 @@ int cl_eq_destroy(cl_eq_solver* s) {
     if (!s) return CL_OK;
     if (s->stream) cudaStreamSynchronize(s->stream);
     void* ptrs[] = {s->w.W1, s->w.W2, s->w.W2T, s->w.W3, s->w.W3T, s->w.b, s->w.norm, s->master, s->m1, s->m2,
-                    s->part, s->grad, s->fail_list, s->fail_list2, s->fail_count};
+                    s->part, s->grad, s->fail_list, s->fail_list2, s->stop_mark, s->fail_count};
     for (void* p : ptrs) if (p) cudaFree(p);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     delete s;
@@ -629,6 +696,15 @@ int cl_eq_solve_device(cl_eq_solver* s, const double* d_totals, const double* d_
         case 4: return bucketed_solve<4>(s, d_totals, d_cold_species, d_logfree, d_iters, d_status, n, start);
         default: return bucketed_solve<5>(s, d_totals, d_cold_species, d_logfree, d_iters, d_status, n, start);
     }
+}
+
+int cl_eq_predict_device(cl_eq_solver* s, const double* d_totals, double* d_logfree, int64_t n) {
+    if (!s || !d_totals || !d_logfree || n < 0) { set_error("null argument"); return CL_ERR_ARG; }
+    if (n == 0) return CL_OK;
+    mlp_predict_kernel<<<grid_for((n + TS - 1) / TS, 1, 148 * 2), MLP_THREADS, mlp_smem_bytes(), s->stream>>>(
+        s->w, s->nc, d_totals, d_logfree, nullptr, nullptr, n);
+    CL_LAUNCH_CHECK("mlp_predict_kernel");
+    return CL_OK;
 }
 
 int cl_eq_solve_host(cl_eq_solver* s, const double* totals, const double* cold_species, double* logfree,

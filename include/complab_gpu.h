@@ -363,6 +363,9 @@ int cl_eq_param_count(const cl_eq_solver* s, int32_t* count);
 int cl_eq_get_params(cl_eq_solver* s, float* host_params);
 int cl_eq_set_params(cl_eq_solver* s, const float* host_params);
 int cl_eq_predict_host(cl_eq_solver* s, const float* x, float* y, int32_t n);
+/* the network's start for n device totals (log10 free components, FP64), the
+ * values CL_EQ_START_LEARNED starts Newton from; no counterpart in the reference */
+int cl_eq_predict_device(cl_eq_solver* s, const double* d_totals, double* d_logfree, int64_t n);
 
 #define CL_SRG_TENSOR 0   /* BF16 tensor-core inference, FP32 accumulate */
 #define CL_SRG_FP32   1   /* FP32 CUDA-core reference kernel */

@@ -487,7 +487,10 @@ double orc_eq_residual(const cl_eq_system* sys, const double* totals, const doub
  *     the clamped value), so J matches F;
  *   - the Newton step is scaled so that no component moves more than 2 decades;
  *   - the Armijo merit is ||F_j / sum_i |S_ij| c_i||_2 with the weights of the
- *     current iterate. */
+ *     current iterate.
+ * A solve whose 40 backtracking trials all fail stops at once (the reserve
+ * would repeat the same failing iteration at a point moved by ~1e-12 of a
+ * step until max_iter). */
 int orc_eq_newton(const cl_eq_system* sys, const double* totals, double* x,
                   int max_iter, double tol, int* converged) {
     const int nc = sys->n_comp, ns = sys->n_species;
@@ -541,6 +544,7 @@ int orc_eq_newton(const cl_eq_system* sys, const double* totals, double* x,
         double fn = 0; for (int j = 0; j < nc; ++j) fn += (F[j]*w[j])*(F[j]*w[j]);
         fn = sqrt(fn);
         double alpha = 1.0;
+        int accepted = 0;
         for (int ls = 0; ls < 40; ++ls) {
             for (int j = 0; j < nc; ++j) {
                 double v = x[j] + alpha * d[j];
@@ -551,10 +555,19 @@ int orc_eq_newton(const cl_eq_system* sys, const double* totals, double* x,
             eq_eval(sys, totals, xt, Ft, ct);
             double fnt = 0; for (int j = 0; j < nc; ++j) fnt += (Ft[j]*w[j])*(Ft[j]*w[j]);
             fnt = sqrt(fnt);
-            if (fnt < fn * (1.0 - 1e-4 * alpha) || alpha < 1e-15) break;
+            if (fnt < fn * (1.0 - 1e-4 * alpha)) { accepted = 1; break; }
+            if (alpha < 1e-15) break;
             alpha *= 0.5;
         }
         for (int j = 0; j < nc; ++j) x[j] = xt[j];
+        /* no trial down to 2^-39 of the step decreased the merit: the next
+         * iterate is the same point to ~1e-12 and fails the same way, so the
+         * solve stops here (not converged unless this point already is) */
+        if (!accepted) {
+            double F2[CL_MAX_COMP], c2[CL_MAX_SPECIES];
+            if (eq_eval(sys, totals, x, F2, c2) <= tol) *converged = 1;
+            return it + 1;
+        }
     }
     double F2[CL_MAX_COMP], c2[CL_MAX_SPECIES];
     if (eq_eval(sys, totals, x, F2, c2) <= tol) *converged = 1;

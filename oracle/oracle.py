@@ -8,6 +8,7 @@ never as the product path.
 import ctypes
 import os
 import subprocess
+import sys
 
 import numpy as np
 
@@ -21,7 +22,7 @@ _ref = None
 
 def build():
     """Compile liboracle.so (and _ref/libref.so when the reference tree exists)."""
-    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    subprocess.run(["make", "-s", "-C", HERE], check=True, stdout=sys.stderr)
 
 
 def _p(a):
