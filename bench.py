@@ -68,7 +68,7 @@ def peaks():
 
 def traffic_from_profile(kernel):
     """DRAM bytes per fluid site from the committed ncu summary, or None."""
-    p = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    p = os.path.join(ROOT, "profiles", "ade_main_kernel_coupled_traffic.txt")
     if not os.path.exists(p):
         return None
     for line in open(p):

@@ -119,6 +119,8 @@ def load_library(path=LIB_PATH):
         ("cl_set_flow_populations", [vp, vp]), ("cl_get_solute_populations", [vp, c_int32, vp]),
         ("cl_reduce", [vp, c_int32, c_int32, c_int32, c_double, P(c_double)]),
         ("cl_precip_convert", [vp, P(c_int64)]), ("cl_dissol_convert", [vp, P(c_int64)]),
+        ("cl_flow_velocity_stats", [vp, P(c_double), P(c_double), P(c_double)]),
+        ("cl_set_flow_pressure", [vp, c_double, c_double]), ("cl_set_transport", [vp, vp, vp, c_double]),
         ("cl_device_bytes", [vp, P(ctypes.c_uint64)]), ("cl_abi_sizes", [vp, c_int32]),
         ("cl_timing_enable", [vp, c_int32]), ("cl_timing_read", [vp, c_int32, P(c_double), P(c_int64)]),
         ("cl_launch_count", [vp, P(c_int64)]), ("cl_set_surrogate", [vp, c_int32, vp]),
@@ -346,6 +348,21 @@ class Lattice:
         ch = c_int64(0)
         self._c(self.lib.cl_precip_convert(self.h, ctypes.byref(ch)), "cl_precip_convert")
         return ch.value
+
+    def velocity_stats(self):
+        """(mean |u| and max u_x over x = 1..nx-2, mean u_x at x = nx-2)."""
+        a, b, c = c_double(), c_double(), c_double()
+        self._c(self.lib.cl_flow_velocity_stats(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)),
+                "cl_flow_velocity_stats")
+        return a.value, b.value, c.value
+
+    def set_flow_pressure(self, rho_in, rho_out):
+        self._c(self.lib.cl_set_flow_pressure(self.h, rho_in, rho_out), "cl_set_flow_pressure")
+
+    def set_transport(self, omega_pore, omega_bio, dt):
+        op = np.ascontiguousarray(omega_pore, np.float64)
+        ob = np.ascontiguousarray(omega_bio, np.float64)
+        self._c(self.lib.cl_set_transport(self.h, _ptr(op), _ptr(ob), dt), "cl_set_transport")
 
     def dissol_convert(self):
         ch = c_int64(0)

@@ -338,6 +338,46 @@ int cl_couple_velocity(cl_ctx* h) {
     return CL_OK;
 }
 
+int cl_flow_velocity_stats(cl_ctx* h, double* pore_mean_u, double* max_ux, double* outlet_mean_ux) {
+    if (!h) return CL_ERR_ARG;
+    Ctx* c = &h->c;
+    if (!c->flow_ready) { set_error("no flow field"); return CL_ERR_STATE; }
+    double v[3];
+    int r = flow_stats(c, v);
+    if (r) return r;
+    const double box = (double)(c->geo.N - 2 * c->geo.plane), plane = (double)c->geo.plane;
+    if (pore_mean_u) *pore_mean_u = v[0] / box;
+    if (max_ux) *max_ux = v[1];
+    if (outlet_mean_ux) *outlet_mean_ux = v[2] / plane;
+    return CL_OK;
+}
+
+int cl_set_flow_pressure(cl_ctx* h, double rho_in, double rho_out) {
+    if (!h || !(rho_in > 0.0) || !(rho_out > 0.0)) { set_error("cl_set_flow_pressure: densities must be positive"); return CL_ERR_ARG; }
+    h->c.cfg.rho_in = rho_in;
+    h->c.cfg.rho_out = rho_out;
+    return CL_OK;
+}
+
+int cl_set_transport(cl_ctx* h, const double* omega_pore, const double* omega_bio, double dt) {
+    if (!h || !omega_pore || !omega_bio || !(dt > 0.0)) { set_error("cl_set_transport: bad argument"); return CL_ERR_ARG; }
+    Ctx* c = &h->c;
+    for (int s = 0; s < c->cfg.n_solutes; ++s) {
+        if (!(omega_pore[s] > 0.0 && omega_pore[s] < 2.0) || !(omega_bio[s] > 0.0 && omega_bio[s] < 2.0)) {
+            set_error("cl_set_transport: relaxation frequencies must lie in (0, 2)"); return CL_ERR_ARG;
+        }
+    }
+    for (int s = 0; s < c->cfg.n_solutes; ++s) {
+        c->cfg.omega_pore[s] = omega_pore[s];
+        c->cfg.omega_bio[s] = omega_bio[s];
+        const int m = c->ap.mob_slot[s];
+        if (m >= 0) { c->ap.omega_pore[m] = (float)omega_pore[s]; c->ap.omega_bio[m] = (float)omega_bio[s]; }
+    }
+    c->cfg.dt = dt;
+    c->ap.dt = dt;
+    return CL_OK;
+}
+
 int cl_update_dynamics(cl_ctx* h) {
     if (!h) return CL_ERR_ARG;
     return update_dynamics(&h->c);

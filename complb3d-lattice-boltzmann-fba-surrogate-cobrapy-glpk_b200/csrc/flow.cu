@@ -293,6 +293,64 @@ int flow_macro(Ctx* c, double* d_rho, float* d_u3, int) {
     return CL_OK;
 }
 
+// Velocity statistics the reference takes after the flow solve for the
+// Peclet calibration (complab.cpp:641-652): the sum of |u| and the maximum
+// of u_x over x = 1..nx-2, the sum of u_x over the plane x = nx-2.  Fixed
+// grid, per-block FP64 partials, one block adds them in index order.
+template <int PARITY>
+__global__ void flow_stats_kernel(FlowK k, double* part) {
+    __shared__ double red[3][256];
+    double su = 0.0, mx = -1.0 / 0.0, so = 0.0;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t lo = k.g.plane, hi = k.g.N - k.g.plane;
+    for (int64_t n = lo + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < hi; n += stride) {
+        int x, y, z;
+        decode(k.g, n, x, y, z);
+        const uint8_t cls = k.cls[n];
+        float jx = 0.f, jy = 0.f, jz = 0.f;
+        if (cls == FLUID || cls == BIO) {
+            float f[19];
+            gather19<PARITY>(k, make_site(k.g, x, y, z, (uint32_t)n), f);
+#pragma unroll
+            for (int i = 0; i < 19; ++i) { jx += c19x(i) * f[i]; jy += c19y(i) * f[i]; jz += c19z(i) * f[i]; }
+        }
+        su += sqrt((double)jx * jx + (double)jy * jy + (double)jz * jz);
+        mx = fmax(mx, (double)jx);
+        if (x == k.g.nx - 2) so += jx;
+    }
+    red[0][threadIdx.x] = su; red[1][threadIdx.x] = mx; red[2][threadIdx.x] = so;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) {
+            red[0][threadIdx.x] += red[0][threadIdx.x + o];
+            red[1][threadIdx.x] = fmax(red[1][threadIdx.x], red[1][threadIdx.x + o]);
+            red[2][threadIdx.x] += red[2][threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) { part[3 * blockIdx.x] = red[0][0]; part[3 * blockIdx.x + 1] = red[1][0]; part[3 * blockIdx.x + 2] = red[2][0]; }
+}
+
+__global__ void flow_stats_final(const double* part, int nb, double* out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double su = 0.0, mx = -1.0 / 0.0, so = 0.0;
+    for (int b = 0; b < nb; ++b) { su += part[3 * b]; mx = fmax(mx, part[3 * b + 1]); so += part[3 * b + 2]; }
+    out[0] = su; out[1] = mx; out[2] = so;
+}
+
+int flow_stats(Ctx* c, double out[3]) {
+    FlowK k = make_flowk(c);
+    const int nb = 148 * 4;
+    double* part = c->d_scratch;
+    if (c->flow_parity == 0) flow_stats_kernel<0><<<nb, 256, 0, c->stream>>>(k, part);
+    else flow_stats_kernel<1><<<nb, 256, 0, c->stream>>>(k, part);
+    flow_stats_final<<<1, 32, 0, c->stream>>>(part, nb, part + 3 * nb);
+    CL_LAUNCH_CHECK("flow_stats_kernel");
+    CL_CUDA(cudaMemcpyAsync(out, part + 3 * nb, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CL_CUDA(cudaStreamSynchronize(c->stream));
+    return CL_OK;
+}
+
 // natural-order copy of the populations (to_natural) or upload from natural
 // order (requires parity 0 afterwards).
 template <int PARITY>

@@ -122,6 +122,7 @@ int flow_init(Ctx* c);
 int flow_step(Ctx* c, int arm_tracer_flag);
 int flow_arm_tracer(Ctx* c, double eps);
 int flow_macro(Ctx* c, double* d_rho, float* d_u3, int want_bc_velocity);
+int flow_stats(Ctx* c, double out[3]);   // sum |u| and max u_x over x = 1..nx-2, sum u_x at x = nx-2
 int classes_from_mask(Ctx* c);
 int ade_init(Ctx* c);
 int ade_step(Ctx* c);

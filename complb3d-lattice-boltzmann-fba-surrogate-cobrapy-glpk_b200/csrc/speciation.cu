@@ -60,12 +60,22 @@ struct MlpSmem {
     float loss[MLP_THREADS];
 };
 
-__device__ void load_weights(MlpSmem& s, const MlpDev& w, int nc) {
+// what the forward pass alone needs (inference): a quarter of MlpSmem, so
+// several blocks share an SM
+struct MlpSmemFwd {
+    __nv_bfloat16 X[TS * P24];
+    __nv_bfloat16 W1[H * P24], W2[H * P72], W3[8 * P72];
+    __nv_bfloat16 A1[TS * P72], A2[TS * P72];
+    float b[2 * H + 8];
+};
+
+template <class SM>
+__device__ void load_weights(SM& s, const MlpDev& w, int nc) {
     auto cp = [](__nv_bfloat16* dst, const __nv_bfloat16* src, int n) {
         for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
     };
-    cp(s.W1, w.W1, H * P24); cp(s.W2, w.W2, H * P72); cp(s.W2T, w.W2T, H * P72);
-    cp(s.W3, w.W3, 8 * P72); cp(s.W3T, w.W3T, H * P24);
+    cp(s.W1, w.W1, H * P24); cp(s.W2, w.W2, H * P72); cp(s.W3, w.W3, 8 * P72);
+    if constexpr (sizeof(SM) == sizeof(MlpSmem)) { cp(s.W2T, w.W2T, H * P72); cp(s.W3T, w.W3T, H * P24); }
     for (int i = threadIdx.x; i < 2 * H + nc; i += blockDim.x) s.b[i] = w.b[i];
 }
 
@@ -73,8 +83,8 @@ __device__ void load_weights(MlpSmem& s, const MlpDev& w, int nc) {
 // (and s.XT when training).  Leaves A1/A2 (and transposes, D1/D2 when
 // training) in shared memory; returns through y_out the standardised outputs
 // of this thread's output fragments via callback.
-template <bool TRAIN>
-__device__ void mlp_forward_tile(MlpSmem& s, int nc, float (*yfrag)[4]) {
+template <bool TRAIN, class SM>
+__device__ void mlp_forward_tile(SM& s, int nc, float (*yfrag)[4]) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
     // Z1 = X W1^T (64 x 64): 32 tiles, 8 per warp
     for (int q = 0; q < 8; ++q) {
@@ -87,7 +97,7 @@ __device__ void mlp_forward_tile(MlpSmem& s, int nc, float (*yfrag)[4]) {
             const float z = acc[r] + s.b[n];
             const float a = gelu(z);
             s.A1[m * P72 + n] = __float2bfloat16_rn(a);
-            if (TRAIN) { s.A1T[n * P72 + m] = __float2bfloat16_rn(a); s.D1[m * H + n] = gelu_d(z); }
+            if constexpr (TRAIN) { s.A1T[n * P72 + m] = __float2bfloat16_rn(a); s.D1[m * H + n] = gelu_d(z); }
         }
     }
     __syncthreads();
@@ -102,7 +112,7 @@ __device__ void mlp_forward_tile(MlpSmem& s, int nc, float (*yfrag)[4]) {
             const float z = acc[r] + s.b[H + n];
             const float a = gelu(z);
             s.A2[m * P72 + n] = __float2bfloat16_rn(a);
-            if (TRAIN) { s.A2T[n * P72 + m] = __float2bfloat16_rn(a); s.D2[m * H + n] = gelu_d(z); }
+            if constexpr (TRAIN) { s.A2T[n * P72 + m] = __float2bfloat16_rn(a); s.D2[m * H + n] = gelu_d(z); }
         }
     }
     __syncthreads();
@@ -289,7 +299,7 @@ __global__ void __launch_bounds__(MLP_THREADS) mlp_predict_kernel(MlpDev w, int 
                                                                   double* logfree, const float* xin, float* yout,
                                                                   int64_t n) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    MlpSmem& s = *reinterpret_cast<MlpSmem*>(smem_raw);
+    MlpSmemFwd& s = *reinterpret_cast<MlpSmemFwd*>(smem_raw);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
     load_weights(s, w, nc);
     __shared__ float nrm[4 * CL_MAX_COMP];
@@ -494,6 +504,7 @@ struct cl_eq_solver {
 };
 
 static size_t mlp_smem_bytes() { return sizeof(MlpSmem); }
+static size_t mlp_fwd_smem_bytes() { return sizeof(MlpSmemFwd); }
 
 static int eq_ensure_fail(cl_eq_solver* s, int64_t n) {
     if (s->fail_cap >= n) return CL_OK;
@@ -621,7 +632,7 @@ cl_eq_solver* cl_eq_create(const cl_eq_system* sys, void* stream, int* status) {
     A((void**)&s->fail_count, 2 * sizeof(unsigned long long));
     if (e != cudaSuccess) return fail(cuda_fail(e, "cl_eq_create"), s);
     if (cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mlp_smem_bytes()) != cudaSuccess ||
-        cudaFuncSetAttribute(mlp_predict_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mlp_smem_bytes()) != cudaSuccess)
+        cudaFuncSetAttribute(mlp_predict_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mlp_fwd_smem_bytes()) != cudaSuccess)
         return fail(cuda_fail(cudaGetLastError(), "cudaFuncSetAttribute(mlp)"), s);
     // default initialisation: Glorot-uniform weights, zero biases, identity normalisation
     std::vector<float> p(np, 0.f);
@@ -683,7 +694,7 @@ int cl_eq_solve_device(cl_eq_solver* s, const double* d_totals, const double* d_
     if (n == 0) return CL_OK;
     if (start == CL_EQ_START_COLD && !d_cold_species) { set_error("cold start needs the species vectors"); return CL_ERR_ARG; }
     if (start == CL_EQ_START_LEARNED) {
-        mlp_predict_kernel<<<grid_for((n + TS - 1) / TS, 1, 148 * 2), MLP_THREADS, mlp_smem_bytes(), s->stream>>>(
+        mlp_predict_kernel<<<grid_for((n + TS - 1) / TS, 1, 148 * 6), MLP_THREADS, mlp_fwd_smem_bytes(), s->stream>>>(
             s->w, s->nc, d_totals, d_logfree, nullptr, nullptr, n);
         CL_LAUNCH_CHECK("mlp_predict_kernel");
     } else if (start != CL_EQ_START_GIVEN && start != CL_EQ_START_COLD) { set_error("unknown start mode"); return CL_ERR_ARG; }
@@ -701,7 +712,7 @@ int cl_eq_solve_device(cl_eq_solver* s, const double* d_totals, const double* d_
 int cl_eq_predict_device(cl_eq_solver* s, const double* d_totals, double* d_logfree, int64_t n) {
     if (!s || !d_totals || !d_logfree || n < 0) { set_error("null argument"); return CL_ERR_ARG; }
     if (n == 0) return CL_OK;
-    mlp_predict_kernel<<<grid_for((n + TS - 1) / TS, 1, 148 * 2), MLP_THREADS, mlp_smem_bytes(), s->stream>>>(
+    mlp_predict_kernel<<<grid_for((n + TS - 1) / TS, 1, 148 * 6), MLP_THREADS, mlp_fwd_smem_bytes(), s->stream>>>(
         s->w, s->nc, d_totals, d_logfree, nullptr, nullptr, n);
     CL_LAUNCH_CHECK("mlp_predict_kernel");
     return CL_OK;
@@ -775,7 +786,7 @@ int cl_eq_predict_host(cl_eq_solver* s, const float* x, float* y, int32_t n) {
     int r = CL_OK;
     cudaError_t e = cudaMemcpyAsync(dx, x, sizeof(float) * n * nc, cudaMemcpyHostToDevice, s->stream);
     if (e == cudaSuccess) {
-        mlp_predict_kernel<<<grid_for((n + TS - 1) / TS, 1, 148 * 2), MLP_THREADS, mlp_smem_bytes(), s->stream>>>(
+        mlp_predict_kernel<<<grid_for((n + TS - 1) / TS, 1, 148 * 6), MLP_THREADS, mlp_fwd_smem_bytes(), s->stream>>>(
             s->w, nc, nullptr, nullptr, dx, dy, n);
         e = cudaGetLastError();
     }

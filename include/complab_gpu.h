@@ -241,6 +241,18 @@ int cl_couple_velocity(cl_ctx* ctx);
  * (updateSoluteDynamics3D, :461-529). */
 int cl_update_dynamics(cl_ctx* ctx);
 
+/* The host driver's Peclet calibration (src/complab.cpp:641-669):
+ * cl_flow_velocity_stats returns computeAverage(velocityNorm) and
+ * computeMax(u_x) over x = 1..nx-2 and computeAverage(u_x) over the plane
+ * x = nx-2 (every site counted, walls as zero); cl_set_flow_pressure is
+ * NSdomainSetup's new deltaP (rho_in = 1, rho_out = 1 - 3 deltaP), followed by
+ * cl_flow_init; cl_set_transport sets the solute relaxation frequencies and
+ * the transport time step derived from the calibrated flow
+ * (complab.cpp:708-727). */
+int cl_flow_velocity_stats(cl_ctx* ctx, double* pore_mean_u, double* max_ux, double* outlet_mean_ux);
+int cl_set_flow_pressure(cl_ctx* ctx, double rho_in, double rho_out);
+int cl_set_transport(cl_ctx* ctx, const double* omega_pore, const double* omega_bio, double dt);
+
 /* ---- transport step (rows a5-a12) ---------------------------------------------
  * cl_ade_init: initializeAtEquilibrium(c0, u=0) for every solute
  *              (src/complab_functions.hh:334-336).
