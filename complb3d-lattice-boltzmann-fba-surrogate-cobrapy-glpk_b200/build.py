@@ -15,6 +15,8 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libcomplab_gpu.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
+HOST = os.path.join(HERE, "host")
+DRIVER = os.path.join(HERE, "complab_b200")
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -65,9 +67,27 @@ def build(verbose=False, extra=None):
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n%s\n%s" % (r.stdout, r.stderr))
+    build_driver()
     if verbose:
         print("built", LIB)
+        print("built", DRIVER)
     return LIB
+
+
+def build_driver():
+    """The host driver (host/*.cpp): CompLaB.xml in, the time loop over the C
+    ABI, fields out.  Plain g++, linked against libcomplab_gpu.so next to it."""
+    srcs = sorted(os.path.join(HOST, f) for f in os.listdir(HOST) if f.endswith(".cpp"))
+    hdrs = [os.path.join(HOST, f) for f in os.listdir(HOST) if f.endswith(".h")]
+    newest = max(os.path.getmtime(p) for p in srcs + hdrs + [LIB, os.path.join(INCLUDE, "complab_gpu.h")])
+    if os.path.exists(DRIVER) and os.path.getmtime(DRIVER) >= newest:
+        return DRIVER
+    cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-o", DRIVER] + srcs + [
+        "-I" + INCLUDE, "-L" + HERE, "-lcomplab_gpu", "-Wl,-rpath,$ORIGIN"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("host driver build failed:\n%s\n%s" % (r.stdout, r.stderr))
+    return DRIVER
 
 
 if __name__ == "__main__":

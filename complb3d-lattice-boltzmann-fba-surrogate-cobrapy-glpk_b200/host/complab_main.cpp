@@ -1,0 +1,250 @@
+// complab_main.cpp -- host driver: CompLaB.xml in, the reference's time loop
+// (src/complab.cpp:560-1860) over the C ABI, fields out.
+//
+//   complab_b200 [CompLaB.xml] [--steps N] [--print-config] [--quiet]
+//
+// Order, as main() of the reference runs it:
+//   read CompLaB.xml and the geometry (readGeometry, complab_functions.hh:127-156);
+//   flow to steady state with the ValueTracer (complab.cpp:614-620); if a Peclet
+//   number is set, the permeability from the outlet Darcy velocity, a corrected
+//   deltaP and a second solve (:641-669);
+//   solute relaxation and dt from the flow (:708-727), velocity coupling (:1096-1101);
+//   then per transport step: collide .. kinetics .. abiotic (+ dissolution) ..
+//   equilibrium .. stream (cl_step), and on their intervals the precipitation
+//   and dissolution node conversions with the dynamics switch, flow re-solve and
+//   re-coupling (:1783-1845).
+// Fields are written as raw little-endian FP64 arrays in site order
+// n = (x*ny + y)*nz + z, one file per solute (and microbe) per output step,
+// with a JSON index; the run summary goes to stdout as one JSON line.
+#include <sys/stat.h>
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <string>
+#include <vector>
+
+#include "../../include/complab_gpu.h"
+#include "complab_xml.h"
+
+using clhost::HostRun;
+
+namespace {
+
+constexpr double kThrd = 1e-12;
+
+struct Ctx {
+    cl_ctx* h = nullptr;
+    ~Ctx() { if (h) cl_destroy(h); }
+};
+
+bool check(int st, const char* what) {
+    if (st < 0) {
+        std::fprintf(stderr, "complab_b200: %s failed (%d): %s\n", what, st, cl_last_error());
+        return false;
+    }
+    return true;
+}
+
+// readGeometry: nx-2 slices of ny*nz integers (y-major, z fastest); the
+// boundary planes repeat the first and last slice
+bool read_geometry(const std::string& file, int nx, int ny, int nz, std::vector<uint8_t>& mask, std::string& err) {
+    std::ifstream f(file);
+    if (!f) { err = "could not open geometry file " + file; return false; }
+    const size_t plane = (size_t)ny * nz;
+    mask.assign((size_t)nx * plane, 0);
+    for (int x = 1; x < nx - 1; ++x)
+        for (size_t p = 0; p < plane; ++p) {
+            long v;
+            if (!(f >> v)) { err = "geometry file " + file + " ends before " + std::to_string((size_t)(nx - 2) * plane) + " values"; return false; }
+            if (v < 0 || v > 255) { err = "material number out of range in " + file; return false; }
+            mask[(size_t)x * plane + p] = (uint8_t)v;
+        }
+    std::memcpy(&mask[0], &mask[plane], plane);
+    std::memcpy(&mask[(size_t)(nx - 1) * plane], &mask[(size_t)(nx - 2) * plane], plane);
+    return true;
+}
+
+bool write_fields(cl_ctx* h, const HostRun& run, long iT, std::vector<std::string>& index) {
+    const cl_config& c = run.cfg;
+    const size_t N = (size_t)c.nx * c.ny * c.nz;
+    std::vector<double> buf(N);
+    auto dump = [&](int field, int idx, const std::string& name) {
+        if (!check(cl_get_field(h, field, idx, buf.data()), "cl_get_field")) return false;
+        const std::string fn = name + "_" + std::to_string(iT) + ".raw";
+        std::ofstream o(run.output_dir + "/" + fn, std::ios::binary);
+        o.write(reinterpret_cast<const char*>(buf.data()), (std::streamsize)(N * sizeof(double)));
+        index.push_back(fn);
+        return (bool)o;
+    };
+    for (int s = 0; s < c.n_solutes; ++s) if (!dump(CL_FIELD_CONC, s, run.subs_names[s])) return false;
+    for (int m = 0; m < c.n_microbes; ++m) if (!dump(CL_FIELD_BIOMASS, m, run.microbe_names[m])) return false;
+    // the material numbers (uint8), which precipitation and dissolution change
+    std::vector<uint8_t> mask(N);
+    if (!check(cl_download_mask(h, mask.data()), "cl_download_mask")) return false;
+    const std::string fn = "mask_" + std::to_string(iT) + ".u8";
+    std::ofstream o(run.output_dir + "/" + fn, std::ios::binary);
+    o.write(reinterpret_cast<const char*>(mask.data()), (std::streamsize)N);
+    index.push_back(fn);
+    return (bool)o;
+}
+
+// collideAndStream until the ValueTracer converges (cl_flow_solve); then the
+// velocity statistics the calibration uses
+bool flow_solve(cl_ctx* h, long max_it, double eps, int* iters) {
+    const int st = cl_flow_solve(h, (int32_t)max_it, eps, iters);
+    return check(st, "cl_flow_solve");
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    std::string xml = "CompLaB.xml";
+    long steps_override = -1;
+    bool print_config = false, quiet = false;
+    for (int i = 1; i < argc; ++i) {
+        const std::string a = argv[i];
+        if (a == "--print-config") print_config = true;
+        else if (a == "--quiet") quiet = true;
+        else if (a == "--steps" && i + 1 < argc) steps_override = std::atol(argv[++i]);
+        else if (!a.empty() && a[0] != '-') xml = a;
+        else { std::fprintf(stderr, "usage: %s [CompLaB.xml] [--steps N] [--print-config] [--quiet]\n", argv[0]); return 2; }
+    }
+    HostRun run;
+    std::string err;
+    if (clhost::read_complab_xml(xml, run, err)) { std::fprintf(stderr, "complab_b200: %s\n", err.c_str()); return 1; }
+    if (print_config) { std::printf("%s\n", clhost::run_json(run).c_str()); return 0; }
+    if (steps_override >= 0) run.ade_max = steps_override;
+    for (const std::string& n : run.notes) if (!quiet) std::fprintf(stderr, "complab_b200: note: %s\n", n.c_str());
+
+    cl_config& c = run.cfg;
+    std::vector<uint8_t> mask;
+    if (!read_geometry(run.input_dir + "/" + run.geom_file, c.nx, c.ny, c.nz, mask, err)) {
+        std::fprintf(stderr, "complab_b200: %s\n", err.c_str());
+        return 1;
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    int st = 0;
+    Ctx ctx;
+    ctx.h = cl_create(&c, nullptr, &st);
+    if (!ctx.h) { std::fprintf(stderr, "complab_b200: cl_create failed (%d): %s\n", st, cl_last_error()); return 1; }
+    cl_ctx* h = ctx.h;
+    if (!check(cl_upload_mask(h, mask.data()), "cl_upload_mask")) return 1;
+
+    // flow and the Peclet calibration
+    const double nsNu = (run.tau - 0.5) / 3.0;
+    double pore_mean_u = 0.0, max_ux = 0.0, outlet_ux = 0.0, pe_achieved = 0.0;
+    int ns_iters = 0;
+    if (!check(cl_flow_init(h), "cl_flow_init")) return 1;
+    if (run.Pe > kThrd) {
+        if (!flow_solve(h, run.ns_max1, run.ns_conv1, &ns_iters)) return 1;
+        if (!check(cl_flow_velocity_stats(h, &pore_mean_u, &max_ux, &outlet_ux), "cl_flow_velocity_stats")) return 1;
+        const double D_fixed = 0.25 * (0.8 - 0.5);          // tau_ADE_fixed = 0.8 (complab.cpp:164)
+        const double perm = outlet_ux * nsNu * run.charcs_length / run.delta_P;
+        const double u_target = run.Pe * D_fixed / run.charcs_length;
+        const double dP_new = u_target * nsNu * run.charcs_length / perm;
+        if (std::fabs(dP_new - run.delta_P) / run.delta_P > 0.01) {
+            run.delta_P = dP_new;
+            if (!check(cl_set_flow_pressure(h, 1.0, 1.0 - 3.0 * dP_new), "cl_set_flow_pressure")) return 1;
+            if (!check(cl_flow_init(h), "cl_flow_init")) return 1;
+            if (!flow_solve(h, run.ns_max1, run.ns_conv1, &ns_iters)) return 1;
+            if (!check(cl_flow_velocity_stats(h, &pore_mean_u, &max_ux, &outlet_ux), "cl_flow_velocity_stats")) return 1;
+        }
+        pe_achieved = outlet_ux * run.charcs_length / D_fixed;
+        if (max_ux / std::sqrt(0.25) > 1.0) { std::fprintf(stderr, "complab_b200: Ma > 1 after the flow solve\n"); return 1; }
+    }
+
+    // solute relaxation and dt from the flow (complab.cpp:708-727)
+    const int S = c.n_solutes;
+    if (S > 0) {
+        double refNu, refTau;
+        if (run.Pe > kThrd) {
+            refNu = pore_mean_u * run.charcs_length / run.Pe;
+            refTau = refNu * 4.0 + 0.5;
+            if (refTau > 2 || refTau <= 0.5) { std::fprintf(stderr, "complab_b200: transport tau=%g invalid\n", refTau); return 1; }
+        } else {
+            refTau = run.tau;
+            refNu = 0.25 * (refTau - 0.5);
+        }
+        std::vector<double> om_p(S), om_b(S);
+        for (int s = 0; s < S; ++s) {
+            const double nu = refNu * run.D_pore[s] / run.D_pore[0];
+            om_p[s] = 1.0 / (nu * 4.0 + 0.5);
+            om_b[s] = 1.0 / (refNu * run.D_bfilm[s] / run.D_pore[0] * 4.0 + 0.5);
+        }
+        const double dt = refNu * run.dx * run.dx / run.D_pore[0];
+        c.dt = dt;
+        for (int s = 0; s < S; ++s) { c.omega_pore[s] = om_p[s]; c.omega_bio[s] = om_b[s]; }
+        if (!check(cl_set_transport(h, om_p.data(), om_b.data(), dt), "cl_set_transport")) return 1;
+    }
+    if (run.Pe > kThrd && !check(cl_couple_velocity(h), "cl_couple_velocity")) return 1;
+    if (!check(cl_ade_init(h), "cl_ade_init")) return 1;
+    // sessile biomass on the microbes' materials (initializeScalarLattice3D)
+    {
+        const size_t N = mask.size();
+        std::vector<double> b(N);
+        for (int m = 0; m < c.n_microbes; ++m) {
+            std::fill(b.begin(), b.end(), 0.0);
+            const auto& mats = run.bio_materials[m];
+            const auto& b0 = run.b0[m];
+            for (size_t n = 0; n < N; ++n)
+                for (size_t k = 0; k < mats.size() && k < b0.size(); ++k)
+                    if (mask[n] == mats[k]) b[n] = b0[k];
+            if (!check(cl_set_field(h, CL_FIELD_BIOMASS, m, b.data()), "cl_set_field")) return 1;
+        }
+    }
+
+    mkdir(run.output_dir.c_str(), 0777);
+    std::vector<std::string> index;
+    long nonconv_steps = 0, precip_changes = 0, dissol_changes = 0, resolves = 0;
+    const auto t1 = std::chrono::steady_clock::now();
+    for (long iT = 0; iT < run.ade_max; ++iT) {
+        st = cl_step(h, 1);
+        if (!check(st, "cl_step")) return 1;
+        if (st == CL_WARN_NOT_CONVERGED) ++nonconv_steps;
+        bool changed = false;
+        if (c.precip_enabled && iT % run.precip_interval == 0) {
+            int64_t ch = 0;
+            if (!check(cl_precip_convert(h, &ch), "cl_precip_convert")) return 1;
+            precip_changes += ch;
+            changed = changed || ch > 0;
+        }
+        if (c.dissol_enabled && iT % run.dissol_interval == 0) {
+            int64_t ch = 0;
+            if (!check(cl_dissol_convert(h, &ch), "cl_dissol_convert")) return 1;
+            dissol_changes += ch;
+            changed = changed || ch > 0;
+        }
+        if (changed && run.Pe > kThrd) {
+            if (!check(cl_update_dynamics(h), "cl_update_dynamics")) return 1;
+            int it2 = 0;
+            st = cl_flow_solve(h, (int32_t)run.ns_max2, run.ns_conv2, &it2);
+            if (!check(st, "cl_flow_solve")) return 1;
+            if (!check(cl_couple_velocity(h), "cl_couple_velocity")) return 1;
+            ++resolves;
+        }
+        if (run.vtk_interval > 0 && iT % run.vtk_interval == 0 && !write_fields(h, run, iT, index)) return 1;
+    }
+    const auto t2 = std::chrono::steady_clock::now();
+    if (!write_fields(h, run, run.ade_max, index)) return 1;
+    {
+        std::ofstream o(run.output_dir + "/fields.json");
+        o << "{\"nx\": " << c.nx << ", \"ny\": " << c.ny << ", \"nz\": " << c.nz
+          << ", \"dtype\": \"float64\", \"order\": \"(x*ny + y)*nz + z\", \"files\": [";
+        for (size_t i = 0; i < index.size(); ++i) o << (i ? ", " : "") << "\"" << index[i] << "\"";
+        o << "]}\n";
+    }
+    const double setup_s = std::chrono::duration<double>(t1 - t0).count();
+    const double loop_s = std::chrono::duration<double>(t2 - t1).count();
+    const double sites = (double)mask.size();
+    std::printf("{\"steps\": %ld, \"setup_s\": %.6f, \"loop_s\": %.6f, \"mlups\": %.3f, \"ns_iters\": %d, "
+                "\"pore_mean_u\": %.9g, \"max_ux\": %.9g, \"outlet_ux\": %.9g, \"delta_P\": %.9g, \"Pe_achieved\": %.6g, "
+                "\"dt\": %.9g, \"nonconverged_steps\": %ld, \"precip_changes\": %lld, \"dissol_changes\": %lld, "
+                "\"flow_resolves\": %ld, \"output\": \"%s\"}\n",
+                run.ade_max, setup_s, loop_s, loop_s > 0 ? sites * run.ade_max / loop_s / 1e6 : 0.0, ns_iters,
+                pore_mean_u, max_ux, outlet_ux, run.delta_P, pe_achieved, c.dt, nonconv_steps,
+                (long long)precip_changes, (long long)dissol_changes, resolves, run.output_dir.c_str());
+    return 0;
+}

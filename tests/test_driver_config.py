@@ -1,0 +1,118 @@
+"""The host driver's CompLaB.xml reader (CPU): the schema, defaults and unit
+handling of the reference's initialize_complab, checked through
+`complab_b200 --print-config` on XML files written here."""
+import json
+import os
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+DRIVER = os.path.join(ROOT, "complb3d-lattice-boltzmann-fba-surrogate-cobrapy-glpk_b200", "complab_b200")
+
+CASE = """<?xml version="1.0" ?>
+<!-- a small abiotic case: A -> P on wall-adjacent voxels, P immobile -->
+<parameters>
+    <path><input_path>input</input_path><output_path>output</output_path></path>
+    <simulation_mode>
+        <biotic_mode>false</biotic_mode>
+        <enable_abiotic_kinetics>true</enable_abiotic_kinetics>
+    </simulation_mode>
+    <LB_numerics>
+        <domain>
+            <nx>{nx}</nx><ny>{ny}</ny><nz>{nz}</nz>
+            <dx>10</dx><unit>um</unit>
+            <characteristic_length>{L}</characteristic_length>
+            <filename>geometry.dat</filename>
+            <material_numbers><pore>2</pore><solid>0</solid><bounce_back>1</bounce_back></material_numbers>
+        </domain>
+        <delta_P>{dP}</delta_P>
+        <Peclet>{Pe}</Peclet>
+        <tau>0.8</tau>
+        <iteration>
+            <ns_max_iT1>3000</ns_max_iT1>
+            <ns_converge_iT1>1e-7</ns_converge_iT1>
+            <ade_max_iT>{steps}</ade_max_iT>
+        </iteration>
+    </LB_numerics>
+    <chemistry>
+        <number_of_substrates>2</number_of_substrates>
+        <substrate0>
+            <name_of_substrates>A</name_of_substrates>
+            <initial_concentration>0.1</initial_concentration>
+            <substrate_diffusion_coefficients><in_pore>1e-9</in_pore><in_biofilm>5e-10</in_biofilm></substrate_diffusion_coefficients>
+            <left_boundary_type>Dirichlet</left_boundary_type><left_boundary_condition>1.0</left_boundary_condition>
+            <right_boundary_type>Neumann</right_boundary_type><right_boundary_condition>0</right_boundary_condition>
+        </substrate0>
+        <substrate1>
+            <name_of_substrates>P</name_of_substrates>
+            <immobile>true</immobile>
+            <left_boundary_type>Neumann</left_boundary_type><left_boundary_condition>0</left_boundary_condition>
+            <right_boundary_type>Neumann</right_boundary_type><right_boundary_condition>0</right_boundary_condition>
+        </substrate1>
+    </chemistry>
+    <rate_table>
+        <reaction0><k>0.05</k><mass>0</mass><nu>0:-1 1:1</nu></reaction0>
+    </rate_table>
+    <precipitation>
+        <enabled>true</enabled><solid_substrate>1</solid_substrate><max_precipRho>0.02</max_precipRho>
+        <surface_only>1</surface_only><update_interval>5</update_interval>
+    </precipitation>
+</parameters>
+"""
+
+
+def write_case(tmp, nx=10, ny=8, nz=8, Pe=0.0, dP=0.0, L=8, steps=20, mask=None):
+    import numpy as np
+    os.makedirs(os.path.join(tmp, "input"), exist_ok=True)
+    xml = os.path.join(tmp, "CompLaB.xml")
+    open(xml, "w").write(CASE.format(nx=nx, ny=ny, nz=nz, Pe=Pe, dP=dP, L=L * 10, steps=steps))
+    if mask is None:
+        mask = np.full((nx, ny, nz), 2, np.uint8)
+        mask[:, :, 0] = 1
+        mask[:, :, -1] = 1
+    with open(os.path.join(tmp, "input", "geometry.dat"), "w") as f:
+        for x in range(nx):
+            f.write("\n".join(str(int(v)) for v in mask[x].reshape(-1)) + "\n")
+    return xml
+
+
+def driver_available():
+    return os.path.exists(DRIVER)
+
+
+@pytest.mark.skipif(not driver_available(), reason="host driver not built")
+def test_print_config_follows_the_schema(tmp_path):
+    xml = write_case(str(tmp_path), Pe=0.0, dP=0.0)
+    out = subprocess.run([DRIVER, xml, "--print-config"], capture_output=True, text=True, check=True).stdout
+    c = json.loads(out)
+    assert (c["nx"], c["ny"], c["nz"]) == (12, 8, 8)           # nx += 2 (complab_functions.hh:769)
+    assert c["dx"] == pytest.approx(10e-6)                     # <unit>um
+    assert c["charcs_length"] == pytest.approx(8.0)            # in lattice units
+    assert c["pore"] == [2] and c["solid"] == 0 and c["bounce_back"] == 1
+    assert c["names"] == ["A", "P"] and c["immobile"] == [0, 1]
+    assert c["c0"] == [0.1, 0.0]
+    assert c["left_type"] == [0, 1] and c["right_type"] == [1, 1]
+    assert c["left_value"][0] == 1.0
+    assert c["enable_abiotic"] == 1 and c["enable_kinetics"] == 0 and c["n_rxn"] == 1
+    assert c["precip_enabled"] == 1 and c["precip_substrate"] == 1 and c["max_precip_rho"] == 0.02
+    assert c["Pe"] == 0.0                                      # delta_P < thrd forces Pe = 0
+    # without flow the transport relaxation comes from tau, dt = nu dx^2 / D0
+    nu = 0.25 * (0.8 - 0.5)
+    assert c["omega_pore"][0] == pytest.approx(1.0 / 0.8)
+    assert c["dt"] == pytest.approx(nu * (10e-6) ** 2 / 1e-9)
+
+
+@pytest.mark.skipif(not driver_available(), reason="host driver not built")
+def test_defaults_and_errors(tmp_path):
+    xml = write_case(str(tmp_path), Pe=2.0, dP=1e-5)
+    c = json.loads(subprocess.run([DRIVER, xml, "--print-config"], capture_output=True, text=True, check=True).stdout)
+    assert c["Pe"] == 2.0 and c["rho_out"] == pytest.approx(1.0 - 3e-5)
+    assert c["ns_max_iT1"] == 3000 and c["ns_converge_iT1"] == 1e-7
+    # a required element missing: the reference terminates, the driver exits 1 with the path
+    text = open(xml).read().replace("<ny>8</ny>", "")
+    open(xml, "w").write(text)
+    r = subprocess.run([DRIVER, xml, "--print-config"], capture_output=True, text=True)
+    assert r.returncode == 1 and "ny" in r.stderr
+    r = subprocess.run([DRIVER, str(tmp_path / "absent.xml"), "--print-config"], capture_output=True, text=True)
+    assert r.returncode == 1
