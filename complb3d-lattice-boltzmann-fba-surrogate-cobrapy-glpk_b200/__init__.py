@@ -24,6 +24,7 @@ OK, WARN_NOT_CONVERGED = 0, 1
 ERR_ARG, ERR_CUDA, ERR_STATE, ERR_NOMEM, ERR_DIVERGED = -1, -2, -3, -4, -5
 BC_DIRICHLET, BC_NEUMANN = 0, 1
 FIELD_CONC, FIELD_BIOMASS, FIELD_VELOCITY, FIELD_FLOW_RHO, FIELD_FLOW_U, FIELD_PHASE, FIELD_EQ_ITERS = range(7)
+FIELD_CA_AGE, FIELD_CA_TOTAL = 7, 8
 RED_SUM, RED_MIN, RED_MAX, RED_COUNT_EQ = range(4)
 EQ_START_COLD, EQ_START_GIVEN, EQ_START_LEARNED = range(3)
 SRG_TENSOR, SRG_FP32 = 0, 1
@@ -91,6 +92,8 @@ class Config(ctypes.Structure):
         ("dissol_apply_at_walls", c_int32),
         ("n_phases", c_int32), ("phases", Phase * MAX_PHASES),
         ("n_srg", c_int32), ("srg", SrgOrganism * MAX_SRG_ORG),
+        ("ca_enabled", c_int32), ("ca_half", c_int32), ("ca_bmax", c_double), ("ca_thrd_frac", c_double),
+        ("microbe_code", c_int32 * MAX_MICROBES), ("ca_seed", ctypes.c_uint64),
     ]
 
 
@@ -124,6 +127,7 @@ def load_library(path=LIB_PATH):
         ("cl_device_bytes", [vp, P(ctypes.c_uint64)]), ("cl_abi_sizes", [vp, c_int32]),
         ("cl_timing_enable", [vp, c_int32]), ("cl_timing_read", [vp, c_int32, P(c_double), P(c_int64)]),
         ("cl_launch_count", [vp, P(c_int64)]), ("cl_set_surrogate", [vp, c_int32, vp]),
+        ("cl_ca_redistribute", [vp, P(c_int32), P(c_int64), P(c_double)]), ("cl_ca_update_mask", [vp, P(c_int64)]),
     ]:
         fn = getattr(lib, name)
         fn.restype = ctypes.c_int
@@ -368,6 +372,19 @@ class Lattice:
         ch = c_int64(0)
         self._c(self.lib.cl_dissol_convert(self.h, ctypes.byref(ch)), "cl_dissol_convert")
         return ch.value
+
+    def ca_update_mask(self):
+        """Initial mask update after seeding the biomass; returns sites changed."""
+        ch = c_int64(0)
+        self._c(self.lib.cl_ca_update_mask(self.h, ctypes.byref(ch)), "cl_ca_update_mask")
+        return ch.value
+
+    def ca_redistribute(self):
+        """One CA block: returns (status, push sweeps, sites whose mask changed, biomass maximum)."""
+        sw, ch, bm = c_int32(0), c_int64(0), c_double(0)
+        st = self._c(self.lib.cl_ca_redistribute(self.h, ctypes.byref(sw), ctypes.byref(ch), ctypes.byref(bm)),
+                     "cl_ca_redistribute")
+        return st, sw.value, ch.value, bm.value
 
     def timing(self, on=True):
         self._c(self.lib.cl_timing_enable(self.h, 1 if on else 0), "cl_timing_enable")

@@ -1,4 +1,4 @@
-// ade.cu -- fused multi-solute D3Q7 advection-diffusion-reaction step (rows a5-a12).
+// ade_kernels.cuh -- fused multi-solute D3Q7 advection-diffusion-reaction step.
 //
 // One launch does, for every interior site and every mobile solute, what the
 // reference does in separate whole-lattice passes (src/complab.cpp:1252-1374,

@@ -4,6 +4,7 @@
 #include <cstdio>
 #include <vector>
 #include <algorithm>
+#include <cmath>
 
 namespace cl {
 
@@ -81,6 +82,16 @@ static int validate(const cl_config* c) {
         }
     }
     if (c->n_phases < 0 || c->n_phases > CL_MAX_PHASES) { set_error("n_phases out of range"); return CL_ERR_ARG; }
+    if (c->ca_enabled) {
+        // complab_functions.hh:1167-1186: Bmax and the biofilm fraction are
+        // required for a CA microbe; each microbe's biofilm material is its code
+        if (c->n_microbes < 1) { set_error("the cellular automaton needs at least one microbe"); return CL_ERR_ARG; }
+        if (!(c->ca_bmax > 0.0) || !std::isfinite(c->ca_bmax)) { set_error("ca_bmax must be positive"); return CL_ERR_ARG; }
+        if (!(c->ca_thrd_frac >= 0.0) || !std::isfinite(c->ca_thrd_frac)) { set_error("ca_thrd_frac must be >= 0"); return CL_ERR_ARG; }
+        if (c->n_pore_codes < 1) { set_error("the cellular automaton needs a pore material"); return CL_ERR_ARG; }
+        for (int m = 0; m < c->n_microbes; ++m)
+            if (c->microbe_code[m] < 0 || c->microbe_code[m] > 255) { set_error("microbe_code must be a material number 0..255"); return CL_ERR_ARG; }
+    }
     if (c->dissol_enabled) {
         // complab.cpp:336-368: at least one phase, reopen_fraction in (0,1),
         // a substrate and a positive full density per phase
@@ -198,6 +209,10 @@ cl_ctx* cl_create(const cl_config* cfg, void* stream, int* status) {
         (r = dalloc(c, &c->d_eq_x, (size_t)(p.eq_warm ? cfg->eq.n_comp : 0) * N)) ||
         (r = dalloc(c, &c->d_phase, (size_t)(p.do_dissol ? N : 0))) ||
         (r = dalloc(c, &c->d_rel, (size_t)(p.do_dissol ? p.S : 0) * N)) ||
+        (r = dalloc(c, &c->d_ca_total, (size_t)(cfg->ca_enabled ? N : 0))) ||
+        (r = dalloc(c, &c->d_ca_age, (size_t)(cfg->ca_enabled ? 2 * N : 0))) ||
+        (r = dalloc(c, &c->d_ca_distpos, (size_t)(cfg->ca_enabled ? N : 0))) ||
+        (r = dalloc(c, &c->d_ca_out, (size_t)(cfg->ca_enabled ? 6 * p.M : 0) * N)) ||
         (r = dalloc(c, &c->d_counters, 8)) || (r = dalloc(c, &c->d_tracer, 1)))
         return fail(r);
     if (c->d_eq_x) cudaMemsetAsync(c->d_eq_x, 0xff, sizeof(double) * cfg->eq.n_comp * N, c->stream);  // NaN
@@ -223,7 +238,7 @@ int cl_destroy(cl_ctx* h) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     void* ptrs[] = {c->d_mask, c->d_ns_cls, c->d_ade_cls, c->d_f, c->d_u, c->d_g, c->d_imm, c->d_bio,
                     c->d_rho_adj, c->d_eq_iters, c->d_eq_x, c->d_phase, c->d_rel, c->d_counters, c->d_tracer,
-                    c->d_energy_part, c->d_scratch};
+                    c->d_energy_part, c->d_scratch, c->d_ca_total, c->d_ca_age, c->d_ca_distpos, c->d_ca_out};
     for (void* p : ptrs) if (p) cudaFree(p);
     for (int o = 0; o < CL_MAX_SRG_ORG; ++o) if (c->d_srg_params[o]) cudaFree(c->d_srg_params[o]);
     for (int k = 0; k < Ctx::kTimedKernels; ++k)
@@ -390,6 +405,7 @@ int cl_ade_init(cl_ctx* h) {
     int r = ade_init(c);
     if (r) return r;
     if ((r = phase_fill(c))) return r;
+    if ((r = ca_init(c))) return r;
     c->ade_ready = true;
     CL_CUDA(cudaStreamSynchronize(c->stream));
     return CL_OK;
@@ -541,6 +557,10 @@ int cl_get_field(cl_ctx* h, int32_t field, int32_t index, double* out) {
             if (!c->d_phase) { set_error("dissolution is not enabled in this context"); return CL_ERR_STATE; }
             u2d_kernel<<<blocks, 256, 0, c->stream>>>(c->d_phase, d, N);
             break;
+        case CL_FIELD_CA_AGE:
+        case CL_FIELD_CA_TOTAL:
+            if (!c->ade_ready) { set_error("call cl_ade_init first"); return CL_ERR_STATE; }
+            r = ca_field(c, field, d); break;
         default: set_error("unknown field"); return CL_ERR_ARG;
     }
     if (r) return r;
@@ -711,6 +731,18 @@ int cl_precip_convert(cl_ctx* h, int64_t* changed) {
 int cl_dissol_convert(cl_ctx* h, int64_t* changed) {
     if (!h || !changed) return CL_ERR_ARG;
     return dissol_convert(&h->c, changed);
+}
+
+int cl_ca_update_mask(cl_ctx* h, int64_t* mask_changes) {
+    if (!h) return CL_ERR_ARG;
+    if (!h->c.ade_ready) { set_error("call cl_ade_init first"); return CL_ERR_STATE; }
+    return ca_update_mask(&h->c, mask_changes);
+}
+
+int cl_ca_redistribute(cl_ctx* h, int32_t* sweeps, int64_t* mask_changes, double* bmax_after) {
+    if (!h) return CL_ERR_ARG;
+    if (!h->c.ade_ready) { set_error("call cl_ade_init first"); return CL_ERR_STATE; }
+    return ca_redistribute(&h->c, sweeps, mask_changes, bmax_after);
 }
 
 }  // extern "C"

@@ -1,5 +1,5 @@
-// dissolution.cu -- mineral release of the dissolvable phases (row a15,
-// surfaceDissolutionKinetics3D, src/dissolutionVOP.hh:265-435).
+// dissolution.cu -- mineral release of the dissolvable phases
+// (surfaceDissolutionKinetics3D, src/dissolutionVOP.hh:265-435).
 //
 // One thread per phase voxel in x = 1..nx-2.  Its open faces are the face
 // neighbours inside x = 1..nx-2 and inside y, z (no wrap) whose mask is not

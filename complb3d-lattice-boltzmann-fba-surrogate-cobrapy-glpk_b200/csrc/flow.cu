@@ -1,4 +1,4 @@
-// flow.cu -- D3Q19 incompressible BGK flow on the AA pattern (rows a1-a4).
+// flow.cu -- D3Q19 incompressible BGK flow on the AA pattern.
 //
 // Replaces Palabos IncBGKdynamics + collideAndStream as the reference drives it
 // (NSdomainSetup, src/complab_functions.hh:245-294; loops src/complab.cpp:596-695).

@@ -1,6 +1,6 @@
 // geometry.cu -- node classes from the mask, the dynamics switch after a mask
-// change, precipitation node conversion and the global reductions (rows a14,
-// a17).  All integer/byte work: results are bit-exact against the oracle.
+// change, precipitation node conversion and the global reductions.  All
+// integer/byte work: results are bit-exact against the oracle.
 #include "internal.h"
 
 namespace cl {

@@ -96,6 +96,13 @@ struct Ctx {
     float*   d_srg_params[CL_MAX_SRG_ORG] = {nullptr, nullptr};
     double*  d_eq_x = nullptr;       // n_comp*N previous converged log10 free components (NaN: none)
     uint8_t* d_phase = nullptr;      // N dissolvable phase id, 0 = none (dissolution only)
+    double*  d_ca_total = nullptr;   // N total biomass (cellular automaton)
+    int32_t* d_ca_age = nullptr;     // 2*N age wavefront, ping-pong
+    uint8_t* d_ca_distpos = nullptr; // N: the reference's distance field is positive (non-wall, not on a last index)
+    double*  d_ca_out = nullptr;     // 6*M*N outflow of each voxel per face and microbe in one sweep
+    uint64_t ca_sweeps = 0;          // sweeps run so far (the generator's counter)
+    int      ca_age_src = 0;         // age plane holding the current ages
+    int64_t  ca_mask_sum = -1;       // mask sum at the last check (complab.cpp old_totMask)
     double*  d_rel = nullptr;        // S*N this step's release of each phase voxel: products per open
                                      // face, and at the phase substrate the voxel's own decrement
     unsigned long long* d_counters = nullptr;  // [0] non-converged Newton solves
@@ -134,6 +141,10 @@ int dissol_convert(Ctx* c, int64_t* changed);
 int phase_seed(Ctx* c);          // grain phases from the mask (initPhaseLattice3D)
 int phase_fill(Ctx* c);          // grain inventories (initial_fill) after ade_init
 int refresh_flags(Ctx* c);       // class flags after a mask / phase change, dynamics kept
+int ca_init(Ctx* c);             // ages and the distance sign from the mask
+int ca_redistribute(Ctx* c, int32_t* sweeps, int64_t* mask_changes, double* bmax_after);
+int ca_update_mask(Ctx* c, int64_t* mask_changes);
+int ca_field(Ctx* c, int which, double* d_out);   // CL_FIELD_CA_AGE / CL_FIELD_CA_TOTAL into N doubles
 int update_dynamics(Ctx* c);
 int reduce_field(Ctx* c, const double* d_field, int op, double arg, const uint8_t* d_mask, double* out);
 

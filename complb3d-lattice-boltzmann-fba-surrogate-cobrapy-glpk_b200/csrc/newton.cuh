@@ -1,4 +1,4 @@
-// newton.cuh -- FP64 Newton speciation for one voxel per thread (rows a10-a12).
+// newton.cuh -- FP64 Newton speciation for one voxel per thread.
 //
 // Restates the Newton-Raphson reserve solver of the reference
 // (src/complab3d_processors_part4_eqsolver_NR_reserve.hh:512-615):

@@ -1,5 +1,4 @@
-// speciation.cu -- batched FP64 Newton speciation and its learned warm start
-// (rows a10, a11, a18).
+// speciation.cu -- batched FP64 Newton speciation and its learned warm start.
 //
 // Batch solve: one voxel per thread.  A warm start (given or learned) gets at
 // most warm_iter Newton iterations; voxels that have not converged by then are

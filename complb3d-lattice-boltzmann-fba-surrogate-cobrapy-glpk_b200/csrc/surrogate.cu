@@ -1,4 +1,4 @@
-// surrogate.cu -- batched per-voxel inference of the surrogate rate network (row a13).
+// surrogate.cu -- batched per-voxel inference of the surrogate rate network.
 //
 // The reference evaluates its exported feed-forward network one voxel at a
 // time with std::vector mat-vec loops (defineSurrogateModel,

@@ -10,8 +10,10 @@
 //   deltaP and a second solve (:641-669);
 //   solute relaxation and dt from the flow (:708-727), velocity coupling (:1096-1101);
 //   then per transport step: collide .. kinetics .. abiotic (+ dissolution) ..
-//   equilibrium .. stream (cl_step), and on their intervals the precipitation
-//   and dissolution node conversions with the dynamics switch, flow re-solve and
+//   equilibrium .. stream (cl_step); the cellular-automaton biomass
+//   redistribution (:1453-1715) with its dynamics switch and flow re-solve on a
+//   mask change (:1734-1780); on their intervals the precipitation and
+//   dissolution node conversions with the dynamics switch, flow re-solve and
 //   re-coupling (:1783-1845).
 // Fields are written as raw little-endian FP64 arrays in site order
 // n = (x*ny + y)*nz + z, one file per solute (and microbe) per output step,
@@ -196,14 +198,54 @@ int main(int argc, char** argv) {
         }
     }
 
+    long resolves = 0, ca_sweeps = 0, ca_blocks = 0, ca_changes = 0;
+    if (c.ca_enabled) {
+        // initial mask update from the seeded biomass, and on a change the
+        // dynamics switch and a flow re-solve (complab.cpp:1068-1091)
+        int64_t ch = 0;
+        if (!check(cl_ca_update_mask(h, &ch), "cl_ca_update_mask")) return 1;
+        ca_changes += ch;
+        if (ch > 0) {
+            if (!check(cl_update_dynamics(h), "cl_update_dynamics")) return 1;
+            if (run.Pe > kThrd) {
+                int it2 = 0;
+                if (!check(cl_flow_solve(h, (int32_t)run.ns_max1, run.ns_conv1, &it2), "cl_flow_solve")) return 1;
+                if (!check(cl_couple_velocity(h), "cl_couple_velocity")) return 1;
+                ++resolves;
+            }
+        }
+    }
+
     mkdir(run.output_dir.c_str(), 0777);
     std::vector<std::string> index;
-    long nonconv_steps = 0, precip_changes = 0, dissol_changes = 0, resolves = 0;
+    long nonconv_steps = 0, precip_changes = 0, dissol_changes = 0, steps_done = 0;
+    const char* stopped = "";
     const auto t1 = std::chrono::steady_clock::now();
     for (long iT = 0; iT < run.ade_max; ++iT) {
         st = cl_step(h, 1);
         if (!check(st, "cl_step")) return 1;
+        ++steps_done;
         if (st == CL_WARN_NOT_CONVERGED) ++nonconv_steps;
+        // CA biomass redistribution (complab.cpp:1453-1715)
+        bool ca_changed = false;
+        if (c.ca_enabled) {
+            int32_t sw = 0;
+            int64_t ch = 0;
+            double bm = 0.0;
+            st = cl_ca_redistribute(h, &sw, &ch, &bm);
+            if (!check(st, "cl_ca_redistribute")) return 1;
+            ca_sweeps += sw;
+            ca_blocks += sw > 0;
+            ca_changes += ch;
+            ca_changed = ch > 0;
+            if (st == CL_WARN_NOT_CONVERGED) {
+                // the reference writes every field and ends the run here
+                std::fprintf(stderr, "complab_b200: CA redistribution did not settle at iT=%ld (max biomass %g)\n", iT, bm);
+                stopped = "ca_not_settled";
+                if (!write_fields(h, run, iT, index)) return 1;
+                break;
+            }
+        }
         bool changed = false;
         if (c.precip_enabled && iT % run.precip_interval == 0) {
             int64_t ch = 0;
@@ -217,8 +259,14 @@ int main(int argc, char** argv) {
             dissol_changes += ch;
             changed = changed || ch > 0;
         }
-        if (changed && run.Pe > kThrd) {
+        // a CA mask change switches the dynamics on ade_update_interval and
+        // re-solves the flow on ns_update_interval (complab.cpp:1734-1780)
+        const bool ca_dyn = ca_changed && (iT % run.ade_update_interval == 0 || iT % run.ns_update_interval == 0);
+        const bool ca_ns = ca_changed && iT % run.ns_update_interval == 0;
+        if ((changed && run.Pe > kThrd) || ca_dyn) {
             if (!check(cl_update_dynamics(h), "cl_update_dynamics")) return 1;
+        }
+        if (run.Pe > kThrd && (changed || ca_ns)) {
             int it2 = 0;
             st = cl_flow_solve(h, (int32_t)run.ns_max2, run.ns_conv2, &it2);
             if (!check(st, "cl_flow_solve")) return 1;
@@ -228,7 +276,7 @@ int main(int argc, char** argv) {
         if (run.vtk_interval > 0 && iT % run.vtk_interval == 0 && !write_fields(h, run, iT, index)) return 1;
     }
     const auto t2 = std::chrono::steady_clock::now();
-    if (!write_fields(h, run, run.ade_max, index)) return 1;
+    if (!*stopped && !write_fields(h, run, run.ade_max, index)) return 1;
     {
         std::ofstream o(run.output_dir + "/fields.json");
         o << "{\"nx\": " << c.nx << ", \"ny\": " << c.ny << ", \"nz\": " << c.nz
@@ -242,9 +290,11 @@ int main(int argc, char** argv) {
     std::printf("{\"steps\": %ld, \"setup_s\": %.6f, \"loop_s\": %.6f, \"mlups\": %.3f, \"ns_iters\": %d, "
                 "\"pore_mean_u\": %.9g, \"max_ux\": %.9g, \"outlet_ux\": %.9g, \"delta_P\": %.9g, \"Pe_achieved\": %.6g, "
                 "\"dt\": %.9g, \"nonconverged_steps\": %ld, \"precip_changes\": %lld, \"dissol_changes\": %lld, "
-                "\"flow_resolves\": %ld, \"output\": \"%s\"}\n",
-                run.ade_max, setup_s, loop_s, loop_s > 0 ? sites * run.ade_max / loop_s / 1e6 : 0.0, ns_iters,
+                "\"ca_sweeps\": %ld, \"ca_blocks\": %ld, \"ca_mask_changes\": %ld, "
+                "\"flow_resolves\": %ld, \"stopped\": \"%s\", \"output\": \"%s\"}\n",
+                steps_done, setup_s, loop_s, loop_s > 0 ? sites * steps_done / loop_s / 1e6 : 0.0, ns_iters,
                 pore_mean_u, max_ux, outlet_ux, run.delta_P, pe_achieved, c.dt, nonconv_steps,
-                (long long)precip_changes, (long long)dissol_changes, resolves, run.output_dir.c_str());
-    return 0;
+                (long long)precip_changes, (long long)dissol_changes, ca_sweeps, ca_blocks, ca_changes,
+                resolves, stopped, run.output_dir.c_str());
+    return *stopped ? 3 : 0;
 }

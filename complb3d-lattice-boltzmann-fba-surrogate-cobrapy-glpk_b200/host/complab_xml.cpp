@@ -164,6 +164,8 @@ int read_complab_xml(const std::string& path, HostRun& run, std::string& err) {
             run.ns_conv1 = num_or(*it, {"ns_converge_iT1"}, 1e-8);
             run.ns_conv2 = num_or(*it, {"ns_converge_iT2"}, 1e-6);
             run.ade_max = (long)num_or(*it, {"ade_max_iT"}, 10000000);
+            run.ns_update_interval = std::max(1L, (long)num_or(*it, {"ns_update_interval"}, 1));
+            run.ade_update_interval = std::max(1L, (long)num_or(*it, {"ade_update_interval"}, 1));
         }
         run.vtk_interval = (long)num_or(P, {"IO", "save_VTK_interval"}, 0);
 
@@ -306,8 +308,34 @@ int read_complab_xml(const std::string& path, HostRun& run, std::string& err) {
             }
             if (c.n_phases == 0) throw std::runtime_error("<dissolution> is enabled but no <phase0> block was given");
         }
-        if (M > 0 && P.has("microbiology") && P["microbiology"].has("maximum_biomass_density"))
-            run.notes.push_back("cellular-automaton biomass redistribution is not part of this library: biomass stays where it grows");
+        // cellular automaton (complab_functions.hh:1167-1186): every microbe this
+        // driver accepts is CA-solved, so the CA runs whenever there is one;
+        // its material code is the first of its material numbers (bio_dynamics[m][0])
+        if (M > 0) {
+            const XmlNode& mic = P["microbiology"];
+            if (!mic.has("thrd_biofilm_fraction"))
+                throw std::runtime_error("thrd_biofilm_fraction must be defined when solver_type is Cellular Automata");
+            c.ca_thrd_frac = mic["thrd_biofilm_fraction"].num();
+            if (mic.has("maximum_biomass_density")) c.ca_bmax = mic["maximum_biomass_density"].num();
+            else if (M == 1)
+                throw std::runtime_error("maximum_biomass_density must be defined when solver_type is Cellular Automata");
+            else c.ca_bmax = 999999999.;
+            c.ca_half = 0;
+            if (mic.has("CA_method")) {
+                const std::string h = lower(mic["CA_method"].str());
+                if (h == "fraction" || h == "0" || h == "no") c.ca_half = 0;
+                else if (h == "half" || h == "1" || h == "yes") c.ca_half = 1;
+                else throw std::runtime_error("CA_method (" + h + ") should be either half or fraction");
+            }
+            for (int m = 0; m < M; ++m) {
+                if (run.bio_materials[m].empty())
+                    throw std::runtime_error("microbe" + std::to_string(m) + " has no material number for its biofilm");
+                c.microbe_code[m] = run.bio_materials[m][0];
+            }
+            // std::srand(time) in the reference; a fixed seed of the counter-based generator here
+            c.ca_seed = mic.has("ca_seed") ? (uint64_t)mic["ca_seed"].integer() : 1;
+            c.ca_enabled = 1;
+        }
         return 0;
     } catch (const std::exception& e) {
         err = e.what();
@@ -338,7 +366,8 @@ std::string run_json(const HostRun& r) {
     o << ", \"tau\": " << r.tau << ", \"delta_P\": " << r.delta_P << ", \"Pe\": " << r.Pe
       << ", \"charcs_length\": " << r.charcs_length << ", \"rho_out\": " << c.rho_out
       << ", \"ns_max_iT1\": " << r.ns_max1 << ", \"ns_converge_iT1\": " << r.ns_conv1
-      << ", \"ade_max_iT\": " << r.ade_max << ", \"n_solutes\": " << c.n_solutes << ", \"names\": [";
+      << ", \"ade_max_iT\": " << r.ade_max << ", \"ns_update_interval\": " << r.ns_update_interval
+      << ", \"ade_update_interval\": " << r.ade_update_interval << ", \"n_solutes\": " << c.n_solutes << ", \"names\": [";
     for (size_t i = 0; i < r.subs_names.size(); ++i) o << (i ? ", " : "") << "\"" << r.subs_names[i] << "\"";
     o << "], \"c0\": ";
     arr(c.c0, c.n_solutes);
@@ -366,7 +395,11 @@ std::string run_json(const HostRun& r) {
     o << ", \"precip_enabled\": " << c.precip_enabled << ", \"precip_substrate\": " << c.precip_substrate
       << ", \"max_precip_rho\": " << c.max_precip_rho << ", \"dissol_enabled\": " << c.dissol_enabled
       << ", \"n_phases\": " << c.n_phases << ", \"precip_phase_id\": " << c.precip_phase_id
-      << ", \"notes\": [";
+      << ", \"ca_enabled\": " << c.ca_enabled << ", \"ca_half\": " << c.ca_half
+      << ", \"ca_bmax\": " << c.ca_bmax << ", \"ca_thrd_frac\": " << c.ca_thrd_frac
+      << ", \"ca_seed\": " << c.ca_seed << ", \"microbe_code\": ";
+    iarr(c.microbe_code, c.n_microbes);
+    o << ", \"notes\": [";
     for (size_t i = 0; i < r.notes.size(); ++i) o << (i ? ", " : "") << "\"" << r.notes[i] << "\"";
     o << "]}";
     return o.str();

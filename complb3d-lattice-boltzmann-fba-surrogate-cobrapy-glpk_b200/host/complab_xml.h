@@ -23,6 +23,7 @@ struct HostRun {
     double dx = 0.0;                 // m, after the <unit> scaling
     double delta_P = 0.0, Pe = 0.0, tau = 0.8, charcs_length = 0.0;   // charcs_length in lattice units
     long ns_max1 = 100000, ns_max2 = 100000, ade_max = 10000000;
+    long ns_update_interval = 1, ade_update_interval = 1;   // geometry-change dynamics / flow updates
     double ns_conv1 = 1e-8, ns_conv2 = 1e-6;
     long vtk_interval = 0;
     // chemistry / microbiology

@@ -107,7 +107,7 @@ typedef struct {
     double  nu[CL_MAX_SOLUTES];
 } cl_phase;
 
-/* ---- surrogate reaction type (row a13) ----------------------------------------
+/* ---- surrogate reaction type ----------------------------------------
  * Feed-forward network with mapminmax scaling (reference defineSurrogateModel,
  * surrogateModel.hh:252-501).  Layers: widths[0] inputs ... widths[n_layers]
  * outputs; tanh on hidden layers, linear output. */
@@ -202,6 +202,16 @@ typedef struct {
     /* surrogate reaction type: organisms, networks uploaded by cl_set_surrogate */
     int32_t n_srg;
     cl_srg_organism srg[CL_MAX_SRG_ORG];
+    /* cellular-automaton biofilm: <microbiology> maximum_biomass_density,
+     * thrd_biofilm_fraction, CA_method; the biofilm material of each microbe
+     * (bio_dynamics[m][0]); the seed of the counter-based generator that stands
+     * for std::rand / std::random_shuffle */
+    int32_t ca_enabled;
+    int32_t ca_half;                   /* CA_method "half": halfPushExcessBiomass3D */
+    double  ca_bmax;
+    double  ca_thrd_frac;
+    int32_t microbe_code[CL_MAX_MICROBES];
+    uint64_t ca_seed;
 } cl_config;
 
 typedef struct cl_ctx cl_ctx;
@@ -222,7 +232,7 @@ int     cl_abi_sizes(int32_t* sizes, int32_t n);
 int cl_upload_mask(cl_ctx* ctx, const uint8_t* mask);
 int cl_download_mask(cl_ctx* ctx, uint8_t* mask);
 
-/* ---- flow (rows a1-a4) -------------------------------------------------------
+/* ---- flow -------------------------------------------------------------------
  * cl_flow_init:  initializeAtEquilibrium with the linear PressureGradient profile
  *                (src/complab_functions.hh:72-84,285-290).
  * cl_flow_steps: n collideAndStream steps (src/complab.cpp:607-620).
@@ -253,7 +263,7 @@ int cl_flow_velocity_stats(cl_ctx* ctx, double* pore_mean_u, double* max_ux, dou
 int cl_set_flow_pressure(cl_ctx* ctx, double rho_in, double rho_out);
 int cl_set_transport(cl_ctx* ctx, const double* omega_pore, const double* omega_bio, double dt);
 
-/* ---- transport step (rows a5-a12) ---------------------------------------------
+/* ---- transport step ----------------------------------------------------------
  * cl_ade_init: initializeAtEquilibrium(c0, u=0) for every solute
  *              (src/complab_functions.hh:334-336).
  * cl_step:     n transport steps in the reference's order (src/complab.cpp:1252-1374,
@@ -296,14 +306,41 @@ int cl_launch_count(const cl_ctx* ctx, int64_t* launches);
 /* network of the surrogate reaction type, slot 0..CL_MAX_SRG_ORG-1 (before cl_step) */
 int cl_set_surrogate(cl_ctx* ctx, int32_t slot, const cl_surrogate_net* net);
 
-/* ---- reductions (row a17) ----------------------------------------------------- */
+/* ---- cellular-automaton biofilm -------------------------------------
+ * One call is the CA block of the reference's step (src/complab.cpp:1453-1715):
+ * updateLocalMaskNtotalLattices3D, then while the biomass maximum exceeds
+ * ca_bmax: a push sweep (pushExcessBiomass3D / halfPushExcessBiomass3D,
+ * complab3d_processors_part1.hh:432-894), the mask / total update, and every
+ * 50 sweeps the age wavefront (updateAgeDistance3D, part2.hh:717-842) to a
+ * fixed point.  The push sweep runs on every over-full voxel at once: the
+ * totals that decide capacities are the sweep's starting values (as the
+ * reference reads its total lattice, updated only between sweeps), each
+ * voxel's outflows are gathered by its neighbours in a fixed order, and a
+ * counter-based hash of (seed, sweep, site) replaces std::rand.  *sweeps =
+ * push sweeps run, *mask_changes = sites whose mask changed; returns
+ * CL_WARN_NOT_CONVERGED when 100 sweeps bring no decrease of the maximum,
+ * when an age relaxation takes more than 1000 passes, or after 1001 sweeps
+ * (the reference ends the run there), and CL_ERR_DIVERGED on a non-finite
+ * biomass.  The ages start at cl_ade_init: -1 wall, 0 pore, 1 biofilm. */
+int cl_ca_redistribute(cl_ctx* ctx, int32_t* sweeps, int64_t* mask_changes, double* bmax_after);
+/* updateLocalMaskNtotalLattices3D alone: the initial mask update after the
+ * biomass is seeded (complab.cpp:1068-1076).  It also resets the mask-sum
+ * baseline: cl_ca_redistribute runs one age pass when the sum of the mask
+ * has moved since the last baseline (complab.cpp:1736-1739).  cl_ade_init
+ * sets the first baseline from the uploaded mask. */
+int cl_ca_update_mask(cl_ctx* ctx, int64_t* mask_changes);
+/* the age field (read) as FP64 */
+#define CL_FIELD_CA_AGE    7
+#define CL_FIELD_CA_TOTAL  8   /* total biomass the CA last computed */
+
+/* ---- reductions ----------------------------------------------------- */
 #define CL_RED_SUM   0
 #define CL_RED_MIN   1
 #define CL_RED_MAX   2
 #define CL_RED_COUNT_EQ 3          /* count of sites whose mask == (int)arg */
 int cl_reduce(cl_ctx* ctx, int32_t field, int32_t index, int32_t op, double arg, double* out);
 
-/* ---- geometry updates (rows a14-a15) --------------------------------------------
+/* ---- geometry updates --------------------------------------------
  * precipNodeConversion3D (src/precipitationVOP.hh:158-219; stamps
  * precip_phase_id on the voxels it seals) and dissolNodeConversion3D
  * (src/dissolutionVOP.hh:459-527; reopens to the first pore code).  *changed =
@@ -317,7 +354,7 @@ int cl_reduce(cl_ctx* ctx, int32_t field, int32_t index, int32_t op, double arg,
 int cl_precip_convert(cl_ctx* ctx, int64_t* changed);
 int cl_dissol_convert(cl_ctx* ctx, int64_t* changed);
 
-/* ---- speciation batch (rows a10-a11, a18) ------------------------------------
+/* ---- speciation batch ----------------------------------------------------------
  * One FP64 Newton solve per entry.  totals: n*n_comp component totals T_j.
  * logfree_io: n*n_comp log10 free component concentrations; on input the start
  *   used by CL_EQ_START_GIVEN, on output the solution.

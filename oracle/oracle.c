@@ -982,6 +982,295 @@ int64_t orc_dissol_convert(const cl_config* cfg, orc_state* st) {
     return changed;
 }
 
+/* ------------------------------------------------- cellular-automaton biofilm */
+/* The CA block of src/complab.cpp:1453-1715 and its processors:
+ *   updateLocalMaskNtotalLattices3D   complab3d_processors_part2.hh:71-212
+ *   pushExcessBiomass3D               complab3d_processors_part1.hh:433-660
+ *   halfPushExcessBiomass3D           complab3d_processors_part1.hh:662-894
+ *   updateAgeDistance3D               complab3d_processors_part2.hh:717-830
+ *   createAgeDomain3D                 complab3d_processors_part3.hh:350-370
+ * Two orders of the push sweep:
+ *   serial = 1: the reference's in-place traversal (x outer, z inner): a
+ *               voxel reads its own biomass as it stands, neighbours receive
+ *               their share at once, capacities come from the total lattice of
+ *               the sweep's start;
+ *   serial = 0: every voxel plans its outflows from the sweep's starting state,
+ *               then every voxel gathers its own outflows and its neighbours'
+ *               inflows in direction order -- the order the CUDA library runs.
+ * std::random_shuffle and std::rand become the splitmix64 hash of (seed,
+ * stream, site) below, in both orders.  The age passes read the previous
+ * ages (Jacobi) and the mask update reads the previous masks. */
+#define ORC_CA_THRD 1e-12
+static const int D6[6][3] = {{1,0,0},{-1,0,0},{0,1,0},{0,-1,0},{0,0,1},{0,0,-1}};
+
+static uint64_t ca_hash(uint64_t seed, uint64_t stream, uint64_t site) {
+    uint64_t z = seed ^ (stream * 0x9E3779B97F4A7C15ull) ^ (site * 0xD1B54A32D192ED03ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+static int ca_wall(const cl_config* c, int m) { return m == c->solid_code || m == c->bb_code; }
+static int ca_pore(const cl_config* c, int m) { return in_list(m, c->pore_codes, c->n_pore_codes); }
+
+void orc_ca_init(const cl_config* cfg, const uint8_t* mask, orc_ca* ca) {
+    const int nx = cfg->nx, ny = cfg->ny, nz = cfg->nz;
+    int64_t sum = 0;
+    for (int x = 0; x < nx; ++x) for (int y = 0; y < ny; ++y) for (int z = 0; z < nz; ++z) {
+        const int64_t n = site(cfg, x, y, z);
+        const int m = mask[n];
+        const int wall = ca_wall(cfg, m);
+        ca->age[n] = wall ? -1 : (ca_pore(cfg, m) ? 0 : 1);
+        ca->distpos[n] = (uint8_t)(!wall && x < nx - 1 && y < ny - 1 && z < nz - 1);
+        ca->total[n] = 0.0;
+        sum += m;
+    }
+    ca->sweeps = 0;
+    ca->mask_sum = sum;
+}
+
+/* updateLocalMaskNtotalLattices3D; returns sites whose mask changed, *sum = mask sum */
+static int64_t ca_mask_total(const cl_config* cfg, orc_state* st, orc_ca* ca, int64_t* sum) {
+    const int nx = cfg->nx, ny = cfg->ny, nz = cfg->nz, M = cfg->n_microbes;
+    const int64_t N = (int64_t)nx * ny * nz;
+    const double thrd_mass = cfg->ca_thrd_frac * cfg->ca_bmax;
+    uint8_t* nm = (uint8_t*)malloc((size_t)N);
+    int64_t changed = 0, s = 0;
+    for (int x = 0; x < nx; ++x) for (int y = 0; y < ny; ++y) for (int z = 0; z < nz; ++z) {
+        const int64_t n = site(cfg, x, y, z);
+        const int mk = st->mask[n];
+        int out = mk;
+        if (!ca_wall(cfg, mk)) {
+            double bmass = 0.0;
+            int newmask = 0;
+            for (int m = 0; m < M; ++m) {
+                const double bm = st->bio[(int64_t)m*N + n];
+                if (bm > ORC_CA_THRD) { bmass += bm; newmask += cfg->microbe_code[m]; }
+            }
+            if (fabs(bmass - ca->total[n]) > ORC_CA_THRD) ca->total[n] = bmass;
+            const int poreflag = ca_pore(cfg, mk);
+            if (!poreflag && bmass < thrd_mass) {
+                newmask = cfg->pore_codes[0];
+                if (cfg->n_pore_codes > 1) {
+                    for (int d = 0; d < 6; ++d) {
+                        const int ax = x + D6[d][0], ay = y + D6[d][1], az = z + D6[d][2];
+                        if (ax < 0 || ax >= nx || ay < 0 || ay >= ny || az < 0 || az >= nz) continue;
+                        const int q = st->mask[site(cfg, ax, ay, az)];
+                        if (!ca_wall(cfg, q) && ca_pore(cfg, q)) { newmask = q; break; }
+                    }
+                }
+                out = newmask;
+            } else if (poreflag && bmass >= thrd_mass && newmask > 0) {
+                out = newmask;
+            }
+        }
+        nm[n] = (uint8_t)out;
+        if (out != mk) ++changed;
+        s += out;
+    }
+    memcpy(st->mask, nm, (size_t)N);
+    free(nm);
+    if (sum) *sum = s;
+    return changed;
+}
+
+/* the neighbours a voxel may push to, in the reference's order +x -x +y -y +z -z:
+ * inside x = 1..nx-2 (bdryGap 1) and the y, z extent (no wrap), not a wall */
+static int ca_candidates(const cl_config* cfg, const uint8_t* mask, int x, int y, int z, int* dir, int64_t* q) {
+    int nc = 0;
+    for (int d = 0; d < 6; ++d) {
+        const int ax = x + D6[d][0], ay = y + D6[d][1], az = z + D6[d][2];
+        if (ax < 1 || ax > cfg->nx - 2 || ay < 0 || ay >= cfg->ny || az < 0 || az >= cfg->nz) continue;
+        const int64_t n = site(cfg, ax, ay, az);
+        if (ca_wall(cfg, mask[n])) continue;
+        dir[nc] = d; q[nc] = n; ++nc;
+    }
+    return nc;
+}
+
+/* one push sweep */
+static void ca_push(const cl_config* cfg, orc_state* st, orc_ca* ca, int serial) {
+    const int nx = cfg->nx, ny = cfg->ny, nz = cfg->nz, M = cfg->n_microbes;
+    const int64_t N = (int64_t)nx * ny * nz;
+    const int half = cfg->ca_half;
+    const double Bmax = cfg->ca_bmax;
+    const uint64_t sw = ca->sweeps;
+    if (!serial) memset(ca->out, 0, sizeof(double) * 6 * M * N);
+    for (int x = 1; x <= nx - 2; ++x) for (int y = 0; y < ny; ++y) for (int z = 0; z < nz; ++z) {
+        const int64_t n = site(cfg, x, y, z);
+        const int mk = st->mask[n];
+        if (ca_wall(cfg, mk) || (half && ca_pore(cfg, mk))) continue;
+        double bMt = ca->total[n];
+        if (!(bMt > Bmax)) continue;
+        double bMd = half ? bMt * 0.5 : bMt - Bmax;
+        if (!half && !(bMd > ORC_CA_THRD)) continue;
+        int dir[6]; int64_t q[6];
+        const int nc = ca_candidates(cfg, st->mask, x, y, z, dir, q);
+        if (nc == 0) continue;            /* boxed in: the excess stays */
+        double Bc[CL_MAX_MICROBES];
+        for (int m = 0; m < M; ++m) Bc[m] = st->bio[(int64_t)m*N + n];
+        int order[6];
+        for (int t = 0; t < nc; ++t) order[t] = t;
+        if (nc > 1) {
+            const uint64_t r = ca_hash(cfg->ca_seed, 2 * sw, (uint64_t)n);
+            for (int i = nc - 1; i > 0; --i) {
+                const int j = (int)((r >> (8 * i)) & 0xff) % (i + 1);
+                const int tmp = order[i]; order[i] = order[j]; order[j] = tmp;
+            }
+        }
+        int chk = 0;
+        for (int t = 0; t < nc; ++t) {
+            const int d = dir[order[t]];
+            const int64_t nb = q[order[t]];
+            const double nbrbMt = ca_pore(cfg, st->mask[nb]) ? 0.0 : ca->total[nb];
+            if (nbrbMt < Bmax) {
+                const double cap = Bmax - nbrbMt;
+                double partial = bMd;
+                if (bMd > cap) { partial = cap; bMd -= cap; }
+                else { bMd = 0.0; chk = 1; }
+                for (int m = 0; m < M; ++m) {
+                    const double cur = serial ? st->bio[(int64_t)m*N + n] : Bc[m];
+                    const double shove = cur / bMt * partial;
+                    if (shove > ORC_CA_THRD) {
+                        if (serial) { st->bio[(int64_t)m*N + n] -= shove; st->bio[(int64_t)m*N + nb] += shove; }
+                        else { Bc[m] -= shove; ca->out[((int64_t)d*M + m)*N + n] += shove; }
+                    }
+                }
+                bMt -= partial;
+            }
+            if (chk) break;
+        }
+        if (chk) continue;
+        /* the rest to one neighbour: the older-age side (age directed), else any */
+        int tl[6], nt = 0;
+        const int a0 = ca->age[n];
+        for (int t = 0; t < nc; ++t) {
+            const int a1 = ca->age[q[t]];
+            if (half ? a0 >= a1 : a0 > a1) tl[nt++] = t;
+        }
+        const uint64_t r = ca_hash(cfg->ca_seed, 2 * sw + 1, (uint64_t)n);
+        int pk;
+        if (nt > 1) pk = tl[r % (uint64_t)nt];
+        else if (nt == 1) pk = tl[0];
+        else pk = nc > 1 ? (int)(r % (uint64_t)nc) : 0;
+        for (int m = 0; m < M; ++m) {
+            const double cur = serial ? st->bio[(int64_t)m*N + n] : Bc[m];
+            const double shove = cur / bMt * bMd;
+            if (serial) { st->bio[(int64_t)m*N + n] -= shove; st->bio[(int64_t)m*N + q[pk]] += shove; }
+            else { Bc[m] -= shove; ca->out[((int64_t)dir[pk]*M + m)*N + n] += shove; }
+        }
+    }
+    if (serial) return;
+    for (int x = 0; x < nx; ++x) for (int y = 0; y < ny; ++y) for (int z = 0; z < nz; ++z) {
+        const int64_t n = site(cfg, x, y, z);
+        for (int m = 0; m < M; ++m) {
+            double b = st->bio[(int64_t)m*N + n];
+            for (int d = 0; d < 6; ++d) b -= ca->out[((int64_t)d*M + m)*N + n];
+            for (int d = 0; d < 6; ++d) {
+                const int wx = x - D6[d][0], wy = y - D6[d][1], wz = z - D6[d][2];
+                if (wx < 1 || wx > nx - 2 || wy < 0 || wy >= ny || wz < 0 || wz >= nz) continue;
+                b += ca->out[((int64_t)d*M + m)*N + site(cfg, wx, wy, wz)];
+            }
+            st->bio[(int64_t)m*N + n] = b;
+        }
+    }
+}
+
+/* one updateAgeDistance3D pass (Jacobi); returns voxels whose age changed */
+static int64_t ca_age_pass(const cl_config* cfg, orc_ca* ca) {
+    const int nx = cfg->nx, ny = cfg->ny, nz = cfg->nz;
+    const int64_t N = (int64_t)nx * ny * nz;
+    const double Bmax = cfg->ca_bmax;
+    int32_t* na = (int32_t*)malloc(sizeof(int32_t) * (size_t)N);
+    int64_t changed = 0;
+    for (int x = 0; x < nx; ++x) for (int y = 0; y < ny; ++y) for (int z = 0; z < nz; ++z) {
+        const int64_t n = site(cfg, x, y, z);
+        const int age = ca->age[n];
+        int out = age;
+        const double B = ca->total[n];
+        if (B > ORC_CA_THRD) {
+            int64_t qs[6]; int nq = 0;
+            for (int d = 0; d < 6; ++d) {
+                const int ax = x + D6[d][0], ay = y + D6[d][1], az = z + D6[d][2];
+                if (ax < 0 || ax >= nx || ay < 0 || ay >= ny || az < 0 || az >= nz) continue;
+                const int64_t q = site(cfg, ax, ay, az);
+                if (ca->distpos[q]) qs[nq++] = q;
+            }
+            if (age == 0) out = 1;
+            else if (age == 1 && (B - Bmax) > -ORC_CA_THRD) {
+                int upd = 1;
+                for (int t = 0; t < nq; ++t) if (ca->age[qs[t]] == 0) { upd = 0; break; }
+                if (upd) out = 2;
+            } else {
+                int count = 0;
+                for (int t = 0; t < nq; ++t)
+                    if (ca->age[qs[t]] >= age && (ca->total[qs[t]] - Bmax) > -ORC_CA_THRD) ++count;
+                if (count == nq) out = age + 1;
+            }
+        }
+        na[n] = out;
+        if (out != age) ++changed;
+    }
+    memcpy(ca->age, na, sizeof(int32_t) * (size_t)N);
+    free(na);
+    return changed;
+}
+
+static double ca_max_total(const cl_config* cfg, const orc_ca* ca) {
+    const int64_t N = (int64_t)cfg->nx * cfg->ny * cfg->nz;
+    double mx = ca->total[0];
+    for (int64_t n = 1; n < N; ++n) if (ca->total[n] > mx || isnan(ca->total[n])) mx = ca->total[n];
+    return mx;
+}
+
+int64_t orc_ca_update_mask(const cl_config* cfg, orc_state* st, orc_ca* ca) {
+    int64_t sum = 0;
+    const int64_t ch = ca_mask_total(cfg, st, ca, &sum);
+    ca->mask_sum = sum;
+    return ch;
+}
+
+int orc_ca_redistribute(const cl_config* cfg, orc_state* st, orc_ca* ca, int serial,
+                        int32_t* sweeps_out, int64_t* changes_out, double* bmax_after) {
+    const double Bmax = cfg->ca_bmax;
+    int64_t sum = 0;
+    int64_t changes = ca_mask_total(cfg, st, ca, &sum);
+    double gmax = ca_max_total(cfg, ca);
+    if (!isfinite(gmax)) return CL_ERR_DIVERGED;
+    int status = CL_OK, sweeps = 0;
+    if (gmax - Bmax > ORC_CA_THRD) {
+        double prev = gmax;
+        int stall = 0;
+        for (int64_t wc = 0; gmax - Bmax > ORC_CA_THRD; ++wc) {
+            ca_push(cfg, st, ca, serial);
+            ca->sweeps += 1;
+            ++sweeps;
+            changes += ca_mask_total(cfg, st, ca, &sum);
+            gmax = ca_max_total(cfg, ca);
+            if (gmax > prev - ORC_CA_THRD) { if (++stall >= 100) { status = CL_WARN_NOT_CONVERGED; break; } }
+            else stall = 0;
+            prev = gmax;
+            if (wc % 50 == 0) {
+                int64_t ch = 1;
+                int passes = 0;
+                while (ch != 0) {
+                    ch = ca_age_pass(cfg, ca);
+                    if (++passes > 1000) break;
+                }
+                if (ch != 0) { status = CL_WARN_NOT_CONVERGED; break; }
+            }
+            if (wc > 1000) { status = CL_WARN_NOT_CONVERGED; break; }
+        }
+    }
+    if (sum != ca->mask_sum) {
+        ca_age_pass(cfg, ca);
+        ca->mask_sum = sum;
+    }
+    if (sweeps_out) *sweeps_out = sweeps;
+    if (changes_out) *changes_out = changes;
+    if (bmax_after) *bmax_after = gmax;
+    return status;
+}
+
 /* ---------------------------------------------------------------- MLP (FP64) */
 static double gelu(double v) { return 0.5 * v * (1.0 + erf(v / sqrt(2.0))); }
 static double gelu_d(double v) {

@@ -84,6 +84,21 @@ void orc_rates(const cl_config* cfg, int abiotic, const double* C, const double*
 int64_t orc_precip_convert(const cl_config* cfg, orc_state* st);
 int64_t orc_dissol_convert(const cl_config* cfg, orc_state* st);
 
+/* ---- cellular-automaton biofilm -------------------------------------------- */
+typedef struct {
+    double*  total;    /* [N] total biomass */
+    int32_t* age;      /* [N] age wavefront */
+    uint8_t* distpos;  /* [N] distance field positive */
+    double*  out;      /* [6][M][N] outflows of one sweep (order serial = 0) */
+    uint64_t sweeps;
+    int64_t  mask_sum;
+} orc_ca;
+void    orc_ca_init(const cl_config* cfg, const uint8_t* mask, orc_ca* ca);
+int64_t orc_ca_update_mask(const cl_config* cfg, orc_state* st, orc_ca* ca);
+/* serial = 1: the reference's in-place traversal order; 0: plan then gather */
+int     orc_ca_redistribute(const cl_config* cfg, orc_state* st, orc_ca* ca, int serial,
+                            int32_t* sweeps, int64_t* mask_changes, double* bmax_after);
+
 /* ---- speciation ------------------------------------------------------------ */
 /* totals from species (calc_component_totals) */
 void orc_eq_totals(const cl_eq_system* sys, const double* species, double* totals);

@@ -59,6 +59,12 @@ def lib():
         _orc.orc_surrogate_forward.argtypes = [vp, vp, vp, ctypes.c_int64]
         _orc.orc_rates.restype = None
         _orc.orc_rates.argtypes = [vp, i, vp, vp, vp, vp]
+        _orc.orc_ca_init.restype = None
+        _orc.orc_ca_init.argtypes = [vp, vp, vp]
+        _orc.orc_ca_update_mask.restype = ctypes.c_int64
+        _orc.orc_ca_update_mask.argtypes = [vp, vp, vp]
+        _orc.orc_ca_redistribute.restype = i
+        _orc.orc_ca_redistribute.argtypes = [vp, vp, vp, i, vp, vp, vp]
     return _orc
 
 
@@ -75,6 +81,11 @@ class OrcState(ctypes.Structure):
                 ("bio", ctypes.c_void_p), ("u", ctypes.c_void_p), ("mask", ctypes.c_void_p),
                 ("ade_class", ctypes.c_void_p), ("rho_bc", ctypes.c_void_p), ("eq_iters", ctypes.c_void_p),
                 ("srg_nets", ctypes.c_void_p), ("phase", ctypes.c_void_p)]
+
+
+class OrcCa(ctypes.Structure):
+    _fields_ = [("total", ctypes.c_void_p), ("age", ctypes.c_void_p), ("distpos", ctypes.c_void_p),
+                ("out", ctypes.c_void_p), ("sweeps", ctypes.c_uint64), ("mask_sum", ctypes.c_int64)]
 
 
 def check_config_layout(cfg):
@@ -187,6 +198,27 @@ class Transport:
 
     def dissol_convert(self):
         return lib().orc_dissol_convert(ctypes.byref(self.cfg), ctypes.byref(self.st))
+
+    # cellular-automaton biofilm
+    def ca_init(self):
+        N, M = self.N, max(self.cfg.n_microbes, 1)
+        self.ca_total = np.zeros(N)
+        self.ca_age = np.zeros(N, np.int32)
+        self.ca_distpos = np.zeros(N, np.uint8)
+        self.ca_out = np.zeros(6 * M * N)
+        self.ca = OrcCa(_p(self.ca_total).value, _p(self.ca_age).value, _p(self.ca_distpos).value,
+                        _p(self.ca_out).value, 0, 0)
+        lib().orc_ca_init(ctypes.byref(self.cfg), _p(self.mask), ctypes.byref(self.ca))
+
+    def ca_update_mask(self):
+        return lib().orc_ca_update_mask(ctypes.byref(self.cfg), ctypes.byref(self.st), ctypes.byref(self.ca))
+
+    def ca_redistribute(self, serial=False):
+        """(status, sweeps, mask changes, biomass maximum) of one CA block."""
+        sw, ch, bm = ctypes.c_int32(0), ctypes.c_int64(0), ctypes.c_double(0)
+        st = lib().orc_ca_redistribute(ctypes.byref(self.cfg), ctypes.byref(self.st), ctypes.byref(self.ca),
+                                       1 if serial else 0, ctypes.byref(sw), ctypes.byref(ch), ctypes.byref(bm))
+        return st, sw.value, ch.value, bm.value
 
 
 def eq_batch(sys, totals, cold_species, x0=None, start=0):

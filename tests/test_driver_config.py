@@ -116,3 +116,88 @@ def test_defaults_and_errors(tmp_path):
     assert r.returncode == 1 and "ny" in r.stderr
     r = subprocess.run([DRIVER, str(tmp_path / "absent.xml"), "--print-config"], capture_output=True, text=True)
     assert r.returncode == 1
+
+
+CA_CASE = """<?xml version="1.0" ?>
+<!-- one CA-solved microbe on material 3, no kinetics: the biomass only moves -->
+<parameters>
+    <path><input_path>input</input_path><output_path>output</output_path></path>
+    <simulation_mode>
+        <biotic_mode>true</biotic_mode>
+        <enable_kinetics>{kin}</enable_kinetics>
+    </simulation_mode>
+    <LB_numerics>
+        <domain>
+            <nx>{nx}</nx><ny>{ny}</ny><nz>{nz}</nz>
+            <dx>10</dx><unit>um</unit>
+            <characteristic_length>80</characteristic_length>
+            <filename>geometry.dat</filename>
+            <material_numbers><pore>2</pore><solid>0</solid><bounce_back>1</bounce_back><microbe0>3</microbe0></material_numbers>
+        </domain>
+        <delta_P>0</delta_P>
+        <Peclet>0</Peclet>
+        <tau>0.8</tau>
+        <iteration>
+            <ade_max_iT>{steps}</ade_max_iT>
+            <ade_update_interval>1</ade_update_interval>
+        </iteration>
+    </LB_numerics>
+    <chemistry>
+        <number_of_substrates>1</number_of_substrates>
+        <substrate0>
+            <name_of_substrates>A</name_of_substrates>
+            <initial_concentration>0.1</initial_concentration>
+            <substrate_diffusion_coefficients><in_pore>1e-9</in_pore><in_biofilm>2e-10</in_biofilm></substrate_diffusion_coefficients>
+            <left_boundary_type>Dirichlet</left_boundary_type><left_boundary_condition>1.0</left_boundary_condition>
+            <right_boundary_type>Neumann</right_boundary_type><right_boundary_condition>0</right_boundary_condition>
+        </substrate0>
+    </chemistry>
+    <microbiology>
+        <number_of_microbes>1</number_of_microbes>
+        <thrd_biofilm_fraction>0.1</thrd_biofilm_fraction>
+        {bmax}
+        <CA_method>{method}</CA_method>
+        <ca_seed>99</ca_seed>
+        <microbe0>
+            <name_of_microbes>B</name_of_microbes>
+            <solver_type>CA</solver_type>
+            <initial_densities>{b0}</initial_densities>
+            <decay_coefficient>0</decay_coefficient>
+        </microbe0>
+    </microbiology>
+</parameters>
+"""
+
+
+def write_ca_case(tmp, mask, steps=6, method="fraction", b0=3.0, bmax=1.0, kinetics=False):
+    nx, ny, nz = mask.shape
+    os.makedirs(os.path.join(tmp, "input"), exist_ok=True)
+    xml = os.path.join(tmp, "CompLaB.xml")
+    bm = "" if bmax is None else "<maximum_biomass_density>%r</maximum_biomass_density>" % bmax
+    open(xml, "w").write(CA_CASE.format(nx=nx - 2, ny=ny, nz=nz, steps=steps, method=method, b0=b0, bmax=bm,
+                                        kin="true" if kinetics else "false"))
+    with open(os.path.join(tmp, "input", "geometry.dat"), "w") as f:
+        for x in range(1, nx - 1):
+            f.write("\n".join(str(int(v)) for v in mask[x].reshape(-1)) + "\n")
+    return xml
+
+
+@pytest.mark.skipif(not driver_available(), reason="host driver not built")
+def test_print_config_cellular_automaton(tmp_path):
+    import numpy as np
+    mask = np.full((12, 8, 8), 2, np.uint8)
+    mask[5, 4, 4] = 3
+    xml = write_ca_case(str(tmp_path), mask, method="half")
+    c = json.loads(subprocess.run([DRIVER, xml, "--print-config"], capture_output=True, text=True, check=True).stdout)
+    assert c["ca_enabled"] == 1 and c["ca_half"] == 1
+    assert c["ca_bmax"] == 1.0 and c["ca_thrd_frac"] == 0.1 and c["ca_seed"] == 99
+    assert c["microbe_code"] == [3] and c["bio"] == [3]
+    assert c["ns_update_interval"] == 1 and c["ade_update_interval"] == 1
+    # complab_functions.hh:1175-1186: Bmax is required for a single CA microbe,
+    # CA_method must be half or fraction
+    xml = write_ca_case(str(tmp_path), mask, bmax=None)
+    r = subprocess.run([DRIVER, xml, "--print-config"], capture_output=True, text=True)
+    assert r.returncode == 1 and "maximum_biomass_density" in r.stderr
+    xml = write_ca_case(str(tmp_path), mask, method="quarter")
+    r = subprocess.run([DRIVER, xml, "--print-config"], capture_output=True, text=True)
+    assert r.returncode == 1 and "CA_method" in r.stderr
