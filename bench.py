@@ -298,6 +298,64 @@ def speciation_bench(pkg, wl, stream, n_train=1 << 20, n_test=1 << 21):
 
 
 # ----------------------------------------------------------------- main arm
+def biotic_ca_bench(pkg, wl, stream, steps=20, warmup=3, shape=(128, 128, 128)):
+    """The biotic workload with the cellular-automaton biofilm: 128^3 sphere
+    pack (porosity 0.35, radii 5-10) in a duct with bounce-back walls on the
+    y / z faces and sealed pores filled, four solutes, dual-Monod kinetics,
+    biomass 10-50 on 2% of the wall-adjacent pore voxels, Bmax 100.  Each step
+    is the transport step and the CA block (its mask / total update and
+    maximum on every step; push sweeps when a voxel exceeds Bmax).  The CA
+    block is also timed on its own on the same state with the biomass scaled
+    x5, so that about half the colonies exceed Bmax and spread."""
+    import torch
+    nx, ny, nz = shape
+    mask = wl.walled_pack(nx, ny, nz, 0.35, 5.0, 10.0, seed=21)
+    cfg = wl.biotic_config(pkg, nx, ny, nz)
+    bio = wl.seed_biomass(mask, 22)
+    lat = pkg.Lattice(cfg, stream=stream)
+    lat.upload_mask(mask)
+    lat.flow_init()
+    lat.flow_steps(200)
+    lat.couple_velocity()
+    lat.ade_init()
+    lat.set_field(pkg.FIELD_BIOMASS, 0, bio)
+    lat.ca_update_mask()
+    for _ in range(warmup):
+        lat.step(1)
+        lat.ca_redistribute()
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * steps + 2)]
+    ev[0].record()
+    for i in range(steps):
+        lat.step(1)
+        ev[1 + 2 * i].record()
+        lat.ca_redistribute()
+        ev[2 + 2 * i].record()
+    ev[-1].record()
+    torch.cuda.synchronize()
+    ms = ev[0].elapsed_time(ev[-1])
+    ca_ms = sum(ev[1 + 2 * i].elapsed_time(ev[2 + 2 * i]) for i in range(steps))
+    N = mask.size
+    # one CA block with work: the seeded colonies at x5
+    b = lat.field(pkg.FIELD_BIOMASS, 0) * 5.0
+    lat.set_field(pkg.FIELD_BIOMASS, 0, b)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    st, sweeps, changes, bmax = lat.ca_redistribute()
+    e1.record()
+    torch.cuda.synchronize()
+    block_ms = e0.elapsed_time(e1)
+    over = int((b > cfg.ca_bmax).sum())
+    lat.close()
+    return {"workload": "biotic + CA: %dx%dx%d sphere pack, porosity 0.35, radii 5-10, walled duct, sealed pores "
+                        "filled; 4 solutes, dual Monod, "
+                        "biomass 10-50 on 2%% of wall-adjacent pore voxels, Bmax 100, fraction push" % shape,
+            "mlups": N * steps / (ms * 1e-3) / 1e6, "ms_per_step": ms / steps, "ca_ms_per_step": ca_ms / steps,
+            "ca_block": {"status": st, "voxels_over_bmax": over, "sweeps": sweeps, "mask_changes": changes,
+                         "ms": block_ms, "ms_per_sweep": block_ms / max(sweeps, 1), "max_after": bmax}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -307,6 +365,7 @@ def main():
     ap.add_argument("--no-speciation", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-biotic", action="store_true")
     ap.add_argument("--shape", default=None, help="override nx,ny,nz (development only)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -399,6 +458,8 @@ def main():
     lat.close()
     if rank == 0 and world == 1 and not args.no_speciation:
         out["speciation"] = speciation_bench(pkg, wl, stream)
+    if rank == 0 and world == 1 and not args.no_biotic:
+        out["biotic_ca"] = biotic_ca_bench(pkg, wl, stream)
     if rank == 0 and world == 1 and not args.no_cpu:
         cm, cdt, threads, sample = cpu_coupled(40)
         out["cpu_baseline"] = {"value": cm, "unit": "MLUPS", "cores": threads, "kind": "port", "sample": sample}

@@ -21,6 +21,7 @@
 // std::rand.  The age sweeps read the previous ages (Jacobi) and run to the
 // fixed point.
 #include <cmath>
+#include <cstring>
 #include "internal.h"
 
 namespace cl {
@@ -164,11 +165,13 @@ __global__ void ca_apply_kernel(CaK k) {
 }
 
 // updateLocalMaskNtotalLattices3D: total and reclassification, new masks into
-// mask_new (the pore relabel reads the neighbours' previous masks)
+// mask_new (the pore relabel reads the neighbours' previous masks).  Counters:
+// [0] masks changed, [1] sum of the new masks, [2] the largest total as the
+// bits of a non-negative double (their integer order is the numeric order).
 __global__ void ca_mask_total_kernel(CaK k) {
     const int64_t N = k.g.N;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    unsigned long long changed = 0, masksum = 0;
+    unsigned long long changed = 0, masksum = 0, maxbits = 0;
     for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < N; n += stride) {
         const int mk = k.mask[n];
         int newmask_out = mk;
@@ -198,6 +201,11 @@ __global__ void ca_mask_total_kernel(CaK k) {
                 newmask_out = newmask;
             }
         }
+        // the maximum covers every voxel, walls included (a sealed voxel keeps
+        // its last total, as the reference's total lattice does)
+        const double t = k.total[n];
+        const unsigned long long tb = (unsigned long long)__double_as_longlong(t);
+        if (t > 0.0 && tb > maxbits) maxbits = tb;
         k.mask_new[n] = (uint8_t)newmask_out;
         if (newmask_out != mk) ++changed;
         masksum += (unsigned long long)newmask_out;
@@ -205,10 +213,13 @@ __global__ void ca_mask_total_kernel(CaK k) {
     for (int o = 16; o > 0; o >>= 1) {
         changed += __shfl_down_sync(0xffffffffu, changed, o);
         masksum += __shfl_down_sync(0xffffffffu, masksum, o);
+        const unsigned long long mb = __shfl_down_sync(0xffffffffu, maxbits, o);
+        if (mb > maxbits) maxbits = mb;
     }
     if ((threadIdx.x & 31) == 0) {
         if (changed) atomicAdd(k.counter, changed);
         if (masksum) atomicAdd(k.counter + 1, masksum);
+        if (maxbits) atomicMax(k.counter + 2, maxbits);
     }
 }
 
@@ -300,8 +311,8 @@ static CaK make_cak(Ctx* c) {
     for (int m = 0; m < CL_MAX_MICROBES; ++m) k.code[m] = c->cfg.microbe_code[m];
     k.seed = c->cfg.ca_seed;
     k.sweep = c->ca_sweeps;
-    // two counters in the last doubles of scratch (N + 65536 doubles), clear of mask_new
-    k.counter = reinterpret_cast<unsigned long long*>(c->d_scratch + c->scratch_bytes / sizeof(double) - 2);
+    // three counters in the last doubles of scratch (N + 65536 doubles), clear of mask_new
+    k.counter = reinterpret_cast<unsigned long long*>(c->d_scratch + c->scratch_bytes / sizeof(double) - 3);
     return k;
 }
 
@@ -309,14 +320,14 @@ static int ca_blocks(const Ctx* c) { return grid_for(c->geo.N, 256, 148 * 16); }
 
 
 
-// launch one counting kernel and read its two counters back
+// launch one counting kernel and read its three counters back
 template <class F>
-static int counted(Ctx* c, const CaK& k, F launch, unsigned long long out[2]) {
-    CL_CUDA(cudaMemsetAsync(k.counter, 0, 2 * sizeof(unsigned long long), c->stream));
+static int counted(Ctx* c, const CaK& k, F launch, unsigned long long out[3]) {
+    CL_CUDA(cudaMemsetAsync(k.counter, 0, 3 * sizeof(unsigned long long), c->stream));
     launch();
     CL_LAUNCH_CHECK("ca kernel");
     c->launches += 1;
-    CL_CUDA(cudaMemcpyAsync(out, k.counter, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+    CL_CUDA(cudaMemcpyAsync(out, k.counter, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
     CL_CUDA(cudaStreamSynchronize(c->stream));
     return CL_OK;
 }
@@ -326,7 +337,7 @@ int ca_init(Ctx* c) {
     if (!c->d_ca_age) return CL_OK;
     c->ca_age_src = 1;                 // make_cak writes age_out = plane 0
     CaK k = make_cak(c);
-    unsigned long long h[2] = {0, 0};
+    unsigned long long h[3] = {0, 0, 0};
     int r = counted(c, k, [&] { ca_init_kernel<<<ca_blocks(c), 256, 0, c->stream>>>(k); }, h);
     if (r) return r;
     c->ca_age_src = 0;
@@ -337,22 +348,24 @@ int ca_init(Ctx* c) {
     return CL_OK;
 }
 
-// updateLocalMaskNtotalLattices3D over the lattice; *masksum = sum of the new masks
-static int mask_total(Ctx* c, int64_t* changes, int64_t* masksum) {
+// updateLocalMaskNtotalLattices3D over the lattice; *masksum = sum of the new
+// masks, *tmax = the largest total (computeMax of the total lattice)
+static int mask_total(Ctx* c, int64_t* changes, int64_t* masksum, double* tmax = nullptr) {
     CaK k = make_cak(c);
-    unsigned long long h[2] = {0, 0};
+    unsigned long long h[3] = {0, 0, 0};
     int r = counted(c, k, [&] { ca_mask_total_kernel<<<ca_blocks(c), 256, 0, c->stream>>>(k); }, h);
     if (r) return r;
     if (h[0]) CL_CUDA(cudaMemcpyAsync(c->d_mask, k.mask_new, c->geo.N, cudaMemcpyDeviceToDevice, c->stream));
     *changes += (int64_t)h[0];
     if (masksum) *masksum = (int64_t)h[1];
+    if (tmax) { double t; std::memcpy(&t, &h[2], sizeof t); *tmax = t; }
     return CL_OK;
 }
 
 // one updateAgeDistance3D pass; *changed = voxels whose age changed
 static int age_sweep(Ctx* c, int64_t* changed) {
     CaK k = make_cak(c);
-    unsigned long long h[2] = {0, 0};
+    unsigned long long h[3] = {0, 0, 0};
     int r = counted(c, k, [&] { ca_age_kernel<<<ca_blocks(c), 256, 0, c->stream>>>(k); }, h);
     if (r) return r;
     c->ca_age_src ^= 1;
@@ -374,10 +387,9 @@ int ca_update_mask(Ctx* c, int64_t* changes_out) {
 int ca_redistribute(Ctx* c, int32_t* sweeps_out, int64_t* changes_out, double* bmax_after) {
     if (!c->d_ca_age) { set_error("the cellular automaton is not enabled in this context"); return CL_ERR_STATE; }
     int64_t changes = 0, sum = 0;
-    int r = mask_total(c, &changes, &sum);
-    if (r) return r;
     double gmax = 0.0;
-    if ((r = reduce_field(c, c->d_ca_total, CL_RED_MAX, 0.0, nullptr, &gmax))) return r;
+    int r = mask_total(c, &changes, &sum, &gmax);
+    if (r) return r;
     if (!std::isfinite(gmax)) { set_error("cellular automaton: non-finite biomass"); return CL_ERR_DIVERGED; }
     int status = CL_OK, sweeps = 0;
     const double bmax = c->cfg.ca_bmax;
@@ -393,8 +405,7 @@ int ca_redistribute(Ctx* c, int32_t* sweeps_out, int64_t* changes_out, double* b
             c->launches += 2;
             c->ca_sweeps += 1;
             ++sweeps;
-            if ((r = mask_total(c, &changes, &sum))) return r;
-            if ((r = reduce_field(c, c->d_ca_total, CL_RED_MAX, 0.0, nullptr, &gmax))) return r;
+            if ((r = mask_total(c, &changes, &sum, &gmax))) return r;
             // complab.cpp:1696-1710: the reference ends the run when 100 sweeps
             // bring no decrease of the maximum, when the age relaxation takes
             // more than 1000 passes, or after 1001 sweeps

@@ -74,6 +74,31 @@ def mark_bounce_back(mat):
     return out
 
 
+def walled_pack(nx, ny, nz, porosity, rmin, rmax, seed):
+    """A sphere pack in a duct: bounce-back walls on the four y / z faces, and
+    every pore voxel that no face path links to the largest pore cluster made
+    solid.  The biofilm automaton moves biomass only across faces and relaxes
+    its age field over the reference's distance field, which is zero on the
+    last y and z index; a colony in a sealed pore, or on a last-index plane
+    whose only inner neighbour is solid, gets an age that never settles, and
+    the reference ends its run there.  This geometry has neither."""
+    mat = sphere_pack(nx, ny, nz, porosity, rmin, rmax, seed)
+    mat[:, 0, :] = mat[:, ny - 1, :] = MAT_BB
+    mat[:, :, 0] = mat[:, :, nz - 1] = MAT_BB
+    from scipy import ndimage
+    pore = (mat != MAT_SOLID) & (mat != MAT_BB)
+    lab, n = ndimage.label(pore)          # face connectivity
+    if n > 1:
+        sizes = np.bincount(lab.reshape(-1))
+        sizes[0] = 0
+        keep = int(np.argmax(sizes))
+        mat[pore & (lab != keep)] = MAT_SOLID
+    mat[mat == MAT_BB] = MAT_SOLID
+    mat[:, 0, :] = mat[:, ny - 1, :] = MAT_SOLID
+    mat[:, :, 0] = mat[:, :, nz - 1] = MAT_SOLID
+    return mark_bounce_back(mat)
+
+
 def channel(nx, ny, nz):
     """Plane channel: walls at y = 0 and y = ny-1 (bounce-back), pore between."""
     mat = np.full((nx, ny, nz), MAT_PORE, np.uint8)
@@ -160,6 +185,33 @@ def seed_biomass(mask, seed, frac=0.02, lo=10.0, hi=50.0):
     b = np.zeros(mask.shape)
     b[pick] = rng.uniform(lo, hi, int(pick.sum()))
     return b
+
+
+def biotic_config(pkg, nx, ny, nz, seed=2, bmax=100.0, thrd_frac=0.01, ca_seed=1):
+    """Biotic kinetics with the cellular-automaton biofilm: four solutes
+    (electron donor, O2, NO3-, product) with D3Q7 tau ~ U[0.6, 0.9]; one
+    sessile microbe (material 3) oxidising the donor by O2 or by NO3- with
+    dual-Monod rates, Vmax ~ U[1e-5, 1e-4] and Ks ~ U[1e-3, 1e-1] in lattice
+    units; the CA redistributes biomass above Bmax (fraction push)."""
+    rng = np.random.default_rng(seed)
+    taus = rng.uniform(0.6, 0.9, 4)
+    inlet = [0.1, 0.05, 0.03, 0.0]
+    c0 = [0.05, 0.02, 0.03, 0.0]
+    sol = [{"tau": float(taus[s]), "c0": c0[s], "left": "D", "left_value": inlet[s], "right": "N"} for s in range(4)]
+    cfg = pkg.make_config(nx, ny, nz, tau_ns=0.8, rho_in=1.001, rho_out=1.0, solutes=sol, microbes=1,
+                          pore_codes=(MAT_PORE,), bio_codes=(MAT_BIO,), dt=1.0)
+    cfg.enable_kinetics = 1
+    vmax = rng.uniform(1e-5, 1e-4, 2)
+    ks = rng.uniform(1e-3, 1e-1, 3)
+    pkg.add_rxn(cfg, microbe=0, k=float(vmax[0]), monod=[(0, float(ks[0])), (1, float(ks[1]))],
+                nu={0: -1.0, 1: -0.5, 3: 1.0}, yield_=0.3)
+    pkg.add_rxn(cfg, microbe=0, k=float(vmax[1]), monod=[(0, float(ks[0])), (2, float(ks[2]))],
+                nu={0: -1.0, 2: -0.8, 3: 1.0}, yield_=0.2)
+    cfg.decay[0] = 1e-6
+    cfg.ca_enabled, cfg.ca_half, cfg.ca_bmax, cfg.ca_thrd_frac = 1, 0, bmax, thrd_frac
+    cfg.microbe_code[0] = MAT_BIO
+    cfg.ca_seed = ca_seed
+    return cfg
 
 
 # solutes of the coupled workload

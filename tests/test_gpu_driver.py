@@ -92,6 +92,8 @@ def ca_channel(shape, seed, n_colonies):
         if mask[x, y, z] == 2:
             mask[x, y, z] = 3
             placed += 1
+    # the driver's inlet and outlet planes repeat the first and last slice
+    mask[0], mask[-1] = mask[1], mask[-2]
     return mask
 
 
