@@ -26,7 +26,8 @@
 
 namespace cl {
 
-constexpr double kCaThrd = 1e-12;        // COMPLAB_THRD
+constexpr double kCaThrd = 1e-12;        // thrd (src/complab3d_processors.hh:60): push and loop
+constexpr double kCaEps = 1e-14;         // COMPLAB_THRD (src/complab_functions.hh:64): mask, total, age
 
 // splitmix64 finaliser over (seed, stream, site)
 __host__ __device__ __forceinline__ uint64_t ca_hash(uint64_t seed, uint64_t stream, uint64_t site) {
@@ -180,9 +181,9 @@ __global__ void ca_mask_total_kernel(CaK k) {
             int newmask = 0;
             for (int m = 0; m < k.M; ++m) {
                 const double bm = k.bio[(int64_t)m * N + n];
-                if (bm > kCaThrd) { bmass += bm; newmask += k.code[m]; }
+                if (bm > kCaEps) { bmass += bm; newmask += k.code[m]; }
             }
-            if (fabs(bmass - k.total[n]) > kCaThrd) k.total[n] = bmass;
+            if (fabs(bmass - k.total[n]) > kCaEps) k.total[n] = bmass;
             const bool poreflag = ca_pore(k, mk);
             if (!poreflag && bmass < k.thrd_mass) {
                 newmask = k.pore[0];
@@ -232,7 +233,7 @@ __global__ void ca_age_kernel(CaK k) {
         const int age = k.age_in[n];
         int out_age = age;
         const double B = k.total[n];
-        if (B > kCaThrd) {
+        if (B > kCaEps) {
             int x, y, z;
             decode(k.g, n, x, y, z);
             int64_t qs[6];
@@ -244,14 +245,14 @@ __global__ void ca_age_kernel(CaK k) {
                 if (k.distpos[q]) qs[nq++] = q;
             }
             if (age == 0) out_age = 1;
-            else if (age == 1 && (B - k.bmax) > -kCaThrd) {
+            else if (age == 1 && (B - k.bmax) > -kCaEps) {
                 bool upd = true;
                 for (int t = 0; t < nq; ++t) if (k.age_in[qs[t]] == 0) { upd = false; break; }
                 if (upd) out_age = 2;
             } else {
                 int count = 0;
                 for (int t = 0; t < nq; ++t)
-                    if (k.age_in[qs[t]] >= age && (k.total[qs[t]] - k.bmax) > -kCaThrd) ++count;
+                    if (k.age_in[qs[t]] >= age && (k.total[qs[t]] - k.bmax) > -kCaEps) ++count;
                 if (count == nq) out_age = age + 1;
             }
         }

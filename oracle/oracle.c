@@ -989,18 +989,24 @@ int64_t orc_dissol_convert(const cl_config* cfg, orc_state* st) {
  *   halfPushExcessBiomass3D           complab3d_processors_part1.hh:662-894
  *   updateAgeDistance3D               complab3d_processors_part2.hh:717-830
  *   createAgeDomain3D                 complab3d_processors_part3.hh:350-370
- * Two orders of the push sweep:
- *   serial = 1: the reference's in-place traversal (x outer, z inner): a
- *               voxel reads its own biomass as it stands, neighbours receive
- *               their share at once, capacities come from the total lattice of
- *               the sweep's start;
- *   serial = 0: every voxel plans its outflows from the sweep's starting state,
- *               then every voxel gathers its own outflows and its neighbours'
- *               inflows in direction order -- the order the CUDA library runs.
- * std::random_shuffle and std::rand become the splitmix64 hash of (seed,
- * stream, site) below, in both orders.  The age passes read the previous
- * ages (Jacobi) and the mask update reads the previous masks. */
-#define ORC_CA_THRD 1e-12
+ * Two orders:
+ *   serial = 1: the reference's processors as they run on one block: in-place
+ *               traversals (x outer, z inner); a pushing voxel reads its own
+ *               biomass as it stands and its neighbours receive their share at
+ *               once, capacities come from the total lattice of the sweep's
+ *               start; the mask update and the age passes read what earlier
+ *               voxels of the same pass wrote.  std::random_shuffle and
+ *               std::rand draw, in call order, from ca_seq_next; the
+ *               reference's own processors run with the same draws in
+ *               oracle/ref/ca_harness.cpp, which pins this order;
+ *   serial = 0: the order the CUDA library runs: every voxel plans its
+ *               outflows from the sweep's starting state, then every voxel
+ *               gathers its own outflows and its neighbours' inflows in
+ *               direction order; the draws are the hash of (seed, stream,
+ *               site); the mask update reads the previous masks and the age
+ *               passes the previous ages (Jacobi). */
+#define ORC_CA_THRD 1e-12          /* thrd, src/complab3d_processors.hh:60 (push and loop); the
+                                      mask, total and age rules use COMPLAB_THRD */
 static const int D6[6][3] = {{1,0,0},{-1,0,0},{0,1,0},{0,-1,0},{0,0,1},{0,0,-1}};
 
 static uint64_t ca_hash(uint64_t seed, uint64_t stream, uint64_t site) {
@@ -1009,6 +1015,8 @@ static uint64_t ca_hash(uint64_t seed, uint64_t stream, uint64_t site) {
     z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
     return z ^ (z >> 31);
 }
+/* the sequential draws of the serial order (one per std::random_shuffle or std::rand call) */
+static uint64_t ca_seq_next(const cl_config* cfg, orc_ca* ca) { return ca_hash(cfg->ca_seed, ~0ull, ca->draws++); }
 static int ca_wall(const cl_config* c, int m) { return m == c->solid_code || m == c->bb_code; }
 static int ca_pore(const cl_config* c, int m) { return in_list(m, c->pore_codes, c->n_pore_codes); }
 
@@ -1025,15 +1033,16 @@ void orc_ca_init(const cl_config* cfg, const uint8_t* mask, orc_ca* ca) {
         sum += m;
     }
     ca->sweeps = 0;
+    ca->draws = 0;
     ca->mask_sum = sum;
 }
 
 /* updateLocalMaskNtotalLattices3D; returns sites whose mask changed, *sum = mask sum */
-static int64_t ca_mask_total(const cl_config* cfg, orc_state* st, orc_ca* ca, int64_t* sum) {
+static int64_t ca_mask_total(const cl_config* cfg, orc_state* st, orc_ca* ca, int64_t* sum, int serial) {
     const int nx = cfg->nx, ny = cfg->ny, nz = cfg->nz, M = cfg->n_microbes;
     const int64_t N = (int64_t)nx * ny * nz;
     const double thrd_mass = cfg->ca_thrd_frac * cfg->ca_bmax;
-    uint8_t* nm = (uint8_t*)malloc((size_t)N);
+    uint8_t* nm = serial ? st->mask : (uint8_t*)malloc((size_t)N);
     int64_t changed = 0, s = 0;
     for (int x = 0; x < nx; ++x) for (int y = 0; y < ny; ++y) for (int z = 0; z < nz; ++z) {
         const int64_t n = site(cfg, x, y, z);
@@ -1044,9 +1053,9 @@ static int64_t ca_mask_total(const cl_config* cfg, orc_state* st, orc_ca* ca, in
             int newmask = 0;
             for (int m = 0; m < M; ++m) {
                 const double bm = st->bio[(int64_t)m*N + n];
-                if (bm > ORC_CA_THRD) { bmass += bm; newmask += cfg->microbe_code[m]; }
+                if (bm > COMPLAB_THRD) { bmass += bm; newmask += cfg->microbe_code[m]; }
             }
-            if (fabs(bmass - ca->total[n]) > ORC_CA_THRD) ca->total[n] = bmass;
+            if (fabs(bmass - ca->total[n]) > COMPLAB_THRD) ca->total[n] = bmass;
             const int poreflag = ca_pore(cfg, mk);
             if (!poreflag && bmass < thrd_mass) {
                 newmask = cfg->pore_codes[0];
@@ -1067,8 +1076,7 @@ static int64_t ca_mask_total(const cl_config* cfg, orc_state* st, orc_ca* ca, in
         if (out != mk) ++changed;
         s += out;
     }
-    memcpy(st->mask, nm, (size_t)N);
-    free(nm);
+    if (!serial) { memcpy(st->mask, nm, (size_t)N); free(nm); }
     if (sum) *sum = s;
     return changed;
 }
@@ -1111,7 +1119,7 @@ static void ca_push(const cl_config* cfg, orc_state* st, orc_ca* ca, int serial)
         int order[6];
         for (int t = 0; t < nc; ++t) order[t] = t;
         if (nc > 1) {
-            const uint64_t r = ca_hash(cfg->ca_seed, 2 * sw, (uint64_t)n);
+            const uint64_t r = serial ? ca_seq_next(cfg, ca) : ca_hash(cfg->ca_seed, 2 * sw, (uint64_t)n);
             for (int i = nc - 1; i > 0; --i) {
                 const int j = (int)((r >> (8 * i)) & 0xff) % (i + 1);
                 const int tmp = order[i]; order[i] = order[j]; order[j] = tmp;
@@ -1147,11 +1155,18 @@ static void ca_push(const cl_config* cfg, orc_state* st, orc_ca* ca, int serial)
             const int a1 = ca->age[q[t]];
             if (half ? a0 >= a1 : a0 > a1) tl[nt++] = t;
         }
-        const uint64_t r = ca_hash(cfg->ca_seed, 2 * sw + 1, (uint64_t)n);
         int pk;
-        if (nt > 1) pk = tl[r % (uint64_t)nt];
-        else if (nt == 1) pk = tl[0];
-        else pk = nc > 1 ? (int)(r % (uint64_t)nc) : 0;
+        if (serial) {
+            /* std::rand() % n with std::rand = the low 31 bits of a draw */
+            if (nt > 1) pk = tl[(int)(ca_seq_next(cfg, ca) & 0x7fffffff) % nt];
+            else if (nt == 1) pk = tl[0];
+            else pk = nc > 1 ? (int)(ca_seq_next(cfg, ca) & 0x7fffffff) % nc : 0;
+        } else {
+            const uint64_t r = ca_hash(cfg->ca_seed, 2 * sw + 1, (uint64_t)n);
+            if (nt > 1) pk = tl[r % (uint64_t)nt];
+            else if (nt == 1) pk = tl[0];
+            else pk = nc > 1 ? (int)(r % (uint64_t)nc) : 0;
+        }
         for (int m = 0; m < M; ++m) {
             const double cur = serial ? st->bio[(int64_t)m*N + n] : Bc[m];
             const double shove = cur / bMt * bMd;
@@ -1175,19 +1190,20 @@ static void ca_push(const cl_config* cfg, orc_state* st, orc_ca* ca, int serial)
     }
 }
 
-/* one updateAgeDistance3D pass (Jacobi); returns voxels whose age changed */
-static int64_t ca_age_pass(const cl_config* cfg, orc_ca* ca) {
+/* one updateAgeDistance3D pass (Jacobi, or in place when serial); returns
+ * voxels whose age changed */
+static int64_t ca_age_pass(const cl_config* cfg, orc_ca* ca, int serial) {
     const int nx = cfg->nx, ny = cfg->ny, nz = cfg->nz;
     const int64_t N = (int64_t)nx * ny * nz;
     const double Bmax = cfg->ca_bmax;
-    int32_t* na = (int32_t*)malloc(sizeof(int32_t) * (size_t)N);
+    int32_t* na = serial ? ca->age : (int32_t*)malloc(sizeof(int32_t) * (size_t)N);
     int64_t changed = 0;
     for (int x = 0; x < nx; ++x) for (int y = 0; y < ny; ++y) for (int z = 0; z < nz; ++z) {
         const int64_t n = site(cfg, x, y, z);
         const int age = ca->age[n];
         int out = age;
         const double B = ca->total[n];
-        if (B > ORC_CA_THRD) {
+        if (B > COMPLAB_THRD) {
             int64_t qs[6]; int nq = 0;
             for (int d = 0; d < 6; ++d) {
                 const int ax = x + D6[d][0], ay = y + D6[d][1], az = z + D6[d][2];
@@ -1196,22 +1212,21 @@ static int64_t ca_age_pass(const cl_config* cfg, orc_ca* ca) {
                 if (ca->distpos[q]) qs[nq++] = q;
             }
             if (age == 0) out = 1;
-            else if (age == 1 && (B - Bmax) > -ORC_CA_THRD) {
+            else if (age == 1 && (B - Bmax) > -COMPLAB_THRD) {
                 int upd = 1;
                 for (int t = 0; t < nq; ++t) if (ca->age[qs[t]] == 0) { upd = 0; break; }
                 if (upd) out = 2;
             } else {
                 int count = 0;
                 for (int t = 0; t < nq; ++t)
-                    if (ca->age[qs[t]] >= age && (ca->total[qs[t]] - Bmax) > -ORC_CA_THRD) ++count;
+                    if (ca->age[qs[t]] >= age && (ca->total[qs[t]] - Bmax) > -COMPLAB_THRD) ++count;
                 if (count == nq) out = age + 1;
             }
         }
         na[n] = out;
         if (out != age) ++changed;
     }
-    memcpy(ca->age, na, sizeof(int32_t) * (size_t)N);
-    free(na);
+    if (!serial) { memcpy(ca->age, na, sizeof(int32_t) * (size_t)N); free(na); }
     return changed;
 }
 
@@ -1222,9 +1237,9 @@ static double ca_max_total(const cl_config* cfg, const orc_ca* ca) {
     return mx;
 }
 
-int64_t orc_ca_update_mask(const cl_config* cfg, orc_state* st, orc_ca* ca) {
+int64_t orc_ca_update_mask(const cl_config* cfg, orc_state* st, orc_ca* ca, int serial) {
     int64_t sum = 0;
-    const int64_t ch = ca_mask_total(cfg, st, ca, &sum);
+    const int64_t ch = ca_mask_total(cfg, st, ca, &sum, serial);
     ca->mask_sum = sum;
     return ch;
 }
@@ -1233,7 +1248,7 @@ int orc_ca_redistribute(const cl_config* cfg, orc_state* st, orc_ca* ca, int ser
                         int32_t* sweeps_out, int64_t* changes_out, double* bmax_after) {
     const double Bmax = cfg->ca_bmax;
     int64_t sum = 0;
-    int64_t changes = ca_mask_total(cfg, st, ca, &sum);
+    int64_t changes = ca_mask_total(cfg, st, ca, &sum, serial);
     double gmax = ca_max_total(cfg, ca);
     if (!isfinite(gmax)) return CL_ERR_DIVERGED;
     int status = CL_OK, sweeps = 0;
@@ -1244,7 +1259,7 @@ int orc_ca_redistribute(const cl_config* cfg, orc_state* st, orc_ca* ca, int ser
             ca_push(cfg, st, ca, serial);
             ca->sweeps += 1;
             ++sweeps;
-            changes += ca_mask_total(cfg, st, ca, &sum);
+            changes += ca_mask_total(cfg, st, ca, &sum, serial);
             gmax = ca_max_total(cfg, ca);
             if (gmax > prev - ORC_CA_THRD) { if (++stall >= 100) { status = CL_WARN_NOT_CONVERGED; break; } }
             else stall = 0;
@@ -1253,7 +1268,7 @@ int orc_ca_redistribute(const cl_config* cfg, orc_state* st, orc_ca* ca, int ser
                 int64_t ch = 1;
                 int passes = 0;
                 while (ch != 0) {
-                    ch = ca_age_pass(cfg, ca);
+                    ch = ca_age_pass(cfg, ca, serial);
                     if (++passes > 1000) break;
                 }
                 if (ch != 0) { status = CL_WARN_NOT_CONVERGED; break; }
@@ -1262,7 +1277,7 @@ int orc_ca_redistribute(const cl_config* cfg, orc_state* st, orc_ca* ca, int ser
         }
     }
     if (sum != ca->mask_sum) {
-        ca_age_pass(cfg, ca);
+        ca_age_pass(cfg, ca, serial);
         ca->mask_sum = sum;
     }
     if (sweeps_out) *sweeps_out = sweeps;

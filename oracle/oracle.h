@@ -92,10 +92,11 @@ typedef struct {
     double*  out;      /* [6][M][N] outflows of one sweep (order serial = 0) */
     uint64_t sweeps;
     int64_t  mask_sum;
+    uint64_t draws;    /* sequential draws taken (serial order) */
 } orc_ca;
 void    orc_ca_init(const cl_config* cfg, const uint8_t* mask, orc_ca* ca);
-int64_t orc_ca_update_mask(const cl_config* cfg, orc_state* st, orc_ca* ca);
-/* serial = 1: the reference's in-place traversal order; 0: plan then gather */
+/* serial = 1: the reference's in-place processor order; 0: plan then gather */
+int64_t orc_ca_update_mask(const cl_config* cfg, orc_state* st, orc_ca* ca, int serial);
 int     orc_ca_redistribute(const cl_config* cfg, orc_state* st, orc_ca* ca, int serial,
                             int32_t* sweeps, int64_t* mask_changes, double* bmax_after);
 

@@ -62,7 +62,7 @@ def lib():
         _orc.orc_ca_init.restype = None
         _orc.orc_ca_init.argtypes = [vp, vp, vp]
         _orc.orc_ca_update_mask.restype = ctypes.c_int64
-        _orc.orc_ca_update_mask.argtypes = [vp, vp, vp]
+        _orc.orc_ca_update_mask.argtypes = [vp, vp, vp, i]
         _orc.orc_ca_redistribute.restype = i
         _orc.orc_ca_redistribute.argtypes = [vp, vp, vp, i, vp, vp, vp]
     return _orc
@@ -85,7 +85,8 @@ class OrcState(ctypes.Structure):
 
 class OrcCa(ctypes.Structure):
     _fields_ = [("total", ctypes.c_void_p), ("age", ctypes.c_void_p), ("distpos", ctypes.c_void_p),
-                ("out", ctypes.c_void_p), ("sweeps", ctypes.c_uint64), ("mask_sum", ctypes.c_int64)]
+                ("out", ctypes.c_void_p), ("sweeps", ctypes.c_uint64), ("mask_sum", ctypes.c_int64),
+                ("draws", ctypes.c_uint64)]
 
 
 def check_config_layout(cfg):
@@ -207,11 +208,12 @@ class Transport:
         self.ca_distpos = np.zeros(N, np.uint8)
         self.ca_out = np.zeros(6 * M * N)
         self.ca = OrcCa(_p(self.ca_total).value, _p(self.ca_age).value, _p(self.ca_distpos).value,
-                        _p(self.ca_out).value, 0, 0)
+                        _p(self.ca_out).value, 0, 0, 0)
         lib().orc_ca_init(ctypes.byref(self.cfg), _p(self.mask), ctypes.byref(self.ca))
 
-    def ca_update_mask(self):
-        return lib().orc_ca_update_mask(ctypes.byref(self.cfg), ctypes.byref(self.st), ctypes.byref(self.ca))
+    def ca_update_mask(self, serial=False):
+        return lib().orc_ca_update_mask(ctypes.byref(self.cfg), ctypes.byref(self.st), ctypes.byref(self.ca),
+                                        1 if serial else 0)
 
     def ca_redistribute(self, serial=False):
         """(status, sweeps, mask changes, biomass maximum) of one CA block."""
@@ -301,3 +303,48 @@ def ref_abiotic_ex13(C, mask=2):
     sr = np.zeros(C.size)
     ref_lib().ref_abiotic_ex13(_p(C), C.size, mask, _p(sr))
     return sr
+
+
+class RefCa:
+    """The reference's own CA processors on one block (oracle/ref/ca_harness.cpp),
+    carrying the same state as Transport's CA arrays: mask, biomass, total,
+    age, the distance sign, the draw counter and the mask-sum baseline."""
+
+    def __init__(self, cfg, mask, bio, distpos, total=None, age=None, mask_sum=None):
+        lib_ = ref_lib()
+        if lib_ is None:
+            raise RuntimeError("oracle/_ref/libref.so is not built")
+        vp, i, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+        lib_.ref_ca_block.restype = i
+        lib_.ref_ca_block.argtypes = [i, i, i, i, i, d, d, i, i, vp, i, vp, ctypes.c_uint64, vp,
+                                      vp, vp, vp, vp, vp, vp, vp, vp, vp]
+        lib_.ref_ca_update_mask.restype = ctypes.c_longlong
+        lib_.ref_ca_update_mask.argtypes = [i, i, i, i, i, d, d, i, i, vp, i, vp, vp, vp, vp, vp, vp, vp]
+        self.lib, self.cfg = lib_, cfg
+        N = cfg.nx * cfg.ny * cfg.nz
+        M = cfg.n_microbes
+        self.mask = np.ascontiguousarray(mask, np.uint8).reshape(-1).copy()
+        self.bio = np.ascontiguousarray(bio, np.float64).reshape(-1)[:M * N].copy()
+        self.total = np.zeros(N) if total is None else np.array(total, np.float64).reshape(-1)
+        self.age = np.array(age, np.int32).reshape(-1) if age is not None else None
+        self.distpos = np.ascontiguousarray(distpos, np.uint8).reshape(-1).copy()
+        self.pore = np.array(list(cfg.pore_codes)[:cfg.n_pore_codes], np.int32)
+        self.codes = np.array(list(cfg.microbe_code)[:M], np.int32)
+        self.draws = ctypes.c_uint64(0)
+        self.mask_sum = ctypes.c_longlong(int(self.mask.astype(np.int64).sum()) if mask_sum is None else mask_sum)
+
+    def _head(self):
+        c = self.cfg
+        return (c.nx, c.ny, c.nz, c.n_microbes, c.ca_half, c.ca_bmax, c.ca_thrd_frac, c.solid_code, c.bb_code,
+                _p(self.pore), int(self.pore.size), _p(self.codes))
+
+    def update_mask(self):
+        return self.lib.ref_ca_update_mask(*self._head(), _p(self.mask), _p(self.bio), _p(self.total),
+                                           _p(self.age), _p(self.distpos), ctypes.byref(self.mask_sum))
+
+    def block(self):
+        sw, ch, gm = ctypes.c_int32(0), ctypes.c_longlong(0), ctypes.c_double(0)
+        st = self.lib.ref_ca_block(*self._head(), self.cfg.ca_seed, ctypes.byref(self.draws), _p(self.mask),
+                                   _p(self.bio), _p(self.total), _p(self.age), _p(self.distpos),
+                                   ctypes.byref(self.mask_sum), ctypes.byref(sw), ctypes.byref(ch), ctypes.byref(gm))
+        return st, sw.value, gm.value

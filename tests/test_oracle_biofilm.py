@@ -60,7 +60,7 @@ def test_mass_balance_and_cap(pkg, half, serial):
     # code while it stays above the threshold
     bm = t.bio.reshape(2, -1)
     was_pore = (mask.reshape(-1) == 2)
-    codes = 3 * (bm[0] > 1e-12) + 4 * (bm[1] > 1e-12)
+    codes = 3 * (bm[0] > 1e-14) + 4 * (bm[1] > 1e-14)
     want = np.where(tot >= 0.1 * BMAX, np.where(was_pore, codes, mask.reshape(-1)), 2)
     open_ = ~wall
     np.testing.assert_array_equal(t.mask[open_], want[open_])
@@ -135,3 +135,74 @@ def test_boxed_in_voxel_keeps_its_excess(pkg):
     assert st == 1 and sweeps == 1 and bmax == 2.5
     assert t.bio.reshape(n, n, n)[4, 4, 4] == 2.5
     assert t.ca_age.reshape(n, n, n)[4, 4, 4] > 1000
+
+
+def _pin_case(pkg, half, M, n_pore, seed):
+    """Dyadic biomass (exact in the reference's (d-1)/4, (d-1)/8 population
+    encoding) on a walled channel with cube grains and colonies away from the
+    x boundary planes.  With the half push both microbes get the same density:
+    a voxel at Bmax pushes half its biomass or nothing depending on the last
+    bit of its total, so shares that stop being dyadic would make the two
+    codes' rounding, not their logic, decide."""
+    nx, ny, nz = 16, 13, 11
+    rng = np.random.default_rng(seed)
+    pores = (2, 5) if n_pore == 2 else (2,)
+    mask = np.full((nx, ny, nz), 2, np.uint8)
+    if n_pore == 2:
+        mask[:, :, nz // 2:] = 5
+    for _ in range(6):
+        x, y, z = rng.integers(1, nx - 4), rng.integers(1, ny - 4), rng.integers(1, nz - 4)
+        mask[x:x + 2, y:y + 2, z:z + 2] = 0
+    mask[:, 0, :] = mask[:, ny - 1, :] = 1
+    mask[:, :, 0] = mask[:, :, nz - 1] = 1
+    cfg = pkg.make_config(nx, ny, nz, solutes=[{"tau": 0.8}], microbes=M, pore_codes=pores, bio_codes=(3, 4))
+    cfg.ca_enabled, cfg.ca_half, cfg.ca_bmax, cfg.ca_thrd_frac = 1, half, 1.0, 0.1
+    cfg.microbe_code[0] = 3
+    if M > 1:
+        cfg.microbe_code[1] = 4
+    cfg.ca_seed = 4321 + seed
+    bio = np.zeros((M, nx, ny, nz))
+    placed = 0
+    while placed < 10:
+        x, y, z = rng.integers(3, nx - 3), rng.integers(1, ny - 1), rng.integers(1, nz - 1)
+        if mask[x, y, z] in (2, 5):
+            mask[x, y, z] = 3
+            v = rng.integers(1, 48) / 8.0
+            for m in range(M):
+                bio[m, x, y, z] = v if half else rng.integers(1, 48) / 8.0
+            placed += 1
+    return cfg, mask, bio
+
+
+@pytest.mark.parametrize("half,M,n_pore", [(0, 1, 1), (1, 1, 1), (0, 2, 1), (1, 2, 1), (0, 1, 2)])
+def test_serial_order_matches_the_reference_processors(pkg, half, M, n_pore):
+    """The oracle's serial order against the reference's own
+    updateLocalMaskNtotalLattices3D / push / updateAgeDistance3D processors,
+    compiled from its sources and run on one block with the same draws: the
+    same sweeps, masks and ages, and biomass equal to 1e-13 (the reference
+    keeps biomass as seven populations, which round differently from one
+    FP64 value once shares stop being dyadic)."""
+    if o.ref_lib() is None:
+        pytest.skip("reference tree absent: oracle/_ref not built")
+    cfg, mask, bio = _pin_case(pkg, half, M, n_pore, seed=3 * half + M + 5 * n_pore)
+    t = seeded(cfg, mask, bio)
+    r = o.RefCa(cfg, mask, bio, t.ca_distpos, total=t.ca_total, age=t.ca_age, mask_sum=int(t.ca.mask_sum))
+    assert t.ca_update_mask(serial=True) == r.update_mask()
+    rng = np.random.default_rng(11)
+    for block in range(3):
+        st, sweeps, _, gmax = t.ca_redistribute(serial=True)
+        rst, rsweeps, rgmax = r.block()
+        assert (st, sweeps) == (rst, rsweeps), block
+        assert sweeps > 0
+        assert gmax == pytest.approx(rgmax, rel=1e-13)
+        np.testing.assert_array_equal(t.mask, r.mask)
+        np.testing.assert_array_equal(t.ca_age, r.age)
+        np.testing.assert_allclose(t.bio[:M * t.N], r.bio, rtol=1e-13, atol=1e-13)
+        np.testing.assert_allclose(t.ca_total, r.total, rtol=1e-13, atol=1e-13)
+        assert t.ca.draws == r.draws.value
+        # dyadic growth between blocks, the same on both sides
+        g = rng.integers(9, 16, size=t.N) / 8.0
+        for m in range(M):
+            b = t.biomass(m) * g
+            t.set_biomass(m, b)
+            r.bio[m * t.N:(m + 1) * t.N] = b
