@@ -775,54 +775,15 @@ static int vox_equilibrium(const rx_ctx* r, int64_t n) {
     return 0;
 }
 
-/* One transport step in the order of src/complab.cpp:1252-1374,1849-1857:
- *   collide (mobile solutes; boundary cells complete their unknown population
- *   from the prescribed density first) -> run_kinetics -> update_rxnLattices ->
- *   dC reset -> run_abiotic_kinetics | surfaceAbioticKinetics3D ->
- *   update_abiotic_rxnLattices -> run_equilibrium_biotic -> stream ->
- *   FlatAdiabaticBoundaryFunctional3D on zero-gradient faces. */
-int64_t orc_transport_step(const cl_config* cfg, orc_state* st) {
+/* The reaction stage of a transport step, between collide and stream
+ * (src/complab.cpp:1264-1374): run_kinetics -> update_rxnLattices -> dC reset
+ * -> run_abiotic_kinetics | surfaceAbioticKinetics3D (+ surfaceDissolutionKinetics3D)
+ * -> update_abiotic_rxnLattices -> run_equilibrium_biotic.  Returns the
+ * number of Newton solves that did not converge. */
+int64_t orc_reaction_stage(const cl_config* cfg, orc_state* st) {
     const int nx = cfg->nx, ny = cfg->ny, nz = cfg->nz, S = cfg->n_solutes, M = cfg->n_microbes;
-    const int64_t N = (int64_t)nx * ny * nz, P = (int64_t)ny * nz;
+    const int64_t N = (int64_t)nx * ny * nz;
     int64_t nonconv = 0;
-    double* g = st->g;
-
-    /* ---- collide (AdvectionDiffusionBGKdynamics, BounceBack, NoDynamics) ---- */
-    #pragma omp parallel for collapse(2) schedule(static)
-    for (int x = 0; x < nx; ++x)
-        for (int y = 0; y < ny; ++y)
-            for (int z = 0; z < nz; ++z) {
-                int64_t n = site(cfg, x, y, z);
-                int cls = st->ade_class[n];
-                for (int s = 0; s < S; ++s) {
-                    if (cfg->immobile[s]) continue;
-                    double gi[7];
-                    for (int i = 0; i < 7; ++i) gi[i] = g[(s*7 + i)*N + n];
-                    if (cls == ORC_NODYN) continue;
-                    if (cls == ORC_BB) {
-                        for (int i = 0; i < 7; ++i) g[(s*7 + i)*N + n] = gi[opp7(i)];
-                        continue;
-                    }
-                    if (x == 0 || x == nx - 1) {
-                        /* AdvectionDiffusionBoundaryDynamics: the one unknown population
-                         * (entering through the face) = prescribed rho - sum of the others */
-                        int unk = (x == 0) ? 4 : 1;
-                        double rb = st->rho_bc[(s*2 + (x == 0 ? 0 : 1))*P + (int64_t)y*nz + z];
-                        double sum = 0; for (int i = 0; i < 7; ++i) if (i != unk) sum += gi[i];
-                        gi[unk] = rb - sum;
-                    }
-                    double om = (cls == ORC_BIO) ? cfg->omega_bio[s] : cfg->omega_pore[s];
-                    double rho = 0; for (int i = 0; i < 7; ++i) rho += gi[i];
-                    double ux = st->u[n], uy = st->u[N + n], uz = st->u[2*N + n];
-                    for (int i = 0; i < 7; ++i) {
-                        double cu = C7[i][0]*ux + C7[i][1]*uy + C7[i][2]*uz;
-                        double geq = T7[i] * rho * (1.0 + 4.0*cu);
-                        g[(s*7 + i)*N + n] = gi[i] - om*(gi[i] - geq);
-                    }
-                }
-            }
-
-    /* ---- reactions ---- */
     int n_bio = 0, n_abio = 0;
     for (int k = 0; k < cfg->n_rxn; ++k) { if (cfg->rxn[k].microbe >= 0) ++n_bio; else ++n_abio; }
     rx_ctx rc;
@@ -902,6 +863,59 @@ int64_t orc_transport_step(const cl_config* cfg, orc_state* st) {
                     }
         }
     }
+
+    return nonconv;
+}
+
+/* One transport step in the order of src/complab.cpp:1252-1374,1849-1857:
+ *   collide (mobile solutes; boundary cells complete their unknown population
+ *   from the prescribed density first) -> run_kinetics -> update_rxnLattices ->
+ *   dC reset -> run_abiotic_kinetics | surfaceAbioticKinetics3D ->
+ *   update_abiotic_rxnLattices -> run_equilibrium_biotic -> stream ->
+ *   FlatAdiabaticBoundaryFunctional3D on zero-gradient faces. */
+int64_t orc_transport_step(const cl_config* cfg, orc_state* st) {
+    const int nx = cfg->nx, ny = cfg->ny, nz = cfg->nz, S = cfg->n_solutes, M = cfg->n_microbes;
+    const int64_t N = (int64_t)nx * ny * nz, P = (int64_t)ny * nz;
+    int64_t nonconv = 0;
+    double* g = st->g;
+
+    /* ---- collide (AdvectionDiffusionBGKdynamics, BounceBack, NoDynamics) ---- */
+    #pragma omp parallel for collapse(2) schedule(static)
+    for (int x = 0; x < nx; ++x)
+        for (int y = 0; y < ny; ++y)
+            for (int z = 0; z < nz; ++z) {
+                int64_t n = site(cfg, x, y, z);
+                int cls = st->ade_class[n];
+                for (int s = 0; s < S; ++s) {
+                    if (cfg->immobile[s]) continue;
+                    double gi[7];
+                    for (int i = 0; i < 7; ++i) gi[i] = g[(s*7 + i)*N + n];
+                    if (cls == ORC_NODYN) continue;
+                    if (cls == ORC_BB) {
+                        for (int i = 0; i < 7; ++i) g[(s*7 + i)*N + n] = gi[opp7(i)];
+                        continue;
+                    }
+                    if (x == 0 || x == nx - 1) {
+                        /* AdvectionDiffusionBoundaryDynamics: the one unknown population
+                         * (entering through the face) = prescribed rho - sum of the others */
+                        int unk = (x == 0) ? 4 : 1;
+                        double rb = st->rho_bc[(s*2 + (x == 0 ? 0 : 1))*P + (int64_t)y*nz + z];
+                        double sum = 0; for (int i = 0; i < 7; ++i) if (i != unk) sum += gi[i];
+                        gi[unk] = rb - sum;
+                    }
+                    double om = (cls == ORC_BIO) ? cfg->omega_bio[s] : cfg->omega_pore[s];
+                    double rho = 0; for (int i = 0; i < 7; ++i) rho += gi[i];
+                    double ux = st->u[n], uy = st->u[N + n], uz = st->u[2*N + n];
+                    for (int i = 0; i < 7; ++i) {
+                        double cu = C7[i][0]*ux + C7[i][1]*uy + C7[i][2]*uz;
+                        double geq = T7[i] * rho * (1.0 + 4.0*cu);
+                        g[(s*7 + i)*N + n] = gi[i] - om*(gi[i] - geq);
+                    }
+                }
+            }
+
+    /* ---- reactions ---- */
+    nonconv += orc_reaction_stage(cfg, st);
 
     /* ---- stream (push, periodic y/z, reflect at x faces) ---- */
     for (int s = 0; s < S; ++s) {

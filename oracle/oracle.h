@@ -72,6 +72,8 @@ typedef struct {
 void orc_ade_init(const cl_config* cfg, orc_state* st);
 /* one transport step; returns the number of Newton solves that did not converge */
 int64_t orc_transport_step(const cl_config* cfg, orc_state* st);
+/* its reaction stage alone (kinetics .. equilibrium on the current densities) */
+int64_t orc_reaction_stage(const cl_config* cfg, orc_state* st);
 /* solute density of every site (mobile: sum of g; immobile: inventory) */
 void orc_solute_density(const cl_config* cfg, const orc_state* st, int s, double* out);
 

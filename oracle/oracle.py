@@ -43,6 +43,8 @@ def lib():
         _orc.orc_flow_solve.argtypes = [vp, vp, vp, vp, i, d, vp]
         _orc.orc_transport_step.restype = ctypes.c_int64
         _orc.orc_transport_step.argtypes = [vp, vp]
+        _orc.orc_reaction_stage.restype = ctypes.c_int64
+        _orc.orc_reaction_stage.argtypes = [vp, vp]
         _orc.orc_precip_convert.restype = ctypes.c_int64
         _orc.orc_precip_convert.argtypes = [vp, vp]
         _orc.orc_dissol_convert.restype = ctypes.c_int64
@@ -197,6 +199,10 @@ class Transport:
     def precip_convert(self):
         return lib().orc_precip_convert(ctypes.byref(self.cfg), ctypes.byref(self.st))
 
+    def reaction_stage(self):
+        """The reaction stage of a step alone (no collide, no stream)."""
+        return lib().orc_reaction_stage(ctypes.byref(self.cfg), ctypes.byref(self.st))
+
     def dissol_convert(self):
         return lib().orc_dissol_convert(ctypes.byref(self.cfg), ctypes.byref(self.st))
 
@@ -348,3 +354,88 @@ class RefCa:
                                    _p(self.bio), _p(self.total), _p(self.age), _p(self.distpos),
                                    ctypes.byref(self.mask_sum), ctypes.byref(sw), ctypes.byref(ch), ctypes.byref(gm))
         return st, sw.value, gm.value
+
+
+_rxn = {}
+
+
+def rxn_lib(variant):
+    """The reference's reaction processors on one block (oracle/ref/rxn_harness.cpp):
+    variant 13 binds the rate laws of examples 05 + 13, variant 14 those of 05 + 14.
+    None when the reference tree was absent at build time."""
+    if variant not in _rxn:
+        path = os.path.join(HERE, "_ref", "librxn%d.so" % variant)
+        if not os.path.exists(path):
+            return None
+        L = ctypes.CDLL(path)
+        vp, i, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+        L.ref_rxn_stage.restype = i
+        L.ref_rxn_stage.argtypes = [i, i, i, i, i, d, i, i, i, vp, vp, vp, vp,
+                                    i, vp, vp, vp, vp, vp, d, i, vp, i,
+                                    i, vp, vp, vp, i, d, i]
+        L.ref_precip_convert.restype = ctypes.c_longlong
+        L.ref_precip_convert.argtypes = [i, i, i, vp, d, i, i, i, i, vp, vp]
+        L.ref_dissol_convert.restype = ctypes.c_longlong
+        L.ref_dissol_convert.argtypes = [i, i, i, i, vp, i, i, i, i, vp, vp, vp, vp, vp, d, vp, vp]
+        _rxn[variant] = L
+    return _rxn[variant]
+
+
+RXN_KINETICS, RXN_ABIOTIC, RXN_SURFACE, RXN_DISSOLUTION, RXN_EQUILIBRIUM = 1, 2, 4, 8, 16
+
+
+def _phase_arrays(cfg):
+    n = cfg.n_phases
+    ids = np.array([cfg.phases[k].id for k in range(n)] or [0], np.int32)
+    mat = np.array([cfg.phases[k].material for k in range(n)] or [0], np.int32)
+    sub = np.array([cfg.phases[k].substrate for k in range(n)] or [0], np.int32)
+    full = np.array([cfg.phases[k].full_density for k in range(n)] or [0.0])
+    prec = np.array([cfg.phases[k].is_precipitate for k in range(n)] or [0], np.int32)
+    return n, ids, mat, sub, full, prec
+
+
+def ref_rxn_stage(variant, cfg, mask, phase, C, B, flags, eq_depth=4):
+    """Run the reference's reaction stage on densities C (S x N) and biomass
+    B (M x N); returns the new (C, B)."""
+    L = rxn_lib(variant)
+    N = cfg.nx * cfg.ny * cfg.nz
+    S, M = cfg.n_solutes, cfg.n_microbes
+    C = np.array(C, np.float64).reshape(S, N).copy()
+    B = np.array(B, np.float64).reshape(max(M, 1), N)[:max(M, 1)].copy()
+    mask = np.ascontiguousarray(mask, np.uint8).reshape(-1)
+    phase = np.ascontiguousarray(phase if phase is not None else np.zeros(N), np.uint8).reshape(-1)
+    n, ids, mat, sub, full, prec = _phase_arrays(cfg)
+    pore = np.array(list(cfg.pore_codes)[:cfg.n_pore_codes], np.int32)
+    e = cfg.eq
+    nc = e.n_comp
+    stoich = np.array([[e.stoich[i][j] for j in range(nc)] for i in range(S)] if nc else [[0.0]], np.float64)
+    logk = np.array([e.logk[i] for i in range(S)], np.float64)
+    cs = np.array([e.comp_species[j] for j in range(max(nc, 1))], np.int32)
+    L.ref_rxn_stage(cfg.nx, cfg.ny, cfg.nz, S, M, cfg.dt, cfg.solid_code, cfg.bb_code, flags,
+                    _p(mask), _p(phase), _p(C), _p(B), n, _p(ids), _p(mat), _p(sub), _p(full), _p(prec),
+                    cfg.reopen_fraction, cfg.dissol_surface_only, _p(pore), int(pore.size),
+                    nc, _p(stoich), _p(logk), _p(cs), e.max_iter, e.tol, eq_depth)
+    return C, B
+
+
+def ref_precip_convert(cfg, P, mask, phase):
+    L = rxn_lib(13)
+    mask = np.ascontiguousarray(mask, np.uint8).reshape(-1).copy()
+    phase = np.ascontiguousarray(phase, np.uint8).reshape(-1).copy()
+    P = np.ascontiguousarray(P, np.float64).reshape(-1)
+    ch = L.ref_precip_convert(cfg.nx, cfg.ny, cfg.nz, _p(P), cfg.max_precip_rho, cfg.solid_code, cfg.bb_code,
+                              cfg.precip_code, cfg.precip_phase_id, _p(mask), _p(phase))
+    return ch, mask, phase
+
+
+def ref_dissol_convert(cfg, C, mask, phase):
+    L = rxn_lib(14)
+    mask = np.ascontiguousarray(mask, np.uint8).reshape(-1).copy()
+    phase = np.ascontiguousarray(phase, np.uint8).reshape(-1).copy()
+    C = np.ascontiguousarray(C, np.float64).reshape(-1)
+    n, ids, mat, sub, full, prec = _phase_arrays(cfg)
+    pore0 = cfg.pore_codes[0] if cfg.n_pore_codes else 2
+    ch = L.ref_dissol_convert(cfg.nx, cfg.ny, cfg.nz, cfg.n_solutes, _p(C), pore0, cfg.solid_code, cfg.bb_code,
+                              n, _p(ids), _p(mat), _p(sub), _p(full), _p(prec), cfg.reopen_fraction,
+                              _p(mask), _p(phase))
+    return ch, mask, phase

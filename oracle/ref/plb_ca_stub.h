@@ -61,6 +61,9 @@ private:
 };
 
 template<typename T, template<typename U> class D>
+using Cell = typename BlockLattice3D<T, D>::Cell;
+
+template<typename T, template<typename U> class D>
 Dot3D computeRelativeDisplacement(const BlockLattice3D<T, D>&, const BlockLattice3D<T, D>&) { return Dot3D{0, 0, 0}; }
 }  // namespace plb
 
