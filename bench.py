@@ -2,17 +2,19 @@
 """Benchmark of the CompLB3D hot path on B200.
 
 Headline: coupled-step MLUPS of the 256x256x512 sphere-pack workload (porosity
-0.35): one transport step (fused D3Q7 ADR of 8 mobile solutes with dual-Monod
+0.35): one transport step (D3Q7 ADR of 8 mobile solutes with dual-Monod
 kinetics, surface-gated CaCO3 precipitation and a 3-component Newton
-speciation in every pore voxel) plus the amortised flow re-solve (500 D3Q19
+speciation in every pore voxel: a reaction launch over the reactive sites and
+a streaming launch, slab by slab) plus the amortised flow re-solve (500 D3Q19
 steps every 200 transport steps = 2.5 flow steps per step) and the node
 conversion every 200 steps.  Inputs are resident in HBM; the state (~13 GB) is
 far larger than L2, so no flush is needed between steps.
 
 The same line reports the learned-vs-cold Newton speciation batch (2^21
 solves of a 5-component x 14-species tableau at a 1e-10 relative residual,
-network trained on 2^20 Newton-produced pairs), the roofline of the dominant
-kernel from CUDA events on its own stream, an end-to-end figure through the
+network trained on 2^20 Newton-produced pairs), the roofline of the transport
+step (its reaction and streaming launches, timed together with CUDA events on
+the context's stream), the biotic + CA workload, an end-to-end figure through the
 C ABI with host buffers, and the FP64 CPU oracle timed on the host cores.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
@@ -68,7 +70,7 @@ def peaks():
 
 def traffic_from_profile(kernel):
     """DRAM bytes per fluid site from the committed ncu summary, or None."""
-    p = os.path.join(ROOT, "profiles", "ade_main_kernel_coupled_traffic.txt")
+    p = os.path.join(ROOT, "profiles", "ade_step_coupled_traffic.txt")
     if not os.path.exists(p):
         return None
     for line in open(p):
@@ -436,13 +438,16 @@ def main():
            "vs_baseline": None, "dtype": "f32 populations, f64 speciation", "data": "synthetic (seeded sphere pack)",
            "config": config_block(), "fluid_mlups": n_fluid * world * args.steps / (ms * 1e-3) / 1e6,
            "gpu_launches": int(launches), "clocks": clk}
-    # roofline of the dominant kernel: the fused transport step
+    # roofline of the dominant work: the transport step, whose reaction and
+    # streaming launches run slab-interleaved on two streams and are timed
+    # together (one event pair per step on the context's stream)
     peak, peak_kind = peaks()
     ade_bytes = n_fluid_int * ADE_BYTES_PER_FLUID_SITE + (N - 2 * FULL[1] * FULL[2])
     if ade_n:
         achieved = ade_bytes / (ade_ms / ade_n * 1e-3) / 1e9
-        tps = traffic_from_profile("ade_main_kernel")
-        out["roofline"] = {"kernel": "ade_main_kernel", "bound": "hbm", "achieved": achieved, "peak": peak,
+        tps = traffic_from_profile("ade_step")
+        out["roofline"] = {"kernel": "transport step: ade_react_kernel + ade_stream_kernel", "bound": "hbm",
+                           "achieved": achieved, "peak": peak,
                            "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind + " (hbm_gbs)",
                            "algorithmic_bytes_per_launch": ade_bytes, "avg_launch_ms": ade_ms / ade_n,
                            "traffic": (tps * n_fluid_int) if tps else None,

@@ -31,7 +31,7 @@ SRG_TENSOR, SRG_FP32 = 0, 1
 MAX_SRG_ORG = 2
 SRG_IN_FIN, SRG_IN_CONC, SRG_IN_BIOMASS = 0, 1, 2
 SRG_OUT_GROWTH, SRG_OUT_FOUT = 0, 1
-KERNEL_ADE_MAIN, KERNEL_FLOW_STEP = 0, 1
+KERNEL_ADE_MAIN, KERNEL_FLOW_STEP, KERNEL_ADE_REACT = 0, 1, 2
 
 c_int32, c_double, c_int64 = ctypes.c_int32, ctypes.c_double, ctypes.c_int64
 

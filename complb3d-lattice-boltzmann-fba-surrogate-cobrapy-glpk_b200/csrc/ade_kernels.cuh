@@ -1,33 +1,37 @@
-// ade_kernels.cuh -- fused multi-solute D3Q7 advection-diffusion-reaction step.
+// ade_kernels.cuh -- the multi-solute D3Q7 advection-diffusion-reaction step.
 //
-// One launch does, for every interior site and every mobile solute, what the
+// One step does, for every interior site and every mobile solute, what the
 // reference does in separate whole-lattice passes (src/complab.cpp:1252-1374,
 // 1849-1857): AdvectionDiffusionBGKdynamics collide, run_kinetics +
 // update_rxnLattices, the dC reset + run_abiotic_kinetics /
 // surfaceAbioticKinetics3D + update_abiotic_rxnLattices, run_equilibrium_biotic
 // (Newton), and stream.  The increment lattices dC/dB of the reference
-// (whole-lattice copies every step, complab.cpp:1264) never exist: increments
-// stay in shared memory of the thread that owns the voxel.
+// (whole-lattice copies every step, complab.cpp:1264) never exist.
 //
 // Per site the reaction chain only needs the solute densities, and every
-// reference processor adds t_i*dC to the post-collision populations, so:
-//   pass 1  gathers the populations and sums the densities,
-//   chain   runs kinetics -> abiotic -> equilibrium on the densities (FP64),
-//   pass 2  re-gathers (L1/L2 hit), collides, adds t_i*dC_total, streams.
-// HBM traffic stays at one read and one write of 7 FP32 populations per
-// solute; the FP64 Newton state never shares registers with the populations.
+// reference processor adds t_i*dC to the post-collision populations; the BGK
+// collision keeps each density, so the chain can run on the pre-collision
+// densities before the streaming launch:
+//   ade_react_kernel   one thread per reactive site (a compact list): gathers
+//                      the populations, sums the densities, runs kinetics ->
+//                      abiotic (+ dissolution) -> equilibrium in FP64, writes
+//                      the total increment of each mobile solute to dc;
+//   ade_stream_kernel  one thread per interior site: gathers, collides, adds
+//                      t_i*dc, streams (AA pattern, in place).
+// The interior is cut into slabs of x planes: slab j streams while slab j+1
+// reacts, on two streams.
 //
-// Boundary planes x = 0 and x = nx-1 run in a second, small launch after the
-// interior one: a zero-gradient face needs the pre-collision density of its
-// neighbour plane, which the interior launch records (FlatAdiabaticBoundary-
-// Functional3D sets the boundary density to that value after each stream).
+// Boundary planes x = 0 and x = nx-1 run in a third, small launch: a
+// zero-gradient face needs the pre-collision density of its neighbour plane,
+// which the streaming launch records (FlatAdiabaticBoundaryFunctional3D sets
+// the boundary density to that value after each stream).
 //
 // Dissolution (surfaceDissolutionKinetics3D) is the one processor that writes
-// other voxels' increments.  A small launch before the fused one evaluates
+// other voxels' increments.  A small launch before the reactions evaluates
 // every phase voxel's release from the water of its open neighbours (their
 // densities after this step's kinetics, recomputed there) and records it per
-// phase voxel; the fused kernel then gathers, at each voxel flagged as next to
-// a phase, its neighbours' records into the abiotic increment, in the order
+// phase voxel; the reaction chain then gathers, at each voxel flagged as next
+// to a phase, its neighbours' records into the abiotic increment, in the order
 // the reference's serial scatter adds them.
 #pragma once
 #include "internal.h"
@@ -355,192 +359,139 @@ __device__ int reaction_chain(const AdeK& k, int64_t n, int x, int y, int z, uin
     return nonconv;
 }
 
-// A tile of kTile = 2 x kBlock sites of whole z-rows is one block iteration;
-// each thread owns two sites of it.  Only the reactive sites (about the
-// porosity's share) run the reaction chain, so after pass 1 the block
-// compacts them into a list and its threads work through that list, each on
-// the shared-memory columns of the site it took and on its own scratch
-// columns: the FP64 chain then runs on full warps, and a tile of two sites
-// per thread keeps about two thirds of the block busy in it.
-constexpr int kBlock = 256;
-constexpr int kSitesPerThread = 2;
-constexpr int kTile = kBlock * kSitesPerThread;
-
-// virtual thread v of a tile -> (row offset, z, stride) as RowMap does for threads
-struct TileMap {
-    int rpb, zstep;
-    __device__ __forceinline__ void at(int nz, int v, int& lrow, int& z0, bool& active) const {
-        if (nz >= kTile) { lrow = 0; z0 = v; active = true; }
-        else { lrow = v / nz; z0 = v - lrow * nz; active = lrow < rpb; }
-    }
-};
-
-__device__ __forceinline__ TileMap make_tilemap(int nz) {
-    TileMap m;
-    if (nz >= kTile) { m.rpb = 1; m.zstep = kTile; }
-    else { m.rpb = kTile / nz; m.zstep = nz; }
-    return m;
-}
+// ---------------------------------------------------------------------------
+// The step as two launches over the interior.
+//
+// ade_react_kernel: one thread per site of the react list (the reactive live
+// sites, in site order).  It gathers the site's populations of this step
+// (pre-collision; the BGK collision keeps each density, so they are the
+// densities the reference's processors read after collide), runs the reaction
+// chain on shared-memory columns of its own, applies the immobile and biomass
+// increments, and writes the mobile solutes' total increments to dc.  Its
+// warps hold only reactive sites and wait on no barrier, so the FP64 chain
+// runs on full warps at the occupancy its registers allow.
+//
+// ade_stream_kernel: one thread per interior site: gather, collide (or the
+// bounce-back swap of a reopened grain), add t_i * dc, scatter.  No FP64, no
+// shared memory: a streaming kernel at full occupancy.
+//
+// Both read the same populations of the step; the second read comes from L2
+// for the part still resident and from HBM otherwise.
+constexpr int kReactBlock = 128;
 
 template <int NMOB, int NC, int PARITY>
-__global__ void __launch_bounds__(kBlock, 2) ade_main_kernel(const __grid_constant__ AdeK k) {
+__global__ void __launch_bounds__(kReactBlock, 4)
+ade_react_kernel(const __grid_constant__ AdeK k, const uint32_t* __restrict__ list, int64_t r0, int64_t count,
+                 float* __restrict__ dc) {
     extern __shared__ double sm[];
-    __shared__ uint32_t s_n[kTile];        // site of each tile column
-    __shared__ int s_xyz[kTile][3];
-    __shared__ uint8_t s_cls[kTile];
-    __shared__ short s_list[kTile];        // compacted reactive columns
-    __shared__ int s_count;
     const int t = threadIdx.x;
     const AdeParams& p = k.p;
     const int Mw = p.M > 0 ? p.M : 1;
-    double* CurT = sm;                       // [S][kTile] densities of the tile's sites
-    double* AppT = CurT + p.S * kTile;       // [S][kTile] their total increments
-    double* Rw = AppT + p.S * kTile;         // [S][kBlock] per-thread scratch
-    double* Bw = Rw + p.S * kBlock;          // [M][kBlock]
-    double* BRw = Bw + Mw * kBlock;          // [M][kBlock]
+    double* Cur = sm;                           // [S][kReactBlock]
+    double* App = Cur + p.S * kReactBlock;      // [S][kReactBlock]
+    double* Rw = App + p.S * kReactBlock;       // [S][kReactBlock]
+    double* Bw = Rw + p.S * kReactBlock;        // [M][kReactBlock]
+    double* BRw = Bw + Mw * kReactBlock;        // [M][kReactBlock]
+    const int64_t N = k.g.N;
+    const uint32_t N32 = (uint32_t)N;
+    unsigned long long nonconv = 0;
+    double* cCur = Cur + t;
+    double* cApp = App + t;
+    for (int64_t r = r0 + (int64_t)blockIdx.x * kReactBlock + t; r < count; r += (int64_t)gridDim.x * kReactBlock) {
+        const uint32_t n = list[r];
+        const uint32_t q = n / (uint32_t)k.g.nz;
+        const int z = (int)(n - q * (uint32_t)k.g.nz);
+        const int x = (int)(q / (uint32_t)k.g.ny);
+        const int y = (int)(q - (uint32_t)x * (uint32_t)k.g.ny);
+        const uint8_t cls = k.cls[n];
+        const Site st = make_site(k.g, x, y, z, n);
+        for (int s = 0; s < p.S; ++s) cApp[s * kReactBlock] = 0.0;
+#pragma unroll
+        for (int m0 = 0; m0 < NMOB; m0 += kGroup) {
+            float f[kGroup][7];
+#pragma unroll
+            for (int g = 0; g < kGroup; ++g)
+                if (m0 + g < NMOB) gather7<PARITY>(k.pop + (int64_t)(m0 + g) * 7 * N, N32, st, f[g]);
+#pragma unroll
+            for (int g = 0; g < kGroup; ++g) {
+                if (m0 + g >= NMOB) continue;
+                float rr = 0.f;
+#pragma unroll
+                for (int i = 0; i < 7; ++i) rr += f[g][i];
+                cCur[p.mob_index[m0 + g] * kReactBlock] = (double)rr;
+            }
+        }
+        for (int s = 0; s < p.S; ++s)
+            if (p.mob_slot[s] < 0) cCur[s * kReactBlock] = k.imm[(int64_t)s * N + n];
+        nonconv += reaction_chain<NC>(k, n, x, y, z, cls, cCur, cApp, kReactBlock, Rw + t, Bw + t, BRw + t,
+                                      kReactBlock);
+        for (int s = 0; s < p.S; ++s)
+            if (p.mob_slot[s] < 0 && cApp[s * kReactBlock] != 0.0) k.imm[(int64_t)s * N + n] += cApp[s * kReactBlock];
+#pragma unroll
+        for (int m = 0; m < NMOB; ++m) dc[(int64_t)m * N + n] = (float)cApp[p.mob_index[m] * kReactBlock];
+    }
+    for (int o = 16; o > 0; o >>= 1) nonconv += __shfl_down_sync(0xffffffffu, nonconv, o);
+    if ((t & 31) == 0 && nonconv) atomicAdd(&k.counters[0], nonconv);
+}
+
+template <int NMOB, int PARITY>
+__global__ void __launch_bounds__(256) ade_stream_kernel(const __grid_constant__ AdeK k,
+                                                          const float* __restrict__ dc, int any_rxn,
+                                                          uint32_t lo, uint32_t hi) {
+    const AdeParams& p = k.p;
     const int64_t N = k.g.N, plane = k.g.plane;
     const uint32_t N32 = (uint32_t)N;
-    const bool any_rxn = p.do_kin || p.do_abio || p.n_srg > 0 || p.do_dissol || NC > 0;
-    unsigned long long nonconv = 0;
-    const TileMap tm = make_tilemap(k.g.nz);
-    const int row_lo = k.g.ny, row_hi = (k.g.nx - 1) * k.g.ny;     // interior x = 1 .. nx-2
-    // every thread of a block runs the same iterations (the barriers below)
-    for (int row0 = row_lo + blockIdx.x * tm.rpb; row0 < row_hi; row0 += gridDim.x * tm.rpb) {
-      for (int zb = 0; zb < k.g.nz; zb += tm.zstep) {
-        // the tile's sites: live (streams) and reactive masks, site data in shared memory
-        unsigned lvm = 0, rcm = 0;
+    for (uint32_t n = lo + blockIdx.x * blockDim.x + threadIdx.x; n < hi; n += gridDim.x * blockDim.x) {
+        const uint8_t cls = k.cls[n];
+        const uint8_t dyn = cls & 3;
+        // bounce-back sites are a no-op of the AA step unless their mask
+        // reopened to pore; NoDynamics sites stream only when one touches a
+        // dynamic site
+        if ((dyn == BB && !(cls & F_REACTIVE)) || (dyn == NODYN && !k.nodyn_coupled)) continue;
+        const uint32_t q = n / (uint32_t)k.g.nz;
+        const int z = (int)(n - q * (uint32_t)k.g.nz);
+        const int x = (int)(q / (uint32_t)k.g.ny);
+        const int y = (int)(q - (uint32_t)x * (uint32_t)k.g.ny);
+        const bool rc = any_rxn && (cls & F_REACTIVE);
+        const Site st = make_site(k.g, x, y, z, n);
+        const float ux = k.u[n], uy = k.u[N + n], uz = k.u[2 * N + n];
+        const bool adj = (x == 1 || x == k.g.nx - 2);
 #pragma unroll
-        for (int j = 0; j < kSitesPerThread; ++j) {
-            const int v = t + j * kBlock;
-            int lrow, z0; bool act;
-            tm.at(k.g.nz, v, lrow, z0, act);
-            const int row = row0 + lrow, z = zb + z0;
-            if (!(act && row < row_hi && z < k.g.nz)) continue;
-            const int x = row / k.g.ny, y = row - x * k.g.ny;
-            const uint32_t n = (uint32_t)row * (uint32_t)k.g.nz + (uint32_t)z;
-            const uint8_t cls = k.cls[n];
-            const uint8_t dyn = cls & 3;
-            // bounce-back sites are a no-op of the AA step, unless their mask
-            // reopened to pore: then they react (the processors test the mask)
-            if ((dyn == BB && !(cls & F_REACTIVE)) || (dyn == NODYN && !k.nodyn_coupled)) continue;
-            lvm |= 1u << j;
-            // the processors test the mask, not the dynamics: a NoDynamics
-            // site whose mask reopened to pore reacts too
-            if (any_rxn && (cls & F_REACTIVE)) rcm |= 1u << j;
-            s_n[v] = n; s_xyz[v][0] = x; s_xyz[v][1] = y; s_xyz[v][2] = z; s_cls[v] = cls;
-        }
-        if (any_rxn) {
-            // pass 1: the populations of a group of solutes in flight at once, then the densities
-#pragma unroll 1
-            for (int j = 0; j < kSitesPerThread; ++j) {
-                if (!((rcm >> j) & 1u)) continue;
-                const int v = t + j * kBlock;
-                const uint32_t n = s_n[v];
-                const Site st = make_site(k.g, s_xyz[v][0], s_xyz[v][1], s_xyz[v][2], n);
-                for (int s = 0; s < p.S; ++s) AppT[s * kTile + v] = 0.0;
+        for (int m0 = 0; m0 < NMOB; m0 += kGroup) {
+            float f[kGroup][7];
 #pragma unroll
-                for (int m0 = 0; m0 < NMOB; m0 += kGroup) {
-                    float f[kGroup][7];
+            for (int g = 0; g < kGroup; ++g)
+                if (m0 + g < NMOB) gather7<PARITY>(k.pop + (int64_t)(m0 + g) * 7 * N, N32, st, f[g]);
 #pragma unroll
-                    for (int q = 0; q < kGroup; ++q)
-                        if (m0 + q < NMOB) gather7<PARITY>(k.pop + (int64_t)(m0 + q) * 7 * N, N32, st, f[q]);
+            for (int g = 0; g < kGroup; ++g) {
+                const int m = m0 + g;
+                if (m >= NMOB) continue;
+                float rho = 0.f;
+                if (dyn == BB) {
 #pragma unroll
-                    for (int q = 0; q < kGroup; ++q) {
-                        if (m0 + q >= NMOB) continue;
-                        float r = 0.f;
+                    for (int i = 1; i < 4; ++i) { const float tmp = f[g][i]; f[g][i] = f[g][i + 3]; f[g][i + 3] = tmp; }
+                } else if (dyn != NODYN) {
+                    const float om = (dyn == BIO) ? p.omega_bio[m] : p.omega_pore[m];
+                    collide7(f[g], om, ux, uy, uz, rho);
+                } else if (adj) {
 #pragma unroll
-                        for (int i = 0; i < 7; ++i) r += f[q][i];
-                        CurT[p.mob_index[m0 + q] * kTile + v] = (double)r;
-                    }
+                    for (int i = 0; i < 7; ++i) rho += f[g][i];
                 }
-                for (int s = 0; s < p.S; ++s)
-                    if (p.mob_slot[s] < 0) CurT[s * kTile + v] = k.imm[(int64_t)s * N + n];
-            }
-            if (t == 0) s_count = 0;
-            __syncthreads();
-            // compact the reactive columns (warp-aggregated slots)
+                const float d = rc ? dc[(int64_t)m * N + n] : 0.f;
+                if (d != 0.f) {
 #pragma unroll
-            for (int j = 0; j < kSitesPerThread; ++j) {
-                const bool rc = (rcm >> j) & 1u;
-                const unsigned ball = __ballot_sync(0xffffffffu, rc);
-                int base = 0;
-                if ((t & 31) == 0 && ball) base = atomicAdd(&s_count, __popc(ball));
-                base = __shfl_sync(0xffffffffu, base, 0);
-                if (rc) s_list[base + __popc(ball & ((1u << (t & 31)) - 1u))] = (short)(t + j * kBlock);
-            }
-            __syncthreads();
-            const int cnt = s_count;
-            for (int r = t; r < cnt; r += kBlock) {
-                const int c = s_list[r];
-                double* cCur = CurT + c;
-                double* cApp = AppT + c;
-                const uint32_t cn = s_n[c];
-                nonconv += reaction_chain<NC>(k, cn, s_xyz[c][0], s_xyz[c][1], s_xyz[c][2], s_cls[c],
-                                              cCur, cApp, kTile, Rw + t, Bw + t, BRw + t, kBlock);
-                for (int s = 0; s < p.S; ++s)
-                    if (p.mob_slot[s] < 0 && cApp[s * kTile] != 0.0) k.imm[(int64_t)s * N + cn] += cApp[s * kTile];
-            }
-            __syncthreads();
-        }
-        // keep the second gather after the chain: hoisting it would hold all
-        // populations in registers across the Newton solve
-        asm volatile("" ::: "memory");
-        // pass 2: gather every solute (L1/L2 hits after pass 1), collide, add t_i*dC, stream
-#pragma unroll 1
-        for (int j = 0; j < kSitesPerThread; ++j) {
-            if (!((lvm >> j) & 1u)) continue;
-            const int v = t + j * kBlock;
-            const bool rc = (rcm >> j) & 1u;
-            const uint32_t n = s_n[v];
-            const int x = s_xyz[v][0];
-            const uint8_t dyn = s_cls[v] & 3;
-            const Site st = make_site(k.g, x, s_xyz[v][1], s_xyz[v][2], n);
-            const float ux = k.u[n], uy = k.u[N + n], uz = k.u[2 * N + n];
-            const bool adj = (x == 1 || x == k.g.nx - 2);
-#pragma unroll
-            for (int m0 = 0; m0 < NMOB; m0 += kGroup) {
-                float f[kGroup][7];
-#pragma unroll
-                for (int q = 0; q < kGroup; ++q)
-                    if (m0 + q < NMOB) gather7<PARITY>(k.pop + (int64_t)(m0 + q) * 7 * N, N32, st, f[q]);
-#pragma unroll
-                for (int q = 0; q < kGroup; ++q) {
-                    const int m = m0 + q;
-                    if (m >= NMOB) continue;
-                    float rho = 0.f;
-                    if (dyn == BB) {
-                        // BounceBack's collision swaps opposite populations; in the
-                        // AA layout swap + scatter leaves every slot as it was, so
-                        // only the reaction increment moves anything
-#pragma unroll
-                        for (int i = 1; i < 4; ++i) { const float tmp = f[q][i]; f[q][i] = f[q][i + 3]; f[q][i + 3] = tmp; }
-                    } else if (dyn != NODYN) {
-                        const float om = (dyn == BIO) ? p.omega_bio[m] : p.omega_pore[m];
-                        collide7(f[q], om, ux, uy, uz, rho);
-                    } else if (adj) {
-#pragma unroll
-                        for (int i = 0; i < 7; ++i) rho += f[q][i];
-                    }
-                    const float d = rc ? (float)AppT[p.mob_index[m] * kTile + v] : 0.f;
-                    if (d != 0.f) {
-#pragma unroll
-                        for (int i = 0; i < 7; ++i) f[q][i] += t7(i) * d;
-                    }
-                    if (adj && dyn != BB) {
-                        const int side = (x == 1) ? 0 : 1;
-                        k.rho_adj[((int64_t)m * 2 + side) * plane + (n - (int64_t)x * plane)] = rho;
-                    }
+                    for (int i = 0; i < 7; ++i) f[g][i] += t7(i) * d;
                 }
-#pragma unroll
-                for (int q = 0; q < kGroup; ++q)
-                    if (m0 + q < NMOB) scatter7<PARITY>(k.pop + (int64_t)(m0 + q) * 7 * N, N32, st, f[q]);
+                if (adj && dyn != BB) {
+                    const int side = (x == 1) ? 0 : 1;
+                    k.rho_adj[((int64_t)m * 2 + side) * plane + (n - (int64_t)x * plane)] = rho;
+                }
             }
+#pragma unroll
+            for (int g = 0; g < kGroup; ++g)
+                if (m0 + g < NMOB) scatter7<PARITY>(k.pop + (int64_t)(m0 + g) * 7 * N, N32, st, f[g]);
         }
-        // no barrier needed before the next tile: after the chain's barrier
-        // every thread reads only its own columns
-      }
     }
-    if (nonconv) atomicAdd(&k.counters[0], nonconv);
 }
 
 // x = 0 and x = nx-1: AdvectionDiffusionBoundaryDynamics (the one unknown
@@ -610,31 +561,79 @@ inline AdeK make_adek(Ctx* c) {
 int dissol_release(Ctx* c, const AdeK& k);
 
 template <int NMOB, int NC>
-inline int launch_step(Ctx* c, const AdeK& k) {
-    const int bd = kBlock;
+inline int launch_react(Ctx* c, const AdeK& k, cudaStream_t st, int64_t r0, int64_t r1, int max_blocks) {
     const int S = c->ap.S, M = c->ap.M > 0 ? c->ap.M : 1;
-    const bool any_rxn = c->ap.do_kin || c->ap.do_abio || c->ap.n_srg > 0 || c->ap.do_dissol || NC > 0;
-    const size_t smem = any_rxn ? ((size_t)2 * S * kTile + (size_t)(S + 2 * M) * kBlock) * sizeof(double) : 0;
-    const int64_t interior = c->geo.N - 2 * c->geo.plane;
-    const int blocks = grid_for(interior, bd, 148 * 8);
-    int r = CL_OK;
-    if (c->ap.do_dissol && (r = dissol_release(c, k))) return r;
-    if ((r = timing_begin(c, CL_KERNEL_ADE_MAIN))) return r;
+    const size_t smem = (size_t)(3 * S + 2 * M) * kReactBlock * sizeof(double);
+    const int rblocks = grid_for(r1 - r0, kReactBlock, max_blocks);
     if (c->ade_parity == 0) {
-        auto kern = ade_main_kernel<NMOB, NC, 0>;
+        auto kern = ade_react_kernel<NMOB, NC, 0>;
         CL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        kern<<<blocks, bd, smem, c->stream>>>(k);
+        kern<<<rblocks, kReactBlock, smem, st>>>(k, c->d_react, r0, r1, c->d_dc);
     } else {
-        auto kern = ade_main_kernel<NMOB, NC, 1>;
+        auto kern = ade_react_kernel<NMOB, NC, 1>;
         CL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        kern<<<blocks, bd, smem, c->stream>>>(k);
+        kern<<<rblocks, kReactBlock, smem, st>>>(k, c->d_react, r0, r1, c->d_dc);
     }
-    CL_LAUNCH_CHECK("ade_main_kernel");
-    if ((r = timing_end(c, CL_KERNEL_ADE_MAIN))) return r;
-    c->launches += 2;
-    const int bblocks = grid_for(2 * c->geo.plane, bd, 148 * 4);
-    if (c->ade_parity == 0) ade_boundary_kernel<NMOB, 0><<<bblocks, bd, 0, c->stream>>>(k);
-    else ade_boundary_kernel<NMOB, 1><<<bblocks, bd, 0, c->stream>>>(k);
+    CL_LAUNCH_CHECK("ade_react_kernel");
+    c->launches += 1;
+    return CL_OK;
+}
+
+template <int NMOB>
+inline int launch_stream(Ctx* c, const AdeK& k, cudaStream_t st, int64_t lo, int64_t hi, int any_rxn, int max_blocks) {
+    const int blocks = grid_for(hi - lo, 256, max_blocks);
+    if (c->ade_parity == 0) ade_stream_kernel<NMOB, 0><<<blocks, 256, 0, st>>>(k, c->d_dc, any_rxn, (uint32_t)lo, (uint32_t)hi);
+    else ade_stream_kernel<NMOB, 1><<<blocks, 256, 0, st>>>(k, c->d_dc, any_rxn, (uint32_t)lo, (uint32_t)hi);
+    CL_LAUNCH_CHECK("ade_stream_kernel");
+    c->launches += 1;
+    return CL_OK;
+}
+
+template <int NMOB, int NC>
+inline int launch_step(Ctx* c, const AdeK& k) {
+    const bool any_rxn = c->ap.do_kin || c->ap.do_abio || c->ap.n_srg > 0 || c->ap.do_dissol || NC > 0;
+    int r = CL_OK;
+    const int64_t lo = c->geo.plane, hi = c->geo.N - c->geo.plane;
+    if (any_rxn) {
+        if (c->react_dirty && (r = build_react_list(c))) return r;
+        if (c->ap.do_dissol && (r = dissol_release(c, k))) return r;
+    }
+    const int G = any_rxn ? c->slabs : 1;
+    if (G <= 1) {
+        if (any_rxn && c->n_react > 0) {
+            if ((r = timing_begin(c, CL_KERNEL_ADE_REACT))) return r;
+            if ((r = launch_react<NMOB, NC>(c, k, c->stream, 0, c->n_react, 148 * 4 * 8))) return r;
+            if ((r = timing_end(c, CL_KERNEL_ADE_REACT))) return r;
+        }
+        if ((r = timing_begin(c, CL_KERNEL_ADE_MAIN))) return r;
+        if ((r = launch_stream<NMOB>(c, k, c->stream, lo, hi, any_rxn ? 1 : 0, 148 * 8))) return r;
+        if ((r = timing_end(c, CL_KERNEL_ADE_MAIN))) return r;
+    } else {
+        // slab j's reactions (s_react) then its streaming (s_stream, after the
+        // reactions of slab j); slab j+1's reactions overlap slab j's streaming.
+        // The two touch disjoint population slots: a site's AA read and write
+        // sets coincide, so slabs of sites never share a slot.
+        // grids of four blocks per SM each, so that both launches fit on an SM
+        const int rmax = 148 * 4, smax = 148 * 4;
+        if ((r = timing_begin(c, CL_KERNEL_ADE_MAIN))) return r;
+        CL_CUDA(cudaEventRecord(c->ev_fork, c->stream));
+        CL_CUDA(cudaStreamWaitEvent(c->s_react, c->ev_fork, 0));
+        CL_CUDA(cudaStreamWaitEvent(c->s_stream, c->ev_fork, 0));
+        for (int j = 0; j < G; ++j) {
+            const int64_t r0 = c->slab_react[j], r1 = c->slab_react[j + 1];
+            if (r1 > r0 && (r = launch_react<NMOB, NC>(c, k, c->s_react, r0, r1, rmax))) return r;
+            CL_CUDA(cudaEventRecord(c->ev_slab[j], c->s_react));
+            CL_CUDA(cudaStreamWaitEvent(c->s_stream, c->ev_slab[j], 0));
+            if ((r = launch_stream<NMOB>(c, k, c->s_stream, c->slab_site[j], c->slab_site[j + 1], 1, smax))) return r;
+        }
+        CL_CUDA(cudaEventRecord(c->ev_join, c->s_stream));
+        CL_CUDA(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
+        if ((r = timing_end(c, CL_KERNEL_ADE_MAIN))) return r;
+    }
+    c->launches += 1;
+    const int bblocks = grid_for(2 * c->geo.plane, 256, 148 * 4);
+    if (c->ade_parity == 0) ade_boundary_kernel<NMOB, 0><<<bblocks, 256, 0, c->stream>>>(k);
+    else ade_boundary_kernel<NMOB, 1><<<bblocks, 256, 0, c->stream>>>(k);
     CL_LAUNCH_CHECK("ade_boundary_kernel");
     c->ade_parity ^= 1;
     return CL_OK;

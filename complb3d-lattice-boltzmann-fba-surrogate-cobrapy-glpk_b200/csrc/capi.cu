@@ -1,6 +1,7 @@
 // capi.cu -- the C ABI of include/complab_gpu.h over the device context.
 #include "internal.h"
 #include <cstring>
+#include <cstdlib>
 #include <cstdio>
 #include <vector>
 #include <algorithm>
@@ -157,6 +158,18 @@ cl_ctx* cl_create(const cl_config* cfg, void* stream, int* status) {
         if (e != cudaSuccess) return fail(cuda_fail(e, "cudaStreamCreate"));
         c->own_stream = true;
     }
+    {
+        // the slab pipeline of the transport step: two streams and their events
+        cudaError_t e = cudaStreamCreateWithFlags(&c->s_react, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->s_stream, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
+        for (int j = 0; j < Ctx::kMaxSlabs && e == cudaSuccess; ++j)
+            e = cudaEventCreateWithFlags(&c->ev_slab[j], cudaEventDisableTiming);
+        if (e != cudaSuccess) return fail(cuda_fail(e, "slab streams"));
+        // eight slabs of at least 32 planes each; small lattices run unsliced
+        c->slabs = std::max(1, std::min(8, (cfg->nx - 2) / 32));
+    }
     // transport parameters
     AdeParams& p = c->ap;
     std::memset(&p, 0, sizeof p);
@@ -209,6 +222,8 @@ cl_ctx* cl_create(const cl_config* cfg, void* stream, int* status) {
         (r = dalloc(c, &c->d_eq_x, (size_t)(p.eq_warm ? cfg->eq.n_comp : 0) * N)) ||
         (r = dalloc(c, &c->d_phase, (size_t)(p.do_dissol ? N : 0))) ||
         (r = dalloc(c, &c->d_rel, (size_t)(p.do_dissol ? p.S : 0) * N)) ||
+        (r = dalloc(c, &c->d_dc, (size_t)((p.do_kin || p.do_abio || p.n_srg > 0 || p.do_dissol ||
+                                             cfg->use_equilibrium) ? p.n_mob : 0) * N)) ||
         (r = dalloc(c, &c->d_ca_total, (size_t)(cfg->ca_enabled ? N : 0))) ||
         (r = dalloc(c, &c->d_ca_age, (size_t)(cfg->ca_enabled ? 2 * N : 0))) ||
         (r = dalloc(c, &c->d_ca_distpos, (size_t)(cfg->ca_enabled ? N : 0))) ||
@@ -238,13 +253,19 @@ int cl_destroy(cl_ctx* h) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     void* ptrs[] = {c->d_mask, c->d_ns_cls, c->d_ade_cls, c->d_f, c->d_u, c->d_g, c->d_imm, c->d_bio,
                     c->d_rho_adj, c->d_eq_iters, c->d_eq_x, c->d_phase, c->d_rel, c->d_counters, c->d_tracer,
-                    c->d_energy_part, c->d_scratch, c->d_ca_total, c->d_ca_age, c->d_ca_distpos, c->d_ca_out};
+                    c->d_energy_part, c->d_scratch, c->d_ca_total, c->d_ca_age, c->d_ca_distpos, c->d_ca_out,
+                    c->d_dc, c->d_react, c->d_react_blk};
     for (void* p : ptrs) if (p) cudaFree(p);
     for (int o = 0; o < CL_MAX_SRG_ORG; ++o) if (c->d_srg_params[o]) cudaFree(c->d_srg_params[o]);
     for (int k = 0; k < Ctx::kTimedKernels; ++k)
         for (int i = 0; i < Ctx::kEventPool; ++i)
             for (int j = 0; j < 2; ++j) if (c->ev[k][i][j]) cudaEventDestroy(c->ev[k][i][j]);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    if (c->s_react) cudaStreamDestroy(c->s_react);
+    if (c->s_stream) cudaStreamDestroy(c->s_stream);
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
+    for (int j = 0; j < Ctx::kMaxSlabs; ++j) if (c->ev_slab[j]) cudaEventDestroy(c->ev_slab[j]);
     delete h;
     return CL_OK;
 }

@@ -1,6 +1,7 @@
 // geometry.cu -- node classes from the mask, the dynamics switch after a mask
 // change, precipitation node conversion and the global reductions.  All
 // integer/byte work: results are bit-exact against the oracle.
+#include <vector>
 #include "internal.h"
 
 namespace cl {
@@ -177,6 +178,108 @@ static int refresh_counts(Ctx* c, ClassK& k) {
     c->n_bgk = (int64_t)h[0];
     c->flow_nodyn_coupled = h[1] > 0;
     c->ade_nodyn_coupled = h[2] > 0;
+    c->react_dirty = true;
+    return CL_OK;
+}
+
+// The react list: interior sites whose transport class is reactive and live
+// (a NoDynamics site only when NoDynamics sites stream), in increasing site
+// order.  Each of kListBlocks blocks owns one contiguous chunk of sites:
+// pass 1 counts, the host scans the counts, pass 2 writes in order.
+constexpr int kListBlocks = 148 * 8;
+
+__device__ __forceinline__ bool react_site(uint8_t cls, int nodyn_coupled) {
+    const uint8_t dyn = cls & 3;
+    return (cls & F_REACTIVE) && !(dyn == NODYN && !nodyn_coupled);
+}
+
+__global__ void react_count_kernel(const uint8_t* cls, int64_t lo, int64_t hi, int64_t chunk, int nodyn_coupled,
+                                   int64_t* counts) {
+    __shared__ int64_t s_part[8];
+    const int64_t b0 = lo + (int64_t)blockIdx.x * chunk, b1 = min(hi, b0 + chunk);
+    int64_t cnt = 0;
+    for (int64_t n = b0 + threadIdx.x; n < b1; n += blockDim.x) cnt += react_site(cls[n], nodyn_coupled);
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, o);
+    if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = cnt;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int64_t t = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s_part[w];
+        counts[blockIdx.x] = t;
+    }
+}
+
+// blockDim.x == 256: the chunk is walked in rounds of 256 sites, each round's
+// hits placed by a block-wide ballot scan
+__global__ void react_write_kernel(const uint8_t* cls, int64_t lo, int64_t hi, int64_t chunk, int nodyn_coupled,
+                                   const int64_t* offsets, uint32_t* list) {
+    __shared__ int s_warp[8];
+    __shared__ int64_t s_base;
+    const int64_t b0 = lo + (int64_t)blockIdx.x * chunk, b1 = min(hi, b0 + chunk);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (threadIdx.x == 0) s_base = offsets[blockIdx.x];
+    __syncthreads();
+    for (int64_t r0 = b0; r0 < b1; r0 += blockDim.x) {
+        const int64_t n = r0 + threadIdx.x;
+        const bool hit = n < b1 && react_site(cls[n], nodyn_coupled);
+        const unsigned ball = __ballot_sync(0xffffffffu, hit);
+        if (lane == 0) s_warp[w] = __popc(ball);
+        __syncthreads();
+        int before = 0, total = 0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) { if (q < w) before += s_warp[q]; total += s_warp[q]; }
+        if (hit) list[s_base + before + __popc(ball & ((1u << lane) - 1u))] = (uint32_t)n;
+        __syncthreads();
+        if (threadIdx.x == 0) s_base += total;
+        __syncthreads();
+    }
+}
+
+// lower_bound of each site bound in the sorted react list (in place)
+__global__ void react_bounds_kernel(const uint32_t* list, int64_t count, int64_t* bounds, int nb) {
+    for (int j = threadIdx.x; j < nb; j += blockDim.x) {
+        const int64_t key = bounds[j];
+        int64_t a = 0, b = count;
+        while (a < b) {
+            const int64_t mid = (a + b) >> 1;
+            if ((int64_t)list[mid] < key) a = mid + 1; else b = mid;
+        }
+        bounds[j] = a;
+    }
+}
+
+int build_react_list(Ctx* c) {
+    const int64_t lo = c->geo.plane, hi = c->geo.N - c->geo.plane;   // interior x
+    const int64_t chunk = (hi - lo + kListBlocks - 1) / kListBlocks;
+    const int nd = c->ade_nodyn_coupled ? 1 : 0;
+    if (!c->d_react_blk) { int r = dalloc(c, &c->d_react_blk, (size_t)kListBlocks); if (r) return r; }
+    react_count_kernel<<<kListBlocks, 256, 0, c->stream>>>(c->d_ade_cls, lo, hi, chunk, nd, c->d_react_blk);
+    CL_LAUNCH_CHECK("react_count_kernel");
+    std::vector<int64_t> h(kListBlocks);
+    CL_CUDA(cudaMemcpyAsync(h.data(), c->d_react_blk, sizeof(int64_t) * kListBlocks, cudaMemcpyDeviceToHost, c->stream));
+    CL_CUDA(cudaStreamSynchronize(c->stream));
+    int64_t total = 0;
+    for (int b = 0; b < kListBlocks; ++b) { const int64_t v = h[b]; h[b] = total; total += v; }
+    if (!c->d_react) {
+        // capacity for every interior site: the list never needs a reallocation
+        int r = dalloc(c, &c->d_react, (size_t)(hi - lo));
+        if (r) return r;
+    }
+    CL_CUDA(cudaMemcpyAsync(c->d_react_blk, h.data(), sizeof(int64_t) * kListBlocks, cudaMemcpyHostToDevice, c->stream));
+    react_write_kernel<<<kListBlocks, 256, 0, c->stream>>>(c->d_ade_cls, lo, hi, chunk, nd, c->d_react_blk, c->d_react);
+    CL_LAUNCH_CHECK("react_write_kernel");
+    CL_CUDA(cudaStreamSynchronize(c->stream));   // h is read by the copy above
+    c->n_react = total;
+    // slab boundaries: whole x planes; each slab's first list entry by binary search
+    const int G = c->slabs;
+    const int64_t planes = c->geo.nx - 2;
+    for (int j = 0; j <= G; ++j) c->slab_site[j] = lo + (planes * j / G) * c->geo.plane;
+    int64_t* d_b = c->d_react_blk;                    // reuse: G+1 bounds in, offsets out
+    CL_CUDA(cudaMemcpyAsync(d_b, c->slab_site, sizeof(int64_t) * (G + 1), cudaMemcpyHostToDevice, c->stream));
+    react_bounds_kernel<<<1, 128, 0, c->stream>>>(c->d_react, total, d_b, G + 1);
+    CL_LAUNCH_CHECK("react_bounds_kernel");
+    CL_CUDA(cudaMemcpyAsync(c->slab_react, d_b, sizeof(int64_t) * (G + 1), cudaMemcpyDeviceToHost, c->stream));
+    CL_CUDA(cudaStreamSynchronize(c->stream));
+    c->react_dirty = false;
     return CL_OK;
 }
 

@@ -105,18 +105,31 @@ struct Ctx {
     int64_t  ca_mask_sum = -1;       // mask sum at the last check (complab.cpp old_totMask)
     double*  d_rel = nullptr;        // S*N this step's release of each phase voxel: products per open
                                      // face, and at the phase substrate the voxel's own decrement
+    float*   d_dc = nullptr;         // n_mob*N this step's reaction increment of each reactive site
+    uint32_t* d_react = nullptr;     // the reactive live sites, increasing (react list)
+    int64_t  n_react = 0;
+    bool     react_dirty = true;     // classes changed since the list was built
+    int64_t* d_react_blk = nullptr;  // per-block counts / offsets of the list build
+    // the step's slabs of x planes: the reaction launch of slab j+1 (stream
+    // s_react) runs while slab j streams (s_stream)
+    static constexpr int kMaxSlabs = 64;
+    int      slabs = 1;
+    int64_t  slab_site[kMaxSlabs + 1] = {};    // first site of each slab (interior x)
+    int64_t  slab_react[kMaxSlabs + 1] = {};   // first react-list entry of each slab
+    cudaStream_t s_react = nullptr, s_stream = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_slab[kMaxSlabs] = {};
     unsigned long long* d_counters = nullptr;  // [0] non-converged Newton solves
     // scratch for reductions / field IO
     double*  d_scratch = nullptr;
     size_t   scratch_bytes = 0;
     uint64_t device_bytes = 0;
     // measurement: event pairs around timed kernels, launch counter
-    static constexpr int kTimedKernels = 2, kEventPool = 512;
+    static constexpr int kTimedKernels = 3, kEventPool = 512;
     bool     timing = false;
     cudaEvent_t ev[kTimedKernels][kEventPool][2] = {};
-    int      ev_used[kTimedKernels] = {0, 0};
-    double   ev_ms[kTimedKernels] = {0.0, 0.0};
-    int64_t  ev_launches[kTimedKernels] = {0, 0};
+    int      ev_used[kTimedKernels] = {0, 0, 0};
+    double   ev_ms[kTimedKernels] = {0.0, 0.0, 0.0};
+    int64_t  ev_launches[kTimedKernels] = {0, 0, 0};
     int64_t  launches = 0;
 };
 
@@ -141,6 +154,7 @@ int dissol_convert(Ctx* c, int64_t* changed);
 int phase_seed(Ctx* c);          // grain phases from the mask (initPhaseLattice3D)
 int phase_fill(Ctx* c);          // grain inventories (initial_fill) after ade_init
 int refresh_flags(Ctx* c);       // class flags after a mask / phase change, dynamics kept
+int build_react_list(Ctx* c);    // the reactive live sites of the transport classes, in site order
 int ca_init(Ctx* c);             // ages and the distance sign from the mask
 int ca_redistribute(Ctx* c, int32_t* sweeps, int64_t* mask_changes, double* bmax_after);
 int ca_update_mask(Ctx* c, int64_t* mask_changes);

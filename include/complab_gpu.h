@@ -297,8 +297,9 @@ int cl_get_solute_populations(cl_ctx* ctx, int32_t s, float* host_out);
  * named kernel while timing is on; cl_timing_read synchronises and returns the
  * summed device time and the number of timed launches since the last read.
  * cl_launch_count: kernels this context launched since it was created. */
-#define CL_KERNEL_ADE_MAIN  0   /* fused transport + reaction step, interior sites */
+#define CL_KERNEL_ADE_MAIN  0   /* transport collide-stream of the interior sites (+ the reaction increments) */
 #define CL_KERNEL_FLOW_STEP 1   /* D3Q19 collide-stream */
+#define CL_KERNEL_ADE_REACT 2   /* the reaction chain of the reactive sites (kinetics .. equilibrium) */
 int cl_timing_enable(cl_ctx* ctx, int32_t on);
 int cl_timing_read(cl_ctx* ctx, int32_t kernel, double* total_ms, int64_t* launches);
 int cl_launch_count(const cl_ctx* ctx, int64_t* launches);
