@@ -40,7 +40,8 @@
 namespace cl {
 
 #define THRD 1e-12
-constexpr int kGroup = 4;   // solutes whose populations are in flight together
+constexpr int kGroup = 4;        // solutes whose populations are in flight together (reactions)
+constexpr int kStreamGroup = 4;  // the same in the streaming launch
 
 struct AdeK {
     Geo g;
@@ -55,28 +56,85 @@ struct AdeK {
     const uint8_t* mask;      // N material numbers
     const uint8_t* phase;     // N phase ids (null without dissolution)
     double* rel;              // S*N releases of the phase voxels (null without dissolution)
-    unsigned long long* counters;
+    unsigned long long* counters;   // [0] non-converged solves, [1] sites without the storage they need
+    const int32_t* sidx;            // N storage index of each site's slots
     int nodyn_coupled;
     int parity;
     AdeParams p;
     EqDev e;
 };
 
-template <int PARITY>
-__device__ __forceinline__ void gather7(const float* pop, uint32_t N, const Site& st, float* f) {
+// A site's slots in the compact storage: its own storage index and those of
+// its six face neighbours (the sites at +c_d, d = 1..6); where x leaves the
+// lattice the own index stands in (that slot is reflected, never read there).
+// Returns false, with in-bounds substitutes, if a slot the step needs has no
+// storage (the caller counts it; the step then reports an error).
+struct SSite {
+    uint32_t s;
+    uint32_t nb[6];
+    bool hxm, hxp;
+    __device__ __forceinline__ bool inx(int dx) const { return dx < 0 ? hxm : (dx > 0 ? hxp : true); }
+};
+
+__device__ __forceinline__ bool make_ssite(const Geo& g, const int32_t* __restrict__ sidx, int x, int y, int z,
+                                           uint32_t n, SSite& t) {
+    const Site st = make_site(g, x, y, z, n);
+    bool ok = true;
+    const int32_t s0 = sidx[n];
+    if (s0 < 0) ok = false;
+    t.s = s0 < 0 ? 0u : (uint32_t)s0;
+    t.hxm = st.hxm;
+    t.hxp = st.hxp;
 #pragma unroll
-    for (int i = 0; i < 7; ++i) {
-        if (PARITY == 0 || !st.inx(-c7x(i))) f[i] = pop[i * N + st.n];
-        else f[i] = pop[opp7(i) * N + st.at(-c7x(i), -c7y(i), -c7z(i))];
+    for (int d = 1; d < 7; ++d) {
+        uint32_t v = t.s;
+        if (st.inx(c7x(d))) {
+            const int32_t q = sidx[st.at(c7x(d), c7y(d), c7z(d))];
+            if (q < 0) ok = false;
+            else v = (uint32_t)q;
+        }
+        t.nb[d - 1] = v;
+    }
+    return ok;
+}
+
+// AA pattern on the storage: even parity reads slot i of the site and writes
+// slot opp(i); odd parity reads slot opp(i) of the upstream neighbour and
+// writes slot i of the downstream one (a population leaving through an x face
+// stays in the site's own slot).  Population arrays keep the stride N.
+template <int PARITY>
+__device__ __forceinline__ void gather7(const float* pop, uint32_t N, const SSite& st, float* f) {
+    f[0] = pop[st.s];
+#pragma unroll
+    for (int i = 1; i < 7; ++i) {
+        if (PARITY == 0 || !st.inx(-c7x(i))) f[i] = pop[i * N + st.s];
+        else f[i] = pop[opp7(i) * N + st.nb[opp7(i) - 1]];
     }
 }
 
 template <int PARITY>
-__device__ __forceinline__ void scatter7(float* pop, uint32_t N, const Site& st, const float* f) {
+__device__ __forceinline__ void scatter7(float* pop, uint32_t N, const SSite& st, const float* f) {
+    pop[st.s] = f[0];
+#pragma unroll
+    for (int i = 1; i < 7; ++i) {
+        if (PARITY == 0 || !st.inx(c7x(i))) pop[opp7(i) * N + st.s] = f[i];
+        else pop[i * N + st.nb[i - 1]] = f[i];
+    }
+}
+
+// the same gather for any site, stored or not: a slot whose owner has no
+// storage still holds its initial value t_i * c0 (field output only)
+template <int PARITY>
+__device__ __forceinline__ void gather7_any(const float* pop, uint32_t N, const int32_t* sidx, const Geo& g, int x,
+                                            int y, int z, uint32_t n, float c0, float* f) {
+    const Site st = make_site(g, x, y, z, n);
 #pragma unroll
     for (int i = 0; i < 7; ++i) {
-        if (PARITY == 0 || !st.inx(c7x(i))) pop[opp7(i) * N + st.n] = f[i];
-        else pop[i * N + st.at(c7x(i), c7y(i), c7z(i))] = f[i];
+        uint32_t owner = n;
+        int idx = i;
+        if (PARITY == 1 && i > 0 && st.inx(-c7x(i))) { owner = st.at(-c7x(i), -c7y(i), -c7z(i)); idx = opp7(i); }
+        const int32_t so = sidx[owner];
+        f[i] = so >= 0 ? pop[idx * N + (uint32_t)so] : t7(idx) * c0;
     }
 }
 
@@ -404,7 +462,8 @@ ade_react_kernel(const __grid_constant__ AdeK k, const uint32_t* __restrict__ li
         const int x = (int)(q / (uint32_t)k.g.ny);
         const int y = (int)(q - (uint32_t)x * (uint32_t)k.g.ny);
         const uint8_t cls = k.cls[n];
-        const Site st = make_site(k.g, x, y, z, n);
+        SSite st;
+        if (!make_ssite(k.g, k.sidx, x, y, z, n, st)) atomicAdd(&k.counters[1], 1ull);
         for (int s = 0; s < p.S; ++s) cApp[s * kReactBlock] = 0.0;
 #pragma unroll
         for (int m0 = 0; m0 < NMOB; m0 += kGroup) {
@@ -453,17 +512,18 @@ __global__ void __launch_bounds__(256) ade_stream_kernel(const __grid_constant__
         const int x = (int)(q / (uint32_t)k.g.ny);
         const int y = (int)(q - (uint32_t)x * (uint32_t)k.g.ny);
         const bool rc = any_rxn && (cls & F_REACTIVE);
-        const Site st = make_site(k.g, x, y, z, n);
+        SSite st;
+        if (!make_ssite(k.g, k.sidx, x, y, z, n, st)) atomicAdd(&k.counters[1], 1ull);
         const float ux = k.u[n], uy = k.u[N + n], uz = k.u[2 * N + n];
         const bool adj = (x == 1 || x == k.g.nx - 2);
 #pragma unroll
-        for (int m0 = 0; m0 < NMOB; m0 += kGroup) {
-            float f[kGroup][7];
+        for (int m0 = 0; m0 < NMOB; m0 += kStreamGroup) {
+            float f[kStreamGroup][7];
 #pragma unroll
-            for (int g = 0; g < kGroup; ++g)
+            for (int g = 0; g < kStreamGroup; ++g)
                 if (m0 + g < NMOB) gather7<PARITY>(k.pop + (int64_t)(m0 + g) * 7 * N, N32, st, f[g]);
 #pragma unroll
-            for (int g = 0; g < kGroup; ++g) {
+            for (int g = 0; g < kStreamGroup; ++g) {
                 const int m = m0 + g;
                 if (m >= NMOB) continue;
                 float rho = 0.f;
@@ -488,7 +548,7 @@ __global__ void __launch_bounds__(256) ade_stream_kernel(const __grid_constant__
                 }
             }
 #pragma unroll
-            for (int g = 0; g < kGroup; ++g)
+            for (int g = 0; g < kStreamGroup; ++g)
                 if (m0 + g < NMOB) scatter7<PARITY>(k.pop + (int64_t)(m0 + g) * 7 * N, N32, st, f[g]);
         }
     }
@@ -510,7 +570,8 @@ __global__ void __launch_bounds__(256) ade_boundary_kernel(const __grid_constant
         if (dyn == NODYN && !k.nodyn_coupled) continue;
         int x, y, z;
         decode(k.g, n, x, y, z);
-        const Site st = make_site(k.g, x, y, z, (uint32_t)n);
+        SSite st;
+        if (!make_ssite(k.g, k.sidx, x, y, z, (uint32_t)n, st)) atomicAdd(&k.counters[1], 1ull);
         const float ux = k.u[n], uy = k.u[N + n], uz = k.u[2 * N + n];
 #pragma unroll
         for (int m = 0; m < NMOB; ++m) {
@@ -550,6 +611,7 @@ inline AdeK make_adek(Ctx* c) {
     k.phase = c->d_phase;
     k.rel = c->d_rel;
     k.counters = c->d_counters;
+    k.sidx = c->d_sidx;
     k.nodyn_coupled = c->ade_nodyn_coupled ? 1 : 0;
     k.parity = c->ade_parity;
     k.p = c->ap;
@@ -594,6 +656,7 @@ inline int launch_step(Ctx* c, const AdeK& k) {
     const bool any_rxn = c->ap.do_kin || c->ap.do_abio || c->ap.n_srg > 0 || c->ap.do_dissol || NC > 0;
     int r = CL_OK;
     const int64_t lo = c->geo.plane, hi = c->geo.N - c->geo.plane;
+    if (c->store_dirty && (r = store_update(c, 0))) return r;
     if (any_rxn) {
         if (c->react_dirty && (r = build_react_list(c))) return r;
         if (c->ap.do_dissol && (r = dissol_release(c, k))) return r;

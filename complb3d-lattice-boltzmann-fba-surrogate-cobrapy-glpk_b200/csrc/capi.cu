@@ -254,7 +254,7 @@ int cl_destroy(cl_ctx* h) {
     void* ptrs[] = {c->d_mask, c->d_ns_cls, c->d_ade_cls, c->d_f, c->d_u, c->d_g, c->d_imm, c->d_bio,
                     c->d_rho_adj, c->d_eq_iters, c->d_eq_x, c->d_phase, c->d_rel, c->d_counters, c->d_tracer,
                     c->d_energy_part, c->d_scratch, c->d_ca_total, c->d_ca_age, c->d_ca_distpos, c->d_ca_out,
-                    c->d_dc, c->d_react, c->d_react_blk};
+                    c->d_dc, c->d_react, c->d_react_blk, c->d_sidx, c->d_site_of};
     for (void* p : ptrs) if (p) cudaFree(p);
     for (int o = 0; o < CL_MAX_SRG_ORG; ++o) if (c->d_srg_params[o]) cudaFree(c->d_srg_params[o]);
     for (int k = 0; k < Ctx::kTimedKernels; ++k)
@@ -474,11 +474,12 @@ int cl_step(cl_ctx* h, int32_t n) {
         int r = ade_step(c);
         if (r) return r;
     }
-    unsigned long long cnt = 0;
-    CL_CUDA(cudaMemcpyAsync(&cnt, c->d_counters, sizeof cnt, cudaMemcpyDeviceToHost, c->stream));
-    CL_CUDA(cudaMemsetAsync(c->d_counters, 0, sizeof cnt, c->stream));
+    unsigned long long cnts[2] = {0, 0};
+    CL_CUDA(cudaMemcpyAsync(cnts, c->d_counters, sizeof cnts, cudaMemcpyDeviceToHost, c->stream));
+    CL_CUDA(cudaMemsetAsync(c->d_counters, 0, sizeof cnts, c->stream));
     CL_CUDA(cudaStreamSynchronize(c->stream));
-    return cnt ? CL_WARN_NOT_CONVERGED : CL_OK;
+    if (cnts[1]) { set_error("transport step: a live site's slots had no storage"); return CL_ERR_STATE; }
+    return cnts[0] ? CL_WARN_NOT_CONVERGED : CL_OK;
 }
 
 }  // extern "C"
@@ -507,20 +508,24 @@ __global__ void d2phase_kernel(const double* a, uint8_t* b, int64_t n, int n_pha
 }
 // set solute populations to t_i * c at the slots that hold each site's
 // pre-collision populations for the current parity
+// every site is stored when this runs (cl_set_field stores them all first)
 template <int PARITY>
-__global__ void ade_set_kernel(Geo g, float* pm, const double* c) {
+__global__ void ade_set_kernel(Geo g, float* pm, const int32_t* sidx, const double* c) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < g.N; n += stride) {
         int x, y, z;
         decode(g, n, x, y, z);
         const float v = (float)c[n];
+        const int32_t sn = sidx[n];
+        if (sn < 0) continue;
 #pragma unroll
         for (int i = 0; i < 7; ++i) {
-            if (PARITY == 0) pm[i * g.N + n] = t7(i) * v;
+            if (PARITY == 0) pm[i * g.N + sn] = t7(i) * v;
             else {
                 const int64_t m = nbr(g, n, x, y, z, -c7x(i), -c7y(i), -c7z(i));
-                if (m < 0) pm[i * g.N + n] = t7(i) * v;
-                else pm[opp7(i) * g.N + m] = t7(i) * v;
+                const int32_t sm = m < 0 ? -1 : sidx[m];
+                if (m < 0) pm[i * g.N + sn] = t7(i) * v;
+                else if (sm >= 0) pm[opp7(i) * g.N + sm] = t7(i) * v;
             }
         }
     }
@@ -605,9 +610,14 @@ int cl_set_field(cl_ctx* h, int32_t field, int32_t index, const double* in) {
             if (slot < 0) {
                 CL_CUDA(cudaMemcpyAsync(c->d_imm + (int64_t)index * N, d, sizeof(double) * N, cudaMemcpyDeviceToDevice, c->stream));
             } else {
+                // densities may be set anywhere, so every site gets storage
+                // (this uses the scratch, so the input is copied again after)
+                int r2 = store_update(c, 1);
+                if (r2) return r2;
+                CL_CUDA(cudaMemcpyAsync(d, in, sizeof(double) * N, cudaMemcpyHostToDevice, c->stream));
                 float* pm = c->d_g + (int64_t)slot * 7 * N;
-                if (c->ade_parity == 0) ade_set_kernel<0><<<blocks, 256, 0, c->stream>>>(c->geo, pm, d);
-                else ade_set_kernel<1><<<blocks, 256, 0, c->stream>>>(c->geo, pm, d);
+                if (c->ade_parity == 0) ade_set_kernel<0><<<blocks, 256, 0, c->stream>>>(c->geo, pm, c->d_sidx, d);
+                else ade_set_kernel<1><<<blocks, 256, 0, c->stream>>>(c->geo, pm, c->d_sidx, d);
             }
             break;
         }

@@ -179,6 +179,7 @@ static int refresh_counts(Ctx* c, ClassK& k) {
     c->flow_nodyn_coupled = h[1] > 0;
     c->ade_nodyn_coupled = h[2] > 0;
     c->react_dirty = true;
+    c->store_dirty = true;
     return CL_OK;
 }
 

@@ -105,6 +105,13 @@ struct Ctx {
     int64_t  ca_mask_sum = -1;       // mask sum at the last check (complab.cpp old_totMask)
     double*  d_rel = nullptr;        // S*N this step's release of each phase voxel: products per open
                                      // face, and at the phase substrate the voxel's own decrement
+    // transport slots are stored compactly: site n's populations live at
+    // storage index sidx[n] (stride N per population array); -1 = never needed
+    // so far, its slots still hold the initial values
+    int32_t* d_sidx = nullptr;       // N
+    uint32_t* d_site_of = nullptr;   // N capacity: site of each storage index
+    int64_t  n_stored = 0;
+    bool     store_dirty = true;     // classes changed: the needed set may have grown
     float*   d_dc = nullptr;         // n_mob*N this step's reaction increment of each reactive site
     uint32_t* d_react = nullptr;     // the reactive live sites, increasing (react list)
     int64_t  n_react = 0;
@@ -118,7 +125,7 @@ struct Ctx {
     int64_t  slab_react[kMaxSlabs + 1] = {};   // first react-list entry of each slab
     cudaStream_t s_react = nullptr, s_stream = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_slab[kMaxSlabs] = {};
-    unsigned long long* d_counters = nullptr;  // [0] non-converged Newton solves
+    unsigned long long* d_counters = nullptr;  // [0] non-converged Newton solves, [1] live sites without storage
     // scratch for reductions / field IO
     double*  d_scratch = nullptr;
     size_t   scratch_bytes = 0;
@@ -155,6 +162,7 @@ int phase_seed(Ctx* c);          // grain phases from the mask (initPhaseLattice
 int phase_fill(Ctx* c);          // grain inventories (initial_fill) after ade_init
 int refresh_flags(Ctx* c);       // class flags after a mask / phase change, dynamics kept
 int build_react_list(Ctx* c);    // the reactive live sites of the transport classes, in site order
+int store_update(Ctx* c, int all); // store the sites the transport now needs (all: every site)
 int ca_init(Ctx* c);             // ages and the distance sign from the mask
 int ca_redistribute(Ctx* c, int32_t* sweeps, int64_t* mask_changes, double* bmax_after);
 int ca_update_mask(Ctx* c, int64_t* mask_changes);
