@@ -36,6 +36,7 @@ struct EqDev {
     signed char ipow[CL_MAX_SPECIES][CL_MAX_COMP];
     int active[CL_MAX_SPECIES];
     int comp_species[CL_MAX_COMP];
+    int neg[CL_MAX_COMP];              // some species carries component j with a negative power
 };
 
 inline void eqdev_from_system(const cl_eq_system& s, EqDev& d) {
@@ -56,7 +57,11 @@ inline void eqdev_from_system(const cl_eq_system& s, EqDev& d) {
         d.logk[i] = i < s.n_species ? s.logk[i] : 0.0;
         d.k10[i] = std::pow(10.0, d.logk[i]);
     }
-    for (int j = 0; j < CL_MAX_COMP; ++j) d.comp_species[j] = j < s.n_comp ? s.comp_species[j] : -1;
+    for (int j = 0; j < CL_MAX_COMP; ++j) {
+        d.comp_species[j] = j < s.n_comp ? s.comp_species[j] : -1;
+        d.neg[j] = 0;
+        for (int i = 0; i < s.n_species && j < s.n_comp; ++i) if (d.ipow[i][j] < 0) d.neg[j] = 1;
+    }
 }
 
 // species concentration from the component logs, clamped as calc_species
@@ -76,9 +81,10 @@ __device__ __forceinline__ double species_c(const EqDev& e, int i, const double*
 template <int NC>
 struct Powers {
     double a[NC], ai[NC];
-    __device__ __forceinline__ void set(const double* x) {
+    // inverses only of the components some species divides by
+    __device__ __forceinline__ void set(const EqDev& e, const double* x) {
 #pragma unroll
-        for (int j = 0; j < NC; ++j) { a[j] = exp10(x[j]); ai[j] = 1.0 / a[j]; }
+        for (int j = 0; j < NC; ++j) { a[j] = exp10(x[j]); ai[j] = e.neg[j] ? 1.0 / a[j] : 0.0; }
     }
 };
 
@@ -113,7 +119,7 @@ __device__ __forceinline__ double eq_residual(const EqDev& e, const double* T, c
 #pragma unroll
     for (int j = 0; j < NC; ++j) { F[j] = -T[j]; sc[j] = 0.0; }
     Powers<NC> pw;
-    pw.set(x);
+    pw.set(e, x);
     for (int i = 0; i < e.ns; ++i) {
         if (!e.active[i]) continue;
         bool clamped;
@@ -157,7 +163,7 @@ __device__ __forceinline__ void eq_eval_full(const EqDev& e, const double* T, co
         for (int b = 0; b < NC; ++b) J[a][b] = 0.0;
     }
     Powers<NC> pw;
-    pw.set(x);
+    pw.set(e, x);
     for (int i = 0; i < e.ns; ++i) {
         if (!e.active[i]) continue;
         bool clamped;
@@ -201,7 +207,9 @@ __device__ int eq_newton_reuse(const EqDev& e, const double* T, double* x, int m
         if (!(rel < 1e300)) { if (stopped) *stopped = 1; return it; }      // NaN / inf
         fn = sqrt(fn);
         // Cholesky of ln10*J (lower triangle), solve L L^T d = -F
-        double L[NC][NC];
+        // the diagonal is kept as its reciprocal (rsqrt), so the factorisation
+        // and both triangular solves multiply instead of dividing
+        double L[NC][NC], Li[NC];
         bool ok = true;
 #pragma unroll
         for (int a = 0; a < NC; ++a) {
@@ -212,9 +220,9 @@ __device__ int eq_newton_reuse(const EqDev& e, const double* T, double* x, int m
                 for (int k = 0; k < b; ++k) s -= L[a][k] * L[b][k];
                 if (a == b) {
                     if (!(s > 1e-300)) { ok = false; s = 1.0; }
-                    L[a][a] = sqrt(s);
+                    Li[a] = rsqrt(s);
                 } else {
-                    L[a][b] = s / L[b][b];
+                    L[a][b] = s * Li[b];
                 }
             }
         }
@@ -225,14 +233,14 @@ __device__ int eq_newton_reuse(const EqDev& e, const double* T, double* x, int m
             double s = -F[a];
 #pragma unroll
             for (int k = 0; k < a; ++k) s -= L[a][k] * d[k];
-            d[a] = s / L[a][a];
+            d[a] = s * Li[a];
         }
 #pragma unroll
         for (int a = NC - 1; a >= 0; --a) {
             double s = d[a];
 #pragma unroll
             for (int k = a + 1; k < NC; ++k) s -= L[k][a] * d[k];
-            d[a] = s / L[a][a];
+            d[a] = s * Li[a];
         }
         // step cap (2 decades), then Armijo backtracking on the weighted residual
         double dmax = 0.0;
@@ -315,7 +323,7 @@ __device__ int eq_newton_plain(const EqDev& e, const double* T, double* x, int m
             for (int b = 0; b < NC; ++b) J[a][b] = 0.0;
         }
         Powers<NC> pw;
-        pw.set(x);
+        pw.set(e, x);
         for (int i = 0; i < e.ns; ++i) {
             if (!e.active[i]) continue;
             bool clamped;
@@ -343,7 +351,9 @@ __device__ int eq_newton_plain(const EqDev& e, const double* T, double* x, int m
         if (!(rel < 1e300) || stuck) { if (stopped) *stopped = 1; return it; }      // NaN / inf, or stuck
         fn = sqrt(fn);
         // Cholesky of ln10*J (lower triangle), solve L L^T d = -F
-        double L[NC][NC];
+        // the diagonal is kept as its reciprocal (rsqrt), so the factorisation
+        // and both triangular solves multiply instead of dividing
+        double L[NC][NC], Li[NC];
         bool ok = true;
 #pragma unroll
         for (int a = 0; a < NC; ++a) {
@@ -354,9 +364,9 @@ __device__ int eq_newton_plain(const EqDev& e, const double* T, double* x, int m
                 for (int k = 0; k < b; ++k) s -= L[a][k] * L[b][k];
                 if (a == b) {
                     if (!(s > 1e-300)) { ok = false; s = 1.0; }
-                    L[a][a] = sqrt(s);
+                    Li[a] = rsqrt(s);
                 } else {
-                    L[a][b] = s / L[b][b];
+                    L[a][b] = s * Li[b];
                 }
             }
         }
@@ -367,14 +377,14 @@ __device__ int eq_newton_plain(const EqDev& e, const double* T, double* x, int m
             double s = -F[a];
 #pragma unroll
             for (int k = 0; k < a; ++k) s -= L[a][k] * d[k];
-            d[a] = s / L[a][a];
+            d[a] = s * Li[a];
         }
 #pragma unroll
         for (int a = NC - 1; a >= 0; --a) {
             double s = d[a];
 #pragma unroll
             for (int k = a + 1; k < NC; ++k) s -= L[k][a] * d[k];
-            d[a] = s / L[a][a];
+            d[a] = s * Li[a];
         }
         // step cap (2 decades), then Armijo backtracking on the weighted residual
         double dmax = 0.0;
@@ -435,7 +445,7 @@ __device__ int eq_newton_warp(const EqDev& e, const double* T, double* x, int ma
             for (int b = 0; b < NC; ++b) J[a][b] = 0.0;
         }
         Powers<NC> pw;
-        pw.set(x);
+        pw.set(e, x);
         for (int i = 0; i < e.ns; ++i) {
             if (!e.active[i]) continue;
             bool clamped;
@@ -463,7 +473,9 @@ __device__ int eq_newton_warp(const EqDev& e, const double* T, double* x, int ma
         if (!(rel < 1e300) || stuck) { if (stopped) *stopped = 1; return it; }      // NaN / inf, or stuck
         fn = sqrt(fn);
         // Cholesky of ln10*J (lower triangle), solve L L^T d = -F
-        double L[NC][NC];
+        // the diagonal is kept as its reciprocal (rsqrt), so the factorisation
+        // and both triangular solves multiply instead of dividing
+        double L[NC][NC], Li[NC];
         bool ok = true;
 #pragma unroll
         for (int a = 0; a < NC; ++a) {
@@ -474,9 +486,9 @@ __device__ int eq_newton_warp(const EqDev& e, const double* T, double* x, int ma
                 for (int k = 0; k < b; ++k) s -= L[a][k] * L[b][k];
                 if (a == b) {
                     if (!(s > 1e-300)) { ok = false; s = 1.0; }
-                    L[a][a] = sqrt(s);
+                    Li[a] = rsqrt(s);
                 } else {
-                    L[a][b] = s / L[b][b];
+                    L[a][b] = s * Li[b];
                 }
             }
         }
@@ -487,14 +499,14 @@ __device__ int eq_newton_warp(const EqDev& e, const double* T, double* x, int ma
             double s = -F[a];
 #pragma unroll
             for (int k = 0; k < a; ++k) s -= L[a][k] * d[k];
-            d[a] = s / L[a][a];
+            d[a] = s * Li[a];
         }
 #pragma unroll
         for (int a = NC - 1; a >= 0; --a) {
             double s = d[a];
 #pragma unroll
             for (int k = a + 1; k < NC; ++k) s -= L[k][a] * d[k];
-            d[a] = s / L[a][a];
+            d[a] = s * Li[a];
         }
         // step cap (2 decades), then Armijo backtracking on the weighted residual
         double dmax = 0.0;
