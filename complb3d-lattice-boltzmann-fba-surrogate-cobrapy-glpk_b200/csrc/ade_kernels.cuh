@@ -53,6 +53,7 @@ struct AdeK {
     float* rho_adj;           // n_mob * 2 * plane
     int32_t* eq_iters;        // N (may be null)
     double* eq_x;             // NC*N previous solutions (null: cold start only)
+    double* eq_xp;            // NC*N the solutions before those
     const uint8_t* mask;      // N material numbers
     const uint8_t* phase;     // N phase ids (null without dissolution)
     double* rel;              // S*N releases of the phase voxels (null without dissolution)
@@ -383,10 +384,24 @@ __device__ int reaction_chain(const AdeK& k, int64_t n, int x, int y, int z, uin
         for (int j = 0; j < NC; ++j) T[j] = fmax(T[j], 1e-30);
         int conv = 0, it = 0;
         bool warm = false;
+        double xprev[NC];
         if (k.eq_x) {
             warm = true;
+            bool two = true;
 #pragma unroll
-            for (int j = 0; j < NC; ++j) { x[j] = k.eq_x[(int64_t)j * N + n]; warm = warm && (x[j] == x[j]); }
+            for (int j = 0; j < NC; ++j) {
+                xprev[j] = k.eq_x[(int64_t)j * N + n];
+                warm = warm && (xprev[j] == xprev[j]);
+                const double xq = k.eq_xp[(int64_t)j * N + n];
+                two = two && (xq == xq);
+                x[j] = xprev[j];
+                if (two) x[j] = fmin(fmax(2.0 * xprev[j] - xq, -30.0), 1.0);
+            }
+            // the linear extrapolation of the last two solutions, or the last one
+            if (!two) {
+#pragma unroll
+                for (int j = 0; j < NC; ++j) x[j] = xprev[j];
+            }
         }
         // the warm attempt (previous solution, warm_iter iterations), then the
         // cold start; one call site keeps one copy of the solver in the kernel
@@ -397,7 +412,7 @@ __device__ int reaction_chain(const AdeK& k, int64_t n, int x, int y, int z, uin
         }
         if (k.eq_x && conv) {
 #pragma unroll
-            for (int j = 0; j < NC; ++j) k.eq_x[(int64_t)j * N + n] = x[j];
+            for (int j = 0; j < NC; ++j) { k.eq_xp[(int64_t)j * N + n] = xprev[j]; k.eq_x[(int64_t)j * N + n] = x[j]; }
         }
         if (k.eq_iters) k.eq_iters[n] = it;
         if (!conv) nonconv = 1;
@@ -607,6 +622,7 @@ inline AdeK make_adek(Ctx* c) {
     k.rho_adj = c->d_rho_adj;
     k.eq_iters = c->d_eq_iters;
     k.eq_x = c->d_eq_x;
+    k.eq_xp = c->d_eq_xp;
     k.mask = c->d_mask;
     k.phase = c->d_phase;
     k.rel = c->d_rel;

@@ -220,6 +220,7 @@ cl_ctx* cl_create(const cl_config* cfg, void* stream, int* status) {
         (r = dalloc(c, &c->d_rho_adj, (size_t)p.n_mob * 2 * c->geo.plane)) ||
         (r = dalloc(c, &c->d_eq_iters, (size_t)(cfg->use_equilibrium ? N : 0))) ||
         (r = dalloc(c, &c->d_eq_x, (size_t)(p.eq_warm ? cfg->eq.n_comp : 0) * N)) ||
+        (r = dalloc(c, &c->d_eq_xp, (size_t)(p.eq_warm ? cfg->eq.n_comp : 0) * N)) ||
         (r = dalloc(c, &c->d_phase, (size_t)(p.do_dissol ? N : 0))) ||
         (r = dalloc(c, &c->d_rel, (size_t)(p.do_dissol ? p.S : 0) * N)) ||
         (r = dalloc(c, &c->d_dc, (size_t)((p.do_kin || p.do_abio || p.n_srg > 0 || p.do_dissol ||
@@ -231,6 +232,7 @@ cl_ctx* cl_create(const cl_config* cfg, void* stream, int* status) {
         (r = dalloc(c, &c->d_counters, 8)) || (r = dalloc(c, &c->d_tracer, 1)))
         return fail(r);
     if (c->d_eq_x) cudaMemsetAsync(c->d_eq_x, 0xff, sizeof(double) * cfg->eq.n_comp * N, c->stream);  // NaN
+    if (c->d_eq_xp) cudaMemsetAsync(c->d_eq_xp, 0xff, sizeof(double) * cfg->eq.n_comp * N, c->stream);
     c->energy_blocks = grid_for(N, 256, 148 * 8);
     if ((r = dalloc(c, &c->d_energy_part, c->energy_blocks))) return fail(r);
     c->scratch_bytes = sizeof(double) * ((size_t)N + 65536);
@@ -252,7 +254,7 @@ int cl_destroy(cl_ctx* h) {
     Ctx* c = &h->c;
     if (c->stream) cudaStreamSynchronize(c->stream);
     void* ptrs[] = {c->d_mask, c->d_ns_cls, c->d_ade_cls, c->d_f, c->d_u, c->d_g, c->d_imm, c->d_bio,
-                    c->d_rho_adj, c->d_eq_iters, c->d_eq_x, c->d_phase, c->d_rel, c->d_counters, c->d_tracer,
+                    c->d_rho_adj, c->d_eq_iters, c->d_eq_x, c->d_eq_xp, c->d_phase, c->d_rel, c->d_counters, c->d_tracer,
                     c->d_energy_part, c->d_scratch, c->d_ca_total, c->d_ca_age, c->d_ca_distpos, c->d_ca_out,
                     c->d_dc, c->d_react, c->d_react_blk, c->d_sidx, c->d_site_of};
     for (void* p : ptrs) if (p) cudaFree(p);

@@ -183,8 +183,9 @@ typedef struct {
     double  decay[CL_MAX_MICROBES];    /* kd, 1/s */
     int32_t use_equilibrium;
     cl_eq_system eq;
-    int32_t eq_warm_previous;          /* 1: start each voxel's Newton from its previous converged solution
-                                          (cold start after eq.warm_iter misses); 0: the reference's cold start */
+    int32_t eq_warm_previous;          /* 1: start each voxel's Newton from its previous converged solutions
+                                          (the linear extrapolation of the last two; cold start after
+                                          eq.warm_iter misses); 0: the reference's cold start */
     /* precipitation / dissolution (reference src/precipitationVOP.hh, src/dissolutionVOP.hh) */
     int32_t precip_enabled;
     int32_t precip_substrate;          /* immobile solute holding the precipitate */
