@@ -12,11 +12,11 @@
 // reference processor adds t_i*dC to the post-collision populations; the BGK
 // collision keeps each density, so the chain can run on the pre-collision
 // densities before the streaming launch:
-//   ade_react_kernel   one thread per reactive site (a compact list): gathers
+//   ade_react_kernel   one thread per reactive site (the live list): gathers
 //                      the populations, sums the densities, runs kinetics ->
 //                      abiotic (+ dissolution) -> equilibrium in FP64, writes
 //                      the total increment of each mobile solute to dc;
-//   ade_stream_kernel  one thread per interior site: gathers, collides, adds
+//   ade_stream_kernel  one thread per live site (the live list): gathers, collides, adds
 //                      t_i*dc, streams (AA pattern, in place).
 // The interior is cut into slabs of x planes: slab j streams while slab j+1
 // reacts, on two streams.
@@ -435,8 +435,11 @@ __device__ int reaction_chain(const AdeK& k, int64_t n, int x, int y, int z, uin
 // ---------------------------------------------------------------------------
 // The step as two launches over the interior.
 //
-// ade_react_kernel: one thread per site of the react list (the reactive live
-// sites, in site order).  It gathers the site's populations of this step
+// Both run over the live list (the interior sites that stream, in site
+// order; rebuilt when the classes change).
+//
+// ade_react_kernel: one thread per entry, the reactive ones working (all but
+// coupled NoDynamics sites).  It gathers the site's populations of this step
 // (pre-collision; the BGK collision keeps each density, so they are the
 // densities the reference's processors read after collide), runs the reaction
 // chain on shared-memory columns of its own, applies the immobile and biomass
@@ -444,9 +447,10 @@ __device__ int reaction_chain(const AdeK& k, int64_t n, int x, int y, int z, uin
 // warps hold only reactive sites and wait on no barrier, so the FP64 chain
 // runs on full warps at the occupancy its registers allow.
 //
-// ade_stream_kernel: one thread per interior site: gather, collide (or the
+// ade_stream_kernel: one thread per entry: gather, collide (or the
 // bounce-back swap of a reopened grain), add t_i * dc, scatter.  No FP64, no
-// shared memory: a streaming kernel at full occupancy.
+// shared memory, and no idle lanes: the solid sites a full-lattice traversal
+// would mask off are not on the list, so every lane has loads in flight.
 //
 // Both read the same populations of the step; the second read comes from L2
 // for the part still resident and from HBM otherwise.
@@ -472,11 +476,12 @@ ade_react_kernel(const __grid_constant__ AdeK k, const uint32_t* __restrict__ li
     double* cApp = App + t;
     for (int64_t r = r0 + (int64_t)blockIdx.x * kReactBlock + t; r < count; r += (int64_t)gridDim.x * kReactBlock) {
         const uint32_t n = list[r];
+        const uint8_t cls = k.cls[n];
+        if (!(cls & F_REACTIVE)) continue;            // streams, does not react (a coupled NoDynamics site)
         const uint32_t q = n / (uint32_t)k.g.nz;
         const int z = (int)(n - q * (uint32_t)k.g.nz);
         const int x = (int)(q / (uint32_t)k.g.ny);
         const int y = (int)(q - (uint32_t)x * (uint32_t)k.g.ny);
-        const uint8_t cls = k.cls[n];
         SSite st;
         if (!make_ssite(k.g, k.sidx, x, y, z, n, st)) atomicAdd(&k.counters[1], 1ull);
         for (int s = 0; s < p.S; ++s) cApp[s * kReactBlock] = 0.0;
@@ -511,17 +516,18 @@ ade_react_kernel(const __grid_constant__ AdeK k, const uint32_t* __restrict__ li
 template <int NMOB, int PARITY>
 __global__ void __launch_bounds__(256) ade_stream_kernel(const __grid_constant__ AdeK k,
                                                           const float* __restrict__ dc, int any_rxn,
-                                                          uint32_t lo, uint32_t hi) {
+                                                          const uint32_t* __restrict__ list, int64_t r0,
+                                                          int64_t r1) {
     const AdeParams& p = k.p;
     const int64_t N = k.g.N, plane = k.g.plane;
     const uint32_t N32 = (uint32_t)N;
-    for (uint32_t n = lo + blockIdx.x * blockDim.x + threadIdx.x; n < hi; n += gridDim.x * blockDim.x) {
+    // one thread per live site (bounce-back sites are a no-op of the AA step
+    // and stay off the list), so every lane of a warp has loads in flight
+    for (int64_t r = r0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < r1;
+         r += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t n = list[r];
         const uint8_t cls = k.cls[n];
         const uint8_t dyn = cls & 3;
-        // bounce-back sites are a no-op of the AA step unless their mask
-        // reopened to pore; NoDynamics sites stream only when one touches a
-        // dynamic site
-        if ((dyn == BB && !(cls & F_REACTIVE)) || (dyn == NODYN && !k.nodyn_coupled)) continue;
         const uint32_t q = n / (uint32_t)k.g.nz;
         const int z = (int)(n - q * (uint32_t)k.g.nz);
         const int x = (int)(q / (uint32_t)k.g.ny);
@@ -646,11 +652,11 @@ inline int launch_react(Ctx* c, const AdeK& k, cudaStream_t st, int64_t r0, int6
     if (c->ade_parity == 0) {
         auto kern = ade_react_kernel<NMOB, NC, 0>;
         CL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        kern<<<rblocks, kReactBlock, smem, st>>>(k, c->d_react, r0, r1, c->d_dc);
+        kern<<<rblocks, kReactBlock, smem, st>>>(k, c->d_live, r0, r1, c->d_dc);
     } else {
         auto kern = ade_react_kernel<NMOB, NC, 1>;
         CL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        kern<<<rblocks, kReactBlock, smem, st>>>(k, c->d_react, r0, r1, c->d_dc);
+        kern<<<rblocks, kReactBlock, smem, st>>>(k, c->d_live, r0, r1, c->d_dc);
     }
     CL_LAUNCH_CHECK("ade_react_kernel");
     c->launches += 1;
@@ -658,10 +664,11 @@ inline int launch_react(Ctx* c, const AdeK& k, cudaStream_t st, int64_t r0, int6
 }
 
 template <int NMOB>
-inline int launch_stream(Ctx* c, const AdeK& k, cudaStream_t st, int64_t lo, int64_t hi, int any_rxn, int max_blocks) {
-    const int blocks = grid_for(hi - lo, 256, max_blocks);
-    if (c->ade_parity == 0) ade_stream_kernel<NMOB, 0><<<blocks, 256, 0, st>>>(k, c->d_dc, any_rxn, (uint32_t)lo, (uint32_t)hi);
-    else ade_stream_kernel<NMOB, 1><<<blocks, 256, 0, st>>>(k, c->d_dc, any_rxn, (uint32_t)lo, (uint32_t)hi);
+inline int launch_stream(Ctx* c, const AdeK& k, cudaStream_t st, int64_t r0, int64_t r1, int any_rxn, int max_blocks) {
+    if (r1 <= r0) return CL_OK;
+    const int blocks = grid_for(r1 - r0, 256, max_blocks);
+    if (c->ade_parity == 0) ade_stream_kernel<NMOB, 0><<<blocks, 256, 0, st>>>(k, c->d_dc, any_rxn, c->d_live, r0, r1);
+    else ade_stream_kernel<NMOB, 1><<<blocks, 256, 0, st>>>(k, c->d_dc, any_rxn, c->d_live, r0, r1);
     CL_LAUNCH_CHECK("ade_stream_kernel");
     c->launches += 1;
     return CL_OK;
@@ -671,21 +678,18 @@ template <int NMOB, int NC>
 inline int launch_step(Ctx* c, const AdeK& k) {
     const bool any_rxn = c->ap.do_kin || c->ap.do_abio || c->ap.n_srg > 0 || c->ap.do_dissol || NC > 0;
     int r = CL_OK;
-    const int64_t lo = c->geo.plane, hi = c->geo.N - c->geo.plane;
     if (c->store_dirty && (r = store_update(c, 0))) return r;
-    if (any_rxn) {
-        if (c->react_dirty && (r = build_react_list(c))) return r;
-        if (c->ap.do_dissol && (r = dissol_release(c, k))) return r;
-    }
+    if (c->live_dirty && (r = build_live_list(c))) return r;
+    if (any_rxn && c->ap.do_dissol && (r = dissol_release(c, k))) return r;
     const int G = any_rxn ? c->slabs : 1;
     if (G <= 1) {
-        if (any_rxn && c->n_react > 0) {
+        if (any_rxn && c->n_live > 0) {
             if ((r = timing_begin(c, CL_KERNEL_ADE_REACT))) return r;
-            if ((r = launch_react<NMOB, NC>(c, k, c->stream, 0, c->n_react, 148 * 4 * 8))) return r;
+            if ((r = launch_react<NMOB, NC>(c, k, c->stream, 0, c->n_live, 148 * 4 * 8))) return r;
             if ((r = timing_end(c, CL_KERNEL_ADE_REACT))) return r;
         }
         if ((r = timing_begin(c, CL_KERNEL_ADE_MAIN))) return r;
-        if ((r = launch_stream<NMOB>(c, k, c->stream, lo, hi, any_rxn ? 1 : 0, 148 * 8))) return r;
+        if ((r = launch_stream<NMOB>(c, k, c->stream, 0, c->n_live, any_rxn ? 1 : 0, 148 * 8))) return r;
         if ((r = timing_end(c, CL_KERNEL_ADE_MAIN))) return r;
     } else {
         // slab j's reactions (s_react) then its streaming (s_stream, after the
@@ -699,11 +703,11 @@ inline int launch_step(Ctx* c, const AdeK& k) {
         CL_CUDA(cudaStreamWaitEvent(c->s_react, c->ev_fork, 0));
         CL_CUDA(cudaStreamWaitEvent(c->s_stream, c->ev_fork, 0));
         for (int j = 0; j < G; ++j) {
-            const int64_t r0 = c->slab_react[j], r1 = c->slab_react[j + 1];
+            const int64_t r0 = c->slab_live[j], r1 = c->slab_live[j + 1];
             if (r1 > r0 && (r = launch_react<NMOB, NC>(c, k, c->s_react, r0, r1, rmax))) return r;
             CL_CUDA(cudaEventRecord(c->ev_slab[j], c->s_react));
             CL_CUDA(cudaStreamWaitEvent(c->s_stream, c->ev_slab[j], 0));
-            if ((r = launch_stream<NMOB>(c, k, c->s_stream, c->slab_site[j], c->slab_site[j + 1], 1, smax))) return r;
+            if ((r = launch_stream<NMOB>(c, k, c->s_stream, r0, r1, 1, smax))) return r;
         }
         CL_CUDA(cudaEventRecord(c->ev_join, c->s_stream));
         CL_CUDA(cudaStreamWaitEvent(c->stream, c->ev_join, 0));

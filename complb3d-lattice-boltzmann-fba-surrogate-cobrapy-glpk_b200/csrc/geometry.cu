@@ -178,28 +178,29 @@ static int refresh_counts(Ctx* c, ClassK& k) {
     c->n_bgk = (int64_t)h[0];
     c->flow_nodyn_coupled = h[1] > 0;
     c->ade_nodyn_coupled = h[2] > 0;
-    c->react_dirty = true;
+    c->live_dirty = true;
     c->store_dirty = true;
     return CL_OK;
 }
 
-// The react list: interior sites whose transport class is reactive and live
-// (a NoDynamics site only when NoDynamics sites stream), in increasing site
-// order.  Each of kListBlocks blocks owns one contiguous chunk of sites:
+// The live list: interior sites whose transport class streams (not a
+// bounce-back site, unless its mask reopened; a NoDynamics site only when
+// NoDynamics sites stream), in increasing site order: the streaming launch
+// runs one thread per entry, the reaction launch the reactive entries.  Each of kListBlocks blocks owns one contiguous chunk of sites:
 // pass 1 counts, the host scans the counts, pass 2 writes in order.
 constexpr int kListBlocks = 148 * 8;
 
-__device__ __forceinline__ bool react_site(uint8_t cls, int nodyn_coupled) {
+__device__ __forceinline__ bool live_site(uint8_t cls, int nodyn_coupled) {
     const uint8_t dyn = cls & 3;
-    return (cls & F_REACTIVE) && !(dyn == NODYN && !nodyn_coupled);
+    return !((dyn == BB && !(cls & F_REACTIVE)) || (dyn == NODYN && !nodyn_coupled));
 }
 
-__global__ void react_count_kernel(const uint8_t* cls, int64_t lo, int64_t hi, int64_t chunk, int nodyn_coupled,
+__global__ void live_count_kernel(const uint8_t* cls, int64_t lo, int64_t hi, int64_t chunk, int nodyn_coupled,
                                    int64_t* counts) {
     __shared__ int64_t s_part[8];
     const int64_t b0 = lo + (int64_t)blockIdx.x * chunk, b1 = min(hi, b0 + chunk);
     int64_t cnt = 0;
-    for (int64_t n = b0 + threadIdx.x; n < b1; n += blockDim.x) cnt += react_site(cls[n], nodyn_coupled);
+    for (int64_t n = b0 + threadIdx.x; n < b1; n += blockDim.x) cnt += live_site(cls[n], nodyn_coupled);
     for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, o);
     if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = cnt;
     __syncthreads();
@@ -212,7 +213,7 @@ __global__ void react_count_kernel(const uint8_t* cls, int64_t lo, int64_t hi, i
 
 // blockDim.x == 256: the chunk is walked in rounds of 256 sites, each round's
 // hits placed by a block-wide ballot scan
-__global__ void react_write_kernel(const uint8_t* cls, int64_t lo, int64_t hi, int64_t chunk, int nodyn_coupled,
+__global__ void live_write_kernel(const uint8_t* cls, int64_t lo, int64_t hi, int64_t chunk, int nodyn_coupled,
                                    const int64_t* offsets, uint32_t* list) {
     __shared__ int s_warp[8];
     __shared__ int64_t s_base;
@@ -222,7 +223,7 @@ __global__ void react_write_kernel(const uint8_t* cls, int64_t lo, int64_t hi, i
     __syncthreads();
     for (int64_t r0 = b0; r0 < b1; r0 += blockDim.x) {
         const int64_t n = r0 + threadIdx.x;
-        const bool hit = n < b1 && react_site(cls[n], nodyn_coupled);
+        const bool hit = n < b1 && live_site(cls[n], nodyn_coupled);
         const unsigned ball = __ballot_sync(0xffffffffu, hit);
         if (lane == 0) s_warp[w] = __popc(ball);
         __syncthreads();
@@ -235,8 +236,8 @@ __global__ void react_write_kernel(const uint8_t* cls, int64_t lo, int64_t hi, i
     }
 }
 
-// lower_bound of each site bound in the sorted react list (in place)
-__global__ void react_bounds_kernel(const uint32_t* list, int64_t count, int64_t* bounds, int nb) {
+// lower_bound of each site bound in the sorted live list (in place)
+__global__ void live_bounds_kernel(const uint32_t* list, int64_t count, int64_t* bounds, int nb) {
     for (int j = threadIdx.x; j < nb; j += blockDim.x) {
         const int64_t key = bounds[j];
         int64_t a = 0, b = count;
@@ -248,39 +249,39 @@ __global__ void react_bounds_kernel(const uint32_t* list, int64_t count, int64_t
     }
 }
 
-int build_react_list(Ctx* c) {
+int build_live_list(Ctx* c) {
     const int64_t lo = c->geo.plane, hi = c->geo.N - c->geo.plane;   // interior x
     const int64_t chunk = (hi - lo + kListBlocks - 1) / kListBlocks;
     const int nd = c->ade_nodyn_coupled ? 1 : 0;
-    if (!c->d_react_blk) { int r = dalloc(c, &c->d_react_blk, (size_t)kListBlocks); if (r) return r; }
-    react_count_kernel<<<kListBlocks, 256, 0, c->stream>>>(c->d_ade_cls, lo, hi, chunk, nd, c->d_react_blk);
-    CL_LAUNCH_CHECK("react_count_kernel");
+    if (!c->d_live_blk) { int r = dalloc(c, &c->d_live_blk, (size_t)kListBlocks); if (r) return r; }
+    live_count_kernel<<<kListBlocks, 256, 0, c->stream>>>(c->d_ade_cls, lo, hi, chunk, nd, c->d_live_blk);
+    CL_LAUNCH_CHECK("live_count_kernel");
     std::vector<int64_t> h(kListBlocks);
-    CL_CUDA(cudaMemcpyAsync(h.data(), c->d_react_blk, sizeof(int64_t) * kListBlocks, cudaMemcpyDeviceToHost, c->stream));
+    CL_CUDA(cudaMemcpyAsync(h.data(), c->d_live_blk, sizeof(int64_t) * kListBlocks, cudaMemcpyDeviceToHost, c->stream));
     CL_CUDA(cudaStreamSynchronize(c->stream));
     int64_t total = 0;
     for (int b = 0; b < kListBlocks; ++b) { const int64_t v = h[b]; h[b] = total; total += v; }
-    if (!c->d_react) {
+    if (!c->d_live) {
         // capacity for every interior site: the list never needs a reallocation
-        int r = dalloc(c, &c->d_react, (size_t)(hi - lo));
+        int r = dalloc(c, &c->d_live, (size_t)(hi - lo));
         if (r) return r;
     }
-    CL_CUDA(cudaMemcpyAsync(c->d_react_blk, h.data(), sizeof(int64_t) * kListBlocks, cudaMemcpyHostToDevice, c->stream));
-    react_write_kernel<<<kListBlocks, 256, 0, c->stream>>>(c->d_ade_cls, lo, hi, chunk, nd, c->d_react_blk, c->d_react);
-    CL_LAUNCH_CHECK("react_write_kernel");
+    CL_CUDA(cudaMemcpyAsync(c->d_live_blk, h.data(), sizeof(int64_t) * kListBlocks, cudaMemcpyHostToDevice, c->stream));
+    live_write_kernel<<<kListBlocks, 256, 0, c->stream>>>(c->d_ade_cls, lo, hi, chunk, nd, c->d_live_blk, c->d_live);
+    CL_LAUNCH_CHECK("live_write_kernel");
     CL_CUDA(cudaStreamSynchronize(c->stream));   // h is read by the copy above
-    c->n_react = total;
+    c->n_live = total;
     // slab boundaries: whole x planes; each slab's first list entry by binary search
     const int G = c->slabs;
     const int64_t planes = c->geo.nx - 2;
     for (int j = 0; j <= G; ++j) c->slab_site[j] = lo + (planes * j / G) * c->geo.plane;
-    int64_t* d_b = c->d_react_blk;                    // reuse: G+1 bounds in, offsets out
+    int64_t* d_b = c->d_live_blk;                    // reuse: G+1 bounds in, offsets out
     CL_CUDA(cudaMemcpyAsync(d_b, c->slab_site, sizeof(int64_t) * (G + 1), cudaMemcpyHostToDevice, c->stream));
-    react_bounds_kernel<<<1, 128, 0, c->stream>>>(c->d_react, total, d_b, G + 1);
-    CL_LAUNCH_CHECK("react_bounds_kernel");
-    CL_CUDA(cudaMemcpyAsync(c->slab_react, d_b, sizeof(int64_t) * (G + 1), cudaMemcpyDeviceToHost, c->stream));
+    live_bounds_kernel<<<1, 128, 0, c->stream>>>(c->d_live, total, d_b, G + 1);
+    CL_LAUNCH_CHECK("live_bounds_kernel");
+    CL_CUDA(cudaMemcpyAsync(c->slab_live, d_b, sizeof(int64_t) * (G + 1), cudaMemcpyDeviceToHost, c->stream));
     CL_CUDA(cudaStreamSynchronize(c->stream));
-    c->react_dirty = false;
+    c->live_dirty = false;
     return CL_OK;
 }
 

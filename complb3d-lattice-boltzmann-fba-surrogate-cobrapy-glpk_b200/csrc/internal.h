@@ -114,16 +114,16 @@ struct Ctx {
     int64_t  n_stored = 0;
     bool     store_dirty = true;     // classes changed: the needed set may have grown
     float*   d_dc = nullptr;         // n_mob*N this step's reaction increment of each reactive site
-    uint32_t* d_react = nullptr;     // the reactive live sites, increasing (react list)
-    int64_t  n_react = 0;
-    bool     react_dirty = true;     // classes changed since the list was built
-    int64_t* d_react_blk = nullptr;  // per-block counts / offsets of the list build
+    uint32_t* d_live = nullptr;      // the live interior sites of the transport, increasing (live list)
+    int64_t  n_live = 0;
+    bool     live_dirty = true;     // classes changed since the list was built
+    int64_t* d_live_blk = nullptr;  // per-block counts / offsets of the list build
     // the step's slabs of x planes: the reaction launch of slab j+1 (stream
     // s_react) runs while slab j streams (s_stream)
     static constexpr int kMaxSlabs = 64;
     int      slabs = 1;
     int64_t  slab_site[kMaxSlabs + 1] = {};    // first site of each slab (interior x)
-    int64_t  slab_react[kMaxSlabs + 1] = {};   // first react-list entry of each slab
+    int64_t  slab_live[kMaxSlabs + 1] = {};   // first live-list entry of each slab
     cudaStream_t s_react = nullptr, s_stream = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_slab[kMaxSlabs] = {};
     unsigned long long* d_counters = nullptr;  // [0] non-converged Newton solves, [1] live sites without storage
@@ -162,7 +162,7 @@ int dissol_convert(Ctx* c, int64_t* changed);
 int phase_seed(Ctx* c);          // grain phases from the mask (initPhaseLattice3D)
 int phase_fill(Ctx* c);          // grain inventories (initial_fill) after ade_init
 int refresh_flags(Ctx* c);       // class flags after a mask / phase change, dynamics kept
-int build_react_list(Ctx* c);    // the reactive live sites of the transport classes, in site order
+int build_live_list(Ctx* c);    // the live interior sites of the transport classes, in site order
 int store_update(Ctx* c, int all); // store the sites the transport now needs (all: every site)
 int ca_init(Ctx* c);             // ages and the distance sign from the mask
 int ca_redistribute(Ctx* c, int32_t* sweeps, int64_t* mask_changes, double* bmax_after);
