@@ -256,7 +256,7 @@ int cl_destroy(cl_ctx* h) {
     void* ptrs[] = {c->d_mask, c->d_ns_cls, c->d_ade_cls, c->d_f, c->d_u, c->d_g, c->d_imm, c->d_bio,
                     c->d_rho_adj, c->d_eq_iters, c->d_eq_x, c->d_eq_xp, c->d_phase, c->d_rel, c->d_counters, c->d_tracer,
                     c->d_energy_part, c->d_scratch, c->d_ca_total, c->d_ca_age, c->d_ca_distpos, c->d_ca_out,
-                    c->d_dc, c->d_live, c->d_live_blk, c->d_sidx, c->d_site_of};
+                    c->d_dc, c->d_live, c->d_live_blk, c->d_sidx, c->d_site_of, c->d_flive};
     for (void* p : ptrs) if (p) cudaFree(p);
     for (int o = 0; o < CL_MAX_SRG_ORG; ++o) if (c->d_srg_params[o]) cudaFree(c->d_srg_params[o]);
     for (int k = 0; k < Ctx::kTimedKernels; ++k)

@@ -21,6 +21,8 @@ struct FlowK {
     int nodyn_coupled;
     double* part;               // per-block energy partial sums
     const FlowTracer* tracer;   // early exit once converged (may be null)
+    const uint32_t* list;       // the sites that stream, increasing
+    int64_t count;
 };
 
 // Palabos bgk_ma2_equilibrium with invRho = 1, deviation form
@@ -123,23 +125,21 @@ __device__ __forceinline__ double flow_site(const FlowK& k, const Site& st, int 
     return e;
 }
 
+// One thread per entry of the flow's site list (bounce-back sites, a no-op
+// of the AA step, and uncoupled NoDynamics sites are not on it), so every
+// lane of a warp has loads in flight.
 template <int PARITY>
 __global__ void __launch_bounds__(256, 3) flow_aa_kernel(FlowK k) {
     if (k.tracer && k.tracer->converged) return;
     double esum = 0.0;
-    const RowMap rm = make_rowmap(k.g.nz);
-    const int rows = k.g.nx * k.g.ny;
-    for (int row0 = blockIdx.x * rm.rpb; row0 < rows; row0 += gridDim.x * rm.rpb) {
-        const int row = row0 + rm.lrow;
-        if (!rm.active || row >= rows) continue;
-        const int x = row / k.g.ny, y = row - x * k.g.ny;
-        for (int z = rm.z0; z < k.g.nz; z += rm.zstep) {
-            const uint32_t n = (uint32_t)row * (uint32_t)k.g.nz + (uint32_t)z;
-            const uint8_t cls = k.cls[n];
-            if (cls == BB) continue;                 // AA bounce-back is a no-op
-            if (cls == NODYN && !k.nodyn_coupled) continue;
-            esum += flow_site<PARITY>(k, make_site(k.g, x, y, z, n), x, cls);
-        }
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < k.count;
+         r += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t n = k.list[r];
+        const uint32_t q = n / (uint32_t)k.g.nz;
+        const int z = (int)(n - q * (uint32_t)k.g.nz);
+        const int x = (int)(q / (uint32_t)k.g.ny);
+        const int y = (int)(q - (uint32_t)x * (uint32_t)k.g.ny);
+        esum += flow_site<PARITY>(k, make_site(k.g, x, y, z, n), x, k.cls[n]);
     }
     // deterministic block reduction of the energy
     __shared__ double red[8];
@@ -200,6 +200,8 @@ static FlowK make_flowk(Ctx* c) {
     k.nodyn_coupled = c->flow_nodyn_coupled ? 1 : 0;
     k.part = c->d_energy_part;
     k.tracer = c->d_tracer;
+    k.list = nullptr;
+    k.count = 0;
     return k;
 }
 
@@ -239,7 +241,10 @@ int flow_init(Ctx* c) {
 
 // One collideAndStream (two launches: the step, then the tracer update).
 int flow_step(Ctx* c, int use_tracer) {
+    if (c->flive_dirty) { int r0 = build_flow_list(c); if (r0) return r0; }
     FlowK k = make_flowk(c);
+    k.list = c->d_flive;
+    k.count = c->n_flive;
     if (!use_tracer) k.tracer = nullptr;
     const int blocks = c->energy_blocks;
     int r = timing_begin(c, CL_KERNEL_FLOW_STEP);

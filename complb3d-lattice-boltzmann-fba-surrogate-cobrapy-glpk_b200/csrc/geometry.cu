@@ -179,6 +179,7 @@ static int refresh_counts(Ctx* c, ClassK& k) {
     c->flow_nodyn_coupled = h[1] > 0;
     c->ade_nodyn_coupled = h[2] > 0;
     c->live_dirty = true;
+    c->flive_dirty = true;
     c->store_dirty = true;
     return CL_OK;
 }
@@ -249,28 +250,47 @@ __global__ void live_bounds_kernel(const uint32_t* list, int64_t count, int64_t*
     }
 }
 
-int build_live_list(Ctx* c) {
-    const int64_t lo = c->geo.plane, hi = c->geo.N - c->geo.plane;   // interior x
+// the sites of [lo, hi) whose class byte passes live_site, in site order,
+// into *list (allocated once with capacity hi - lo); *count their number
+static int compact_sites(Ctx* c, const uint8_t* cls, int64_t lo, int64_t hi, int coupled, uint32_t** list,
+                         int64_t* count) {
     const int64_t chunk = (hi - lo + kListBlocks - 1) / kListBlocks;
-    const int nd = c->ade_nodyn_coupled ? 1 : 0;
     if (!c->d_live_blk) { int r = dalloc(c, &c->d_live_blk, (size_t)kListBlocks); if (r) return r; }
-    live_count_kernel<<<kListBlocks, 256, 0, c->stream>>>(c->d_ade_cls, lo, hi, chunk, nd, c->d_live_blk);
+    live_count_kernel<<<kListBlocks, 256, 0, c->stream>>>(cls, lo, hi, chunk, coupled, c->d_live_blk);
     CL_LAUNCH_CHECK("live_count_kernel");
     std::vector<int64_t> h(kListBlocks);
     CL_CUDA(cudaMemcpyAsync(h.data(), c->d_live_blk, sizeof(int64_t) * kListBlocks, cudaMemcpyDeviceToHost, c->stream));
     CL_CUDA(cudaStreamSynchronize(c->stream));
     int64_t total = 0;
     for (int b = 0; b < kListBlocks; ++b) { const int64_t v = h[b]; h[b] = total; total += v; }
-    if (!c->d_live) {
-        // capacity for every interior site: the list never needs a reallocation
-        int r = dalloc(c, &c->d_live, (size_t)(hi - lo));
+    if (!*list) {
+        // capacity for every site of the range: the list never needs a reallocation
+        int r = dalloc(c, list, (size_t)(hi - lo));
         if (r) return r;
     }
     CL_CUDA(cudaMemcpyAsync(c->d_live_blk, h.data(), sizeof(int64_t) * kListBlocks, cudaMemcpyHostToDevice, c->stream));
-    live_write_kernel<<<kListBlocks, 256, 0, c->stream>>>(c->d_ade_cls, lo, hi, chunk, nd, c->d_live_blk, c->d_live);
+    live_write_kernel<<<kListBlocks, 256, 0, c->stream>>>(cls, lo, hi, chunk, coupled, c->d_live_blk, *list);
     CL_LAUNCH_CHECK("live_write_kernel");
     CL_CUDA(cudaStreamSynchronize(c->stream));   // h is read by the copy above
-    c->n_live = total;
+    *count = total;
+    return CL_OK;
+}
+
+// The flow's list: every site that is not bounce-back (a no-op of the AA
+// step) and not an uncoupled NoDynamics site, boundary planes included.  The
+// flow class byte carries no flags, so live_site reads it as it is.
+int build_flow_list(Ctx* c) {
+    int r = compact_sites(c, c->d_ns_cls, 0, c->geo.N, c->flow_nodyn_coupled ? 1 : 0, &c->d_flive, &c->n_flive);
+    if (r) return r;
+    c->flive_dirty = false;
+    return CL_OK;
+}
+
+int build_live_list(Ctx* c) {
+    const int64_t lo = c->geo.plane, hi = c->geo.N - c->geo.plane;   // interior x
+    int r = compact_sites(c, c->d_ade_cls, lo, hi, c->ade_nodyn_coupled ? 1 : 0, &c->d_live, &c->n_live);
+    if (r) return r;
+    const int64_t total = c->n_live;
     // slab boundaries: whole x planes; each slab's first list entry by binary search
     const int G = c->slabs;
     const int64_t planes = c->geo.nx - 2;

@@ -115,6 +115,9 @@ struct Ctx {
     bool     store_dirty = true;     // classes changed: the needed set may have grown
     float*   d_dc = nullptr;         // n_mob*N this step's reaction increment of each reactive site
     uint32_t* d_live = nullptr;      // the live interior sites of the transport, increasing (live list)
+    uint32_t* d_flive = nullptr;     // the flow's sites that stream, increasing
+    int64_t  n_flive = 0;
+    bool     flive_dirty = true;
     int64_t  n_live = 0;
     bool     live_dirty = true;     // classes changed since the list was built
     int64_t* d_live_blk = nullptr;  // per-block counts / offsets of the list build
@@ -163,6 +166,7 @@ int phase_seed(Ctx* c);          // grain phases from the mask (initPhaseLattice
 int phase_fill(Ctx* c);          // grain inventories (initial_fill) after ade_init
 int refresh_flags(Ctx* c);       // class flags after a mask / phase change, dynamics kept
 int build_live_list(Ctx* c);    // the live interior sites of the transport classes, in site order
+int build_flow_list(Ctx* c);    // the flow sites that stream (not bounce-back), in site order
 int store_update(Ctx* c, int all); // store the sites the transport now needs (all: every site)
 int ca_init(Ctx* c);             // ages and the distance sign from the mask
 int ca_redistribute(Ctx* c, int32_t* sweeps, int64_t* mask_changes, double* bmax_after);
