@@ -81,17 +81,58 @@ def traffic_from_profile(kernel):
 
 
 class Clocks:
-    """nvidia-smi clock sampling during the timed region."""
+    """SM clock and clock-event reasons sampled during the timed region: an
+    NVML thread every 10 ms (plus one sample at start and one at stop, so a
+    short region still has some), or nvidia-smi at 200 ms without NVML."""
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, dev):
         self.dev = dev
-        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.nv = None
         self.p = None
+        self.sm, self.reasons, self.mx = [], set(), None
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            try:
+                import torch
+                uuid = str(torch.cuda.get_device_properties(dev).uuid)
+                h = nv.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+            except Exception:
+                h = nv.nvmlDeviceGetHandleByIndex(dev)
+            self.mx = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self.bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                         "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                         "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                         "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+            self.nv, self.h = nv, h
+        except Exception:
+            self.nv = None
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def _sample(self):
+        nv = self.nv
+        self.sm.append(float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)))
+        r = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+        for k, b in self.bits.items():
+            if r & b:
+                self.reasons.add(k)
+
+    def _loop(self):
+        while not self.stop_ev.wait(0.01):
+            self._sample()
 
     def start(self):
+        if self.nv is not None:
+            import threading
+            self._sample()
+            self.stop_ev = threading.Event()
+            self.th = threading.Thread(target=self._loop, daemon=True)
+            self.th.start()
+            return
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.Q,
                                        "--format=csv,noheader,nounits", "-lms", "200"],
@@ -100,6 +141,12 @@ class Clocks:
             self.p = None
 
     def stop(self):
+        if self.nv is not None:
+            self._sample()
+            self.stop_ev.set()
+            self.th.join()
+            return {"sm_mhz": statistics.median(self.sm), "sm_max_mhz": self.mx, "reasons": sorted(self.reasons),
+                    "samples": len(self.sm), "source": "nvml"}
         if self.p is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.p.terminate()
@@ -110,18 +157,17 @@ class Clocks:
         self.f.flush()
         rows = [l.strip().split(",") for l in open(self.f.name) if l.strip()]
         sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for r in rows:
             r = [x.strip() for x in r]
             try:
                 sm.append(float(r[1])); mx = float(r[2])
             except (ValueError, IndexError):
                 continue
-            for k, nm in enumerate(names):
+            for k, nm in enumerate(self.NAMES):
                 if len(r) > 5 + k and r[5 + k].lower().startswith("active"):
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi"}
 
 
 def max_over_ranks(value, dist=None, device=None):

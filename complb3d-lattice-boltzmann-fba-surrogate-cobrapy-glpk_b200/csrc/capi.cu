@@ -256,7 +256,7 @@ int cl_destroy(cl_ctx* h) {
     void* ptrs[] = {c->d_mask, c->d_ns_cls, c->d_ade_cls, c->d_f, c->d_u, c->d_g, c->d_imm, c->d_bio,
                     c->d_rho_adj, c->d_eq_iters, c->d_eq_x, c->d_eq_xp, c->d_phase, c->d_rel, c->d_counters, c->d_tracer,
                     c->d_energy_part, c->d_scratch, c->d_ca_total, c->d_ca_age, c->d_ca_distpos, c->d_ca_out,
-                    c->d_dc, c->d_live, c->d_live_blk, c->d_sidx, c->d_site_of, c->d_flive};
+                    c->d_dc, c->d_live, c->d_live_blk, c->d_sidx, c->d_site_of, c->d_flive, c->d_fsidx};
     for (void* p : ptrs) if (p) cudaFree(p);
     for (int o = 0; o < CL_MAX_SRG_ORG; ++o) if (c->d_srg_params[o]) cudaFree(c->d_srg_params[o]);
     for (int k = 0; k < Ctx::kTimedKernels; ++k)
@@ -317,6 +317,17 @@ static int run_flow(Ctx* c, int32_t n, int use_tracer) {
     return CL_OK;
 }
 
+// after a synchronising call: a flow site that streamed without the storage it
+// needed (counted by the step) is an error
+static int flow_storage_check(Ctx* c) {
+    unsigned long long cnt = 0;
+    CL_CUDA(cudaMemcpyAsync(&cnt, c->d_counters + 2, sizeof cnt, cudaMemcpyDeviceToHost, c->stream));
+    CL_CUDA(cudaMemsetAsync(c->d_counters + 2, 0, sizeof cnt, c->stream));
+    CL_CUDA(cudaStreamSynchronize(c->stream));
+    if (cnt) { set_error("flow step: a streaming site's slots had no storage"); return CL_ERR_STATE; }
+    return CL_OK;
+}
+
 int cl_flow_steps(cl_ctx* h, int32_t n) {
     if (!h || n < 0) return CL_ERR_ARG;
     Ctx* c = &h->c;
@@ -325,7 +336,7 @@ int cl_flow_steps(cl_ctx* h, int32_t n) {
     if (r) return r;
     if ((r = run_flow(c, n, 0))) return r;
     CL_CUDA(cudaStreamSynchronize(c->stream));
-    return CL_OK;
+    return flow_storage_check(c);
 }
 
 int cl_flow_solve(cl_ctx* h, int32_t max_it, double eps, int32_t* iters) {
@@ -348,6 +359,7 @@ int cl_flow_solve(cl_ctx* h, int32_t max_it, double eps, int32_t* iters) {
     }
     CL_CUDA(cudaMemcpyAsync(&tr, c->d_tracer, sizeof tr, cudaMemcpyDeviceToHost, c->stream));
     CL_CUDA(cudaStreamSynchronize(c->stream));
+    if ((r = flow_storage_check(c))) return r;
     // parity follows the steps actually executed
     c->flow_parity = tr.steps_done & 1;
     // the reference's loop counter at exit: the index of the converging step, or max_it
@@ -655,6 +667,7 @@ int cl_set_field(cl_ctx* h, int32_t field, int32_t index, const double* in) {
 int cl_get_flow_populations(cl_ctx* h, float* out) {
     if (!h || !out) return CL_ERR_ARG;
     Ctx* c = &h->c;
+    if (!c->flow_ready) { set_error("no flow field"); return CL_ERR_STATE; }
     const int64_t N = c->geo.N;
     float* tmp = nullptr;
     CL_CUDA(cudaMalloc(&tmp, sizeof(float) * 19 * N));
@@ -671,6 +684,7 @@ int cl_get_flow_populations(cl_ctx* h, float* out) {
 int cl_set_flow_populations(cl_ctx* h, const float* in) {
     if (!h || !in) return CL_ERR_ARG;
     Ctx* c = &h->c;
+    if (!c->mask_ready) { set_error("upload the mask first"); return CL_ERR_STATE; }
     const int64_t N = c->geo.N;
     float* tmp = nullptr;
     CL_CUDA(cudaMalloc(&tmp, sizeof(float) * 19 * N));

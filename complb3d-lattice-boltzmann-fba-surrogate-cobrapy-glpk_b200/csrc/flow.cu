@@ -7,6 +7,14 @@
 // 76 B read + 76 B write per fluid site per step.  The pressure boundaries on
 // the x faces (regularized density boundary) and the energy reduction that
 // drives the convergence tracer are fused into the same kernel.
+//
+// Slots are stored compactly: the sites that stream and their 18 D3Q19
+// neighbours get storage indices in site order (fsidx; population arrays keep
+// the stride N), so the slots of a run of pore sites are contiguous and a
+// warp's loads fill whole sectors instead of fetching the solid sites' slots at
+// the ends of every run.  An unstored site's slots read as 0, the value the
+// full-lattice layout holds there (flow_init gives non-BGK sites 0 and nothing
+// writes a slot no streaming site reaches).
 #include "internal.h"
 #include <cmath>
 
@@ -23,6 +31,8 @@ struct FlowK {
     const FlowTracer* tracer;   // early exit once converged (may be null)
     const uint32_t* list;       // the sites that stream, increasing
     int64_t count;
+    const int32_t* sidx;        // N storage index of each site's slots (-1: none, reads 0)
+    unsigned long long* counters;   // [2] streaming sites without the storage they need
 };
 
 // Palabos bgk_ma2_equilibrium with invRho = 1, deviation form
@@ -65,29 +75,62 @@ __device__ __forceinline__ void regularize(float* f, float rb, float& jx) {
     }
 }
 
+// Storage indices of a site's slots: sl[0] its own, sl[i] that of the site at
+// +c_i (its own where x leaves the lattice; that slot is reflected, never
+// read there).  Returns false, with in-bounds substitutes, if one is missing.
 template <int PARITY>
-__device__ __forceinline__ void gather19(const FlowK& k, const Site& st, float* f) {
+__device__ __forceinline__ bool flow_slots(const FlowK& k, const Site& st, uint32_t* sl) {
+    bool ok = true;
+    const int32_t s0 = k.sidx[st.n];
+    if (s0 < 0) ok = false;
+    sl[0] = s0 < 0 ? 0u : (uint32_t)s0;
+    if (PARITY == 1) {
+#pragma unroll
+        for (int i = 1; i < 19; ++i) {
+            uint32_t v = sl[0];
+            if (st.inx(c19x(i))) {
+                const int32_t q = k.sidx[st.at(c19x(i), c19y(i), c19z(i))];
+                if (q < 0) ok = false;
+                else v = (uint32_t)q;
+            }
+            sl[i] = v;
+        }
+    }
+    return ok;
+}
+
+// AA pattern on the storage: even parity reads slot i of the site and writes
+// slot opp(i); odd parity reads slot opp(i) of the upstream neighbour and
+// writes slot i of the downstream one (x faces reflect into the own slots).
+template <int PARITY>
+__device__ __forceinline__ void gather19(const FlowK& k, const Site& st, const uint32_t* sl, float* f) {
     const uint32_t N = (uint32_t)k.g.N;
 #pragma unroll
     for (int i = 0; i < 19; ++i) {
-        if (PARITY == 0 || !st.inx(-c19x(i))) {
-            f[i] = k.f[i * N + st.n];
-        } else {
-            f[i] = k.f[opp19(i) * N + st.at(-c19x(i), -c19y(i), -c19z(i))];
-        }
+        if (PARITY == 0 || !st.inx(-c19x(i))) f[i] = k.f[i * N + sl[0]];
+        else f[i] = k.f[opp19(i) * N + sl[opp19(i)]];
     }
 }
 
 template <int PARITY>
-__device__ __forceinline__ void scatter19(const FlowK& k, const Site& st, const float* f) {
+__device__ __forceinline__ void scatter19(const FlowK& k, const Site& st, const uint32_t* sl, const float* f) {
     const uint32_t N = (uint32_t)k.g.N;
 #pragma unroll
     for (int i = 0; i < 19; ++i) {
-        if (PARITY == 0 || !st.inx(c19x(i))) {
-            k.f[opp19(i) * N + st.n] = f[i];
-        } else {
-            k.f[i * N + st.at(c19x(i), c19y(i), c19z(i))] = f[i];
-        }
+        if (PARITY == 0 || !st.inx(c19x(i))) k.f[opp19(i) * N + sl[0]] = f[i];
+        else k.f[i * N + sl[i]] = f[i];
+    }
+}
+
+// the same gather for any site, stored or not (field output, statistics)
+template <int PARITY>
+__device__ __forceinline__ void gather19_any(const FlowK& k, const Site& st, float* f) {
+    const uint32_t N = (uint32_t)k.g.N;
+#pragma unroll
+    for (int i = 0; i < 19; ++i) {
+        const bool own = PARITY == 0 || !st.inx(-c19x(i));
+        const int32_t s = k.sidx[own ? st.n : st.at(-c19x(i), -c19y(i), -c19z(i))];
+        f[i] = s < 0 ? 0.f : k.f[(own ? i : opp19(i)) * N + (uint32_t)s];
     }
 }
 
@@ -101,7 +144,9 @@ __device__ __forceinline__ Site site_of(const Geo& g, int64_t n) {
 template <int PARITY>
 __device__ __forceinline__ double flow_site(const FlowK& k, const Site& st, int x, uint8_t cls) {
     float f[19];
-    gather19<PARITY>(k, st, f);
+    uint32_t sl[19];
+    if (!flow_slots<PARITY>(k, st, sl)) atomicAdd(&k.counters[2], 1ull);
+    gather19<PARITY>(k, st, sl, f);
     double e = 0.0;
     if (cls != NODYN) {
         const float om = (cls == BIO) ? k.omega_bio : k.omega;
@@ -121,7 +166,7 @@ __device__ __forceinline__ double flow_site(const FlowK& k, const Site& st, int 
         for (int i = 0; i < 19; ++i) f[i] = f[i] * (1.f - om) + om * feq19(i, rb, jx, jy, jz, jsq);
         e = 0.5 * (double)jsq;
     }
-    scatter19<PARITY>(k, st, f);
+    scatter19<PARITY>(k, st, sl, f);
     return e;
 }
 
@@ -202,13 +247,19 @@ static FlowK make_flowk(Ctx* c) {
     k.tracer = c->d_tracer;
     k.list = nullptr;
     k.count = 0;
+    k.sidx = c->d_fsidx;
+    k.counters = c->d_counters;
     return k;
 }
 
-// initializeAtEquilibrium with the linear density profile; non-BGK sites hold 0.
-__global__ void flow_init_kernel(Geo g, float* f, const uint8_t* cls, double rho_in, double rho_out) {
+// initializeAtEquilibrium with the linear density profile into the stored
+// slots; non-BGK sites hold 0 (BGK sites stream, so they are all stored).
+__global__ void flow_init_kernel(Geo g, float* f, const int32_t* sidx, const uint8_t* cls, double rho_in,
+                                 double rho_out) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < g.N; n += stride) {
+        const int32_t s = sidx[n];
+        if (s < 0) continue;
         int x, y, z;
         decode(g, n, x, y, z);
         const uint8_t c = cls[n];
@@ -216,8 +267,73 @@ __global__ void flow_init_kernel(Geo g, float* f, const uint8_t* cls, double rho
         const double rho = rho_in + (rho_out - rho_in) * (double)x / (double)(g.nx - 1);
         const float rb = bgk ? (float)(rho - 1.0) : 0.f;
 #pragma unroll
-        for (int i = 0; i < 19; ++i) f[i * g.N + n] = t19(i) * rb;
+        for (int i = 0; i < 19; ++i) f[i * g.N + s] = t19(i) * rb;
     }
+}
+
+// the flow's live sites: every class but bounce-back, NoDynamics only when
+// some NoDynamics site touches a dynamic one (the class byte has no flags)
+__device__ __forceinline__ bool flow_live(uint8_t cls, int nodyn_coupled) {
+    return !(cls == BB || (cls == NODYN && !nodyn_coupled));
+}
+
+// need[n] = 1 when site n has no storage yet and streams, has a D3Q19
+// neighbour that streams, or is given a nonzero population (nat, natural
+// order, may be null)
+__global__ void flow_need_kernel(Geo g, const uint8_t* cls, int nodyn_coupled, const int32_t* sidx,
+                                 const float* nat, uint8_t* need) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < g.N; n += stride) {
+        bool nd = false;
+        if (sidx[n] < 0) {
+            if (flow_live(cls[n], nodyn_coupled)) nd = true;
+            else {
+                int x, y, z;
+                decode(g, n, x, y, z);
+                const Site st = make_site(g, x, y, z, (uint32_t)n);
+#pragma unroll
+                for (int i = 1; i < 19; ++i)
+                    if (st.inx(c19x(i)) && flow_live(cls[st.at(c19x(i), c19y(i), c19z(i))], nodyn_coupled)) nd = true;
+            }
+            if (!nd && nat)
+                for (int i = 0; i < 19; ++i)
+                    if (__float_as_uint(nat[i * g.N + n]) != 0u) nd = true;
+        }
+        need[n] = nd ? 1 : 0;
+    }
+}
+
+// zero slots of storage indices [lo, hi): a site entering the storage holds
+// what the full-lattice layout holds at a site nothing has written
+__global__ void flow_zero_kernel(float* f, int64_t N, int64_t lo, int64_t hi) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t s = lo + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < hi; s += stride)
+#pragma unroll
+        for (int i = 0; i < 19; ++i) f[i * N + s] = 0.f;
+}
+
+int flow_store_update(Ctx* c, const float* d_nat) {
+    const int64_t N = c->geo.N;
+    if (!c->d_fsidx) {
+        int r = dalloc(c, &c->d_fsidx, (size_t)N);
+        if (r) return r;
+        CL_CUDA(cudaMemsetAsync(c->d_fsidx, 0xff, sizeof(int32_t) * N, c->stream));
+        c->n_fstored = 0;
+    }
+    if (c->n_fstored == N) { c->fstore_dirty = false; return CL_OK; }
+    uint8_t* need = reinterpret_cast<uint8_t*>(c->d_scratch);            // N bytes
+    flow_need_kernel<<<grid_for(N, 256, 148 * 16), 256, 0, c->stream>>>(
+        c->geo, c->d_ns_cls, c->flow_nodyn_coupled ? 1 : 0, c->d_fsidx, d_nat, need);
+    CL_LAUNCH_CHECK("flow_need_kernel");
+    int64_t first = 0, added = 0;
+    int r = assign_storage(c, need, c->d_fsidx, nullptr, &c->n_fstored, &first, &added);
+    if (r) return r;
+    if (added > 0) {
+        flow_zero_kernel<<<grid_for(added, 256, 148 * 16), 256, 0, c->stream>>>(c->d_f, N, first, first + added);
+        CL_LAUNCH_CHECK("flow_zero_kernel");
+    }
+    c->fstore_dirty = false;
+    return CL_OK;
 }
 
 __global__ void tracer_reset_kernel(FlowTracer* tr, double eps) {
@@ -232,8 +348,13 @@ int flow_arm_tracer(Ctx* c, double eps) {
 }
 
 int flow_init(Ctx* c) {
+    // the storage starts afresh from the current classes
+    if (c->d_fsidx) CL_CUDA(cudaMemsetAsync(c->d_fsidx, 0xff, sizeof(int32_t) * c->geo.N, c->stream));
+    c->n_fstored = 0;
+    int r = flow_store_update(c, nullptr);
+    if (r) return r;
     flow_init_kernel<<<grid_for(c->geo.N, 256, 148 * 16), 256, 0, c->stream>>>(
-        c->geo, c->d_f, c->d_ns_cls, c->cfg.rho_in, c->cfg.rho_out);
+        c->geo, c->d_f, c->d_fsidx, c->d_ns_cls, c->cfg.rho_in, c->cfg.rho_out);
     CL_LAUNCH_CHECK("flow_init_kernel");
     c->flow_parity = 0;
     return flow_arm_tracer(c, 0.0);
@@ -241,6 +362,7 @@ int flow_init(Ctx* c) {
 
 // One collideAndStream (two launches: the step, then the tracer update).
 int flow_step(Ctx* c, int use_tracer) {
+    if (c->fstore_dirty) { int r0 = flow_store_update(c, nullptr); if (r0) return r0; }
     if (c->flive_dirty) { int r0 = build_flow_list(c); if (r0) return r0; }
     FlowK k = make_flowk(c);
     k.list = c->d_flive;
@@ -271,7 +393,7 @@ __global__ void flow_macro_kernel(FlowK k, double* rho, float* u) {
         decode(k.g, n, x, y, z);
         const uint8_t cls = k.cls[n];
         float f[19];
-        gather19<PARITY>(k, make_site(k.g, x, y, z, (uint32_t)n), f);
+        gather19_any<PARITY>(k, make_site(k.g, x, y, z, (uint32_t)n), f);
         float rb = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
         const bool bgk = (cls == FLUID || cls == BIO);
         if (bgk && x == 0) { rb = k.rb_in; regularize<-1>(f, rb, jx); }
@@ -290,6 +412,7 @@ __global__ void flow_macro_kernel(FlowK k, double* rho, float* u) {
 }
 
 int flow_macro(Ctx* c, double* d_rho, float* d_u3, int) {
+    if (!c->d_fsidx) { int r = flow_store_update(c, nullptr); if (r) return r; }
     FlowK k = make_flowk(c);
     const int blocks = grid_for(c->geo.N, 256, 148 * 16);
     if (c->flow_parity == 0) flow_macro_kernel<0><<<blocks, 256, 0, c->stream>>>(k, d_rho, d_u3);
@@ -315,7 +438,7 @@ __global__ void flow_stats_kernel(FlowK k, double* part) {
         float jx = 0.f, jy = 0.f, jz = 0.f;
         if (cls == FLUID || cls == BIO) {
             float f[19];
-            gather19<PARITY>(k, make_site(k.g, x, y, z, (uint32_t)n), f);
+            gather19_any<PARITY>(k, make_site(k.g, x, y, z, (uint32_t)n), f);
 #pragma unroll
             for (int i = 0; i < 19; ++i) { jx += c19x(i) * f[i]; jy += c19y(i) * f[i]; jz += c19z(i) * f[i]; }
         }
@@ -344,6 +467,7 @@ __global__ void flow_stats_final(const double* part, int nb, double* out) {
 }
 
 int flow_stats(Ctx* c, double out[3]) {
+    if (!c->d_fsidx) { int r = flow_store_update(c, nullptr); if (r) return r; }
     FlowK k = make_flowk(c);
     const int nb = 148 * 4;
     double* part = c->d_scratch;
@@ -364,17 +488,24 @@ __global__ void flow_io_kernel(FlowK k, float* nat, int to_natural) {
     for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < k.g.N; n += stride) {
         if (to_natural) {
             float f[19];
-            gather19<PARITY>(k, site_of(k.g, n), f);
+            gather19_any<PARITY>(k, site_of(k.g, n), f);
 #pragma unroll
             for (int i = 0; i < 19; ++i) nat[i * k.g.N + n] = f[i];
         } else {
+            // every site given a nonzero population is stored by now
+            const int32_t s = k.sidx[n];
+            if (s < 0) continue;
 #pragma unroll
-            for (int i = 0; i < 19; ++i) k.f[i * k.g.N + n] = nat[i * k.g.N + n];
+            for (int i = 0; i < 19; ++i) k.f[i * k.g.N + s] = nat[i * k.g.N + n];
         }
     }
 }
 
 int flow_population_io(Ctx* c, float* d_nat, int to_natural) {
+    if (!to_natural || !c->d_fsidx) {
+        int r = flow_store_update(c, to_natural ? nullptr : d_nat);
+        if (r) return r;
+    }
     FlowK k = make_flowk(c);
     const int blocks = grid_for(c->geo.N, 256, 148 * 16);
     if (!to_natural || c->flow_parity == 0) flow_io_kernel<0><<<blocks, 256, 0, c->stream>>>(k, d_nat, to_natural);

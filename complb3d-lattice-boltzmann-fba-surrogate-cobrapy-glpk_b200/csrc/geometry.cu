@@ -181,6 +181,7 @@ static int refresh_counts(Ctx* c, ClassK& k) {
     c->live_dirty = true;
     c->flive_dirty = true;
     c->store_dirty = true;
+    c->fstore_dirty = true;
     return CL_OK;
 }
 

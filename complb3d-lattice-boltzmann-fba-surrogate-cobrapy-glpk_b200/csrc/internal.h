@@ -113,6 +113,12 @@ struct Ctx {
     uint32_t* d_site_of = nullptr;   // N capacity: site of each storage index
     int64_t  n_stored = 0;
     bool     store_dirty = true;     // classes changed: the needed set may have grown
+    // flow slots are stored the same way: the sites that stream and their 18
+    // D3Q19 neighbours; an unstored site's slots hold 0 (flow_init gives every
+    // non-BGK site 0, and BGK sites always stream)
+    int32_t* d_fsidx = nullptr;      // N
+    int64_t  n_fstored = 0;
+    bool     fstore_dirty = true;
     float*   d_dc = nullptr;         // n_mob*N this step's reaction increment of each reactive site
     uint32_t* d_live = nullptr;      // the live interior sites of the transport, increasing (live list)
     uint32_t* d_flive = nullptr;     // the flow's sites that stream, increasing
@@ -129,7 +135,7 @@ struct Ctx {
     int64_t  slab_live[kMaxSlabs + 1] = {};   // first live-list entry of each slab
     cudaStream_t s_react = nullptr, s_stream = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_slab[kMaxSlabs] = {};
-    unsigned long long* d_counters = nullptr;  // [0] non-converged Newton solves, [1] live sites without storage
+    unsigned long long* d_counters = nullptr;  // [0] non-converged Newton solves, [1] transport / [2] flow sites without storage
     // scratch for reductions / field IO
     double*  d_scratch = nullptr;
     size_t   scratch_bytes = 0;
@@ -168,6 +174,10 @@ int refresh_flags(Ctx* c);       // class flags after a mask / phase change, dyn
 int build_live_list(Ctx* c);    // the live interior sites of the transport classes, in site order
 int build_flow_list(Ctx* c);    // the flow sites that stream (not bounce-back), in site order
 int store_update(Ctx* c, int all); // store the sites the transport now needs (all: every site)
+// storage indices for the sites flagged in need, after the *n_stored assigned
+int assign_storage(Ctx* c, const uint8_t* need, int32_t* sidx, uint32_t* site_of, int64_t* n_stored,
+                   int64_t* first, int64_t* added);
+int flow_store_update(Ctx* c, const float* d_natural);  // store the sites the flow needs (+ nonzero inputs)
 int ca_init(Ctx* c);             // ages and the distance sign from the mask
 int ca_redistribute(Ctx* c, int32_t* sweeps, int64_t* mask_changes, double* bmax_after);
 int ca_update_mask(Ctx* c, int64_t* mask_changes);

@@ -1,4 +1,5 @@
-// storage.cu -- compact storage of the transport populations.
+// storage.cu -- compact storage of the transport populations (and the
+// index assignment the flow's compact storage shares).
 //
 // A step reads and writes the slots of the live sites (the AA read and write
 // sets of a site are its own slots and, in the odd parity, the slots its face
@@ -84,7 +85,7 @@ __global__ void store_write_kernel(const uint8_t* need, int64_t N, int64_t chunk
         for (int q = 0; q < (int)(blockDim.x >> 5); ++q) { if (q < w) before += s_warp[q]; total += s_warp[q]; }
         if (hit) {
             const int64_t idx = s_base + before + __popc(ball & ((1u << lane) - 1u));
-            site_of[idx] = (uint32_t)n;
+            if (site_of) site_of[idx] = (uint32_t)n;
             sidx[n] = (int32_t)idx;
         }
         __syncthreads();
@@ -104,6 +105,33 @@ __global__ void store_init_kernel(float* pop, int64_t N, int n_mob, InitPop ip, 
         }
 }
 
+// Storage indices for the sites flagged in need (scratch, N bytes), in site
+// order after the *n_stored already assigned; *first and *added give the new
+// range.  site_of (may be null) records the site of each new index.
+int assign_storage(Ctx* c, const uint8_t* need, int32_t* sidx, uint32_t* site_of, int64_t* n_stored,
+                   int64_t* first, int64_t* added) {
+    const int64_t N = c->geo.N;
+    int64_t* counts = reinterpret_cast<int64_t*>(c->d_scratch + N / 8 + 8);  // after the need bytes
+    const int64_t chunk = (N + kStoreBlocks - 1) / kStoreBlocks;
+    store_count_kernel<<<kStoreBlocks, 256, 0, c->stream>>>(need, N, chunk, counts);
+    CL_LAUNCH_CHECK("store_count_kernel");
+    std::vector<int64_t> h(kStoreBlocks);
+    CL_CUDA(cudaMemcpyAsync(h.data(), counts, sizeof(int64_t) * kStoreBlocks, cudaMemcpyDeviceToHost, c->stream));
+    CL_CUDA(cudaStreamSynchronize(c->stream));
+    int64_t total = 0;
+    for (int b = 0; b < kStoreBlocks; ++b) { const int64_t v = h[b]; h[b] = total; total += v; }
+    *first = *n_stored;
+    *added = total;
+    if (total == 0) return CL_OK;
+    if (*n_stored + total > N) { set_error("storage overflow"); return CL_ERR_STATE; }
+    CL_CUDA(cudaMemcpyAsync(counts, h.data(), sizeof(int64_t) * kStoreBlocks, cudaMemcpyHostToDevice, c->stream));
+    store_write_kernel<<<kStoreBlocks, 256, 0, c->stream>>>(need, N, chunk, counts, *n_stored, site_of, sidx);
+    CL_LAUNCH_CHECK("store_write_kernel");
+    CL_CUDA(cudaStreamSynchronize(c->stream));   // h is read by the copy above
+    *n_stored += total;
+    return CL_OK;
+}
+
 int store_update(Ctx* c, int all) {
     const int64_t N = c->geo.N;
     if (!c->d_sidx) {
@@ -114,31 +142,18 @@ int store_update(Ctx* c, int all) {
     }
     if (c->n_stored == N) { c->store_dirty = false; return CL_OK; }
     uint8_t* need = reinterpret_cast<uint8_t*>(c->d_scratch);            // N bytes
-    int64_t* counts = reinterpret_cast<int64_t*>(c->d_scratch + N / 8 + 8); // after them
     store_need_kernel<<<grid_for(N, 256, 148 * 16), 256, 0, c->stream>>>(
         c->geo, c->d_ade_cls, c->ade_nodyn_coupled ? 1 : 0, all, c->d_sidx, need);
     CL_LAUNCH_CHECK("store_need_kernel");
-    const int64_t chunk = (N + kStoreBlocks - 1) / kStoreBlocks;
-    store_count_kernel<<<kStoreBlocks, 256, 0, c->stream>>>(need, N, chunk, counts);
-    CL_LAUNCH_CHECK("store_count_kernel");
-    std::vector<int64_t> h(kStoreBlocks);
-    CL_CUDA(cudaMemcpyAsync(h.data(), counts, sizeof(int64_t) * kStoreBlocks, cudaMemcpyDeviceToHost, c->stream));
-    CL_CUDA(cudaStreamSynchronize(c->stream));
-    int64_t total = 0;
-    for (int b = 0; b < kStoreBlocks; ++b) { const int64_t v = h[b]; h[b] = total; total += v; }
+    int64_t first = 0, total = 0;
+    int r = assign_storage(c, need, c->d_sidx, c->d_site_of, &c->n_stored, &first, &total);
+    if (r) return r;
     if (total > 0) {
-        if (c->n_stored + total > N) { set_error("transport storage overflow"); return CL_ERR_STATE; }
-        CL_CUDA(cudaMemcpyAsync(counts, h.data(), sizeof(int64_t) * kStoreBlocks, cudaMemcpyHostToDevice, c->stream));
-        store_write_kernel<<<kStoreBlocks, 256, 0, c->stream>>>(need, N, chunk, counts, c->n_stored, c->d_site_of,
-                                                                c->d_sidx);
-        CL_LAUNCH_CHECK("store_write_kernel");
         InitPop ip{};
         for (int m = 0; m < c->ap.n_mob; ++m) ip.c0[m] = (float)c->cfg.c0[c->ap.mob_index[m]];
         store_init_kernel<<<grid_for(total, 256, 148 * 16), 256, 0, c->stream>>>(
-            c->d_g, N, c->ap.n_mob, ip, c->n_stored, c->n_stored + total);
+            c->d_g, N, c->ap.n_mob, ip, first, first + total);
         CL_LAUNCH_CHECK("store_init_kernel");
-        CL_CUDA(cudaStreamSynchronize(c->stream));   // h is read by the copy above
-        c->n_stored += total;
     }
     c->store_dirty = false;
     return CL_OK;

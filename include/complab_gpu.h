@@ -287,8 +287,10 @@ int cl_step(cl_ctx* ctx, int32_t n);
 int cl_get_field(cl_ctx* ctx, int32_t field, int32_t index, double* host_out);
 int cl_set_field(cl_ctx* ctx, int32_t field, int32_t index, const double* host_in);
 
-/* raw populations (debug/parity): flow 19*N floats as deviations f-t_i in the
- * natural (post-stream) order; solute s: 7*N floats of g_i. */
+/* raw populations (debug/parity, checkpoints): flow 19*N floats as deviations
+ * f-t_i in the natural (post-stream) order; solute s: 7*N floats of g_i.
+ * Reading the flow needs a flow field (cl_flow_init or a set), setting it the
+ * mask (CL_ERR_STATE otherwise). */
 int cl_get_flow_populations(cl_ctx* ctx, float* host_out);
 int cl_set_flow_populations(cl_ctx* ctx, const float* host_in);
 int cl_get_solute_populations(cl_ctx* ctx, int32_t s, float* host_out);

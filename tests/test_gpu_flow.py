@@ -115,3 +115,95 @@ def test_couple_velocity(gpu_lib, pkg, wl):
     for k in range(3):
         np.testing.assert_allclose(lat.field(pkg.FIELD_VELOCITY, k), lat.field(pkg.FIELD_FLOW_U, k), rtol=0, atol=0)
     lat.close()
+
+
+def _dilate19(wl, live):
+    """live or a D3Q19 neighbour live (x not periodic, y and z periodic)."""
+    out = live.copy()
+    for (dx, dy, dz) in wl.D3Q19[1:]:
+        sh = np.roll(np.roll(live, dy, axis=1), dz, axis=2)
+        if dx == 1:
+            out[1:] |= sh[:-1]
+        elif dx == -1:
+            out[:-1] |= sh[1:]
+        else:
+            out |= sh
+    return out
+
+
+def _sealed_block(wl, nx=22, ny=16, nz=16):
+    """A duct with a 7^3 block: a bounce-back shell around a solid (NoDynamics)
+    5^3 core that no streaming site reaches."""
+    mask = np.full((nx, ny, nz), wl.MAT_PORE, np.uint8)
+    mask[8:15, 4:11, 4:11] = wl.MAT_BB
+    mask[9:14, 5:10, 5:10] = wl.MAT_SOLID
+    return mask
+
+
+def test_flow_compact_storage_matches_full_layout(gpu_lib, pkg, wl):
+    """The compact flow storage (the sites that stream and their D3Q19
+    neighbours) against every site stored, which is the full-lattice layout
+    (storage index = site index): the same state set in natural order on both,
+    then steps of both parities, then the sealed core opened (a mask change
+    that stores new sites) and more steps.  Bit-exact: the arithmetic is the
+    same, only the addressing differs.  -0.0 marks the unneeded sites of the
+    full layout (any nonzero bit pattern is stored; the arithmetic reads it as
+    the 0 an unstored site reads as), and compares equal to 0."""
+    mask = _sealed_block(wl)
+    nx, ny, nz = mask.shape
+    cfg = pkg.make_config(nx, ny, nz, tau_ns=0.8, rho_in=1.001, rho_out=1.0)
+    ns, _ = o.classes(cfg, mask.reshape(-1))
+    need = _dilate19(wl, np.isin(ns, [2, 3]).reshape(mask.shape)).reshape(-1)
+    assert need.sum() == mask.size - 5 ** 3
+    a = pkg.Lattice(cfg)
+    a.upload_mask(mask)
+    a.flow_init()
+    a.flow_steps(41)
+    P = a.flow_populations()
+    assert np.all(P[:, ~need] == 0.0)
+    full = P.copy()
+    full[:, ~need] = -0.0
+    b = pkg.Lattice(cfg)
+    b.upload_mask(mask)
+    b.set_flow_populations(full)
+    c = pkg.Lattice(cfg)
+    c.upload_mask(mask)
+    c.set_flow_populations(P)
+    np.testing.assert_array_equal(c.flow_populations(), P)
+    for lat in (a, b, c):
+        lat.flow_steps(7)
+    pa, pb, pc = (lat.flow_populations() for lat in (a, b, c))
+    np.testing.assert_array_equal(pb, pc)
+    np.testing.assert_array_equal(pa, pc)
+    # the inner 3^3 of the core reads only core slots at either parity: stored
+    # -0.0 on the full layout, unstored 0 on the compact one
+    inner = np.zeros(mask.shape, bool)
+    inner[10:13, 6:9, 6:9] = True
+    inner = inner.reshape(-1)
+    assert np.signbit(pb[:, inner]).all() and not np.signbit(pc[:, inner]).any()
+    opened = mask.copy()
+    opened[8:15, 4:11, 4:11] = wl.MAT_PORE
+    for lat in (a, b, c):
+        lat.upload_mask(opened)
+        lat.flow_steps(9)
+    pa, pb, pc = (lat.flow_populations() for lat in (a, b, c))
+    np.testing.assert_array_equal(pb, pc)
+    np.testing.assert_array_equal(pa, pc)
+    core = np.zeros(mask.shape, bool)
+    core[9:14, 5:10, 5:10] = True
+    assert np.abs(pc[:, core.reshape(-1)]).max() > 0      # the flow reached the opened core
+    rho_b, rho_c = b.field(pkg.FIELD_FLOW_RHO), c.field(pkg.FIELD_FLOW_RHO)
+    np.testing.assert_array_equal(rho_b, rho_c)
+    for lat in (a, b, c):
+        lat.close()
+
+
+def test_flow_populations_need_state(gpu_lib, pkg, wl):
+    mask = _sealed_block(wl)
+    cfg = pkg.make_config(*mask.shape, tau_ns=0.8)
+    lat = pkg.Lattice(cfg)
+    with pytest.raises(pkg.CLError):
+        lat.flow_populations()                  # no flow field yet
+    with pytest.raises(pkg.CLError):
+        lat.set_flow_populations(np.zeros((19, mask.size), np.float32))   # no mask yet
+    lat.close()
