@@ -41,7 +41,11 @@ namespace cl {
 
 #define THRD 1e-12
 constexpr int kGroup = 4;        // solutes whose populations are in flight together (reactions)
-constexpr int kStreamGroup = 4;  // the same in the streaming launch
+constexpr int kStreamGroupEven = 4, kStreamGroupOdd = 4;
+// the same in the streaming launch: an odd step's loads and stores address
+// neighbours' slots, so fewer solutes are in flight there to stay within the
+// 128 registers of two 256-thread blocks per SM
+template <int PARITY> constexpr int stream_group() { return PARITY ? kStreamGroupOdd : kStreamGroupEven; }
 
 struct AdeK {
     Geo g;
@@ -69,7 +73,8 @@ struct AdeK {
 // its six face neighbours (the sites at +c_d, d = 1..6); where x leaves the
 // lattice the own index stands in (that slot is reflected, never read there).
 // Returns false, with in-bounds substitutes, if a slot the step needs has no
-// storage (the caller counts it; the step then reports an error).
+// storage (the caller counts it; the step then reports an error).  An even
+// step touches only the site's own slots: PARITY 0 looks up no neighbour.
 struct SSite {
     uint32_t s;
     uint32_t nb[6];
@@ -77,6 +82,7 @@ struct SSite {
     __device__ __forceinline__ bool inx(int dx) const { return dx < 0 ? hxm : (dx > 0 ? hxp : true); }
 };
 
+template <int PARITY = 1>
 __device__ __forceinline__ bool make_ssite(const Geo& g, const int32_t* __restrict__ sidx, int x, int y, int z,
                                            uint32_t n, SSite& t) {
     const Site st = make_site(g, x, y, z, n);
@@ -89,7 +95,7 @@ __device__ __forceinline__ bool make_ssite(const Geo& g, const int32_t* __restri
 #pragma unroll
     for (int d = 1; d < 7; ++d) {
         uint32_t v = t.s;
-        if (st.inx(c7x(d))) {
+        if (PARITY == 1 && st.inx(c7x(d))) {
             const int32_t q = sidx[st.at(c7x(d), c7y(d), c7z(d))];
             if (q < 0) ok = false;
             else v = (uint32_t)q;
@@ -483,7 +489,7 @@ ade_react_kernel(const __grid_constant__ AdeK k, const uint32_t* __restrict__ li
         const int x = (int)(q / (uint32_t)k.g.ny);
         const int y = (int)(q - (uint32_t)x * (uint32_t)k.g.ny);
         SSite st;
-        if (!make_ssite(k.g, k.sidx, x, y, z, n, st)) atomicAdd(&k.counters[1], 1ull);
+        if (!make_ssite<PARITY>(k.g, k.sidx, x, y, z, n, st)) atomicAdd(&k.counters[1], 1ull);
         for (int s = 0; s < p.S; ++s) cApp[s * kReactBlock] = 0.0;
 #pragma unroll
         for (int m0 = 0; m0 < NMOB; m0 += kGroup) {
@@ -514,7 +520,7 @@ ade_react_kernel(const __grid_constant__ AdeK k, const uint32_t* __restrict__ li
 }
 
 template <int NMOB, int PARITY>
-__global__ void __launch_bounds__(256) ade_stream_kernel(const __grid_constant__ AdeK k,
+__global__ void __launch_bounds__(256, 2) ade_stream_kernel(const __grid_constant__ AdeK k,
                                                           const float* __restrict__ dc, int any_rxn,
                                                           const uint32_t* __restrict__ list, int64_t r0,
                                                           int64_t r1) {
@@ -534,17 +540,18 @@ __global__ void __launch_bounds__(256) ade_stream_kernel(const __grid_constant__
         const int y = (int)(q - (uint32_t)x * (uint32_t)k.g.ny);
         const bool rc = any_rxn && (cls & F_REACTIVE);
         SSite st;
-        if (!make_ssite(k.g, k.sidx, x, y, z, n, st)) atomicAdd(&k.counters[1], 1ull);
+        if (!make_ssite<PARITY>(k.g, k.sidx, x, y, z, n, st)) atomicAdd(&k.counters[1], 1ull);
         const float ux = k.u[n], uy = k.u[N + n], uz = k.u[2 * N + n];
         const bool adj = (x == 1 || x == k.g.nx - 2);
+        constexpr int kSG = stream_group<PARITY>();
 #pragma unroll
-        for (int m0 = 0; m0 < NMOB; m0 += kStreamGroup) {
-            float f[kStreamGroup][7];
+        for (int m0 = 0; m0 < NMOB; m0 += kSG) {
+            float f[kSG][7];
 #pragma unroll
-            for (int g = 0; g < kStreamGroup; ++g)
+            for (int g = 0; g < kSG; ++g)
                 if (m0 + g < NMOB) gather7<PARITY>(k.pop + (int64_t)(m0 + g) * 7 * N, N32, st, f[g]);
 #pragma unroll
-            for (int g = 0; g < kStreamGroup; ++g) {
+            for (int g = 0; g < kSG; ++g) {
                 const int m = m0 + g;
                 if (m >= NMOB) continue;
                 float rho = 0.f;
@@ -569,7 +576,7 @@ __global__ void __launch_bounds__(256) ade_stream_kernel(const __grid_constant__
                 }
             }
 #pragma unroll
-            for (int g = 0; g < kStreamGroup; ++g)
+            for (int g = 0; g < kSG; ++g)
                 if (m0 + g < NMOB) scatter7<PARITY>(k.pop + (int64_t)(m0 + g) * 7 * N, N32, st, f[g]);
         }
     }
@@ -592,7 +599,7 @@ __global__ void __launch_bounds__(256) ade_boundary_kernel(const __grid_constant
         int x, y, z;
         decode(k.g, n, x, y, z);
         SSite st;
-        if (!make_ssite(k.g, k.sidx, x, y, z, (uint32_t)n, st)) atomicAdd(&k.counters[1], 1ull);
+        if (!make_ssite<PARITY>(k.g, k.sidx, x, y, z, (uint32_t)n, st)) atomicAdd(&k.counters[1], 1ull);
         const float ux = k.u[n], uy = k.u[N + n], uz = k.u[2 * N + n];
 #pragma unroll
         for (int m = 0; m < NMOB; ++m) {

@@ -23,7 +23,7 @@ template <int NMOB, int PARITY>
 __device__ __forceinline__ void voxel_densities(const AdeK& k, int x, int y, int z, uint32_t n, double* C) {
     const AdeParams& p = k.p;
     SSite st;
-    if (!make_ssite(k.g, k.sidx, x, y, z, n, st)) atomicAdd(&k.counters[1], 1ull);
+    if (!make_ssite<PARITY>(k.g, k.sidx, x, y, z, n, st)) atomicAdd(&k.counters[1], 1ull);
     const uint32_t N32 = (uint32_t)k.g.N;
 #pragma unroll
     for (int m = 0; m < NMOB; ++m) {
