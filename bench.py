@@ -234,6 +234,25 @@ def cpu_coupled(steps, seed=5):
     return N * steps / dt / 1e6, dt, threads, sample
 
 
+def cpu_pcf(n=16384):
+    """The oracle's PCF + Anderson (the reference's code restated; identical
+    iterates, tests/test_oracle_pcf.py) on the first n voxels of the
+    speciation batch, all host threads: solves per second."""
+    pkg, wl = load_pkg(), load_workloads()
+    from oracle import oracle as o
+    S, logk, cs = wl.tableau(5, 9, seed=4)
+    sys_ = pkg.EqSystem()
+    pkg.set_eq_system(sys_, S, logk, cs, max_iter=200, tol=1e-10, warm_iter=6)
+    T, _, _, _ = wl.speciation_batch(S, logk, n, seed=302)
+    c = wl.cold_species(S, T, cs)
+    t0 = time.perf_counter()
+    _, it, cv = o.pcf_batch(sys_, c)
+    dt = time.perf_counter() - t0
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"solves_per_s": n / dt, "cores": threads, "kind": "port", "mean_iters": float(it.mean()),
+            "converged": float(cv.mean()), "sample": "%d voxels of the same batch" % n}
+
+
 def run_reference(args, rank):
     if rank != 0:
         return
@@ -331,6 +350,17 @@ def speciation_bench(pkg, wl, stream, n_train=1 << 20, n_test=1 << 21):
                             pkg.EQ_START_GIVEN)
         res["breakdown_ms"][name] = timed(run)
         res["breakdown_ms"][name + "_mean_iters"] = float(I.float().mean().item())
+    # the reference's live solver (PCF + Anderson) on the same voxels, from
+    # their cold species vectors (calculate_species_concentrations)
+    Pout = torch.zeros_like(eC)
+    PI = torch.zeros(n_test, dtype=torch.int32, device=dev)
+    PC = torch.zeros(n_test, dtype=torch.uint8, device=dev)
+    pcf_run = lambda: eq.pcf_device(eC.data_ptr(), Pout.data_ptr(), PI.data_ptr(), PC.data_ptr(), n_test)
+    pcf_run()
+    pms = timed(pcf_run)
+    res["pcf"] = {"ms": pms, "solves_per_s": n_test / (pms * 1e-3), "mean_iters": float(PI.float().mean().item()),
+                  "converged": float(PC.float().mean().item()),
+                  "solver": "PCF + Anderson depth 4, ||f||_2 < 1e-10, <= 200 iterations (the reference's settings)"}
     # same roots and residuals where both converged
     from_cold, from_learned = res["cold"].pop("x"), res["learned"].pop("x")
     both = res["cold"].pop("ok") & res["learned"].pop("ok")
@@ -514,6 +544,8 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         cm, cdt, threads, sample = cpu_coupled(40)
         out["cpu_baseline"] = {"value": cm, "unit": "MLUPS", "cores": threads, "kind": "port", "sample": sample}
+        if "speciation" in out:
+            out["speciation"]["pcf"]["cpu"] = cpu_pcf()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

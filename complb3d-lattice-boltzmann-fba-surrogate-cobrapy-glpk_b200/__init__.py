@@ -27,6 +27,7 @@ FIELD_CONC, FIELD_BIOMASS, FIELD_VELOCITY, FIELD_FLOW_RHO, FIELD_FLOW_U, FIELD_P
 FIELD_CA_AGE, FIELD_CA_TOTAL = 7, 8
 RED_SUM, RED_MIN, RED_MAX, RED_COUNT_EQ = range(4)
 EQ_START_COLD, EQ_START_GIVEN, EQ_START_LEARNED = range(3)
+EQ_SOLVER_NEWTON, EQ_SOLVER_PCF = 0, 1
 SRG_TENSOR, SRG_FP32 = 0, 1
 MAX_SRG_ORG = 2
 SRG_IN_FIN, SRG_IN_CONC, SRG_IN_BIOMASS = 0, 1, 2
@@ -45,7 +46,8 @@ class Rxn(ctypes.Structure):
 class EqSystem(ctypes.Structure):
     _fields_ = [("n_comp", c_int32), ("n_species", c_int32), ("comp_species", c_int32 * MAX_COMP),
                 ("stoich", (c_double * MAX_COMP) * MAX_SPECIES), ("logk", c_double * MAX_SPECIES),
-                ("max_iter", c_int32), ("tol", c_double), ("warm_iter", c_int32)]
+                ("max_iter", c_int32), ("tol", c_double), ("warm_iter", c_int32),
+                ("solver", c_int32), ("anderson_depth", c_int32)]
 
 
 class Phase(ctypes.Structure):
@@ -235,8 +237,10 @@ def add_phase(cfg, substrate, full_density, material=0, initial_fill=0.0, is_pre
     return ph
 
 
-def set_eq_system(sys, stoich, logk, comp_species, max_iter=100, tol=1e-10, warm_iter=8):
-    """Fill an EqSystem from an (ns x nc) stoichiometry matrix."""
+def set_eq_system(sys, stoich, logk, comp_species, max_iter=100, tol=1e-10, warm_iter=8, solver=0,
+                  anderson_depth=0):
+    """Fill an EqSystem from an (ns x nc) stoichiometry matrix.  solver:
+    EQ_SOLVER_NEWTON or EQ_SOLVER_PCF (the reference's live PCF + Anderson)."""
     stoich = np.asarray(stoich, float)
     ns, nc = stoich.shape
     sys.n_comp, sys.n_species = nc, ns
@@ -247,6 +251,7 @@ def set_eq_system(sys, stoich, logk, comp_species, max_iter=100, tol=1e-10, warm
             sys.stoich[i][j] = stoich[i, j]
         sys.logk[i] = logk[i]
     sys.max_iter, sys.tol, sys.warm_iter = max_iter, tol, warm_iter
+    sys.solver, sys.anderson_depth = solver, anderson_depth
     return sys
 
 
@@ -425,6 +430,7 @@ def _bind_eq(lib):
         ("cl_eq_param_count", [vp, P(c_int32)]), ("cl_eq_get_params", [vp, vp]),
         ("cl_eq_set_params", [vp, vp]), ("cl_eq_predict_host", [vp, vp, vp, c_int32]),
         ("cl_eq_predict_device", [vp, vp, vp, c_int64]),
+        ("cl_eq_pcf_device", [vp, vp, vp, vp, vp, c_int64]), ("cl_eq_pcf_host", [vp, vp, vp, vp, vp, c_int64]),
         ("cl_surrogate_batch_device", [P(SurrogateNet), vp, vp, c_int64, c_int32, vp]),
         ("cl_surrogate_batch_host", [P(SurrogateNet), vp, vp, c_int64, c_int32]),
     ]:
@@ -474,6 +480,22 @@ class EqSolver:
         _check(self.lib, self.lib.cl_eq_solve_host(self.h, _ptr(T), _ptr(cs) if cs is not None else None, _ptr(x),
                                                    _ptr(it), _ptr(stt), n, start), "cl_eq_solve_host")
         return x, it, stt
+
+    def pcf(self, species):
+        """The reference's live solve (PCF + Anderson) of each row of species
+        (n x n_species): species out, iterations, converged flags."""
+        c = np.ascontiguousarray(species, np.float64).reshape(-1, self.ns)
+        n = c.shape[0]
+        out = np.zeros_like(c)
+        it = np.zeros(n, np.int32)
+        cv = np.zeros(n, np.uint8)
+        _check(self.lib, self.lib.cl_eq_pcf_host(self.h, _ptr(c), _ptr(out), _ptr(it), _ptr(cv), n), "cl_eq_pcf_host")
+        return out, it, cv
+
+    def pcf_device(self, d_in, d_out, d_iters, d_conv, n):
+        """PCF + Anderson on device species rows (device pointers)."""
+        return _check(self.lib, self.lib.cl_eq_pcf_device(self.h, d_in, d_out, d_iters, d_conv, n),
+                      "cl_eq_pcf_device")
 
     def solve_device(self, d_totals, d_cold, d_x, d_iters, d_status, n, start):
         """Device-pointer variant (ints from torch.Tensor.data_ptr())."""

@@ -36,6 +36,7 @@
 #pragma once
 #include "internal.h"
 #include "newton.cuh"
+#include "pcf.cuh"
 
 namespace cl {
 
@@ -321,10 +322,36 @@ __device__ __forceinline__ void dissol_gather(const AdeK& k, int64_t n, int x, i
     }
 }
 
+// run_equilibrium_biotic with the reference's live solver
+// (part4_eqsolver.hh:1355-1494 -> calculate_species_concentrations, :1187):
+// totals and cold start from the voxel's species, PCF + Anderson, and the
+// species it ends at applied through the processor's limiter whether or not
+// the solve converged.  Returns 1 if the solve did not converge.
+template <int NC>
+__device__ __forceinline__ int pcf_voxel(const EqDev& e, int S, int max_iter, double tol, double* Cur, double* App,
+                                      int cs, int32_t* iters_out) {
+    double T[NC], x[NC];
+    pcf_totals_and_start<NC>(e, Cur, cs, T, x);
+    int conv = 0;
+    const int it = eq_pcf<NC>(e, T, Cur, cs, x, max_iter, tol, e.depth, &conv);
+    if (iters_out) *iters_out = it;
+    for (int s = 0; s < S && s < e.ns; ++s) {
+        const double c0 = Cur[s * cs];
+        const double conc = fmax(c0, 1e-30);
+        double eqc = e.active[s] ? pcf_species<NC>(e, s, x, conc) : pcf_passive(conc);
+        double d = eqc - conc;
+        const double mx = fmax(1e-9, 0.1 * fabs(conc));
+        if (fabs(d) > mx) d = d > 0 ? mx : -mx;
+        if (conc + d < 1e-20) d = 1e-20 - conc;
+        if (fabs(d) > THRD) { Cur[s * cs] += d; App[s * cs] += d; }
+    }
+    return conv ? 0 : 1;
+}
+
 // The reaction chain of one voxel.  Cur holds the current densities (updated
 // as each processor applies its increments), App the total increment per
 // solute.  Returns 1 if the equilibrium solve did not converge.
-template <int NC>
+template <int NC, int SOLVER>
 __device__ int reaction_chain(const AdeK& k, int64_t n, int x, int y, int z, uint8_t cls, double* Cur, double* App,
                               int cs, double* R, double* B, double* BR, int bd) {
     const AdeParams& p = k.p;
@@ -368,6 +395,12 @@ __device__ int reaction_chain(const AdeK& k, int64_t n, int x, int y, int z, uin
     // 1e-30; Newton applied only when converged (run_equilibrium_NR, NR_reserve.hh:734)
     if constexpr (NC > 0) {
         const EqDev& e = k.e;
+        if constexpr (SOLVER == CL_EQ_SOLVER_PCF) {
+            int32_t it = 0;
+            nonconv = pcf_voxel<NC>(e, p.S, p.eq.max_iter, p.eq.tol, Cur, App, cs, &it);
+            if (k.eq_iters) k.eq_iters[n] = it;
+            return nonconv;
+        }
         double x[NC], T[NC];
 #pragma unroll
         for (int j = 0; j < NC; ++j) T[j] = 0.0;
@@ -462,7 +495,7 @@ __device__ int reaction_chain(const AdeK& k, int64_t n, int x, int y, int z, uin
 // for the part still resident and from HBM otherwise.
 constexpr int kReactBlock = 128;
 
-template <int NMOB, int NC, int PARITY>
+template <int NMOB, int NC, int PARITY, int SOLVER>
 __global__ void __launch_bounds__(kReactBlock, 4)
 ade_react_kernel(const __grid_constant__ AdeK k, const uint32_t* __restrict__ list, int64_t r0, int64_t count,
                  float* __restrict__ dc) {
@@ -508,7 +541,7 @@ ade_react_kernel(const __grid_constant__ AdeK k, const uint32_t* __restrict__ li
         }
         for (int s = 0; s < p.S; ++s)
             if (p.mob_slot[s] < 0) cCur[s * kReactBlock] = k.imm[(int64_t)s * N + n];
-        nonconv += reaction_chain<NC>(k, n, x, y, z, cls, cCur, cApp, kReactBlock, Rw + t, Bw + t, BRw + t,
+        nonconv += reaction_chain<NC, SOLVER>(k, n, x, y, z, cls, cCur, cApp, kReactBlock, Rw + t, Bw + t, BRw + t,
                                       kReactBlock);
         for (int s = 0; s < p.S; ++s)
             if (p.mob_slot[s] < 0 && cApp[s * kReactBlock] != 0.0) k.imm[(int64_t)s * N + n] += cApp[s * kReactBlock];
@@ -651,23 +684,32 @@ inline AdeK make_adek(Ctx* c) {
 // the phase voxels' releases of this step (dissolution.cu), before the fused launch
 int dissol_release(Ctx* c, const AdeK& k);
 
+template <int NMOB, int NC, int PARITY, int SOLVER>
+inline int launch_react_as(Ctx* c, const AdeK& k, cudaStream_t st, int64_t r0, int64_t r1, int rblocks,
+                           size_t smem) {
+    auto kern = ade_react_kernel<NMOB, NC, PARITY, SOLVER>;
+    CL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<rblocks, kReactBlock, smem, st>>>(k, c->d_live, r0, r1, c->d_dc);
+    CL_LAUNCH_CHECK("ade_react_kernel");
+    c->launches += 1;
+    return CL_OK;
+}
+
+// the reaction launch over list entries [r0, r1); the PCF solver (equilibrium
+// components only) is a separate instantiation so the Newton one keeps its
+// registers
 template <int NMOB, int NC>
 inline int launch_react(Ctx* c, const AdeK& k, cudaStream_t st, int64_t r0, int64_t r1, int max_blocks) {
     const int S = c->ap.S, M = c->ap.M > 0 ? c->ap.M : 1;
     const size_t smem = (size_t)(3 * S + 2 * M) * kReactBlock * sizeof(double);
     const int rblocks = grid_for(r1 - r0, kReactBlock, max_blocks);
-    if (c->ade_parity == 0) {
-        auto kern = ade_react_kernel<NMOB, NC, 0>;
-        CL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        kern<<<rblocks, kReactBlock, smem, st>>>(k, c->d_live, r0, r1, c->d_dc);
-    } else {
-        auto kern = ade_react_kernel<NMOB, NC, 1>;
-        CL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        kern<<<rblocks, kReactBlock, smem, st>>>(k, c->d_live, r0, r1, c->d_dc);
-    }
-    CL_LAUNCH_CHECK("ade_react_kernel");
-    c->launches += 1;
-    return CL_OK;
+    constexpr int PCF = NC > 0 ? CL_EQ_SOLVER_PCF : CL_EQ_SOLVER_NEWTON;
+    const bool pcf = NC > 0 && k.e.solver == CL_EQ_SOLVER_PCF;
+    if (c->ade_parity == 0)
+        return pcf ? launch_react_as<NMOB, NC, 0, PCF>(c, k, st, r0, r1, rblocks, smem)
+                   : launch_react_as<NMOB, NC, 0, CL_EQ_SOLVER_NEWTON>(c, k, st, r0, r1, rblocks, smem);
+    return pcf ? launch_react_as<NMOB, NC, 1, PCF>(c, k, st, r0, r1, rblocks, smem)
+               : launch_react_as<NMOB, NC, 1, CL_EQ_SOLVER_NEWTON>(c, k, st, r0, r1, rblocks, smem);
 }
 
 template <int NMOB>

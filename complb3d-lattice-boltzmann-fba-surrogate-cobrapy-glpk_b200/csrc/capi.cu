@@ -119,6 +119,11 @@ static int validate(const cl_config* c) {
             set_error("equilibrium in the transport step needs 1..5 components and one species per solute");
             return CL_ERR_ARG;
         }
+        if ((e.solver != CL_EQ_SOLVER_NEWTON && e.solver != CL_EQ_SOLVER_PCF) || e.anderson_depth < 0 ||
+            e.anderson_depth > 8) {
+            set_error("unknown equilibrium solver, or anderson_depth outside 0..8");
+            return CL_ERR_ARG;
+        }
     }
     return CL_OK;
 }

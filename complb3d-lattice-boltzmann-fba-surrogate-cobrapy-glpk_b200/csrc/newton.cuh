@@ -37,6 +37,9 @@ struct EqDev {
     int active[CL_MAX_SPECIES];
     int comp_species[CL_MAX_COMP];
     int neg[CL_MAX_COMP];              // some species carries component j with a negative power
+    double inv_mu[CL_MAX_COMP];        // PCF: 1 / the smallest positive coefficient of component j (at most 1)
+    int solver;                        // CL_EQ_SOLVER_* of the transport step
+    int depth;                         // PCF Anderson depth
 };
 
 inline void eqdev_from_system(const cl_eq_system& s, EqDev& d) {
@@ -61,7 +64,17 @@ inline void eqdev_from_system(const cl_eq_system& s, EqDev& d) {
         d.comp_species[j] = j < s.n_comp ? s.comp_species[j] : -1;
         d.neg[j] = 0;
         for (int i = 0; i < s.n_species && j < s.n_comp; ++i) if (d.ipow[i][j] < 0) d.neg[j] = 1;
+        // pcf_residual's mu_min (part4_eqsolver.hh:690-697): starts at 1, equilibrium species only
+        double mu_min = 1.0;
+        for (int i = 0; i < s.n_species && j < s.n_comp; ++i) {
+            if (!d.active[i]) continue;
+            const double mu = s.stoich[i][j];
+            if (mu > 1e-10 && mu < mu_min) mu_min = mu;
+        }
+        d.inv_mu[j] = 1.0 / mu_min;
     }
+    d.solver = s.solver;
+    d.depth = s.anderson_depth > 0 ? s.anderson_depth : 4;
 }
 
 // species concentration from the component logs, clamped as calc_species

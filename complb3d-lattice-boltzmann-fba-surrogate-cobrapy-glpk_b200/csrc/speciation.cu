@@ -15,6 +15,7 @@
 // the starting point.
 #include "internal.h"
 #include "newton.cuh"
+#include "pcf.cuh"
 #include "mma.cuh"
 #include <cmath>
 #include <vector>
@@ -480,6 +481,33 @@ __global__ void newton_pass_warp_kernel(EqDev e, const double* totals, const dou
 
 using namespace cl;
 
+// calculate_species_concentrations (part4_eqsolver.hh:1187-1214) per entry:
+// one PCF + Anderson solve per thread from the entry's species row.
+template <int NC>
+__global__ void __launch_bounds__(128) pcf_batch_kernel(const __grid_constant__ EqDev e, const double* in,
+                                                        double* out, int32_t* iters, uint8_t* conv, int64_t n,
+                                                        int max_iter, double tol, unsigned long long* nonconv) {
+    unsigned long long miss = 0;
+    const int ns = e.ns;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const double* c = in + k * ns;
+        double T[NC], x[NC];
+        pcf_totals_and_start<NC>(e, c, 1, T, x);
+        int cv = 0;
+        const int it = eq_pcf<NC>(e, T, c, 1, x, max_iter, tol, e.depth, &cv);
+        for (int i = 0; i < ns; ++i) {
+            double v = e.active[i] ? pcf_species<NC>(e, i, x, c[i]) : pcf_passive(c[i]);
+            if (isnan(v) || isinf(v)) v = pcf_passive(c[i]);
+            out[k * ns + i] = pcf_max(pcf_min(v, 10.0), 1e-30);
+        }
+        if (iters) iters[k] = it;
+        if (conv) conv[k] = (uint8_t)cv;
+        miss += cv ? 0 : 1;
+    }
+    for (int o = 16; o > 0; o >>= 1) miss += __shfl_down_sync(0xffffffffu, miss, o);
+    if ((threadIdx.x & 31) == 0 && miss) atomicAdd(nonconv, miss);
+}
+
 struct cl_eq_solver {
     cl_eq_system sys;
     EqDev e;
@@ -499,6 +527,7 @@ struct cl_eq_solver {
     uint8_t* stop_mark = nullptr;     // solves that stopped early in the current phase
     int64_t fail_cap = 0;
     unsigned long long* fail_count = nullptr;   // two counters
+    unsigned long long* pcf_count = nullptr;    // PCF solves that did not converge
     uint64_t adam_t = 0;
 };
 
@@ -602,6 +631,12 @@ cl_eq_solver* cl_eq_create(const cl_eq_system* sys, void* stream, int* status) {
         if (status) *status = CL_ERR_ARG;
         return nullptr;
     }
+    if ((sys->solver != CL_EQ_SOLVER_NEWTON && sys->solver != CL_EQ_SOLVER_PCF) || sys->anderson_depth < 0 ||
+        sys->anderson_depth > kPcfMaxDepth) {
+        set_error("unknown equilibrium solver, or anderson_depth outside 0..8");
+        if (status) *status = CL_ERR_ARG;
+        return nullptr;
+    }
     cl_eq_solver* s = new cl_eq_solver();
     s->sys = *sys;
     eqdev_from_system(*sys, s->e);
@@ -629,6 +664,7 @@ cl_eq_solver* cl_eq_create(const cl_eq_system* sys, void* stream, int* status) {
     A((void**)&s->part, sizeof(float) * (size_t)s->part_blocks * (np + 1));
     A((void**)&s->grad, sizeof(float) * (np + 1));
     A((void**)&s->fail_count, 2 * sizeof(unsigned long long));
+    A((void**)&s->pcf_count, sizeof(unsigned long long));
     if (e != cudaSuccess) return fail(cuda_fail(e, "cl_eq_create"), s);
     if (cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mlp_smem_bytes()) != cudaSuccess ||
         cudaFuncSetAttribute(mlp_predict_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mlp_fwd_smem_bytes()) != cudaSuccess)
@@ -659,7 +695,7 @@ int cl_eq_destroy(cl_eq_solver* s) {
     if (!s) return CL_OK;
     if (s->stream) cudaStreamSynchronize(s->stream);
     void* ptrs[] = {s->w.W1, s->w.W2, s->w.W2T, s->w.W3, s->w.W3T, s->w.b, s->w.norm, s->master, s->m1, s->m2,
-                    s->part, s->grad, s->fail_list, s->fail_list2, s->stop_mark, s->fail_count};
+                    s->part, s->grad, s->fail_list, s->fail_list2, s->stop_mark, s->fail_count, s->pcf_count};
     for (void* p : ptrs) if (p) cudaFree(p);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     delete s;
@@ -706,6 +742,54 @@ int cl_eq_solve_device(cl_eq_solver* s, const double* d_totals, const double* d_
         case 4: return bucketed_solve<4>(s, d_totals, d_cold_species, d_logfree, d_iters, d_status, n, start);
         default: return bucketed_solve<5>(s, d_totals, d_cold_species, d_logfree, d_iters, d_status, n, start);
     }
+}
+
+int cl_eq_pcf_device(cl_eq_solver* s, const double* d_in, double* d_out, int32_t* d_iters, uint8_t* d_conv,
+                     int64_t n) {
+    if (!s || !d_in || !d_out || n < 0) { set_error("null argument"); return CL_ERR_ARG; }
+    if (n == 0) return CL_OK;
+    CL_CUDA(cudaMemsetAsync(s->pcf_count, 0, sizeof(unsigned long long), s->stream));
+    const int blocks = grid_for(n, 128, 148 * 8);
+    const int mi = s->sys.max_iter;
+    const double tol = s->sys.tol;
+    switch (s->nc) {
+        case 1: pcf_batch_kernel<1><<<blocks, 128, 0, s->stream>>>(s->e, d_in, d_out, d_iters, d_conv, n, mi, tol, s->pcf_count); break;
+        case 2: pcf_batch_kernel<2><<<blocks, 128, 0, s->stream>>>(s->e, d_in, d_out, d_iters, d_conv, n, mi, tol, s->pcf_count); break;
+        case 3: pcf_batch_kernel<3><<<blocks, 128, 0, s->stream>>>(s->e, d_in, d_out, d_iters, d_conv, n, mi, tol, s->pcf_count); break;
+        case 4: pcf_batch_kernel<4><<<blocks, 128, 0, s->stream>>>(s->e, d_in, d_out, d_iters, d_conv, n, mi, tol, s->pcf_count); break;
+        default: pcf_batch_kernel<5><<<blocks, 128, 0, s->stream>>>(s->e, d_in, d_out, d_iters, d_conv, n, mi, tol, s->pcf_count); break;
+    }
+    CL_LAUNCH_CHECK("pcf_batch_kernel");
+    unsigned long long miss = 0;
+    CL_CUDA(cudaMemcpyAsync(&miss, s->pcf_count, sizeof miss, cudaMemcpyDeviceToHost, s->stream));
+    CL_CUDA(cudaStreamSynchronize(s->stream));
+    return miss ? CL_WARN_NOT_CONVERGED : CL_OK;
+}
+
+int cl_eq_pcf_host(cl_eq_solver* s, const double* in, double* out, int32_t* iters, uint8_t* conv, int64_t n) {
+    if (!s || !in || !out || n < 0) { set_error("null argument"); return CL_ERR_ARG; }
+    if (n == 0) return CL_OK;
+    const int ns = s->sys.n_species;
+    double *dIn = nullptr, *dOut = nullptr;
+    int32_t* dI = nullptr;
+    uint8_t* dC = nullptr;
+    int r = CL_OK;
+    cudaError_t e = cudaMalloc(&dIn, sizeof(double) * n * ns);
+    if (e == cudaSuccess) e = cudaMalloc(&dOut, sizeof(double) * n * ns);
+    if (e == cudaSuccess) e = cudaMalloc(&dI, sizeof(int32_t) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&dC, n);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dIn, in, sizeof(double) * n * ns, cudaMemcpyHostToDevice, s->stream);
+    if (e != cudaSuccess) r = cuda_fail(e, "cl_eq_pcf_host");
+    if (!r) r = cl_eq_pcf_device(s, dIn, dOut, dI, dC, n);
+    if (r >= 0) {
+        e = cudaMemcpyAsync(out, dOut, sizeof(double) * n * ns, cudaMemcpyDeviceToHost, s->stream);
+        if (e == cudaSuccess && iters) e = cudaMemcpyAsync(iters, dI, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s->stream);
+        if (e == cudaSuccess && conv) e = cudaMemcpyAsync(conv, dC, n, cudaMemcpyDeviceToHost, s->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+        if (e != cudaSuccess) r = cuda_fail(e, "cl_eq_pcf_host");
+    }
+    cudaFree(dIn); cudaFree(dOut); cudaFree(dI); cudaFree(dC);
+    return r;
 }
 
 int cl_eq_predict_device(cl_eq_solver* s, const double* d_totals, double* d_logfree, int64_t n) {

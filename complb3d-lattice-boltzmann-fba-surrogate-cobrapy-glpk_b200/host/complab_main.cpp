@@ -1,7 +1,10 @@
 // complab_main.cpp -- host driver: CompLaB.xml in, the reference's time loop
 // (src/complab.cpp:560-1860) over the C ABI, fields out.
 //
-//   complab_b200 [CompLaB.xml] [--steps N] [--print-config] [--quiet]
+//   complab_b200 [CompLaB.xml] [--steps N] [--eq-solver newton|pcf] [--print-config] [--quiet]
+//
+// --eq-solver pcf runs the reference's live speciation solver (PCF + Anderson)
+// in the transport step; the default is Newton (or the XML's <solver>).
 //
 // Order, as main() of the reference runs it:
 //   read CompLaB.xml and the geometry (readGeometry, complab_functions.hh:127-156);
@@ -105,18 +108,27 @@ bool flow_solve(cl_ctx* h, long max_it, double eps, int* iters) {
 int main(int argc, char** argv) {
     std::string xml = "CompLaB.xml";
     long steps_override = -1;
+    int eq_solver = -1;
     bool print_config = false, quiet = false;
     for (int i = 1; i < argc; ++i) {
         const std::string a = argv[i];
         if (a == "--print-config") print_config = true;
         else if (a == "--quiet") quiet = true;
         else if (a == "--steps" && i + 1 < argc) steps_override = std::atol(argv[++i]);
+        else if (a == "--eq-solver" && i + 1 < argc && (std::strcmp(argv[i + 1], "pcf") == 0 ||
+                                                         std::strcmp(argv[i + 1], "newton") == 0))
+            eq_solver = std::strcmp(argv[++i], "pcf") == 0 ? CL_EQ_SOLVER_PCF : CL_EQ_SOLVER_NEWTON;
         else if (!a.empty() && a[0] != '-') xml = a;
-        else { std::fprintf(stderr, "usage: %s [CompLaB.xml] [--steps N] [--print-config] [--quiet]\n", argv[0]); return 2; }
+        else {
+            std::fprintf(stderr, "usage: %s [CompLaB.xml] [--steps N] [--eq-solver newton|pcf] [--print-config] [--quiet]\n",
+                         argv[0]);
+            return 2;
+        }
     }
     HostRun run;
     std::string err;
     if (clhost::read_complab_xml(xml, run, err)) { std::fprintf(stderr, "complab_b200: %s\n", err.c_str()); return 1; }
+    if (eq_solver >= 0) run.cfg.eq.solver = eq_solver;
     if (print_config) { std::printf("%s\n", clhost::run_json(run).c_str()); return 0; }
     if (steps_override >= 0) run.ade_max = steps_override;
     for (const std::string& n : run.notes) if (!quiet) std::fprintf(stderr, "complab_b200: note: %s\n", n.c_str());

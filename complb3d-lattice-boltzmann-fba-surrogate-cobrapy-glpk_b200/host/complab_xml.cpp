@@ -267,6 +267,15 @@ int read_complab_xml(const std::string& path, HostRun& run, std::string& err) {
             // Newton from its last converged solution (reference: cold start)
             if (const XmlNode* w = eq->find("warm_start"))
                 c.eq_warm_previous = lower(w->str()) == "previous" ? 1 : 0;
+            // extension: <solver>pcf</solver> runs the reference's live solver
+            // (PCF + Anderson, depth 4: complab.cpp:423-425) instead of Newton
+            if (const XmlNode* sv = eq->find("solver")) {
+                const std::string v = lower(sv->str());
+                if (v == "pcf") e.solver = CL_EQ_SOLVER_PCF;
+                else if (v == "newton") e.solver = CL_EQ_SOLVER_NEWTON;
+                else throw std::runtime_error("equilibrium solver must be newton or pcf");
+            }
+            e.anderson_depth = 4;
         }
 
         // precipitation (complab.cpp:272-294)
@@ -388,7 +397,8 @@ std::string run_json(const HostRun& r) {
     o << ", \"dt\": " << c.dt << ", \"n_microbes\": " << c.n_microbes
       << ", \"enable_kinetics\": " << c.enable_kinetics << ", \"enable_abiotic\": " << c.enable_abiotic
       << ", \"n_rxn\": " << c.n_rxn << ", \"use_equilibrium\": " << c.use_equilibrium
-      << ", \"n_comp\": " << c.eq.n_comp << ", \"comp_species\": ";
+      << ", \"n_comp\": " << c.eq.n_comp << ", \"eq_solver\": \"" << (c.eq.solver == CL_EQ_SOLVER_PCF ? "pcf" : "newton")
+      << "\", \"comp_species\": ";
     iarr(c.eq.comp_species, c.eq.n_comp);
     o << ", \"logk\": ";
     arr(c.eq.logk, c.use_equilibrium ? c.n_solutes : 0);

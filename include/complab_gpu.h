@@ -75,16 +75,33 @@ typedef struct {
 
 /* Components-and-species tableau (reference EquilibriumChemistry<T>,
  * src/complab3d_processors_part4_eqsolver.hh:186-1271).  Species are the
- * solutes in order; rows of all zeros are non-equilibrium species. */
+ * solutes in order; rows of all zeros are non-equilibrium species.
+ * solver selects the equilibrium solve of the transport step:
+ *   CL_EQ_SOLVER_NEWTON  Newton in log10 free components (the reference's
+ *                        reserve solver, NR_reserve.hh:512-615, with the
+ *                        safeguards listed in the design notes); a voxel whose
+ *                        solve does not converge is left unchanged;
+ *   CL_EQ_SOLVER_PCF     the reference's live solver: positive continued
+ *                        fractions with Anderson acceleration
+ *                        (solve_equilibrium_anderson, part4_eqsolver.hh:952-1172;
+ *                        convergence ||f||_2 < tol on the PCF correction, at most
+ *                        max_iter iterations, depth anderson_depth (0: 4, the
+ *                        setting of complab.cpp:425), condition limit 1e10,
+ *                        mixing 1); its result is applied whether or not it
+ *                        converged, as run_equilibrium_biotic applies it. */
+#define CL_EQ_SOLVER_NEWTON 0
+#define CL_EQ_SOLVER_PCF    1
 typedef struct {
     int32_t n_comp;
     int32_t n_species;                 /* == number of solutes it acts on */
     int32_t comp_species[CL_MAX_COMP]; /* species index named like component j, or -1 */
     double  stoich[CL_MAX_SPECIES][CL_MAX_COMP];
     double  logk[CL_MAX_SPECIES];
-    int32_t max_iter;                  /* Newton iterations (cold) */
-    double  tol;                       /* relative mass-balance residual */
+    int32_t max_iter;                  /* Newton iterations (cold); PCF iterations */
+    double  tol;                       /* Newton: relative mass-balance residual; PCF: ||f||_2 */
     int32_t warm_iter;                 /* k: Newton iterations allowed from the learned start */
+    int32_t solver;                    /* CL_EQ_SOLVER_* of the transport step */
+    int32_t anderson_depth;            /* PCF history depth (0: 4) */
 } cl_eq_system;
 
 /* Dissolvable solid phase (reference SolidPhase, src/dissolutionVOP.hh:142-154)
@@ -399,6 +416,21 @@ int cl_eq_solve_host(cl_eq_solver* s, const double* totals, const double* cold_s
 int cl_eq_solve_noalloc(const cl_eq_system* sys, const double* d_totals, const double* d_cold_species,
                         double* d_logfree, int32_t* d_iters, uint8_t* d_status,
                         int64_t n, int32_t start, void* stream);
+
+/* The reference's live speciation entry point, calculate_species_concentrations
+ * (src/complab3d_processors_part4_eqsolver.hh:1187-1214): per entry, the
+ * component totals of the given species (clamped to [1e-30, 10]), the PCF +
+ * Anderson solve from the reference's cold start, and the species it returns
+ * (non-equilibrium species pass through clamped; NaN / inf fall back to the
+ * input).  species_in / species_out: n*n_species.  iters: the reference's
+ * iteration count (getLastIterations); converged: 1 if ||f||_2 < tol was
+ * reached (didConverge).  Either may be NULL.  Uses the solver's tableau,
+ * max_iter, tol and anderson_depth.  Returns CL_WARN_NOT_CONVERGED if some
+ * entry did not converge. */
+int cl_eq_pcf_device(cl_eq_solver* s, const double* d_species_in, double* d_species_out,
+                     int32_t* d_iters, uint8_t* d_converged, int64_t n);
+int cl_eq_pcf_host(cl_eq_solver* s, const double* species_in, double* species_out,
+                   int32_t* iters, uint8_t* converged, int64_t n);
 
 /* ---- learned warm start: MLP n_comp -> 64 -> 64 -> n_comp, GELU, BF16 weights,
  *      FP32 accumulate, trained on the device by the library's own forward and

@@ -574,6 +574,203 @@ int orc_eq_newton(const cl_eq_system* sys, const double* totals, double* x,
     return max_iter;
 }
 
+/* ---- the reference's live solver: PCF + Anderson acceleration -------------
+ * Restates EquilibriumChemistry<T>::calculate_species_concentrations
+ * (src/complab3d_processors_part4_eqsolver.hh:1187-1214) and what it calls:
+ * calc_component_totals (:520-538), calc_species (:442-496),
+ * calc_reactive_product_sums (:540-640), pcf_residual (:664-726),
+ * qr_decomposition (:817-868), solve_upper_triangular (:887-904) and
+ * solve_equilibrium_anderson (:952-1172), with the reference's constants
+ * (condition limit 1e10, mixing 1).  The arithmetic is done in the
+ * reference's order (plain double multiply and add, glibc pow / log10), so
+ * built with the same compiler flags it reproduces the reference's iterates. */
+#define PCF_COND_TOL 1e10
+#define PCF_MAX_DEPTH 16
+/* std::min / std::max as the reference calls them: a NaN first argument
+ * passes through */
+static inline double smin(double a, double b) { return (b < a) ? b : a; }
+static inline double smax(double a, double b) { return (a < b) ? b : a; }
+
+/* calc_species: equilibrium species from the log free components; the others
+ * keep their input value (clamped), as does a species whose power overflows */
+static void pcf_species(const cl_eq_system* sys, const double* x, const double* init, double* c) {
+    for (int i = 0; i < sys->n_species; ++i) {
+        if (!eq_species_active(sys, i)) { c[i] = init[i] > MIN_CONC ? smin(init[i], MAX_CONC) : MIN_CONC; continue; }
+        double lc = sys->logk[i];
+        for (int j = 0; j < sys->n_comp; ++j) lc += sys->stoich[i][j] * x[j];
+        lc = smax(smin(lc, MAX_LOG_C), MIN_LOG_C);
+        double v = pow(10.0, lc);
+        if (isnan(v) || isinf(v)) v = init[i] > MIN_CONC ? init[i] : MIN_CONC;
+        c[i] = smax(smin(v, MAX_CONC), MIN_CONC);
+    }
+}
+
+/* the smallest positive stoichiometric coefficient of each component (at most 1) */
+static double pcf_mu_min(const cl_eq_system* sys, int j) {
+    double mu_min = 1.0;
+    for (int i = 0; i < sys->n_species; ++i) {
+        if (!eq_species_active(sys, i)) continue;
+        const double mu = sys->stoich[i][j];
+        if (mu > 1e-10 && mu < mu_min) mu_min = mu;
+    }
+    return mu_min;
+}
+
+/* pcf_residual: f_j = log10(S_P / S_R) / mu_min_j, clamped to +-10; 0 for a
+ * non-finite value and for an absent component (T_j <= 1e-18) */
+static void pcf_correction(const cl_eq_system* sys, const double* T, const double* x, const double* init,
+                           double* f) {
+    double c[CL_MAX_SPECIES];
+    pcf_species(sys, x, init, c);
+    for (int j = 0; j < sys->n_comp; ++j) {
+        double pos = 0.0, neg = 0.0;
+        for (int i = 0; i < sys->n_species; ++i) {
+            if (!eq_species_active(sys, i)) continue;
+            const double mu = sys->stoich[i][j];
+            const double ci = smax(c[i], MIN_CONC);
+            if (mu > 1e-15) pos += mu * ci;
+            else if (mu < -1e-15) neg += fabs(mu) * ci;
+        }
+        double sr, sp;
+        if (T[j] >= 0.0) { sr = pos; sp = T[j] + neg; }
+        else { sr = fabs(T[j]) + pos; sp = neg; }
+        sr = smax(sr, MIN_CONC);
+        sp = smax(sp, MIN_CONC);
+        double v = (1.0 / pcf_mu_min(sys, j)) * (log10(sp) - log10(sr));
+        v = smax(smin(v, 10.0), -10.0);
+        if (isnan(v) || isinf(v)) v = 0.0;
+        if (T[j] <= 1e-18) v = 0.0;
+        f[j] = v;
+    }
+}
+
+static double pcf_norm(const double* v, int n) {
+    double s = 0.0;
+    for (int k = 0; k < n; ++k) s += v[k] * v[k];
+    return sqrt(s);
+}
+
+/* classical Gram-Schmidt on the columns cols[0..m-1] (length n); R upper
+ * triangle; *cond = max / min of the |R_jj| above 1e-30 */
+static void pcf_qr(double cols[][CL_MAX_COMP], int m, int n, double Q[][CL_MAX_COMP],
+                   double R[][PCF_MAX_DEPTH], double* cond) {
+    double rmax = 0.0, rmin = DBL_MAX;
+    for (int j = 0; j < m; ++j) {
+        for (int k = 0; k < n; ++k) Q[j][k] = cols[j][k];
+        for (int i = 0; i < j; ++i) {
+            double d = 0.0;
+            for (int k = 0; k < n; ++k) d += Q[i][k] * cols[j][k];
+            R[i][j] = d;
+            for (int k = 0; k < n; ++k) Q[j][k] -= R[i][j] * Q[i][k];
+        }
+        R[j][j] = pcf_norm(Q[j], n);
+        if (R[j][j] > 1e-15)
+            for (int k = 0; k < n; ++k) Q[j][k] /= R[j][j];
+        const double a = fabs(R[j][j]);
+        if (a > rmax) rmax = a;
+        if (a > 1e-30 && a < rmin) rmin = a;
+    }
+    *cond = m == 0 ? 1.0 : (rmin > 1e-30 ? rmax / rmin : DBL_MAX);
+}
+
+/* one solve; species_in as given to calculate_species_concentrations.  Returns
+ * 1 if ||f||_2 < tol was reached; *iters = getLastIterations() */
+int orc_pcf_solve(const cl_eq_system* sys, const double* species_in, double* species_out, int* iters) {
+    const int nc = sys->n_comp, ns = sys->n_species;
+    const int depth = sys->anderson_depth > 0 ? (sys->anderson_depth < PCF_MAX_DEPTH - 1 ? sys->anderson_depth
+                                                                                         : PCF_MAX_DEPTH - 2) : 4;
+    double T[CL_MAX_COMP], x[CL_MAX_COMP], xn[CL_MAX_COMP], f[CL_MAX_COMP];
+    *iters = 0;
+    if (nc == 0 || ns == 0) {
+        for (int i = 0; i < ns; ++i) species_out[i] = species_in[i];
+        return 1;
+    }
+    orc_eq_totals(sys, species_in, T);
+    orc_eq_cold_start(sys, species_in, x);
+    /* history of iterates and corrections, oldest first; depth + 2 entries at most */
+    double hx[PCF_MAX_DEPTH][CL_MAX_COMP], hf[PCF_MAX_DEPTH][CL_MAX_COMP];
+    int hn = 0;
+    pcf_correction(sys, T, x, species_in, f);
+    for (int j = 0; j < nc; ++j) xn[j] = smax(smin(x[j] + f[j], MAX_LOG_C), MIN_LOG_C);
+    for (int j = 0; j < nc; ++j) { hx[0][j] = x[j]; hf[0][j] = f[j]; x[j] = xn[j]; }
+    hn = 1;
+    int conv = 0;
+    for (int it = 1; it < sys->max_iter; ++it) {
+        *iters = it;
+        pcf_correction(sys, T, x, species_in, f);
+        if (pcf_norm(f, nc) < sys->tol) { conv = 1; break; }
+        for (int j = 0; j < nc; ++j) { hx[hn][j] = x[j]; hf[hn][j] = f[j]; }
+        ++hn;
+        int m = hn - 1 < depth ? hn - 1 : depth;
+        if (m < 1) {
+            for (int j = 0; j < nc; ++j) xn[j] = x[j] + f[j];
+        } else {
+            double dF[PCF_MAX_DEPTH][CL_MAX_COMP], dX[PCF_MAX_DEPTH][CL_MAX_COMP];
+            double Q[PCF_MAX_DEPTH][CL_MAX_COMP], R[PCF_MAX_DEPTH][PCF_MAX_DEPTH], cond;
+            for (int i = 0; i < m; ++i) {
+                const int a = hn - m - 1 + i;
+                for (int j = 0; j < nc; ++j) { dF[i][j] = hf[a + 1][j] - hf[a][j]; dX[i][j] = hx[a + 1][j] - hx[a][j]; }
+            }
+            int first = 0;      /* columns dropped from the front */
+            pcf_qr(dF, m, nc, Q, R, &cond);
+            while (cond > PCF_COND_TOL && m - first > 1) {
+                ++first;
+                pcf_qr(dF + first, m - first, nc, Q, R, &cond);
+            }
+            const int mm = m - first;
+            double g[PCF_MAX_DEPTH], qf[PCF_MAX_DEPTH];
+            for (int i = 0; i < mm; ++i) {
+                double d = 0.0;
+                for (int k = 0; k < nc; ++k) d += Q[i][k] * f[k];
+                qf[i] = d;
+            }
+            for (int i = mm - 1; i >= 0; --i) {
+                double v = qf[i];
+                for (int k = i + 1; k < mm; ++k) v -= R[i][k] * g[k];
+                if (fabs(R[i][i]) > 1e-30) v /= R[i][i];
+                g[i] = v;
+            }
+            double sx[CL_MAX_COMP] = {0}, sf[CL_MAX_COMP] = {0};
+            for (int i = 0; i < mm; ++i)
+                for (int j = 0; j < nc; ++j) {
+                    sx[j] += dX[first + i][j] * g[i];
+                    sf[j] += dF[first + i][j] * g[i];
+                }
+            for (int j = 0; j < nc; ++j) xn[j] = x[j] - sx[j] + 1.0 * (f[j] - sf[j]);
+        }
+        for (int j = 0; j < nc; ++j) {
+            double v = smax(smin(xn[j], MAX_LOG_C), MIN_LOG_C);
+            if (isnan(v) || isinf(v)) v = x[j];
+            x[j] = v;
+        }
+        /* keep the depth + 1 newest entries */
+        while (hn > depth + 1) {
+            for (int a = 1; a < hn; ++a)
+                for (int j = 0; j < nc; ++j) { hx[a - 1][j] = hx[a][j]; hf[a - 1][j] = hf[a][j]; }
+            --hn;
+        }
+    }
+    pcf_species(sys, x, species_in, species_out);
+    for (int i = 0; i < ns; ++i) {
+        double v = species_out[i];
+        if (isnan(v) || isinf(v)) v = species_in[i] > MIN_CONC ? smin(species_in[i], MAX_CONC) : MIN_CONC;
+        species_out[i] = smax(smin(v, MAX_CONC), MIN_CONC);
+    }
+    return conv;
+}
+
+void orc_pcf_batch(const cl_eq_system* sys, const double* species_in, double* species_out, int32_t* iters,
+                   uint8_t* conv, int64_t n) {
+    const int ns = sys->n_species;
+    #pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t k = 0; k < n; ++k) {
+        int it = 0;
+        const int cv = orc_pcf_solve(sys, species_in + k*ns, species_out + k*ns, &it);
+        if (iters) iters[k] = it;
+        if (conv) conv[k] = (uint8_t)cv;
+    }
+}
+
 void orc_eq_batch(const cl_eq_system* sys, const double* totals, const double* cold_species,
                   double* x_io, int32_t* iters, uint8_t* status, int64_t n, int start) {
     const int nc = sys->n_comp, ns = sys->n_species;
@@ -746,14 +943,28 @@ static void vox_dissolve(const rx_ctx* r, int x, int y, int z, double* dab) {
     }
 }
 
-/* run_equilibrium_biotic (part4_eqsolver.hh:1355-1494), Newton solve;
- * returns 1 if it did not converge */
+/* run_equilibrium_biotic (part4_eqsolver.hh:1355-1494) with the Newton solve
+ * or the reference's PCF + Anderson; returns 1 if it did not converge */
 static int vox_equilibrium(const rx_ctx* r, int64_t n) {
     const cl_config* cfg = r->cfg;
     const int S = cfg->n_solutes;
     const cl_eq_system* sys = &cfg->eq;
     double conc[CL_MAX_SPECIES], T[CL_MAX_COMP], xx[CL_MAX_COMP], eqc[CL_MAX_SPECIES];
     for (int s = 0; s < S; ++s) { double c = vox_dens(r, s, n); conc[s] = c > MIN_CONC ? c : MIN_CONC; }
+    if (sys->solver == CL_EQ_SOLVER_PCF) {
+        /* the reference's live solver: its result is applied whether or not it converged */
+        int it = 0;
+        const int cv = orc_pcf_solve(sys, conc, eqc, &it);
+        if (r->st->eq_iters) r->st->eq_iters[n] = it;
+        for (int s = 0; s < S && s < sys->n_species; ++s) {
+            double d = eqc[s] - conc[s];
+            double mx = 0.1 * fabs(conc[s]); if (mx < 1e-9) mx = 1e-9;
+            if (fabs(d) > mx) d = d > 0 ? mx : -mx;
+            if (conc[s] + d < 1e-20) d = 1e-20 - conc[s];
+            if (fabs(d) > THRD) vox_apply(r, s, n, d);
+        }
+        return cv ? 0 : 1;
+    }
     orc_eq_totals(sys, conc, T);
     orc_eq_cold_start(sys, conc, xx);
     int conv = 0;

@@ -115,6 +115,10 @@ void orc_eq_species(const cl_eq_system* sys, const double* x, double* c);
 /* batch: start = CL_EQ_START_COLD uses cold_species, else x_io is the start */
 void orc_eq_batch(const cl_eq_system* sys, const double* totals, const double* cold_species,
                   double* x_io, int32_t* iters, uint8_t* status, int64_t n, int start);
+/* the reference's live solver (PCF + Anderson), calculate_species_concentrations */
+int  orc_pcf_solve(const cl_eq_system* sys, const double* species_in, double* species_out, int* iters);
+void orc_pcf_batch(const cl_eq_system* sys, const double* species_in, double* species_out, int32_t* iters,
+                   uint8_t* conv, int64_t n);
 
 /* ---- MLP n_in -> H -> H -> n_out, GELU, FP64 (gradient oracle) ------------ */
 /* params packed: W1[H][n_in] b1[H] W2[H][H] b2[H] W3[n_out][H] b3[n_out];

@@ -55,6 +55,8 @@ def lib():
         _orc.orc_eq_residual.argtypes = [vp, vp, vp]
         _orc.orc_eq_batch.restype = None
         _orc.orc_eq_batch.argtypes = [vp, vp, vp, vp, vp, vp, ctypes.c_int64, i]
+        _orc.orc_pcf_batch.restype = None
+        _orc.orc_pcf_batch.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int64]
         _orc.orc_mlp_forward_backward.restype = d
         _orc.orc_mlp_forward_backward.argtypes = [i, i, i, vp, vp, vp, i, vp, vp]
         _orc.orc_surrogate_forward.restype = None
@@ -239,6 +241,18 @@ def eq_batch(sys, totals, cold_species, x0=None, start=0):
                        _p(np.ascontiguousarray(cold_species, np.float64)), _p(x), _p(it), _p(stt),
                        ctypes.c_int64(n), start)
     return x, it, stt
+
+
+def pcf_batch(sys, species):
+    """The reference's live solve (PCF + Anderson) of each row of species:
+    (species out, iterations, converged)."""
+    c = np.ascontiguousarray(species, np.float64).reshape(-1, sys.n_species)
+    n = c.shape[0]
+    out = np.zeros_like(c)
+    it = np.zeros(n, np.int32)
+    cv = np.zeros(n, np.uint8)
+    lib().orc_pcf_batch(ctypes.byref(sys), _p(c), _p(out), _p(it), _p(cv), ctypes.c_int64(n))
+    return out, it, cv
 
 
 def eq_residual(sys, totals, x):

@@ -201,3 +201,34 @@ def test_print_config_cellular_automaton(tmp_path):
     xml = write_ca_case(str(tmp_path), mask, method="quarter")
     r = subprocess.run([DRIVER, xml, "--print-config"], capture_output=True, text=True)
     assert r.returncode == 1 and "CA_method" in r.stderr
+
+
+EQ_BLOCK = """    <equilibrium>
+        <enabled>true</enabled>
+        <components>A</components>
+        <stoichiometry><species0>1</species0><species1>0</species1></stoichiometry>
+        <logK><species0>0</species0><species1>0</species1></logK>
+        {solver}
+    </equilibrium>
+</parameters>
+"""
+
+
+@pytest.mark.skipif(not driver_available(), reason="host driver not built")
+@pytest.mark.parametrize("xml_solver,flag,want", [("", None, "newton"), ("<solver>pcf</solver>", None, "pcf"),
+                                                  ("<solver>PCF</solver>", "newton", "newton"),
+                                                  ("", "pcf", "pcf")])
+def test_equilibrium_solver_choice(tmp_path, xml_solver, flag, want):
+    """<equilibrium><solver> (extension) and --eq-solver pick the transport
+    step's speciation: Newton by default, the reference's PCF + Anderson on
+    request; the command line wins."""
+    xml = write_case(str(tmp_path))
+    text = open(xml).read().replace("</parameters>\n", EQ_BLOCK.format(solver=xml_solver))
+    open(xml, "w").write(text)
+    cmd = [DRIVER, xml, "--print-config"] + (["--eq-solver", flag] if flag else [])
+    c = json.loads(subprocess.run(cmd, capture_output=True, text=True, check=True).stdout)
+    assert c["use_equilibrium"] == 1 and c["eq_solver"] == want
+    open(xml, "w").write(text.replace(xml_solver, "<solver>anderson</solver>") if xml_solver else text)
+    if xml_solver:
+        r = subprocess.run([DRIVER, xml, "--print-config"], capture_output=True, text=True)
+        assert r.returncode == 1 and "solver" in r.stderr
