@@ -368,7 +368,9 @@ int flow_step(Ctx* c, int use_tracer) {
     k.list = c->d_flive;
     k.count = c->n_flive;
     if (!use_tracer) k.tracer = nullptr;
-    const int blocks = c->energy_blocks;
+    // one wave: three 256-thread blocks (80 registers) per SM, each walking
+    // the list grid-stride, so no block waits in a tail
+    const int blocks = c->energy_blocks < 148 * 3 ? c->energy_blocks : 148 * 3;
     int r = timing_begin(c, CL_KERNEL_FLOW_STEP);
     if (r) return r;
     if (c->flow_parity == 0) flow_aa_kernel<0><<<blocks, 256, 0, c->stream>>>(k);
