@@ -517,10 +517,8 @@ ade_react_kernel(const __grid_constant__ AdeK k, const uint32_t* __restrict__ li
         const uint32_t n = list[r];
         const uint8_t cls = k.cls[n];
         if (!(cls & F_REACTIVE)) continue;            // streams, does not react (a coupled NoDynamics site)
-        const uint32_t q = n / (uint32_t)k.g.nz;
-        const int z = (int)(n - q * (uint32_t)k.g.nz);
-        const int x = (int)(q / (uint32_t)k.g.ny);
-        const int y = (int)(q - (uint32_t)x * (uint32_t)k.g.ny);
+        int x, y, z;
+        decode(k.g, n, x, y, z);
         SSite st;
         if (!make_ssite<PARITY>(k.g, k.sidx, x, y, z, n, st)) atomicAdd(&k.counters[1], 1ull);
         for (int s = 0; s < p.S; ++s) cApp[s * kReactBlock] = 0.0;
@@ -567,10 +565,8 @@ __global__ void __launch_bounds__(256, 2) ade_stream_kernel(const __grid_constan
         const uint32_t n = list[r];
         const uint8_t cls = k.cls[n];
         const uint8_t dyn = cls & 3;
-        const uint32_t q = n / (uint32_t)k.g.nz;
-        const int z = (int)(n - q * (uint32_t)k.g.nz);
-        const int x = (int)(q / (uint32_t)k.g.ny);
-        const int y = (int)(q - (uint32_t)x * (uint32_t)k.g.ny);
+        int x, y, z;
+        decode(k.g, n, x, y, z);
         const bool rc = any_rxn && (cls & F_REACTIVE);
         SSite st;
         if (!make_ssite<PARITY>(k.g, k.sidx, x, y, z, n, st)) atomicAdd(&k.counters[1], 1ull);

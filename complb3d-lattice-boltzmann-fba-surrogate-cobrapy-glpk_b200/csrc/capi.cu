@@ -155,6 +155,8 @@ cl_ctx* cl_create(const cl_config* cfg, void* stream, int* status) {
     c->geo.nx = cfg->nx; c->geo.ny = cfg->ny; c->geo.nz = cfg->nz;
     c->geo.plane = (int64_t)cfg->ny * cfg->nz;
     c->geo.N = c->geo.plane * cfg->nx;
+    c->geo.by_nz.init((uint32_t)cfg->nz);
+    c->geo.by_ny.init((uint32_t)cfg->ny);
     const int64_t N = c->geo.N;
     auto fail = [&](int s) { if (status) *status = s; cl_destroy(h); return (cl_ctx*)nullptr; };
     if (stream) { c->stream = (cudaStream_t)stream; c->own_stream = false; }

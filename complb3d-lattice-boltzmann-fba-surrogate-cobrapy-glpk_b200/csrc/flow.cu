@@ -180,10 +180,8 @@ __global__ void __launch_bounds__(256, 3) flow_aa_kernel(FlowK k) {
     for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < k.count;
          r += (int64_t)gridDim.x * blockDim.x) {
         const uint32_t n = k.list[r];
-        const uint32_t q = n / (uint32_t)k.g.nz;
-        const int z = (int)(n - q * (uint32_t)k.g.nz);
-        const int x = (int)(q / (uint32_t)k.g.ny);
-        const int y = (int)(q - (uint32_t)x * (uint32_t)k.g.ny);
+        int x, y, z;
+        decode(k.g, n, x, y, z);
         esum += flow_site<PARITY>(k, make_site(k.g, x, y, z, n), x, k.cls[n]);
     }
     // deterministic block reduction of the energy

@@ -48,16 +48,44 @@ enum : uint8_t { NODYN = 0, BB = 1, FLUID = 2, BIO = 3 };
 // x = 1..nx-2 carries a dissolvable phase), phase-self (carries one itself)
 enum : uint8_t { F_REACTIVE = 4, F_SURFACE = 8, F_PHASE_NBR = 16, F_PHASE_SELF = 32 };
 
+// Unsigned 32-bit division by a divisor fixed at set-up (Granlund and
+// Montgomery, "Division by invariant integers using multiplication", 1994,
+// the round-down variant with the extra add): q = (t + ((n - t) >> s1)) >> s2,
+// t = umulhi(m, n), exact for every 32-bit n.  Site decoding uses it instead
+// of a hardware-less 32/64-bit division on every site of every launch.
+struct FastDiv {
+    uint32_t d, m, s1, s2;
+    __host__ void init(uint32_t div) {
+        d = div;
+        uint32_t l = 0;
+        while (l < 32 && (1ull << l) < (unsigned long long)div) ++l;     // ceil(log2 d)
+        m = (uint32_t)((((1ull << 32) * ((1ull << l) - div)) / div) + 1);
+        s1 = l > 0 ? 1u : 0u;
+        s2 = l > 0 ? l - 1 : 0u;
+    }
+    __host__ __device__ __forceinline__ uint32_t div(uint32_t n) const {
+#ifdef __CUDA_ARCH__
+        const uint32_t t = __umulhi(m, n);
+#else
+        const uint32_t t = (uint32_t)(((unsigned long long)m * n) >> 32);
+#endif
+        return (t + ((n - t) >> s1)) >> s2;
+    }
+};
+
 struct Geo {
     int nx, ny, nz;
     int64_t N, plane;   // N = nx*ny*nz, plane = ny*nz
+    FastDiv by_nz, by_ny;
 };
 
+// site index -> (x, y, z); the context keeps N below 2^32
 __device__ __forceinline__ void decode(const Geo& g, int64_t n, int& x, int& y, int& z) {
-    int64_t q = n / g.nz;
-    z = (int)(n - q * g.nz);
-    x = (int)(q / g.ny);
-    y = (int)(q - (int64_t)x * g.ny);
+    const uint32_t n32 = (uint32_t)n;
+    const uint32_t q = g.by_nz.div(n32);
+    z = (int)(n32 - q * (uint32_t)g.nz);
+    x = (int)g.by_ny.div(q);
+    y = (int)(q - (uint32_t)x * (uint32_t)g.ny);
 }
 
 // Site index of (x+dx, y+dy, z+dz) with y,z periodic; returns -1 when x+dx
