@@ -57,8 +57,8 @@ struct AdeK {
     double* bio;              // M*N
     float* rho_adj;           // n_mob * 2 * plane
     int32_t* eq_iters;        // N (may be null)
-    double* eq_x;             // NC*N previous solutions (null: cold start only)
-    double* eq_xp;            // NC*N the solutions before those
+    double* eq_x;             // NC*N previous solutions, by storage index (null: cold start only)
+    double* eq_xp;            // NC*N the solutions before those, by storage index
     const uint8_t* mask;      // N material numbers
     const uint8_t* phase;     // N phase ids (null without dissolution)
     double* rel;              // S*N releases of the phase voxels (null without dissolution)
@@ -352,7 +352,8 @@ __device__ __forceinline__ int pcf_voxel(const EqDev& e, int S, int max_iter, do
 // as each processor applies its increments), App the total increment per
 // solute.  Returns 1 if the equilibrium solve did not converge.
 template <int NC, int SOLVER>
-__device__ int reaction_chain(const AdeK& k, int64_t n, int x, int y, int z, uint8_t cls, double* Cur, double* App,
+__device__ int reaction_chain(const AdeK& k, int64_t n, uint32_t sto, int x, int y, int z, uint8_t cls, double* Cur,
+                              double* App,
                               int cs, double* R, double* B, double* BR, int bd) {
     const AdeParams& p = k.p;
     const int64_t N = k.g.N;
@@ -429,9 +430,9 @@ __device__ int reaction_chain(const AdeK& k, int64_t n, int x, int y, int z, uin
             bool two = true;
 #pragma unroll
             for (int j = 0; j < NC; ++j) {
-                xprev[j] = k.eq_x[(int64_t)j * N + n];
+                xprev[j] = k.eq_x[(int64_t)j * N + sto];
                 warm = warm && (xprev[j] == xprev[j]);
-                const double xq = k.eq_xp[(int64_t)j * N + n];
+                const double xq = k.eq_xp[(int64_t)j * N + sto];
                 two = two && (xq == xq);
                 x[j] = xprev[j];
                 if (two) x[j] = fmin(fmax(2.0 * xprev[j] - xq, -30.0), 1.0);
@@ -451,7 +452,7 @@ __device__ int reaction_chain(const AdeK& k, int64_t n, int x, int y, int z, uin
         }
         if (k.eq_x && conv) {
 #pragma unroll
-            for (int j = 0; j < NC; ++j) { k.eq_xp[(int64_t)j * N + n] = xprev[j]; k.eq_x[(int64_t)j * N + n] = x[j]; }
+            for (int j = 0; j < NC; ++j) { k.eq_xp[(int64_t)j * N + sto] = xprev[j]; k.eq_x[(int64_t)j * N + sto] = x[j]; }
         }
         if (k.eq_iters) k.eq_iters[n] = it;
         if (!conv) nonconv = 1;
@@ -539,12 +540,12 @@ ade_react_kernel(const __grid_constant__ AdeK k, const uint32_t* __restrict__ li
         }
         for (int s = 0; s < p.S; ++s)
             if (p.mob_slot[s] < 0) cCur[s * kReactBlock] = k.imm[(int64_t)s * N + n];
-        nonconv += reaction_chain<NC, SOLVER>(k, n, x, y, z, cls, cCur, cApp, kReactBlock, Rw + t, Bw + t, BRw + t,
+        nonconv += reaction_chain<NC, SOLVER>(k, n, st.s, x, y, z, cls, cCur, cApp, kReactBlock, Rw + t, Bw + t, BRw + t,
                                       kReactBlock);
         for (int s = 0; s < p.S; ++s)
             if (p.mob_slot[s] < 0 && cApp[s * kReactBlock] != 0.0) k.imm[(int64_t)s * N + n] += cApp[s * kReactBlock];
 #pragma unroll
-        for (int m = 0; m < NMOB; ++m) dc[(int64_t)m * N + n] = (float)cApp[p.mob_index[m] * kReactBlock];
+        for (int m = 0; m < NMOB; ++m) dc[(int64_t)m * N + st.s] = (float)cApp[p.mob_index[m] * kReactBlock];
     }
     for (int o = 16; o > 0; o >>= 1) nonconv += __shfl_down_sync(0xffffffffu, nonconv, o);
     if ((t & 31) == 0 && nonconv) atomicAdd(&k.counters[0], nonconv);
@@ -594,7 +595,7 @@ __global__ void __launch_bounds__(256, 2) ade_stream_kernel(const __grid_constan
 #pragma unroll
                     for (int i = 0; i < 7; ++i) rho += f[g][i];
                 }
-                const float d = rc ? dc[(int64_t)m * N + n] : 0.f;
+                const float d = rc ? dc[(int64_t)m * N + st.s] : 0.f;
                 if (d != 0.f) {
 #pragma unroll
                     for (int i = 0; i < 7; ++i) f[g][i] += t7(i) * d;
