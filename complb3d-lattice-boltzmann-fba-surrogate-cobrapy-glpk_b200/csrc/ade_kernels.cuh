@@ -447,7 +447,8 @@ __device__ int reaction_chain(const AdeK& k, int64_t n, uint32_t sto, int x, int
         // cold start; one call site keeps one copy of the solver in the kernel
         for (int phase = warm ? 0 : 1; phase < 2; ++phase) {
             if (phase == 1) cold(x);
-            it += eq_newton<NC>(e, T, x, phase == 0 ? p.eq.warm_iter : p.eq.max_iter, p.eq.tol, &conv);
+            it += eq_newton<NC>(e, T, x, phase == 0 ? p.eq.warm_iter : p.eq.max_iter, p.eq.tol, &conv, nullptr, R,
+                                bd);
             if (conv) break;
         }
         if (k.eq_x && conv) {
@@ -459,7 +460,9 @@ __device__ int reaction_chain(const AdeK& k, int64_t n, uint32_t sto, int x, int
         else {
             for (int s = 0; s < p.S && s < e.ns; ++s) {
                 const double conc = fmax(Cur[s * cs], 1e-30);
-                double eqc = e.active[s] ? species_c<NC>(e, s, x) : fmin(conc, 10.0);
+                // the species of the converged point: kept by the last evaluation
+                // (the R column is free during the solve), else recomputed
+                double eqc = !e.active[s] ? fmin(conc, 10.0) : (NC <= 3 ? R[s * bd] : species_c<NC>(e, s, x));
                 eqc = fmin(fmax(eqc, 1e-30), 10.0);
                 double d = eqc - conc;
                 const double mx = fmax(1e-9, 0.1 * fabs(conc));

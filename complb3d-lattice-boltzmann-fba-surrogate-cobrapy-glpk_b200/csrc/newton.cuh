@@ -166,9 +166,12 @@ __device__ __forceinline__ void eq_cold_start(const EqDev& e, const double* spec
 // taken; *conv = 1 when the residual test passed.
 // F = S^T c - T, sc = |S|^T c and the lower triangle of S^T diag(c) S
 // (clamped species excluded) in one pass over the species
+// (cbuf: where given, each equilibrium species' concentration is stored at
+// cbuf[i * cstride], so a caller finds the species of the returned point)
 template <int NC>
 __device__ __forceinline__ void eq_eval_full(const EqDev& e, const double* T, const double* x,
-                                             double* F, double* sc, double (*J)[NC]) {
+                                             double* F, double* sc, double (*J)[NC], double* cbuf = nullptr,
+                                             int cstride = 0) {
 #pragma unroll
     for (int a = 0; a < NC; ++a) {
         F[a] = -T[a]; sc[a] = 0.0;
@@ -181,6 +184,7 @@ __device__ __forceinline__ void eq_eval_full(const EqDev& e, const double* T, co
         if (!e.active[i]) continue;
         bool clamped;
         const double c = species_eval<NC>(e, i, x, pw, clamped);
+        if (cbuf) cbuf[i * cstride] = c;
         const double cj = clamped ? 0.0 : c;
 #pragma unroll
         for (int a = 0; a < NC; ++a) {
@@ -202,11 +206,11 @@ __device__ __forceinline__ void eq_eval_full(const EqDev& e, const double* T, co
 // number of steps taken; *conv = 1 at the relative residual tolerance.
 template <int NC>
 __device__ int eq_newton_reuse(const EqDev& e, const double* T, double* x, int max_iter, double tol, int* conv,
-                               int* stopped) {
+                               int* stopped, double* cbuf = nullptr, int cstride = 0) {
     const double ln10 = 2.302585092994046;
     *conv = 0;
     double F[NC], sc[NC], J[NC][NC];
-    eq_eval_full<NC>(e, T, x, F, sc, J);
+    eq_eval_full<NC>(e, T, x, F, sc, J, cbuf, cstride);
     for (int it = 0; it < max_iter; ++it) {
         double rel = 0.0, fn = 0.0, w[NC];
 #pragma unroll
@@ -267,7 +271,7 @@ __device__ int eq_newton_reuse(const EqDev& e, const double* T, double* x, int m
         double xt[NC], Ft[NC], sct[NC];
 #pragma unroll
         for (int a = 0; a < NC; ++a) xt[a] = fmin(fmax(d[a] + x[a], -30.0), 1.0);
-        eq_eval_full<NC>(e, T, xt, Ft, sct, J);      // J is free once L is formed
+        eq_eval_full<NC>(e, T, xt, Ft, sct, J, cbuf, cstride);   // J is free once L is formed
         double fnt = 0.0;
 #pragma unroll
         for (int a = 0; a < NC; ++a) { const double r = Ft[a] * w[a]; fnt = fma(r, r, fnt); }
@@ -293,7 +297,7 @@ __device__ int eq_newton_reuse(const EqDev& e, const double* T, double* x, int m
         }
 #pragma unroll
         for (int a = 0; a < NC; ++a) x[a] = xt[a];
-        eq_eval_full<NC>(e, T, x, F, sc, J);
+        eq_eval_full<NC>(e, T, x, F, sc, J, cbuf, cstride);
         if (!accepted) {
             // every trial failed: the next iterate is this point to ~1e-12 of
             // a step and fails the same way, so the solve stops here
@@ -579,9 +583,12 @@ __device__ int eq_newton_warp(const EqDev& e, const double* T, double* x, int ma
 // converging (NaN, singular Jacobian, or every backtracking trial failed):
 // continuing from x would repeat the same failure.
 template <int NC>
+// cbuf (up to three components): on return it holds the species of x, the
+// point the last full evaluation was made at (every return follows one)
 __device__ __forceinline__ int eq_newton(const EqDev& e, const double* T, double* x, int max_iter, double tol,
-                                         int* conv, int* stopped = nullptr) {
-    if constexpr (NC <= 3) return eq_newton_reuse<NC>(e, T, x, max_iter, tol, conv, stopped);
+                                         int* conv, int* stopped = nullptr, double* cbuf = nullptr,
+                                         int cstride = 0) {
+    if constexpr (NC <= 3) return eq_newton_reuse<NC>(e, T, x, max_iter, tol, conv, stopped, cbuf, cstride);
     else return eq_newton_plain<NC>(e, T, x, max_iter, tol, conv, stopped);
 }
 
