@@ -11,7 +11,7 @@
 // MMA with FP32 accumulation over 64-sample tiles staged in shared memory;
 // master weights are FP32, the MMA operands BF16.  Training is plain Adam on
 // the MSE of v, driven on the device by the library's own kernels on the pairs
-// (T, x) that Newton produced.  Newton stays the judge: the network only picks
+// (T, x) that Newton produced.  Newton stays the arbiter: the network only picks
 // the starting point.
 #include "internal.h"
 #include "newton.cuh"
