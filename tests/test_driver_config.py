@@ -232,3 +232,50 @@ def test_equilibrium_solver_choice(tmp_path, xml_solver, flag, want):
     if xml_solver:
         r = subprocess.run([DRIVER, xml, "--print-config"], capture_output=True, text=True)
         assert r.returncode == 1 and "solver" in r.stderr
+
+
+REF_EXAMPLES = os.environ.get("COMPLAB_REFERENCE_EXAMPLES", "/root/reference/examples")
+SUPPORTED = ["01_flow_only", "02_diffusion_only", "03_abiotic_kinetics", "04_equilibrium",
+             "05_biotic_cellular_automaton", "13_precipitation", "14_dissolution", "15_precip_and_dissolution"]
+MOBILE_BIOMASS = ["06_biotic_finite_difference", "07_biotic_lattice_boltzmann", "08_two_microbes"]
+
+
+def _example_xml(name):
+    d = os.path.join(REF_EXAMPLES, name)
+    if not os.path.isdir(d):
+        pytest.skip("reference examples absent")
+    xs = sorted(f for f in os.listdir(d) if f.endswith(".xml"))
+    assert xs, name
+    return d, xs[0]
+
+
+@pytest.mark.skipif(not driver_available(), reason="host driver not built")
+@pytest.mark.parametrize("name", SUPPORTED)
+def test_reference_example_configs_parse(name):
+    """The reference's own example inputs (CPU, when the reference tree is
+    present): the driver reads each CompLaB.xml of the examples whose
+    reaction types this library implements, in the reference's schema."""
+    d, xml = _example_xml(name)
+    r = subprocess.run([DRIVER, xml, "--print-config"], cwd=d, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    c = json.loads(r.stdout)
+    assert c["nx"] >= 3 and c["ny"] >= 1 and c["nz"] >= 1
+    assert len(c["names"]) >= 1
+    if name == "04_equilibrium":
+        assert c["use_equilibrium"] == 1 and c["n_comp"] >= 1
+    if name in ("13_precipitation", "15_precip_and_dissolution"):
+        assert c["precip_enabled"] == 1
+    if name in ("14_dissolution", "15_precip_and_dissolution"):
+        assert c["dissol_enabled"] == 1 and c["n_phases"] >= 1
+    if name == "05_biotic_cellular_automaton":
+        assert c["ca_enabled"] == 1
+
+
+@pytest.mark.skipif(not driver_available(), reason="host driver not built")
+@pytest.mark.parametrize("name", MOBILE_BIOMASS)
+def test_reference_examples_with_mobile_biomass_are_refused(name):
+    """Mobile biomass (finite-difference or LBM biomass lattices) is outside
+    this library's hot path: the driver says so and exits 1."""
+    d, xml = _example_xml(name)
+    r = subprocess.run([DRIVER, xml, "--print-config"], cwd=d, capture_output=True, text=True)
+    assert r.returncode == 1 and "mobile biomass" in r.stderr
