@@ -420,6 +420,7 @@ int cl_set_transport(cl_ctx* h, const double* omega_pore, const double* omega_bi
     if (!h || !omega_pore || !omega_bio || !(dt > 0.0)) { set_error("cl_set_transport: bad argument"); return CL_ERR_ARG; }
     Ctx* c = &h->c;
     for (int s = 0; s < c->cfg.n_solutes; ++s) {
+        if (c->ap.mob_slot[s] < 0) continue;     // an immobile solute has no lattice to relax (D = 0 gives 2)
         if (!(omega_pore[s] > 0.0 && omega_pore[s] < 2.0) || !(omega_bio[s] > 0.0 && omega_bio[s] < 2.0)) {
             set_error("cl_set_transport: relaxation frequencies must lie in (0, 2)"); return CL_ERR_ARG;
         }

@@ -276,7 +276,8 @@ int cl_update_dynamics(cl_ctx* ctx);
  * NSdomainSetup's new deltaP (rho_in = 1, rho_out = 1 - 3 deltaP), followed by
  * cl_flow_init; cl_set_transport sets the solute relaxation frequencies and
  * the transport time step derived from the calibrated flow
- * (complab.cpp:708-727). */
+ * (complab.cpp:708-727); the values of immobile solutes are not used (with a
+ * zero diffusion coefficient their frequency is 2). */
 int cl_flow_velocity_stats(cl_ctx* ctx, double* pore_mean_u, double* max_ux, double* outlet_mean_ux);
 int cl_set_flow_pressure(cl_ctx* ctx, double rho_in, double rho_out);
 int cl_set_transport(cl_ctx* ctx, const double* omega_pore, const double* omega_bio, double dt);

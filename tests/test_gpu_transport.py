@@ -241,3 +241,16 @@ def test_surrogate_reaction_type(gpu_lib, pkg, wl):
         assert rel_l2(bg, bo) < 1e-5, m
         assert not np.allclose(bo, (b0, b1)[m].reshape(-1))      # the organisms did something
     lat.close()
+
+
+def test_set_transport_ignores_immobile_relaxation(gpu_lib, pkg, wl):
+    """The driver derives every solute's relaxation from its diffusion
+    coefficient; an immobile solute (D = 0) gets 2, outside (0, 2), and has
+    no lattice to relax: accepted and ignored.  A mobile one at 2 is refused."""
+    mask = wl.sphere_pack(12, 8, 8, 0.6, 1.5, 2.5, seed=3)
+    cfg = pkg.make_config(*mask.shape, solutes=[{"tau": 0.8}, {"immobile": True}])
+    lat = pkg.Lattice(cfg)
+    lat.set_transport([1.25, 2.0], [1.25, 2.0], 0.01)
+    with pytest.raises(pkg.CLError):
+        lat.set_transport([2.0, 2.0], [2.0, 2.0], 0.01)
+    lat.close()
