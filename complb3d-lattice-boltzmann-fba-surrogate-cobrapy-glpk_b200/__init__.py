@@ -33,6 +33,8 @@ MAX_SRG_ORG = 2
 SRG_IN_FIN, SRG_IN_CONC, SRG_IN_BIOMASS = 0, 1, 2
 SRG_OUT_GROWTH, SRG_OUT_FOUT = 0, 1
 KERNEL_ADE_MAIN, KERNEL_FLOW_STEP, KERNEL_ADE_REACT = 0, 1, 2
+OPT_COMPILED_CHEM, OPT_FAST_VARIANT = 1, 2
+CHEM_COUPLED, CHEM_BIOTIC4 = 1, 2
 
 c_int32, c_double, c_int64 = ctypes.c_int32, ctypes.c_double, ctypes.c_int64
 
@@ -125,6 +127,8 @@ def load_library(path=LIB_PATH):
         ("cl_reduce", [vp, c_int32, c_int32, c_int32, c_double, P(c_double)]),
         ("cl_precip_convert", [vp, P(c_int64)]), ("cl_dissol_convert", [vp, P(c_int64)]),
         ("cl_flow_velocity_stats", [vp, P(c_double), P(c_double), P(c_double)]),
+        ("cl_flow_velocity_norm_masked", [vp, c_int32, P(c_double), P(c_int64)]),
+        ("cl_set_option", [vp, c_int32, c_int64]), ("cl_get_option", [vp, c_int32, P(c_int64)]),
         ("cl_set_flow_pressure", [vp, c_double, c_double]), ("cl_set_transport", [vp, vp, vp, c_double]),
         ("cl_device_bytes", [vp, P(ctypes.c_uint64)]), ("cl_abi_sizes", [vp, c_int32]),
         ("cl_timing_enable", [vp, c_int32]), ("cl_timing_read", [vp, c_int32, P(c_double), P(c_int64)]),
@@ -324,6 +328,14 @@ class Lattice:
     def step(self, n=1):
         return self._c(self.lib.cl_step(self.h, n), "cl_step")
 
+    def set_option(self, key, value):
+        self._c(self.lib.cl_set_option(self.h, key, int(value)), "cl_set_option")
+
+    def get_option(self, key):
+        v = c_int64(0)
+        self._c(self.lib.cl_get_option(self.h, key, ctypes.byref(v)), "cl_get_option")
+        return v.value
+
     def field(self, field, index=0):
         out = np.empty(self.N, np.float64)
         self._c(self.lib.cl_get_field(self.h, field, index, _ptr(out)), "cl_get_field")
@@ -364,6 +376,13 @@ class Lattice:
         self._c(self.lib.cl_flow_velocity_stats(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)),
                 "cl_flow_velocity_stats")
         return a.value, b.value, c.value
+
+    def velocity_norm_masked(self, code):
+        """(sum of |u|, site count) over the sites of material `code` in x = 1..nx-2."""
+        a, n = c_double(), c_int64()
+        self._c(self.lib.cl_flow_velocity_norm_masked(self.h, code, ctypes.byref(a), ctypes.byref(n)),
+                "cl_flow_velocity_norm_masked")
+        return a.value, n.value
 
     def set_flow_pressure(self, rho_in, rho_out):
         self._c(self.lib.cl_set_flow_pressure(self.h, rho_in, rho_out), "cl_set_flow_pressure")

@@ -217,6 +217,7 @@ cl_ctx* cl_create(const cl_config* cfg, void* stream, int* status) {
     p.dissol_walls = cfg->dissol_apply_at_walls;
     p.n_phases = cfg->n_phases;
     for (int k = 0; k < cfg->n_phases; ++k) p.phase[k] = cfg->phases[k];
+    c->chem = chem_match(*cfg);
     // device memory
     int r = CL_OK;
     if ((r = dalloc(c, &c->d_mask, N)) || (r = dalloc(c, &c->d_ns_cls, N)) || (r = dalloc(c, &c->d_ade_cls, N)) ||
@@ -409,6 +410,18 @@ int cl_flow_velocity_stats(cl_ctx* h, double* pore_mean_u, double* max_ux, doubl
     return CL_OK;
 }
 
+int cl_flow_velocity_norm_masked(cl_ctx* h, int32_t code, double* sum_norm, int64_t* count) {
+    if (!h || code < 0 || code > 255) { set_error("cl_flow_velocity_norm_masked: bad argument"); return CL_ERR_ARG; }
+    Ctx* c = &h->c;
+    if (!c->flow_ready) { set_error("no flow field"); return CL_ERR_STATE; }
+    double v[2];
+    int r = flow_norm_masked(c, code, v);
+    if (r) return r;
+    if (sum_norm) *sum_norm = v[0];
+    if (count) *count = (int64_t)(v[1] + 0.5);
+    return CL_OK;
+}
+
 int cl_set_flow_pressure(cl_ctx* h, double rho_in, double rho_out) {
     if (!h || !(rho_in > 0.0) || !(rho_out > 0.0)) { set_error("cl_set_flow_pressure: densities must be positive"); return CL_ERR_ARG; }
     h->c.cfg.rho_in = rho_in;
@@ -483,6 +496,28 @@ int cl_set_surrogate(cl_ctx* h, int32_t slot, const cl_surrogate_net* net) {
     d.params = c->d_srg_params[slot];
     c->ap.net[slot] = d;
     return CL_OK;
+}
+
+int cl_set_option(cl_ctx* h, int32_t key, int64_t value) {
+    if (!h) return CL_ERR_ARG;
+    Ctx* c = &h->c;
+    switch (key) {
+        case CL_OPT_COMPILED_CHEM: c->chem_on = value != 0; return CL_OK;
+        case CL_OPT_FAST_VARIANT:
+            if (value < 0 || value > 4) { set_error("cl_set_option: variant 0..4"); return CL_ERR_ARG; }
+            c->fast_variant = (int)value; return CL_OK;
+        default: set_error("cl_set_option: unknown key"); return CL_ERR_ARG;
+    }
+}
+
+int cl_get_option(cl_ctx* h, int32_t key, int64_t* value) {
+    if (!h || !value) return CL_ERR_ARG;
+    Ctx* c = &h->c;
+    switch (key) {
+        case CL_OPT_COMPILED_CHEM: *value = c->chem_on ? c->chem : 0; return CL_OK;
+        case CL_OPT_FAST_VARIANT: *value = c->fast_variant; return CL_OK;
+        default: set_error("cl_get_option: unknown key"); return CL_ERR_ARG;
+    }
 }
 
 int cl_step(cl_ctx* h, int32_t n) {

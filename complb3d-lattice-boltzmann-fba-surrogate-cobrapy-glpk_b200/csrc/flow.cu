@@ -480,6 +480,60 @@ int flow_stats(Ctx* c, double out[3]) {
     return CL_OK;
 }
 
+// sum of the velocity norm and count over the sites of one material in
+// x = 1..nx-2: the masked computeAverage(*computeVelocityNorm(...), geometry,
+// code) and MaskedScalarCounts3D of the reference's Peclet calibration
+// (src/complab.cpp:625-640).  Bounce-back sites count with velocity zero.
+template <int PARITY>
+__global__ void flow_norm_masked_kernel(FlowK k, const uint8_t* mask, int code, double* part) {
+    __shared__ double red[2][256];
+    double su = 0.0, cnt = 0.0;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t lo = k.g.plane, hi = k.g.N - k.g.plane;
+    for (int64_t n = lo + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < hi; n += stride) {
+        if (mask[n] != code) continue;
+        cnt += 1.0;
+        const uint8_t cls = k.cls[n];
+        if (cls != FLUID && cls != BIO) continue;
+        int x, y, z;
+        decode(k.g, n, x, y, z);
+        float f[19];
+        gather19_any<PARITY>(k, make_site(k.g, x, y, z, (uint32_t)n), f);
+        float jx = 0.f, jy = 0.f, jz = 0.f;
+#pragma unroll
+        for (int i = 0; i < 19; ++i) { jx += c19x(i) * f[i]; jy += c19y(i) * f[i]; jz += c19z(i) * f[i]; }
+        su += sqrt((double)jx * jx + (double)jy * jy + (double)jz * jz);
+    }
+    red[0][threadIdx.x] = su; red[1][threadIdx.x] = cnt;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) { red[0][threadIdx.x] += red[0][threadIdx.x + o]; red[1][threadIdx.x] += red[1][threadIdx.x + o]; }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) { part[2 * blockIdx.x] = red[0][0]; part[2 * blockIdx.x + 1] = red[1][0]; }
+}
+
+__global__ void flow_norm_masked_final(const double* part, int nb, double* out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double su = 0.0, cnt = 0.0;
+    for (int b = 0; b < nb; ++b) { su += part[2 * b]; cnt += part[2 * b + 1]; }
+    out[0] = su; out[1] = cnt;
+}
+
+int flow_norm_masked(Ctx* c, int code, double out[2]) {
+    if (!c->d_fsidx) { int r = flow_store_update(c, nullptr); if (r) return r; }
+    FlowK k = make_flowk(c);
+    const int nb = 148 * 4;
+    double* part = c->d_scratch;
+    if (c->flow_parity == 0) flow_norm_masked_kernel<0><<<nb, 256, 0, c->stream>>>(k, c->d_mask, code, part);
+    else flow_norm_masked_kernel<1><<<nb, 256, 0, c->stream>>>(k, c->d_mask, code, part);
+    flow_norm_masked_final<<<1, 32, 0, c->stream>>>(part, nb, part + 2 * nb);
+    CL_LAUNCH_CHECK("flow_norm_masked_kernel");
+    CL_CUDA(cudaMemcpyAsync(out, part + 2 * nb, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CL_CUDA(cudaStreamSynchronize(c->stream));
+    return CL_OK;
+}
+
 // natural-order copy of the populations (to_natural) or upload from natural
 // order (requires parity 0 afterwards).
 template <int PARITY>

@@ -149,6 +149,11 @@ struct Ctx {
     double   ev_ms[kTimedKernels] = {0.0, 0.0, 0.0};
     int64_t  ev_launches[kTimedKernels] = {0, 0, 0};
     int64_t  launches = 0;
+    // compiled chemistry (chem.cuh) whose structure this configuration has,
+    // 0 = none; its one-launch transport step runs while chem_on
+    int      chem = 0;
+    bool     chem_on = true;
+    int      fast_variant = 0;   // launch shape of the one-launch step (block size, blocks per SM)
 };
 
 // event bracket around one launch of a timed kernel (no-op when timing is off)
@@ -160,10 +165,14 @@ int flow_init(Ctx* c);
 int flow_step(Ctx* c, int arm_tracer_flag);
 int flow_arm_tracer(Ctx* c, double eps);
 int flow_macro(Ctx* c, double* d_rho, float* d_u3, int want_bc_velocity);
-int flow_stats(Ctx* c, double out[3]);   // sum |u| and max u_x over x = 1..nx-2, sum u_x at x = nx-2
+int flow_stats(Ctx* c, double out[3]);
+int flow_norm_masked(Ctx* c, int code, double out[2]);   // sum |u| and count of one material, x = 1..nx-2   // sum |u| and max u_x over x = 1..nx-2, sum u_x at x = nx-2
 int classes_from_mask(Ctx* c);
 int ade_init(Ctx* c);
 int ade_step(Ctx* c);
+int ade_step_fast(Ctx* c);      // the transport step of the compiled chemistry c->chem
+int chem_match(const cl_config& cfg);   // id of the compiled chemistry cfg has the structure of, or 0
+const char* chem_name(int id);
 int ade_density(Ctx* c, int s, double* d_out);
 int flow_population_io(Ctx* c, float* d_natural, int to_natural);
 int ade_population_io(Ctx* c, int slot, float* d_natural);

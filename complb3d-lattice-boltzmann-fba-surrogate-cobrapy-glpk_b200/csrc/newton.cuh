@@ -126,14 +126,15 @@ __device__ __forceinline__ double species_eval(const EqDev& e, int i, const doub
 }
 
 // F, and the relative residual
-template <int NC>
+template <int NC, int NS = 0>
 __device__ __forceinline__ double eq_residual(const EqDev& e, const double* T, const double* x, double* F) {
     double sc[NC];
 #pragma unroll
     for (int j = 0; j < NC; ++j) { F[j] = -T[j]; sc[j] = 0.0; }
     Powers<NC> pw;
     pw.set(e, x);
-    for (int i = 0; i < e.ns; ++i) {
+#pragma unroll (NS > 0 ? NS : 1)
+    for (int i = 0; i < (NS > 0 ? NS : e.ns); ++i) {
         if (!e.active[i]) continue;
         bool clamped;
         const double c = species_eval<NC>(e, i, x, pw, clamped);
@@ -168,7 +169,7 @@ __device__ __forceinline__ void eq_cold_start(const EqDev& e, const double* spec
 // (clamped species excluded) in one pass over the species
 // (cbuf: where given, each equilibrium species' concentration is stored at
 // cbuf[i * cstride], so a caller finds the species of the returned point)
-template <int NC>
+template <int NC, int NS = 0>
 __device__ __forceinline__ void eq_eval_full(const EqDev& e, const double* T, const double* x,
                                              double* F, double* sc, double (*J)[NC], double* cbuf = nullptr,
                                              int cstride = 0) {
@@ -180,7 +181,8 @@ __device__ __forceinline__ void eq_eval_full(const EqDev& e, const double* T, co
     }
     Powers<NC> pw;
     pw.set(e, x);
-    for (int i = 0; i < e.ns; ++i) {
+#pragma unroll (NS > 0 ? NS : 1)
+    for (int i = 0; i < (NS > 0 ? NS : e.ns); ++i) {
         if (!e.active[i]) continue;
         bool clamped;
         const double c = species_eval<NC>(e, i, x, pw, clamped);
@@ -204,13 +206,13 @@ __device__ __forceinline__ void eq_eval_full(const EqDev& e, const double* T, co
 // shorter step the point is evaluated again.  The iterates are the same as
 // evaluating residual and Jacobian afresh at every iterate.  Returns the
 // number of steps taken; *conv = 1 at the relative residual tolerance.
-template <int NC>
-__device__ int eq_newton_reuse(const EqDev& e, const double* T, double* x, int max_iter, double tol, int* conv,
+template <int NC, int NS = 0>
+__device__ __forceinline__ int eq_newton_reuse(const EqDev& e, const double* T, double* x, int max_iter, double tol, int* conv,
                                int* stopped, double* cbuf = nullptr, int cstride = 0) {
     const double ln10 = 2.302585092994046;
     *conv = 0;
     double F[NC], sc[NC], J[NC][NC];
-    eq_eval_full<NC>(e, T, x, F, sc, J, cbuf, cstride);
+    eq_eval_full<NC, NS>(e, T, x, F, sc, J, cbuf, cstride);
     for (int it = 0; it < max_iter; ++it) {
         double rel = 0.0, fn = 0.0, w[NC];
 #pragma unroll
@@ -271,7 +273,7 @@ __device__ int eq_newton_reuse(const EqDev& e, const double* T, double* x, int m
         double xt[NC], Ft[NC], sct[NC];
 #pragma unroll
         for (int a = 0; a < NC; ++a) xt[a] = fmin(fmax(d[a] + x[a], -30.0), 1.0);
-        eq_eval_full<NC>(e, T, xt, Ft, sct, J, cbuf, cstride);   // J is free once L is formed
+        eq_eval_full<NC, NS>(e, T, xt, Ft, sct, J, cbuf, cstride);   // J is free once L is formed
         double fnt = 0.0;
 #pragma unroll
         for (int a = 0; a < NC; ++a) { const double r = Ft[a] * w[a]; fnt = fma(r, r, fnt); }
@@ -286,7 +288,7 @@ __device__ int eq_newton_reuse(const EqDev& e, const double* T, double* x, int m
         for (int ls = 1; ls < 40; ++ls) {
 #pragma unroll
             for (int a = 0; a < NC; ++a) xt[a] = fmin(fmax(fma(alpha, d[a], x[a]), -30.0), 1.0);
-            eq_residual<NC>(e, T, xt, Ft);
+            eq_residual<NC, NS>(e, T, xt, Ft);
             fnt = 0.0;
 #pragma unroll
             for (int a = 0; a < NC; ++a) { const double r = Ft[a] * w[a]; fnt = fma(r, r, fnt); }
@@ -297,7 +299,7 @@ __device__ int eq_newton_reuse(const EqDev& e, const double* T, double* x, int m
         }
 #pragma unroll
         for (int a = 0; a < NC; ++a) x[a] = xt[a];
-        eq_eval_full<NC>(e, T, x, F, sc, J, cbuf, cstride);
+        eq_eval_full<NC, NS>(e, T, x, F, sc, J, cbuf, cstride);
         if (!accepted) {
             // every trial failed: the next iterate is this point to ~1e-12 of
             // a step and fails the same way, so the solve stops here
@@ -324,8 +326,8 @@ __device__ int eq_newton_reuse(const EqDev& e, const double* T, double* x, int m
 
 // The same iteration with residual and Jacobian evaluated afresh at every
 // iterate (fewer live registers; used above three components).
-template <int NC>
-__device__ int eq_newton_plain(const EqDev& e, const double* T, double* x, int max_iter, double tol, int* conv,
+template <int NC, int NS = 0>
+__device__ __forceinline__ int eq_newton_plain(const EqDev& e, const double* T, double* x, int max_iter, double tol, int* conv,
                                int* stopped) {
     const double ln10 = 2.302585092994046;
     *conv = 0;
@@ -341,7 +343,8 @@ __device__ int eq_newton_plain(const EqDev& e, const double* T, double* x, int m
         }
         Powers<NC> pw;
         pw.set(e, x);
-        for (int i = 0; i < e.ns; ++i) {
+#pragma unroll (NS > 0 ? NS : 1)
+        for (int i = 0; i < (NS > 0 ? NS : e.ns); ++i) {
             if (!e.active[i]) continue;
             bool clamped;
             const double c = species_eval<NC>(e, i, x, pw, clamped);
@@ -418,7 +421,7 @@ __device__ int eq_newton_plain(const EqDev& e, const double* T, double* x, int m
 #pragma unroll
             for (int a = 0; a < NC; ++a) xt[a] = fmin(fmax(fma(alpha, d[a], x[a]), -30.0), 1.0);
             double Ft[NC];
-            eq_residual<NC>(e, T, xt, Ft);
+            eq_residual<NC, NS>(e, T, xt, Ft);
             double fnt = 0.0;
 #pragma unroll
             for (int a = 0; a < NC; ++a) { const double r = Ft[a] * w[a]; fnt = fma(r, r, fnt); }
@@ -435,7 +438,7 @@ __device__ int eq_newton_plain(const EqDev& e, const double* T, double* x, int m
         stuck = !accepted;
     }
     double Fe[NC];
-    if (eq_residual<NC>(e, T, x, Fe) <= tol) *conv = 1;
+    if (eq_residual<NC, NS>(e, T, x, Fe) <= tol) *conv = 1;
     else if (stuck && stopped) *stopped = 1;
     return max_iter;
 }
@@ -582,14 +585,16 @@ __device__ int eq_newton_warp(const EqDev& e, const double* T, double* x, int ma
 // *stopped (optional) is set when the solve ended before max_iter without
 // converging (NaN, singular Jacobian, or every backtracking trial failed):
 // continuing from x would repeat the same failure.
-template <int NC>
+// NS > 0: the species count is that compile-time constant (every species
+// loop unrolled, so a register array can take the species); 0: e.ns.
+template <int NC, int NS = 0>
 // cbuf (up to three components): on return it holds the species of x, the
 // point the last full evaluation was made at (every return follows one)
 __device__ __forceinline__ int eq_newton(const EqDev& e, const double* T, double* x, int max_iter, double tol,
                                          int* conv, int* stopped = nullptr, double* cbuf = nullptr,
                                          int cstride = 0) {
-    if constexpr (NC <= 3) return eq_newton_reuse<NC>(e, T, x, max_iter, tol, conv, stopped, cbuf, cstride);
-    else return eq_newton_plain<NC>(e, T, x, max_iter, tol, conv, stopped);
+    if constexpr (NC <= 3) return eq_newton_reuse<NC, NS>(e, T, x, max_iter, tol, conv, stopped, cbuf, cstride);
+    else return eq_newton_plain<NC, NS>(e, T, x, max_iter, tol, conv, stopped);
 }
 
 // component totals (calc_component_totals, part4_eqsolver.hh:520-538)

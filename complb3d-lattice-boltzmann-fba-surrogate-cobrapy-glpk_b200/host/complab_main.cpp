@@ -103,6 +103,40 @@ bool flow_solve(cl_ctx* h, long max_it, double eps, int* iters) {
     return check(st, "cl_flow_solve");
 }
 
+// PoreMeanU of the first solve with sessile microbes (complab.cpp:625-640):
+// each pore material adds its masked mean velocity norm times its site count;
+// each biofilm microbe adds the masked mean of its first material times the
+// site count of all its materials; the sum is divided by the total count.  A
+// material with no sites adds nothing (its masked mean would be 0/0).
+bool weighted_pore_mean(cl_ctx* h, const cl_config& c, const HostRun& run, double* out) {
+    double vel = 0.0;
+    int64_t total = 0;
+    auto masked = [&](int code, double* sum, int64_t* cnt) {
+        return check(cl_flow_velocity_norm_masked(h, code, sum, cnt), "cl_flow_velocity_norm_masked");
+    };
+    for (int i = 0; i < c.n_pore_codes; ++i) {
+        double su; int64_t n;
+        if (!masked(c.pore_codes[i], &su, &n)) return false;
+        total += n;
+        vel += su;
+    }
+    for (const auto& mats : run.bio_materials) {
+        if (mats.empty()) continue;
+        int64_t film = 0;
+        double su0 = 0.0; int64_t n0 = 0;
+        for (size_t k = 0; k < mats.size(); ++k) {
+            double su; int64_t n;
+            if (!masked(mats[k], &su, &n)) return false;
+            film += n;
+            if (k == 0) { su0 = su; n0 = n; }
+        }
+        total += film;
+        if (n0 > 0) vel += su0 / (double)n0 * (double)film;
+    }
+    if (total > 0) *out = vel / (double)total;
+    return true;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -155,6 +189,12 @@ int main(int argc, char** argv) {
     if (run.Pe > kThrd) {
         if (!flow_solve(h, run.ns_max1, run.ns_conv1, &ns_iters)) return 1;
         if (!check(cl_flow_velocity_stats(h, &pore_mean_u, &max_ux, &outlet_ux), "cl_flow_velocity_stats")) return 1;
+        // with sessile microbes the first solve's pore mean is the count-weighted
+        // mean over the pore materials and each microbe's biofilm materials, the
+        // biofilm taking the mean of its first material (complab.cpp:625-640)
+        bool sessile = false;
+        for (const auto& mats : run.bio_materials) sessile = sessile || !mats.empty();
+        if (sessile && !weighted_pore_mean(h, c, run, &pore_mean_u)) return 1;
         const double D_fixed = 0.25 * (0.8 - 0.5);          // tau_ADE_fixed = 0.8 (complab.cpp:164)
         const double perm = outlet_ux * nsNu * run.charcs_length / run.delta_P;
         const double u_target = run.Pe * D_fixed / run.charcs_length;
@@ -167,7 +207,18 @@ int main(int argc, char** argv) {
             if (!check(cl_flow_velocity_stats(h, &pore_mean_u, &max_ux, &outlet_ux), "cl_flow_velocity_stats")) return 1;
         }
         pe_achieved = outlet_ux * run.charcs_length / D_fixed;
-        if (max_ux / std::sqrt(0.25) > 1.0) { std::fprintf(stderr, "complab_b200: Ma > 1 after the flow solve\n"); return 1; }
+        // performStabilityChecks (complab.cpp:77-93, 673-686): Ma = u_max / sqrt(1/3)
+        // and CFL = u_max below 1, tau_NS in (0.5, 2); warnings for Ma > 0.3 and
+        // a grid Peclet number u_max / D above 2
+        const double Ma = max_ux / std::sqrt(1.0 / 3.0), Pe_grid = D_fixed > kThrd ? max_ux / D_fixed : 0.0;
+        if (!(Ma < 1.0) || !(max_ux < 1.0) || !(run.tau > 0.5 && run.tau < 2.0)) {
+            std::fprintf(stderr, "complab_b200: stability check failed before the run (Ma %g, CFL %g, tau_NS %g): "
+                                 "lower deltaP or Pe, or adjust tau\n", Ma, max_ux, run.tau);
+            return 1;
+        }
+        if (Ma > 0.3) std::fprintf(stderr, "complab_b200: warning: Ma=%g > 0.3 (flow re-solves may diverge)\n", Ma);
+        if (!(Pe_grid < 2.0))
+            std::fprintf(stderr, "complab_b200: warning: Pe_grid=%g > 2 (advection may overshoot into negatives)\n", Pe_grid);
     }
 
     // solute relaxation and dt from the flow (complab.cpp:708-727)

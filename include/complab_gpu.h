@@ -280,6 +280,12 @@ int cl_update_dynamics(cl_ctx* ctx);
  * zero diffusion coefficient their frequency is 2). */
 int cl_flow_velocity_stats(cl_ctx* ctx, double* pore_mean_u, double* max_ux, double* outlet_mean_ux);
 int cl_set_flow_pressure(cl_ctx* ctx, double rho_in, double rho_out);
+/* The masked pore mean of the same calibration when a sessile microbe exists
+ * (complab.cpp:625-640): the sum of the velocity norm and the number of sites
+ * over the sites of material `code` in x = 1..nx-2 (MaskedScalarCounts3D and
+ * the masked computeAverage(*computeVelocityNorm)); the caller weights the
+ * pore and biofilm materials as the reference does. */
+int cl_flow_velocity_norm_masked(cl_ctx* ctx, int32_t code, double* sum_norm, int64_t* count);
 int cl_set_transport(cl_ctx* ctx, const double* omega_pore, const double* omega_bio, double dt);
 
 /* ---- transport step ----------------------------------------------------------
@@ -293,6 +299,23 @@ int cl_set_transport(cl_ctx* ctx, const double* omega_pore, const double* omega_
  *              on an interval. */
 int cl_ade_init(cl_ctx* ctx);
 int cl_step(cl_ctx* ctx, int32_t n);
+
+/* Compiled chemistries.  The reference compiles its rate laws into the
+ * program (defineKinetics.hh / defineAbioticKinetics.hh, included by
+ * src/complab.cpp); the library likewise compiles chemistries in, each a fixed
+ * structure (solute and microbe counts, which solutes are mobile, the rate
+ * laws' terms, the number of equilibrium components) whose values still come
+ * from cl_config.  cl_create selects the compiled chemistry whose structure
+ * the configuration has; its transport step runs in one launch with every
+ * voxel's state in registers.  Other configurations run the run-time rate
+ * table.  Both give the same fields.
+ *   CL_OPT_COMPILED_CHEM  set: 0 = use the run-time table even when a compiled
+ *                         chemistry matches, 1 = use it (default);
+ *                         get: the id of the compiled chemistry in use, 0 = none. */
+#define CL_OPT_COMPILED_CHEM 1
+#define CL_OPT_FAST_VARIANT  2   /* launch shape of the compiled chemistry's step, 0..4 */
+int cl_set_option(cl_ctx* ctx, int32_t key, int64_t value);
+int cl_get_option(cl_ctx* ctx, int32_t key, int64_t* value);
 
 /* field access (host FP64 buffers of nx*ny*nz values) */
 #define CL_FIELD_CONC      0   /* solute density (index = solute) */

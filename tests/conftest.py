@@ -26,6 +26,22 @@ def load_workloads():
     return importlib.import_module("complab_b200.workloads")
 
 
+def reference_root():
+    """The reference source tree, for the CPU tests that read its example
+    inputs: $COMPLAB_REFERENCE, else the `reference_path` recorded in
+    BASELINE.json at the repository root; None when neither names an existing
+    directory (those tests then skip)."""
+    cand = os.environ.get("COMPLAB_REFERENCE")
+    if not cand:
+        try:
+            import json
+            with open(os.path.join(ROOT, "BASELINE.json")) as f:
+                cand = json.load(f).get("reference_path")
+        except (OSError, ValueError):
+            cand = None
+    return cand if cand and os.path.isdir(cand) else None
+
+
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200) and the built libcomplab_gpu.so")
 

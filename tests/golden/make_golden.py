@@ -1,7 +1,8 @@
 """Generate the committed golden fixtures from the reference's own code.
 
-Run in a container that has the reference tree (default /root/reference) and
-the compiled oracle/_ref/libref.so (``make -C oracle``):
+Run in a container that has the reference tree (given as the argument, or
+$COMPLAB_REFERENCE, or BASELINE.json's reference_path) and the compiled
+oracle/_ref/libref.so (``make -C oracle``):
 
     python tests/golden/make_golden.py [REFERENCE_ROOT]
 
@@ -52,9 +53,11 @@ def parse_shipped_net(ref_root):
 
 
 def main():
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     from oracle import oracle as o
-    from conftest import load_workloads
+    from conftest import load_workloads, reference_root
+    ref_root = sys.argv[1] if len(sys.argv) > 1 else reference_root()
+    if not ref_root:
+        raise SystemExit("no reference tree: pass its path or set COMPLAB_REFERENCE")
     wl = load_workloads()
     if o.ref_lib() is None:
         raise SystemExit("build oracle/_ref first: make -C oracle")

@@ -234,15 +234,19 @@ def test_equilibrium_solver_choice(tmp_path, xml_solver, flag, want):
         assert r.returncode == 1 and "solver" in r.stderr
 
 
-REF_EXAMPLES = os.environ.get("COMPLAB_REFERENCE_EXAMPLES", "/root/reference/examples")
+def _ref_examples():
+    from conftest import reference_root
+    root = reference_root()
+    return os.path.join(root, "examples") if root else None
 SUPPORTED = ["01_flow_only", "02_diffusion_only", "03_abiotic_kinetics", "04_equilibrium",
              "05_biotic_cellular_automaton", "13_precipitation", "14_dissolution", "15_precip_and_dissolution"]
 MOBILE_BIOMASS = ["06_biotic_finite_difference", "07_biotic_lattice_boltzmann", "08_two_microbes"]
 
 
 def _example_xml(name):
-    d = os.path.join(REF_EXAMPLES, name)
-    if not os.path.isdir(d):
+    ex = _ref_examples()
+    d = os.path.join(ex, name) if ex else ""
+    if not ex or not os.path.isdir(d):
         pytest.skip("reference examples absent")
     xs = sorted(f for f in os.listdir(d) if f.endswith(".xml"))
     assert xs, name
