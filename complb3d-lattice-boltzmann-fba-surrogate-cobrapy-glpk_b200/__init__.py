@@ -42,7 +42,7 @@ c_int32, c_double, c_int64 = ctypes.c_int32, ctypes.c_double, ctypes.c_int64
 class Rxn(ctypes.Structure):
     _fields_ = [("microbe", c_int32), ("n_monod", c_int32), ("monod_s", c_int32 * MAX_MONOD),
                 ("monod_ks", c_double * MAX_MONOD), ("n_mass", c_int32), ("mass_s", c_int32 * 2),
-                ("k", c_double), ("nu", c_double * MAX_SOLUTES), ("yield_", c_double)]
+                ("k", c_double), ("nu", c_double * MAX_SOLUTES), ("yield_", c_double), ("ksp", c_double)]
 
 
 class EqSystem(ctypes.Structure):
@@ -205,10 +205,11 @@ def make_config(nx, ny, nz, tau_ns=0.8, rho_in=1.001, rho_out=1.0, solutes=(), m
     return c
 
 
-def add_rxn(cfg, microbe=-1, k=0.0, monod=(), mass=(), nu=None, yield_=0.0):
-    """Append one table-driven rate expression to cfg."""
+def add_rxn(cfg, microbe=-1, k=0.0, monod=(), mass=(), nu=None, yield_=0.0, ksp=0.0):
+    """Append one table-driven rate expression to cfg (ksp > 0: the
+    mass-action product P enters as max(P / ksp - 1, 0))."""
     r = cfg.rxn[cfg.n_rxn]
-    r.microbe, r.k, r.yield_ = microbe, k, yield_
+    r.microbe, r.k, r.yield_, r.ksp = microbe, k, yield_, ksp
     r.n_monod = len(monod)
     for j, (s, ks) in enumerate(monod):
         r.monod_s[j], r.monod_ks[j] = s, ks

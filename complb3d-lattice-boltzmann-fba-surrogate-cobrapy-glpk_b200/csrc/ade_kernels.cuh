@@ -182,9 +182,18 @@ static __device__ void rates_dev(const AdeParams& p, int abiotic, const double* 
             const double c = c0 < THRD ? 0.0 : c0;
             rate *= c / (r.monod_ks[j] + c);
         }
-        for (int j = 0; j < r.n_mass; ++j) {
-            const double c0 = C[r.mass_s[j] * cs];
-            rate *= c0 < THRD ? 0.0 : c0;
+        if (r.ksp > 0.0) {
+            double prod = 1.0;
+            for (int j = 0; j < r.n_mass; ++j) {
+                const double c0 = C[r.mass_s[j] * cs];
+                prod *= c0 < THRD ? 0.0 : c0;
+            }
+            rate *= fmax(prod / r.ksp - 1.0, 0.0);
+        } else {
+            for (int j = 0; j < r.n_mass; ++j) {
+                const double c0 = C[r.mass_s[j] * cs];
+                rate *= c0 < THRD ? 0.0 : c0;
+            }
         }
         for (int s = 0; s < p.S; ++s) R[s * bd] = fma(r.nu[s], rate, R[s * bd]);
         if (!abiotic) BR[r.microbe * bd] = fma(r.yield, rate, BR[r.microbe * bd]);

@@ -82,7 +82,7 @@ inline bool rxn_is(const cl_rxn& r, int microbe, std::initializer_list<int> mono
 // immobile mineral (CaCO3(s)); one sessile microbe.
 //   reaction 0  microbe 0: k B  DOC/(Ks+DOC)  O2/(Ks+O2)      (aerobic oxidation)
 //   reaction 1  microbe 0: k B  DOC/(Ks+DOC)  NO3/(Ks+NO3)    (denitrification)
-//   reaction 2  abiotic:   k [Ca2+][CO3--]                    (precipitation)
+//   reaction 2  abiotic:   k [Ca2+][CO3--], or k (Omega - 1)+ with a Ksp (precipitation)
 // Equilibrium: 3 components (HCO3-, Ca2+, H+) over the 9 solutes as species.
 struct ChemCoupled {
     static constexpr int kId = 1;
@@ -128,8 +128,15 @@ struct ChemCoupled {
         for (int s = 0; s < S; ++s) R[s] = 0.0;
         const cl_rxn& r = p.rxn[2];
         double rate = r.k;
-        rate *= chem_mass(C[4]);
-        rate *= chem_mass(C[6]);
+        if (r.ksp > 0.0) {
+            double prod = 1.0;
+            prod *= chem_mass(C[4]);
+            prod *= chem_mass(C[6]);
+            rate *= fmax(prod / r.ksp - 1.0, 0.0);
+        } else {
+            rate *= chem_mass(C[4]);
+            rate *= chem_mass(C[6]);
+        }
         chem_add<S>(r, rate, R);
         chem_close_abiotic<S>(R);
     }

@@ -212,6 +212,7 @@ int read_complab_xml(const std::string& path, HostRun& run, std::string& err) {
                 x.microbe = r->has("microbe") ? (int32_t)(*r)["microbe"].integer() : -1;
                 x.k = (*r)["k"].num();
                 x.yield = num_or(*r, {"yield"}, 0.0);
+                x.ksp = num_or(*r, {"ksp"}, 0.0);
                 if (r->has("monod"))
                     for (auto& pv : pairs((*r)["monod"])) {
                         if (x.n_monod == CL_MAX_MONOD) throw std::runtime_error("too many Monod terms in " + r->path);

@@ -226,13 +226,15 @@ def coupled_config(pkg, nx, ny, nz, seed=5, warm_previous=True):
                  CaCO3(aq) (logK -7.13) as secondary species, Newton to a 1e-10
                  relative residual every step in every pore voxel, started
                  from the voxel's previous solution (cold start after 4 misses);
-      precipitation Ca2+ + CO3-- -> CaCO3(s), rate 1e-6 [Ca][CO3], on wall-
-                 adjacent voxels only; a voxel whose inventory reaches 1.0
-                 becomes solid (node conversion every 200 steps)."""
+      precipitation Ca2+ + CO3-- -> CaCO3(s) on wall-adjacent voxels only,
+                 saturation-index driven: rate 1e-6 (Omega - 1) per step above
+                 saturation, Omega = [Ca][CO3] / Ksp, log Ksp = -8.48 (calcite);
+                 the inflow is supersaturated (pH 8, Omega ~ 30); a voxel whose
+                 inventory reaches 1.0 becomes solid (node conversion)."""
     rng = np.random.default_rng(seed)
     taus = rng.uniform(0.6, 0.9, 8)
-    inlet = [2e-3, 2.5e-4, 5e-4, 2e-3, 1e-3, 1e-7, 1e-30, 1e-30]
-    c0 = [1e-3, 2.5e-4, 1e-4, 2e-3, 1e-3, 1e-7, 1e-30, 1e-30]
+    inlet = [2e-3, 2.5e-4, 5e-4, 5e-3, 5e-3, 1e-8, 1e-30, 1e-30]
+    c0 = [1e-3, 2.5e-4, 1e-4, 5e-3, 5e-3, 1e-8, 1e-30, 1e-30]
     sol = [{"tau": float(taus[s]), "c0": c0[s], "left": "D", "left_value": inlet[s], "right": "N"} for s in range(8)]
     sol.append({"immobile": True, "c0": 0.0})
     cfg = pkg.make_config(nx, ny, nz, tau_ns=0.8, rho_in=1.0005, rho_out=1.0, solutes=sol, microbes=1, dt=1.0)
@@ -250,7 +252,7 @@ def coupled_config(pkg, nx, ny, nz, seed=5, warm_previous=True):
     cfg.precip_substrate = 8
     cfg.max_precip_rho = 1.0
     cfg.precip_code = MAT_SOLID
-    pkg.add_rxn(cfg, k=1e-6, mass=[4, 6], nu={4: -1.0, 6: -1.0, 8: 1.0})
+    pkg.add_rxn(cfg, k=1e-6, mass=[4, 6], nu={4: -1.0, 6: -1.0, 8: 1.0}, ksp=10.0 ** -8.48)
     cfg.use_equilibrium = 1
     S = np.zeros((9, 3))
     S[3, 0] = 1; S[4, 1] = 1; S[5, 2] = 1
@@ -260,6 +262,26 @@ def coupled_config(pkg, nx, ny, nz, seed=5, warm_previous=True):
     pkg.set_eq_system(cfg.eq, S, logk, [3, 4, 5], max_iter=100, tol=1e-10, warm_iter=4)
     cfg.eq_warm_previous = 1 if warm_previous else 0
     return cfg
+
+
+def seed_mineral(mask, seed, full, frac=0.5):
+    """Pre-existing mineral coatings: an inventory U[0, full) on `frac` of the
+    wall-adjacent pore voxels of x = 1..nx-2, so that precipitation carries some
+    of them across the conversion threshold during a run."""
+    rng = np.random.default_rng(seed)
+    pore = mask == MAT_PORE
+    wall = (mask == MAT_SOLID) | (mask == MAT_BB)
+    near = np.zeros_like(pore)
+    for ax in range(3):
+        for sh in (1, -1):
+            near |= np.roll(wall, sh, axis=ax)
+    cand = pore & near
+    cand[0] = False
+    cand[-1] = False
+    pick = cand & (rng.random(mask.shape) < frac)
+    m = np.zeros(mask.shape)
+    m[pick] = rng.uniform(0.0, full, int(pick.sum()))
+    return m
 
 
 def cold_species(S, T, comp_species=None):

@@ -59,8 +59,11 @@ extern "C" {
  *  examples/13_precipitation/defineAbioticKinetics.hh:39-58) and the dual-Monod
  * law of the 128^3 biotic workload:
  *   r = k * (B_m if microbe >= 0) * prod_j C[monod_s[j]]/(Ks[j] + C[monod_s[j]])
- *         * prod_j C[mass_s[j]]
- *   subsR[s] += nu[s] * r ;  bioR[microbe] += yield * r                      */
+ *         * P,   P = prod_j C[mass_s[j]]
+ *   subsR[s] += nu[s] * r ;  bioR[microbe] += yield * r
+ * With ksp > 0 the mass-action factor P becomes the saturation-index drive
+ * max(P / ksp - 1, 0) (precipitation at a rate k (Omega - 1) above
+ * saturation; an extension: the reference has no solubility products). */
 typedef struct {
     int32_t microbe;                   /* -1 = abiotic */
     int32_t n_monod;
@@ -71,6 +74,7 @@ typedef struct {
     double  k;
     double  nu[CL_MAX_SOLUTES];
     double  yield;
+    double  ksp;                       /* > 0: saturation-index drive on the mass-action product */
 } cl_rxn;
 
 /* Components-and-species tableau (reference EquilibriumChemistry<T>,

@@ -327,9 +327,20 @@ void orc_rates(const cl_config* cfg, int abiotic, const double* C, const double*
             double c = C[r->monod_s[j]]; if (c < 0) c = 0;
             rate *= c / (r->monod_ks[j] + c);
         }
-        for (int j = 0; j < r->n_mass; ++j) {
-            double c = C[r->mass_s[j]]; if (c < 0) c = 0;
-            rate *= c;
+        if (r->ksp > 0.0) {
+            /* saturation-index drive (an extension; the reference has no
+             * solubility products): max(P / ksp - 1, 0) */
+            double prod = 1.0;
+            for (int j = 0; j < r->n_mass; ++j) {
+                double c = C[r->mass_s[j]]; if (c < 0) c = 0;
+                prod *= c;
+            }
+            rate *= fmax(prod / r->ksp - 1.0, 0.0);
+        } else {
+            for (int j = 0; j < r->n_mass; ++j) {
+                double c = C[r->mass_s[j]]; if (c < 0) c = 0;
+                rate *= c;
+            }
         }
         for (int s = 0; s < cfg->n_solutes; ++s) subsR[s] += r->nu[s] * rate;
         if (r->microbe >= 0 && bioR) bioR[r->microbe] += r->yield * rate;
