@@ -16,8 +16,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libcomplab_gpu.so")
 
-MAX_SOLUTES, MAX_MICROBES, MAX_RXN, MAX_MONOD = 16, 4, 16, 3
-MAX_COMP, MAX_SPECIES, MAX_CODES, MAX_PHASES = 8, 16, 8, 4
+MAX_SOLUTES, MAX_MICROBES, MAX_RXN, MAX_MONOD = 32, 12, 16, 3
+MAX_COMP, MAX_SPECIES, MAX_CODES, MAX_PHASES = 24, 128, 8, 4
 SRG_MAX_LAYERS, SRG_MAX_WIDTH = 5, 32
 
 OK, WARN_NOT_CONVERGED = 0, 1

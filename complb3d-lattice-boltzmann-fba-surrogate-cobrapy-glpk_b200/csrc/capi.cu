@@ -207,7 +207,13 @@ cl_ctx* cl_create(const cl_config* cfg, void* stream, int* status) {
     p.n_rxn = cfg->n_rxn;
     for (int k = 0; k < cfg->n_rxn; ++k) p.rxn[k] = cfg->rxn[k];
     for (int m = 0; m < CL_MAX_MICROBES; ++m) p.decay[m] = cfg->decay[m];
-    p.eq = cfg->eq;
+    p.eq.n_comp = cfg->eq.n_comp;
+    p.eq.n_species = cfg->eq.n_species;
+    p.eq.max_iter = cfg->eq.max_iter;
+    p.eq.warm_iter = cfg->eq.warm_iter;
+    p.eq.solver = cfg->eq.solver;
+    p.eq.anderson_depth = cfg->eq.anderson_depth;
+    p.eq.tol = cfg->eq.tol;
     p.solid_code = cfg->solid_code;
     p.bb_code = cfg->bb_code;
     p.n_srg = cfg->n_srg;

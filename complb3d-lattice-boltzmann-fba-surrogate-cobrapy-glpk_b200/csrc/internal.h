@@ -39,6 +39,14 @@ struct SrgNetDev {
     const float* params;
 };
 
+// The equilibrium settings the transport kernels read (the tableau itself
+// travels as EqDev).
+struct EqParams {
+    int    n_comp, n_species;
+    int    max_iter, warm_iter, solver, anderson_depth;
+    double tol;
+};
+
 // Per-solute transport parameters passed by value to the transport kernels.
 struct AdeParams {
     int    S;                          // all solutes
@@ -55,7 +63,7 @@ struct AdeParams {
     int    n_rxn;
     cl_rxn rxn[CL_MAX_RXN];
     double decay[CL_MAX_MICROBES];
-    cl_eq_system eq;
+    EqParams eq;
     int    solid_code, bb_code;
     int    n_srg;
     cl_srg_organism srg[CL_MAX_SRG_ORG];

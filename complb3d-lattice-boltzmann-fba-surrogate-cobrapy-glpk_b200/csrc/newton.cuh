@@ -26,29 +26,35 @@
 
 namespace cl {
 
+// the one-thread solvers' tableau: up to kEqDevSpecies species (one per
+// solute in the transport step) over up to kEqDevComp components (five are
+// instantiated); larger tableaux go to the warp solver (speciation_large.cu)
+constexpr int kEqDevSpecies = CL_MAX_SOLUTES, kEqDevComp = 8;
 struct EqDev {
     int ns;
     int all_int;                       // every stoichiometric coefficient is an integer in [-8, 8]
-    double stoich[CL_MAX_SPECIES][CL_MAX_COMP];
-    double absS[CL_MAX_SPECIES][CL_MAX_COMP];
-    double logk[CL_MAX_SPECIES];
-    double k10[CL_MAX_SPECIES];        // 10^logK
-    signed char ipow[CL_MAX_SPECIES][CL_MAX_COMP];
-    int active[CL_MAX_SPECIES];
-    int comp_species[CL_MAX_COMP];
-    int neg[CL_MAX_COMP];              // some species carries component j with a negative power
-    double inv_mu[CL_MAX_COMP];        // PCF: 1 / the smallest positive coefficient of component j (at most 1)
+    double stoich[kEqDevSpecies][kEqDevComp];
+    double absS[kEqDevSpecies][kEqDevComp];
+    double logk[kEqDevSpecies];
+    double k10[kEqDevSpecies];         // 10^logK
+    signed char ipow[kEqDevSpecies][kEqDevComp];
+    int active[kEqDevSpecies];
+    int comp_species[kEqDevComp];
+    int neg[kEqDevComp];               // some species carries component j with a negative power
+    double inv_mu[kEqDevComp];         // PCF: 1 / the smallest positive coefficient of component j (at most 1)
     int solver;                        // CL_EQ_SOLVER_* of the transport step
     int depth;                         // PCF Anderson depth
 };
 
+// (callers hold n_species <= kEqDevSpecies and n_comp <= kEqDevComp)
 inline void eqdev_from_system(const cl_eq_system& s, EqDev& d) {
-    d.ns = s.n_species;
+    d.ns = s.n_species < kEqDevSpecies ? s.n_species : kEqDevSpecies;
+    const int ns = d.ns, ncm = s.n_comp < kEqDevComp ? s.n_comp : kEqDevComp;
     d.all_int = 1;
-    for (int i = 0; i < CL_MAX_SPECIES; ++i) {
+    for (int i = 0; i < kEqDevSpecies; ++i) {
         int act = 0;
-        for (int j = 0; j < CL_MAX_COMP; ++j) {
-            double v = (i < s.n_species && j < s.n_comp) ? s.stoich[i][j] : 0.0;
+        for (int j = 0; j < kEqDevComp; ++j) {
+            double v = (i < ns && j < ncm) ? s.stoich[i][j] : 0.0;
             d.stoich[i][j] = v;
             d.absS[i][j] = v < 0 ? -v : v;
             if (v > 1e-10 || v < -1e-10) act = 1;
@@ -57,16 +63,16 @@ inline void eqdev_from_system(const cl_eq_system& s, EqDev& d) {
             d.ipow[i][j] = (signed char)r;
         }
         d.active[i] = act;
-        d.logk[i] = i < s.n_species ? s.logk[i] : 0.0;
+        d.logk[i] = i < ns ? s.logk[i] : 0.0;
         d.k10[i] = std::pow(10.0, d.logk[i]);
     }
-    for (int j = 0; j < CL_MAX_COMP; ++j) {
-        d.comp_species[j] = j < s.n_comp ? s.comp_species[j] : -1;
+    for (int j = 0; j < kEqDevComp; ++j) {
+        d.comp_species[j] = j < ncm ? s.comp_species[j] : -1;
         d.neg[j] = 0;
-        for (int i = 0; i < s.n_species && j < s.n_comp; ++i) if (d.ipow[i][j] < 0) d.neg[j] = 1;
+        for (int i = 0; i < ns && j < ncm; ++i) if (d.ipow[i][j] < 0) d.neg[j] = 1;
         // pcf_residual's mu_min (part4_eqsolver.hh:690-697): starts at 1, equilibrium species only
         double mu_min = 1.0;
-        for (int i = 0; i < s.n_species && j < s.n_comp; ++i) {
+        for (int i = 0; i < ns && j < ncm; ++i) {
             if (!d.active[i]) continue;
             const double mu = s.stoich[i][j];
             if (mu > 1e-10 && mu < mu_min) mu_min = mu;

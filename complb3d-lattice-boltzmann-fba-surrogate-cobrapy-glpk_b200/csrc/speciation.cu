@@ -15,6 +15,7 @@
 // the starting point.
 #include "internal.h"
 #include "newton.cuh"
+#include "speciation_large.h"
 #include "pcf.cuh"
 #include "mma.cuh"
 #include <cmath>
@@ -529,7 +530,64 @@ struct cl_eq_solver {
     unsigned long long* fail_count = nullptr;   // two counters
     unsigned long long* pcf_count = nullptr;    // PCF solves that did not converge
     uint64_t adam_t = 0;
+    // tableaux beyond the one-thread solver (more than 5 components or more
+    // species than kEqDevSpecies): the warp solver of speciation_large.cu on a
+    // device copy of the tableau; no network, no PCF
+    bool large = false;
+    LgTableau lg{};
+    double* lg_stoich = nullptr;
+    double* lg_logk = nullptr;
+    uint8_t* lg_active = nullptr;
 };
+
+// entry points that need the network or the one-thread solvers refuse a large tableau
+static bool refuse_large(const cl_eq_solver* s, const char* what) {
+    if (!s->large) return false;
+    set_error(std::string(what) + ": not available for tableaux above 5 components or " +
+              std::to_string(kEqDevSpecies) + " species (the batch Newton solve is)");
+    return true;
+}
+
+static cl_eq_solver* create_large(const cl_eq_system* sys, void* stream, int* status) {
+    const int nc = sys->n_comp, ns = sys->n_species;
+    cl_eq_solver* s = new cl_eq_solver();
+    auto fail = [&](int st) { if (status) *status = st; cl_eq_destroy(s); return (cl_eq_solver*)nullptr; };
+    s->sys = *sys;
+    s->nc = nc;
+    s->large = true;
+    if (stream) s->stream = (cudaStream_t)stream;
+    else {
+        if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(CL_ERR_CUDA);
+        s->own_stream = true;
+    }
+    std::vector<double> St((size_t)ns * nc), lk(ns);
+    std::vector<uint8_t> act(ns, 0);
+    for (int i = 0; i < ns; ++i) {
+        lk[i] = sys->logk[i];
+        for (int j = 0; j < nc; ++j) {
+            const double v = sys->stoich[i][j];
+            St[(size_t)i * nc + j] = v;
+            if (v > 1e-10 || v < -1e-10) act[i] = 1;
+        }
+    }
+    cudaError_t e = cudaMalloc(&s->lg_stoich, sizeof(double) * St.size());
+    if (e == cudaSuccess) e = cudaMalloc(&s->lg_logk, sizeof(double) * ns);
+    if (e == cudaSuccess) e = cudaMalloc(&s->lg_active, ns);
+    if (e == cudaSuccess) e = cudaMalloc(&s->fail_count, 2 * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(s->lg_stoich, St.data(), sizeof(double) * St.size(), cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(s->lg_logk, lk.data(), sizeof(double) * ns, cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(s->lg_active, act.data(), ns, cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) return fail(cuda_fail(e, "cl_eq_create"));
+    s->lg.nc = nc;
+    s->lg.ns = ns;
+    s->lg.stoich = s->lg_stoich;
+    s->lg.logk = s->lg_logk;
+    s->lg.active = s->lg_active;
+    for (int j = 0; j < CL_MAX_COMP; ++j) s->lg.comp_species[j] = j < nc ? sys->comp_species[j] : -1;
+    if (status) *status = CL_OK;
+    return s;
+}
 
 static size_t mlp_smem_bytes() { return sizeof(MlpSmem); }
 static size_t mlp_fwd_smem_bytes() { return sizeof(MlpSmemFwd); }
@@ -626,11 +684,25 @@ extern "C" {
 
 cl_eq_solver* cl_eq_create(const cl_eq_system* sys, void* stream, int* status) {
     auto fail = [&](int st, cl_eq_solver* s) { if (status) *status = st; cl_eq_destroy(s); return (cl_eq_solver*)nullptr; };
-    if (!sys || sys->n_comp < 1 || sys->n_comp > 5 || sys->n_species < sys->n_comp || sys->n_species > CL_MAX_SPECIES) {
-        set_error("speciation batch needs 1..5 components and n_comp <= n_species <= 16");
+    if (!sys || sys->n_comp < 1 || sys->n_comp > CL_MAX_COMP || sys->n_species < sys->n_comp ||
+        sys->n_species > CL_MAX_SPECIES) {
+        set_error("speciation batch needs 1.." + std::to_string(CL_MAX_COMP) + " components and n_comp <= n_species <= " +
+                  std::to_string(CL_MAX_SPECIES));
         if (status) *status = CL_ERR_ARG;
         return nullptr;
     }
+    for (int j = 0; j < sys->n_comp; ++j)
+        if (sys->comp_species[j] < -1 || sys->comp_species[j] >= sys->n_species) {
+            set_error("comp_species out of range");
+            if (status) *status = CL_ERR_ARG;
+            return nullptr;
+        }
+    if (sys->max_iter < 0 || sys->warm_iter < 0) {
+        set_error("max_iter and warm_iter must be >= 0");
+        if (status) *status = CL_ERR_ARG;
+        return nullptr;
+    }
+    if (sys->n_comp > 5 || sys->n_species > kEqDevSpecies) return create_large(sys, stream, status);
     if ((sys->solver != CL_EQ_SOLVER_NEWTON && sys->solver != CL_EQ_SOLVER_PCF) || sys->anderson_depth < 0 ||
         sys->anderson_depth > kPcfMaxDepth) {
         set_error("unknown equilibrium solver, or anderson_depth outside 0..8");
@@ -695,7 +767,8 @@ int cl_eq_destroy(cl_eq_solver* s) {
     if (!s) return CL_OK;
     if (s->stream) cudaStreamSynchronize(s->stream);
     void* ptrs[] = {s->w.W1, s->w.W2, s->w.W2T, s->w.W3, s->w.W3T, s->w.b, s->w.norm, s->master, s->m1, s->m2,
-                    s->part, s->grad, s->fail_list, s->fail_list2, s->stop_mark, s->fail_count, s->pcf_count};
+                    s->part, s->grad, s->fail_list, s->fail_list2, s->stop_mark, s->fail_count, s->pcf_count,
+                    s->lg_stoich, s->lg_logk, s->lg_active};
     for (void* p : ptrs) if (p) cudaFree(p);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     delete s;
@@ -710,6 +783,7 @@ int cl_eq_param_count(const cl_eq_solver* s, int32_t* count) {
 
 int cl_eq_get_params(cl_eq_solver* s, float* host) {
     if (!s || !host) return CL_ERR_ARG;
+    if (refuse_large(s, "cl_eq_get_params")) return CL_ERR_ARG;
     CL_CUDA(cudaMemcpyAsync(host, s->master, sizeof(float) * s->n_params, cudaMemcpyDeviceToHost, s->stream));
     CL_CUDA(cudaStreamSynchronize(s->stream));
     return CL_OK;
@@ -717,6 +791,7 @@ int cl_eq_get_params(cl_eq_solver* s, float* host) {
 
 int cl_eq_set_params(cl_eq_solver* s, const float* host) {
     if (!s || !host) return CL_ERR_ARG;
+    if (refuse_large(s, "cl_eq_set_params")) return CL_ERR_ARG;
     int r = upload_params(s, host);
     if (r) return r;
     CL_CUDA(cudaStreamSynchronize(s->stream));
@@ -728,6 +803,14 @@ int cl_eq_solve_device(cl_eq_solver* s, const double* d_totals, const double* d_
     if (!s || !d_totals || !d_logfree || n < 0) { set_error("null argument"); return CL_ERR_ARG; }
     if (n == 0) return CL_OK;
     if (start == CL_EQ_START_COLD && !d_cold_species) { set_error("cold start needs the species vectors"); return CL_ERR_ARG; }
+    if (s->large) {
+        if (start != CL_EQ_START_GIVEN && start != CL_EQ_START_COLD) {
+            set_error("large tableaux start cold or from a given point");
+            return CL_ERR_ARG;
+        }
+        return lg_solve(s->lg, s->stream, d_totals, d_cold_species, d_logfree, d_iters, d_status, n, start,
+                        s->sys.max_iter, s->sys.warm_iter, s->sys.tol, s->fail_count);
+    }
     if (start == CL_EQ_START_LEARNED) {
         mlp_predict_kernel<<<grid_for((n + TS - 1) / TS, 1, 148 * 6), MLP_THREADS, mlp_fwd_smem_bytes(), s->stream>>>(
             s->w, s->nc, d_totals, d_logfree, nullptr, nullptr, n);
@@ -747,6 +830,7 @@ int cl_eq_solve_device(cl_eq_solver* s, const double* d_totals, const double* d_
 int cl_eq_pcf_device(cl_eq_solver* s, const double* d_in, double* d_out, int32_t* d_iters, uint8_t* d_conv,
                      int64_t n) {
     if (!s || !d_in || !d_out || n < 0) { set_error("null argument"); return CL_ERR_ARG; }
+    if (refuse_large(s, "cl_eq_pcf_device")) return CL_ERR_ARG;
     if (n == 0) return CL_OK;
     CL_CUDA(cudaMemsetAsync(s->pcf_count, 0, sizeof(unsigned long long), s->stream));
     const int blocks = grid_for(n, 128, 148 * 8);
@@ -794,6 +878,7 @@ int cl_eq_pcf_host(cl_eq_solver* s, const double* in, double* out, int32_t* iter
 
 int cl_eq_predict_device(cl_eq_solver* s, const double* d_totals, double* d_logfree, int64_t n) {
     if (!s || !d_totals || !d_logfree || n < 0) { set_error("null argument"); return CL_ERR_ARG; }
+    if (refuse_large(s, "cl_eq_predict_device")) return CL_ERR_ARG;
     if (n == 0) return CL_OK;
     mlp_predict_kernel<<<grid_for((n + TS - 1) / TS, 1, 148 * 6), MLP_THREADS, mlp_fwd_smem_bytes(), s->stream>>>(
         s->w, s->nc, d_totals, d_logfree, nullptr, nullptr, n);
@@ -834,6 +919,7 @@ int cl_eq_solve_host(cl_eq_solver* s, const double* totals, const double* cold_s
 // gradients of one batch (no update), for checks against the FP64 oracle
 int cl_eq_grad_host(cl_eq_solver* s, const float* x, const float* y, int32_t n, float* loss, float* grads) {
     if (!s || !x || !y || n <= 0) { set_error("null argument"); return CL_ERR_ARG; }
+    if (refuse_large(s, "cl_eq_grad_host")) return CL_ERR_ARG;
     const int nc = s->nc, np = s->n_params;
     float *dx = nullptr, *dy = nullptr;
     CL_CUDA(cudaMalloc(&dx, sizeof(float) * n * nc));
@@ -862,6 +948,7 @@ int cl_eq_grad_host(cl_eq_solver* s, const float* x, const float* y, int32_t n, 
 
 int cl_eq_predict_host(cl_eq_solver* s, const float* x, float* y, int32_t n) {
     if (!s || !x || !y || n <= 0) { set_error("null argument"); return CL_ERR_ARG; }
+    if (refuse_large(s, "cl_eq_predict_host")) return CL_ERR_ARG;
     const int nc = s->nc;
     float *dx = nullptr, *dy = nullptr;
     CL_CUDA(cudaMalloc(&dx, sizeof(float) * n * nc));
@@ -902,6 +989,7 @@ extern "C" int cl_eq_train(cl_eq_solver* s, const double* d_totals, const double
     if (!s || !d_totals || !d_logfree || n_pairs < TS || epochs < 1 || batch < TS) {
         set_error("cl_eq_train: bad arguments"); return CL_ERR_ARG;
     }
+    if (refuse_large(s, "cl_eq_train")) return CL_ERR_ARG;
     const int nc = s->nc, np = s->n_params;
     // normalisation from a strided sample of at most 65536 pairs
     const int64_t m = std::min<int64_t>(n_pairs, 65536);
@@ -1015,7 +1103,7 @@ static int noalloc_scratch(unsigned long long** out) {
 extern "C" int cl_eq_solve_noalloc(const cl_eq_system* sys, const double* d_totals, const double* d_cold_species,
                                    double* d_logfree, int32_t* d_iters, uint8_t* d_status, int64_t n, int32_t start,
                                    void* stream) {
-    if (!sys || sys->n_comp < 1 || sys->n_comp > 5 || sys->n_species < sys->n_comp || sys->n_species > CL_MAX_SPECIES) {
+    if (!sys || sys->n_comp < 1 || sys->n_comp > 5 || sys->n_species < sys->n_comp || sys->n_species > kEqDevSpecies) {
         set_error("cl_eq_solve_noalloc: 1..5 components and n_comp <= n_species <= 16");
         return CL_ERR_ARG;
     }

@@ -245,7 +245,7 @@ int read_complab_xml(const std::string& path, HostRun& run, std::string& err) {
             cl_eq_system& e = c.eq;
             const std::vector<std::string> comps = eq->has("components") ? (*eq)["components"].words()
                                                                           : std::vector<std::string>{};
-            if (comps.empty() || (int)comps.size() > CL_MAX_COMP) throw std::runtime_error("equilibrium needs 1..8 components");
+            if (comps.empty() || (int)comps.size() > CL_MAX_COMP) throw std::runtime_error("equilibrium needs 1.." + std::to_string(CL_MAX_COMP) + " components");
             e.n_comp = (int32_t)comps.size();
             e.n_species = S;
             for (int j = 0; j < e.n_comp; ++j) {

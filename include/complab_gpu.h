@@ -32,12 +32,12 @@
 extern "C" {
 #endif
 
-#define CL_MAX_SOLUTES   16
-#define CL_MAX_MICROBES  4
+#define CL_MAX_SOLUTES   32
+#define CL_MAX_MICROBES  12
 #define CL_MAX_RXN       16
 #define CL_MAX_MONOD     3
-#define CL_MAX_COMP      8
-#define CL_MAX_SPECIES   16
+#define CL_MAX_COMP      24      /* tableau components (batch speciation); the transport step takes 1..5 */
+#define CL_MAX_SPECIES   128     /* tableau species (batch speciation); the transport step: one per solute */
 #define CL_MAX_CODES     8
 #define CL_MAX_PHASES    4
 
@@ -78,8 +78,11 @@ typedef struct {
 } cl_rxn;
 
 /* Components-and-species tableau (reference EquilibriumChemistry<T>,
- * src/complab3d_processors_part4_eqsolver.hh:186-1271).  Species are the
- * solutes in order; rows of all zeros are non-equilibrium species.
+ * src/complab3d_processors_part4_eqsolver.hh:186-1271).  In the transport
+ * step the species are the solutes in order (1..5 components); the batch
+ * solver takes up to CL_MAX_COMP components over CL_MAX_SPECIES species (the
+ * reference's uranium network is 17 x 95).  Rows of all zeros are
+ * non-equilibrium species.
  * solver selects the equilibrium solve of the transport step:
  *   CL_EQ_SOLVER_NEWTON  Newton in log10 free components (the reference's
  *                        reserve solver, NR_reserve.hh:512-615, with the
