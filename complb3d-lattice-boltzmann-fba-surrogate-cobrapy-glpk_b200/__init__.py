@@ -34,7 +34,8 @@ SRG_IN_FIN, SRG_IN_CONC, SRG_IN_BIOMASS = 0, 1, 2
 SRG_OUT_GROWTH, SRG_OUT_FOUT = 0, 1
 KERNEL_ADE_MAIN, KERNEL_FLOW_STEP, KERNEL_ADE_REACT = 0, 1, 2
 OPT_COMPILED_CHEM, OPT_FAST_VARIANT = 1, 2
-CHEM_COUPLED, CHEM_BIOTIC4 = 1, 2
+CHEM_COUPLED, CHEM_BIOTIC4, CHEM_ZHAO24 = 1, 2, 3
+RATELAW_TABLE, RATELAW_ZHAO = 0, 1
 
 c_int32, c_double, c_int64 = ctypes.c_int32, ctypes.c_double, ctypes.c_int64
 
@@ -98,6 +99,7 @@ class Config(ctypes.Structure):
         ("n_srg", c_int32), ("srg", SrgOrganism * MAX_SRG_ORG),
         ("ca_enabled", c_int32), ("ca_half", c_int32), ("ca_bmax", c_double), ("ca_thrd_frac", c_double),
         ("microbe_code", c_int32 * MAX_MICROBES), ("ca_seed", ctypes.c_uint64),
+        ("rate_law", c_int32),
     ]
 
 

@@ -74,7 +74,7 @@ __device__ __forceinline__ int fast_chain(const AdeK& k, int64_t n, uint32_t sto
             const double b = m < M ? k.bio[m * N + n] : 0.0;
             B[m] = b < THRD ? 0.0 : b;
         }
-        Chem::kinetics(p, C, B, R, BR);
+        Chem::kinetics(p, C, B, R, BR, k.mask[n]);
 #pragma unroll
         for (int s = 0; s < S; ++s) {
             const double d = R[s] * p.dt;
@@ -100,7 +100,7 @@ __device__ __forceinline__ int fast_chain(const AdeK& k, int64_t n, uint32_t sto
     const bool dis = p.do_dissol && (cls & (F_PHASE_NBR | F_PHASE_SELF));
     if (abio || dis) {
         if (abio) {
-            Chem::abiotic(p, C, R);
+            Chem::abiotic(p, C, R, k.mask[n]);
 #pragma unroll
             for (int s = 0; s < S; ++s) {
                 const double d = R[s] * p.dt;
@@ -328,6 +328,7 @@ int fast_step(Ctx* c) {
 int chem_match(const cl_config& cfg) {
     if (ChemCoupled::matches(cfg)) return ChemCoupled::kId;
     if (ChemBiotic4::matches(cfg)) return ChemBiotic4::kId;
+    if (ChemZhao24::matches(cfg)) return ChemZhao24::kId;
     return 0;
 }
 
@@ -335,6 +336,7 @@ const char* chem_name(int id) {
     switch (id) {
         case ChemCoupled::kId: return ChemCoupled::kName;
         case ChemBiotic4::kId: return ChemBiotic4::kName;
+        case ChemZhao24::kId: return ChemZhao24::kName;
         default: return "run-time rate table";
     }
 }
@@ -343,6 +345,7 @@ int ade_step_fast(Ctx* c) {
     switch (c->chem) {
         case ChemCoupled::kId: return fast_step<ChemCoupled>(c);
         case ChemBiotic4::kId: return fast_step<ChemBiotic4>(c);
+        case ChemZhao24::kId: return fast_step<ChemZhao24>(c);
         default: set_error("no compiled chemistry selected"); return CL_ERR_STATE;
     }
 }

@@ -52,6 +52,7 @@ static int validate(const cl_config* c) {
     if (c->n_solutes < 0 || c->n_solutes > CL_MAX_SOLUTES) { set_error("n_solutes out of range"); return CL_ERR_ARG; }
     if (c->n_microbes < 0 || c->n_microbes > CL_MAX_MICROBES) { set_error("n_microbes out of range"); return CL_ERR_ARG; }
     if (c->n_rxn < 0 || c->n_rxn > CL_MAX_RXN) { set_error("n_rxn out of range"); return CL_ERR_ARG; }
+    if (c->rate_law != CL_RATELAW_TABLE && c->rate_law != CL_RATELAW_ZHAO) { set_error("unknown rate_law"); return CL_ERR_ARG; }
     {
         const int64_t N = (int64_t)c->nx * c->ny * c->nz;
         if (N * 19 >= (int64_t)1 << 32) { set_error("lattice too large: 19*nx*ny*nz must stay below 2^32"); return CL_ERR_ARG; }
@@ -200,7 +201,7 @@ cl_ctx* cl_create(const cl_config* cfg, void* stream, int* status) {
     int n_bio = 0, n_abio = 0;
     for (int k = 0; k < cfg->n_rxn; ++k) (cfg->rxn[k].microbe >= 0 ? n_bio : n_abio)++;
     p.do_kin = cfg->enable_kinetics && (n_bio > 0 || cfg->n_microbes > 0);
-    p.do_abio = cfg->enable_abiotic && n_abio > 0 && cfg->n_solutes > 0;
+    p.do_abio = cfg->enable_abiotic && (n_abio > 0 || cfg->rate_law != CL_RATELAW_TABLE) && cfg->n_solutes > 0;
     p.surface_only = cfg->precip_enabled && cfg->abiotic_surface_only;
     p.do_eq = cfg->use_equilibrium;
     p.eq_warm = cfg->use_equilibrium && cfg->eq_warm_previous;
@@ -224,6 +225,11 @@ cl_ctx* cl_create(const cl_config* cfg, void* stream, int* status) {
     p.n_phases = cfg->n_phases;
     for (int k = 0; k < cfg->n_phases; ++k) p.phase[k] = cfg->phases[k];
     c->chem = chem_match(*cfg);
+    if (cfg->rate_law != CL_RATELAW_TABLE && c->chem == 0) {
+        set_error("the compiled rate law needs the layout it was written for (CL_RATELAW_ZHAO: 24 substrates "
+                  "with 2, 4, 5, 6, 9, 13, 21, 22, 23 immobile, 12 microbes, no equilibrium, no dissolution)");
+        return fail(CL_ERR_ARG);
+    }
     // device memory
     int r = CL_OK;
     if ((r = dalloc(c, &c->d_mask, N)) || (r = dalloc(c, &c->d_ns_cls, N)) || (r = dalloc(c, &c->d_ade_cls, N)) ||
@@ -508,7 +514,13 @@ int cl_set_option(cl_ctx* h, int32_t key, int64_t value) {
     if (!h) return CL_ERR_ARG;
     Ctx* c = &h->c;
     switch (key) {
-        case CL_OPT_COMPILED_CHEM: c->chem_on = value != 0; return CL_OK;
+        case CL_OPT_COMPILED_CHEM:
+            if (value == 0 && c->cfg.rate_law != CL_RATELAW_TABLE) {
+                set_error("cl_set_option: a compiled rate law has no run-time table form");
+                return CL_ERR_ARG;
+            }
+            c->chem_on = value != 0;
+            return CL_OK;
         case CL_OPT_FAST_VARIANT:
             if (value < 0 || value > 4) { set_error("cl_set_option: variant 0..4"); return CL_ERR_ARG; }
             c->fast_variant = (int)value; return CL_OK;

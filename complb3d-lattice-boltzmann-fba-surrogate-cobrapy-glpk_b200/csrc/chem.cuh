@@ -20,13 +20,15 @@
 //   S, NMOB, M, NC                  solutes, mobile solutes, microbes, components
 //   mobile(s), slot(s)              whether solute s has a lattice, and its slot
 //   matches(cfg)                    host: the configuration has this structure
-//   kinetics(p, C, B, R, BR)        rates per second (defineRxnKinetics)
-//   abiotic(p, C, R)                rates per second (defineAbioticRxnKinetics)
+//   kinetics(p, C, B, R, BR, mask)  rates per second (defineRxnKinetics); B floored
+//                                   at thrd, C as stored
+//   abiotic(p, C, R, mask)          rates per second (defineAbioticRxnKinetics)
 // Rates follow the run-time table's arithmetic (rates_dev) term for term, so
 // a configuration runs to the same numbers on either launch.
 #pragma once
 #include <cmath>
 #include "internal.h"
+#include "../../include/complab_ratelaw.hpp"
 
 namespace cl {
 
@@ -95,10 +97,11 @@ struct ChemCoupled {
         for (int s = 0; s < S; ++s) if ((c.immobile[s] != 0) == mobile(s)) return false;
         if (!c.use_equilibrium || c.eq.n_comp != NC || c.eq.n_species != S || c.eq.solver != CL_EQ_SOLVER_NEWTON)
             return false;
-        return rxn_is(c.rxn[0], 0, {0, 1}, {}) && rxn_is(c.rxn[1], 0, {0, 2}, {}) && rxn_is(c.rxn[2], -1, {}, {4, 6});
+        return c.rate_law == CL_RATELAW_TABLE && rxn_is(c.rxn[0], 0, {0, 1}, {}) && rxn_is(c.rxn[1], 0, {0, 2}, {}) &&
+               rxn_is(c.rxn[2], -1, {}, {4, 6});
     }
     __host__ __device__ static void kinetics(const AdeParams& p, const double (&C)[S], const double (&B)[MW],
-                                             double (&R)[S], double (&BR)[MW]) {
+                                             double (&R)[S], double (&BR)[MW], int) {
 #pragma unroll
         for (int s = 0; s < S; ++s) R[s] = 0.0;
         BR[0] = 0.0;
@@ -123,7 +126,7 @@ struct ChemCoupled {
         }
         chem_close_biotic<S, MW>(p, M, B, R, BR);
     }
-    __host__ __device__ static void abiotic(const AdeParams& p, const double (&C)[S], double (&R)[S]) {
+    __host__ __device__ static void abiotic(const AdeParams& p, const double (&C)[S], double (&R)[S], int) {
 #pragma unroll
         for (int s = 0; s < S; ++s) R[s] = 0.0;
         const cl_rxn& r = p.rxn[2];
@@ -154,10 +157,10 @@ struct ChemBiotic4 {
     static bool matches(const cl_config& c) {
         if (c.n_solutes != S || c.n_microbes != M || c.n_rxn != 2 || c.n_srg != 0 || c.use_equilibrium) return false;
         for (int s = 0; s < S; ++s) if (c.immobile[s]) return false;
-        return rxn_is(c.rxn[0], 0, {0, 1}, {}) && rxn_is(c.rxn[1], 0, {0, 2}, {});
+        return c.rate_law == CL_RATELAW_TABLE && rxn_is(c.rxn[0], 0, {0, 1}, {}) && rxn_is(c.rxn[1], 0, {0, 2}, {});
     }
     __host__ __device__ static void kinetics(const AdeParams& p, const double (&C)[S], const double (&B)[MW],
-                                             double (&R)[S], double (&BR)[MW]) {
+                                             double (&R)[S], double (&BR)[MW], int) {
 #pragma unroll
         for (int s = 0; s < S; ++s) R[s] = 0.0;
         BR[0] = 0.0;
@@ -182,9 +185,49 @@ struct ChemBiotic4 {
         }
         chem_close_biotic<S, MW>(p, M, B, R, BR);
     }
-    __host__ __device__ static void abiotic(const AdeParams&, const double (&)[S], double (&R)[S]) {
+    __host__ __device__ static void abiotic(const AdeParams&, const double (&)[S], double (&R)[S], int) {
 #pragma unroll
         for (int s = 0; s < S; ++s) R[s] = 0.0;
+    }
+};
+
+// ---- the reference's default network: the Zhao uranium / iron / sulfur model ----
+// The 24-substrate layout (speciation off) with its 12 biomass pools held as
+// sessile fields; the rate laws are clrl::zhao (include/complab_ratelaw.hpp),
+// called with the concentrations and biomass floored at thrd and the voxel's
+// mask, as run_kinetics / run_abiotic_kinetics call defineRxnKinetics /
+// defineAbioticRxnKinetics (complab3d_processors_part1.hh:63-249).
+struct ChemZhao24 {
+    static constexpr int kId = 3;
+    static constexpr const char* kName = "Zhao uranium network (24 substrates, 12 biomass pools)";
+    static constexpr int S = 24, NMOB = 15, M = 12, NC = 0, MW = 12;
+    __host__ __device__ static constexpr bool mobile(int s) {
+        return !(s == 2 || s == 4 || s == 5 || s == 6 || s == 9 || s == 13 || s == 21 || s == 22 || s == 23);
+    }
+    // rank of solute s among the mobile ones
+    __host__ __device__ static constexpr int slot(int s) {
+        int k = 0;
+        for (int q = 0; q < s; ++q) k += mobile(q) ? 1 : 0;
+        return k;
+    }
+    static bool matches(const cl_config& c) {
+        if (c.rate_law != CL_RATELAW_ZHAO || c.n_solutes != S || c.n_microbes != M || c.n_srg != 0) return false;
+        if (c.use_equilibrium || c.dissol_enabled) return false;
+        for (int s = 0; s < S; ++s) if ((c.immobile[s] != 0) == mobile(s)) return false;
+        return true;
+    }
+    __host__ __device__ static void kinetics(const AdeParams&, const double (&C)[S], const double (&B)[MW],
+                                             double (&R)[S], double (&BR)[MW], int mask) {
+        double Cf[S];
+#pragma unroll
+        for (int s = 0; s < S; ++s) Cf[s] = C[s] < THRD ? 0.0 : C[s];
+        clrl::zhao::kinetics(clrl::cspan{B, MW}, clrl::cspan{Cf, S}, clrl::dspan{R, S}, clrl::dspan{BR, MW}, mask);
+    }
+    __host__ __device__ static void abiotic(const AdeParams&, const double (&C)[S], double (&R)[S], int mask) {
+        double Cf[S];
+#pragma unroll
+        for (int s = 0; s < S; ++s) Cf[s] = C[s] < THRD ? 0.0 : C[s];
+        clrl::zhao::abiotic(clrl::cspan{Cf, S}, clrl::dspan{R, S}, mask);
     }
 };
 

@@ -237,7 +237,17 @@ typedef struct {
     double  ca_thrd_frac;
     int32_t microbe_code[CL_MAX_MICROBES];
     uint64_t ca_seed;
+    /* the rate laws: CL_RATELAW_TABLE runs the rxn table above; a compiled law
+     * (include/complab_ratelaw.hpp) replaces the table as the reference's
+     * compiled defineKinetics.hh / defineAbioticKinetics.hh do:
+     *   CL_RATELAW_ZHAO  the reference's default Zhao uranium / iron / sulfur
+     *                    network, on its 24-substrate layout (speciation off)
+     *                    with 12 sessile biomass pools; substrates 2, 4, 5, 6,
+     *                    9, 13, 21, 22, 23 immobile */
+    int32_t rate_law;
 } cl_config;
+#define CL_RATELAW_TABLE 0
+#define CL_RATELAW_ZHAO  1
 
 typedef struct cl_ctx cl_ctx;
 

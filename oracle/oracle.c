@@ -841,7 +841,8 @@ static void vox_kinetics(const rx_ctx* r, int64_t n) {
     for (int s = 0; s < S; ++s) { double c = vox_dens(r, s, n); C[s] = c < THRD ? 0.0 : c; dC[s] = 0.0; }
     for (int b = 0; b < M; ++b) { double v = r->st->bio[b*N + n]; Bm[b] = v < THRD ? 0.0 : v; dB[b] = 0.0; }
     if (r->any_bio) {
-        orc_rates(cfg, 0, C, Bm, R, BR);
+        if (r->st->kin) r->st->kin(Bm, M, C, S, R, BR, r->st->mask[n]);
+        else orc_rates(cfg, 0, C, Bm, R, BR);
         for (int s = 0; s < S; ++s) {
             double d = R[s] * cfg->dt;
             dC[s] = (d > THRD || d < -THRD) ? d : 0.0;
@@ -878,7 +879,8 @@ static void vox_abiotic(const rx_ctx* r, int x, int y, int z, int64_t n, double*
     if (!fire) return;
     double C[CL_MAX_SOLUTES], R[CL_MAX_SOLUTES];
     for (int s = 0; s < S; ++s) { double c = vox_dens(r, s, n); C[s] = c < THRD ? 0.0 : c; }
-    orc_rates(cfg, 1, C, NULL, R, NULL);
+    if (st->abio) st->abio(C, S, R, st->mask[n]);
+    else orc_rates(cfg, 1, C, NULL, R, NULL);
     for (int s = 0; s < S; ++s) {
         double d = R[s] * cfg->dt;
         dC[s] = (d > THRD || d < -THRD) ? d : 0.0;
@@ -1012,7 +1014,7 @@ int64_t orc_reaction_stage(const cl_config* cfg, orc_state* st) {
     rc.cfg = cfg; rc.st = st; rc.N = N;
     rc.any_bio = cfg->enable_kinetics && (n_bio > 0 || M > 0);
     rc.any_srg = cfg->n_srg > 0 && st->srg_nets;
-    rc.any_abio = cfg->enable_abiotic && S > 0 && n_abio > 0;
+    rc.any_abio = cfg->enable_abiotic && S > 0 && (n_abio > 0 || st->abio != NULL);
     const int dissol = cfg->dissol_enabled && cfg->n_phases > 0 && st->phase;
     if (!dissol) {
         /* processors run over the whole lattice in turn, and each reads only

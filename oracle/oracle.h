@@ -67,6 +67,11 @@ typedef struct {
     int32_t* eq_iters; /* [N] Newton iterations of the last equilibrium step (may be NULL) */
     const cl_surrogate_net* srg_nets;  /* [CL_MAX_SRG_ORG] networks of the surrogate organisms (may be NULL) */
     uint8_t* phase;    /* [N] dissolvable phase id, 0 = none (may be NULL without dissolution) */
+    /* compiled rate laws standing in for the rate table (NULL: the table):
+     * kin(B, nB, C, nC, subsR, bioR, mask) and abio(C, nC, subsR, mask), the
+     * defineRxnKinetics / defineAbioticRxnKinetics signatures over arrays */
+    void (*kin)(const double*, int, const double*, int, double*, double*, int);
+    void (*abio)(const double*, int, double*, int);
 } orc_state;
 
 void orc_ade_init(const cl_config* cfg, orc_state* st);

@@ -84,7 +84,8 @@ class OrcState(ctypes.Structure):
     _fields_ = [("g", ctypes.c_void_p), ("g_tmp", ctypes.c_void_p), ("imm", ctypes.c_void_p),
                 ("bio", ctypes.c_void_p), ("u", ctypes.c_void_p), ("mask", ctypes.c_void_p),
                 ("ade_class", ctypes.c_void_p), ("rho_bc", ctypes.c_void_p), ("eq_iters", ctypes.c_void_p),
-                ("srg_nets", ctypes.c_void_p), ("phase", ctypes.c_void_p)]
+                ("srg_nets", ctypes.c_void_p), ("phase", ctypes.c_void_p),
+                ("kin", ctypes.c_void_p), ("abio", ctypes.c_void_p)]
 
 
 class OrcCa(ctypes.Structure):
@@ -191,6 +192,12 @@ class Transport:
         arr = (type(nets[0]) * len(nets))(*nets)
         self._nets = arr
         self.st.srg_nets = ctypes.addressof(arr)
+
+    def set_rate_law(self, kin_addr, abio_addr):
+        """Compiled rate laws (C function addresses with the signatures of
+        orc_state.kin / orc_state.abio) in place of the rate table."""
+        self.st.kin = kin_addr
+        self.st.abio = abio_addr
 
     def set_biomass(self, m, values):
         self.bio[m * self.N:(m + 1) * self.N] = np.asarray(values, np.float64).reshape(-1)
