@@ -23,6 +23,7 @@
 // operation for operation, so both give the same fields.
 #include "ade_kernels.cuh"
 #include "chem.cuh"
+#include "learned.cuh"
 
 namespace cl {
 
@@ -152,6 +153,11 @@ __device__ __forceinline__ int fast_chain(const AdeK& k, int64_t n, uint32_t sto
                 for (int j = 0; j < NC; ++j) x[j] = xprev[j];
             }
         }
+        // no previous solution of its own: the network's guess, once trained
+        if (!warm && k.learn_w) {
+            learn_start<NC>(k.learn_w, k.learn_norm, T, x);
+            warm = true;
+        }
         for (int phase = warm ? 0 : 1; phase < 2; ++phase) {
             if (phase == 1) {
 #pragma unroll
@@ -172,6 +178,8 @@ __device__ __forceinline__ int fast_chain(const AdeK& k, int64_t n, uint32_t sto
             for (int j = 0; j < NC; ++j) { k.eq_xp[(int64_t)j * N + sto] = xprev[j]; k.eq_x[(int64_t)j * N + sto] = x[j]; }
         }
         if (k.eq_iters) k.eq_iters[n] = it;
+        if (conv && k.pair_T && learn_sampled((uint32_t)n, k.pair_salt, k.pair_mask))
+            learn_store<NC>(k.pair_T, k.pair_X, k.pair_count, k.pair_cap, T, x);
         if (!conv) nonconv = 1;
         else {
 #pragma unroll

@@ -64,6 +64,15 @@ struct AdeK {
     double* rel;              // S*N releases of the phase voxels (null without dissolution)
     unsigned long long* counters;   // [0] non-converged solves, [1] sites without the storage they need
     const int32_t* sidx;            // N storage index of each site's slots
+    // learned warm start (one-launch step only): network weights when trained,
+    // and the ring the converged pairs of the sampled voxels go to
+    const float* learn_w;
+    const float* learn_norm;
+    double* pair_T;
+    double* pair_X;
+    unsigned long long* pair_count;
+    int64_t pair_cap;
+    uint32_t pair_salt, pair_mask;
     int nodyn_coupled;
     int parity;
     AdeParams p;
@@ -683,6 +692,24 @@ inline AdeK make_adek(Ctx* c) {
     k.rel = c->d_rel;
     k.counters = c->d_counters;
     k.sidx = c->d_sidx;
+    k.learn_w = nullptr;
+    k.learn_norm = nullptr;
+    k.pair_T = k.pair_X = nullptr;
+    k.pair_count = nullptr;
+    k.pair_cap = 0;
+    k.pair_salt = (uint32_t)(c->step_index * 0x632BE5ABu);
+    k.pair_mask = (1u << c->learn_shift) - 1u;
+    if (c->learn && c->learn_interval > 0) {
+        k.pair_T = c->d_pair_T;
+        k.pair_X = c->d_pair_X;
+        k.pair_count = c->d_pair_count;
+        k.pair_cap = c->pair_cap;
+        if (c->learn_ready) {
+            int trained = 0;
+            eq_solver_network(c->learn, &k.learn_w, &k.learn_norm, &trained);
+            if (!trained) k.learn_w = k.learn_norm = nullptr;
+        }
+    }
     k.nodyn_coupled = c->ade_nodyn_coupled ? 1 : 0;
     k.parity = c->ade_parity;
     k.p = c->ap;

@@ -276,7 +276,9 @@ int cl_destroy(cl_ctx* h) {
     void* ptrs[] = {c->d_mask, c->d_ns_cls, c->d_ade_cls, c->d_f, c->d_u, c->d_g, c->d_imm, c->d_bio,
                     c->d_rho_adj, c->d_eq_iters, c->d_eq_x, c->d_eq_xp, c->d_phase, c->d_rel, c->d_counters, c->d_tracer,
                     c->d_energy_part, c->d_scratch, c->d_ca_total, c->d_ca_age, c->d_ca_distpos, c->d_ca_out,
-                    c->d_dc, c->d_live, c->d_live_blk, c->d_sidx, c->d_site_of, c->d_flive, c->d_fsidx};
+                    c->d_dc, c->d_live, c->d_live_blk, c->d_sidx, c->d_site_of, c->d_flive, c->d_fsidx,
+                    c->d_pair_T, c->d_pair_X, c->d_pair_count};
+    if (c->learn) cl_eq_destroy(c->learn);
     for (void* p : ptrs) if (p) cudaFree(p);
     for (int o = 0; o < CL_MAX_SRG_ORG; ++o) if (c->d_srg_params[o]) cudaFree(c->d_srg_params[o]);
     for (int k = 0; k < Ctx::kTimedKernels; ++k)
@@ -510,6 +512,52 @@ int cl_set_surrogate(cl_ctx* h, int32_t slot, const cl_surrogate_net* net) {
     return CL_OK;
 }
 
+// learning on (interval > 0) or off: the network and its ring of pairs
+static int learn_enable(Ctx* c, int64_t interval) {
+    if (interval < 0 || interval > (1 << 30)) { set_error("cl_set_option: learning interval >= 0"); return CL_ERR_ARG; }
+    if (interval == 0) { c->learn_interval = 0; return CL_OK; }
+    const cl_eq_system& e = c->cfg.eq;
+    if (!c->cfg.use_equilibrium || e.solver != CL_EQ_SOLVER_NEWTON || e.n_comp > 5 || c->chem == 0 || !c->chem_on) {
+        set_error("the learned start needs Newton speciation (1..5 components) in a compiled chemistry's step");
+        return CL_ERR_STATE;
+    }
+    if (!c->learn) {
+        int st = CL_OK;
+        c->learn = cl_eq_create(&e, c->stream, &st);
+        if (!c->learn) return st;
+        c->pair_cap = 1 << 20;
+        int r = CL_OK;
+        if ((r = dalloc(c, &c->d_pair_T, (size_t)c->pair_cap * e.n_comp)) ||
+            (r = dalloc(c, &c->d_pair_X, (size_t)c->pair_cap * e.n_comp)) || (r = dalloc(c, &c->d_pair_count, 1)))
+            return r;
+        CL_CUDA(cudaMemsetAsync(c->d_pair_count, 0, sizeof(unsigned long long), c->stream));
+    }
+    c->learn_interval = (int)interval;
+    c->learn_steps = 0;
+    return CL_OK;
+}
+
+// after a step: every learn_interval steps, train on the ring and empty it
+static int learn_after_step(Ctx* c) {
+    if (!c->learn || c->learn_interval <= 0) return CL_OK;
+    if (++c->learn_steps < c->learn_interval) return CL_OK;
+    c->learn_steps = 0;
+    unsigned long long cnt = 0;
+    CL_CUDA(cudaMemcpyAsync(&cnt, c->d_pair_count, sizeof cnt, cudaMemcpyDeviceToHost, c->stream));
+    CL_CUDA(cudaStreamSynchronize(c->stream));
+    const int64_t n = std::min<int64_t>((int64_t)cnt, c->pair_cap);
+    if (n < 4096) return CL_OK;                 // fewer than one training batch: keep collecting
+    float loss = 0.f;
+    int r = cl_eq_train(c->learn, c->d_pair_T, c->d_pair_X, n, c->learn_epochs, 4096, 3e-3f,
+                        (uint64_t)c->step_index, &loss);
+    if (r < 0) return r;
+    c->learn_loss = loss;
+    c->learn_ready = true;
+    ++c->learn_trainings;
+    CL_CUDA(cudaMemsetAsync(c->d_pair_count, 0, sizeof(unsigned long long), c->stream));
+    return CL_OK;
+}
+
 int cl_set_option(cl_ctx* h, int32_t key, int64_t value) {
     if (!h) return CL_ERR_ARG;
     Ctx* c = &h->c;
@@ -524,6 +572,14 @@ int cl_set_option(cl_ctx* h, int32_t key, int64_t value) {
         case CL_OPT_FAST_VARIANT:
             if (value < 0 || value > 4) { set_error("cl_set_option: variant 0..4"); return CL_ERR_ARG; }
             c->fast_variant = (int)value; return CL_OK;
+        case CL_OPT_EQ_LEARN: return learn_enable(c, value);
+        case CL_OPT_EQ_FORGET: {
+            const int nc = c->cfg.eq.n_comp;
+            if (c->d_eq_x) CL_CUDA(cudaMemsetAsync(c->d_eq_x, 0xff, sizeof(double) * nc * c->geo.N, c->stream));
+            if (c->d_eq_xp) CL_CUDA(cudaMemsetAsync(c->d_eq_xp, 0xff, sizeof(double) * nc * c->geo.N, c->stream));
+            CL_CUDA(cudaStreamSynchronize(c->stream));
+            return CL_OK;
+        }
         default: set_error("cl_set_option: unknown key"); return CL_ERR_ARG;
     }
 }
@@ -534,6 +590,8 @@ int cl_get_option(cl_ctx* h, int32_t key, int64_t* value) {
     switch (key) {
         case CL_OPT_COMPILED_CHEM: *value = c->chem_on ? c->chem : 0; return CL_OK;
         case CL_OPT_FAST_VARIANT: *value = c->fast_variant; return CL_OK;
+        case CL_OPT_EQ_LEARN: *value = c->learn_interval; return CL_OK;
+        case CL_OPT_EQ_LEARN_TRAININGS: *value = c->learn_trainings; return CL_OK;
         default: set_error("cl_get_option: unknown key"); return CL_ERR_ARG;
     }
 }
@@ -548,6 +606,8 @@ int cl_step(cl_ctx* h, int32_t n) {
     for (int32_t i = 0; i < n; ++i) {
         int r = ade_step(c);
         if (r) return r;
+        ++c->step_index;
+        if ((r = learn_after_step(c))) return r;
     }
     unsigned long long cnts[2] = {0, 0};
     CL_CUDA(cudaMemcpyAsync(cnts, c->d_counters, sizeof cnts, cudaMemcpyDeviceToHost, c->stream));

@@ -2,6 +2,7 @@
 // translation units of libcomplab_gpu.so.  Not part of the C ABI.
 #pragma once
 #include <cuda_runtime.h>
+struct cl_eq_solver;
 #include <cstdint>
 #include <string>
 #include "../../include/complab_gpu.h"
@@ -162,7 +163,26 @@ struct Ctx {
     int      chem = 0;
     bool     chem_on = true;
     int      fast_variant = 0;   // launch shape of the one-launch step (block size, blocks per SM)
+    // learned warm start inside the step (learned.cuh): the network and its
+    // trainer, the ring of sampled converged pairs, the training interval
+    cl_eq_solver* learn = nullptr;
+    int      learn_interval = 0;        // steps between trainings, 0 = off
+    int      learn_shift = 4;           // one converged voxel in 2^shift joins the ring per step
+    int      learn_epochs = 2;
+    bool     learn_ready = false;       // the network has been trained at least once
+    double*  d_pair_T = nullptr;        // [cap][n_comp]
+    double*  d_pair_X = nullptr;
+    unsigned long long* d_pair_count = nullptr;
+    int64_t  pair_cap = 0;
+    int64_t  learn_steps = 0;           // steps since the last training
+    int64_t  step_index = 0;            // steps taken (the ring's sample salt)
+    float    learn_loss = 0.f;
+    int64_t  learn_trainings = 0;
 };
+
+// the network of a speciation solver for the step's learned start: FP32
+// master weights and standardisation (device), trained flag
+int eq_solver_network(cl_eq_solver* s, const float** master, const float** norm, int* trained);
 
 // event bracket around one launch of a timed kernel (no-op when timing is off)
 int timing_begin(Ctx* c, int kernel);

@@ -548,6 +548,14 @@ static bool refuse_large(const cl_eq_solver* s, const char* what) {
     return true;
 }
 
+int cl::eq_solver_network(cl_eq_solver* s, const float** master, const float** norm, int* trained) {
+    if (!s || s->large) return CL_ERR_ARG;
+    *master = s->master;
+    *norm = s->w.norm;
+    *trained = s->trained ? 1 : 0;
+    return CL_OK;
+}
+
 static cl_eq_solver* create_large(const cl_eq_system* sys, void* stream, int* status) {
     const int nc = sys->n_comp, ns = sys->n_species;
     cl_eq_solver* s = new cl_eq_solver();

@@ -331,6 +331,23 @@ int cl_step(cl_ctx* ctx, int32_t n);
  *                         get: the id of the compiled chemistry in use, 0 = none. */
 #define CL_OPT_COMPILED_CHEM 1
 #define CL_OPT_FAST_VARIANT  2   /* launch shape of the compiled chemistry's step, 0..4 */
+/* The learned warm start in the step (a compiled chemistry with Newton
+ * speciation of 1..5 components; no counterpart in the reference).
+ *   CL_OPT_EQ_LEARN  set K > 0: every step stores the (totals -> log10 free
+ *                    components) pairs of a sampled one in 16 of the converged
+ *                    voxels in a ring on the device (2^20 pairs); every K steps
+ *                    the library's network (n_comp -> 64 -> 64 -> n_comp, GELU,
+ *                    BF16 weights, FP32 accumulate) is trained on the device on
+ *                    the ring (two epochs) and the ring is emptied.  Once
+ *                    trained, a voxel with no previous solution of its own starts
+ *                    Newton from the network's guess, with the reference's cold
+ *                    start after eq.warm_iter iterations.  0: off.  get: K.
+ *   CL_OPT_EQ_FORGET set: every voxel forgets its previous solutions (the next
+ *                    step starts each solve from the network or cold).
+ *   CL_OPT_EQ_LEARN_TRAININGS get: trainings done so far. */
+#define CL_OPT_EQ_LEARN            3
+#define CL_OPT_EQ_FORGET           4
+#define CL_OPT_EQ_LEARN_TRAININGS  5
 int cl_set_option(cl_ctx* ctx, int32_t key, int64_t value);
 int cl_get_option(cl_ctx* ctx, int32_t key, int64_t* value);
 

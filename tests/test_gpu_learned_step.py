@@ -1,0 +1,50 @@
+"""The learned warm start inside the transport step (CL_OPT_EQ_LEARN): the
+network is trained on the device during the run on the pairs the step's own
+Newton solves produce, and gives the start of every voxel that has no
+previous solution of its own.
+
+Two contexts run the coupled chemistry from the same state, one learning
+(training every 5 steps) and one not.  After 20 steps both forget their
+previous solutions and take one more step: the learning one starts from the
+network, the other from the reference's cold start.  Newton's 1e-10 relative
+residual decides convergence in both, so the fields agree to rel. L2 <= 1e-6,
+and the learned start needs fewer iterations per voxel."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(b), 1e-300))
+
+
+def test_learned_start_in_the_step(gpu_lib, pkg, wl):
+    mask = wl.sphere_pack(66, 32, 32, 0.45, 2.0, 4.0, seed=71)
+    nx, ny, nz = mask.shape
+    cfg = wl.coupled_config(pkg, nx, ny, nz)
+    bio = wl.seed_biomass(mask, 72, frac=0.2)
+    out = {}
+    for learn in (True, False):
+        lat = pkg.Lattice(cfg)
+        lat.upload_mask(mask)
+        lat.flow_init()
+        lat.flow_steps(100)
+        lat.couple_velocity()
+        lat.ade_init()
+        lat.set_field(pkg.FIELD_BIOMASS, 0, bio)
+        if learn:
+            lat.set_option(pkg.OPT_EQ_LEARN, 5)
+        for _ in range(20):
+            assert lat.step(1) == pkg.OK
+        if learn:
+            assert lat.get_option(pkg.OPT_EQ_LEARN_TRAININGS) >= 2
+        lat.set_option(pkg.OPT_EQ_FORGET, 1)
+        assert lat.step(1) == pkg.OK
+        react = (mask == 2).reshape(-1)
+        it = lat.field(pkg.FIELD_EQ_ITERS).reshape(-1)[react]
+        out[learn] = ([lat.field(pkg.FIELD_CONC, s).reshape(-1) for s in range(cfg.n_solutes)], it.mean())
+        lat.close()
+    for s in range(cfg.n_solutes):
+        assert rel_l2(out[True][0][s], out[False][0][s]) <= 1e-6, s
+    assert out[True][1] < out[False][1], (out[True][1], out[False][1])
