@@ -35,6 +35,7 @@ SRG_OUT_GROWTH, SRG_OUT_FOUT = 0, 1
 KERNEL_ADE_MAIN, KERNEL_FLOW_STEP, KERNEL_ADE_REACT = 0, 1, 2
 OPT_COMPILED_CHEM, OPT_FAST_VARIANT, OPT_EQ_LEARN, OPT_EQ_FORGET, OPT_EQ_LEARN_TRAININGS = 1, 2, 3, 4, 5
 CHEM_COUPLED, CHEM_BIOTIC4, CHEM_ZHAO24 = 1, 2, 3
+OP_KINETICS, OP_SURROGATE, OP_ABIOTIC, OP_EQUILIBRIUM, OP_ALL = 1, 2, 4, 8, 15
 RATELAW_TABLE, RATELAW_ZHAO = 0, 1
 
 c_int32, c_double, c_int64 = ctypes.c_int32, ctypes.c_double, ctypes.c_int64
@@ -131,6 +132,8 @@ def load_library(path=LIB_PATH):
         ("cl_flow_velocity_stats", [vp, P(c_double), P(c_double), P(c_double)]),
         ("cl_flow_velocity_norm_masked", [vp, c_int32, P(c_double), P(c_int64)]),
         ("cl_set_option", [vp, c_int32, c_int64]), ("cl_get_option", [vp, c_int32, P(c_int64)]),
+        ("cl_op_collide", [vp]), ("cl_op_stream", [vp]), ("cl_op_reactions", [vp, c_int32]),
+        ("cl_op_kinetics", [vp]), ("cl_op_surrogate", [vp]), ("cl_op_abiotic", [vp]), ("cl_op_equilibrium", [vp]),
         ("cl_set_flow_pressure", [vp, c_double, c_double]), ("cl_set_transport", [vp, vp, vp, c_double]),
         ("cl_device_bytes", [vp, P(ctypes.c_uint64)]), ("cl_abi_sizes", [vp, c_int32]),
         ("cl_timing_enable", [vp, c_int32]), ("cl_timing_read", [vp, c_int32, P(c_double), P(c_int64)]),
@@ -330,6 +333,16 @@ class Lattice:
 
     def step(self, n=1):
         return self._c(self.lib.cl_step(self.h, n), "cl_step")
+
+    # the step taken apart (the reference's processor calls)
+    def op_collide(self):
+        return self._c(self.lib.cl_op_collide(self.h), "cl_op_collide")
+
+    def op_reactions(self, ops=OP_ALL):
+        return self._c(self.lib.cl_op_reactions(self.h, ops), "cl_op_reactions")
+
+    def op_stream(self):
+        return self._c(self.lib.cl_op_stream(self.h), "cl_op_stream")
 
     def set_option(self, key, value):
         self._c(self.lib.cl_set_option(self.h, key, int(value)), "cl_set_option")

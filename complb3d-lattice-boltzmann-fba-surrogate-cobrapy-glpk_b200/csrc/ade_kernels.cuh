@@ -295,11 +295,12 @@ static __device__ __noinline__ void surrogate_chain(const AdeParams& p, const do
 // run_kinetics (part1.hh:63-146) and run_surrogate3D deposit into the same
 // dC/dB lattices, each contribution only if above thrd: the increments of one
 // voxel into R (solutes) and BR (biomass), B its floored biomass.  Not applied.
+// ops (the per-operator entry points): bit 1 kinetics, bit 2 surrogate
 __device__ __forceinline__ void kinetics_increments(const AdeParams& p, const double* bio, int64_t N, int64_t n,
                                                     const double* Cur, int cs, double* R, double* B, double* BR,
-                                                    int bd) {
+                                                    int bd, int ops = 15) {
     for (int m = 0; m < p.M; ++m) { const double b = bio[m * N + n]; B[m * bd] = b < THRD ? 0.0 : b; }
-    if (p.do_kin) {
+    if (p.do_kin && (ops & 1)) {
         rates_dev(p, 0, Cur, cs, B, R, BR, bd);
         for (int s = 0; s < p.S; ++s) {
             const double d = R[s * bd] * p.dt;
@@ -313,7 +314,7 @@ __device__ __forceinline__ void kinetics_increments(const AdeParams& p, const do
         for (int s = 0; s < p.S; ++s) R[s * bd] = 0.0;
         for (int m = 0; m < p.M; ++m) BR[m * bd] = 0.0;
     }
-    if (p.n_srg > 0) surrogate_chain(p, Cur, cs, B, R, BR, bd);
+    if (p.n_srg > 0 && (ops & 2)) surrogate_chain(p, Cur, cs, B, R, BR, bd);
 }
 
 // The dissolution increments that reach voxel n (surfaceDissolutionKinetics3D,
@@ -369,17 +370,19 @@ __device__ __forceinline__ int pcf_voxel(const EqDev& e, int S, int max_iter, do
 // The reaction chain of one voxel.  Cur holds the current densities (updated
 // as each processor applies its increments), App the total increment per
 // solute.  Returns 1 if the equilibrium solve did not converge.
+// ops selects processors for the per-operator entry points (bit 1 kinetics,
+// 2 surrogate, 4 abiotic + dissolution, 8 equilibrium); the step runs all.
 template <int NC, int SOLVER>
 __device__ int reaction_chain(const AdeK& k, int64_t n, uint32_t sto, int x, int y, int z, uint8_t cls, double* Cur,
                               double* App,
-                              int cs, double* R, double* B, double* BR, int bd) {
+                              int cs, double* R, double* B, double* BR, int bd, int ops = 15) {
     const AdeParams& p = k.p;
     const int64_t N = k.g.N;
     int nonconv = 0;
     // kinetics and surrogate increments; update_rxnLattices (:338-429) applies
     // the sums that exceed thrd
-    if (p.do_kin || p.n_srg > 0) {
-        kinetics_increments(p, k.bio, N, n, Cur, cs, R, B, BR, bd);
+    if ((p.do_kin && (ops & 1)) || (p.n_srg > 0 && (ops & 2))) {
+        kinetics_increments(p, k.bio, N, n, Cur, cs, R, B, BR, bd, ops);
         for (int s = 0; s < p.S; ++s) {
             const double d = R[s * bd];
             if (d > THRD || d < -THRD) { Cur[s * cs] += d; App[s * cs] += d; }
@@ -392,8 +395,8 @@ __device__ int reaction_chain(const AdeK& k, int64_t n, uint32_t sto, int x, int
     // dC = dC0; run_abiotic_kinetics | surfaceAbioticKinetics3D (thresholded);
     // + surfaceDissolutionKinetics3D; update_abiotic_rxnLattices applies the
     // sums that exceed thrd
-    const bool abio = p.do_abio && (!p.surface_only || (cls & F_SURFACE));
-    const bool dis = p.do_dissol && (cls & (F_PHASE_NBR | F_PHASE_SELF));
+    const bool abio = p.do_abio && (ops & 4) && (!p.surface_only || (cls & F_SURFACE));
+    const bool dis = p.do_dissol && (ops & 4) && (cls & (F_PHASE_NBR | F_PHASE_SELF));
     if (abio || dis) {
         if (abio) {
             rates_dev(p, 1, Cur, cs, nullptr, R, nullptr, bd);
@@ -413,6 +416,7 @@ __device__ int reaction_chain(const AdeK& k, int64_t n, uint32_t sto, int x, int
     // run_equilibrium_biotic (part4_eqsolver.hh:1355-1494): species floored at
     // 1e-30; Newton applied only when converged (run_equilibrium_NR, NR_reserve.hh:734)
     if constexpr (NC > 0) {
+        if (!(ops & 8)) return nonconv;
         const EqDev& e = k.e;
         if constexpr (SOLVER == CL_EQ_SOLVER_PCF) {
             int32_t it = 0;

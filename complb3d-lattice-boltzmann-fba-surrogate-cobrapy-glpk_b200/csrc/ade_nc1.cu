@@ -1,6 +1,7 @@
 // ade_nc1.cu -- instantiations of the fused transport step with 1 equilibrium
 // components (0: no equilibrium), one translation unit per count so they build in parallel.
 #include "ade_kernels.cuh"
+#include "ops.cuh"
 
 namespace cl {
 
@@ -19,5 +20,7 @@ int ade_step_nc1(Ctx* c) {
                  return CL_ERR_ARG;
     }
 }
+
+int ade_ops_nc1(Ctx* c, const AdeK& k, int ops) { return launch_ops<1>(c, k, ops); }
 
 }  // namespace cl

@@ -1,6 +1,7 @@
 // ade_nc3.cu -- instantiations of the fused transport step with 3 equilibrium
 // components (0: no equilibrium), one translation unit per count so they build in parallel.
 #include "ade_kernels.cuh"
+#include "ops.cuh"
 
 namespace cl {
 
@@ -19,5 +20,7 @@ int ade_step_nc3(Ctx* c) {
                  return CL_ERR_ARG;
     }
 }
+
+int ade_ops_nc3(Ctx* c, const AdeK& k, int ops) { return launch_ops<3>(c, k, ops); }
 
 }  // namespace cl

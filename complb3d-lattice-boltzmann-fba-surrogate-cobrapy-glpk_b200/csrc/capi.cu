@@ -596,10 +596,22 @@ int cl_get_option(cl_ctx* h, int32_t key, int64_t* value) {
     }
 }
 
+int cl_op_collide(cl_ctx* h) { return h ? ops_collide(&h->c) : CL_ERR_ARG; }
+int cl_op_stream(cl_ctx* h) { return h ? ops_stream(&h->c) : CL_ERR_ARG; }
+int cl_op_reactions(cl_ctx* h, int32_t ops) {
+    if (!h || ops < 0 || ops > CL_OP_ALL) { set_error("cl_op_reactions: ops is a mask of CL_OP_*"); return CL_ERR_ARG; }
+    return ops ? ops_react(&h->c, ops) : CL_OK;
+}
+int cl_op_kinetics(cl_ctx* h) { return cl_op_reactions(h, CL_OP_KINETICS); }
+int cl_op_surrogate(cl_ctx* h) { return cl_op_reactions(h, CL_OP_SURROGATE); }
+int cl_op_abiotic(cl_ctx* h) { return cl_op_reactions(h, CL_OP_ABIOTIC); }
+int cl_op_equilibrium(cl_ctx* h) { return cl_op_reactions(h, CL_OP_EQUILIBRIUM); }
+
 int cl_step(cl_ctx* h, int32_t n) {
     if (!h || n < 0) return CL_ERR_ARG;
     Ctx* c = &h->c;
     if (!c->ade_ready) { set_error("call cl_ade_init first"); return CL_ERR_STATE; }
+    if (c->op_collided) { set_error("cl_step between cl_op_collide and cl_op_stream"); return CL_ERR_STATE; }
     for (int o = 0; o < c->ap.n_srg; ++o)
         if (!c->ap.net[c->ap.srg[o].net].params) { set_error("surrogate network slot not set"); return CL_ERR_STATE; }
     if (c->ap.n_mob == 0) { set_error("no mobile solute"); return CL_ERR_STATE; }

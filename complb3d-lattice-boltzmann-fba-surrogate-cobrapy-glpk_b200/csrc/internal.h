@@ -178,6 +178,7 @@ struct Ctx {
     int64_t  step_index = 0;            // steps taken (the ring's sample salt)
     float    learn_loss = 0.f;
     int64_t  learn_trainings = 0;
+    bool     op_collided = false;       // cl_op_collide ran; cl_op_stream completes the step
 };
 
 // the network of a speciation solver for the step's learned start: FP32
@@ -198,7 +199,11 @@ int flow_norm_masked(Ctx* c, int code, double out[2]);   // sum |u| and count of
 int classes_from_mask(Ctx* c);
 int ade_init(Ctx* c);
 int ade_step(Ctx* c);
-int ade_step_fast(Ctx* c);      // the transport step of the compiled chemistry c->chem
+int ade_step_fast(Ctx* c);
+// the per-operator entry points (ops.cu)
+int ops_collide(Ctx* c);
+int ops_react(Ctx* c, int ops);
+int ops_stream(Ctx* c);      // the transport step of the compiled chemistry c->chem
 int chem_match(const cl_config& cfg);   // id of the compiled chemistry cfg has the structure of, or 0
 const char* chem_name(int id);
 int ade_density(Ctx* c, int s, double* d_out);

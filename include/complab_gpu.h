@@ -317,6 +317,39 @@ int cl_set_transport(cl_ctx* ctx, const double* omega_pore, const double* omega_
 int cl_ade_init(cl_ctx* ctx);
 int cl_step(cl_ctx* ctx, int32_t n);
 
+/* The step taken apart, for callers that keep the reference's processor
+ * calls (src/complab.cpp:1252-1374, 1849-1857):
+ *   cl_op_collide      collide of every mobile solute, populations written back
+ *                      in place (AdvectionDiffusionBGKdynamics collide());
+ *   cl_op_kinetics     run_kinetics + update_rxnLattices (part1.hh:63-146, 338-429);
+ *   cl_op_surrogate    run_surrogate3D + update_rxnLattices (surrogate.hh:74-295);
+ *   cl_op_abiotic      the dC reset, run_abiotic_kinetics or surfaceAbioticKinetics3D,
+ *                      surfaceDissolutionKinetics3D, update_abiotic_rxnLattices
+ *                      (part1.hh:158-336, precipitationVOP.hh:53-145,
+ *                      dissolutionVOP.hh:265-435);
+ *   cl_op_equilibrium  run_equilibrium_biotic (part4_eqsolver.hh:1355-1494);
+ *   cl_op_reactions    the processors of the mask `ops` in one pass (kinetics and
+ *                      surrogate then share one increment, as they share dC);
+ *   cl_op_stream       stream (and the x-face boundary sites), ending the step.
+ * cl_op_collide, any reaction operators, cl_op_stream is one cl_step (to FP32
+ * rounding: the reactions read densities summed after the collision); the
+ * reaction operators also run alone on the current state.  The node
+ * conversions and the biofilm automaton are cl_precip_convert,
+ * cl_dissol_convert and cl_ca_redistribute.  Each call synchronises; the
+ * rate table only (a compiled rate law runs in cl_step). */
+#define CL_OP_KINETICS    1
+#define CL_OP_SURROGATE   2
+#define CL_OP_ABIOTIC     4
+#define CL_OP_EQUILIBRIUM 8
+#define CL_OP_ALL         15
+int cl_op_collide(cl_ctx* ctx);
+int cl_op_kinetics(cl_ctx* ctx);
+int cl_op_surrogate(cl_ctx* ctx);
+int cl_op_abiotic(cl_ctx* ctx);
+int cl_op_equilibrium(cl_ctx* ctx);
+int cl_op_reactions(cl_ctx* ctx, int32_t ops);
+int cl_op_stream(cl_ctx* ctx);
+
 /* Compiled chemistries.  The reference compiles its rate laws into the
  * program (defineKinetics.hh / defineAbioticKinetics.hh, included by
  * src/complab.cpp); the library likewise compiles chemistries in, each a fixed

@@ -1005,6 +1005,12 @@ static int vox_equilibrium(const rx_ctx* r, int64_t n) {
  * -> update_abiotic_rxnLattices -> run_equilibrium_biotic.  Returns the
  * number of Newton solves that did not converge. */
 int64_t orc_reaction_stage(const cl_config* cfg, orc_state* st) {
+    return orc_reaction_ops(cfg, st, ORC_OP_ALL);
+}
+
+/* the processors of the reaction stage selected by ops (ORC_OP_*), each as
+ * in orc_reaction_stage; kinetics and surrogate share one increment lattice */
+int64_t orc_reaction_ops(const cl_config* cfg, orc_state* st, int ops) {
     const int nx = cfg->nx, ny = cfg->ny, nz = cfg->nz, S = cfg->n_solutes, M = cfg->n_microbes;
     const int64_t N = (int64_t)nx * ny * nz;
     int64_t nonconv = 0;
@@ -1012,10 +1018,11 @@ int64_t orc_reaction_stage(const cl_config* cfg, orc_state* st) {
     for (int k = 0; k < cfg->n_rxn; ++k) { if (cfg->rxn[k].microbe >= 0) ++n_bio; else ++n_abio; }
     rx_ctx rc;
     rc.cfg = cfg; rc.st = st; rc.N = N;
-    rc.any_bio = cfg->enable_kinetics && (n_bio > 0 || M > 0);
-    rc.any_srg = cfg->n_srg > 0 && st->srg_nets;
-    rc.any_abio = cfg->enable_abiotic && S > 0 && (n_abio > 0 || st->abio != NULL);
-    const int dissol = cfg->dissol_enabled && cfg->n_phases > 0 && st->phase;
+    rc.any_bio = cfg->enable_kinetics && (n_bio > 0 || M > 0) && (ops & ORC_OP_KINETICS);
+    rc.any_srg = cfg->n_srg > 0 && st->srg_nets && (ops & ORC_OP_SURROGATE);
+    rc.any_abio = cfg->enable_abiotic && S > 0 && (n_abio > 0 || st->abio != NULL) && (ops & ORC_OP_ABIOTIC);
+    const int dissol = cfg->dissol_enabled && cfg->n_phases > 0 && st->phase && (ops & ORC_OP_ABIOTIC);
+    const int eq = cfg->use_equilibrium && (ops & ORC_OP_EQUILIBRIUM);
     if (!dissol) {
         /* processors run over the whole lattice in turn, and each reads only
          * its own voxel, so one pass per voxel is exact */
@@ -1031,7 +1038,7 @@ int64_t orc_reaction_stage(const cl_config* cfg, orc_state* st) {
                         vox_abiotic(&rc, x, y, z, n, dC);
                         for (int s = 0; s < S; ++s) if (dC[s] > THRD || dC[s] < -THRD) vox_apply(&rc, s, n, dC[s]);
                     }
-                    if (cfg->use_equilibrium) nonconv += vox_equilibrium(&rc, n);
+                    if (eq) nonconv += vox_equilibrium(&rc, n);
                 }
     } else {
         /* surfaceDissolutionKinetics3D writes the dC of face neighbours, so the
@@ -1076,7 +1083,7 @@ int64_t orc_reaction_stage(const cl_config* cfg, orc_state* st) {
                     }
                 }
         free(dab);
-        if (cfg->use_equilibrium) {
+        if (eq) {
             #pragma omp parallel for collapse(2) reduction(+:nonconv) schedule(dynamic, 4)
             for (int x = 1; x < nx - 1; ++x)
                 for (int y = 0; y < ny; ++y)
@@ -1098,9 +1105,16 @@ int64_t orc_reaction_stage(const cl_config* cfg, orc_state* st) {
  *   update_abiotic_rxnLattices -> run_equilibrium_biotic -> stream ->
  *   FlatAdiabaticBoundaryFunctional3D on zero-gradient faces. */
 int64_t orc_transport_step(const cl_config* cfg, orc_state* st) {
-    const int nx = cfg->nx, ny = cfg->ny, nz = cfg->nz, S = cfg->n_solutes, M = cfg->n_microbes;
+    orc_collide(cfg, st);
+    const int64_t nonconv = orc_reaction_stage(cfg, st);
+    orc_stream(cfg, st);
+    return nonconv;
+}
+
+/* collide of every mobile solute in place (the first part of a step) */
+void orc_collide(const cl_config* cfg, orc_state* st) {
+    const int nx = cfg->nx, ny = cfg->ny, nz = cfg->nz, S = cfg->n_solutes;
     const int64_t N = (int64_t)nx * ny * nz, P = (int64_t)ny * nz;
-    int64_t nonconv = 0;
     double* g = st->g;
 
     /* ---- collide (AdvectionDiffusionBGKdynamics, BounceBack, NoDynamics) ---- */
@@ -1138,9 +1152,14 @@ int64_t orc_transport_step(const cl_config* cfg, orc_state* st) {
                 }
             }
 
-    /* ---- reactions ---- */
-    nonconv += orc_reaction_stage(cfg, st);
+}
 
+/* stream every mobile solute (push, periodic y/z, reflect at x faces), then
+ * the zero-gradient faces (the last part of a step) */
+void orc_stream(const cl_config* cfg, orc_state* st) {
+    const int nx = cfg->nx, ny = cfg->ny, nz = cfg->nz, S = cfg->n_solutes;
+    const int64_t N = (int64_t)nx * ny * nz, P = (int64_t)ny * nz;
+    double* g = st->g;
     /* ---- stream (push, periodic y/z, reflect at x faces) ---- */
     for (int s = 0; s < S; ++s) {
         if (cfg->immobile[s]) continue;
@@ -1171,7 +1190,6 @@ int64_t orc_transport_step(const cl_config* cfg, orc_state* st) {
                 }
         }
     }
-    return nonconv;
 }
 
 /* precipNodeConversion3D (src/precipitationVOP.hh:158-219) */

@@ -79,6 +79,18 @@ void orc_ade_init(const cl_config* cfg, orc_state* st);
 int64_t orc_transport_step(const cl_config* cfg, orc_state* st);
 /* its reaction stage alone (kinetics .. equilibrium on the current densities) */
 int64_t orc_reaction_stage(const cl_config* cfg, orc_state* st);
+/* the step in its three parts: orc_transport_step = orc_collide, then
+ * orc_reaction_stage, then orc_stream; orc_reaction_ops runs the processors
+ * selected by ops (kinetics and surrogate share one increment lattice, as
+ * run_kinetics and run_surrogate3D share dC; abiotic includes dissolution) */
+#define ORC_OP_KINETICS    1
+#define ORC_OP_SURROGATE   2
+#define ORC_OP_ABIOTIC     4
+#define ORC_OP_EQUILIBRIUM 8
+#define ORC_OP_ALL         15
+void    orc_collide(const cl_config* cfg, orc_state* st);
+int64_t orc_reaction_ops(const cl_config* cfg, orc_state* st, int ops);
+void    orc_stream(const cl_config* cfg, orc_state* st);
 /* solute density of every site (mobile: sum of g; immobile: inventory) */
 void orc_solute_density(const cl_config* cfg, const orc_state* st, int s, double* out);
 

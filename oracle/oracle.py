@@ -45,6 +45,12 @@ def lib():
         _orc.orc_transport_step.argtypes = [vp, vp]
         _orc.orc_reaction_stage.restype = ctypes.c_int64
         _orc.orc_reaction_stage.argtypes = [vp, vp]
+        _orc.orc_reaction_ops.restype = ctypes.c_int64
+        _orc.orc_reaction_ops.argtypes = [vp, vp, i]
+        _orc.orc_collide.restype = None
+        _orc.orc_collide.argtypes = [vp, vp]
+        _orc.orc_stream.restype = None
+        _orc.orc_stream.argtypes = [vp, vp]
         _orc.orc_precip_convert.restype = ctypes.c_int64
         _orc.orc_precip_convert.argtypes = [vp, vp]
         _orc.orc_dissol_convert.restype = ctypes.c_int64
@@ -207,6 +213,17 @@ class Transport:
 
     def precip_convert(self):
         return lib().orc_precip_convert(ctypes.byref(self.cfg), ctypes.byref(self.st))
+
+    def collide(self):
+        lib().orc_collide(ctypes.byref(self.cfg), ctypes.byref(self.st))
+
+    def reaction_ops(self, ops):
+        """The reaction processors selected by ops (1 kinetics, 2 surrogate,
+        4 abiotic + dissolution, 8 equilibrium) on the current state."""
+        return lib().orc_reaction_ops(ctypes.byref(self.cfg), ctypes.byref(self.st), ops)
+
+    def stream(self):
+        lib().orc_stream(ctypes.byref(self.cfg), ctypes.byref(self.st))
 
     def reaction_stage(self):
         """The reaction stage of a step alone (no collide, no stream)."""
