@@ -186,11 +186,16 @@ def job_mlups(sites_per_rank, world, steps, ms):
 
 
 def coupled_setup(pkg, wl, shape, seed, stream=None):
+    """The coupled workload: sphere pack, the coupled chemistry with
+    saturation-driven precipitation and acid dissolution of the precipitate,
+    biomass on 2% of the wall-adjacent pore voxels, and mineral coatings
+    U[0, 1) of a full voxel on half of them (so node conversions happen)."""
     nx, ny, nz = shape
     mask = wl.sphere_pack(nx, ny, nz, 0.35, 5.0, 10.0, seed=seed)
-    cfg = wl.coupled_config(pkg, nx, ny, nz)
+    cfg = wl.coupled_config(pkg, nx, ny, nz, dissolution=True)
     bio = wl.seed_biomass(mask, seed + 1)
-    return cfg, mask, bio
+    mineral = wl.seed_mineral(mask, seed + 2, cfg.max_precip_rho)
+    return cfg, mask, bio, mineral
 
 
 def fluid_counts(cfg, mask):
@@ -198,15 +203,19 @@ def fluid_counts(cfg, mask):
     return int(fluid[1:-1].sum()), int(fluid.sum())
 
 
-def coupled_step(lat, i):
-    """One coupled step: transport, the amortised flow re-solve, and every 200
-    steps the node conversion with its dynamics switch and velocity coupling."""
+def coupled_step(lat, i, geometry=False):
+    """One coupled step: transport, the amortised flow re-solve (500 steps per
+    200 transport steps), and, when `geometry`, the node conversions
+    (precipitation seals, dissolution reopens) with the dynamics switch and
+    the velocity re-coupling.  Returns the voxels converted."""
     lat.step(1)
     lat.flow_steps(2 if i % 2 == 0 else 3)
-    if i % 200 == 199:
-        lat.precip_convert()
-        lat.update_dynamics()
-        lat.couple_velocity()
+    if not geometry:
+        return 0
+    changed = lat.precip_convert() + lat.dissol_convert()
+    lat.update_dynamics()
+    lat.couple_velocity()
+    return changed
 
 
 # ----------------------------------------------------------------- CPU legs
@@ -215,12 +224,13 @@ def cpu_coupled(steps, seed=5):
     coupled workload: returns (MLUPS, seconds, threads, sample text)."""
     pkg, wl = load_pkg(), load_workloads()
     from oracle import oracle as o
-    cfg, mask, bio = coupled_setup(pkg, wl, CPU_SAMPLE, seed)
+    cfg, mask, bio, mineral = coupled_setup(pkg, wl, CPU_SAMPLE, seed)
     fl = o.Flow(cfg, mask)
     fl.step(50)
     _, u = fl.macro()
     tr = o.Transport(cfg, mask, u=u)
     tr.set_biomass(0, bio)
+    tr.set_conc(8, mineral)
     tr.step(1)
     t0 = time.perf_counter()
     for i in range(steps):
@@ -375,6 +385,158 @@ def speciation_bench(pkg, wl, stream, n_train=1 << 20, n_test=1 << 21):
     return res
 
 
+# ----------------------------------------------------------------- other workloads
+def transport_roofline(ms, launches, n_fluid_int, bytes_per_site, n_interior, peak, peak_kind, kernel):
+    if not launches:
+        return None
+    b = n_fluid_int * bytes_per_site + n_interior
+    a = b / (ms / launches * 1e-3) / 1e9
+    return {"kernel": kernel, "bound": "hbm", "achieved": a, "peak": peak, "unit": "GB/s", "frac": a / peak,
+            "peak_source": peak_kind + " (hbm_gbs)", "algorithmic_bytes_per_launch": b,
+            "avg_launch_ms": ms / launches, "traffic": None}
+
+
+def surrogate_bench(pkg, wl, stream, steps=20, warmup=3, shape=(256, 256, 256)):
+    """The surrogate-rate workload: 256^3 sphere pack (porosity 0.4), two
+    organisms each with a 3 -> 20 tanh -> 20 tanh -> 4 network (mapminmax,
+    weights ~N(0, 0.3)), six solutes, the networks evaluated per voxel in the
+    step; transport step MLUPS and its roofline, and the FP64 oracle on a 64^3
+    sample of the same workload."""
+    import torch
+    nx, ny, nz = shape
+    mask = wl.sphere_pack(nx, ny, nz, 0.40, 4.0, 8.0, seed=31)
+    cfg = wl.surrogate_config(pkg, nx, ny, nz)
+    nets = wl.surrogate_nets(pkg)
+    b = [wl.seed_biomass(mask, 32 + m, frac=0.3, lo=0.005, hi=0.05) for m in range(2)]
+    lat = pkg.Lattice(cfg, stream=stream)
+    lat.upload_mask(mask)
+    lat.flow_init()
+    lat.flow_steps(200)
+    lat.couple_velocity()
+    for slot in range(2):
+        lat.set_surrogate(slot, nets[slot])
+    lat.ade_init()
+    for m in range(2):
+        lat.set_field(pkg.FIELD_BIOMASS, m, b[m])
+    for _ in range(warmup):
+        lat.step(1)
+    torch.cuda.synchronize()
+    lat.timing(True)
+    lat.timing_read(pkg.KERNEL_ADE_MAIN)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        lat.step(1)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    ade_ms, ade_n = lat.timing_read(pkg.KERNEL_ADE_MAIN)
+    lat.timing(False)
+    lat.close()
+    N = mask.size
+    n_fluid_int, _ = fluid_counts(cfg, mask)
+    peak, peak_kind = peaks()
+    roof = transport_roofline(ade_ms, ade_n, n_fluid_int, 6 * 56 + 12 + 2 * 8, N - 2 * ny * nz, peak, peak_kind,
+                              "transport step with the per-voxel networks (reaction + streaming launches)")
+    return {"workload": "surrogate: %dx%dx%d sphere pack, porosity 0.4, 2 organisms x (3->20->20->4), 6 solutes"
+                        % shape, "mlups": N * steps / (ms * 1e-3) / 1e6, "ms_per_step": ms / steps,
+            "roofline": roof}
+
+
+def cpu_surrogate(steps=40, shape=(64, 64, 64)):
+    pkg, wl = load_pkg(), load_workloads()
+    from oracle import oracle as o
+    nx, ny, nz = shape
+    mask = wl.sphere_pack(nx, ny, nz, 0.40, 4.0, 8.0, seed=31)
+    cfg = wl.surrogate_config(pkg, nx, ny, nz)
+    nets = wl.surrogate_nets(pkg)
+    fl = o.Flow(cfg, mask)
+    fl.step(30)
+    _, u = fl.macro()
+    tr = o.Transport(cfg, mask, u=u)
+    tr.set_surrogates(nets)
+    for m in range(2):
+        tr.set_biomass(m, wl.seed_biomass(mask, 32 + m, frac=0.3, lo=0.005, hi=0.05))
+    t0 = time.perf_counter()
+    tr.step(steps)
+    dt = time.perf_counter() - t0
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": mask.size * steps / dt / 1e6, "unit": "MLUPS", "cores": threads, "kind": "port",
+            "sample": "%dx%dx%d of the same workload, %d transport steps" % (nx, ny, nz, steps)}
+
+
+def cpu_biotic_ca(steps=40, shape=(64, 64, 64)):
+    """The FP64 oracle on a 64^3 sample of the biotic + CA workload: transport
+    step and CA block per step."""
+    pkg, wl = load_pkg(), load_workloads()
+    from oracle import oracle as o
+    nx, ny, nz = shape
+    mask = wl.walled_pack(nx, ny, nz, 0.35, 5.0, 10.0, seed=21)
+    cfg = wl.biotic_config(pkg, nx, ny, nz)
+    fl = o.Flow(cfg, mask)
+    fl.step(30)
+    _, u = fl.macro()
+    tr = o.Transport(cfg, mask, u=u)
+    tr.set_biomass(0, wl.seed_biomass(mask, 22))
+    tr.ca_init()
+    tr.ca_update_mask()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        tr.step(1)
+        tr.ca_redistribute()
+    dt = time.perf_counter() - t0
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": mask.size * steps / dt / 1e6, "unit": "MLUPS", "cores": threads, "kind": "port",
+            "sample": "%dx%dx%d of the same workload, %d steps (transport + CA block)" % (nx, ny, nz, steps)}
+
+
+def learned_step_bench(pkg, wl, stream, shape=(256, 128, 128), steps=40, interval=10):
+    """The learned warm start inside the coupled step: the network is trained
+    on the device every `interval` steps on the step's own Newton pairs; then
+    every voxel forgets its previous solution and one more step runs, started
+    from the network, against the same step started cold.  Newton
+    iterations per reactive voxel of that step, the Newton time (the
+    transport step), and the training time."""
+    import torch
+    cfg, mask, bio, mineral = coupled_setup(pkg, wl, shape, seed=15)
+    react = (mask == 2)
+    react[0] = react[-1] = False
+    res = {}
+    for learn in (True, False):
+        lat = pkg.Lattice(cfg, stream=stream)
+        lat.upload_mask(mask)
+        lat.flow_init()
+        lat.flow_steps(100)
+        lat.couple_velocity()
+        lat.ade_init()
+        lat.set_field(pkg.FIELD_BIOMASS, 0, bio)
+        lat.set_field(pkg.FIELD_CONC, 8, mineral)
+        if learn:
+            lat.set_option(pkg.OPT_EQ_LEARN, interval)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            lat.step(1)
+        torch.cuda.synchronize()
+        run_s = time.perf_counter() - t0
+        lat.set_option(pkg.OPT_EQ_FORGET, 1)
+        lat.timing(True)
+        lat.timing_read(pkg.KERNEL_ADE_MAIN)
+        lat.step(1)
+        ms, n = lat.timing_read(pkg.KERNEL_ADE_MAIN)
+        lat.timing(False)
+        it = lat.field(pkg.FIELD_EQ_ITERS).reshape(mask.shape)[react]
+        res["learned" if learn else "cold"] = {"mean_iters": float(it.mean()), "max_iters": int(it.max()),
+                                               "step_ms": ms / max(n, 1), "run_s": run_s}
+        if learn:
+            res["trainings"] = lat.get_option(pkg.OPT_EQ_LEARN_TRAININGS)
+        lat.close()
+    res["workload"] = ("coupled %dx%dx%d, network trained every %d steps over %d steps on 1/16 of the converged "
+                       "voxels' pairs, then one step with every voxel's history cleared" % (shape + (interval, steps)))
+    res["training_overhead_s"] = res["learned"]["run_s"] - res["cold"]["run_s"]
+    return res
+
+
 # ----------------------------------------------------------------- main arm
 def biotic_ca_bench(pkg, wl, stream, steps=20, warmup=3, shape=(128, 128, 128)):
     """The biotic workload with the cellular-automaton biofilm: 128^3 sphere
@@ -426,10 +588,16 @@ def biotic_ca_bench(pkg, wl, stream, steps=20, warmup=3, shape=(128, 128, 128)):
     block_ms = e0.elapsed_time(e1)
     over = int((b > cfg.ca_bmax).sum())
     lat.close()
+    n_fluid_int, _ = fluid_counts(cfg, mask)
+    peak, peak_kind = peaks()
+    # the transport step of this workload alone (steps without the CA block)
+    roof = transport_roofline(ms - ca_ms, steps, n_fluid_int, 4 * 56 + 12 + 8, N - 2 * ny * nz, peak, peak_kind,
+                              "transport step (4 solutes, dual Monod) of the biotic + CA workload")
     return {"workload": "biotic + CA: %dx%dx%d sphere pack, porosity 0.35, radii 5-10, walled duct, sealed pores "
                         "filled; 4 solutes, dual Monod, "
                         "biomass 10-50 on 2%% of wall-adjacent pore voxels, Bmax 100, fraction push" % shape,
             "mlups": N * steps / (ms * 1e-3) / 1e6, "ms_per_step": ms / steps, "ca_ms_per_step": ca_ms / steps,
+            "roofline": roof,
             "ca_block": {"status": st, "voxels_over_bmax": over, "sweeps": sweeps, "mask_changes": changes,
                          "ms": block_ms, "ms_per_sweep": block_ms / max(sweeps, 1), "max_after": bmax}}
 
@@ -468,7 +636,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     pkg, wl = load_pkg(), load_workloads()
     stream = torch.cuda.current_stream().cuda_stream
-    cfg, mask, bio = coupled_setup(pkg, wl, FULL, seed=5 + rank)
+    cfg, mask, bio, mineral = coupled_setup(pkg, wl, FULL, seed=5 + rank)
     n_fluid_int, n_fluid = fluid_counts(cfg, mask)
     N = int(np.prod(FULL))
     lat = pkg.Lattice(cfg, stream=stream)
@@ -478,6 +646,7 @@ def main():
     lat.couple_velocity()
     lat.ade_init()
     lat.set_field(pkg.FIELD_BIOMASS, 0, bio)
+    lat.set_field(pkg.FIELD_CONC, 8, mineral)
     for i in range(args.warmup):
         coupled_step(lat, i)
     torch.cuda.synchronize()
@@ -493,8 +662,12 @@ def main():
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.nvtx.range_push("timed")       # lets a profiler select the timed launches
     e0.record()
+    converted = 0
     for i in range(args.steps):
-        coupled_step(lat, args.warmup + i)
+        # the geometry block of every 200 steps falls on the first timed step
+        # (with fewer than 200 timed steps it is counted more often than the
+        # workload runs it, never less)
+        converted += coupled_step(lat, args.warmup + i, geometry=(i % 200 == 0))
     e1.record()
     torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
@@ -513,7 +686,11 @@ def main():
            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32 populations, f64 speciation", "data": "synthetic (seeded sphere pack)",
            "config": config_block(), "fluid_mlups": n_fluid * world * args.steps / (ms * 1e-3) / 1e6,
-           "gpu_launches": int(launches), "clocks": clk}
+           "gpu_launches": int(launches), "clocks": clk,
+           "geometry": {"blocks_timed": (args.steps + 199) // 200, "voxels_converted": int(converted),
+                        "block": "precipitation seal + dissolution reopen + dynamics switch + velocity re-coupling"},
+           "transport_launch": "one launch per step (compiled chemistry: %s)" % (
+               "coupled carbonate" if lat.get_option(pkg.OPT_COMPILED_CHEM) == pkg.CHEM_COUPLED else "none")}
     # roofline of the dominant work: the transport step, whose reaction and
     # streaming launches run slab-interleaved on two streams and are timed
     # together (one event pair per step on the context's stream)
@@ -521,8 +698,9 @@ def main():
     ade_bytes = n_fluid_int * ADE_BYTES_PER_FLUID_SITE + (N - 2 * FULL[1] * FULL[2])
     if ade_n:
         achieved = ade_bytes / (ade_ms / ade_n * 1e-3) / 1e9
-        tps = traffic_from_profile("ade_step")
-        out["roofline"] = {"kernel": "transport step: ade_react_kernel + ade_stream_kernel", "bound": "hbm",
+        tps = traffic_from_profile("ade_fast")
+        out["roofline"] = {"kernel": "transport step: ade_fast_kernel (gather, FP64 reaction chain, collide, "
+                                     "stream in one launch)", "bound": "hbm",
                            "achieved": achieved, "peak": peak,
                            "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind + " (hbm_gbs)",
                            "algorithmic_bytes_per_launch": ade_bytes, "avg_launch_ms": ade_ms / ade_n,
@@ -535,17 +713,22 @@ def main():
                               "launches": flow_n, "share_of_step": flow_ms / ms if ms else None}
     # end to end through the C ABI with pinned host buffers
     if not args.no_e2e:
-        out["e2e"] = e2e_run(pkg, torch, cfg, mask, bio, args.steps, stream, world)
+        out["e2e"] = e2e_run(pkg, torch, cfg, mask, bio, mineral, args.steps, stream, world)
     lat.close()
     if rank == 0 and world == 1 and not args.no_speciation:
         out["speciation"] = speciation_bench(pkg, wl, stream)
     if rank == 0 and world == 1 and not args.no_biotic:
         out["biotic_ca"] = biotic_ca_bench(pkg, wl, stream)
+        out["surrogate"] = surrogate_bench(pkg, wl, stream)
+        out["learned_step"] = learned_step_bench(pkg, wl, stream)
     if rank == 0 and world == 1 and not args.no_cpu:
         cm, cdt, threads, sample = cpu_coupled(40)
         out["cpu_baseline"] = {"value": cm, "unit": "MLUPS", "cores": threads, "kind": "port", "sample": sample}
         if "speciation" in out:
             out["speciation"]["pcf"]["cpu"] = cpu_pcf()
+        if "biotic_ca" in out:
+            out["biotic_ca"]["cpu_baseline"] = cpu_biotic_ca()
+            out["surrogate"]["cpu_baseline"] = cpu_surrogate()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -553,13 +736,14 @@ def main():
         print(json.dumps(out), flush=True)
 
 
-def e2e_run(pkg, torch, cfg, mask, bio, steps, stream, world):
+def e2e_run(pkg, torch, cfg, mask, bio, mineral, steps, stream, world):
     """The same job through the public C ABI with pinned host buffers: upload
     the geometry and the biomass, initialise, run the steps, read every solute
     field back; the copies are inside the timed region."""
     N = mask.size
     h_mask = torch.from_numpy(np.ascontiguousarray(mask.reshape(-1))).pin_memory().numpy()
     h_bio = torch.from_numpy(np.ascontiguousarray(bio.reshape(-1))).pin_memory().numpy()
+    h_min = torch.from_numpy(np.ascontiguousarray(mineral.reshape(-1))).pin_memory().numpy()
     h_out = torch.empty((cfg.n_solutes, N), dtype=torch.float64).pin_memory().numpy()
     lat = pkg.Lattice(cfg, stream=stream)
     torch.cuda.synchronize()
@@ -569,8 +753,9 @@ def e2e_run(pkg, torch, cfg, mask, bio, steps, stream, world):
     lat.couple_velocity()
     lat.ade_init()
     lat.set_field(pkg.FIELD_BIOMASS, 0, h_bio)
+    lat.set_field(pkg.FIELD_CONC, 8, h_min)
     for i in range(steps):
-        coupled_step(lat, i)
+        coupled_step(lat, i, geometry=(i % 200 == 0))
     for s in range(cfg.n_solutes):
         lat._c(lat.lib.cl_get_field(lat.h, pkg.FIELD_CONC, s, pkg._ptr(h_out[s])), "cl_get_field")
     torch.cuda.synchronize()
@@ -578,7 +763,7 @@ def e2e_run(pkg, torch, cfg, mask, bio, steps, stream, world):
     lat.close()
     import torch.distributed as dist
     dt = max_over_ranks(dt, dist, "cuda")
-    h2d = h_mask.nbytes + h_bio.nbytes
+    h2d = h_mask.nbytes + h_bio.nbytes + h_min.nbytes
     d2h = h_out.nbytes
     return {"value": job_mlups(N, world, steps, dt * 1e3), "unit": "MLUPS", "h2d_bytes_per_step": h2d // steps,
             "d2h_bytes_per_step": d2h // steps,

@@ -218,7 +218,7 @@ def biotic_config(pkg, nx, ny, nz, seed=2, bmax=100.0, thrd_frac=0.01, ca_seed=1
 COUPLED_SOLUTES = ["DOC", "O2", "NO3-", "HCO3-", "Ca2+", "H+", "CO3--", "CaCO3(aq)", "CaCO3(s)"]
 
 
-def coupled_config(pkg, nx, ny, nz, seed=5, warm_previous=True):
+def coupled_config(pkg, nx, ny, nz, seed=5, warm_previous=True, dissolution=False):
     """Flow + 8 mobile solutes + 1 immobile mineral:
       kinetics   dual-Monod oxidation of DOC by O2 and by NO3- (one sessile
                  microbe), Vmax ~ U[1e-5, 1e-4], Ks ~ U[1e-3, 1e-1] per step;
@@ -230,7 +230,13 @@ def coupled_config(pkg, nx, ny, nz, seed=5, warm_previous=True):
                  saturation-index driven: rate 1e-6 (Omega - 1) per step above
                  saturation, Omega = [Ca][CO3] / Ksp, log Ksp = -8.48 (calcite);
                  the inflow is supersaturated (pH 8, Omega ~ 30); a voxel whose
-                 inventory reaches 1.0 becomes solid (node conversion)."""
+                 inventory reaches 1.0 becomes solid (node conversion);
+      dissolution (with dissolution=True) the sealed voxels carry the CaCO3(s)
+                 phase, which acid dissolves at its wetted faces, rate
+                 1e-2 [mineral][H+] per step, releasing Ca2+ and HCO3- and
+                 consuming H+; a voxel whose mineral falls below 1e-3 of a full
+                 voxel reopens (a volume-fraction threshold of ~0; the
+                 reference requires a reopen fraction inside (0, 1))."""
     rng = np.random.default_rng(seed)
     taus = rng.uniform(0.6, 0.9, 8)
     inlet = [2e-3, 2.5e-4, 5e-4, 5e-3, 5e-3, 1e-8, 1e-30, 1e-30]
@@ -261,6 +267,13 @@ def coupled_config(pkg, nx, ny, nz, seed=5, warm_previous=True):
     logk = [0, 0, 0, 0, 0, 0, -10.33, -7.13, 0]
     pkg.set_eq_system(cfg.eq, S, logk, [3, 4, 5], max_iter=100, tol=1e-10, warm_iter=4)
     cfg.eq_warm_previous = 1 if warm_previous else 0
+    if dissolution:
+        cfg.dissol_enabled = 1
+        cfg.reopen_fraction = 1e-3
+        cfg.dissol_surface_only = 1
+        cfg.dissol_apply_at_walls = 1
+        pkg.add_phase(cfg, substrate=8, full_density=cfg.max_precip_rho, is_precipitate=True,
+                      k=1e-2, mass=[5], nu={4: 1.0, 3: 1.0, 5: -1.0})
     return cfg
 
 
