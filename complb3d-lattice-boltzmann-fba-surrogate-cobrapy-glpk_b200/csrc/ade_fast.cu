@@ -291,6 +291,89 @@ ade_fast_kernel(const __grid_constant__ AdeK k, const uint32_t* __restrict__ lis
     if ((threadIdx.x & 31) == 0 && nonconv) atomicAdd(&k.counters[0], nonconv);
 }
 
+// The compiled chain alone (the split design): densities of this step in,
+// each mobile solute's total increment out to dc (by storage index), for the
+// run-time-table streaming launch to add after its collision.
+template <class Chem, int PARITY>
+__global__ void __launch_bounds__(128, 3)
+ade_fast_react_kernel(const __grid_constant__ AdeK k, const uint32_t* __restrict__ list, int64_t r0, int64_t r1,
+                      float* __restrict__ dc) {
+    constexpr int S = Chem::S;
+    const int64_t N = k.g.N;
+    const uint32_t N32 = (uint32_t)N;
+    unsigned long long nonconv = 0;
+    for (int64_t r = r0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < r1; r += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t n = list[r];
+        const uint8_t cls = k.cls[n];
+        if (!(cls & F_REACTIVE)) continue;
+        int x, y, z;
+        decode(k.g, n, x, y, z);
+        SSite st;
+        if (!make_ssite<PARITY>(k.g, k.sidx, x, y, z, n, st)) atomicAdd(&k.counters[1], 1ull);
+        double C[S], A[S];
+#pragma unroll
+        for (int s0 = 0; s0 < S; s0 += kGroup) {
+            float f[kGroup][7];
+#pragma unroll
+            for (int g = 0; g < kGroup; ++g)
+                if (s0 + g < S && Chem::mobile(s0 + g))
+                    gather7<PARITY>(k.pop + (int64_t)Chem::slot(s0 + g) * 7 * N, N32, st, f[g]);
+#pragma unroll
+            for (int g = 0; g < kGroup; ++g) {
+                const int s = s0 + g;
+                if (s >= S) continue;
+                if (Chem::mobile(s)) {
+                    float rr = 0.f;
+#pragma unroll
+                    for (int i = 0; i < 7; ++i) rr += f[g][i];
+                    C[s] = (double)rr;
+                } else {
+                    C[s] = k.imm[(int64_t)s * N + n];
+                }
+                A[s] = 0.0;
+            }
+        }
+        nonconv += fast_chain<Chem>(k, n, st.s, x, y, z, cls, C, A);
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            if (Chem::mobile(s)) dc[(int64_t)Chem::slot(s) * N + st.s] = (float)A[s];
+            else if (A[s] != 0.0) k.imm[(int64_t)s * N + n] += A[s];
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) nonconv += __shfl_down_sync(0xffffffffu, nonconv, o);
+    if ((threadIdx.x & 31) == 0 && nonconv) atomicAdd(&k.counters[0], nonconv);
+}
+
+// the split design: slab j's compiled reactions (s_react), then its
+// streaming (s_stream), slab j+1's reactions overlapping slab j's streaming
+template <class Chem>
+int fast_split(Ctx* c, const AdeK& k) {
+    constexpr int NMOB = Chem::NMOB;
+    const int G = c->slabs;
+    CL_CUDA(cudaEventRecord(c->ev_fork, c->stream));
+    CL_CUDA(cudaStreamWaitEvent(c->s_react, c->ev_fork, 0));
+    CL_CUDA(cudaStreamWaitEvent(c->s_stream, c->ev_fork, 0));
+    for (int j = 0; j < G; ++j) {
+        const int64_t r0 = G > 1 ? c->slab_live[j] : 0, r1 = G > 1 ? c->slab_live[j + 1] : c->n_live;
+        if (r1 > r0) {
+            const int rb = grid_for(r1 - r0, 128, 148 * 3);
+            if (c->ade_parity == 0)
+                ade_fast_react_kernel<Chem, 0><<<rb, 128, 0, c->s_react>>>(k, c->d_live, r0, r1, c->d_dc);
+            else
+                ade_fast_react_kernel<Chem, 1><<<rb, 128, 0, c->s_react>>>(k, c->d_live, r0, r1, c->d_dc);
+            CL_LAUNCH_CHECK("ade_fast_react_kernel");
+            c->launches += 1;
+        }
+        CL_CUDA(cudaEventRecord(c->ev_slab[j], c->s_react));
+        CL_CUDA(cudaStreamWaitEvent(c->s_stream, c->ev_slab[j], 0));
+        int r = launch_stream<NMOB>(c, k, c->s_stream, r0, r1, 1, 148 * 4);
+        if (r) return r;
+    }
+    CL_CUDA(cudaEventRecord(c->ev_join, c->s_stream));
+    CL_CUDA(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
+    return CL_OK;
+}
+
 template <class Chem, int B, int MB>
 int fast_launch(Ctx* c, const AdeK& k, int any_rxn) {
     const int blocks = grid_for(c->n_live, B, 148 * MB * 16);
@@ -318,6 +401,7 @@ int fast_step(Ctx* c) {
             case 2: r = fast_launch<Chem, 128, 2>(c, k, ar); break;
             case 3: r = fast_launch<Chem, 64, 6>(c, k, ar); break;
             case 4: r = fast_launch<Chem, 64, 5>(c, k, ar); break;
+            case 5: r = ar ? fast_split<Chem>(c, k) : fast_launch<Chem, 128, 4>(c, k, ar); break;
             default: r = fast_launch<Chem, 128, 4>(c, k, ar); break;
         }
         if (r) return r;
