@@ -499,9 +499,10 @@ int cl_eq_solve_host(cl_eq_solver* s, const double* totals, const double* cold_s
  * CL_EQ_NOALLOC_MAX_N entries (8 MiB) that every GPU loading the library
  * holds until exit; larger n is rejected with CL_ERR_ARG.  The first call on
  * a device looks up that array's device address, so make it before any
- * stream capture.  All calls share the array: calls that overlap on the GPU
- * race, and it keeps the last call's contents (the counter is cleared on
- * every call). */
+ * stream capture, and do not reset the device (cudaDeviceReset) between
+ * calls: the address belongs to the context such a reset destroys.  All
+ * calls share the array: calls that overlap on the GPU race, and it keeps the
+ * last call's contents (the counter is cleared on every call). */
 #define CL_EQ_NOALLOC_MAX_N       1048576
 #define CL_EQ_NOALLOC_MAX_DEVICES 64
 int cl_eq_solve_noalloc(const cl_eq_system* sys, const double* d_totals, const double* d_cold_species,

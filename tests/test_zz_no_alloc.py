@@ -7,12 +7,16 @@ array inside the library.
 Checked through the C ABI against the existing entry point
 (cl_eq_solve_device) on the same inputs, on two calls in a row, within the
 tolerance the other speciation tests use (1e-8 in log10 free concentration;
-statuses and iteration counts equal).  Collected last so that a run stopping
-at the first failure has already run every other test."""
+statuses and iteration counts equal), and the converged solutions checked
+against the FP64 oracle's relative mass-balance residual (<= 1e-10).
+Collected last so that a run stopping at the first failure has already run
+every other test."""
 import ctypes
 
 import numpy as np
 import pytest
+
+from oracle import oracle as o
 
 pytestmark = pytest.mark.gpu
 
@@ -69,6 +73,8 @@ def test_noalloc_matches_existing_entry_point(gpu_lib, pkg, wl):
         np.testing.assert_array_equal(inn, ir)
         ok = sr <= 1
         np.testing.assert_allclose(xn[ok], xr[ok], rtol=0, atol=1e-8)
+        sample = np.nonzero(ok)[0][::10]
+        assert np.all(o.eq_residual(sys_, T[sample], xn[sample]) <= 1e-10)
 
 
 def test_noalloc_rejects_oversize_batch(gpu_lib, pkg, wl):
