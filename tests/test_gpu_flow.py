@@ -114,6 +114,12 @@ def test_couple_velocity(gpu_lib, pkg, wl):
     lat.couple_velocity()
     for k in range(3):
         np.testing.assert_allclose(lat.field(pkg.FIELD_VELOCITY, k), lat.field(pkg.FIELD_FLOW_U, k), rtol=0, atol=0)
+    # the coupled field against the FP64 oracle's velocity after the same steps
+    fl = o.Flow(cfg, mask)
+    fl.step(51)
+    _, uo = fl.macro()
+    u = np.stack([lat.field(pkg.FIELD_VELOCITY, k).reshape(-1) for k in range(3)])
+    assert np.linalg.norm(u - uo) <= 2e-4 * np.linalg.norm(uo)
     lat.close()
 
 

@@ -59,6 +59,37 @@ def test_carbonate_fixture_gpu(gpu_lib, pkg):
     np.testing.assert_allclose(c, z["out4"], rtol=1e-6)
 
 
+def bf16_dataflow_grads(p, x, y, nc, H=64):
+    """The gradient the tensor-core kernel computes, restated in FP64 with its
+    BF16 roundings at the same points: weights, inputs, both activations and
+    the three back-propagated deltas are MMA operands and so BF16; biases,
+    gelu' and every accumulation stay wide."""
+    from scipy.special import erf
+    gelu = lambda z: 0.5 * z * (1 + erf(z / np.sqrt(2)))
+    gelu_d = lambda z: 0.5 * (1 + erf(z / np.sqrt(2))) + z / np.sqrt(2 * np.pi) * np.exp(-0.5 * z * z)
+    p = p.astype(np.float64)
+    W1 = bf16(p[:H * nc]).reshape(H, nc); b1 = p[H * nc:H * nc + H]
+    o = H * nc + H
+    W2 = bf16(p[o:o + H * H]).reshape(H, H); b2 = p[o + H * H:o + H * H + H]
+    o = o + H * H + H
+    W3 = bf16(p[o:o + nc * H]).reshape(nc, H); b3 = p[o + nc * H:o + nc * H + nc]
+    n = x.shape[0]
+    X = bf16(x)
+    Z1 = X @ W1.T + b1
+    A1 = bf16(gelu(Z1))
+    Z2 = A1 @ W2.T + b2
+    A2 = bf16(gelu(Z2))
+    Y = A2 @ W3.T + b3
+    e = Y - y
+    loss = float((e * e).sum())
+    dY = bf16(2 * e / (n * nc))
+    dZ2 = bf16((dY @ W3) * gelu_d(Z2))
+    dZ1 = bf16((dZ2 @ W2) * gelu_d(Z1))
+    g = np.concatenate([(dZ1.T @ X).ravel(), dZ1.sum(0), (dZ2.T @ A1).ravel(), dZ2.sum(0),
+                        (dY.T @ A2).ravel(), dY.sum(0)])
+    return loss / (n * nc), g
+
+
 def test_mlp_gradients_match_oracle(gpu_lib, pkg, wl):
     sys_, S, logk, cs = system(pkg, wl)
     eq = pkg.EqSolver(sys_)
@@ -79,6 +110,13 @@ def test_mlp_gradients_match_oracle(gpu_lib, pkg, wl):
     assert loss_g == pytest.approx(loss_o, rel=2e-2)
     err = np.linalg.norm(g_g - g_o) / np.linalg.norm(g_o)
     assert err < 3e-2, err
+    # against the kernel's own BF16 dataflow (activations and deltas rounded
+    # where the kernel feeds them to the MMA): only the order of the FP32
+    # accumulations and rare BF16 rounding ties differ
+    loss_b, g_b = bf16_dataflow_grads(p, x.astype(np.float64), y.astype(np.float64), nc)
+    assert loss_g == pytest.approx(loss_b, rel=1e-3)
+    err_b = np.linalg.norm(g_g - g_b) / np.linalg.norm(g_b)
+    assert err_b < 1e-3, err_b
     # forward through the inference kernel
     yp = eq.predict(x)
     _, _, yh = o.mlp_forward_backward(nc, H, nc, pb, bf16(x), y.astype(np.float64), want_grad=False)
