@@ -570,7 +570,7 @@ int cl_set_option(cl_ctx* h, int32_t key, int64_t value) {
             c->chem_on = value != 0;
             return CL_OK;
         case CL_OPT_FAST_VARIANT:
-            if (value < 0 || value > 5) { set_error("cl_set_option: variant 0..5"); return CL_ERR_ARG; }
+            if (value < 0 || value > 6) { set_error("cl_set_option: variant 0..6"); return CL_ERR_ARG; }
             c->fast_variant = (int)value; return CL_OK;
         case CL_OPT_EQ_LEARN: return learn_enable(c, value);
         case CL_OPT_EQ_FORGET: {

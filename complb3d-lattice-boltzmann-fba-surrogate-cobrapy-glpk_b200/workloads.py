@@ -222,15 +222,20 @@ def coupled_config(pkg, nx, ny, nz, seed=5, warm_previous=True, dissolution=Fals
     """Flow + 8 mobile solutes + 1 immobile mineral:
       kinetics   dual-Monod oxidation of DOC by O2 and by NO3- (one sessile
                  microbe), Vmax ~ U[1e-5, 1e-4], Ks ~ U[1e-3, 1e-1] per step;
-      speciation components HCO3-, Ca2+, H+ with CO3-- (logK -10.33) and
-                 CaCO3(aq) (logK -7.13) as secondary species, Newton to a 1e-10
-                 relative residual every step in every pore voxel, started
-                 from the voxel's previous solution (cold start after 4 misses);
+      speciation components CO3--, Ca2+, H+ with HCO3- (= CO3-- + H+, logK
+                 10.33) and CaCO3(aq) (= Ca2+ + CO3--, logK 3.2) as secondary
+                 species, so every component total is positive at pH 8 (the
+                 reference floors totals at 1e-30); Newton to a 1e-10 relative
+                 residual every step in every pore voxel, started from the
+                 voxel's previous solution (cold start after 4 misses);
       precipitation Ca2+ + CO3-- -> CaCO3(s) on wall-adjacent voxels only,
                  saturation-index driven: rate 1e-6 (Omega - 1) per step above
                  saturation, Omega = [Ca][CO3] / Ksp, log Ksp = -8.48 (calcite);
-                 the inflow is supersaturated (pH 8, Omega ~ 30); a voxel whose
-                 inventory reaches 1.0 becomes solid (node conversion);
+                 the pore water and the inflow start at the speciated
+                 composition of pH 8, free Ca 5e-4 and CO3 2e-5 (Omega ~ 3,
+                 precipitating a tenth of the free carbonate per step at a
+                 wall); a voxel whose inventory reaches 1.0 becomes solid (node
+                 conversion);
       dissolution (with dissolution=True) the sealed voxels carry the CaCO3(s)
                  phase, which acid dissolves at its wetted faces, rate
                  1e-2 [mineral][H+] per step, releasing Ca2+ and HCO3- and
@@ -239,8 +244,12 @@ def coupled_config(pkg, nx, ny, nz, seed=5, warm_previous=True, dissolution=Fals
                  reference requires a reopen fraction inside (0, 1))."""
     rng = np.random.default_rng(seed)
     taus = rng.uniform(0.6, 0.9, 8)
-    inlet = [2e-3, 2.5e-4, 5e-4, 5e-3, 5e-3, 1e-8, 1e-30, 1e-30]
-    c0 = [1e-3, 2.5e-4, 1e-4, 5e-3, 5e-3, 1e-8, 1e-30, 1e-30]
+    # speciated carbonate water: free H+, CO3--, Ca2+ and the complexes they form
+    h, co3, ca = 1e-8, 2e-5, 5e-4
+    hco3 = 10.0 ** 10.33 * co3 * h
+    caco3 = 10.0 ** 3.2 * ca * co3
+    inlet = [2e-3, 2.5e-4, 5e-4, hco3, ca, h, co3, caco3]
+    c0 = [1e-3, 2.5e-4, 1e-4, hco3, ca, h, co3, caco3]
     sol = [{"tau": float(taus[s]), "c0": c0[s], "left": "D", "left_value": inlet[s], "right": "N"} for s in range(8)]
     sol.append({"immobile": True, "c0": 0.0})
     cfg = pkg.make_config(nx, ny, nz, tau_ns=0.8, rho_in=1.0005, rho_out=1.0, solutes=sol, microbes=1, dt=1.0)
@@ -261,11 +270,11 @@ def coupled_config(pkg, nx, ny, nz, seed=5, warm_previous=True, dissolution=Fals
     pkg.add_rxn(cfg, k=1e-6, mass=[4, 6], nu={4: -1.0, 6: -1.0, 8: 1.0}, ksp=10.0 ** -8.48)
     cfg.use_equilibrium = 1
     S = np.zeros((9, 3))
-    S[3, 0] = 1; S[4, 1] = 1; S[5, 2] = 1
-    S[6] = [1, 0, -1]
-    S[7] = [1, 1, -1]
-    logk = [0, 0, 0, 0, 0, 0, -10.33, -7.13, 0]
-    pkg.set_eq_system(cfg.eq, S, logk, [3, 4, 5], max_iter=100, tol=1e-10, warm_iter=4)
+    S[6, 0] = 1; S[4, 1] = 1; S[5, 2] = 1
+    S[3] = [1, 0, 1]
+    S[7] = [1, 1, 0]
+    logk = [0, 0, 0, 10.33, 0, 0, 0, 3.2, 0]
+    pkg.set_eq_system(cfg.eq, S, logk, [6, 4, 5], max_iter=100, tol=1e-10, warm_iter=4)
     cfg.eq_warm_previous = 1 if warm_previous else 0
     if dissolution:
         cfg.dissol_enabled = 1

@@ -21,13 +21,14 @@ def rel_l2(a, b):
     return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(b), 1e-300))
 
 
-def _run(pkg, cfg, mask, bio, steps, compiled, flow_steps=60):
+def _run(pkg, cfg, mask, bio, steps, compiled, flow_steps=60, variant=0):
     lat = pkg.Lattice(cfg)
     lat.upload_mask(mask)
     lat.flow_init()
     lat.flow_steps(flow_steps)
     lat.couple_velocity()
     lat.set_option(pkg.OPT_COMPILED_CHEM, 1 if compiled else 0)
+    lat.set_option(pkg.OPT_FAST_VARIANT, variant)
     lat.ade_init()
     lat.set_field(pkg.FIELD_BIOMASS, 0, bio)
     for _ in range(steps):
@@ -42,13 +43,17 @@ def _run(pkg, cfg, mask, bio, steps, compiled, flow_steps=60):
     return out
 
 
+# launch designs of the compiled step: 0 one launch, 5 reaction launch +
+# streaming launch by slabs, 6 one launch with the inputs staged in shared
+# memory by asynchronous copies
+@pytest.mark.parametrize("variant", [0, 5, 6])
 @pytest.mark.parametrize("steps", [1, 2, 25])
-def test_coupled_compiled_matches_table_and_oracle(gpu_lib, pkg, wl, steps):
+def test_coupled_compiled_matches_table_and_oracle(gpu_lib, pkg, wl, steps, variant):
     mask = wl.sphere_pack(34, 16, 16, 0.45, 2.0, 4.0, seed=3)
     nx, ny, nz = mask.shape
-    cfg = wl.coupled_config(pkg, nx, ny, nz)
+    cfg = wl.coupled_config(pkg, nx, ny, nz, dissolution=True)
     bio = wl.seed_biomass(mask, 4, frac=0.3)
-    fast = _run(pkg, cfg, mask, bio, steps, True)
+    fast = _run(pkg, cfg, mask, bio, steps, True, variant=variant)
     table = _run(pkg, cfg, mask, bio, steps, False)
     assert fast["chem"] == pkg.CHEM_COUPLED and table["chem"] == 0
     for s in range(cfg.n_solutes):
@@ -63,14 +68,15 @@ def test_coupled_compiled_matches_table_and_oracle(gpu_lib, pkg, wl, steps):
     assert rel_l2(fast["bio"], tr.biomass(0)) < 1e-5
 
 
-def test_biotic_compiled_matches_table_and_oracle(gpu_lib, pkg, wl):
+@pytest.mark.parametrize("variant", [0, 6])
+def test_biotic_compiled_matches_table_and_oracle(gpu_lib, pkg, wl, variant):
     mask = wl.sphere_pack(30, 16, 16, 0.4, 2.0, 4.0, seed=8)
     nx, ny, nz = mask.shape
     cfg = wl.biotic_config(pkg, nx, ny, nz)
     cfg.ca_enabled = 0
     cfg.dt = 50.0
     bio = wl.seed_biomass(mask, 9, frac=0.3)
-    fast = _run(pkg, cfg, mask, bio, 30, True)
+    fast = _run(pkg, cfg, mask, bio, 30, True, variant=variant)
     table = _run(pkg, cfg, mask, bio, 30, False)
     assert fast["chem"] == pkg.CHEM_BIOTIC4 and table["chem"] == 0
     for s in range(cfg.n_solutes):

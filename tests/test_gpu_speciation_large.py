@@ -5,9 +5,10 @@ and the FP64 oracle (tests/golden/uranium_tableau.npz).
   - from the known answers perturbed by up to half a decade per component:
     every solve converges to the 1e-10 relative residual and reaches the known
     answer to 1e-8 in log10;
-  - from the reference's cold start: where the GPU and the oracle both
-    converge, the same solutions to 1e-8 in log10, and convergence on about
-    as many samples as the oracle (within 4 of 64);
+  - from the reference's cold start: every converged solve at the known
+    answer (1e-8 in log10), at least as many converged as the oracle's Newton
+    (their line searches see different rounding and part ways on the hard
+    samples), and where both converge the same solutions;
   - tableaux this size have no network or PCF entry: those calls are refused.
 """
 import os
@@ -49,11 +50,11 @@ def test_uranium_cold_start_matches_oracle(gpu_lib, pkg):
     xg, itg, stg = eq.solve(d["totals"], d["cold"], start=pkg.EQ_START_COLD)
     xo, ito, sto = o.eq_batch(sys_, d["totals"], d["cold"], start=0)
     okg, oko = stg <= 1, sto <= 1
-    assert abs(int(okg.sum()) - int(oko.sum())) <= 4, (okg.sum(), oko.sum())
+    assert okg.sum() >= oko.sum(), (okg.sum(), oko.sum())
+    assert np.abs(xg[okg] - d["xstar"][okg]).max() <= 1e-8
     both = okg & oko
     assert both.sum() >= 10
     assert np.abs(xg[both] - xo[both]).max() <= 1e-8
-    assert np.abs(xg[okg] - d["xstar"][okg]).max() <= 1e-8
     with pytest.raises(pkg.CLError):
         eq.pcf(d["cold"])
     eq.close()
