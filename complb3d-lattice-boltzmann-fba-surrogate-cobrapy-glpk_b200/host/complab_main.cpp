@@ -1,7 +1,13 @@
 // complab_main.cpp -- host driver: CompLaB.xml in, the reference's time loop
 // (src/complab.cpp:560-1860) over the C ABI, fields out.
 //
-//   complab_b200 [CompLaB.xml] [--steps N] [--eq-solver newton|pcf] [--print-config] [--quiet]
+//   complab_b200 [CompLaB.xml] [--steps N] [--eq-solver newton|pcf] [--rates rates.xml]
+//                [--dump-config FILE] [--print-config] [--quiet]
+//
+// --rates supplies the rate-law blocks (<rate_table>, dissolution <rate_k> ...)
+// that the main file lacks; --dump-config writes the cl_config the transport
+// loop starts from (after the Peclet calibration) as raw bytes to FILE and the
+// geometry as read to FILE.mask, so that a checker can replay the run.
 //
 // --eq-solver pcf runs the reference's live speciation solver (PCF + Anderson)
 // in the transport step; the default is Newton (or the XML's <solver>).
@@ -96,6 +102,15 @@ bool write_fields(cl_ctx* h, const HostRun& run, long iT, std::vector<std::strin
     return (bool)o;
 }
 
+// the configuration as raw cl_config bytes and the geometry as read
+bool dump_config(const std::string& path, const cl_config& c, const std::vector<uint8_t>& mask) {
+    std::ofstream o(path, std::ios::binary), om(path + ".mask", std::ios::binary);
+    o.write(reinterpret_cast<const char*>(&c), (std::streamsize)sizeof c);
+    om.write(reinterpret_cast<const char*>(mask.data()), (std::streamsize)mask.size());
+    if (!o || !om) std::fprintf(stderr, "complab_b200: cannot write %s\n", path.c_str());
+    return (bool)o && (bool)om;
+}
+
 // collideAndStream until the ValueTracer converges (cl_flow_solve); then the
 // velocity statistics the calibration uses
 bool flow_solve(cl_ctx* h, long max_it, double eps, int* iters) {
@@ -140,7 +155,7 @@ bool weighted_pore_mean(cl_ctx* h, const cl_config& c, const HostRun& run, doubl
 }  // namespace
 
 int main(int argc, char** argv) {
-    std::string xml = "CompLaB.xml";
+    std::string xml = "CompLaB.xml", rates, dump;
     long steps_override = -1;
     int eq_solver = -1;
     bool print_config = false, quiet = false;
@@ -149,29 +164,39 @@ int main(int argc, char** argv) {
         if (a == "--print-config") print_config = true;
         else if (a == "--quiet") quiet = true;
         else if (a == "--steps" && i + 1 < argc) steps_override = std::atol(argv[++i]);
+        else if (a == "--rates" && i + 1 < argc) rates = argv[++i];
+        else if (a == "--dump-config" && i + 1 < argc) dump = argv[++i];
         else if (a == "--eq-solver" && i + 1 < argc && (std::strcmp(argv[i + 1], "pcf") == 0 ||
                                                          std::strcmp(argv[i + 1], "newton") == 0))
             eq_solver = std::strcmp(argv[++i], "pcf") == 0 ? CL_EQ_SOLVER_PCF : CL_EQ_SOLVER_NEWTON;
         else if (!a.empty() && a[0] != '-') xml = a;
         else {
-            std::fprintf(stderr, "usage: %s [CompLaB.xml] [--steps N] [--eq-solver newton|pcf] [--print-config] [--quiet]\n",
+            std::fprintf(stderr, "usage: %s [CompLaB.xml] [--steps N] [--eq-solver newton|pcf] [--rates rates.xml] "
+                         "[--dump-config FILE] [--print-config] [--quiet]\n",
                          argv[0]);
             return 2;
         }
     }
     HostRun run;
     std::string err;
-    if (clhost::read_complab_xml(xml, run, err)) { std::fprintf(stderr, "complab_b200: %s\n", err.c_str()); return 1; }
+    if (clhost::read_complab_xml(xml, run, err, rates)) { std::fprintf(stderr, "complab_b200: %s\n", err.c_str()); return 1; }
     if (eq_solver >= 0) run.cfg.eq.solver = eq_solver;
-    if (print_config) { std::printf("%s\n", clhost::run_json(run).c_str()); return 0; }
+    if (print_config && dump.empty()) { std::printf("%s\n", clhost::run_json(run).c_str()); return 0; }
     if (steps_override >= 0) run.ade_max = steps_override;
-    for (const std::string& n : run.notes) if (!quiet) std::fprintf(stderr, "complab_b200: note: %s\n", n.c_str());
+    if (!print_config)
+        for (const std::string& n : run.notes) if (!quiet) std::fprintf(stderr, "complab_b200: note: %s\n", n.c_str());
 
     cl_config& c = run.cfg;
     std::vector<uint8_t> mask;
     if (!read_geometry(run.input_dir + "/" + run.geom_file, c.nx, c.ny, c.nz, mask, err)) {
         std::fprintf(stderr, "complab_b200: %s\n", err.c_str());
         return 1;
+    }
+    // with --print-config, the dump is the configuration as parsed (before
+    // any flow calibration) and needs no GPU
+    if (print_config) {
+        std::printf("%s\n", clhost::run_json(run).c_str());
+        return dump_config(dump, c, mask) ? 0 : 1;
     }
     const auto t0 = std::chrono::steady_clock::now();
     int st = 0;
@@ -202,6 +227,8 @@ int main(int argc, char** argv) {
         if (std::fabs(dP_new - run.delta_P) / run.delta_P > 0.01) {
             run.delta_P = dP_new;
             if (!check(cl_set_flow_pressure(h, 1.0, 1.0 - 3.0 * dP_new), "cl_set_flow_pressure")) return 1;
+            c.rho_in = 1.0;
+            c.rho_out = 1.0 - 3.0 * dP_new;
             if (!check(cl_flow_init(h), "cl_flow_init")) return 1;
             if (!flow_solve(h, run.ns_max1, run.ns_conv1, &ns_iters)) return 1;
             if (!check(cl_flow_velocity_stats(h, &pore_mean_u, &max_ux, &outlet_ux), "cl_flow_velocity_stats")) return 1;
@@ -246,6 +273,7 @@ int main(int argc, char** argv) {
     }
     if (run.Pe > kThrd && !check(cl_couple_velocity(h), "cl_couple_velocity")) return 1;
     if (!check(cl_ade_init(h), "cl_ade_init")) return 1;
+    if (!dump.empty() && !dump_config(dump, c, mask)) return 1;
     // sessile biomass on the microbes' materials (initializeScalarLattice3D)
     {
         const size_t N = mask.size();

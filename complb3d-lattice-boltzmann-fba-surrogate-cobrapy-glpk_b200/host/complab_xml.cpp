@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <sstream>
 
 #include "xml_lite.h"
@@ -54,10 +55,14 @@ int bc_type(const XmlNode& n) {
 
 }  // namespace
 
-int read_complab_xml(const std::string& path, HostRun& run, std::string& err) {
+int read_complab_xml(const std::string& path, HostRun& run, std::string& err, const std::string& rates) {
     try {
         XmlDoc doc(path);
         const XmlNode& P = doc["parameters"];
+        // the rate-law blocks the main file lacks come from the rates file
+        std::unique_ptr<XmlDoc> rdoc;
+        if (!rates.empty()) rdoc = std::make_unique<XmlDoc>(rates);
+        const XmlNode* RP = rdoc ? &(*rdoc)["parameters"] : nullptr;
         cl_config& c = run.cfg;
         std::memset(&c, 0, sizeof c);
         const size_t slash = path.find_last_of('/');
@@ -204,7 +209,16 @@ int read_complab_xml(const std::string& path, HostRun& run, std::string& err) {
 
         // rate laws: the table that stands for defineKinetics.hh /
         // defineAbioticKinetics.hh
-        if (const XmlNode* rt = opt(P, {"rate_table"})) {
+        const XmlNode* rtab = opt(P, {"rate_table"});
+        if (!rtab && RP) rtab = opt(*RP, {"rate_table"});
+        if (const XmlNode* rt = rtab) {
+            // <decay>m:kd ...</decay>: first-order decay that the compiled rate law
+            // applies itself, in place of the microbe's <decay_coefficient>
+            if (const XmlNode* dk = rt->find("decay"))
+                for (auto& pv : pairs(*dk)) {
+                    if (pv.first < 0 || pv.first >= M) throw std::runtime_error("decay microbe index out of range in " + dk->path);
+                    c.decay[pv.first] = pv.second;
+                }
             for (int k = 0; k < CL_MAX_RXN; ++k) {
                 const XmlNode* r = rt->find("reaction" + std::to_string(k));
                 if (!r) break;
@@ -308,11 +322,15 @@ int read_complab_xml(const std::string& path, HostRun& run, std::string& err) {
                 q.full_density = num_or(*ph, {"full_density"}, 0.0);
                 q.initial_fill = num_or(*ph, {"initial_fill"}, 0.0);
                 q.is_precipitate = ph->has("is_precipitate") && (*ph)["is_precipitate"].flag() ? 1 : 0;
-                q.k = num_or(*ph, {"rate_k"}, 0.0);
-                if (ph->has("rate_mass"))
-                    for (double v : (*ph)["rate_mass"].nums()) if (q.n_mass < 2) q.mass_s[q.n_mass++] = (int32_t)v;
-                if (ph->has("rate_nu"))
-                    for (auto& pv : pairs((*ph)["rate_nu"])) if (pv.first >= 0 && pv.first < S) q.nu[pv.first] = pv.second;
+                const XmlNode* rsrc = ph;
+                if (!ph->has("rate_k") && RP)
+                    if (const XmlNode* rd = RP->find("dissolution"))
+                        if (const XmlNode* rp = rd->find("phase" + std::to_string(k))) rsrc = rp;
+                q.k = num_or(*rsrc, {"rate_k"}, 0.0);
+                if (rsrc->has("rate_mass"))
+                    for (double v : (*rsrc)["rate_mass"].nums()) if (q.n_mass < 2) q.mass_s[q.n_mass++] = (int32_t)v;
+                if (rsrc->has("rate_nu"))
+                    for (auto& pv : pairs((*rsrc)["rate_nu"])) if (pv.first >= 0 && pv.first < S) q.nu[pv.first] = pv.second;
                 if (q.is_precipitate) c.precip_phase_id = q.id;
                 ++c.n_phases;
             }
@@ -377,7 +395,10 @@ std::string run_json(const HostRun& r) {
       << ", \"charcs_length\": " << r.charcs_length << ", \"rho_out\": " << c.rho_out
       << ", \"ns_max_iT1\": " << r.ns_max1 << ", \"ns_converge_iT1\": " << r.ns_conv1
       << ", \"ade_max_iT\": " << r.ade_max << ", \"ns_update_interval\": " << r.ns_update_interval
-      << ", \"ade_update_interval\": " << r.ade_update_interval << ", \"n_solutes\": " << c.n_solutes << ", \"names\": [";
+      << ", \"ade_update_interval\": " << r.ade_update_interval << ", \"ns_max_iT2\": " << r.ns_max2
+      << ", \"ns_converge_iT2\": " << r.ns_conv2 << ", \"precip_interval\": " << r.precip_interval
+      << ", \"dissol_interval\": " << r.dissol_interval << ", \"vtk_interval\": " << r.vtk_interval
+      << ", \"n_solutes\": " << c.n_solutes << ", \"names\": [";
     for (size_t i = 0; i < r.subs_names.size(); ++i) o << (i ? ", " : "") << "\"" << r.subs_names[i] << "\"";
     o << "], \"c0\": ";
     arr(c.c0, c.n_solutes);
@@ -410,7 +431,22 @@ std::string run_json(const HostRun& r) {
       << ", \"ca_bmax\": " << c.ca_bmax << ", \"ca_thrd_frac\": " << c.ca_thrd_frac
       << ", \"ca_seed\": " << c.ca_seed << ", \"microbe_code\": ";
     iarr(c.microbe_code, c.n_microbes);
-    o << ", \"notes\": [";
+    // per microbe: its biofilm materials and the initial density on each
+    o << ", \"bio_materials\": [";
+    for (size_t m = 0; m < r.bio_materials.size(); ++m) {
+        o << (m ? ", " : "") << "[";
+        for (size_t k = 0; k < r.bio_materials[m].size(); ++k) o << (k ? ", " : "") << r.bio_materials[m][k];
+        o << "]";
+    }
+    o << "], \"microbe_names\": [";
+    for (size_t m = 0; m < r.microbe_names.size(); ++m) o << (m ? ", " : "") << "\"" << r.microbe_names[m] << "\"";
+    o << "], \"b0\": [";
+    for (size_t m = 0; m < r.b0.size(); ++m) {
+        o << (m ? ", " : "") << "[";
+        for (size_t k = 0; k < r.b0[m].size(); ++k) o << (k ? ", " : "") << r.b0[m][k];
+        o << "]";
+    }
+    o << "], \"notes\": [";
     for (size_t i = 0; i < r.notes.size(); ++i) o << (i ? ", " : "") << "\"" << r.notes[i] << "\"";
     o << "]}";
     return o.str();

@@ -8,7 +8,10 @@
 // reading XML: <rate_table> stands for defineKinetics.hh /
 // defineAbioticKinetics.hh (the table form of cl_rxn), and <rate_k>,
 // <rate_mass>, <rate_nu> inside a dissolution <phaseN> stand for
-// defineDissolutionRate.
+// defineDissolutionRate.  Because the reference keeps those laws in compiled
+// headers, its own example inputs carry none of them: a second file given as
+// `rates` (root <parameters>, holding <rate_table> and/or
+// <dissolution><phaseN><rate_k>...) supplies the blocks the main file lacks.
 #pragma once
 #include <string>
 #include <vector>
@@ -38,7 +41,7 @@ struct HostRun {
 };
 
 // Returns 0 on success; on failure -1 with a message in err.
-int read_complab_xml(const std::string& path, HostRun& run, std::string& err);
+int read_complab_xml(const std::string& path, HostRun& run, std::string& err, const std::string& rates = "");
 
 // The parsed run as JSON (used by --print-config and the tests).
 std::string run_json(const HostRun& run);

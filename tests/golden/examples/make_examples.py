@@ -1,0 +1,44 @@
+"""Copy the reference's example inputs that the host driver runs into this
+folder, so that the GPU tests can run them where the reference tree is absent.
+
+    python tests/golden/examples/make_examples.py [REFERENCE_ROOT]
+
+For each supported example (examples/<name>/ of the reference: CompLaB.xml and
+input/*) the files are copied unchanged into tests/golden/examples/<name>/.
+The reference keeps each example's rate law in a compiled header
+(examples/<name>/defineKinetics.hh, defineAbioticKinetics.hh); the table form
+of those laws, which the driver reads with --rates, is the hand-written
+rates.xml beside each copy (not produced by this script).  The header and the
+table are compared on random inputs by
+tests/test_oracle_pins.py::test_oracle_rates_match_example_headers and
+tests/test_ratelaw_port.py.
+"""
+import os
+import shutil
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(HERE))))
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(HERE)), "tests"))
+
+SUPPORTED = ["01_flow_only", "02_diffusion_only", "03_abiotic_kinetics", "04_equilibrium",
+             "05_biotic_cellular_automaton", "13_precipitation", "14_dissolution", "15_precip_and_dissolution"]
+
+
+def main():
+    from conftest import reference_root
+    root = sys.argv[1] if len(sys.argv) > 1 else reference_root()
+    if not root:
+        raise SystemExit("no reference tree: pass its path or set COMPLAB_REFERENCE")
+    for name in SUPPORTED:
+        src = os.path.join(root, "examples", name)
+        dst = os.path.join(HERE, name)
+        os.makedirs(os.path.join(dst, "input"), exist_ok=True)
+        shutil.copyfile(os.path.join(src, "CompLaB.xml"), os.path.join(dst, "CompLaB.xml"))
+        for f in sorted(os.listdir(os.path.join(src, "input"))):
+            shutil.copyfile(os.path.join(src, "input", f), os.path.join(dst, "input", f))
+        print("copied", name)
+
+
+if __name__ == "__main__":
+    main()

@@ -244,6 +244,10 @@ MOBILE_BIOMASS = ["06_biotic_finite_difference", "07_biotic_lattice_boltzmann", 
 
 
 def _example_xml(name):
+    # the supported examples travel as fixtures (tests/golden/examples)
+    fx = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "examples", name)
+    if os.path.isdir(fx):
+        return fx, "CompLaB.xml"
     ex = _ref_examples()
     d = os.path.join(ex, name) if ex else ""
     if not ex or not os.path.isdir(d):
@@ -283,3 +287,40 @@ def test_reference_examples_with_mobile_biomass_are_refused(name):
     d, xml = _example_xml(name)
     r = subprocess.run([DRIVER, xml, "--print-config"], cwd=d, capture_output=True, text=True)
     assert r.returncode == 1 and "mobile biomass" in r.stderr
+
+
+@pytest.mark.skipif(not driver_available(), reason="host driver not built")
+@pytest.mark.parametrize("name", SUPPORTED)
+def test_example_rate_tables_and_config_dump(name, tmp_path):
+    """Each example fixture with its rates.xml (the table form of the rate law
+    the reference compiles in): the driver loads the table, and --dump-config
+    writes the parsed cl_config, byte for byte the size of the ABI struct,
+    with the geometry beside it (no GPU needed in --print-config mode)."""
+    import numpy as np
+    from conftest import load_pkg
+    pkg = load_pkg()
+    d, xml = _example_xml(name)
+    args = [DRIVER, xml, "--print-config", "--dump-config", str(tmp_path / "c.bin")]
+    if os.path.exists(os.path.join(d, "rates.xml")):
+        args[2:2] = ["--rates", "rates.xml"]
+    r = subprocess.run(args, cwd=d, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    c = json.loads(r.stdout)
+    raw = open(tmp_path / "c.bin", "rb").read()
+    assert len(raw) == ctypes_sizeof(pkg.Config)
+    cfg = pkg.Config.from_buffer_copy(raw)
+    assert (cfg.nx, cfg.ny, cfg.nz) == (c["nx"], c["ny"], c["nz"])
+    mask = np.fromfile(tmp_path / "c.bin.mask", np.uint8)
+    assert mask.size == cfg.nx * cfg.ny * cfg.nz
+    want_rxn = {"03_abiotic_kinetics": 1, "05_biotic_cellular_automaton": 1, "13_precipitation": 1,
+                "15_precip_and_dissolution": 1}.get(name, 0)
+    assert cfg.n_rxn == want_rxn
+    if name == "05_biotic_cellular_automaton":
+        assert cfg.decay[0] == 1e-6 and cfg.rxn[0].monod_ks[0] == 5e-2 and cfg.rxn[0].nu[0] == -2.5
+    if name in ("14_dissolution", "15_precip_and_dissolution"):
+        assert cfg.n_phases == 1 and cfg.phases[0].k > 0 and cfg.phases[0].n_mass == 1
+
+
+def ctypes_sizeof(t):
+    import ctypes
+    return ctypes.sizeof(t)
