@@ -166,22 +166,34 @@ __device__ __forceinline__ int fast_chain(const AdeK& k, int64_t n, uint32_t sto
                 for (int j = 0; j < NC; ++j) x[j] = xprev[j];
             }
         }
-        // no previous solution of its own: the network's guess, once trained
+        // the reference's cold start: log10 of each component's own species
+        auto cold = [&](double* xs) {
+#pragma unroll
+            for (int j = 0; j < NC; ++j) {
+                const int idx = e.comp_species[j];
+                double c = 1e-7;
+#pragma unroll
+                for (int s = 0; s < S; ++s) if (s == idx) c = C[s];
+                xs[j] = log10(fmin(fmax(c, 1e-30), 10.0));
+            }
+        };
+        // no previous solution of its own: the network's guess, once trained,
+        // where it is closer to equilibrium than the cold start by the relative
+        // mass-balance residual (the cold start reads the voxel's own species,
+        // which transport keeps near equilibrium)
         if (!warm && k.learn_w) {
-            learn_start<NC>(k.learn_w, k.learn_norm, T, x);
-            warm = true;
+            LearnVec<NC> tv;
+#pragma unroll
+            for (int j = 0; j < NC; ++j) tv.v[j] = T[j];
+            const LearnVec<NC> xv = learn_start<NC>(k.learn_w, k.learn_norm, tv);
+#pragma unroll
+            for (int j = 0; j < NC; ++j) x[j] = xv.v[j];
+            double xc[NC], F[NC];
+            cold(xc);
+            warm = eq_residual<NC, S>(e, T, x, F) < eq_residual<NC, S>(e, T, xc, F);
         }
         for (int phase = warm ? 0 : 1; phase < 2; ++phase) {
-            if (phase == 1) {
-#pragma unroll
-                for (int j = 0; j < NC; ++j) {
-                    const int idx = e.comp_species[j];
-                    double c = 1e-7;
-#pragma unroll
-                    for (int s = 0; s < S; ++s) if (s == idx) c = C[s];
-                    x[j] = log10(fmin(fmax(c, 1e-30), 10.0));
-                }
-            }
+            if (phase == 1) cold(x);
             it += eq_newton<NC, S>(e, T, x, phase == 0 ? p.eq.warm_iter : p.eq.max_iter, p.eq.tol, &conv, nullptr,
                                    R, 1);
             if (conv) break;

@@ -8,8 +8,9 @@
 // tensor-core forward/backward with FP32 master weights) on the ring, and
 // from then on a voxel with no previous solution of its own (the first step,
 // a reopened or newly stored voxel, after a reset) starts Newton from the
-// network's guess, falling back to the reference's cold start after warm_iter
-// iterations.  Newton's 1e-10 relative residual still decides convergence,
+// network's guess where that guess has a smaller relative mass-balance
+// residual than the reference's cold start, falling back to the cold start
+// after warm_iter iterations.  Newton's 1e-10 relative residual still decides convergence,
 // so the fields do not depend on the guess beyond that tolerance.
 #pragma once
 #include <cmath>
@@ -24,9 +25,19 @@ __device__ __forceinline__ float learn_gelu(float z) { return 0.5f * z * (1.f + 
 // (layout W1[H][NC] b1[H] W2[H][H] b2[H] W3[NC][H] b3[NC]) and the
 // standardisation norm = mu_in[NC] sd_in[NC] mu_out[NC] sd_out[NC] of the
 // trainer (inputs log10 T, outputs x - log10 T)
+// values in and out by value: a call with pointers would put the caller's
+// arrays on the stack for the whole reaction chain
 template <int NC>
-__device__ __noinline__ void learn_start(const float* __restrict__ w, const float* __restrict__ norm, const double* T,
-                                         double* x) {
+struct LearnVec {
+    double v[NC];
+};
+
+template <int NC>
+__device__ __noinline__ LearnVec<NC> learn_start(const float* __restrict__ w, const float* __restrict__ norm,
+                                                 const LearnVec<NC> Tv) {
+    const double* T = Tv.v;
+    LearnVec<NC> out;
+    double* x = out.v;
     constexpr int H = kLearnHidden;
     const float* W1 = w;
     const float* b1 = W1 + H * NC;
@@ -62,6 +73,7 @@ __device__ __noinline__ void learn_start(const float* __restrict__ w, const floa
         const double v = (double)u[k] + (double)__ldg(norm + 2 * NC + k) + (double)__ldg(norm + 3 * NC + k) * (double)y[k];
         x[k] = fmin(fmax(v, -30.0), 1.0);
     }
+    return out;
 }
 
 // the pair of a converged voxel goes to the ring when its site hash falls in

@@ -913,7 +913,8 @@ int cl_eq_solve_host(cl_eq_solver* s, const double* totals, const double* cold_s
     if (e == cudaSuccess && start == CL_EQ_START_GIVEN) e = cudaMemcpyAsync(dX, logfree, sizeof(double) * n * nc, cudaMemcpyHostToDevice, s->stream);
     if (e != cudaSuccess) r = cuda_fail(e, "cl_eq_solve_host");
     if (!r) r = cl_eq_solve_device(s, dT, dC, dX, dI, dS, n, start);
-    if (!r) {
+    // CL_WARN_NOT_CONVERGED still returns every entry's solution and status
+    if (r >= 0) {
         e = cudaMemcpyAsync(logfree, dX, sizeof(double) * n * nc, cudaMemcpyDeviceToHost, s->stream);
         if (e == cudaSuccess && iters) e = cudaMemcpyAsync(iters, dI, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s->stream);
         if (e == cudaSuccess && status) e = cudaMemcpyAsync(status, dS, n, cudaMemcpyDeviceToHost, s->stream);

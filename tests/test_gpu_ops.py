@@ -74,7 +74,15 @@ def test_each_operator_against_oracle(gpu_lib, pkg, wl):
 
     def same(what):
         for s in range(cfg.n_solutes):
-            assert rel_l2(lat.field(pkg.FIELD_CONC, s).reshape(-1), tr.density(s)) < 1e-4, (what, s)
+            g, r = lat.field(pkg.FIELD_CONC, s).reshape(-1), tr.density(s)
+            e = rel_l2(g, r)
+            if not e < 1e-4:
+                # where the fields part: the x planes of the largest differences
+                d = np.abs(g - r).reshape(mask.shape)
+                worst = np.argsort(d.reshape(-1))[::-1][:8]
+                where = [tuple(int(v) for v in np.unravel_index(w, mask.shape)) for w in worst]
+                pytest.fail("%s: solute %d rel. L2 %.3g; largest at %s (gpu %s, oracle %s)" % (
+                    what, s, e, where, g[worst].tolist(), r[worst].tolist()))
         assert rel_l2(lat.field(pkg.FIELD_BIOMASS, 0).reshape(-1), tr.biomass(0)) < 1e-5, what
 
     for _ in range(3):
