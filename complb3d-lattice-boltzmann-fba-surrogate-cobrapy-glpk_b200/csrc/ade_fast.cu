@@ -134,15 +134,19 @@ __device__ __forceinline__ int fast_chain(const AdeK& k, int64_t n, uint32_t sto
     if constexpr (NC > 0) {
         if (!p.do_eq) return 0;
         const EqDev& e = k.e;
+        const typename Chem::Tab tb{e};
         double x[NC], T[NC];
 #pragma unroll
         for (int j = 0; j < NC; ++j) T[j] = 0.0;
 #pragma unroll
         for (int i = 0; i < S; ++i) {
-            if (!e.active[i]) continue;
+            if (!tb.active(i)) continue;
             const double c = fmin(fmax(C[i], 1e-30), 10.0);
 #pragma unroll
-            for (int j = 0; j < NC; ++j) T[j] = fma(e.stoich[i][j], c, T[j]);
+            for (int j = 0; j < NC; ++j) {
+                if constexpr (Chem::Tab::kFixed) { if (tb.ipow(i, j) == 0) continue; }
+                T[j] = fma(tb.s(i, j), c, T[j]);
+            }
         }
 #pragma unroll
         for (int j = 0; j < NC; ++j) T[j] = fmax(T[j], 1e-30);
@@ -190,12 +194,11 @@ __device__ __forceinline__ int fast_chain(const AdeK& k, int64_t n, uint32_t sto
             for (int j = 0; j < NC; ++j) x[j] = xv.v[j];
             double xc[NC], F[NC];
             cold(xc);
-            warm = eq_residual<NC, S>(e, T, x, F) < eq_residual<NC, S>(e, T, xc, F);
+            warm = eq_residual_t<NC, S>(tb, T, x, F) < eq_residual_t<NC, S>(tb, T, xc, F);
         }
         for (int phase = warm ? 0 : 1; phase < 2; ++phase) {
             if (phase == 1) cold(x);
-            it += eq_newton<NC, S>(e, T, x, phase == 0 ? p.eq.warm_iter : p.eq.max_iter, p.eq.tol, &conv, nullptr,
-                                   R, 1);
+            it += eq_newton_t<NC, S>(tb, T, x, phase == 0 ? p.eq.warm_iter : p.eq.max_iter, p.eq.tol, &conv, R, 1);
             if (conv) break;
         }
         if (k.eq_x && conv) {
@@ -210,7 +213,7 @@ __device__ __forceinline__ int fast_chain(const AdeK& k, int64_t n, uint32_t sto
 #pragma unroll
             for (int s = 0; s < S; ++s) {
                 const double conc = fmax(C[s], 1e-30);
-                double eqc = !e.active[s] ? fmin(conc, 10.0) : (NC <= 3 ? R[s] : species_c<NC>(e, s, x));
+                double eqc = !tb.active(s) ? fmin(conc, 10.0) : (NC <= 3 ? R[s] : species_c<NC>(e, s, x));
                 eqc = fmin(fmax(eqc, 1e-30), 10.0);
                 double d = eqc - conc;
                 const double mx = fmax(1e-9, 0.1 * fabs(conc));

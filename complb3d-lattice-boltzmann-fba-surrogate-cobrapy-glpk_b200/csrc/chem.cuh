@@ -8,8 +8,10 @@
 // chemistry is a type that fixes, at compile time, how many solutes and
 // microbes there are, which solutes are mobile, how many equilibrium
 // components the tableau has, and the structure of its rate laws.  The
-// values (rate constants, half-saturations, stoichiometry, logK, relaxation,
-// boundary values) stay run-time inputs in cl_config.
+// values (rate constants, half-saturations, logK, relaxation, boundary
+// values) stay run-time inputs in cl_config; a chemistry may also fix its
+// tableau's stoichiometry (Tab = TabFixed<...>), which the configuration must
+// then hold exactly, so that its Newton solve folds every zero coefficient.
 //
 // With every size known, the transport step keeps a voxel's whole state in
 // registers and unrolls every loop over solutes, species and reactions (the
@@ -23,11 +25,14 @@
 //   kinetics(p, C, B, R, BR, mask)  rates per second (defineRxnKinetics); B floored
 //                                   at thrd, C as stored
 //   abiotic(p, C, R, mask)          rates per second (defineAbioticRxnKinetics)
+//   Tab                             the tableau the Newton solve reads: TabRun
+//                                   (cl_config's) or TabFixed (compiled in)
 // Rates follow the run-time table's arithmetic (rates_dev) term for term, so
 // a configuration runs to the same numbers on either launch.
 #pragma once
 #include <cmath>
 #include "internal.h"
+#include "newton.cuh"
 #include "../../include/complab_ratelaw.hpp"
 
 namespace cl {
@@ -85,18 +90,32 @@ inline bool rxn_is(const cl_rxn& r, int microbe, std::initializer_list<int> mono
 //   reaction 0  microbe 0: k B  DOC/(Ks+DOC)  O2/(Ks+O2)      (aerobic oxidation)
 //   reaction 1  microbe 0: k B  DOC/(Ks+DOC)  NO3/(Ks+NO3)    (denitrification)
 //   reaction 2  abiotic:   k [Ca2+][CO3--], or k (Omega - 1)+ with a Ksp (precipitation)
-// Equilibrium: 3 components (HCO3-, Ca2+, H+) over the 9 solutes as species.
+// Equilibrium: 3 components, CO3-- (species 6), Ca2+ (4) and H+ (5), with
+// HCO3- (3) = CO3-- + H+ and CaCO3(aq) (7) = CO3-- + Ca2+ (stoichiometry
+// compiled in, logK from the run).
 struct ChemCoupled {
     static constexpr int kId = 1;
     static constexpr const char* kName = "coupled carbonate (8 mobile + 1 mineral, dual Monod, 3 components)";
     static constexpr int S = 9, NMOB = 8, M = 1, NC = 3, MW = 1;
     __host__ __device__ static constexpr bool mobile(int s) { return s < 8; }
     __host__ __device__ static constexpr int slot(int s) { return s; }
+    struct Fix {
+        static constexpr int ns = S, nc = NC;
+        __host__ __device__ static constexpr int coef(int i, int j) {
+            return i == 6 ? (j == 0) : i == 4 ? (j == 1) : i == 5 ? (j == 2)
+                 : i == 3 ? (j == 0 || j == 2) : i == 7 ? (j == 0 || j == 1) : 0;
+        }
+        __host__ __device__ static constexpr int comp_species(int j) { return j == 0 ? 6 : j == 1 ? 4 : 5; }
+    };
+    using Tab = TabFixed<Fix>;
     static bool matches(const cl_config& c) {
         if (c.n_solutes != S || c.n_microbes != M || c.n_rxn != 3 || c.n_srg != 0) return false;
         for (int s = 0; s < S; ++s) if ((c.immobile[s] != 0) == mobile(s)) return false;
         if (!c.use_equilibrium || c.eq.n_comp != NC || c.eq.n_species != S || c.eq.solver != CL_EQ_SOLVER_NEWTON)
             return false;
+        for (int i = 0; i < S; ++i)
+            for (int j = 0; j < NC; ++j) if (c.eq.stoich[i][j] != (double)Fix::coef(i, j)) return false;
+        for (int j = 0; j < NC; ++j) if (c.eq.comp_species[j] != Fix::comp_species(j)) return false;
         return c.rate_law == CL_RATELAW_TABLE && rxn_is(c.rxn[0], 0, {0, 1}, {}) && rxn_is(c.rxn[1], 0, {0, 2}, {}) &&
                rxn_is(c.rxn[2], -1, {}, {4, 6});
     }
@@ -152,6 +171,7 @@ struct ChemBiotic4 {
     static constexpr int kId = 2;
     static constexpr const char* kName = "biotic dual Monod (4 mobile solutes, 1 microbe)";
     static constexpr int S = 4, NMOB = 4, M = 1, NC = 0, MW = 1;
+    using Tab = TabRun;
     __host__ __device__ static constexpr bool mobile(int) { return true; }
     __host__ __device__ static constexpr int slot(int s) { return s; }
     static bool matches(const cl_config& c) {
@@ -201,6 +221,7 @@ struct ChemZhao24 {
     static constexpr int kId = 3;
     static constexpr const char* kName = "Zhao uranium network (24 substrates, 12 biomass pools)";
     static constexpr int S = 24, NMOB = 15, M = 12, NC = 0, MW = 12;
+    using Tab = TabRun;
     __host__ __device__ static constexpr bool mobile(int s) {
         return !(s == 2 || s == 4 || s == 5 || s == 6 || s == 9 || s == 13 || s == 21 || s == 22 || s == 23);
     }

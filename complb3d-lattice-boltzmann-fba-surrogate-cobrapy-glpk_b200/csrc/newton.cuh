@@ -83,6 +83,50 @@ inline void eqdev_from_system(const cl_eq_system& s, EqDev& d) {
     d.depth = s.anderson_depth > 0 ? s.anderson_depth : 4;
 }
 
+// The tableau a solve reads.  TabRun: the run-time tableau (EqDev).
+// TabFixed<Fix>: an integer stoichiometry fixed at compile time
+// (Fix::ns, Fix::coef(i, j), with the equilibrium constants still from the
+// run), so that after the species and component loops unroll every zero
+// coefficient, every unit power and every inactive species folds away.
+struct TabRun {
+    static constexpr bool kFixed = false;
+    const EqDev& e;
+    __device__ __forceinline__ int ns() const { return e.ns; }
+    __device__ __forceinline__ bool active(int i) const { return e.active[i] != 0; }
+    __device__ __forceinline__ double s(int i, int j) const { return e.stoich[i][j]; }
+    __device__ __forceinline__ double abs_s(int i, int j) const { return e.absS[i][j]; }
+    __device__ __forceinline__ int ipow(int i, int j) const { return e.ipow[i][j]; }
+    __device__ __forceinline__ bool all_int() const { return e.all_int != 0; }
+    __device__ __forceinline__ bool neg(int j) const { return e.neg[j] != 0; }
+    __device__ __forceinline__ double logk(int i) const { return e.logk[i]; }
+    __device__ __forceinline__ double k10(int i) const { return e.k10[i]; }
+};
+
+template <class Fix>
+struct TabFixed {
+    static constexpr bool kFixed = true;
+    const EqDev& e;
+    __device__ __forceinline__ static constexpr int ns() { return Fix::ns; }
+    __device__ __forceinline__ static constexpr bool active(int i) {
+        bool a = false;
+        for (int j = 0; j < Fix::nc; ++j) a = a || Fix::coef(i, j) != 0;
+        return a;
+    }
+    __device__ __forceinline__ static constexpr double s(int i, int j) { return (double)Fix::coef(i, j); }
+    __device__ __forceinline__ static constexpr double abs_s(int i, int j) {
+        return (double)(Fix::coef(i, j) < 0 ? -Fix::coef(i, j) : Fix::coef(i, j));
+    }
+    __device__ __forceinline__ static constexpr int ipow(int i, int j) { return Fix::coef(i, j); }
+    __device__ __forceinline__ static constexpr bool all_int() { return true; }
+    __device__ __forceinline__ static constexpr bool neg(int j) {
+        bool n = false;
+        for (int i = 0; i < Fix::ns; ++i) n = n || Fix::coef(i, j) < 0;
+        return n;
+    }
+    __device__ __forceinline__ double logk(int i) const { return e.logk[i]; }
+    __device__ __forceinline__ double k10(int i) const { return e.k10[i]; }
+};
+
 // species concentration from the component logs, clamped as calc_species
 template <int NC>
 __device__ __forceinline__ double species_c(const EqDev& e, int i, const double* x) {
@@ -101,26 +145,31 @@ template <int NC>
 struct Powers {
     double a[NC], ai[NC];
     // inverses only of the components some species divides by
-    __device__ __forceinline__ void set(const EqDev& e, const double* x) {
+    template <class Tab>
+    __device__ __forceinline__ void set(const Tab& t, const double* x) {
 #pragma unroll
-        for (int j = 0; j < NC; ++j) { a[j] = exp10(x[j]); ai[j] = e.neg[j] ? 1.0 / a[j] : 0.0; }
+        for (int j = 0; j < NC; ++j) { a[j] = exp10(x[j]); ai[j] = t.neg(j) ? 1.0 / a[j] : 0.0; }
     }
+    __device__ __forceinline__ void set(const EqDev& e, const double* x) { set(TabRun{e}, x); }
 };
 
-template <int NC>
-__device__ __forceinline__ double species_eval(const EqDev& e, int i, const double* x, const Powers<NC>& pw,
+template <int NC, class Tab>
+__device__ __forceinline__ double species_eval(const Tab& tb, int i, const double* x, const Powers<NC>& pw,
                                                bool& clamped) {
-    double lc = e.logk[i];
+    double lc = tb.logk(i);
 #pragma unroll
-    for (int j = 0; j < NC; ++j) lc = fma(e.stoich[i][j], x[j], lc);
+    for (int j = 0; j < NC; ++j) {
+        if constexpr (Tab::kFixed) { if (tb.ipow(i, j) == 0) continue; }
+        lc = fma(tb.s(i, j), x[j], lc);
+    }
     if (lc > 1.0) { clamped = true; return 10.0; }
     if (lc < -30.0) { clamped = true; return 1e-30; }
     clamped = false;
-    if (!e.all_int) return exp10(lc);
-    double p = e.k10[i];
+    if (!tb.all_int()) return exp10(lc);
+    double p = tb.k10(i);
 #pragma unroll
     for (int j = 0; j < NC; ++j) {
-        const int q = e.ipow[i][j];
+        const int q = tb.ipow(i, j);
         if (q == 0) continue;
         const double b = q > 0 ? pw.a[j] : pw.ai[j];
         const int m = q > 0 ? q : -q;
@@ -131,21 +180,31 @@ __device__ __forceinline__ double species_eval(const EqDev& e, int i, const doub
     return p;
 }
 
+template <int NC>
+__device__ __forceinline__ double species_eval(const EqDev& e, int i, const double* x, const Powers<NC>& pw,
+                                               bool& clamped) {
+    return species_eval<NC>(TabRun{e}, i, x, pw, clamped);
+}
+
 // F, and the relative residual
-template <int NC, int NS = 0>
-__device__ __forceinline__ double eq_residual(const EqDev& e, const double* T, const double* x, double* F) {
+template <int NC, int NS = 0, class Tab>
+__device__ __forceinline__ double eq_residual_t(const Tab& tb, const double* T, const double* x, double* F) {
     double sc[NC];
 #pragma unroll
     for (int j = 0; j < NC; ++j) { F[j] = -T[j]; sc[j] = 0.0; }
     Powers<NC> pw;
-    pw.set(e, x);
+    pw.set(tb, x);
 #pragma unroll (NS > 0 ? NS : 1)
-    for (int i = 0; i < (NS > 0 ? NS : e.ns); ++i) {
-        if (!e.active[i]) continue;
+    for (int i = 0; i < (NS > 0 ? NS : tb.ns()); ++i) {
+        if (!tb.active(i)) continue;
         bool clamped;
-        const double c = species_eval<NC>(e, i, x, pw, clamped);
+        const double c = species_eval<NC>(tb, i, x, pw, clamped);
 #pragma unroll
-        for (int j = 0; j < NC; ++j) { F[j] = fma(e.stoich[i][j], c, F[j]); sc[j] = fma(e.absS[i][j], c, sc[j]); }
+        for (int j = 0; j < NC; ++j) {
+            if constexpr (Tab::kFixed) { if (tb.ipow(i, j) == 0) continue; }
+            F[j] = fma(tb.s(i, j), c, F[j]);
+            sc[j] = fma(tb.abs_s(i, j), c, sc[j]);
+        }
     }
     double rel = 0.0;
 #pragma unroll
@@ -154,6 +213,11 @@ __device__ __forceinline__ double eq_residual(const EqDev& e, const double* T, c
         rel = (r > rel || r != r) ? r : rel;
     }
     return rel;
+}
+
+template <int NC, int NS = 0>
+__device__ __forceinline__ double eq_residual(const EqDev& e, const double* T, const double* x, double* F) {
+    return eq_residual_t<NC, NS>(TabRun{e}, T, x, F);
 }
 
 // reference cold start (solve_equilibrium_anderson, part4_eqsolver.hh:977-994)
@@ -175,8 +239,8 @@ __device__ __forceinline__ void eq_cold_start(const EqDev& e, const double* spec
 // (clamped species excluded) in one pass over the species
 // (cbuf: where given, each equilibrium species' concentration is stored at
 // cbuf[i * cstride], so a caller finds the species of the returned point)
-template <int NC, int NS = 0>
-__device__ __forceinline__ void eq_eval_full(const EqDev& e, const double* T, const double* x,
+template <int NC, int NS = 0, class Tab>
+__device__ __forceinline__ void eq_eval_full(const Tab& tb, const double* T, const double* x,
                                              double* F, double* sc, double (*J)[NC], double* cbuf = nullptr,
                                              int cstride = 0) {
 #pragma unroll
@@ -186,22 +250,26 @@ __device__ __forceinline__ void eq_eval_full(const EqDev& e, const double* T, co
         for (int b = 0; b < NC; ++b) J[a][b] = 0.0;
     }
     Powers<NC> pw;
-    pw.set(e, x);
+    pw.set(tb, x);
 #pragma unroll (NS > 0 ? NS : 1)
-    for (int i = 0; i < (NS > 0 ? NS : e.ns); ++i) {
-        if (!e.active[i]) continue;
+    for (int i = 0; i < (NS > 0 ? NS : tb.ns()); ++i) {
+        if (!tb.active(i)) continue;
         bool clamped;
-        const double c = species_eval<NC>(e, i, x, pw, clamped);
+        const double c = species_eval<NC>(tb, i, x, pw, clamped);
         if (cbuf) cbuf[i * cstride] = c;
         const double cj = clamped ? 0.0 : c;
 #pragma unroll
         for (int a = 0; a < NC; ++a) {
-            const double sa = e.stoich[i][a];
+            if constexpr (Tab::kFixed) { if (tb.ipow(i, a) == 0) continue; }
+            const double sa = tb.s(i, a);
             F[a] = fma(sa, c, F[a]);
-            sc[a] = fma(e.absS[i][a], c, sc[a]);
+            sc[a] = fma(tb.abs_s(i, a), c, sc[a]);
             const double sac = sa * cj;
 #pragma unroll
-            for (int b = 0; b <= a; ++b) J[a][b] = fma(sac, e.stoich[i][b], J[a][b]);
+            for (int b = 0; b <= a; ++b) {
+                if constexpr (Tab::kFixed) { if (tb.ipow(i, b) == 0) continue; }
+                J[a][b] = fma(sac, tb.s(i, b), J[a][b]);
+            }
         }
     }
 }
@@ -212,8 +280,8 @@ __device__ __forceinline__ void eq_eval_full(const EqDev& e, const double* T, co
 // shorter step the point is evaluated again.  The iterates are the same as
 // evaluating residual and Jacobian afresh at every iterate.  Returns the
 // number of steps taken; *conv = 1 at the relative residual tolerance.
-template <int NC, int NS = 0>
-__device__ __forceinline__ int eq_newton_reuse(const EqDev& e, const double* T, double* x, int max_iter, double tol, int* conv,
+template <int NC, int NS = 0, class Tab>
+__device__ __forceinline__ int eq_newton_reuse(const Tab& e, const double* T, double* x, int max_iter, double tol, int* conv,
                                int* stopped, double* cbuf = nullptr, int cstride = 0) {
     const double ln10 = 2.302585092994046;
     *conv = 0;
@@ -294,7 +362,7 @@ __device__ __forceinline__ int eq_newton_reuse(const EqDev& e, const double* T, 
         for (int ls = 1; ls < 40; ++ls) {
 #pragma unroll
             for (int a = 0; a < NC; ++a) xt[a] = fmin(fmax(fma(alpha, d[a], x[a]), -30.0), 1.0);
-            eq_residual<NC, NS>(e, T, xt, Ft);
+            eq_residual_t<NC, NS>(e, T, xt, Ft);
             fnt = 0.0;
 #pragma unroll
             for (int a = 0; a < NC; ++a) { const double r = Ft[a] * w[a]; fnt = fma(r, r, fnt); }
@@ -332,8 +400,8 @@ __device__ __forceinline__ int eq_newton_reuse(const EqDev& e, const double* T, 
 
 // The same iteration with residual and Jacobian evaluated afresh at every
 // iterate (fewer live registers; used above three components).
-template <int NC, int NS = 0>
-__device__ __forceinline__ int eq_newton_plain(const EqDev& e, const double* T, double* x, int max_iter, double tol, int* conv,
+template <int NC, int NS = 0, class Tab>
+__device__ __forceinline__ int eq_newton_plain(const Tab& tb, const double* T, double* x, int max_iter, double tol, int* conv,
                                int* stopped) {
     const double ln10 = 2.302585092994046;
     *conv = 0;
@@ -348,21 +416,21 @@ __device__ __forceinline__ int eq_newton_plain(const EqDev& e, const double* T, 
             for (int b = 0; b < NC; ++b) J[a][b] = 0.0;
         }
         Powers<NC> pw;
-        pw.set(e, x);
+        pw.set(tb, x);
 #pragma unroll (NS > 0 ? NS : 1)
-        for (int i = 0; i < (NS > 0 ? NS : e.ns); ++i) {
-            if (!e.active[i]) continue;
+        for (int i = 0; i < (NS > 0 ? NS : tb.ns()); ++i) {
+            if (!tb.active(i)) continue;
             bool clamped;
-            const double c = species_eval<NC>(e, i, x, pw, clamped);
+            const double c = species_eval<NC>(tb, i, x, pw, clamped);
             const double cj = clamped ? 0.0 : c;
 #pragma unroll
             for (int a = 0; a < NC; ++a) {
-                const double sa = e.stoich[i][a];
+                const double sa = tb.s(i, a);
                 F[a] = fma(sa, c, F[a]);
-                sc[a] = fma(e.absS[i][a], c, sc[a]);
+                sc[a] = fma(tb.abs_s(i, a), c, sc[a]);
                 const double sac = sa * cj;
 #pragma unroll
-                for (int b = 0; b <= a; ++b) J[a][b] = fma(sac, e.stoich[i][b], J[a][b]);
+                for (int b = 0; b <= a; ++b) J[a][b] = fma(sac, tb.s(i, b), J[a][b]);
             }
         }
         double rel = 0.0, fn = 0.0, w[NC];
@@ -427,7 +495,7 @@ __device__ __forceinline__ int eq_newton_plain(const EqDev& e, const double* T, 
 #pragma unroll
             for (int a = 0; a < NC; ++a) xt[a] = fmin(fmax(fma(alpha, d[a], x[a]), -30.0), 1.0);
             double Ft[NC];
-            eq_residual<NC, NS>(e, T, xt, Ft);
+            eq_residual_t<NC, NS>(tb, T, xt, Ft);
             double fnt = 0.0;
 #pragma unroll
             for (int a = 0; a < NC; ++a) { const double r = Ft[a] * w[a]; fnt = fma(r, r, fnt); }
@@ -444,7 +512,7 @@ __device__ __forceinline__ int eq_newton_plain(const EqDev& e, const double* T, 
         stuck = !accepted;
     }
     double Fe[NC];
-    if (eq_residual<NC, NS>(e, T, x, Fe) <= tol) *conv = 1;
+    if (eq_residual_t<NC, NS>(tb, T, x, Fe) <= tol) *conv = 1;
     else if (stuck && stopped) *stopped = 1;
     return max_iter;
 }
@@ -599,8 +667,16 @@ template <int NC, int NS = 0>
 __device__ __forceinline__ int eq_newton(const EqDev& e, const double* T, double* x, int max_iter, double tol,
                                          int* conv, int* stopped = nullptr, double* cbuf = nullptr,
                                          int cstride = 0) {
-    if constexpr (NC <= 3) return eq_newton_reuse<NC, NS>(e, T, x, max_iter, tol, conv, stopped, cbuf, cstride);
-    else return eq_newton_plain<NC, NS>(e, T, x, max_iter, tol, conv, stopped);
+    if constexpr (NC <= 3) return eq_newton_reuse<NC, NS>(TabRun{e}, T, x, max_iter, tol, conv, stopped, cbuf, cstride);
+    else return eq_newton_plain<NC, NS>(TabRun{e}, T, x, max_iter, tol, conv, stopped);
+}
+
+// the same on a given tableau policy (TabRun or TabFixed)
+template <int NC, int NS, class Tab>
+__device__ __forceinline__ int eq_newton_t(const Tab& tb, const double* T, double* x, int max_iter, double tol,
+                                           int* conv, double* cbuf, int cstride) {
+    if constexpr (NC <= 3) return eq_newton_reuse<NC, NS>(tb, T, x, max_iter, tol, conv, nullptr, cbuf, cstride);
+    else return eq_newton_plain<NC, NS>(tb, T, x, max_iter, tol, conv, nullptr);
 }
 
 // component totals (calc_component_totals, part4_eqsolver.hh:520-538)
