@@ -56,23 +56,13 @@ __device__ __forceinline__ void fast_dissol_gather(const AdeK& k, int64_t n, int
     }
 }
 
-// A voxel's biomass and previous Newton solutions already staged in shared
-// memory (the staged launch), with the stride of the staging columns.
-struct ChainStage {
-    const double* bio;
-    const double* wx;
-    const double* wxp;
-    int stride;
-};
-
 // The reaction chain of one voxel on register arrays (reaction_chain with
 // the Newton solver).  C: densities, updated as each processor applies its
 // increments; A: the total increment per solute.  Returns 1 if the
 // equilibrium solve did not converge.
 template <class Chem>
 __device__ __forceinline__ int fast_chain(const AdeK& k, int64_t n, uint32_t sto, int x, int y, int z, uint8_t cls,
-                                          double (&C)[Chem::S], double (&A)[Chem::S],
-                                          const ChainStage* sg = nullptr) {
+                                          double (&C)[Chem::S], double (&A)[Chem::S]) {
     constexpr int S = Chem::S, M = Chem::M, MW = Chem::MW, NC = Chem::NC;
     const AdeParams& p = k.p;
     const int64_t N = k.g.N;
@@ -82,7 +72,7 @@ __device__ __forceinline__ int fast_chain(const AdeK& k, int64_t n, uint32_t sto
         double B[MW], BR[MW];
 #pragma unroll
         for (int m = 0; m < MW; ++m) {
-            const double b = m < M ? (sg ? sg->bio[m * sg->stride] : k.bio[m * N + n]) : 0.0;
+            const double b = m < M ? k.bio[m * N + n] : 0.0;
             B[m] = b < THRD ? 0.0 : b;
         }
         Chem::kinetics(p, C, B, R, BR, k.mask[n]);
@@ -105,8 +95,7 @@ __device__ __forceinline__ int fast_chain(const AdeK& k, int64_t n, uint32_t sto
         for (int m = 0; m < M; ++m) {
             const double d = BR[m];
             if (d > THRD || d < -THRD) {
-                if (sg) k.bio[m * N + n] = sg->bio[m * sg->stride] + d;
-                else k.bio[m * N + n] += d;
+                k.bio[m * N + n] += d;
             }
         }
     }
@@ -158,9 +147,9 @@ __device__ __forceinline__ int fast_chain(const AdeK& k, int64_t n, uint32_t sto
             bool two = true;
 #pragma unroll
             for (int j = 0; j < NC; ++j) {
-                xprev[j] = sg ? sg->wx[j * sg->stride] : k.eq_x[(int64_t)j * N + sto];
+                xprev[j] = (double)k.eq_x[(int64_t)j * N + sto];
                 warm = warm && (xprev[j] == xprev[j]);
-                const double xq = sg ? sg->wxp[j * sg->stride] : k.eq_xp[(int64_t)j * N + sto];
+                const double xq = (double)k.eq_xp[(int64_t)j * N + sto];
                 two = two && (xq == xq);
                 x[j] = xprev[j];
                 if (two) x[j] = fmin(fmax(2.0 * xprev[j] - xq, -30.0), 1.0);
@@ -203,7 +192,10 @@ __device__ __forceinline__ int fast_chain(const AdeK& k, int64_t n, uint32_t sto
         }
         if (k.eq_x && conv) {
 #pragma unroll
-            for (int j = 0; j < NC; ++j) { k.eq_xp[(int64_t)j * N + sto] = xprev[j]; k.eq_x[(int64_t)j * N + sto] = x[j]; }
+            for (int j = 0; j < NC; ++j) {
+                k.eq_xp[(int64_t)j * N + sto] = (float)xprev[j];
+                k.eq_x[(int64_t)j * N + sto] = (float)x[j];
+            }
         }
         if (k.eq_iters) k.eq_iters[n] = it;
         if (conv && k.pair_T && learn_sampled((uint32_t)n, k.pair_salt, k.pair_mask))
@@ -319,285 +311,6 @@ ade_fast_kernel(const __grid_constant__ AdeK k, const uint32_t* __restrict__ lis
     if ((threadIdx.x & 31) == 0 && nonconv) atomicAdd(&k.counters[0], nonconv);
 }
 
-// ---------------------------------------------------------------------------
-// The staged launch.  Each thread owns one voxel of a 64-voxel tile at a time
-// and keeps the next tile's inputs coming while it computes: the populations
-// of its next voxel, its previous Newton solutions, biomass, immobile
-// inventories and velocity are copied global -> shared with cp.async (no
-// register holds them in flight), double-buffered, so the loads of tile t+1
-// overlap the FP64 chain of tile t.  A thread reads only its own column of
-// the staging buffers, so no barrier is needed; wait_group orders each
-// thread's own copies.  The arithmetic is the fused launch's.
-constexpr int kStageT = 64;
-
-__device__ __forceinline__ void cpa4(void* smem, const void* gmem) {
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cpa8(void* smem, const void* gmem) {
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int PENDING>
-__device__ __forceinline__ void cpa_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(PENDING) : "memory"); }
-
-template <class Chem>
-struct StageBuf {
-    static constexpr int NIMM = Chem::S - Chem::NMOB > 0 ? Chem::S - Chem::NMOB : 1;
-    static constexpr int NCW = Chem::NC > 0 ? Chem::NC : 1;
-    float pop[Chem::NMOB * 7][kStageT];
-    float u[3][kStageT];
-    double wx[NCW][kStageT], wxp[NCW][kStageT];
-    double bio[Chem::MW][kStageT];
-    double imm[NIMM][kStageT];
-};
-
-// rank of an immobile solute among the immobile ones
-template <class Chem>
-__host__ __device__ constexpr int imm_rank(int s) {
-    int k = 0;
-    for (int q = 0; q < s; ++q) k += Chem::mobile(q) ? 0 : 1;
-    return k;
-}
-
-// what a thread carries from the staging of its voxel to its computation
-struct StageSite {
-    int valid;
-    uint32_t n;
-    uint8_t cls;
-    int x, y, z;
-    SSite st;
-};
-
-template <class Chem, int PARITY>
-__device__ __forceinline__ void stage_issue(const AdeK& k, const uint32_t* __restrict__ list, int64_t r, int64_t count,
-                                            StageBuf<Chem>& B, int t, StageSite& ss) {
-    constexpr int S = Chem::S, NMOB = Chem::NMOB, NC = Chem::NC;
-    const int64_t N = k.g.N;
-    const uint32_t N32 = (uint32_t)N;
-    ss.valid = r < count;
-    if (!ss.valid) return;
-    ss.n = list[r];
-    ss.cls = k.cls[ss.n];
-    decode(k.g, ss.n, ss.x, ss.y, ss.z);
-    if (!make_ssite<PARITY>(k.g, k.sidx, ss.x, ss.y, ss.z, ss.n, ss.st)) atomicAdd(&k.counters[1], 1ull);
-    const SSite& st = ss.st;
-#pragma unroll
-    for (int m = 0; m < NMOB; ++m) {
-        const float* pm = k.pop + (int64_t)m * 7 * N;
-        cpa4(&B.pop[m * 7][t], pm + st.s);
-#pragma unroll
-        for (int i = 1; i < 7; ++i) {
-            const float* src = (PARITY == 0 || !st.inx(-c7x(i))) ? pm + (uint32_t)i * N32 + st.s
-                                                                 : pm + (uint32_t)opp7(i) * N32 + st.nb[opp7(i) - 1];
-            cpa4(&B.pop[m * 7 + i][t], src);
-        }
-    }
-#pragma unroll
-    for (int c = 0; c < 3; ++c) cpa4(&B.u[c][t], k.u + (int64_t)c * N + ss.n);
-    if (ss.cls & F_REACTIVE) {
-#pragma unroll
-        for (int m = 0; m < Chem::M; ++m) cpa8(&B.bio[m][t], k.bio + (int64_t)m * N + ss.n);
-#pragma unroll
-        for (int s = 0; s < S; ++s)
-            if (!Chem::mobile(s)) cpa8(&B.imm[imm_rank<Chem>(s)][t], k.imm + (int64_t)s * N + ss.n);
-        if constexpr (NC > 0) {
-            if (k.eq_x) {
-#pragma unroll
-                for (int j = 0; j < NC; ++j) {
-                    cpa8(&B.wx[j][t], k.eq_x + (int64_t)j * N + st.s);
-                    cpa8(&B.wxp[j][t], k.eq_xp + (int64_t)j * N + st.s);
-                }
-            }
-        }
-    }
-}
-
-template <class Chem, int PARITY>
-__global__ void __launch_bounds__(kStageT, 5)
-ade_stage_kernel(const __grid_constant__ AdeK k, const uint32_t* __restrict__ list, int64_t count, int any_rxn) {
-    constexpr int S = Chem::S, NMOB = Chem::NMOB;
-    extern __shared__ __align__(16) unsigned char stage_raw[];
-    StageBuf<Chem>* buf = reinterpret_cast<StageBuf<Chem>*>(stage_raw);
-    const AdeParams& p = k.p;
-    const int64_t N = k.g.N, plane = k.g.plane;
-    const uint32_t N32 = (uint32_t)N;
-    const int t = threadIdx.x;
-    const int64_t ntiles = (count + kStageT - 1) / kStageT;
-    unsigned long long nonconv = 0;
-    StageSite nxt, cur;
-    int64_t tile = blockIdx.x;
-    stage_issue<Chem, PARITY>(k, list, tile * kStageT + t, count, buf[0], t, nxt);
-    cpa_commit();
-    int b = 0;
-    for (; tile < ntiles; tile += gridDim.x, b ^= 1) {
-        cur = nxt;
-        stage_issue<Chem, PARITY>(k, list, (tile + gridDim.x) * kStageT + t, count, buf[b ^ 1], t, nxt);
-        cpa_commit();
-        cpa_wait<1>();
-        if (!cur.valid) continue;
-        StageBuf<Chem>& B = buf[b];
-        const uint32_t n = cur.n;
-        const uint8_t cls = cur.cls, dyn = cls & 3;
-        const int x = cur.x;
-        float dcv[NMOB];
-#pragma unroll
-        for (int m = 0; m < NMOB; ++m) dcv[m] = 0.f;
-        if (any_rxn && (cls & F_REACTIVE)) {
-            double C[S], A[S];
-#pragma unroll
-            for (int s = 0; s < S; ++s) {
-                if (Chem::mobile(s)) {
-                    const int m = Chem::slot(s);
-                    float rr = 0.f;
-#pragma unroll
-                    for (int i = 0; i < 7; ++i) rr += B.pop[m * 7 + i][t];
-                    C[s] = (double)rr;
-                } else {
-                    C[s] = B.imm[imm_rank<Chem>(s)][t];
-                }
-                A[s] = 0.0;
-            }
-            const ChainStage sg{&B.bio[0][t], &B.wx[0][t], &B.wxp[0][t], kStageT};
-            nonconv += fast_chain<Chem>(k, n, cur.st.s, x, cur.y, cur.z, cls, C, A, &sg);
-#pragma unroll
-            for (int s = 0; s < S; ++s) {
-                if (Chem::mobile(s)) dcv[Chem::slot(s)] = (float)A[s];
-                else if (A[s] != 0.0) k.imm[(int64_t)s * N + n] = B.imm[imm_rank<Chem>(s)][t] + A[s];
-            }
-        }
-        const float ux = B.u[0][t], uy = B.u[1][t], uz = B.u[2][t];
-        const bool adj = (x == 1 || x == k.g.nx - 2);
-#pragma unroll
-        for (int m = 0; m < NMOB; ++m) {
-            float f[7];
-#pragma unroll
-            for (int i = 0; i < 7; ++i) f[i] = B.pop[m * 7 + i][t];
-            float rho = 0.f;
-            if (dyn == BB) {
-#pragma unroll
-                for (int i = 1; i < 4; ++i) { const float tmp = f[i]; f[i] = f[i + 3]; f[i + 3] = tmp; }
-            } else if (dyn != NODYN) {
-                const float om = (dyn == BIO) ? p.omega_bio[m] : p.omega_pore[m];
-                collide7(f, om, ux, uy, uz, rho);
-            } else if (adj) {
-#pragma unroll
-                for (int i = 0; i < 7; ++i) rho += f[i];
-            }
-            const float d = dcv[m];
-            if (d != 0.f) {
-#pragma unroll
-                for (int i = 0; i < 7; ++i) f[i] += t7(i) * d;
-            }
-            if (adj && dyn != BB) {
-                const int side = (x == 1) ? 0 : 1;
-                k.rho_adj[((int64_t)m * 2 + side) * plane + (n - (int64_t)x * plane)] = rho;
-            }
-            scatter7<PARITY>(k.pop + (int64_t)m * 7 * N, N32, cur.st, f);
-        }
-    }
-    cpa_wait<0>();
-    for (int o = 16; o > 0; o >>= 1) nonconv += __shfl_down_sync(0xffffffffu, nonconv, o);
-    if ((t & 31) == 0 && nonconv) atomicAdd(&k.counters[0], nonconv);
-}
-
-template <class Chem>
-int stage_launch(Ctx* c, const AdeK& k, int any_rxn) {
-    const size_t smem = 2 * sizeof(StageBuf<Chem>);
-    const int blocks = grid_for((c->n_live + kStageT - 1) / kStageT, 1, 148 * 5);
-    auto go = [&](auto kern) -> int {
-        CL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        kern<<<blocks, kStageT, smem, c->stream>>>(k, c->d_live, c->n_live, any_rxn);
-        CL_LAUNCH_CHECK("ade_stage_kernel");
-        return CL_OK;
-    };
-    return c->ade_parity == 0 ? go(ade_stage_kernel<Chem, 0>) : go(ade_stage_kernel<Chem, 1>);
-}
-
-// The compiled chain alone (the split design): densities of this step in,
-// each mobile solute's total increment out to dc (by storage index), for the
-// run-time-table streaming launch to add after its collision.
-template <class Chem, int PARITY>
-__global__ void __launch_bounds__(128, 3)
-ade_fast_react_kernel(const __grid_constant__ AdeK k, const uint32_t* __restrict__ list, int64_t r0, int64_t r1,
-                      float* __restrict__ dc) {
-    constexpr int S = Chem::S;
-    const int64_t N = k.g.N;
-    const uint32_t N32 = (uint32_t)N;
-    unsigned long long nonconv = 0;
-    for (int64_t r = r0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < r1; r += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t n = list[r];
-        const uint8_t cls = k.cls[n];
-        if (!(cls & F_REACTIVE)) continue;
-        int x, y, z;
-        decode(k.g, n, x, y, z);
-        SSite st;
-        if (!make_ssite<PARITY>(k.g, k.sidx, x, y, z, n, st)) atomicAdd(&k.counters[1], 1ull);
-        double C[S], A[S];
-#pragma unroll
-        for (int s0 = 0; s0 < S; s0 += kGroup) {
-            float f[kGroup][7];
-#pragma unroll
-            for (int g = 0; g < kGroup; ++g)
-                if (s0 + g < S && Chem::mobile(s0 + g))
-                    gather7<PARITY>(k.pop + (int64_t)Chem::slot(s0 + g) * 7 * N, N32, st, f[g]);
-#pragma unroll
-            for (int g = 0; g < kGroup; ++g) {
-                const int s = s0 + g;
-                if (s >= S) continue;
-                if (Chem::mobile(s)) {
-                    float rr = 0.f;
-#pragma unroll
-                    for (int i = 0; i < 7; ++i) rr += f[g][i];
-                    C[s] = (double)rr;
-                } else {
-                    C[s] = k.imm[(int64_t)s * N + n];
-                }
-                A[s] = 0.0;
-            }
-        }
-        nonconv += fast_chain<Chem>(k, n, st.s, x, y, z, cls, C, A);
-#pragma unroll
-        for (int s = 0; s < S; ++s) {
-            if (Chem::mobile(s)) dc[(int64_t)Chem::slot(s) * N + st.s] = (float)A[s];
-            else if (A[s] != 0.0) k.imm[(int64_t)s * N + n] += A[s];
-        }
-    }
-    for (int o = 16; o > 0; o >>= 1) nonconv += __shfl_down_sync(0xffffffffu, nonconv, o);
-    if ((threadIdx.x & 31) == 0 && nonconv) atomicAdd(&k.counters[0], nonconv);
-}
-
-// the split design: slab j's compiled reactions (s_react), then its
-// streaming (s_stream), slab j+1's reactions overlapping slab j's streaming
-template <class Chem>
-int fast_split(Ctx* c, const AdeK& k) {
-    constexpr int NMOB = Chem::NMOB;
-    const int G = c->slabs;
-    CL_CUDA(cudaEventRecord(c->ev_fork, c->stream));
-    CL_CUDA(cudaStreamWaitEvent(c->s_react, c->ev_fork, 0));
-    CL_CUDA(cudaStreamWaitEvent(c->s_stream, c->ev_fork, 0));
-    for (int j = 0; j < G; ++j) {
-        const int64_t r0 = G > 1 ? c->slab_live[j] : 0, r1 = G > 1 ? c->slab_live[j + 1] : c->n_live;
-        if (r1 > r0) {
-            const int rb = grid_for(r1 - r0, 128, 148 * 3);
-            if (c->ade_parity == 0)
-                ade_fast_react_kernel<Chem, 0><<<rb, 128, 0, c->s_react>>>(k, c->d_live, r0, r1, c->d_dc);
-            else
-                ade_fast_react_kernel<Chem, 1><<<rb, 128, 0, c->s_react>>>(k, c->d_live, r0, r1, c->d_dc);
-            CL_LAUNCH_CHECK("ade_fast_react_kernel");
-            c->launches += 1;
-        }
-        CL_CUDA(cudaEventRecord(c->ev_slab[j], c->s_react));
-        CL_CUDA(cudaStreamWaitEvent(c->s_stream, c->ev_slab[j], 0));
-        int r = launch_stream<NMOB>(c, k, c->s_stream, r0, r1, 1, 148 * 4);
-        if (r) return r;
-    }
-    CL_CUDA(cudaEventRecord(c->ev_join, c->s_stream));
-    CL_CUDA(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
-    return CL_OK;
-}
-
 template <class Chem, int B, int MB>
 int fast_launch(Ctx* c, const AdeK& k, int any_rxn) {
     const int blocks = grid_for(c->n_live, B, 148 * MB * 16);
@@ -620,13 +333,12 @@ int fast_step(Ctx* c) {
     if (c->n_live > 0) {
         if ((r = timing_begin(c, CL_KERNEL_ADE_MAIN))) return r;
         const int ar = any_rxn ? 1 : 0;
+        // launch shapes (threads per block x blocks per SM, which sets the
+        // register cap): 128x4 measured fastest on the coupled workload
         switch (c->fast_variant) {
             case 1: r = fast_launch<Chem, 128, 3>(c, k, ar); break;
-            case 2: r = fast_launch<Chem, 128, 2>(c, k, ar); break;
-            case 3: r = fast_launch<Chem, 64, 6>(c, k, ar); break;
-            case 4: r = fast_launch<Chem, 64, 5>(c, k, ar); break;
-            case 5: r = ar ? fast_split<Chem>(c, k) : fast_launch<Chem, 128, 4>(c, k, ar); break;
-            case 6: r = stage_launch<Chem>(c, k, ar); break;
+            case 2: r = fast_launch<Chem, 64, 6>(c, k, ar); break;
+            case 3: r = fast_launch<Chem, 64, 5>(c, k, ar); break;
             default: r = fast_launch<Chem, 128, 4>(c, k, ar); break;
         }
         if (r) return r;

@@ -57,8 +57,13 @@ struct AdeK {
     double* bio;              // M*N
     float* rho_adj;           // n_mob * 2 * plane
     int32_t* eq_iters;        // N (may be null)
-    double* eq_x;             // NC*N previous solutions, by storage index (null: cold start only)
-    double* eq_xp;            // NC*N the solutions before those, by storage index
+    // NC*N previous solutions and the ones before those, by storage index
+    // (null: cold start only); FP32: a start needs no more, and transport
+    // moves nearly every voxel's totals by more than the 1e-10 tolerance each
+    // step, so a solve almost never stops at its start anyway (on the coupled
+    // workload a few voxels in 1e5 per step)
+    float* eq_x;
+    float* eq_xp;
     const uint8_t* mask;      // N material numbers
     const uint8_t* phase;     // N phase ids (null without dissolution)
     double* rel;              // S*N releases of the phase voxels (null without dissolution)
@@ -452,9 +457,9 @@ __device__ int reaction_chain(const AdeK& k, int64_t n, uint32_t sto, int x, int
             bool two = true;
 #pragma unroll
             for (int j = 0; j < NC; ++j) {
-                xprev[j] = k.eq_x[(int64_t)j * N + sto];
+                xprev[j] = (double)k.eq_x[(int64_t)j * N + sto];
                 warm = warm && (xprev[j] == xprev[j]);
-                const double xq = k.eq_xp[(int64_t)j * N + sto];
+                const double xq = (double)k.eq_xp[(int64_t)j * N + sto];
                 two = two && (xq == xq);
                 x[j] = xprev[j];
                 if (two) x[j] = fmin(fmax(2.0 * xprev[j] - xq, -30.0), 1.0);
@@ -475,7 +480,10 @@ __device__ int reaction_chain(const AdeK& k, int64_t n, uint32_t sto, int x, int
         }
         if (k.eq_x && conv) {
 #pragma unroll
-            for (int j = 0; j < NC; ++j) { k.eq_xp[(int64_t)j * N + sto] = xprev[j]; k.eq_x[(int64_t)j * N + sto] = x[j]; }
+            for (int j = 0; j < NC; ++j) {
+                k.eq_xp[(int64_t)j * N + sto] = (float)xprev[j];
+                k.eq_x[(int64_t)j * N + sto] = (float)x[j];
+            }
         }
         if (k.eq_iters) k.eq_iters[n] = it;
         if (!conv) nonconv = 1;

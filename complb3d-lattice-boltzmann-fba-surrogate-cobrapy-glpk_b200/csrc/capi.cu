@@ -251,8 +251,8 @@ cl_ctx* cl_create(const cl_config* cfg, void* stream, int* status) {
         (r = dalloc(c, &c->d_ca_out, (size_t)(cfg->ca_enabled ? 6 * p.M : 0) * N)) ||
         (r = dalloc(c, &c->d_counters, 8)) || (r = dalloc(c, &c->d_tracer, 1)))
         return fail(r);
-    if (c->d_eq_x) cudaMemsetAsync(c->d_eq_x, 0xff, sizeof(double) * cfg->eq.n_comp * N, c->stream);  // NaN
-    if (c->d_eq_xp) cudaMemsetAsync(c->d_eq_xp, 0xff, sizeof(double) * cfg->eq.n_comp * N, c->stream);
+    if (c->d_eq_x) cudaMemsetAsync(c->d_eq_x, 0xff, sizeof(float) * cfg->eq.n_comp * N, c->stream);  // NaN
+    if (c->d_eq_xp) cudaMemsetAsync(c->d_eq_xp, 0xff, sizeof(float) * cfg->eq.n_comp * N, c->stream);
     c->energy_blocks = grid_for(N, 256, 148 * 8);
     if ((r = dalloc(c, &c->d_energy_part, c->energy_blocks))) return fail(r);
     c->scratch_bytes = sizeof(double) * ((size_t)N + 65536);
@@ -570,13 +570,13 @@ int cl_set_option(cl_ctx* h, int32_t key, int64_t value) {
             c->chem_on = value != 0;
             return CL_OK;
         case CL_OPT_FAST_VARIANT:
-            if (value < 0 || value > 6) { set_error("cl_set_option: variant 0..6"); return CL_ERR_ARG; }
+            if (value < 0 || value > 3) { set_error("cl_set_option: variant 0..3"); return CL_ERR_ARG; }
             c->fast_variant = (int)value; return CL_OK;
         case CL_OPT_EQ_LEARN: return learn_enable(c, value);
         case CL_OPT_EQ_FORGET: {
             const int nc = c->cfg.eq.n_comp;
-            if (c->d_eq_x) CL_CUDA(cudaMemsetAsync(c->d_eq_x, 0xff, sizeof(double) * nc * c->geo.N, c->stream));
-            if (c->d_eq_xp) CL_CUDA(cudaMemsetAsync(c->d_eq_xp, 0xff, sizeof(double) * nc * c->geo.N, c->stream));
+            if (c->d_eq_x) CL_CUDA(cudaMemsetAsync(c->d_eq_x, 0xff, sizeof(float) * nc * c->geo.N, c->stream));
+            if (c->d_eq_xp) CL_CUDA(cudaMemsetAsync(c->d_eq_xp, 0xff, sizeof(float) * nc * c->geo.N, c->stream));
             CL_CUDA(cudaStreamSynchronize(c->stream));
             return CL_OK;
         }

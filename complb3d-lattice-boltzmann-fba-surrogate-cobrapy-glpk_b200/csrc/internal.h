@@ -103,8 +103,8 @@ struct Ctx {
     float*   d_rho_adj = nullptr;    // n_mob*2*plane : pre-collision density next to each x face
     int32_t* d_eq_iters = nullptr;   // N
     float*   d_srg_params[CL_MAX_SRG_ORG] = {nullptr, nullptr};
-    double*  d_eq_x = nullptr;       // n_comp*N previous converged log10 free components, by storage index (NaN: none)
-    double*  d_eq_xp = nullptr;      // n_comp*N the solution before that, by storage index (NaN: none)
+    float*   d_eq_x = nullptr;       // n_comp*N previous converged log10 free components, by storage index (NaN: none)
+    float*   d_eq_xp = nullptr;      // n_comp*N the solution before that, by storage index (NaN: none)
     uint8_t* d_phase = nullptr;      // N dissolvable phase id, 0 = none (dissolution only)
     double*  d_ca_total = nullptr;   // N total biomass (cellular automaton)
     int32_t* d_ca_age = nullptr;     // 2*N age wavefront, ping-pong

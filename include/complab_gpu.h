@@ -363,7 +363,7 @@ int cl_op_stream(cl_ctx* ctx);
  *                         chemistry matches, 1 = use it (default);
  *                         get: the id of the compiled chemistry in use, 0 = none. */
 #define CL_OPT_COMPILED_CHEM 1
-#define CL_OPT_FAST_VARIANT  2   /* launch design of the compiled chemistry's step, 0..6 */
+#define CL_OPT_FAST_VARIANT  2   /* launch shape of the compiled chemistry's step, 0..3 */
 /* The learned warm start in the step (a compiled chemistry with Newton
  * speciation of 1..5 components; no counterpart in the reference).
  *   CL_OPT_EQ_LEARN  set K > 0: every step stores the (totals -> log10 free

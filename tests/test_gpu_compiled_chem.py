@@ -43,10 +43,9 @@ def _run(pkg, cfg, mask, bio, steps, compiled, flow_steps=60, variant=0):
     return out
 
 
-# launch designs of the compiled step: 0 one launch, 5 reaction launch +
-# streaming launch by slabs, 6 one launch with the inputs staged in shared
-# memory by asynchronous copies
-@pytest.mark.parametrize("variant", [0, 5, 6])
+# launch shapes of the one-launch step: 0 128 threads x 4 blocks per SM,
+# 2 64 x 6 (a different register cap, so different code)
+@pytest.mark.parametrize("variant", [0, 2])
 @pytest.mark.parametrize("steps", [1, 2, 25])
 def test_coupled_compiled_matches_table_and_oracle(gpu_lib, pkg, wl, steps, variant):
     mask = wl.sphere_pack(34, 16, 16, 0.45, 2.0, 4.0, seed=3)
@@ -68,7 +67,7 @@ def test_coupled_compiled_matches_table_and_oracle(gpu_lib, pkg, wl, steps, vari
     assert rel_l2(fast["bio"], tr.biomass(0)) < 1e-5
 
 
-@pytest.mark.parametrize("variant", [0, 6])
+@pytest.mark.parametrize("variant", [0, 2])
 def test_biotic_compiled_matches_table_and_oracle(gpu_lib, pkg, wl, variant):
     mask = wl.sphere_pack(30, 16, 16, 0.4, 2.0, 4.0, seed=8)
     nx, ny, nz = mask.shape
