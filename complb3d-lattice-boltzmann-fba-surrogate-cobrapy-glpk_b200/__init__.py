@@ -139,12 +139,23 @@ def load_library(path=LIB_PATH):
         ("cl_timing_enable", [vp, c_int32]), ("cl_timing_read", [vp, c_int32, P(c_double), P(c_int64)]),
         ("cl_launch_count", [vp, P(c_int64)]), ("cl_set_surrogate", [vp, c_int32, vp]),
         ("cl_ca_redistribute", [vp, P(c_int32), P(c_int64), P(c_double)]), ("cl_ca_update_mask", [vp, P(c_int64)]),
+        ("cl_math_exp10", [vp, vp, c_int64, c_int32]),
     ]:
         fn = getattr(lib, name)
         fn.restype = ctypes.c_int
         fn.argtypes = args
     _lib = lib
     return lib
+
+
+def math_exp10(x, which=0):
+    """The library's FP64 10^x (which=0, the Newton solves' own) or CUDA's
+    exp10 (which=1) on the GPU, for accuracy checks."""
+    lib = load_library()
+    xs = np.ascontiguousarray(x, np.float64)
+    y = np.zeros_like(xs)
+    _check(lib, lib.cl_math_exp10(_ptr(xs), _ptr(y), xs.size, which), "cl_math_exp10")
+    return y
 
 
 def check_abi(lib=None):

@@ -127,6 +127,38 @@ struct TabFixed {
     __device__ __forceinline__ double k10(int i) const { return e.k10[i]; }
 };
 
+// 10^x in FP64 for the Newton solves, about 1 ulp: Cody-Waite argument
+// reduction y = x log2(10) = n + f with n = rint(y), |f| <= 1/2, the
+// product carried as an exact two-term sum (Dekker's FMA split, with the
+// tail of log2(10)); 2^f = e^t, t = f ln 2, by the Taylor series to degree 13
+// (|t| <= 0.347, truncation below 5e-18) evaluated in Estrin's scheme, so the
+// dependent chain is five operations deep; the result scaled by 2^n through
+// the exponent field.  Arguments outside |x| < 300 (never reached by the
+// clamped logs) go to the library's exp10.
+__device__ __forceinline__ double cl_exp10(double x) {
+    if (!(fabs(x) < 300.0)) return exp10(x);
+    constexpr double kL2T = 3.321928094887362, kL2T_lo = 1.661617516973592e-16;   // log2(10) = kL2T + kL2T_lo
+    constexpr double kLn2 = 0.6931471805599453, kLn2_lo = 2.3190468138462996e-17;
+    const double yh = x * kL2T;
+    const double yl = fma(x, kL2T, -yh) + x * kL2T_lo;
+    const double n = rint(yh);
+    const double f = (yh - n) + yl;                  // yh - n is exact
+    const double t = fma(f, kLn2, f * kLn2_lo);
+    const double t2 = t * t, t4 = t2 * t2, t8 = t4 * t4;
+    const double p01 = fma(t, 1.0, 1.0);
+    const double p23 = fma(t, 1.0 / 6.0, 0.5);
+    const double p45 = fma(t, 1.0 / 120.0, 1.0 / 24.0);
+    const double p67 = fma(t, 1.0 / 5040.0, 1.0 / 720.0);
+    const double p89 = fma(t, 1.0 / 362880.0, 1.0 / 40320.0);
+    const double pab = fma(t, 1.0 / 39916800.0, 1.0 / 3628800.0);
+    const double pcd = fma(t, 1.0 / 6227020800.0, 1.0 / 479001600.0);
+    const double q0 = fma(p23, t2, p01), q1 = fma(p67, t2, p45), q2 = fma(pab, t2, p89);
+    const double r0 = fma(q1, t4, q0), r1 = fma(pcd, t4, q2);
+    const double p = fma(r1, t8, r0);
+    const long long e = (long long)n + 1023;
+    return p * __longlong_as_double(e << 52);
+}
+
 // species concentration from the component logs, clamped as calc_species
 template <int NC>
 __device__ __forceinline__ double species_c(const EqDev& e, int i, const double* x) {
@@ -134,7 +166,7 @@ __device__ __forceinline__ double species_c(const EqDev& e, int i, const double*
 #pragma unroll
     for (int j = 0; j < NC; ++j) lc = fma(e.stoich[i][j], x[j], lc);
     lc = fmin(fmax(lc, -30.0), 1.0);
-    return exp10(lc);
+    return cl_exp10(lc);
 }
 
 // Free-component activities a_j = 10^x_j and their inverses, once per
@@ -148,7 +180,7 @@ struct Powers {
     template <class Tab>
     __device__ __forceinline__ void set(const Tab& t, const double* x) {
 #pragma unroll
-        for (int j = 0; j < NC; ++j) { a[j] = exp10(x[j]); ai[j] = t.neg(j) ? 1.0 / a[j] : 0.0; }
+        for (int j = 0; j < NC; ++j) { a[j] = cl_exp10(x[j]); ai[j] = t.neg(j) ? 1.0 / a[j] : 0.0; }
     }
     __device__ __forceinline__ void set(const EqDev& e, const double* x) { set(TabRun{e}, x); }
 };
@@ -165,7 +197,7 @@ __device__ __forceinline__ double species_eval(const Tab& tb, int i, const doubl
     if (lc > 1.0) { clamped = true; return 10.0; }
     if (lc < -30.0) { clamped = true; return 1e-30; }
     clamped = false;
-    if (!tb.all_int()) return exp10(lc);
+    if (!tb.all_int()) return cl_exp10(lc);
     double p = tb.k10(i);
 #pragma unroll
     for (int j = 0; j < NC; ++j) {

@@ -1156,3 +1156,25 @@ extern "C" int cl_eq_solve_noalloc(const cl_eq_system* sys, const double* d_tota
     CL_LAUNCH_CHECK("cl_eq_solve_noalloc");
     return CL_OK;
 }
+
+namespace cl {
+__global__ void exp10_check_kernel(const double* x, double* y, int64_t n, int which) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        y[i] = which ? exp10(x[i]) : cl_exp10(x[i]);
+}
+}  // namespace cl
+
+extern "C" int cl_math_exp10(const double* x, double* y, int64_t n, int32_t which) {
+    if (!x || !y || n < 0) { set_error("null argument"); return CL_ERR_ARG; }
+    if (n == 0) return CL_OK;
+    double* d = nullptr;
+    CL_CUDA(cudaMalloc(&d, sizeof(double) * 2 * n));
+    cudaError_t e = cudaMemcpy(d, x, sizeof(double) * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        cl::exp10_check_kernel<<<cl::grid_for(n, 256, 148 * 8), 256>>>(d, d + n, n, which);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(y, d + n, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    return e == cudaSuccess ? CL_OK : cl::cuda_fail(e, "cl_math_exp10");
+}

@@ -23,6 +23,7 @@
 // to the residual tolerance.
 #include "internal.h"
 #include "speciation_large.h"
+#include "newton.cuh"
 
 namespace cl {
 
@@ -57,7 +58,7 @@ __device__ __forceinline__ void lg_species(const LgTableau& e, const double* St,
             for (int j = 0; j < e.nc; ++j) lc = fma(St[j * e.ns + i], xs[j], lc);
             if (lc > 1.0) c = 10.0;
             else if (lc < -30.0) c = 1e-30;
-            else { c = exp10(lc); cj = c; }
+            else { c = cl_exp10(lc); cj = c; }
         }
         W.c[i] = c;
         W.cj[i] = cj;

@@ -262,6 +262,9 @@ int     cl_device_bytes(const cl_ctx* ctx, uint64_t* bytes);
 /* sizeof of the ABI structs, for binding checks: [cl_config, cl_rxn,
  * cl_eq_system, cl_phase, cl_surrogate_net]; returns how many were written */
 int     cl_abi_sizes(int32_t* sizes, int32_t n);
+/* the FP64 10^x the Newton solves use (which = 0) or CUDA's exp10 (which = 1)
+ * on n host values, for accuracy checks; no counterpart in the reference */
+int     cl_math_exp10(const double* x, double* y, int64_t n, int32_t which);
 
 /* geometry: one material number per site, 0..255 (readGeometry, src/complab_functions.hh:127-156) */
 int cl_upload_mask(cl_ctx* ctx, const uint8_t* mask);
