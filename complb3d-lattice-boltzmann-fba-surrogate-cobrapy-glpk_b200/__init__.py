@@ -24,7 +24,7 @@ OK, WARN_NOT_CONVERGED = 0, 1
 ERR_ARG, ERR_CUDA, ERR_STATE, ERR_NOMEM, ERR_DIVERGED = -1, -2, -3, -4, -5
 BC_DIRICHLET, BC_NEUMANN = 0, 1
 FIELD_CONC, FIELD_BIOMASS, FIELD_VELOCITY, FIELD_FLOW_RHO, FIELD_FLOW_U, FIELD_PHASE, FIELD_EQ_ITERS = range(7)
-FIELD_CA_AGE, FIELD_CA_TOTAL = 7, 8
+FIELD_CA_AGE, FIELD_CA_TOTAL, FIELD_EQ_START = 7, 8, 9
 RED_SUM, RED_MIN, RED_MAX, RED_COUNT_EQ = range(4)
 EQ_START_COLD, EQ_START_GIVEN, EQ_START_LEARNED = range(3)
 EQ_SOLVER_NEWTON, EQ_SOLVER_PCF = 0, 1
@@ -127,6 +127,7 @@ def load_library(path=LIB_PATH):
         ("cl_step", [vp, c_int32]), ("cl_get_field", [vp, c_int32, c_int32, vp]),
         ("cl_set_field", [vp, c_int32, c_int32, vp]), ("cl_get_flow_populations", [vp, vp]),
         ("cl_set_flow_populations", [vp, vp]), ("cl_get_solute_populations", [vp, c_int32, vp]),
+        ("cl_set_solute_populations", [vp, c_int32, vp]),
         ("cl_reduce", [vp, c_int32, c_int32, c_int32, c_double, P(c_double)]),
         ("cl_precip_convert", [vp, P(c_int64)]), ("cl_dissol_convert", [vp, P(c_int64)]),
         ("cl_flow_velocity_stats", [vp, P(c_double), P(c_double), P(c_double)]),
@@ -386,6 +387,11 @@ class Lattice:
         out = np.empty(7 * self.N, np.float32)
         self._c(self.lib.cl_get_solute_populations(self.h, s, _ptr(out)), "cl_get_solute_populations")
         return out.reshape(7, self.N)
+
+    def set_solute_populations(self, s, g):
+        v = np.ascontiguousarray(g, dtype=np.float32).reshape(-1)
+        assert v.size == 7 * self.N
+        self._c(self.lib.cl_set_solute_populations(self.h, s, _ptr(v)), "cl_set_solute_populations")
 
     def reduce(self, field, index, op, arg=0.0):
         out = c_double(0)

@@ -726,6 +726,10 @@ int cl_get_field(cl_ctx* h, int32_t field, int32_t index, double* out) {
             if (!c->d_eq_iters) return CL_ERR_STATE;
             i2d_kernel<<<blocks, 256, 0, c->stream>>>(c->d_eq_iters, d, N);
             break;
+        case CL_FIELD_EQ_START:
+            if (!c->ade_ready) return CL_ERR_STATE;
+            r = eq_start_io(c, index, d, 1);
+            break;
         case CL_FIELD_PHASE:
             if (!c->d_phase) { set_error("dissolution is not enabled in this context"); return CL_ERR_STATE; }
             u2d_kernel<<<blocks, 256, 0, c->stream>>>(c->d_phase, d, N);
@@ -776,6 +780,12 @@ int cl_set_field(cl_ctx* h, int32_t field, int32_t index, const double* in) {
             if (index < 0 || index > 2) return CL_ERR_ARG;
             d2f_kernel<<<blocks, 256, 0, c->stream>>>(d, c->d_u + index * N, N);
             break;
+        case CL_FIELD_EQ_START: {
+            if (!c->ade_ready) return CL_ERR_STATE;
+            const int r2 = eq_start_io(c, index, d, 0);
+            if (r2) return r2;
+            break;
+        }
         case CL_FIELD_PHASE: {
             if (!c->d_phase) { set_error("dissolution is not enabled in this context"); return CL_ERR_STATE; }
             int* d_bad = reinterpret_cast<int*>(c->d_scratch + N);
@@ -826,6 +836,20 @@ int cl_set_flow_populations(cl_ctx* h, const float* in) {
     if (!r) { e = cudaStreamSynchronize(c->stream); if (e != cudaSuccess) r = cuda_fail(e, "sync"); }
     cudaFree(tmp);
     if (!r) c->flow_ready = true;
+    return r;
+}
+
+int cl_set_solute_populations(cl_ctx* h, int32_t s, const float* in) {
+    if (!h || !in) return CL_ERR_ARG;
+    Ctx* c = &h->c;
+    if (!c->ade_ready) { set_error("call cl_ade_init first"); return CL_ERR_STATE; }
+    if (s < 0 || s >= c->ap.S || c->ap.mob_slot[s] < 0) { set_error("not a mobile solute"); return CL_ERR_ARG; }
+    const int64_t N = c->geo.N;
+    float* tmp = nullptr;
+    CL_CUDA(cudaMalloc(&tmp, sizeof(float) * 7 * N));
+    cudaError_t e = cudaMemcpyAsync(tmp, in, sizeof(float) * 7 * N, cudaMemcpyHostToDevice, c->stream);
+    int r = e == cudaSuccess ? ade_population_set(c, c->ap.mob_slot[s], tmp) : cuda_fail(e, "cl_set_solute_populations");
+    cudaFree(tmp);
     return r;
 }
 

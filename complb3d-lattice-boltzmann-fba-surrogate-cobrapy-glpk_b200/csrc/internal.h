@@ -216,7 +216,11 @@ int phase_fill(Ctx* c);          // grain inventories (initial_fill) after ade_i
 int refresh_flags(Ctx* c);       // class flags after a mask / phase change, dynamics kept
 int build_live_list(Ctx* c);    // the live interior sites of the transport classes, in site order
 int build_flow_list(Ctx* c);    // the flow sites that stream (not bounce-back), in site order
-int store_update(Ctx* c, int all); // store the sites the transport now needs (all: every site)
+// store the sites the transport now needs (all: every site; extra: a device
+// byte per site, nonzero where a site must be stored as well)
+int store_update(Ctx* c, int all, const uint8_t* extra = nullptr);
+int ade_population_set(Ctx* c, int slot, const float* d_nat);   // natural order -> storage
+int eq_start_io(Ctx* c, int j, double* d_nat, int to_natural);   // Newton warm start j <-> natural order
 // storage indices for the sites flagged in need, after the *n_stored assigned
 int assign_storage(Ctx* c, const uint8_t* need, int32_t* sidx, uint32_t* site_of, int64_t* n_stored,
                    int64_t* first, int64_t* added);

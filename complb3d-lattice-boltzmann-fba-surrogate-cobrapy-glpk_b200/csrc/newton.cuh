@@ -131,12 +131,11 @@ struct TabFixed {
 // reduction y = x log2(10) = n + f with n = rint(y), |f| <= 1/2, the
 // product carried as an exact two-term sum (Dekker's FMA split, with the
 // tail of log2(10)); 2^f = e^t, t = f ln 2, by the Taylor series to degree 13
-// (|t| <= 0.347, truncation below 5e-18) evaluated in Estrin's scheme, so the
-// dependent chain is five operations deep; the result scaled by 2^n through
-// the exponent field.  Arguments outside |x| < 300 (never reached by the
-// clamped logs) go to the library's exp10.
+// in Horner's form (|t| <= 0.347, truncation below 5e-18); the result scaled
+// by 2^n through the exponent field.  Domain |x| < 300 (every caller clamps
+// its logs to [-30, 1]); NaN gives NaN.  Measured on the coupled step it is
+// 2 % faster than the library's exp10 (whose wider domain costs more).
 __device__ __forceinline__ double cl_exp10(double x) {
-    if (!(fabs(x) < 300.0)) return exp10(x);
     constexpr double kL2T = 3.321928094887362, kL2T_lo = 1.661617516973592e-16;   // log2(10) = kL2T + kL2T_lo
     constexpr double kLn2 = 0.6931471805599453, kLn2_lo = 2.3190468138462996e-17;
     const double yh = x * kL2T;
@@ -144,17 +143,20 @@ __device__ __forceinline__ double cl_exp10(double x) {
     const double n = rint(yh);
     const double f = (yh - n) + yl;                  // yh - n is exact
     const double t = fma(f, kLn2, f * kLn2_lo);
-    const double t2 = t * t, t4 = t2 * t2, t8 = t4 * t4;
-    const double p01 = fma(t, 1.0, 1.0);
-    const double p23 = fma(t, 1.0 / 6.0, 0.5);
-    const double p45 = fma(t, 1.0 / 120.0, 1.0 / 24.0);
-    const double p67 = fma(t, 1.0 / 5040.0, 1.0 / 720.0);
-    const double p89 = fma(t, 1.0 / 362880.0, 1.0 / 40320.0);
-    const double pab = fma(t, 1.0 / 39916800.0, 1.0 / 3628800.0);
-    const double pcd = fma(t, 1.0 / 6227020800.0, 1.0 / 479001600.0);
-    const double q0 = fma(p23, t2, p01), q1 = fma(p67, t2, p45), q2 = fma(pab, t2, p89);
-    const double r0 = fma(q1, t4, q0), r1 = fma(pcd, t4, q2);
-    const double p = fma(r1, t8, r0);
+    double p = 1.0 / 6227020800.0;                   // 1/13!
+    p = fma(p, t, 1.0 / 479001600.0);
+    p = fma(p, t, 1.0 / 39916800.0);
+    p = fma(p, t, 1.0 / 3628800.0);
+    p = fma(p, t, 1.0 / 362880.0);
+    p = fma(p, t, 1.0 / 40320.0);
+    p = fma(p, t, 1.0 / 5040.0);
+    p = fma(p, t, 1.0 / 720.0);
+    p = fma(p, t, 1.0 / 120.0);
+    p = fma(p, t, 1.0 / 24.0);
+    p = fma(p, t, 1.0 / 6.0);
+    p = fma(p, t, 1.0 / 2.0);
+    p = fma(p, t, 1.0);
+    p = fma(p, t, 1.0);
     const long long e = (long long)n + 1023;
     return p * __longlong_as_double(e << 52);
 }

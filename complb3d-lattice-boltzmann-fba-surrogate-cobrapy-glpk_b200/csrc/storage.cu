@@ -31,12 +31,12 @@ __device__ __forceinline__ bool ade_live(uint8_t cls, int nodyn_coupled) {
 
 // need[n] = 1 when site n has no storage yet and is live, next to a live site, or all is set
 __global__ void store_need_kernel(Geo g, const uint8_t* cls, int nodyn_coupled, int all, const int32_t* sidx,
-                                  uint8_t* need) {
+                                  const uint8_t* extra, uint8_t* need) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < g.N; n += stride) {
         bool nd = false;
         if (sidx[n] < 0) {
-            if (all || ade_live(cls[n], nodyn_coupled)) nd = true;
+            if (all || ade_live(cls[n], nodyn_coupled) || (extra && extra[n])) nd = true;
             else {
                 int x, y, z;
                 decode(g, n, x, y, z);
@@ -132,7 +132,7 @@ int assign_storage(Ctx* c, const uint8_t* need, int32_t* sidx, uint32_t* site_of
     return CL_OK;
 }
 
-int store_update(Ctx* c, int all) {
+int store_update(Ctx* c, int all, const uint8_t* extra) {
     const int64_t N = c->geo.N;
     if (!c->d_sidx) {
         int r = CL_OK;
@@ -143,7 +143,7 @@ int store_update(Ctx* c, int all) {
     if (c->n_stored == N) { c->store_dirty = false; return CL_OK; }
     uint8_t* need = reinterpret_cast<uint8_t*>(c->d_scratch);            // N bytes
     store_need_kernel<<<grid_for(N, 256, 148 * 16), 256, 0, c->stream>>>(
-        c->geo, c->d_ade_cls, c->ade_nodyn_coupled ? 1 : 0, all, c->d_sidx, need);
+        c->geo, c->d_ade_cls, c->ade_nodyn_coupled ? 1 : 0, all, c->d_sidx, extra, need);
     CL_LAUNCH_CHECK("store_need_kernel");
     int64_t first = 0, total = 0;
     int r = assign_storage(c, need, c->d_sidx, c->d_site_of, &c->n_stored, &first, &total);

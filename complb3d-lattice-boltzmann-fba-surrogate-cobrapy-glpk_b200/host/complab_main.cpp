@@ -2,7 +2,12 @@
 // (src/complab.cpp:560-1860) over the C ABI, fields out.
 //
 //   complab_b200 [CompLaB.xml] [--steps N] [--eq-solver newton|pcf] [--rates rates.xml]
-//                [--dump-config FILE] [--print-config] [--quiet]
+//                [--restart DIR] [--dump-config FILE] [--print-config] [--quiet]
+//
+// Output: at every <save_VTK_interval> and at the end, the fields as raw FP64
+// arrays and as the reference's VTI files; at every <save_CHK_interval> a
+// checkpoint folder chk_<steps>/ (formats: complab_io.h), which --restart
+// resumes from (the configuration still comes from CompLaB.xml).
 //
 // --rates supplies the rate-law blocks (<rate_table>, dissolution <rate_k> ...)
 // that the main file lacks; --dump-config writes the cl_config the transport
@@ -38,6 +43,7 @@
 #include <vector>
 
 #include "../../include/complab_gpu.h"
+#include "complab_io.h"
 #include "complab_xml.h"
 
 using clhost::HostRun;
@@ -90,8 +96,25 @@ bool write_fields(cl_ctx* h, const HostRun& run, long iT, std::vector<std::strin
         index.push_back(fn);
         return (bool)o;
     };
-    for (int s = 0; s < c.n_solutes; ++s) if (!dump(CL_FIELD_CONC, s, run.subs_names[s])) return false;
-    for (int m = 0; m < c.n_microbes; ++m) if (!dump(CL_FIELD_BIOMASS, m, run.microbe_names[m])) return false;
+    // the reference's VTI files (writeAdvVTI, writeNsVTI) beside the raw arrays
+    std::string err;
+    auto vti = [&](const std::string& prefix, std::vector<clhost::VtiArray> arrays) {
+        const std::string fn = clhost::vti_name(prefix, iT);
+        if (!clhost::write_vti(run.output_dir + "/" + fn, c.nx, c.ny, c.nz, arrays, err)) {
+            std::fprintf(stderr, "complab_b200: %s\n", err.c_str());
+            return false;
+        }
+        index.push_back(fn);
+        return true;
+    };
+    for (int s = 0; s < c.n_solutes; ++s) {
+        if (!dump(CL_FIELD_CONC, s, run.subs_names[s])) return false;
+        if (!vti(run.subs_names[s] + "_", {{"Density", 1, true, buf}})) return false;
+    }
+    for (int m = 0; m < c.n_microbes; ++m) {
+        if (!dump(CL_FIELD_BIOMASS, m, run.microbe_names[m])) return false;
+        if (!vti(run.microbe_names[m] + "_", {{"Density", 1, true, buf}})) return false;
+    }
     // the material numbers (uint8), which precipitation and dissolution change
     std::vector<uint8_t> mask(N);
     if (!check(cl_download_mask(h, mask.data()), "cl_download_mask")) return false;
@@ -99,7 +122,18 @@ bool write_fields(cl_ctx* h, const HostRun& run, long iT, std::vector<std::strin
     std::ofstream o(run.output_dir + "/" + fn, std::ios::binary);
     o.write(reinterpret_cast<const char*>(mask.data()), (std::streamsize)N);
     index.push_back(fn);
-    return (bool)o;
+    if (!o) return false;
+    if (!vti(run.mask_filename + "_", {{"Density", 1, true, std::vector<double>(mask.begin(), mask.end())}}))
+        return false;
+    if (run.Pe > kThrd) {
+        std::vector<double> u(3 * N), norm(N);
+        for (int k = 0; k < 3; ++k)
+            if (!check(cl_get_field(h, CL_FIELD_FLOW_U, k, u.data() + (size_t)k * N), "cl_get_field")) return false;
+        for (size_t n = 0; n < N; ++n)
+            norm[n] = std::sqrt(u[n] * u[n] + u[N + n] * u[N + n] + u[2 * N + n] * u[2 * N + n]);
+        if (!vti("nsLattice_", {{"velocityNorm", 1, false, norm}, {"velocity", 3, false, u}})) return false;
+    }
+    return true;
 }
 
 // the configuration as raw cl_config bytes and the geometry as read
@@ -155,7 +189,7 @@ bool weighted_pore_mean(cl_ctx* h, const cl_config& c, const HostRun& run, doubl
 }  // namespace
 
 int main(int argc, char** argv) {
-    std::string xml = "CompLaB.xml", rates, dump;
+    std::string xml = "CompLaB.xml", rates, dump, restart;
     long steps_override = -1;
     int eq_solver = -1;
     bool print_config = false, quiet = false;
@@ -166,13 +200,14 @@ int main(int argc, char** argv) {
         else if (a == "--steps" && i + 1 < argc) steps_override = std::atol(argv[++i]);
         else if (a == "--rates" && i + 1 < argc) rates = argv[++i];
         else if (a == "--dump-config" && i + 1 < argc) dump = argv[++i];
+        else if (a == "--restart" && i + 1 < argc) restart = argv[++i];
         else if (a == "--eq-solver" && i + 1 < argc && (std::strcmp(argv[i + 1], "pcf") == 0 ||
                                                          std::strcmp(argv[i + 1], "newton") == 0))
             eq_solver = std::strcmp(argv[++i], "pcf") == 0 ? CL_EQ_SOLVER_PCF : CL_EQ_SOLVER_NEWTON;
         else if (!a.empty() && a[0] != '-') xml = a;
         else {
             std::fprintf(stderr, "usage: %s [CompLaB.xml] [--steps N] [--eq-solver newton|pcf] [--rates rates.xml] "
-                         "[--dump-config FILE] [--print-config] [--quiet]\n",
+                         "[--restart DIR] [--dump-config FILE] [--print-config] [--quiet]\n",
                          argv[0]);
             return 2;
         }
@@ -198,6 +233,20 @@ int main(int argc, char** argv) {
         std::printf("%s\n", clhost::run_json(run).c_str());
         return dump_config(dump, c, mask) ? 0 : 1;
     }
+    // a restart takes the geometry (as it was when saved), the calibrated
+    // pressure, dt and relaxation from the checkpoint
+    clhost::Checkpoint chk;
+    if (!restart.empty()) {
+        if (!clhost::read_checkpoint(restart, run, chk, mask, err)) {
+            std::fprintf(stderr, "complab_b200: %s\n", err.c_str());
+            return 1;
+        }
+        c.rho_in = chk.rho_in;
+        c.rho_out = chk.rho_out;
+        c.dt = chk.dt;
+        run.delta_P = chk.delta_P;
+        for (int s = 0; s < c.n_solutes; ++s) { c.omega_pore[s] = chk.omega_pore[s]; c.omega_bio[s] = chk.omega_bio[s]; }
+    }
     const auto t0 = std::chrono::steady_clock::now();
     int st = 0;
     Ctx ctx;
@@ -211,7 +260,11 @@ int main(int argc, char** argv) {
     double pore_mean_u = 0.0, max_ux = 0.0, outlet_ux = 0.0, pe_achieved = 0.0;
     int ns_iters = 0;
     if (!check(cl_flow_init(h), "cl_flow_init")) return 1;
-    if (run.Pe > kThrd) {
+    if (!restart.empty() && chk.has_flow && !clhost::restore_flow(h, run, restart, err)) {
+        std::fprintf(stderr, "complab_b200: %s\n", err.c_str());
+        return 1;
+    }
+    if (run.Pe > kThrd && restart.empty()) {
         if (!flow_solve(h, run.ns_max1, run.ns_conv1, &ns_iters)) return 1;
         if (!check(cl_flow_velocity_stats(h, &pore_mean_u, &max_ux, &outlet_ux), "cl_flow_velocity_stats")) return 1;
         // with sessile microbes the first solve's pore mean is the count-weighted
@@ -250,7 +303,9 @@ int main(int argc, char** argv) {
 
     // solute relaxation and dt from the flow (complab.cpp:708-727)
     const int S = c.n_solutes;
-    if (S > 0) {
+    if (S > 0 && !restart.empty()) {
+        if (!check(cl_set_transport(h, c.omega_pore, c.omega_bio, c.dt), "cl_set_transport")) return 1;
+    } else if (S > 0) {
         double refNu, refTau;
         if (run.Pe > kThrd) {
             refNu = pore_mean_u * run.charcs_length / run.Pe;
@@ -274,8 +329,12 @@ int main(int argc, char** argv) {
     if (run.Pe > kThrd && !check(cl_couple_velocity(h), "cl_couple_velocity")) return 1;
     if (!check(cl_ade_init(h), "cl_ade_init")) return 1;
     if (!dump.empty() && !dump_config(dump, c, mask)) return 1;
+    if (!restart.empty() && !clhost::restore_transport(h, run, restart, err)) {
+        std::fprintf(stderr, "complab_b200: %s\n", err.c_str());
+        return 1;
+    }
     // sessile biomass on the microbes' materials (initializeScalarLattice3D)
-    {
+    if (restart.empty()) {
         const size_t N = mask.size();
         std::vector<double> b(N);
         for (int m = 0; m < c.n_microbes; ++m) {
@@ -312,7 +371,7 @@ int main(int argc, char** argv) {
     long nonconv_steps = 0, precip_changes = 0, dissol_changes = 0, steps_done = 0;
     const char* stopped = "";
     const auto t1 = std::chrono::steady_clock::now();
-    for (long iT = 0; iT < run.ade_max; ++iT) {
+    for (long iT = restart.empty() ? 0 : chk.steps; iT < run.ade_max; ++iT) {
         st = cl_step(h, 1);
         if (!check(st, "cl_step")) return 1;
         ++steps_done;
@@ -365,6 +424,23 @@ int main(int argc, char** argv) {
             ++resolves;
         }
         if (run.vtk_interval > 0 && iT % run.vtk_interval == 0 && !write_fields(h, run, iT, index)) return 1;
+        // checkpoint of the state after iT + 1 steps (the reference's save_CHK_interval)
+        if (run.chk_interval > 0 && (iT + 1) % run.chk_interval == 0) {
+            clhost::Checkpoint now;
+            now.steps = iT + 1;
+            now.rho_in = c.rho_in;
+            now.rho_out = c.rho_out;
+            now.dt = c.dt;
+            now.delta_P = run.delta_P;
+            now.omega_pore.assign(c.omega_pore, c.omega_pore + c.n_solutes);
+            now.omega_bio.assign(c.omega_bio, c.omega_bio + c.n_solutes);
+            now.has_flow = run.Pe > kThrd;
+            const std::string dir = run.output_dir + "/chk_" + std::to_string(iT + 1);
+            if (!clhost::save_checkpoint(h, run, now, dir, err)) {
+                std::fprintf(stderr, "complab_b200: %s\n", err.c_str());
+                return 1;
+            }
+        }
     }
     const auto t2 = std::chrono::steady_clock::now();
     if (!*stopped && !write_fields(h, run, run.ade_max, index)) return 1;

@@ -173,6 +173,8 @@ int read_complab_xml(const std::string& path, HostRun& run, std::string& err, co
             run.ade_update_interval = std::max(1L, (long)num_or(*it, {"ade_update_interval"}, 1));
         }
         run.vtk_interval = (long)num_or(P, {"IO", "save_VTK_interval"}, 0);
+        run.chk_interval = (long)num_or(P, {"IO", "save_CHK_interval"}, 0);
+        if (const XmlNode* mf = opt(P, {"IO", "mask_filename"})) run.mask_filename = mf->str();
 
         // substrates (complab_functions.hh:1031-1048; immobile complab.cpp:244-266)
         for (int s = 0; s < S; ++s) {
@@ -397,7 +399,7 @@ std::string run_json(const HostRun& r) {
       << ", \"ade_max_iT\": " << r.ade_max << ", \"ns_update_interval\": " << r.ns_update_interval
       << ", \"ade_update_interval\": " << r.ade_update_interval << ", \"ns_max_iT2\": " << r.ns_max2
       << ", \"ns_converge_iT2\": " << r.ns_conv2 << ", \"precip_interval\": " << r.precip_interval
-      << ", \"dissol_interval\": " << r.dissol_interval << ", \"vtk_interval\": " << r.vtk_interval
+      << ", \"dissol_interval\": " << r.dissol_interval << ", \"vtk_interval\": " << r.vtk_interval << ", \"chk_interval\": " << r.chk_interval
       << ", \"n_solutes\": " << c.n_solutes << ", \"names\": [";
     for (size_t i = 0; i < r.subs_names.size(); ++i) o << (i ? ", " : "") << "\"" << r.subs_names[i] << "\"";
     o << "], \"c0\": ";

@@ -28,7 +28,8 @@ struct HostRun {
     long ns_max1 = 100000, ns_max2 = 100000, ade_max = 10000000;
     long ns_update_interval = 1, ade_update_interval = 1;   // geometry-change dynamics / flow updates
     double ns_conv1 = 1e-8, ns_conv2 = 1e-6;
-    long vtk_interval = 0;
+    long vtk_interval = 0, chk_interval = 0;     // <IO> save_VTK_interval, save_CHK_interval
+    std::string mask_filename = "maskLattice";
     // chemistry / microbiology
     std::vector<std::string> subs_names, microbe_names;
     std::vector<double> D_pore, D_bfilm;

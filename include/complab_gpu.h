@@ -401,10 +401,12 @@ int cl_set_field(cl_ctx* ctx, int32_t field, int32_t index, const double* host_i
 /* raw populations (debug/parity, checkpoints): flow 19*N floats as deviations
  * f-t_i in the natural (post-stream) order; solute s: 7*N floats of g_i.
  * Reading the flow needs a flow field (cl_flow_init or a set), setting it the
- * mask (CL_ERR_STATE otherwise). */
+ * mask (CL_ERR_STATE otherwise); setting a solute's needs cl_ade_init.  A
+ * get followed by a set restores the state bit for bit, at either parity. */
 int cl_get_flow_populations(cl_ctx* ctx, float* host_out);
 int cl_set_flow_populations(cl_ctx* ctx, const float* host_in);
 int cl_get_solute_populations(cl_ctx* ctx, int32_t s, float* host_out);
+int cl_set_solute_populations(cl_ctx* ctx, int32_t s, const float* host_in);
 
 /* ---- measurement ----------------------------------------------------------------
  * CUDA events recorded on the context's stream around every launch of the
@@ -447,6 +449,11 @@ int cl_ca_update_mask(cl_ctx* ctx, int64_t* mask_changes);
 /* the age field (read) as FP64 */
 #define CL_FIELD_CA_AGE    7
 #define CL_FIELD_CA_TOTAL  8   /* total biomass the CA last computed */
+/* the Newton warm starts of the transport step (eq_warm_previous), read and
+ * written for checkpoints: index j < n_comp the last converged log10 free
+ * component j of each site, n_comp <= j < 2 n_comp the one before; NaN where
+ * a site has none (stored in FP32) */
+#define CL_FIELD_EQ_START  9
 
 /* ---- reductions ----------------------------------------------------- */
 #define CL_RED_SUM   0
