@@ -100,7 +100,7 @@ class Config(ctypes.Structure):
         ("n_srg", c_int32), ("srg", SrgOrganism * MAX_SRG_ORG),
         ("ca_enabled", c_int32), ("ca_half", c_int32), ("ca_bmax", c_double), ("ca_thrd_frac", c_double),
         ("microbe_code", c_int32 * MAX_MICROBES), ("ca_seed", ctypes.c_uint64),
-        ("rate_law", c_int32),
+        ("rate_law", c_int32), ("microbe_carrier", c_int32 * MAX_MICROBES),
     ]
 
 

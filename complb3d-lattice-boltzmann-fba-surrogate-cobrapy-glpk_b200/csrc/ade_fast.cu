@@ -355,6 +355,8 @@ int fast_step(Ctx* c) {
 }
 
 int chem_match(const cl_config& cfg) {
+    // microbes solved by LBM run the rate table's launches
+    for (int m = 0; m < CL_MAX_MICROBES; ++m) if (cfg.microbe_carrier[m]) return 0;
     if (ChemCoupled::matches(cfg)) return ChemCoupled::kId;
     if (ChemBiotic4::matches(cfg)) return ChemBiotic4::kId;
     if (ChemZhao24::matches(cfg)) return ChemZhao24::kId;

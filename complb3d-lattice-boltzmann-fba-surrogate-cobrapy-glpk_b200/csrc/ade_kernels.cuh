@@ -304,7 +304,11 @@ static __device__ __noinline__ void surrogate_chain(const AdeParams& p, const do
 __device__ __forceinline__ void kinetics_increments(const AdeParams& p, const double* bio, int64_t N, int64_t n,
                                                     const double* Cur, int cs, double* R, double* B, double* BR,
                                                     int bd, int ops = 15) {
-    for (int m = 0; m < p.M; ++m) { const double b = bio[m * N + n]; B[m * bd] = b < THRD ? 0.0 : b; }
+    for (int m = 0; m < p.M; ++m) {
+        // a microbe solved by LBM: its biomass is its carrier solute's density
+        const double b = p.carrier[m] >= 0 ? Cur[p.carrier[m] * cs] : bio[m * N + n];
+        B[m * bd] = b < THRD ? 0.0 : b;
+    }
     if (p.do_kin && (ops & 1)) {
         rates_dev(p, 0, Cur, cs, B, R, BR, bd);
         for (int s = 0; s < p.S; ++s) {
@@ -315,6 +319,11 @@ __device__ __forceinline__ void kinetics_increments(const AdeParams& p, const do
             const double d = BR[m * bd] * p.dt;
             BR[m * bd] = (d > THRD || d < -THRD) ? d : 0.0;
         }
+        // the dB of a microbe solved by LBM goes to its lattice (update_rxnLattices
+        // adds the bFree lattices' dB as it adds the solutes' dC)
+        if (p.n_carried)
+            for (int m = 0; m < p.M; ++m)
+                if (p.carrier[m] >= 0) { R[p.carrier[m] * bd] += BR[m * bd]; BR[m * bd] = 0.0; }
     } else {
         for (int s = 0; s < p.S; ++s) R[s * bd] = 0.0;
         for (int m = 0; m < p.M; ++m) BR[m * bd] = 0.0;

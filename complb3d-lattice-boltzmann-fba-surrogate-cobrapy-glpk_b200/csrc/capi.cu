@@ -53,6 +53,18 @@ static int validate(const cl_config* c) {
     if (c->n_microbes < 0 || c->n_microbes > CL_MAX_MICROBES) { set_error("n_microbes out of range"); return CL_ERR_ARG; }
     if (c->n_rxn < 0 || c->n_rxn > CL_MAX_RXN) { set_error("n_rxn out of range"); return CL_ERR_ARG; }
     if (c->rate_law != CL_RATELAW_TABLE && c->rate_law != CL_RATELAW_ZHAO) { set_error("unknown rate_law"); return CL_ERR_ARG; }
+    for (int m = 0; m < CL_MAX_MICROBES; ++m) {
+        const int cs = c->microbe_carrier[m];
+        if (cs == 0) continue;
+        if (m >= c->n_microbes || cs < 0 || cs > c->n_solutes || c->immobile[cs - 1]) {
+            set_error("microbe_carrier must name a mobile solute (index + 1) of an existing microbe");
+            return CL_ERR_ARG;
+        }
+        if (c->rate_law != CL_RATELAW_TABLE || c->n_srg > 0 || (c->ca_enabled && c->microbe_code[m] > 0)) {
+            set_error("a microbe carried by a solute runs the rate table only (no surrogate, no CA on it)");
+            return CL_ERR_ARG;
+        }
+    }
     {
         const int64_t N = (int64_t)c->nx * c->ny * c->nz;
         if (N * 19 >= (int64_t)1 << 32) { set_error("lattice too large: 19*nx*ny*nz must stay below 2^32"); return CL_ERR_ARG; }
@@ -208,6 +220,11 @@ cl_ctx* cl_create(const cl_config* cfg, void* stream, int* status) {
     p.n_rxn = cfg->n_rxn;
     for (int k = 0; k < cfg->n_rxn; ++k) p.rxn[k] = cfg->rxn[k];
     for (int m = 0; m < CL_MAX_MICROBES; ++m) p.decay[m] = cfg->decay[m];
+    p.n_carried = 0;
+    for (int m = 0; m < CL_MAX_MICROBES; ++m) {
+        p.carrier[m] = m < cfg->n_microbes ? cfg->microbe_carrier[m] - 1 : -1;
+        if (p.carrier[m] >= 0) ++p.n_carried;
+    }
     p.eq.n_comp = cfg->eq.n_comp;
     p.eq.n_species = cfg->eq.n_species;
     p.eq.max_iter = cfg->eq.max_iter;

@@ -64,6 +64,8 @@ struct AdeParams {
     int    n_rxn;
     cl_rxn rxn[CL_MAX_RXN];
     double decay[CL_MAX_MICROBES];
+    int    carrier[CL_MAX_MICROBES];   // solute whose density is microbe m's biomass, or -1 (sessile)
+    int    n_carried;
     EqParams eq;
     int    solid_code, bb_code;
     int    n_srg;

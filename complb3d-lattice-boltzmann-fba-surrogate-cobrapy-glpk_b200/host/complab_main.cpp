@@ -112,6 +112,7 @@ bool write_fields(cl_ctx* h, const HostRun& run, long iT, std::vector<std::strin
         if (!vti(run.subs_names[s] + "_", {{"Density", 1, true, buf}})) return false;
     }
     for (int m = 0; m < c.n_microbes; ++m) {
+        if (c.microbe_carrier[m]) continue;      // written as its carrier solute
         if (!dump(CL_FIELD_BIOMASS, m, run.microbe_names[m])) return false;
         if (!vti(run.microbe_names[m] + "_", {{"Density", 1, true, buf}})) return false;
     }
@@ -319,7 +320,7 @@ int main(int argc, char** argv) {
         for (int s = 0; s < S; ++s) {
             const double nu = refNu * run.D_pore[s] / run.D_pore[0];
             om_p[s] = 1.0 / (nu * 4.0 + 0.5);
-            om_b[s] = 1.0 / (refNu * run.D_bfilm[s] / run.D_pore[0] * 4.0 + 0.5);
+            om_b[s] = 1.0 / (refNu * run.D_bfilm[s] / run.D_bfilm_ref[s] * 4.0 + 0.5);
         }
         const double dt = refNu * run.dx * run.dx / run.D_pore[0];
         c.dt = dt;
@@ -338,6 +339,7 @@ int main(int argc, char** argv) {
         const size_t N = mask.size();
         std::vector<double> b(N);
         for (int m = 0; m < c.n_microbes; ++m) {
+            if (c.microbe_carrier[m]) continue;      // an LBM-solved microbe starts as its carrier's c0
             std::fill(b.begin(), b.end(), 0.0);
             const auto& mats = run.bio_materials[m];
             const auto& b0 = run.b0[m];

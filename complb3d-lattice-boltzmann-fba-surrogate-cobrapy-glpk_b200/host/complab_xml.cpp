@@ -95,7 +95,7 @@ int read_complab_xml(const std::string& path, HostRun& run, std::string& err, co
         double dx = dom["dx"].num();
         run.geom_file = dom["filename"].str();
         const XmlNode& chem = P["chemistry"];
-        const int S = (int)chem["number_of_substrates"].integer();
+        int S = (int)chem["number_of_substrates"].integer();
         if (S < 0 || S > CL_MAX_SOLUTES) throw std::runtime_error("number_of_substrates out of range");
         c.n_solutes = S;
         for (int s = 0; s < S; ++s) {
@@ -106,7 +106,9 @@ int read_complab_xml(const std::string& path, HostRun& run, std::string& err, co
             c.right_value[s] = sub["right_boundary_condition"].num();
         }
 
-        // microbiology (CA-solved sessile biomass only)
+        // microbiology: CA-solved sessile biomass, or LBM-solved biomass
+        // carried by an extra mobile solute (a planktonic bFree lattice,
+        // complab.cpp:788-797); finite-difference biomass is refused
         int M = 0;
         if (run.biotic_mode) {
             const XmlNode& mic = P["microbiology"];
@@ -115,10 +117,10 @@ int read_complab_xml(const std::string& path, HostRun& run, std::string& err, co
             for (int m = 0; m < M; ++m) {
                 const XmlNode& mb = mic["microbe" + std::to_string(m)];
                 const std::string st = lower(mb["solver_type"].str());
-                if (st == "fd" || st == "finite difference" || st == "finite_difference" ||
-                    st == "lbm" || st == "lb" || st == "lattice boltzmann")
+                if (st == "fd" || st == "finite difference" || st == "finite_difference")
                     throw std::runtime_error("microbe" + std::to_string(m) + ": solver_type " + mb["solver_type"].str() +
-                                             " (mobile biomass) is not part of this library; use CA");
+                                             " (finite-difference mobile biomass) is not part of this library; use CA or LBM");
+                run.carried.push_back(st == "lbm" || st == "lb" || st == "lattice boltzmann" ? 1 : 0);
                 run.b0.push_back(mb["initial_densities"].nums());
                 run.microbe_names.push_back(mb.has("name_of_microbes") ? mb["name_of_microbes"].str()
                                                                        : "microbe" + std::to_string(m));
@@ -185,7 +187,31 @@ int read_complab_xml(const std::string& path, HostRun& run, std::string& err, co
             run.D_bfilm.push_back(num_or(sub, {"substrate_diffusion_coefficients", "in_biofilm"}, 2e-10));
             c.c0[s] = num_or(sub, {"initial_concentration"}, 0.0);
             c.immobile[s] = sub.has("immobile") && sub["immobile"].flag() ? 1 : 0;
+            run.D_bfilm_ref.push_back(0.0);
         }
+        for (int s = 0; s < S; ++s) run.D_bfilm_ref[s] = run.D_pore[0];
+        // an LBM-solved microbe: one more mobile solute named after it, with
+        // its diffusion, its boundaries and its initial density everywhere
+        // (soluteDomainSetup with vec_b0_free, complab.cpp:791-792)
+        for (int m = 0; m < M; ++m) {
+            if (!run.carried[m]) continue;
+            if (S >= CL_MAX_SOLUTES) throw std::runtime_error("too many solutes with the LBM-solved microbes");
+            const XmlNode& mb = P["microbiology"]["microbe" + std::to_string(m)];
+            const int s = S++;
+            run.subs_names.push_back(run.microbe_names[m]);
+            const double dp = num_or(mb, {"biomass_diffusion_coefficients", "in_pore"}, 0.0);
+            run.D_pore.push_back(dp);
+            run.D_bfilm.push_back(num_or(mb, {"biomass_diffusion_coefficients", "in_biofilm"}, 0.0));
+            run.D_bfilm_ref.push_back(dp);
+            c.c0[s] = run.b0[m].empty() ? 0.0 : run.b0[m][0];
+            c.immobile[s] = 0;
+            c.left_type[s] = mb.has("left_boundary_type") ? bc_type(mb["left_boundary_type"]) : CL_BC_NEUMANN;
+            c.right_type[s] = mb.has("right_boundary_type") ? bc_type(mb["right_boundary_type"]) : CL_BC_NEUMANN;
+            c.left_value[s] = num_or(mb, {"left_boundary_condition"}, 0.0);
+            c.right_value[s] = num_or(mb, {"right_boundary_condition"}, 0.0);
+            c.microbe_carrier[m] = s + 1;
+        }
+        c.n_solutes = S;
         if (enable_abiotic && S < 1) throw std::runtime_error("abiotic kinetics needs at least one substrate");
 
         // flow numbers; the solute relaxation and dt follow from the flow
@@ -205,7 +231,7 @@ int read_complab_xml(const std::string& path, HostRun& run, std::string& err, co
         for (int s = 0; s < S; ++s) {
             const double nu = refNu * run.D_pore[s] / run.D_pore[0];
             c.omega_pore[s] = 1.0 / (nu * 4.0 + 0.5);
-            c.omega_bio[s] = 1.0 / (refNu * run.D_bfilm[s] / run.D_pore[0] * 4.0 + 0.5);
+            c.omega_bio[s] = 1.0 / (refNu * run.D_bfilm[s] / run.D_bfilm_ref[s] * 4.0 + 0.5);
         }
         c.dt = S > 0 ? refNu * dx * dx / run.D_pore[0] : 1.0;
 
@@ -341,7 +367,9 @@ int read_complab_xml(const std::string& path, HostRun& run, std::string& err, co
         // cellular automaton (complab_functions.hh:1167-1186): every microbe this
         // driver accepts is CA-solved, so the CA runs whenever there is one;
         // its material code is the first of its material numbers (bio_dynamics[m][0])
-        if (M > 0) {
+        int n_ca = 0;
+        for (int m = 0; m < M; ++m) n_ca += run.carried[m] ? 0 : 1;
+        if (n_ca > 0) {
             const XmlNode& mic = P["microbiology"];
             if (!mic.has("thrd_biofilm_fraction"))
                 throw std::runtime_error("thrd_biofilm_fraction must be defined when solver_type is Cellular Automata");
@@ -358,6 +386,7 @@ int read_complab_xml(const std::string& path, HostRun& run, std::string& err, co
                 else throw std::runtime_error("CA_method (" + h + ") should be either half or fraction");
             }
             for (int m = 0; m < M; ++m) {
+                if (run.carried[m]) continue;            // the CA moves sessile biomass only
                 if (run.bio_materials[m].empty())
                     throw std::runtime_error("microbe" + std::to_string(m) + " has no material number for its biofilm");
                 c.microbe_code[m] = run.bio_materials[m][0];

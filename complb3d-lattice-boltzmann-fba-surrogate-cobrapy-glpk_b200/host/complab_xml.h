@@ -33,6 +33,8 @@ struct HostRun {
     // chemistry / microbiology
     std::vector<std::string> subs_names, microbe_names;
     std::vector<double> D_pore, D_bfilm;
+    std::vector<double> D_bfilm_ref;                 // divisor of the biofilm relaxation (complab.cpp:725, :738)
+    std::vector<int> carried;                        // per microbe: 1 if solved by LBM (a carrier solute)
     std::vector<std::vector<int>> bio_materials;    // per microbe: its biofilm material numbers
     std::vector<std::vector<double>> b0;            // per microbe: initial density per material
     bool biotic_mode = true;

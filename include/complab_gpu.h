@@ -245,6 +245,13 @@ typedef struct {
      *                    with 12 sessile biomass pools; substrates 2, 4, 5, 6,
      *                    9, 13, 21, 22, 23 immobile */
     int32_t rate_law;
+    /* microbes solved by LBM (the reference's planktonic biomass, solver_type
+     * LBM: soluteDomainSetup of a bFree lattice, complab.cpp:788-797): 0 =
+     * sessile (the FP64 biomass field); s + 1 = the microbe's biomass is the
+     * density of mobile solute s, which carries its transport and boundary
+     * conditions; the kinetics read it and add the microbe's growth to it.
+     * Table rate laws only; no surrogate organisms or CA on such a microbe. */
+    int32_t microbe_carrier[CL_MAX_MICROBES];
 } cl_config;
 #define CL_RATELAW_TABLE 0
 #define CL_RATELAW_ZHAO  1

@@ -839,7 +839,13 @@ static void vox_kinetics(const rx_ctx* r, int64_t n) {
     double C[CL_MAX_SOLUTES], Bm[CL_MAX_MICROBES], R[CL_MAX_SOLUTES], BR[CL_MAX_MICROBES];
     double dC[CL_MAX_SOLUTES], dB[CL_MAX_MICROBES];
     for (int s = 0; s < S; ++s) { double c = vox_dens(r, s, n); C[s] = c < THRD ? 0.0 : c; dC[s] = 0.0; }
-    for (int b = 0; b < M; ++b) { double v = r->st->bio[b*N + n]; Bm[b] = v < THRD ? 0.0 : v; dB[b] = 0.0; }
+    /* a microbe solved by LBM (microbe_carrier): its biomass is the density
+     * of its carrier solute, its dB goes to that lattice */
+    for (int b = 0; b < M; ++b) {
+        const int cr = cfg->microbe_carrier[b] - 1;
+        double v = cr >= 0 ? C[cr] : r->st->bio[b*N + n];
+        Bm[b] = v < THRD ? 0.0 : v; dB[b] = 0.0;
+    }
     if (r->any_bio) {
         if (r->st->kin) r->st->kin(Bm, M, C, S, R, BR, r->st->mask[n]);
         else orc_rates(cfg, 0, C, Bm, R, BR);
@@ -853,6 +859,8 @@ static void vox_kinetics(const rx_ctx* r, int64_t n) {
         }
     }
     if (r->any_srg) orc_surrogate_voxel(cfg, r->st->srg_nets, C, Bm, dC, dB);
+    for (int b = 0; b < M; ++b)
+        if (cfg->microbe_carrier[b] > 0) { dC[cfg->microbe_carrier[b] - 1] += dB[b]; dB[b] = 0.0; }
     for (int s = 0; s < S; ++s) if (dC[s] > THRD || dC[s] < -THRD) vox_apply(r, s, n, dC[s]);
     for (int b = 0; b < M; ++b) if (dB[b] > THRD || dB[b] < -THRD) r->st->bio[b*N + n] += dB[b];
 }

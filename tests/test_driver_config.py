@@ -239,8 +239,9 @@ def _ref_examples():
     root = reference_root()
     return os.path.join(root, "examples") if root else None
 SUPPORTED = ["01_flow_only", "02_diffusion_only", "03_abiotic_kinetics", "04_equilibrium",
-             "05_biotic_cellular_automaton", "13_precipitation", "14_dissolution", "15_precip_and_dissolution"]
-MOBILE_BIOMASS = ["06_biotic_finite_difference", "07_biotic_lattice_boltzmann", "08_two_microbes"]
+             "05_biotic_cellular_automaton", "07_biotic_lattice_boltzmann", "08_two_microbes",
+             "13_precipitation", "14_dissolution", "15_precip_and_dissolution"]
+MOBILE_BIOMASS = ["06_biotic_finite_difference"]
 
 
 def _example_xml(name):
@@ -312,13 +313,20 @@ def test_example_rate_tables_and_config_dump(name, tmp_path):
     assert (cfg.nx, cfg.ny, cfg.nz) == (c["nx"], c["ny"], c["nz"])
     mask = np.fromfile(tmp_path / "c.bin.mask", np.uint8)
     assert mask.size == cfg.nx * cfg.ny * cfg.nz
-    want_rxn = {"03_abiotic_kinetics": 1, "05_biotic_cellular_automaton": 1, "13_precipitation": 1,
-                "15_precip_and_dissolution": 1}.get(name, 0)
+    want_rxn = {"03_abiotic_kinetics": 1, "05_biotic_cellular_automaton": 1, "07_biotic_lattice_boltzmann": 1,
+                "08_two_microbes": 2, "13_precipitation": 1, "15_precip_and_dissolution": 1}.get(name, 0)
     assert cfg.n_rxn == want_rxn
     if name == "05_biotic_cellular_automaton":
         assert cfg.decay[0] == 1e-6 and cfg.rxn[0].monod_ks[0] == 5e-2 and cfg.rxn[0].nu[0] == -2.5
     if name in ("14_dissolution", "15_precip_and_dissolution"):
         assert cfg.n_phases == 1 and cfg.phases[0].k > 0 and cfg.phases[0].n_mass == 1
+    # an LBM-solved microbe is carried by one more mobile solute named after it
+    if name == "07_biotic_lattice_boltzmann":
+        assert cfg.n_solutes == 3 and cfg.microbe_carrier[0] == 3 and c["names"][2] == "Bug"
+        assert cfg.ca_enabled == 0 and cfg.c0[2] == 1.0
+    if name == "08_two_microbes":
+        assert cfg.microbe_carrier[0] == 0 and cfg.microbe_carrier[1] == 3 and cfg.ca_enabled == 1
+        assert cfg.microbe_code[0] == 3 and cfg.microbe_code[1] == 0
 
 
 def ctypes_sizeof(t):
