@@ -254,3 +254,32 @@ def test_set_transport_ignores_immobile_relaxation(gpu_lib, pkg, wl):
     with pytest.raises(pkg.CLError):
         lat.set_transport([2.0, 2.0], [2.0, 2.0], 0.01)
     lat.close()
+
+
+def test_lbm_solved_microbe_carried_by_a_solute(gpu_lib, pkg, wl):
+    """A microbe solved by LBM (the reference's planktonic bFree lattice):
+    solute 2 carries its biomass, advected and diffused with its own
+    relaxation; dual-Monod growth on solutes 0 and 1 reads that density and
+    adds to it.  Against the oracle after 1, 4 and 34 steps (rel. L2 <= 1e-4);
+    the sessile field stays zero."""
+    mask = wl.sphere_pack(26, 16, 16, 0.5, 2.0, 4.0, seed=19)
+    nx, ny, nz = mask.shape
+    sol = [{"tau": 0.8, "c0": 0.05, "left": "D", "left_value": 0.2, "right": "N"},
+           {"tau": 0.7, "c0": 0.02, "left": "D", "left_value": 0.1, "right": "N"},
+           {"tau": 0.55, "c0": 1.0, "left": "N", "right": "N"}]
+    cfg = pkg.make_config(nx, ny, nz, tau_ns=0.8, rho_in=1.0005, rho_out=1.0, solutes=sol, microbes=1, dt=1.0)
+    cfg.enable_kinetics = 1
+    pkg.add_rxn(cfg, microbe=0, k=2e-3, monod=[(0, 5e-2), (1, 1e-2)], nu={0: -1.0, 1: -0.5}, yield_=0.4)
+    cfg.decay[0] = 1e-5
+    cfg.microbe_carrier[0] = 3
+    lat, u = flow_field(pkg, cfg, mask)
+    lat.ade_init()
+    ref = o.Transport(cfg, mask, u=u)
+    for n in (1, 3, 30):
+        lat.step(n)
+        ref.step(n)
+        for s in range(3):
+            assert rel_l2(lat.field(pkg.FIELD_CONC, s).reshape(-1), ref.density(s)) < 1e-4, (n, s)
+    assert not np.allclose(ref.density(2), ref.density(2)[0])      # the biomass grew unevenly
+    assert np.all(lat.field(pkg.FIELD_BIOMASS, 0) == 0.0)
+    lat.close()
