@@ -443,6 +443,62 @@ def surrogate_bench(pkg, wl, stream, steps=20, warmup=3, shape=(256, 256, 256)):
             "roofline": roof}
 
 
+def c1_bench(pkg, wl, stream, flow_steps=2000, ade_steps=1000, cpu=True):
+    """The 64^3 flow + transport configuration as stated: spheres r 4-8 to
+    porosity 0.40 in 64^3 voxels (plus the two boundary planes), rho
+    1.001 / 1.000, tau 0.8, 2000 flow steps; then one solute, tau 0.7,
+    Dirichlet C = 1 inlet, zero-gradient outlet, 1000 transport steps.  Flow
+    and transport MLUPS (all sites) on the GPU, and the FP64 oracle on the
+    same domain for 100 + 100 steps."""
+    import torch
+    nx, ny, nz = 66, 64, 64
+    mask = wl.sphere_pack(nx, ny, nz, 0.40, 4.0, 8.0, seed=101)
+    cfg = pkg.make_config(nx, ny, nz, tau_ns=0.8, rho_in=1.001, rho_out=1.0,
+                          solutes=[{"tau": 0.7, "c0": 0.0, "left": "D", "left_value": 1.0, "right": "N"}])
+    lat = pkg.Lattice(cfg, stream=stream)
+    lat.upload_mask(mask)
+    lat.flow_init()
+    lat.flow_steps(20)
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    torch.cuda.synchronize()
+    e[0].record()
+    lat.flow_steps(flow_steps)
+    e[1].record()
+    lat.couple_velocity()
+    lat.ade_init()
+    lat.step(5)
+    torch.cuda.synchronize()
+    e[2].record()
+    lat.step(ade_steps)
+    e[3].record()
+    torch.cuda.synchronize()
+    fms, ams = e[0].elapsed_time(e[1]), e[2].elapsed_time(e[3])
+    outlet = float(lat.field(pkg.FIELD_CONC, 0).reshape(nx, ny, nz)[nx - 2].mean())
+    lat.close()
+    N = mask.size
+    res = {"workload": "64^3 spheres r 4-8, porosity 0.40, tau 0.8, 2000 flow steps; one solute, tau 0.7, "
+                       "1000 transport steps (FP32 populations)",
+           "flow_mlups": N * flow_steps / (fms * 1e-3) / 1e6, "transport_mlups": N * ade_steps / (ams * 1e-3) / 1e6,
+           "flow_ms": fms, "transport_ms": ams, "outlet_mean_after": outlet}
+    if not cpu:
+        return res
+    from oracle import oracle as o
+    fl = o.Flow(cfg, mask)
+    t0 = time.perf_counter()
+    fl.step(100)
+    cf = time.perf_counter() - t0
+    _, u = fl.macro()
+    tr = o.Transport(cfg, mask, u=u)
+    t0 = time.perf_counter()
+    tr.step(100)
+    ca = time.perf_counter() - t0
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    res["cpu_baseline"] = {"flow_mlups": N * 100 / cf / 1e6, "transport_mlups": N * 100 / ca / 1e6,
+                           "unit": "MLUPS", "cores": threads, "kind": "port",
+                           "sample": "the same 66x64x64 domain, 100 flow + 100 transport steps (FP64 oracle)"}
+    return res
+
+
 def cpu_surrogate(steps=40, shape=(64, 64, 64)):
     pkg, wl = load_pkg(), load_workloads()
     from oracle import oracle as o
@@ -720,6 +776,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_biotic:
         out["biotic_ca"] = biotic_ca_bench(pkg, wl, stream)
         out["surrogate"] = surrogate_bench(pkg, wl, stream)
+        out["flow_transport_64"] = c1_bench(pkg, wl, stream, cpu=not args.no_cpu)
         out["learned_step"] = learned_step_bench(pkg, wl, stream)
     if rank == 0 and world == 1 and not args.no_cpu:
         cm, cdt, threads, sample = cpu_coupled(40)
