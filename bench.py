@@ -757,6 +757,9 @@ def main():
         tps = traffic_from_profile("ade_fast")
         out["roofline"] = {"kernel": "transport step: ade_fast_kernel (gather, FP64 reaction chain, collide, "
                                      "stream in one launch)", "bound": "hbm",
+                           "limiter": "issue latency of the FP64 Newton chain at 24% warp occupancy (ncu); the "
+                                      "same launch without the chain streams at ~0.6 of the HBM peak",
+                           "target_frac": 0.60,
                            "achieved": achieved, "peak": peak,
                            "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind + " (hbm_gbs)",
                            "algorithmic_bytes_per_launch": ade_bytes, "avg_launch_ms": ade_ms / ade_n,
