@@ -41,3 +41,22 @@ def test_error_paths_without_gpu(pkg):
     cfg = pkg.make_config(8, 4, 4, tau_ns=0.5)
     h = lib.cl_create(ctypes.byref(cfg), None, ctypes.byref(st))
     assert not h and st.value == pkg.ERR_ARG
+
+
+def test_microbe_carrier_validation_without_gpu(pkg):
+    """A microbe carried by a solute must name a mobile solute and run the
+    rate table: refused otherwise, before any CUDA call."""
+    import ctypes
+    lib = pkg.load_library()
+    st = ctypes.c_int(0)
+    sol = [{"c0": 0.1}, {"immobile": True}]
+    cfg = pkg.make_config(8, 4, 4, solutes=sol, microbes=1)
+    cfg.microbe_carrier[0] = 2                     # solute 1 is immobile
+    assert not lib.cl_create(ctypes.byref(cfg), None, ctypes.byref(st)) and st.value == pkg.ERR_ARG
+    assert b"microbe_carrier" in lib.cl_last_error()
+    cfg.microbe_carrier[0] = 5                     # no such solute
+    assert not lib.cl_create(ctypes.byref(cfg), None, ctypes.byref(st)) and st.value == pkg.ERR_ARG
+    cfg = pkg.make_config(8, 4, 4, solutes=sol, microbes=1)
+    cfg.microbe_carrier[0] = 1
+    cfg.rate_law = pkg.RATELAW_ZHAO                # compiled rate laws read sessile biomass
+    assert not lib.cl_create(ctypes.byref(cfg), None, ctypes.byref(st)) and st.value == pkg.ERR_ARG
