@@ -209,7 +209,8 @@ __global__ void eq_start_set_kernel(int64_t N, const int32_t* sidx, float* col, 
 int eq_start_io(Ctx* c, int j, double* d_nat, int to_natural) {
     const int nc = c->cfg.eq.n_comp;
     if (!c->d_eq_x || j < 0 || j >= 2 * nc) { set_error("no warm starts in this context, or index out of range"); return CL_ERR_ARG; }
-    if (c->store_dirty) { int r = store_update(c, 0); if (r) return r; }
+    // (a read brings the storage up to date first; a write finds it so)
+    if (to_natural && c->store_dirty) { int r = store_update(c, 0); if (r) return r; }
     const int64_t N = c->geo.N;
     float* col = (j < nc ? c->d_eq_x : c->d_eq_xp) + (int64_t)(j % nc) * N;
     const int blocks = grid_for(N, 256, 148 * 16);

@@ -799,6 +799,13 @@ int cl_set_field(cl_ctx* h, int32_t field, int32_t index, const double* in) {
             break;
         case CL_FIELD_EQ_START: {
             if (!c->ade_ready) return CL_ERR_STATE;
+            // storage first (its update uses the scratch that holds the input),
+            // then the input again
+            if (c->store_dirty) {
+                const int r2 = store_update(c, 0);
+                if (r2) return r2;
+                CL_CUDA(cudaMemcpyAsync(d, in, sizeof(double) * N, cudaMemcpyHostToDevice, c->stream));
+            }
             const int r2 = eq_start_io(c, index, d, 0);
             if (r2) return r2;
             break;
