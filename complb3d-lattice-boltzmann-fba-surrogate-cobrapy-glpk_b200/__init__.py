@@ -24,7 +24,7 @@ OK, WARN_NOT_CONVERGED = 0, 1
 ERR_ARG, ERR_CUDA, ERR_STATE, ERR_NOMEM, ERR_DIVERGED = -1, -2, -3, -4, -5
 BC_DIRICHLET, BC_NEUMANN = 0, 1
 FIELD_CONC, FIELD_BIOMASS, FIELD_VELOCITY, FIELD_FLOW_RHO, FIELD_FLOW_U, FIELD_PHASE, FIELD_EQ_ITERS = range(7)
-FIELD_CA_AGE, FIELD_CA_TOTAL, FIELD_EQ_START = 7, 8, 9
+FIELD_CA_AGE, FIELD_CA_TOTAL, FIELD_EQ_START, FIELD_DYNAMICS = 7, 8, 9, 10
 RED_SUM, RED_MIN, RED_MAX, RED_COUNT_EQ = range(4)
 EQ_START_COLD, EQ_START_GIVEN, EQ_START_LEARNED = range(3)
 EQ_SOLVER_NEWTON, EQ_SOLVER_PCF = 0, 1

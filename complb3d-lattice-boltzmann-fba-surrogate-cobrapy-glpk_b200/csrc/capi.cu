@@ -662,6 +662,18 @@ __global__ void i2d_kernel(const int32_t* a, double* b, int64_t n) {
 __global__ void u2d_kernel(const uint8_t* a, double* b, int64_t n) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) b[i] = a[i];
 }
+// dynamics classes (the low two bits of a class byte) <-> doubles; a value
+// that is not a class 0..3 sets *bad and leaves the byte as it was
+__global__ void cls2d_kernel(const uint8_t* a, double* b, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) b[i] = a[i] & 3;
+}
+__global__ void d2cls_kernel(const double* a, uint8_t* b, int64_t n, int* bad) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double v = a[i];
+        if (v >= 0.0 && v <= 3.0 && v == (double)(int)v) b[i] = (uint8_t)((b[i] & ~3) | (int)v);
+        else *bad = 1;
+    }
+}
 // phase ids from doubles; any value that is not an id 0..n_phases sets *bad
 __global__ void d2phase_kernel(const double* a, uint8_t* b, int64_t n, int n_phases, int* bad) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -747,6 +759,10 @@ int cl_get_field(cl_ctx* h, int32_t field, int32_t index, double* out) {
             if (!c->ade_ready) return CL_ERR_STATE;
             r = eq_start_io(c, index, d, 1);
             break;
+        case CL_FIELD_DYNAMICS:
+            if (!c->mask_ready || index < 0 || index > 1) { set_error("dynamics: index 0 (flow) or 1 (transport), after the mask"); return CL_ERR_ARG; }
+            cls2d_kernel<<<blocks, 256, 0, c->stream>>>(index == 0 ? c->d_ns_cls : c->d_ade_cls, d, N);
+            break;
         case CL_FIELD_PHASE:
             if (!c->d_phase) { set_error("dissolution is not enabled in this context"); return CL_ERR_STATE; }
             u2d_kernel<<<blocks, 256, 0, c->stream>>>(c->d_phase, d, N);
@@ -797,6 +813,21 @@ int cl_set_field(cl_ctx* h, int32_t field, int32_t index, const double* in) {
             if (index < 0 || index > 2) return CL_ERR_ARG;
             d2f_kernel<<<blocks, 256, 0, c->stream>>>(d, c->d_u + index * N, N);
             break;
+        case CL_FIELD_DYNAMICS: {
+            if (!c->mask_ready || index < 0 || index > 1) { set_error("dynamics: index 0 (flow) or 1 (transport), after the mask"); return CL_ERR_ARG; }
+            int* d_bad = reinterpret_cast<int*>(c->d_scratch + N);
+            CL_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(int), c->stream));
+            d2cls_kernel<<<blocks, 256, 0, c->stream>>>(d, index == 0 ? c->d_ns_cls : c->d_ade_cls, N, d_bad);
+            CL_LAUNCH_CHECK("d2cls_kernel");
+            int bad = 0;
+            CL_CUDA(cudaMemcpyAsync(&bad, d_bad, sizeof bad, cudaMemcpyDeviceToHost, c->stream));
+            CL_CUDA(cudaStreamSynchronize(c->stream));
+            // the flags, counts, site lists and storage follow the classes
+            const int r2 = refresh_flags(c);
+            if (r2) return r2;
+            if (bad) { set_error("dynamics classes are 0 NoDynamics, 1 bounce-back, 2 pore, 3 biofilm"); return CL_ERR_ARG; }
+            break;
+        }
         case CL_FIELD_EQ_START: {
             if (!c->ade_ready) return CL_ERR_STATE;
             // storage first (its update uses the scratch that holds the input),

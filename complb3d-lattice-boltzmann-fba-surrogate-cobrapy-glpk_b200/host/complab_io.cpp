@@ -133,6 +133,15 @@ bool save_checkpoint(cl_ctx* h, const HostRun& run, const Checkpoint& chk, const
     std::vector<uint8_t> mask(N);
     if (!ok(cl_download_mask(h, mask.data()), "cl_download_mask", err)) return false;
     if (!write_raw(dir + "/mask.u8", mask.data(), N, err)) return false;
+    {
+        std::vector<double> cd(N);
+        std::vector<uint8_t> cls(2 * N);
+        for (int k = 0; k < 2; ++k) {
+            if (!ok(cl_get_field(h, CL_FIELD_DYNAMICS, k, cd.data()), "cl_get_field", err)) return false;
+            for (size_t n = 0; n < N; ++n) cls[k * N + n] = (uint8_t)cd[n];
+        }
+        if (!write_raw(dir + "/dynamics.u8", cls.data(), 2 * N, err)) return false;
+    }
     if (chk.has_flow) {
         std::vector<float> f(19 * N);
         if (!ok(cl_get_flow_populations(h, f.data()), "cl_get_flow_populations", err)) return false;
@@ -217,6 +226,19 @@ bool read_checkpoint(const std::string& dir, const HostRun& run, Checkpoint& chk
     }
     mask.assign((size_t)c.nx * c.ny * c.nz, 0);
     return read_raw(dir + "/mask.u8", mask.data(), mask.size(), err);
+}
+
+bool restore_dynamics(cl_ctx* h, const HostRun& run, const std::string& dir, std::string& err) {
+    const cl_config& c = run.cfg;
+    const size_t N = (size_t)c.nx * c.ny * c.nz;
+    std::vector<uint8_t> cls(2 * N);
+    if (!read_raw(dir + "/dynamics.u8", cls.data(), cls.size(), err)) return false;
+    std::vector<double> cd(N);
+    for (int k = 0; k < 2; ++k) {
+        for (size_t n = 0; n < N; ++n) cd[n] = cls[k * N + n];
+        if (!ok(cl_set_field(h, CL_FIELD_DYNAMICS, k, cd.data()), "cl_set_field", err)) return false;
+    }
+    return true;
 }
 
 bool restore_flow(cl_ctx* h, const HostRun& run, const std::string& dir, std::string& err) {

@@ -14,6 +14,8 @@
 // sizes, the steps done, the calibrated pressure, dt and relaxation of the
 // run) and raw little-endian arrays in site order n = (x*ny + y)*nz + z:
 //   mask.u8              material numbers (N bytes)
+//   dynamics.u8          2*N dynamics classes, the flow's then the solutes'
+//                        (they follow the node conversions' dynamics switches)
 //   flow.f32             19*N flow deviations f_i - t_i, natural order (when a flow exists)
 //   solute_<s>.f32       7*N populations of a mobile solute, natural order
 //   solute_<s>.f64       N inventory values of an immobile solute
@@ -57,6 +59,8 @@ bool save_checkpoint(cl_ctx* h, const HostRun& run, const Checkpoint& chk, const
 // header and geometry (before the context exists)
 bool read_checkpoint(const std::string& dir, const HostRun& run, Checkpoint& chk, std::vector<uint8_t>& mask,
                      std::string& err);
+// the dynamics classes (right after the mask upload)
+bool restore_dynamics(cl_ctx* h, const HostRun& run, const std::string& dir, std::string& err);
 // the flow populations (after the mask upload)
 bool restore_flow(cl_ctx* h, const HostRun& run, const std::string& dir, std::string& err);
 // the transport state (after cl_ade_init)

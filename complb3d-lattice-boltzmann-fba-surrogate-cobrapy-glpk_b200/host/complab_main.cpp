@@ -255,6 +255,10 @@ int main(int argc, char** argv) {
     if (!ctx.h) { std::fprintf(stderr, "complab_b200: cl_create failed (%d): %s\n", st, cl_last_error()); return 1; }
     cl_ctx* h = ctx.h;
     if (!check(cl_upload_mask(h, mask.data()), "cl_upload_mask")) return 1;
+    if (!restart.empty() && !clhost::restore_dynamics(h, run, restart, err)) {
+        std::fprintf(stderr, "complab_b200: %s\n", err.c_str());
+        return 1;
+    }
 
     // flow and the Peclet calibration
     const double nsNu = (run.tau - 0.5) / 3.0;

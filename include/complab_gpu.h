@@ -461,6 +461,12 @@ int cl_ca_update_mask(cl_ctx* ctx, int64_t* mask_changes);
  * component j of each site, n_comp <= j < 2 n_comp the one before; NaN where
  * a site has none (stored in FP32) */
 #define CL_FIELD_EQ_START  9
+/* the sites' dynamics (index 0 the flow's, 1 the solutes'): 0 NoDynamics,
+ * 1 bounce-back, 2 pore, 3 biofilm.  They follow the mask at upload and then
+ * change only by cl_update_dynamics, the reference's dynamics switches, so
+ * after node conversions they are part of the state a checkpoint keeps
+ * (a precipitated voxel keeps its solute dynamics, complab.cpp:1829-1836) */
+#define CL_FIELD_DYNAMICS 10
 
 /* ---- reductions ----------------------------------------------------- */
 #define CL_RED_SUM   0

@@ -1,6 +1,6 @@
 """Checkpoint and restart through the C ABI: the state a transport step reads
-(flow and solute populations in natural order, immobile inventories, biomass,
-phase ids, the Newton warm starts) taken from one context after 5 steps of
+(dynamics classes, flow and solute populations in natural order, immobile
+inventories, biomass, phase ids, the Newton warm starts) taken from one context after 5 steps of
 the coupled chemistry with dissolution, restored into a fresh context, and
 both stepped 7 more times: every field bit for bit equal.  The restored
 context starts at the other AA parity and with its own compact storage, so
@@ -37,6 +37,7 @@ def test_checkpoint_restart_is_bit_exact(gpu_lib, pkg, wl):
         assert a.step(1) == pkg.OK
     nc = cfg.eq.n_comp
     chk = {"flow": a.flow_populations().copy(), "mask": a.mask().copy(),
+           "dyn": [a.field(pkg.FIELD_DYNAMICS, k).copy() for k in range(2)],
            "sol": [a.solute_populations(s).copy() for s in range(8)],
            "imm": a.field(pkg.FIELD_CONC, 8).copy(), "bio": a.field(pkg.FIELD_BIOMASS, 0).copy(),
            "phase": a.field(pkg.FIELD_PHASE).copy(),
@@ -45,6 +46,8 @@ def test_checkpoint_restart_is_bit_exact(gpu_lib, pkg, wl):
 
     b = pkg.Lattice(cfg)
     b.upload_mask(chk["mask"])
+    for k in range(2):
+        b.set_field(pkg.FIELD_DYNAMICS, k, chk["dyn"][k])
     b.set_flow_populations(chk["flow"])
     b.couple_velocity()
     b.ade_init()
