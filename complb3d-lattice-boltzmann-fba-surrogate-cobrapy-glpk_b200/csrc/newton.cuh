@@ -15,7 +15,8 @@
 //   - convergence: relative mass-balance residual max_j |F_j| / sum_i |S_ij| c_i <= tol;
 //   - species at a clamp bound contribute nothing to J;
 //   - the step is scaled so that no component moves more than 2 decades;
-//   - the Armijo merit is ||F_j / sum_i |S_ij| c_i||_2 with the current weights;
+//   - the Armijo merit is ||F_j / sum_i |S_ij| c_i||_2 with the current weights
+//     (its test compared in squares);
 //   - a solve whose 40 backtracking trials all fail stops (the next iterate
 //     would be the same point to ~1e-12 of a step).
 // Species are evaluated on the fly (no per-species storage), the component
@@ -332,7 +333,7 @@ __device__ __forceinline__ int eq_newton_reuse(const Tab& e, const double* T, do
         }
         if (rel <= tol) { *conv = 1; return it; }
         if (!(rel < 1e300)) { if (stopped) *stopped = 1; return it; }      // NaN / inf
-        fn = sqrt(fn);
+        // fn, fnt: squared weighted residual norms (the Armijo test compares squares)
         // Cholesky of ln10*J (lower triangle), solve L L^T d = -F
         // the diagonal is kept as its reciprocal (rsqrt), so the factorisation
         // and both triangular solves multiply instead of dividing
@@ -385,8 +386,7 @@ __device__ __forceinline__ int eq_newton_reuse(const Tab& e, const double* T, do
         double fnt = 0.0;
 #pragma unroll
         for (int a = 0; a < NC; ++a) { const double r = Ft[a] * w[a]; fnt = fma(r, r, fnt); }
-        fnt = sqrt(fnt);
-        if (fnt < fn * (1.0 - 1e-4)) {
+        if (fnt < fn * ((1.0 - 1e-4) * (1.0 - 1e-4))) {
 #pragma unroll
             for (int a = 0; a < NC; ++a) { x[a] = xt[a]; F[a] = Ft[a]; sc[a] = sct[a]; }
             continue;
@@ -400,8 +400,8 @@ __device__ __forceinline__ int eq_newton_reuse(const Tab& e, const double* T, do
             fnt = 0.0;
 #pragma unroll
             for (int a = 0; a < NC; ++a) { const double r = Ft[a] * w[a]; fnt = fma(r, r, fnt); }
-            fnt = sqrt(fnt);
-            if (fnt < fn * (1.0 - 1e-4 * alpha)) { accepted = true; break; }
+            const double q = 1.0 - 1e-4 * alpha;
+            if (fnt < fn * (q * q)) { accepted = true; break; }
             if (alpha < 1e-15) break;
             alpha *= 0.5;
         }
@@ -477,7 +477,7 @@ __device__ __forceinline__ int eq_newton_plain(const Tab& tb, const double* T, d
         }
         if (rel <= tol) { *conv = 1; return it; }
         if (!(rel < 1e300) || stuck) { if (stopped) *stopped = 1; return it; }      // NaN / inf, or stuck
-        fn = sqrt(fn);
+        // fn, fnt: squared weighted residual norms (the Armijo test compares squares)
         // Cholesky of ln10*J (lower triangle), solve L L^T d = -F
         // the diagonal is kept as its reciprocal (rsqrt), so the factorisation
         // and both triangular solves multiply instead of dividing
@@ -533,8 +533,8 @@ __device__ __forceinline__ int eq_newton_plain(const Tab& tb, const double* T, d
             double fnt = 0.0;
 #pragma unroll
             for (int a = 0; a < NC; ++a) { const double r = Ft[a] * w[a]; fnt = fma(r, r, fnt); }
-            fnt = sqrt(fnt);
-            if (fnt < fn * (1.0 - 1e-4 * alpha)) { accepted = true; break; }
+            const double q = 1.0 - 1e-4 * alpha;
+            if (fnt < fn * (q * q)) { accepted = true; break; }
             if (alpha < 1e-15) break;
             alpha *= 0.5;
         }
@@ -599,7 +599,7 @@ __device__ int eq_newton_warp(const EqDev& e, const double* T, double* x, int ma
         }
         if (rel <= tol) { *conv = 1; return it; }
         if (!(rel < 1e300) || stuck) { if (stopped) *stopped = 1; return it; }      // NaN / inf, or stuck
-        fn = sqrt(fn);
+        // fn, fnt: squared weighted residual norms (the Armijo test compares squares)
         // Cholesky of ln10*J (lower triangle), solve L L^T d = -F
         // the diagonal is kept as its reciprocal (rsqrt), so the factorisation
         // and both triangular solves multiply instead of dividing
@@ -665,8 +665,8 @@ __device__ int eq_newton_warp(const EqDev& e, const double* T, double* x, int ma
                 double fnt = 0.0;
 #pragma unroll
                 for (int a = 0; a < NC; ++a) { const double r = Ft[a] * w[a]; fnt = fma(r, r, fnt); }
-                fnt = sqrt(fnt);
-                pass = fnt < fn * (1.0 - 1e-4 * alpha);
+                const double q = 1.0 - 1e-4 * alpha;
+                pass = fnt < fn * (q * q);
             }
             const unsigned bal = __ballot_sync(0xffffffffu, pass);
             const int src = bal ? __ffs(bal) - 1 : 39 - base;     // else the last trial (k = 39)
