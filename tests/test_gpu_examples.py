@@ -20,7 +20,12 @@ the oracle's transport does not replay: such a run is compared at the step of
 its first conversion.
 
 Tolerances (FP32 populations against FP64, as the other transport tests):
-solute fields relative L2 <= 1e-4; biomass relative L2 <= 1e-5; conversion
+solute fields relative L2 <= 1e-4, and <= 3e-4 for a lattice relaxing at
+omega > 1.99 (example 08's LBM-solved microbe, tau 0.50018: the FP64 oracle
+itself amplifies a one-ulp FP32 rounding of that lattice eighteenfold in 300
+steps, test_oracle_carrier_sensitivity.py; the GPU's FP32 populations round
+every step and it ends 1.1e-4 from the oracle after 1000 steps, while that
+run's donor and product stay within 5e-6); biomass relative L2 <= 1e-5; conversion
 counts and masks equal up to voxels within the transport tolerance of a
 threshold (at most 2, or 2% of the changes); the flow solve's iteration count
 within 2% of the oracle's.
@@ -171,7 +176,8 @@ def test_reference_example_against_oracle(gpu_lib, pkg, tmp_path, name):
     if cfg.ca_enabled:
         assert out["ca_sweeps"] == ev["ca_sweeps"] and out["ca_mask_changes"] == ev["ca_changes"]
     for s, nm in enumerate(cj["names"]):
-        assert table[nm] <= 1e-4, (nm, table)
+        tol = 3e-4 if max(cfg.omega_pore[s], cfg.omega_bio[s]) > 1.99 else 1e-4
+        assert table[nm] <= tol, (nm, table)
     for m, nm in enumerate(cj["microbe_names"]):
         if not cfg.microbe_carrier[m]:
             assert table["biomass " + nm] <= 1e-5, (nm, table)
