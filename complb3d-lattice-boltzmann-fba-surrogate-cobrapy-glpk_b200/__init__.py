@@ -27,6 +27,7 @@ FIELD_CONC, FIELD_BIOMASS, FIELD_VELOCITY, FIELD_FLOW_RHO, FIELD_FLOW_U, FIELD_P
 FIELD_CA_AGE, FIELD_CA_TOTAL, FIELD_EQ_START, FIELD_DYNAMICS = 7, 8, 9, 10
 RED_SUM, RED_MIN, RED_MAX, RED_COUNT_EQ = range(4)
 EQ_START_COLD, EQ_START_GIVEN, EQ_START_LEARNED = range(3)
+EQ_NET_TCGEN05, EQ_NET_MMA_SYNC = 0, 1
 EQ_SOLVER_NEWTON, EQ_SOLVER_PCF = 0, 1
 SRG_TENSOR, SRG_FP32 = 0, 1
 MAX_SRG_ORG = 2
@@ -480,7 +481,7 @@ def _bind_eq(lib):
                          P(ctypes.c_float)]),
         ("cl_eq_grad_host", [vp, vp, vp, c_int32, P(ctypes.c_float), vp]),
         ("cl_eq_param_count", [vp, P(c_int32)]), ("cl_eq_get_params", [vp, vp]),
-        ("cl_eq_set_params", [vp, vp]), ("cl_eq_predict_host", [vp, vp, vp, c_int32]),
+        ("cl_eq_set_params", [vp, vp]), ("cl_eq_predict_host", [vp, vp, vp, c_int32]), ("cl_eq_set_network_path", [vp, c_int32]),
         ("cl_eq_predict_device", [vp, vp, vp, c_int64]),
         ("cl_eq_pcf_device", [vp, vp, vp, vp, vp, c_int64]), ("cl_eq_pcf_host", [vp, vp, vp, vp, vp, c_int64]),
         ("cl_surrogate_batch_device", [P(SurrogateNet), vp, vp, c_int64, c_int32, vp]),
@@ -581,6 +582,10 @@ class EqSolver:
     def set_params(self, p):
         p = np.ascontiguousarray(p, np.float32)
         _check(self.lib, self.lib.cl_eq_set_params(self.h, _ptr(p)), "cl_eq_set_params")
+
+    def set_network_path(self, path):
+        """EQ_NET_TCGEN05 (default) or EQ_NET_MMA_SYNC for the network's inference."""
+        _check(self.lib, self.lib.cl_eq_set_network_path(self.h, path), "cl_eq_set_network_path")
 
     def predict(self, x):
         x = np.ascontiguousarray(x, np.float32)

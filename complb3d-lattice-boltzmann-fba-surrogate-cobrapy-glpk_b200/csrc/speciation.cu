@@ -18,6 +18,7 @@
 #include "speciation_large.h"
 #include "pcf.cuh"
 #include "mma.cuh"
+#include "umma.cuh"
 #include <cmath>
 #include <vector>
 #include <random>
@@ -340,6 +341,165 @@ __global__ void __launch_bounds__(MLP_THREADS) mlp_predict_kernel(MlpDev w, int 
     }
 }
 
+// The same inference on the fifth-generation tensor core: 128 samples per
+// tile (one per thread, M = 128), the three layers as tcgen05.mma chains on
+// shared-memory operands (layer 1 K = 16, layers 2 and 3 K = 64 in four
+// MMAs; N = 64, 64, 16) accumulating in 64 TMEM columns, each layer's GELU
+// epilogue reading its row from TMEM and writing the next layer's BF16
+// operand.  Operands, activations and accumulation are those of
+// mlp_predict_kernel (BF16 in, FP32 accumulate, BF16 activations); only the
+// order of the FP32 sums differs.  One thread issues the MMAs; completion is
+// an mbarrier phase per layer, each wait bounded (on a timeout the kernel
+// sets *err and stops after freeing its TMEM).
+constexpr int TC_TS = 128, TC_THREADS = 128, TC_COLS = 64;
+
+struct MlpSmemTc {
+    alignas(128) unsigned char X[TC_TS * KP * 2];    // [128][16] K-major core matrices
+    alignas(128) unsigned char A[TC_TS * H * 2];     // [128][64]
+    alignas(128) unsigned char W1[H * KP * 2];       // [64][16]
+    alignas(128) unsigned char W2[H * H * 2];        // [64][64]
+    alignas(128) unsigned char W3[16 * H * 2];       // [16][64], rows >= nc zero
+    float b[2 * H + 16];
+    float nrm[4 * CL_MAX_COMP];
+    alignas(8) unsigned long long bar;
+    uint32_t tmem;
+};
+
+__device__ __forceinline__ void tc_put_bf16(unsigned char* tile, int row, int k, int kch, float v) {
+    *reinterpret_cast<__nv_bfloat16*>(tile + umma_off(row, k, kch)) = __float2bfloat16_rn(v);
+}
+
+// GELU of 16 columns of this thread's row plus bias, into the next operand
+__device__ __forceinline__ void tc_gelu16(unsigned char* A, int row, int n0, const float* acc, const float* bias) {
+    uint32_t w[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) w[j] = pack_bf16(gelu(acc[2 * j] + bias[n0 + 2 * j]), gelu(acc[2 * j + 1] + bias[n0 + 2 * j + 1]));
+    *reinterpret_cast<uint4*>(A + umma_off(row, n0, H / 8)) = make_uint4(w[0], w[1], w[2], w[3]);
+    *reinterpret_cast<uint4*>(A + umma_off(row, n0 + 8, H / 8)) = make_uint4(w[4], w[5], w[6], w[7]);
+}
+
+__global__ void __launch_bounds__(TC_THREADS) mlp_predict_tc_kernel(MlpDev w, int nc, const double* totals,
+                                                                   double* logfree, const float* xin, float* yout,
+                                                                   int64_t n, unsigned int* err) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    MlpSmemTc& s = *reinterpret_cast<MlpSmemTc*>(smem_raw);
+    const int tid = threadIdx.x, warp = tid >> 5;
+    // weights into the K-major core-matrix layout, biases, normalisation
+    for (int i = tid; i < H * KP; i += TC_THREADS) {
+        const int r = i / KP, k = i - r * KP;
+        *reinterpret_cast<__nv_bfloat16*>(s.W1 + umma_off(r, k, KP / 8)) = w.W1[r * P24 + k];
+    }
+    for (int i = tid; i < H * H; i += TC_THREADS) {
+        const int r = i / H, k = i - r * H;
+        *reinterpret_cast<__nv_bfloat16*>(s.W2 + umma_off(r, k, H / 8)) = w.W2[r * P72 + k];
+    }
+    for (int i = tid; i < 16 * H; i += TC_THREADS) {
+        const int r = i / H, k = i - r * H;
+        *reinterpret_cast<__nv_bfloat16*>(s.W3 + umma_off(r, k, H / 8)) =
+            r < nc && r < 8 ? w.W3[r * P72 + k] : __float2bfloat16_rn(0.f);
+    }
+    for (int i = tid; i < 2 * H + 16; i += TC_THREADS) s.b[i] = i < 2 * H + nc ? w.b[i] : 0.f;
+    for (int i = tid; i < 4 * nc; i += TC_THREADS) s.nrm[i] = w.norm[i];
+    const uint32_t bar = smem_u32(&s.bar);
+    if (tid == 0) mbar_init(bar, 1);
+    if (warp == 0) tmem_alloc(smem_u32(&s.tmem), TC_COLS);
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s.tmem;
+    const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+    const uint32_t aX = smem_u32(s.X), aA = smem_u32(s.A), aW1 = smem_u32(s.W1), aW2 = smem_u32(s.W2),
+                   aW3 = smem_u32(s.W3);
+    constexpr int kLimit = 1 << 20;
+    uint32_t phase = 0;
+    bool ok = true;
+    const int64_t ntiles = (n + TC_TS - 1) / TC_TS;
+    for (int64_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+        const int64_t s0 = tile * TC_TS;
+        const int m = tid;                       // this thread's sample and TMEM lane
+        const bool valid = s0 + m < n;
+        // layer-1 operand: the standardised inputs, zero beyond nc and n
+        {
+            uint32_t wv[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                float v2[2];
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int k = 2 * j + h;
+                    float v = 0.f;
+                    if (valid && k < nc) {
+                        if (totals) v = (float)((log10(fmax(totals[(s0 + m) * nc + k], 1e-30)) - s.nrm[k]) / s.nrm[nc + k]);
+                        else v = xin[(s0 + m) * nc + k];
+                    }
+                    v2[h] = v;
+                }
+                wv[j] = pack_bf16(v2[0], v2[1]);
+            }
+            *reinterpret_cast<uint4*>(s.X + umma_off(m, 0, KP / 8)) = make_uint4(wv[0], wv[1], wv[2], wv[3]);
+            *reinterpret_cast<uint4*>(s.X + umma_off(m, 8, KP / 8)) = make_uint4(wv[4], wv[5], wv[6], wv[7]);
+        }
+        // three layers: operand ready -> one thread issues -> commit -> all wait -> epilogue
+#pragma unroll 1
+        for (int layer = 0; layer < 3; ++layer) {
+            fence_async_smem();
+            tc_fence_before();
+            __syncthreads();
+            tc_fence_after();
+            if (tid == 0) {
+                if (layer == 0) {
+                    umma_bf16(tmem, umma_desc(aX, 0, KP / 8), umma_desc(aW1, 0, KP / 8), umma_idesc_bf16(H), 0);
+                } else {
+                    const uint32_t wB = layer == 1 ? aW2 : aW3;
+                    const uint32_t id = umma_idesc_bf16(layer == 1 ? H : 16);
+#pragma unroll
+                    for (int kb = 0; kb < H / 16; ++kb)
+                        umma_bf16(tmem, umma_desc(aA, kb, H / 8), umma_desc(wB, kb, H / 8), id, kb > 0);
+                }
+                umma_commit(bar);
+            }
+            // every thread leaves together if any wait timed out
+            if (!__syncthreads_and(mbar_wait(bar, phase & 1u, kLimit))) { ok = false; break; }
+            ++phase;
+            tc_fence_after();
+            if (layer < 2) {
+                const float* bias = s.b + layer * H;
+#pragma unroll
+                for (int c = 0; c < H / 16; ++c) {
+                    float acc[16];
+                    tmem_ld16(lane_addr + (uint32_t)(16 * c), acc);
+                    tc_gelu16(s.A, m, 16 * c, acc, bias);
+                }
+            } else {
+                float acc[16];
+                tmem_ld16(lane_addr, acc);
+                if (valid) {
+                    for (int k = 0; k < nc; ++k) {
+                        const float y = acc[k] + s.b[2 * H + k];
+                        if (totals) {
+                            const double u = log10(fmax(totals[(s0 + m) * nc + k], 1e-30));
+                            const double v = (double)y * s.nrm[3 * nc + k] + s.nrm[2 * nc + k];
+                            logfree[(s0 + m) * nc + k] = fmin(fmax(u + v, -30.0), 1.0);
+                        } else {
+                            yout[(s0 + m) * nc + k] = y;
+                        }
+                    }
+                }
+            }
+        }
+    }
+    if (!ok) {
+        // one more bounded wait for MMAs still in flight before the TMEM goes
+        mbar_wait(bar, phase & 1u, kLimit);
+        if (tid == 0) atomicOr(err, 1u);
+    }
+    // every thread's TMEM reads are done before the allocating warp frees it
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, TC_COLS);
+}
+
 // ---------------------------------------------------------------- Newton batch
 template <int NC>
 __global__ void newton_first_kernel(EqDev e, const double* totals, const double* cold_species, double* logfree,
@@ -528,6 +688,8 @@ struct cl_eq_solver {
     uint8_t* stop_mark = nullptr;     // solves that stopped early in the current phase
     int64_t fail_cap = 0;
     unsigned long long* fail_count = nullptr;   // two counters
+    int net_path = CL_EQ_NET_TCGEN05;           // the network's inference kernel
+    unsigned int* tc_err = nullptr;             // set by the tcgen05 kernel on a wait timeout
     unsigned long long* pcf_count = nullptr;    // PCF solves that did not converge
     uint64_t adam_t = 0;
     // tableaux beyond the one-thread solver (more than 5 components or more
@@ -599,6 +761,33 @@ static cl_eq_solver* create_large(const cl_eq_system* sys, void* stream, int* st
 
 static size_t mlp_smem_bytes() { return sizeof(MlpSmem); }
 static size_t mlp_fwd_smem_bytes() { return sizeof(MlpSmemFwd); }
+
+// the network's inference on the selected tensor-core path (mode as
+// mlp_predict_kernel: totals -> logfree, or raw xin -> yout)
+static int predict_launch(cl_eq_solver* s, const double* totals, double* logfree, const float* xin, float* yout,
+                          int64_t n) {
+    if (s->net_path == CL_EQ_NET_TCGEN05) {
+        mlp_predict_tc_kernel<<<grid_for((n + TC_TS - 1) / TC_TS, 1, 148 * 4), TC_THREADS, sizeof(MlpSmemTc),
+                                s->stream>>>(s->w, s->nc, totals, logfree, xin, yout, n, s->tc_err);
+        CL_LAUNCH_CHECK("mlp_predict_tc_kernel");
+    } else {
+        mlp_predict_kernel<<<grid_for((n + TS - 1) / TS, 1, 148 * 6), MLP_THREADS, mlp_fwd_smem_bytes(), s->stream>>>(
+            s->w, s->nc, totals, logfree, xin, yout, n);
+        CL_LAUNCH_CHECK("mlp_predict_kernel");
+    }
+    return CL_OK;
+}
+
+// a tcgen05 inference that timed out waiting for its MMAs (read after a
+// synchronisation of the solver's stream); clears the flag
+static int tc_error(cl_eq_solver* s, const char* where) {
+    unsigned int v = 0;
+    CL_CUDA(cudaMemcpy(&v, s->tc_err, sizeof(v), cudaMemcpyDeviceToHost));
+    if (!v) return CL_OK;
+    CL_CUDA(cudaMemset(s->tc_err, 0, sizeof(v)));
+    set_error(std::string(where) + ": the tensor-core inference timed out waiting for its MMAs");
+    return CL_ERR_CUDA;
+}
 
 static int eq_ensure_fail(cl_eq_solver* s, int64_t n) {
     if (s->fail_cap >= n) return CL_OK;
@@ -744,10 +933,12 @@ cl_eq_solver* cl_eq_create(const cl_eq_system* sys, void* stream, int* status) {
     A((void**)&s->part, sizeof(float) * (size_t)s->part_blocks * (np + 1));
     A((void**)&s->grad, sizeof(float) * (np + 1));
     A((void**)&s->fail_count, 2 * sizeof(unsigned long long));
+    A((void**)&s->tc_err, sizeof(unsigned int));
     A((void**)&s->pcf_count, sizeof(unsigned long long));
     if (e != cudaSuccess) return fail(cuda_fail(e, "cl_eq_create"), s);
     if (cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mlp_smem_bytes()) != cudaSuccess ||
-        cudaFuncSetAttribute(mlp_predict_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mlp_fwd_smem_bytes()) != cudaSuccess)
+        cudaFuncSetAttribute(mlp_predict_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mlp_fwd_smem_bytes()) != cudaSuccess ||
+        cudaFuncSetAttribute(mlp_predict_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MlpSmemTc)) != cudaSuccess)
         return fail(cuda_fail(cudaGetLastError(), "cudaFuncSetAttribute(mlp)"), s);
     // default initialisation: Glorot-uniform weights, zero biases, identity normalisation
     std::vector<float> p(np, 0.f);
@@ -776,7 +967,7 @@ int cl_eq_destroy(cl_eq_solver* s) {
     if (s->stream) cudaStreamSynchronize(s->stream);
     void* ptrs[] = {s->w.W1, s->w.W2, s->w.W2T, s->w.W3, s->w.W3T, s->w.b, s->w.norm, s->master, s->m1, s->m2,
                     s->part, s->grad, s->fail_list, s->fail_list2, s->stop_mark, s->fail_count, s->pcf_count,
-                    s->lg_stoich, s->lg_logk, s->lg_active};
+                    s->lg_stoich, s->lg_logk, s->lg_active, s->tc_err};
     for (void* p : ptrs) if (p) cudaFree(p);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     delete s;
@@ -820,9 +1011,8 @@ int cl_eq_solve_device(cl_eq_solver* s, const double* d_totals, const double* d_
                         s->sys.max_iter, s->sys.warm_iter, s->sys.tol, s->fail_count);
     }
     if (start == CL_EQ_START_LEARNED) {
-        mlp_predict_kernel<<<grid_for((n + TS - 1) / TS, 1, 148 * 6), MLP_THREADS, mlp_fwd_smem_bytes(), s->stream>>>(
-            s->w, s->nc, d_totals, d_logfree, nullptr, nullptr, n);
-        CL_LAUNCH_CHECK("mlp_predict_kernel");
+        const int rp = predict_launch(s, d_totals, d_logfree, nullptr, nullptr, n);
+        if (rp) return rp;
     } else if (start != CL_EQ_START_GIVEN && start != CL_EQ_START_COLD) { set_error("unknown start mode"); return CL_ERR_ARG; }
     int r = eq_ensure_fail(s, n);
     if (r) return r;
@@ -888,10 +1078,7 @@ int cl_eq_predict_device(cl_eq_solver* s, const double* d_totals, double* d_logf
     if (!s || !d_totals || !d_logfree || n < 0) { set_error("null argument"); return CL_ERR_ARG; }
     if (refuse_large(s, "cl_eq_predict_device")) return CL_ERR_ARG;
     if (n == 0) return CL_OK;
-    mlp_predict_kernel<<<grid_for((n + TS - 1) / TS, 1, 148 * 6), MLP_THREADS, mlp_fwd_smem_bytes(), s->stream>>>(
-        s->w, s->nc, d_totals, d_logfree, nullptr, nullptr, n);
-    CL_LAUNCH_CHECK("mlp_predict_kernel");
-    return CL_OK;
+    return predict_launch(s, d_totals, d_logfree, nullptr, nullptr, n);
 }
 
 int cl_eq_solve_host(cl_eq_solver* s, const double* totals, const double* cold_species, double* logfree,
@@ -955,6 +1142,16 @@ int cl_eq_grad_host(cl_eq_solver* s, const float* x, const float* y, int32_t n, 
     return r;
 }
 
+int cl_eq_set_network_path(cl_eq_solver* s, int32_t path) {
+    if (!s) { set_error("null argument"); return CL_ERR_ARG; }
+    if (path != CL_EQ_NET_TCGEN05 && path != CL_EQ_NET_MMA_SYNC) {
+        set_error("cl_eq_set_network_path: CL_EQ_NET_TCGEN05 or CL_EQ_NET_MMA_SYNC");
+        return CL_ERR_ARG;
+    }
+    s->net_path = path;
+    return CL_OK;
+}
+
 int cl_eq_predict_host(cl_eq_solver* s, const float* x, float* y, int32_t n) {
     if (!s || !x || !y || n <= 0) { set_error("null argument"); return CL_ERR_ARG; }
     if (refuse_large(s, "cl_eq_predict_host")) return CL_ERR_ARG;
@@ -964,13 +1161,12 @@ int cl_eq_predict_host(cl_eq_solver* s, const float* x, float* y, int32_t n) {
     CL_CUDA(cudaMalloc(&dy, sizeof(float) * n * nc));
     int r = CL_OK;
     cudaError_t e = cudaMemcpyAsync(dx, x, sizeof(float) * n * nc, cudaMemcpyHostToDevice, s->stream);
-    if (e == cudaSuccess) {
-        mlp_predict_kernel<<<grid_for((n + TS - 1) / TS, 1, 148 * 6), MLP_THREADS, mlp_fwd_smem_bytes(), s->stream>>>(
-            s->w, nc, nullptr, nullptr, dx, dy, n);
-        e = cudaGetLastError();
+    if (e == cudaSuccess) r = predict_launch(s, nullptr, nullptr, dx, dy, n);
+    if (e == cudaSuccess && r == CL_OK) {
+        e = cudaMemcpyAsync(y, dy, sizeof(float) * n * nc, cudaMemcpyDeviceToHost, s->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+        if (e == cudaSuccess) r = tc_error(s, "cl_eq_predict_host");
     }
-    if (e == cudaSuccess) e = cudaMemcpyAsync(y, dy, sizeof(float) * n * nc, cudaMemcpyDeviceToHost, s->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
     if (e != cudaSuccess) r = cuda_fail(e, "cl_eq_predict_host");
     cudaFree(dx); cudaFree(dy);
     return r;

@@ -563,6 +563,17 @@ int cl_eq_param_count(const cl_eq_solver* s, int32_t* count);
 int cl_eq_get_params(cl_eq_solver* s, float* host_params);
 int cl_eq_set_params(cl_eq_solver* s, const float* host_params);
 int cl_eq_predict_host(cl_eq_solver* s, const float* x, float* y, int32_t n);
+/* The tensor-core path of the network's inference (cl_eq_predict_*, the
+ * learned start of cl_eq_solve_*): CL_EQ_NET_TCGEN05 (default) runs 128
+ * samples per CTA through tcgen05.mma with the accumulators in tensor memory;
+ * CL_EQ_NET_MMA_SYNC runs 64-sample tiles through warp-level mma.sync.  Both
+ * take BF16 operands and activations with FP32 accumulation.  Training
+ * (cl_eq_train, cl_eq_grad_host) runs the warp-level path.  A tcgen05
+ * inference whose wait on its MMAs times out is reported as CL_ERR_CUDA by
+ * cl_eq_predict_host. */
+#define CL_EQ_NET_TCGEN05  0
+#define CL_EQ_NET_MMA_SYNC 1
+int cl_eq_set_network_path(cl_eq_solver* s, int32_t path);
 /* the network's start for n device totals (log10 free components, FP64), the
  * values CL_EQ_START_LEARNED starts Newton from; no counterpart in the reference */
 int cl_eq_predict_device(cl_eq_solver* s, const double* d_totals, double* d_logfree, int64_t n);
