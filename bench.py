@@ -431,13 +431,16 @@ def surrogate_bench(pkg, wl, stream, steps=20, warmup=3, shape=(256, 256, 256)):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     ade_ms, ade_n = lat.timing_read(pkg.KERNEL_ADE_MAIN)
+    compiled = lat.get_option(pkg.OPT_COMPILED_CHEM) == pkg.CHEM_SURROGATE2
     lat.timing(False)
     lat.close()
     N = mask.size
     n_fluid_int, _ = fluid_counts(cfg, mask)
     peak, peak_kind = peaks()
+    how = ("one launch: ade_fast_kernel with the networks' weights in its parameter space" if compiled
+           else "reaction + streaming launches")
     roof = transport_roofline(ade_ms, ade_n, n_fluid_int, 6 * 56 + 12 + 2 * 8, N - 2 * ny * nz, peak, peak_kind,
-                              "transport step with the per-voxel networks (reaction + streaming launches)")
+                              "transport step with the per-voxel networks (%s)" % how)
     return {"workload": "surrogate: %dx%dx%d sphere pack, porosity 0.4, 2 organisms x (3->20->20->4), 6 solutes"
                         % shape, "mlups": N * steps / (ms * 1e-3) / 1e6, "ms_per_step": ms / steps,
             "roofline": roof}

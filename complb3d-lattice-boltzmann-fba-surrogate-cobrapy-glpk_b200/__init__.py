@@ -35,7 +35,7 @@ SRG_IN_FIN, SRG_IN_CONC, SRG_IN_BIOMASS = 0, 1, 2
 SRG_OUT_GROWTH, SRG_OUT_FOUT = 0, 1
 KERNEL_ADE_MAIN, KERNEL_FLOW_STEP, KERNEL_ADE_REACT = 0, 1, 2
 OPT_COMPILED_CHEM, OPT_FAST_VARIANT, OPT_EQ_LEARN, OPT_EQ_FORGET, OPT_EQ_LEARN_TRAININGS = 1, 2, 3, 4, 5
-CHEM_COUPLED, CHEM_BIOTIC4, CHEM_ZHAO24 = 1, 2, 3
+CHEM_COUPLED, CHEM_BIOTIC4, CHEM_ZHAO24, CHEM_SURROGATE2 = 1, 2, 3, 4
 OP_KINETICS, OP_SURROGATE, OP_ABIOTIC, OP_EQUILIBRIUM, OP_ALL = 1, 2, 4, 8, 15
 RATELAW_TABLE, RATELAW_ZHAO = 0, 1
 

@@ -5,7 +5,7 @@
 namespace cl {
 
 int ade_step(Ctx* c) {
-    if (c->chem > 0 && c->chem_on) return ade_step_fast(c);
+    if (c->chem > 0 && c->chem_on && chem_ready(c)) return ade_step_fast(c);
     const int nc = c->ap.do_eq ? c->cfg.eq.n_comp : 0;
     switch (nc) {
         case 0: return ade_step_nc0(c);

@@ -61,30 +61,43 @@ __device__ __forceinline__ void fast_dissol_gather(const AdeK& k, int64_t n, int
 // increments; A: the total increment per solute.  Returns 1 if the
 // equilibrium solve did not converge.
 template <class Chem>
-__device__ __forceinline__ int fast_chain(const AdeK& k, int64_t n, uint32_t sto, int x, int y, int z, uint8_t cls,
-                                          double (&C)[Chem::S], double (&A)[Chem::S]) {
+__device__ __forceinline__ int fast_chain(const AdeK& k, const typename Chem::Consts& kc, int64_t n, uint32_t sto,
+                                          int x, int y, int z, uint8_t cls, double (&C)[Chem::S],
+                                          double (&A)[Chem::S]) {
     constexpr int S = Chem::S, M = Chem::M, MW = Chem::MW, NC = Chem::NC;
     const AdeParams& p = k.p;
     const int64_t N = k.g.N;
     int nonconv = 0;
     double R[S];
-    if (p.do_kin) {
+    // kinetics and the surrogate networks deposit into the same increments,
+    // applied together (kinetics_increments + the update of reaction_chain)
+    if (p.do_kin || (Chem::kSrg && p.n_srg > 0)) {
         double B[MW], BR[MW];
 #pragma unroll
         for (int m = 0; m < MW; ++m) {
             const double b = m < M ? k.bio[m * N + n] : 0.0;
             B[m] = b < THRD ? 0.0 : b;
         }
-        Chem::kinetics(p, C, B, R, BR, k.mask[n]);
+        if (p.do_kin) {
+            Chem::kinetics(p, C, B, R, BR, k.mask[n]);
 #pragma unroll
-        for (int s = 0; s < S; ++s) {
-            const double d = R[s] * p.dt;
-            R[s] = (d > THRD || d < -THRD) ? d : 0.0;
+            for (int s = 0; s < S; ++s) {
+                const double d = R[s] * p.dt;
+                R[s] = (d > THRD || d < -THRD) ? d : 0.0;
+            }
+#pragma unroll
+            for (int m = 0; m < MW; ++m) {
+                const double d = BR[m] * p.dt;
+                BR[m] = (d > THRD || d < -THRD) ? d : 0.0;
+            }
+        } else {
+#pragma unroll
+            for (int s = 0; s < S; ++s) R[s] = 0.0;
+#pragma unroll
+            for (int m = 0; m < MW; ++m) BR[m] = 0.0;
         }
-#pragma unroll
-        for (int m = 0; m < MW; ++m) {
-            const double d = BR[m] * p.dt;
-            BR[m] = (d > THRD || d < -THRD) ? d : 0.0;
+        if constexpr (Chem::kSrg) {
+            if (p.n_srg > 0) Chem::surrogate(p, kc, C, B, R, BR);
         }
 #pragma unroll
         for (int s = 0; s < S; ++s) {
@@ -220,7 +233,8 @@ __device__ __forceinline__ int fast_chain(const AdeK& k, int64_t n, uint32_t sto
 
 template <class Chem, int PARITY, int kFastBlock, int kMinBlocks>
 __global__ void __launch_bounds__(kFastBlock, kMinBlocks)
-ade_fast_kernel(const __grid_constant__ AdeK k, const uint32_t* __restrict__ list, int64_t count, int any_rxn) {
+ade_fast_kernel(const __grid_constant__ AdeK k, const __grid_constant__ typename Chem::Consts kc,
+                const uint32_t* __restrict__ list, int64_t count, int any_rxn) {
     constexpr int S = Chem::S, NMOB = Chem::NMOB;
     const AdeParams& p = k.p;
     const int64_t N = k.g.N, plane = k.g.plane;
@@ -261,7 +275,7 @@ ade_fast_kernel(const __grid_constant__ AdeK k, const uint32_t* __restrict__ lis
                     A[s] = 0.0;
                 }
             }
-            nonconv += fast_chain<Chem>(k, n, st.s, x, y, z, cls, C, A);
+            nonconv += fast_chain<Chem>(k, kc, n, st.s, x, y, z, cls, C, A);
 #pragma unroll
             for (int s = 0; s < S; ++s) {
                 if (Chem::mobile(s)) dcv[Chem::slot(s)] = (float)A[s];
@@ -312,12 +326,12 @@ ade_fast_kernel(const __grid_constant__ AdeK k, const uint32_t* __restrict__ lis
 }
 
 template <class Chem, int B, int MB>
-int fast_launch(Ctx* c, const AdeK& k, int any_rxn) {
+int fast_launch(Ctx* c, const AdeK& k, const typename Chem::Consts& kc, int any_rxn) {
     const int blocks = grid_for(c->n_live, B, 148 * MB * 16);
     if (c->ade_parity == 0)
-        ade_fast_kernel<Chem, 0, B, MB><<<blocks, B, 0, c->stream>>>(k, c->d_live, c->n_live, any_rxn);
+        ade_fast_kernel<Chem, 0, B, MB><<<blocks, B, 0, c->stream>>>(k, kc, c->d_live, c->n_live, any_rxn);
     else
-        ade_fast_kernel<Chem, 1, B, MB><<<blocks, B, 0, c->stream>>>(k, c->d_live, c->n_live, any_rxn);
+        ade_fast_kernel<Chem, 1, B, MB><<<blocks, B, 0, c->stream>>>(k, kc, c->d_live, c->n_live, any_rxn);
     CL_LAUNCH_CHECK("ade_fast_kernel");
     return CL_OK;
 }
@@ -325,7 +339,15 @@ int fast_launch(Ctx* c, const AdeK& k, int any_rxn) {
 template <class Chem>
 int fast_step(Ctx* c) {
     AdeK k = make_adek(c);
-    const bool any_rxn = c->ap.do_kin || c->ap.do_abio || c->ap.do_dissol || (Chem::NC > 0 && c->ap.do_eq);
+    const bool any_rxn = c->ap.do_kin || c->ap.do_abio || c->ap.do_dissol || (Chem::NC > 0 && c->ap.do_eq) ||
+                         (Chem::kSrg && c->ap.n_srg > 0);
+    typename Chem::Consts kc{};
+    if constexpr (Chem::kSrg) {
+        for (int o = 0; o < 2; ++o) {
+            if (c->h_srg_params[o].size() != (size_t)Chem::kP) { set_error("surrogate network not set"); return CL_ERR_STATE; }
+            for (int i = 0; i < Chem::kP; ++i) kc.w[o][i] = c->h_srg_params[o][i];
+        }
+    }
     int r = CL_OK;
     if (c->store_dirty && (r = store_update(c, 0))) return r;
     if (c->live_dirty && (r = build_live_list(c))) return r;
@@ -336,10 +358,10 @@ int fast_step(Ctx* c) {
         // launch shapes (threads per block x blocks per SM, which sets the
         // register cap): 128x4 measured fastest on the coupled workload
         switch (c->fast_variant) {
-            case 1: r = fast_launch<Chem, 128, 3>(c, k, ar); break;
-            case 2: r = fast_launch<Chem, 64, 6>(c, k, ar); break;
-            case 3: r = fast_launch<Chem, 64, 5>(c, k, ar); break;
-            default: r = fast_launch<Chem, 128, 4>(c, k, ar); break;
+            case 1: r = fast_launch<Chem, 128, 3>(c, k, kc, ar); break;
+            case 2: r = fast_launch<Chem, 64, 6>(c, k, kc, ar); break;
+            case 3: r = fast_launch<Chem, 64, 5>(c, k, kc, ar); break;
+            default: r = fast_launch<Chem, 128, 4>(c, k, kc, ar); break;
         }
         if (r) return r;
         c->launches += 1;
@@ -360,6 +382,7 @@ int chem_match(const cl_config& cfg) {
     if (ChemCoupled::matches(cfg)) return ChemCoupled::kId;
     if (ChemBiotic4::matches(cfg)) return ChemBiotic4::kId;
     if (ChemZhao24::matches(cfg)) return ChemZhao24::kId;
+    if (ChemSurrogate2::matches(cfg)) return ChemSurrogate2::kId;
     return 0;
 }
 
@@ -368,8 +391,17 @@ const char* chem_name(int id) {
         case ChemCoupled::kId: return ChemCoupled::kName;
         case ChemBiotic4::kId: return ChemBiotic4::kName;
         case ChemZhao24::kId: return ChemZhao24::kName;
+        case ChemSurrogate2::kId: return ChemSurrogate2::kName;
         default: return "run-time rate table";
     }
+}
+
+// whether the context holds what its compiled chemistry's step needs (a
+// surrogate chemistry: both networks set, of the compiled shape); otherwise
+// the step runs the run-time-table launches
+bool chem_ready(const Ctx* c) {
+    if (c->chem == ChemSurrogate2::kId) return ChemSurrogate2::ready(c->ap);
+    return true;
 }
 
 int ade_step_fast(Ctx* c) {
@@ -377,6 +409,7 @@ int ade_step_fast(Ctx* c) {
         case ChemCoupled::kId: return fast_step<ChemCoupled>(c);
         case ChemBiotic4::kId: return fast_step<ChemBiotic4>(c);
         case ChemZhao24::kId: return fast_step<ChemZhao24>(c);
+        case ChemSurrogate2::kId: return fast_step<ChemSurrogate2>(c);
         default: set_error("no compiled chemistry selected"); return CL_ERR_STATE;
     }
 }

@@ -526,6 +526,7 @@ int cl_set_surrogate(cl_ctx* h, int32_t slot, const cl_surrogate_net* net) {
     CL_CUDA(cudaStreamSynchronize(c->stream));
     d.params = c->d_srg_params[slot];
     c->ap.net[slot] = d;
+    c->h_srg_params[slot] = std::move(hp);
     return CL_OK;
 }
 

@@ -27,6 +27,9 @@
 //   abiotic(p, C, R, mask)          rates per second (defineAbioticRxnKinetics)
 //   Tab                             the tableau the Newton solve reads: TabRun
 //                                   (cl_config's) or TabFixed (compiled in)
+//   kSrg, Consts                    whether the step runs surrogate networks
+//                                   (surrogate(p, consts, C, B, D, DB)), and the
+//                                   constants the kernel takes for them
 // Rates follow the run-time table's arithmetic (rates_dev) term for term, so
 // a configuration runs to the same numbers on either launch.
 #pragma once
@@ -93,10 +96,16 @@ inline bool rxn_is(const cl_rxn& r, int microbe, std::initializer_list<int> mono
 // Equilibrium: 3 components, CO3-- (species 6), Ca2+ (4) and H+ (5), with
 // HCO3- (3) = CO3-- + H+ and CaCO3(aq) (7) = CO3-- + Ca2+ (stoichiometry
 // compiled in, logK from the run).
+// what a chemistry passes to the fused kernel besides AdeK (in the kernel's
+// parameter space): nothing, for a chemistry without networks
+struct NoConsts { int unused; };
+
 struct ChemCoupled {
     static constexpr int kId = 1;
     static constexpr const char* kName = "coupled carbonate (8 mobile + 1 mineral, dual Monod, 3 components)";
     static constexpr int S = 9, NMOB = 8, M = 1, NC = 3, MW = 1;
+    static constexpr bool kSrg = false;     // no surrogate networks
+    using Consts = NoConsts;
     __host__ __device__ static constexpr bool mobile(int s) { return s < 8; }
     __host__ __device__ static constexpr int slot(int s) { return s; }
     struct Fix {
@@ -171,6 +180,8 @@ struct ChemBiotic4 {
     static constexpr int kId = 2;
     static constexpr const char* kName = "biotic dual Monod (4 mobile solutes, 1 microbe)";
     static constexpr int S = 4, NMOB = 4, M = 1, NC = 0, MW = 1;
+    static constexpr bool kSrg = false;     // no surrogate networks
+    using Consts = NoConsts;
     using Tab = TabRun;
     __host__ __device__ static constexpr bool mobile(int) { return true; }
     __host__ __device__ static constexpr int slot(int s) { return s; }
@@ -221,6 +232,8 @@ struct ChemZhao24 {
     static constexpr int kId = 3;
     static constexpr const char* kName = "Zhao uranium network (24 substrates, 12 biomass pools)";
     static constexpr int S = 24, NMOB = 15, M = 12, NC = 0, MW = 12;
+    static constexpr bool kSrg = false;     // no surrogate networks
+    using Consts = NoConsts;
     using Tab = TabRun;
     __host__ __device__ static constexpr bool mobile(int s) {
         return !(s == 2 || s == 4 || s == 5 || s == 6 || s == 9 || s == 13 || s == 21 || s == 22 || s == 23);
@@ -251,5 +264,155 @@ struct ChemZhao24 {
         clrl::zhao::abiotic(clrl::cspan{Cf, S}, clrl::dspan{R, S}, mask);
     }
 };
+
+// ---- the surrogate workload: two organisms' networks in the step ------------------
+// Six mobile solutes and two sessile microbes, no rate table reactions (the
+// table's decay of each microbe still applies), the surrogate reaction type
+// of two organisms (organism o on microbe o with network o), each network
+// 3 -> 20 tanh -> 20 tanh -> 4.  surrogate() is run_surrogate3D
+// (src/complab3d_processors_surrogate.hh:94-295) as surrogate_chain of
+// ade_kernels.cuh evaluates it, operation for operation, with the network's
+// shape compiled in and its weights in the kernel's parameter space, so that
+// every weight is an operand of its FMA rather than a load.
+struct ChemSurrogate2 {
+    static constexpr int kId = 4;
+    static constexpr const char* kName = "surrogate rates (6 mobile solutes, 2 organisms, 3-20-20-4 networks)";
+    static constexpr int S = 6, NMOB = 6, M = 2, NC = 0, MW = 2;
+    static constexpr bool kSrg = true;
+    static constexpr int kL = 3;
+    __host__ __device__ static constexpr int width(int l) { return l == 0 ? 3 : l == 3 ? 4 : 20; }
+    __host__ __device__ static constexpr int poff(int l) {
+        int o = 0;
+        for (int j = 0; j < l; ++j) o += width(j + 1) * width(j) + width(j + 1);
+        return o;
+    }
+    static constexpr int kP = (20 * 3 + 20) + (20 * 20 + 20) + (4 * 20 + 4);   // parameters per network
+    struct Consts { float w[2][kP]; };
+    using Tab = TabRun;
+    __host__ __device__ static constexpr bool mobile(int) { return true; }
+    __host__ __device__ static constexpr int slot(int s) { return s; }
+    static bool matches(const cl_config& c) {
+        if (c.n_solutes != S || c.n_microbes != M || c.n_rxn != 0 || c.n_srg != 2 || c.use_equilibrium) return false;
+        for (int s = 0; s < S; ++s) if (c.immobile[s]) return false;
+        for (int o = 0; o < 2; ++o) if (c.srg[o].microbe != o || c.srg[o].net != o) return false;
+        return c.rate_law == CL_RATELAW_TABLE;
+    }
+    // host: the networks set on the context have the compiled shape
+    static bool ready(const AdeParams& ap) {
+        for (int o = 0; o < 2; ++o) {
+            const SrgNetDev& d = ap.net[o];
+            if (d.L != kL || !d.params) return false;
+            for (int l = 0; l <= kL; ++l) if (d.w[l] != width(l)) return false;
+            for (int l = 0; l < kL; ++l) if (d.poff[l] != poff(l)) return false;
+        }
+        return true;
+    }
+    // rates_dev with no reactions: the microbes' decay
+    __host__ __device__ static void kinetics(const AdeParams& p, const double (&)[S], const double (&B)[MW],
+                                             double (&R)[S], double (&BR)[MW], int) {
+#pragma unroll
+        for (int s = 0; s < S; ++s) R[s] = 0.0;
+#pragma unroll
+        for (int m = 0; m < MW; ++m) BR[m] = 0.0;
+#pragma unroll
+        for (int m = 0; m < M; ++m) BR[m] -= p.decay[m] * fmax(B[m], 0.0);
+#pragma unroll
+        for (int m = 0; m < MW; ++m) if (!isfinite(BR[m])) BR[m] = 0.0;
+    }
+    __host__ __device__ static void abiotic(const AdeParams&, const double (&)[S], double (&R)[S], int) {
+#pragma unroll
+        for (int s = 0; s < S; ++s) R[s] = 0.0;
+    }
+    // the surrogate increments of one voxel, added into D and DB
+    __device__ static void surrogate(const AdeParams& p, const Consts& kc, const double (&Cur)[S],
+                                     const double (&B)[MW], double (&D)[S], double (&DB)[MW]) {
+        bool any = false;
+#pragma unroll
+        for (int o = 0; o < 2; ++o) any = any || B[o] > THRD;
+        if (!any) return;
+        double conc[S], draw[S];
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            const double c = Cur[s];
+            conc[s] = c > THRD ? c : 0.0;
+            draw[s] = 0.0;
+        }
+#pragma unroll
+        for (int o = 0; o < 2; ++o) {
+            const cl_srg_organism& org = p.srg[o];
+            const SrgNetDev& net = p.net[o];
+            const double b = B[o];
+            if (!(b > THRD)) continue;
+            double fin[S];
+            const double denom = b * org.mw * p.dt;
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                const double av = conc[s];
+                const double mm = (org.kc[s] + av > 0.0) ? av / (org.kc[s] + av) : 0.0;
+                double exh = 0.0;
+                if (denom > 1e-30) { exh = -av * 3.6e6 / denom; if (exh < -1e4) exh = -1e4; }
+                double v = org.vmax[s] > THRD ? org.vmax[s] * mm : -exh * mm;
+                const double cap = -exh;
+                if (cap > 0.0 && v > cap) v = cap;
+                fin[s] = v;
+            }
+            float a[20], t[20];
+#pragma unroll
+            for (int i = 0; i < width(0); ++i) {
+                const int kind = org.in_kind[i], idx = org.in_index[i];
+                double sel_f = 0.0, sel_c = 0.0;
+#pragma unroll
+                for (int s = 0; s < S; ++s) if (s == idx) { sel_f = fin[s]; sel_c = conc[s]; }
+                float v = kind == CL_SRG_IN_FIN ? (float)sel_f : kind == CL_SRG_IN_CONC ? (float)sel_c : (float)b;
+                v = fminf(fmaxf(v, net.xlo[i]), net.xhi[i]);
+                a[i] = (v - net.xo[i]) * net.xg[i] + net.xymin;
+            }
+#pragma unroll
+            for (int l = 0; l < kL; ++l) {
+                const int wi = width(l), wo = width(l + 1);
+                const float* W = kc.w[o] + poff(l);
+#pragma unroll
+                for (int q = 0; q < wo; ++q) {
+                    float acc = W[wo * wi + q];
+#pragma unroll
+                    for (int i = 0; i < wi; ++i) acc = fmaf(W[q * wi + i], a[i], acc);
+                    t[q] = (l < kL - 1) ? tanhf(acc) : acc;
+                }
+#pragma unroll
+                for (int q = 0; q < wo; ++q) a[q] = t[q];
+            }
+            double mu = 0.0;
+            double fout[S];
+#pragma unroll
+            for (int s = 0; s < S; ++s) fout[s] = fin[s];
+#pragma unroll
+            for (int q = 0; q < width(kL); ++q) {
+                const double y = ((double)a[q] - net.yymin) / net.yg[q] + net.yo[q];
+                if (org.out_kind[q] == CL_SRG_OUT_GROWTH) mu = y;
+                else {
+                    const int idx = org.out_index[q];
+#pragma unroll
+                    for (int s = 0; s < S; ++s) if (s == idx) fout[s] = y;
+                }
+            }
+            if (mu < 1e-8 || !isfinite(mu)) mu = 0.0;
+            double dB = (fabs(mu) < THRD) ? -org.kd * b * p.dt : mu * b * p.dt / 3600.0;
+            if (dB + b < 0.0) dB = -b;
+            if (fabs(dB) > THRD) DB[o] += dB;
+#pragma unroll
+            for (int s = 0; s < S; ++s) draw[s] += -fout[s] * b * org.mw * p.dt / 3.6e6;
+        }
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            double d = draw[s];
+            if (fabs(d) <= THRD) continue;
+            if (d + conc[s] < 0.0) d = -conc[s];
+            if (d > 0.0) d = 0.0;
+            if (fabs(d) > THRD) D[s] += d;
+        }
+    }
+};
+
+static_assert(ChemSurrogate2::poff(ChemSurrogate2::kL) == ChemSurrogate2::kP, "network size");
 
 }  // namespace cl

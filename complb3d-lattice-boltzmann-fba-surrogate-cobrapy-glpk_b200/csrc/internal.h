@@ -5,6 +5,7 @@
 struct cl_eq_solver;
 #include <cstdint>
 #include <string>
+#include <vector>
 #include "../../include/complab_gpu.h"
 #include "lattice.cuh"
 
@@ -105,6 +106,7 @@ struct Ctx {
     float*   d_rho_adj = nullptr;    // n_mob*2*plane : pre-collision density next to each x face
     int32_t* d_eq_iters = nullptr;   // N
     float*   d_srg_params[CL_MAX_SRG_ORG] = {nullptr, nullptr};
+    std::vector<float> h_srg_params[CL_MAX_SRG_ORG];   // host copies (a compiled chemistry's kernel takes them)
     float*   d_eq_x = nullptr;       // n_comp*N previous converged log10 free components, by storage index (NaN: none)
     float*   d_eq_xp = nullptr;      // n_comp*N the solution before that, by storage index (NaN: none)
     uint8_t* d_phase = nullptr;      // N dissolvable phase id, 0 = none (dissolution only)
@@ -207,6 +209,7 @@ int ops_collide(Ctx* c);
 int ops_react(Ctx* c, int ops);
 int ops_stream(Ctx* c);      // the transport step of the compiled chemistry c->chem
 int chem_match(const cl_config& cfg);   // id of the compiled chemistry cfg has the structure of, or 0
+bool chem_ready(const Ctx* c);          // the context holds what its compiled chemistry needs
 const char* chem_name(int id);
 int ade_density(Ctx* c, int s, double* d_out);
 int flow_population_io(Ctx* c, float* d_natural, int to_natural);

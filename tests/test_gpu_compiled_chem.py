@@ -87,3 +87,63 @@ def test_biotic_compiled_matches_table_and_oracle(gpu_lib, pkg, wl, variant):
     for s in range(cfg.n_solutes):
         assert rel_l2(fast["conc"][s], tr.density(s)) < 1e-4, s
     assert rel_l2(fast["bio"], tr.biomass(0)) < 1e-5
+
+
+def test_surrogate_compiled_matches_table_and_oracle(gpu_lib, pkg, wl):
+    """The surrogate workload's structure (six mobile solutes, two organisms
+    with 3 -> 20 -> 20 -> 4 networks) runs its step in one launch with the
+    networks' weights in the kernel's parameter space; the same fields as the
+    run-time launches (rel. L2 <= 1e-12) and as the FP64 oracle."""
+    mask = wl.sphere_pack(34, 20, 20, 0.40, 2.0, 4.0, seed=41)
+    nx, ny, nz = mask.shape
+    cfg = wl.surrogate_config(pkg, nx, ny, nz)
+    nets = wl.surrogate_nets(pkg)
+    bio = [wl.seed_biomass(mask, 42 + m, frac=0.3, lo=0.005, hi=0.05) for m in range(2)]
+
+    def run(compiled, steps=30):
+        lat = pkg.Lattice(cfg)
+        lat.upload_mask(mask)
+        lat.flow_init()
+        lat.flow_steps(60)
+        lat.couple_velocity()
+        lat.set_option(pkg.OPT_COMPILED_CHEM, 1 if compiled else 0)
+        for slot in range(2):
+            lat.set_surrogate(slot, nets[slot])
+        lat.ade_init()
+        for m in range(2):
+            lat.set_field(pkg.FIELD_BIOMASS, m, bio[m])
+        for _ in range(steps):
+            lat.step(1)
+        out = {"conc": [lat.field(pkg.FIELD_CONC, s).reshape(-1) for s in range(cfg.n_solutes)],
+               "bio": [lat.field(pkg.FIELD_BIOMASS, m).reshape(-1) for m in range(2)],
+               "chem": lat.get_option(pkg.OPT_COMPILED_CHEM),
+               "u": np.stack([lat.field(pkg.FIELD_VELOCITY, k).reshape(-1) for k in range(3)])}
+        lat.close()
+        return out
+
+    fast, table = run(True), run(False)
+    assert fast["chem"] == pkg.CHEM_SURROGATE2 and table["chem"] == 0
+    for s in range(cfg.n_solutes):
+        assert rel_l2(fast["conc"][s], table["conc"][s]) <= 1e-12, s
+    for m in range(2):
+        assert rel_l2(fast["bio"][m], table["bio"][m]) <= 1e-12, m
+    tr = o.Transport(cfg, mask, u=fast["u"])
+    tr.set_surrogates(nets)
+    for m in range(2):
+        tr.set_biomass(m, bio[m])
+    tr.step(30)
+    for s in range(cfg.n_solutes):
+        assert rel_l2(fast["conc"][s], tr.density(s)) < 1e-4, s
+    for m in range(2):
+        assert rel_l2(fast["bio"][m], tr.biomass(m)) < 1e-5, m
+    # a network of another shape: the step falls back to the run-time launches
+    lat = pkg.Lattice(cfg)
+    lat.upload_mask(mask)
+    lat.flow_init()
+    odd = pkg.make_surrogate_net([3, 8, 4], [np.full((8, 3), 0.1), np.full((4, 8), 0.1)],
+                                 [np.zeros(8), np.zeros(4)], np.zeros(3), np.ones(3), np.zeros(4), np.ones(4))
+    lat.set_surrogate(0, odd)
+    lat.set_surrogate(1, nets[1])
+    lat.ade_init()
+    assert lat.step(1) == pkg.OK
+    lat.close()
