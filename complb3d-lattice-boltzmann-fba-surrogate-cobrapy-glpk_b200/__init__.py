@@ -29,7 +29,7 @@ RED_SUM, RED_MIN, RED_MAX, RED_COUNT_EQ = range(4)
 EQ_START_COLD, EQ_START_GIVEN, EQ_START_LEARNED = range(3)
 EQ_NET_TCGEN05, EQ_NET_MMA_SYNC = 0, 1
 EQ_SOLVER_NEWTON, EQ_SOLVER_PCF = 0, 1
-SRG_TENSOR, SRG_FP32 = 0, 1
+SRG_TENSOR, SRG_FP32, SRG_TCGEN05 = 0, 1, 2
 MAX_SRG_ORG = 2
 SRG_IN_FIN, SRG_IN_CONC, SRG_IN_BIOMASS = 0, 1, 2
 SRG_OUT_GROWTH, SRG_OUT_FOUT = 0, 1

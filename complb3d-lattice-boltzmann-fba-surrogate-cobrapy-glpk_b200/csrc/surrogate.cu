@@ -9,9 +9,12 @@
 // CL_SRG_TENSOR: one warp carries 16 voxels through every layer with BF16
 //   m16n8k16 tensor-core MMAs (FP32 accumulate); weights are staged once per
 //   block in shared memory, padded to K multiples of 16 and N multiples of 8.
+// CL_SRG_TCGEN05: 128 voxels per CTA through tcgen05.mma (M = 128, K and N
+//   padded to 16 and 32 columns), FP32 accumulators in tensor memory.
 // CL_SRG_FP32: the FP32 CUDA-core reference kernel, one voxel per thread.
 #include "internal.h"
 #include "mma.cuh"
+#include "umma.cuh"
 
 namespace cl {
 
@@ -102,6 +105,133 @@ __global__ void __launch_bounds__(SRG_WARPS * 32) srg_tensor_kernel(SrgDev d, co
     }
 }
 
+// The same inference on the fifth-generation tensor core: one voxel per
+// thread and TMEM lane, 128 per CTA; per layer one thread issues K/16 MMAs
+// (K = pad16 of the layer's input width, N = pad16 of its output width, both
+// at most 32) on the activation tile and the layer's weights, held in shared
+// memory as K-major 8x8 core matrices (umma.cuh); the epilogue reads the
+// thread's row from TMEM, adds the bias, applies tansig and writes the next
+// layer's BF16 operand (the output layer: the reverse mapminmax).  Every wait
+// on the MMAs is bounded; a timeout sets g_srg_tc_err and the CTA stops.
+__device__ unsigned int g_srg_tc_err;
+constexpr int SRG_TC = 128;
+
+struct SrgSmemTc {
+    alignas(128) unsigned char act[SRG_TC * SW * 2];                 // [128][32]
+    alignas(128) unsigned char W[CL_SRG_MAX_LAYERS][SW * SW * 2];    // [32 out][32 in] per layer
+    float B[CL_SRG_MAX_LAYERS][SW];
+    alignas(8) unsigned long long bar;
+    uint32_t tmem;
+};
+
+__global__ void __launch_bounds__(SRG_TC) srg_tc_kernel(SrgDev d, const float* params, const float* x, float* y,
+                                                        int64_t n) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    SrgSmemTc& s = *reinterpret_cast<SrgSmemTc*>(sm);
+    const int tid = threadIdx.x, warp = tid >> 5;
+    for (int l = 0; l < d.L; ++l) {
+        const int wi = d.w[l], wo = d.w[l + 1];
+        const float* p = params + d.poff[l];
+        for (int e = tid; e < SW * SW; e += SRG_TC) {
+            const int o = e / SW, i = e - o * SW;
+            const float v = (o < wo && i < wi) ? p[o * wi + i] : 0.f;
+            *reinterpret_cast<__nv_bfloat16*>(s.W[l] + umma_off(o, i, SW / 8)) = __float2bfloat16_rn(v);
+        }
+        for (int o = tid; o < SW; o += SRG_TC) s.B[l][o] = (o < wo) ? p[wo * wi + o] : 0.f;
+    }
+    const uint32_t bar = smem_u32(&s.bar);
+    if (tid == 0) mbar_init(bar, 1);
+    if (warp == 0) tmem_alloc(smem_u32(&s.tmem), 32);
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s.tmem, lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+    const uint32_t aAct = smem_u32(s.act);
+    constexpr int kLimit = 1 << 20;
+    const int win = d.w[0], wout = d.w[d.L];
+    uint32_t phase = 0;
+    bool ok = true;
+    const int64_t ntiles = (n + SRG_TC - 1) / SRG_TC;
+    for (int64_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+        const int64_t s0 = tile * SRG_TC;
+        const int m = tid;
+        const bool valid = s0 + m < n;
+        // input: clamp, mapminmax, BF16, zero beyond the input width
+        for (int c = 0; c < SW / 8; ++c) {
+            uint32_t wv[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                float v2[2];
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int i = 8 * c + 2 * j + h;
+                    float v = 0.f;
+                    if (valid && i < win) {
+                        float xv = x[(s0 + m) * win + i];
+                        xv = fminf(fmaxf(xv, d.xlo[i]), d.xhi[i]);
+                        v = (xv - d.xo[i]) * d.xg[i] + d.xymin;
+                    }
+                    v2[h] = v;
+                }
+                wv[j] = pack_bf16(v2[0], v2[1]);
+            }
+            *reinterpret_cast<uint4*>(s.act + umma_off(m, 8 * c, SW / 8)) = make_uint4(wv[0], wv[1], wv[2], wv[3]);
+        }
+        for (int l = 0; l < d.L; ++l) {
+            const int K = pad16(d.w[l]), N = pad16(d.w[l + 1]);
+            const bool last = (l == d.L - 1);
+            fence_async_smem();
+            tc_fence_before();
+            __syncthreads();
+            tc_fence_after();
+            if (tid == 0) {
+                const uint32_t aW = smem_u32(s.W[l]);
+                for (int kb = 0; kb < K / 16; ++kb)
+                    umma_bf16(tmem, umma_desc(aAct, kb, SW / 8), umma_desc(aW, kb, SW / 8), umma_idesc_bf16(N), kb > 0);
+                umma_commit(bar);
+            }
+            if (!__syncthreads_and(mbar_wait(bar, phase & 1u, kLimit))) { ok = false; break; }
+            ++phase;
+            tc_fence_after();
+            for (int c = 0; c < N / 16; ++c) {
+                float acc[16];
+                tmem_ld16(lane_addr + (uint32_t)(16 * c), acc);
+                if (last) {
+                    if (valid)
+                        for (int j = 0; j < 16; ++j) {
+                            const int o = 16 * c + j;
+                            if (o < wout) y[(s0 + m) * wout + o] = (acc[j] + s.B[l][o] - d.yymin) / d.yg[o] + d.yo[o];
+                        }
+                } else {
+                    uint32_t wv[8];
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        const int o = 16 * c + 2 * j;
+                        const float v0 = o < d.w[l + 1] ? tanhf(acc[2 * j] + s.B[l][o]) : 0.f;
+                        const float v1 = o + 1 < d.w[l + 1] ? tanhf(acc[2 * j + 1] + s.B[l][o + 1]) : 0.f;
+                        wv[j] = pack_bf16(v0, v1);
+                    }
+                    *reinterpret_cast<uint4*>(s.act + umma_off(m, 16 * c, SW / 8)) = make_uint4(wv[0], wv[1], wv[2], wv[3]);
+                    *reinterpret_cast<uint4*>(s.act + umma_off(m, 16 * c + 8, SW / 8)) = make_uint4(wv[4], wv[5], wv[6], wv[7]);
+                }
+            }
+            if (!last && N < SW) {
+                // columns beyond this layer's output: zero
+                const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+                for (int c = N / 8; c < SW / 8; ++c) *reinterpret_cast<uint4*>(s.act + umma_off(m, 8 * c, SW / 8)) = z;
+            }
+        }
+    }
+    if (!ok) {
+        mbar_wait(bar, phase & 1u, kLimit);
+        if (tid == 0) atomicOr(&g_srg_tc_err, 1u);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, 32);
+}
+
 // FP32 CUDA-core reference: one voxel per thread, weights in shared memory
 __global__ void srg_fp32_kernel(SrgDev d, const float* params, int n_params, const float* x, float* y, int64_t n) {
     extern __shared__ __align__(16) unsigned char sm[];
@@ -174,6 +304,10 @@ extern "C" int cl_surrogate_batch_device(const cl_surrogate_net* net, const floa
         const int64_t tiles = (n + 15) / 16;
         const int blocks = grid_for(tiles, SRG_WARPS, 148 * 4);
         srg_tensor_kernel<<<blocks, SRG_WARPS * 32, smem, st>>>(d, dp, d_x, d_y, n);
+    } else if (mode == CL_SRG_TCGEN05) {
+        CL_CUDA(cudaFuncSetAttribute(srg_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SrgSmemTc)));
+        srg_tc_kernel<<<grid_for((n + SRG_TC - 1) / SRG_TC, 1, 148 * 4), SRG_TC, sizeof(SrgSmemTc), st>>>(d, dp, d_x,
+                                                                                                          d_y, n);
     } else {
         srg_fp32_kernel<<<grid_for(n, 256, 148 * 8), 256, sizeof(float) * np, st>>>(d, dp, np, d_x, d_y, n);
     }
@@ -197,6 +331,18 @@ extern "C" int cl_surrogate_batch_host(const cl_surrogate_net* net, const float*
     if (!r) {
         e = cudaMemcpy(y, dy, sizeof(float) * n * wout, cudaMemcpyDeviceToHost);
         if (e != cudaSuccess) r = cuda_fail(e, "copy");
+    }
+    if (!r && mode == CL_SRG_TCGEN05) {
+        unsigned int v = 0;
+        e = cudaMemcpyFromSymbol(&v, g_srg_tc_err, sizeof(v));
+        if (e == cudaSuccess && v) {
+            const unsigned int z = 0;
+            cudaMemcpyToSymbol(g_srg_tc_err, &z, sizeof(z));
+            set_error("cl_surrogate_batch_host: the tensor-core inference timed out waiting for its MMAs");
+            r = CL_ERR_CUDA;
+        } else if (e != cudaSuccess) {
+            r = cuda_fail(e, "copy");
+        }
     }
     cudaFree(dx); cudaFree(dy);
     return r;

@@ -580,6 +580,8 @@ int cl_eq_predict_device(cl_eq_solver* s, const double* d_totals, double* d_logf
 
 #define CL_SRG_TENSOR 0   /* BF16 tensor-core inference, FP32 accumulate */
 #define CL_SRG_FP32   1   /* FP32 CUDA-core reference kernel */
+#define CL_SRG_TCGEN05 2  /* BF16 on tcgen05.mma, FP32 accumulators in tensor memory (128 voxels per CTA);
+                             cl_surrogate_batch_host reports a timed-out MMA wait as CL_ERR_CUDA */
 int cl_surrogate_batch_device(const cl_surrogate_net* net, const float* d_x, float* d_y,
                               int64_t n, int32_t mode, void* stream);
 int cl_surrogate_batch_host(const cl_surrogate_net* net, const float* x, float* y,

@@ -48,3 +48,9 @@ def test_tensor_core_matches_fp32(gpu_lib, pkg, n):
     assert np.max(np.abs(y32 - yo) / span) < 1e-5
     assert np.max(np.abs(ytc - y32) / span) < 2e-2
     assert np.max(np.abs(ytc - yo) / span) < 2e-2       # the tensor path against FP64 directly
+    # the tcgen05 path: the same BF16 operands and activations as the warp
+    # MMA path, only the order of the FP32 sums differs
+    y5 = pkg.surrogate_batch(net, x, mode=pkg.SRG_TCGEN05)
+    assert np.isfinite(y5).all()
+    assert np.max(np.abs(y5 - ytc) / span) < 5e-3
+    assert np.max(np.abs(y5 - yo) / span) < 2e-2
