@@ -296,6 +296,7 @@ int cl_destroy(cl_ctx* h) {
                     c->d_dc, c->d_live, c->d_live_blk, c->d_sidx, c->d_site_of, c->d_flive, c->d_fsidx,
                     c->d_pair_T, c->d_pair_X, c->d_pair_count};
     if (c->learn) cl_eq_destroy(c->learn);
+    if (c->flow_graph) cudaGraphExecDestroy(c->flow_graph);
     for (void* p : ptrs) if (p) cudaFree(p);
     for (int o = 0; o < CL_MAX_SRG_ORG; ++o) if (c->d_srg_params[o]) cudaFree(c->d_srg_params[o]);
     for (int k = 0; k < Ctx::kTimedKernels; ++k)
@@ -348,8 +349,71 @@ int cl_flow_init(cl_ctx* h) {
     return CL_OK;
 }
 
+// Runs of flow steps are replayed from a CUDA graph: a chunk of
+// kFlowGraphSteps steps (an even number, so the AA parity comes back) is
+// captured once per FlowGraphKey and launched as one graph, so a small
+// lattice steps at the kernels' pace instead of the host's launch rate.
+// Timed runs (cl_timing) and contexts on the legacy default stream launch
+// step by step.
+constexpr int kFlowGraphSteps = 32;
+
+static FlowGraphKey flow_key(const Ctx* c, int use_tracer) {
+    FlowGraphKey k{};
+    k.f = c->d_f; k.list = c->d_flive; k.sidx = c->d_fsidx; k.cls = c->d_ns_cls; k.tracer = c->d_tracer;
+    k.part = c->d_energy_part; k.count = c->n_flive; k.n_bgk = c->n_bgk;
+    k.tau_ns = c->cfg.tau_ns; k.perm_ratio = c->cfg.perm_ratio; k.rho_in = c->cfg.rho_in; k.rho_out = c->cfg.rho_out;
+    k.energy_blocks = c->energy_blocks; k.nodyn_coupled = c->flow_nodyn_coupled ? 1 : 0; k.use_tracer = use_tracer;
+    k.parity = c->flow_parity; k.stream = c->stream;
+    return k;
+}
+
+static bool same_key(const FlowGraphKey& a, const FlowGraphKey& b) {
+    return a.f == b.f && a.list == b.list && a.sidx == b.sidx && a.cls == b.cls && a.tracer == b.tracer &&
+           a.part == b.part && a.count == b.count && a.n_bgk == b.n_bgk && a.tau_ns == b.tau_ns &&
+           a.perm_ratio == b.perm_ratio && a.rho_in == b.rho_in && a.rho_out == b.rho_out &&
+           a.energy_blocks == b.energy_blocks && a.nodyn_coupled == b.nodyn_coupled &&
+           a.use_tracer == b.use_tracer && a.parity == b.parity && a.stream == b.stream;
+}
+
+static int flow_graph_ready(Ctx* c, int use_tracer) {
+    const FlowGraphKey key = flow_key(c, use_tracer);
+    if (c->flow_graph && same_key(key, c->flow_graph_key)) return CL_OK;
+    if (c->flow_graph) { cudaGraphExecDestroy(c->flow_graph); c->flow_graph = nullptr; }
+    CL_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    const int64_t launches0 = c->launches;
+    const int parity0 = c->flow_parity;
+    int r = CL_OK;
+    for (int s = 0; s < kFlowGraphSteps && !r; ++s) r = flow_step(c, use_tracer);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    c->launches = launches0;                 // nothing ran yet
+    c->flow_parity = parity0;
+    if (r) { if (g) cudaGraphDestroy(g); return r; }
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    const cudaError_t ei = cudaGraphInstantiate(&c->flow_graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) { c->flow_graph = nullptr; return cuda_fail(ei, "cudaGraphInstantiate"); }
+    c->flow_graph_key = key;
+    return CL_OK;
+}
+
 static int run_flow(Ctx* c, int32_t n, int use_tracer) {
-    for (int32_t i = 0; i < n; ++i) {
+    int32_t i = 0;
+    // a step that brings the storage or the list up to date runs plainly
+    while (i < n && (c->fstore_dirty || c->flive_dirty)) {
+        int r = flow_step(c, use_tracer);
+        if (r) return r;
+        ++i;
+    }
+    if (!c->timing && c->stream != nullptr && n - i >= kFlowGraphSteps) {
+        int r = flow_graph_ready(c, use_tracer);
+        if (r) return r;
+        for (; n - i >= kFlowGraphSteps; i += kFlowGraphSteps) {
+            CL_CUDA(cudaGraphLaunch(c->flow_graph, c->stream));
+            c->launches += 2 * kFlowGraphSteps;
+        }
+    }
+    for (; i < n; ++i) {
         int r = flow_step(c, use_tracer);
         if (r) return r;
     }

@@ -77,6 +77,16 @@ struct AdeParams {
     cl_phase phase[CL_MAX_PHASES];
 };
 
+// What a captured run of flow steps depends on: the launches it replays
+// read these, so a graph is reused only while all of them are unchanged.
+struct FlowGraphKey {
+    const void* f; const void* list; const void* sidx; const void* cls; const void* tracer; const void* part;
+    int64_t count, n_bgk;
+    double tau_ns, perm_ratio, rho_in, rho_out;
+    int energy_blocks, nodyn_coupled, use_tracer, parity;
+    cudaStream_t stream;
+};
+
 struct Ctx {
     cl_config cfg;
     Geo geo;
@@ -107,6 +117,8 @@ struct Ctx {
     int32_t* d_eq_iters = nullptr;   // N
     float*   d_srg_params[CL_MAX_SRG_ORG] = {nullptr, nullptr};
     std::vector<float> h_srg_params[CL_MAX_SRG_ORG];   // host copies (a compiled chemistry's kernel takes them)
+    cudaGraphExec_t flow_graph = nullptr;   // a captured run of flow steps, valid for flow_graph_key
+    FlowGraphKey flow_graph_key{};
     float*   d_eq_x = nullptr;       // n_comp*N previous converged log10 free components, by storage index (NaN: none)
     float*   d_eq_xp = nullptr;      // n_comp*N the solution before that, by storage index (NaN: none)
     uint8_t* d_phase = nullptr;      // N dissolvable phase id, 0 = none (dissolution only)
