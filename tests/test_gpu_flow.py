@@ -213,3 +213,30 @@ def test_flow_populations_need_state(gpu_lib, pkg, wl):
     with pytest.raises(pkg.CLError):
         lat.set_flow_populations(np.zeros((19, mask.size), np.float32))   # no mask yet
     lat.close()
+
+
+def test_graph_replayed_runs_match_step_by_step(gpu_lib, pkg, wl):
+    """Runs of flow steps are replayed from a captured CUDA graph of 32 steps
+    (cl_timing on launches them step by step): the same populations bit for
+    bit over runs of 70 steps (two graph chunks and six steps), an odd run
+    that changes the parity the next capture starts from, a pressure change
+    (a new capture), and a converging flow_solve."""
+    mask = _pack(wl)
+    nx, ny, nz = mask.shape
+    cfg = pkg.make_config(nx, ny, nz, tau_ns=0.8, rho_in=1.001, rho_out=1.0)
+    out = []
+    for timed in (False, True):
+        lat = pkg.Lattice(cfg)
+        lat.upload_mask(mask)
+        lat.flow_init()
+        lat.timing(timed)
+        lat.flow_steps(70)
+        lat.flow_steps(33)
+        lat.flow_steps(64)
+        lat.set_flow_pressure(1.002, 1.0)
+        lat.flow_steps(70)
+        it, _ = lat.flow_solve(20000, 1e-6)
+        out.append((lat.flow_populations().copy(), it))
+        lat.close()
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    assert out[0][1] == out[1][1]
