@@ -140,7 +140,7 @@ def load_library(path=LIB_PATH):
         ("cl_device_bytes", [vp, P(ctypes.c_uint64)]), ("cl_abi_sizes", [vp, c_int32]),
         ("cl_timing_enable", [vp, c_int32]), ("cl_timing_read", [vp, c_int32, P(c_double), P(c_int64)]),
         ("cl_launch_count", [vp, P(c_int64)]), ("cl_set_surrogate", [vp, c_int32, vp]),
-        ("cl_ca_redistribute", [vp, P(c_int32), P(c_int64), P(c_double)]), ("cl_ca_update_mask", [vp, P(c_int64)]),
+        ("cl_ca_redistribute", [vp, P(c_int32), P(c_int64), P(c_double)]), ("cl_ca_update_mask", [vp, P(c_int64)]), ("cl_fd_diffuse", [vp, c_double, ctypes.c_uint32]),
         ("cl_math_exp10", [vp, vp, c_int64, c_int32]),
     ]:
         fn = getattr(lib, name)
@@ -436,6 +436,10 @@ class Lattice:
         ch = c_int64(0)
         self._c(self.lib.cl_ca_update_mask(self.h, ctypes.byref(ch)), "cl_ca_update_mask")
         return ch.value
+
+    def fd_diffuse(self, nu, microbes):
+        """One finite-difference step of the sessile biomass of the microbes whose bit is set."""
+        self._c(self.lib.cl_fd_diffuse(self.h, float(nu), int(microbes)), "cl_fd_diffuse")
 
     def ca_redistribute(self):
         """One CA block: returns (status, push sweeps, sites whose mask changed, biomass maximum)."""

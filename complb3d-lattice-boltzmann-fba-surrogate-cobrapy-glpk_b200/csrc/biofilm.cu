@@ -451,4 +451,80 @@ int ca_field(Ctx* c, int which, double* d_out) {
     return CL_OK;
 }
 
+// ---- finite-difference sessile biomass (solver_type FD) ---------------------
+// fdDiffusion3D (src/complab3d_processors_part2.hh:258-420): one explicit
+// step B += nu * (d2B/dx2 + d2B/dy2 + d2B/dz2) of the biomass of the microbes
+// in `sel`, on the sites of x = 1 .. nx-2 whose material number exceeds 1,
+// reading the copy taken before the step.  Per direction, the upstream side
+// at the lattice's first plane or next to a site with a material number
+// below 2 takes the centre value (no flux); otherwise the downstream side
+// does so at the last plane or next to such a site; otherwise both
+// neighbours are read (the reference's order of tests, so a site walled on
+// both sides still reads its downstream neighbour).  Values below thrd count
+// as zero; a result not above thrd leaves the biomass as it was.  A
+// neighbour outside the lattice reads zero.  The sums follow the reference's
+// order with no fused multiply-adds, so the oracle's FP64 result is matched
+// bit for bit.
+__global__ void fd_diffuse_kernel(Geo g, const uint8_t* __restrict__ mask, const double* __restrict__ copy,
+                                  double* __restrict__ bio, int M, uint32_t sel, double nu) {
+    const int64_t N = g.N, plane = g.plane, nz = g.nz;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < N; n += stride) {
+        int x, y, z;
+        decode(g, n, x, y, z);
+        if (x < 1 || x > g.nx - 2 || mask[n] <= 1) continue;
+        int mxp = 0, mxn = 0, myp = 0, myn = 0, mzp = 0, mzn = 0;
+        if (x == 1) mxp = mask[n + plane];
+        else if (x == g.nx - 2) mxn = mask[n - plane];
+        else { mxp = mask[n + plane]; mxn = mask[n - plane]; }
+        if (y == 0) { if (y + 1 < g.ny) myp = mask[n + nz]; }
+        else if (y == g.ny - 1) myn = mask[n - nz];
+        else { myp = mask[n + nz]; myn = mask[n - nz]; }
+        if (z == 0) { if (z + 1 < g.nz) mzp = mask[n + 1]; }
+        else if (z == g.nz - 1) mzn = mask[n - 1];
+        else { mzp = mask[n + 1]; mzn = mask[n - 1]; }
+        for (int m = 0; m < M; ++m) {
+            if (!((sel >> m) & 1u)) continue;
+            const double* cp = copy + (int64_t)m * N;
+            auto at = [&](int64_t q, bool inside) { return inside ? cp[q] : 0.0; };
+            double b0 = cp[n], bxp, bxn, byp, byn, bzp, bzn;
+            if (x == 1 || mxn < 2) { bxp = at(n + plane, x + 1 < g.nx); bxn = b0; }
+            else if (x == g.nx - 2 || mxp < 2) { bxp = b0; bxn = cp[n - plane]; }
+            else { bxp = cp[n + plane]; bxn = cp[n - plane]; }
+            if (y == 0 || myn < 2) { byp = at(n + nz, y + 1 < g.ny); byn = b0; }
+            else if (y == g.ny - 1 || myp < 2) { byp = b0; byn = cp[n - nz]; }
+            else { byp = cp[n + nz]; byn = cp[n - nz]; }
+            if (z == 0 || mzn < 2) { bzp = at(n + 1, z + 1 < g.nz); bzn = b0; }
+            else if (z == g.nz - 1 || mzp < 2) { bzp = b0; bzn = cp[n - 1]; }
+            else { bzp = cp[n + 1]; bzn = cp[n - 1]; }
+            if (b0 < kCaEps) b0 = 0.0;
+            if (bxp < kCaEps) bxp = 0.0;
+            if (bxn < kCaEps) bxn = 0.0;
+            if (byp < kCaEps) byp = 0.0;
+            if (byn < kCaEps) byn = 0.0;
+            if (bzp < kCaEps) bzp = 0.0;
+            if (bzn < kCaEps) bzn = 0.0;
+            const double b2 = 2.0 * b0;
+            const double lx = __dadd_rn(__dadd_rn(bxp, -b2), bxn);
+            const double ly = __dadd_rn(__dadd_rn(byp, -b2), byn);
+            const double lz = __dadd_rn(__dadd_rn(bzp, -b2), bzn);
+            const double nb = __dadd_rn(b0, __dmul_rn(nu, __dadd_rn(__dadd_rn(lx, ly), lz)));
+            if (nb > kCaEps) bio[(int64_t)m * N + n] = nb;
+        }
+    }
+}
+
+int fd_diffuse(Ctx* c, double nu, uint32_t sel) {
+    const int M = c->cfg.n_microbes;
+    const int64_t N = c->geo.N;
+    if (M <= 0 || !c->d_bio) { set_error("cl_fd_diffuse: no sessile biomass"); return CL_ERR_STATE; }
+    if (!c->d_fd_copy) { int r = dalloc(c, &c->d_fd_copy, (size_t)M * N); if (r) return r; }
+    CL_CUDA(cudaMemcpyAsync(c->d_fd_copy, c->d_bio, sizeof(double) * M * N, cudaMemcpyDeviceToDevice, c->stream));
+    fd_diffuse_kernel<<<grid_for(N, 256, 148 * 16), 256, 0, c->stream>>>(c->geo, c->d_mask, c->d_fd_copy, c->d_bio, M,
+                                                                        sel, nu);
+    CL_LAUNCH_CHECK("fd_diffuse_kernel");
+    c->launches += 1;
+    return CL_OK;
+}
+
 }  // namespace cl

@@ -294,7 +294,7 @@ int cl_destroy(cl_ctx* h) {
                     c->d_rho_adj, c->d_eq_iters, c->d_eq_x, c->d_eq_xp, c->d_phase, c->d_rel, c->d_counters, c->d_tracer,
                     c->d_energy_part, c->d_scratch, c->d_ca_total, c->d_ca_age, c->d_ca_distpos, c->d_ca_out,
                     c->d_dc, c->d_live, c->d_live_blk, c->d_sidx, c->d_site_of, c->d_flive, c->d_fsidx,
-                    c->d_pair_T, c->d_pair_X, c->d_pair_count};
+                    c->d_pair_T, c->d_pair_X, c->d_pair_count, c->d_fd_copy};
     if (c->learn) cl_eq_destroy(c->learn);
     if (c->flow_graph) cudaGraphExecDestroy(c->flow_graph);
     for (void* p : ptrs) if (p) cudaFree(p);
@@ -1061,6 +1061,16 @@ int cl_ca_update_mask(cl_ctx* h, int64_t* mask_changes) {
     if (!h) return CL_ERR_ARG;
     if (!h->c.ade_ready) { set_error("call cl_ade_init first"); return CL_ERR_STATE; }
     return ca_update_mask(&h->c, mask_changes);
+}
+
+int cl_fd_diffuse(cl_ctx* h, double nu, uint32_t microbes) {
+    if (!h || !(nu >= 0.0) || !std::isfinite(nu)) { set_error("cl_fd_diffuse: bad argument"); return CL_ERR_ARG; }
+    if (!h->c.ade_ready) { set_error("call cl_ade_init first"); return CL_ERR_STATE; }
+    if (h->c.cfg.n_microbes < 32 && (microbes >> h->c.cfg.n_microbes) != 0u) {
+        set_error("cl_fd_diffuse: a selected microbe does not exist");
+        return CL_ERR_ARG;
+    }
+    return fd_diffuse(&h->c, nu, microbes);
 }
 
 int cl_ca_redistribute(cl_ctx* h, int32_t* sweeps, int64_t* mask_changes, double* bmax_after) {

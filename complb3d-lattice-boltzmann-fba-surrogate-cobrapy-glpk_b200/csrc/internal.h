@@ -117,6 +117,7 @@ struct Ctx {
     int32_t* d_eq_iters = nullptr;   // N
     float*   d_srg_params[CL_MAX_SRG_ORG] = {nullptr, nullptr};
     std::vector<float> h_srg_params[CL_MAX_SRG_ORG];   // host copies (a compiled chemistry's kernel takes them)
+    double*  d_fd_copy = nullptr;        // the sessile biomass before a finite-difference step
     cudaGraphExec_t flow_graph = nullptr;   // a captured run of flow steps, valid for flow_graph_key
     FlowGraphKey flow_graph_key{};
     float*   d_eq_x = nullptr;       // n_comp*N previous converged log10 free components, by storage index (NaN: none)
@@ -220,6 +221,7 @@ int ade_step_fast(Ctx* c);
 int ops_collide(Ctx* c);
 int ops_react(Ctx* c, int ops);
 int ops_stream(Ctx* c);      // the transport step of the compiled chemistry c->chem
+int fd_diffuse(Ctx* c, double nu, uint32_t sel);   // fdDiffusion3D of the microbes in sel
 int chem_match(const cl_config& cfg);   // id of the compiled chemistry cfg has the structure of, or 0
 bool chem_ready(const Ctx* c);          // the context holds what its compiled chemistry needs
 const char* chem_name(int id);

@@ -355,6 +355,11 @@ int main(int argc, char** argv) {
     }
 
     long resolves = 0, ca_sweeps = 0, ca_blocks = 0, ca_changes = 0;
+    // finite-difference microbes and their nu = bioNUinPore[0] (refNu from the
+    // first solute's pore relaxation, complab.cpp:716-736)
+    uint32_t fd_bits = 0;
+    for (int m = 0; m < c.n_microbes && m < 32; ++m) if (m < (int)run.fd.size() && run.fd[m]) fd_bits |= 1u << m;
+    const double fd_nu = c.n_solutes > 0 ? (1.0 / c.omega_pore[0] - 0.5) / 4.0 * fd_nu_ratio(run) : 0.0;
     if (c.ca_enabled) {
         // initial mask update from the seeded biomass, and on a change the
         // dynamics switch and a flow re-solve (complab.cpp:1068-1091)
@@ -382,9 +387,18 @@ int main(int argc, char** argv) {
         if (!check(st, "cl_step")) return 1;
         ++steps_done;
         if (st == CL_WARN_NOT_CONVERGED) ++nonconv_steps;
-        // CA biomass redistribution (complab.cpp:1453-1715)
+        // CA biomass redistribution (complab.cpp:1453-1715), or the
+        // finite-difference step of sessile biomass: the mask update, one
+        // diffusion step, the mask update (complab.cpp:1716-1731)
         bool ca_changed = false;
-        if (c.ca_enabled) {
+        if (c.ca_enabled && fd_bits) {
+            int64_t ch1 = 0, ch2 = 0;
+            if (!check(cl_ca_update_mask(h, &ch1), "cl_ca_update_mask")) return 1;
+            if (!check(cl_fd_diffuse(h, fd_nu, fd_bits), "cl_fd_diffuse")) return 1;
+            if (!check(cl_ca_update_mask(h, &ch2), "cl_ca_update_mask")) return 1;
+            ca_changes += ch1 + ch2;
+            ca_changed = ch1 + ch2 > 0;
+        } else if (c.ca_enabled) {
             int32_t sw = 0;
             int64_t ch = 0;
             double bm = 0.0;

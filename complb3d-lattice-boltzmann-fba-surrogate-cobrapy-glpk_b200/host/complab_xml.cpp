@@ -106,9 +106,9 @@ int read_complab_xml(const std::string& path, HostRun& run, std::string& err, co
             c.right_value[s] = sub["right_boundary_condition"].num();
         }
 
-        // microbiology: CA-solved sessile biomass, or LBM-solved biomass
-        // carried by an extra mobile solute (a planktonic bFree lattice,
-        // complab.cpp:788-797); finite-difference biomass is refused
+        // microbiology: CA- or finite-difference-solved sessile biomass, or
+        // LBM-solved biomass carried by an extra mobile solute (a planktonic
+        // bFree lattice, complab.cpp:788-797)
         int M = 0;
         if (run.biotic_mode) {
             const XmlNode& mic = P["microbiology"];
@@ -117,9 +117,15 @@ int read_complab_xml(const std::string& path, HostRun& run, std::string& err, co
             for (int m = 0; m < M; ++m) {
                 const XmlNode& mb = mic["microbe" + std::to_string(m)];
                 const std::string st = lower(mb["solver_type"].str());
-                if (st == "fd" || st == "finite difference" || st == "finite_difference")
-                    throw std::runtime_error("microbe" + std::to_string(m) + ": solver_type " + mb["solver_type"].str() +
-                                             " (finite-difference mobile biomass) is not part of this library; use CA or LBM");
+                const bool fd = st == "fd" || st == "finite difference" || st == "finite_difference";
+                // the biomass pore diffusion coefficient, which finite differences need
+                // (complab_functions.hh:1123-1130); microbe 0's sets their nu
+                const XmlNode* dpo = opt(mb, {"biomass_diffusion_coefficients", "in_pore"});
+                if (fd && !dpo)
+                    throw std::runtime_error("microbe" + std::to_string(m) +
+                                             ": biomass_diffusion_coefficients must be defined when solver_type is Finite Difference");
+                if (m == 0 && dpo) run.D_bmass_pore0 = dpo->num();
+                run.fd.push_back(fd ? 1 : 0);
                 run.carried.push_back(st == "lbm" || st == "lb" || st == "lattice boltzmann" ? 1 : 0);
                 run.b0.push_back(mb["initial_densities"].nums());
                 run.microbe_names.push_back(mb.has("name_of_microbes") ? mb["name_of_microbes"].str()
@@ -364,11 +370,16 @@ int read_complab_xml(const std::string& path, HostRun& run, std::string& err, co
             }
             if (c.n_phases == 0) throw std::runtime_error("<dissolution> is enabled but no <phase0> block was given");
         }
-        // cellular automaton (complab_functions.hh:1167-1186): every microbe this
-        // driver accepts is CA-solved, so the CA runs whenever there is one;
-        // its material code is the first of its material numbers (bio_dynamics[m][0])
-        int n_ca = 0;
-        for (int m = 0; m < M; ++m) n_ca += run.carried[m] ? 0 : 1;
+        // cellular automaton (complab_functions.hh:1167-1186): every sessile
+        // microbe is CA- or finite-difference-solved; both keep the mask and
+        // total-biomass state of the CA (finite differences run its mask
+        // update around their diffusion step, complab.cpp:1716-1731); a
+        // microbe's material code is the first of its material numbers
+        // (bio_dynamics[m][0])
+        int n_ca = 0, n_fd = 0;
+        for (int m = 0; m < M; ++m) { n_ca += run.carried[m] ? 0 : 1; n_fd += run.fd[m]; }
+        if (n_fd > 0 && n_fd != n_ca)
+            throw std::runtime_error("finite-difference and cellular-automaton microbes in one run are not supported");
         if (n_ca > 0) {
             const XmlNode& mic = P["microbiology"];
             if (!mic.has("thrd_biofilm_fraction"))
@@ -400,6 +411,14 @@ int read_complab_xml(const std::string& path, HostRun& run, std::string& err, co
         err = e.what();
         return -1;
     }
+}
+
+
+// nu of the finite-difference step over refNu: bioNUinPore[0] / refNu =
+// D_bmass_pore[0] / D_pore[0] where microbe 0's coefficient is positive, else 0
+// (complab.cpp:731-736)
+double fd_nu_ratio(const HostRun& r) {
+    return (r.D_bmass_pore0 > 0 && !r.D_pore.empty() && r.D_pore[0] > 0) ? r.D_bmass_pore0 / r.D_pore[0] : 0.0;
 }
 
 std::string run_json(const HostRun& r) {
@@ -469,7 +488,11 @@ std::string run_json(const HostRun& r) {
         for (size_t k = 0; k < r.bio_materials[m].size(); ++k) o << (k ? ", " : "") << r.bio_materials[m][k];
         o << "]";
     }
-    o << "], \"microbe_names\": [";
+    // finite-difference microbes, and nu / refNu of their step (bioNUinPore[0])
+    o << "], \"fd\": [";
+    for (size_t m = 0; m < r.fd.size(); ++m) o << (m ? ", " : "") << r.fd[m];
+    o << "], \"fd_nu_ratio\": " << fd_nu_ratio(r);
+    o << ", \"microbe_names\": [";
     for (size_t m = 0; m < r.microbe_names.size(); ++m) o << (m ? ", " : "") << "\"" << r.microbe_names[m] << "\"";
     o << "], \"b0\": [";
     for (size_t m = 0; m < r.b0.size(); ++m) {

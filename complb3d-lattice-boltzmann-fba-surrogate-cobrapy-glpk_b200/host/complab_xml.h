@@ -35,6 +35,8 @@ struct HostRun {
     std::vector<double> D_pore, D_bfilm;
     std::vector<double> D_bfilm_ref;                 // divisor of the biofilm relaxation (complab.cpp:725, :738)
     std::vector<int> carried;                        // per microbe: 1 if solved by LBM (a carrier solute)
+    std::vector<int> fd;                             // per microbe: 1 if solved by finite differences (sessile)
+    double D_bmass_pore0 = -99.0;                    // microbe 0's biomass pore diffusion (bioNUinPore[0], complab.cpp:731-736)
     std::vector<std::vector<int>> bio_materials;    // per microbe: its biofilm material numbers
     std::vector<std::vector<double>> b0;            // per microbe: initial density per material
     bool biotic_mode = true;
@@ -47,6 +49,8 @@ struct HostRun {
 int read_complab_xml(const std::string& path, HostRun& run, std::string& err, const std::string& rates = "");
 
 // The parsed run as JSON (used by --print-config and the tests).
+// nu of the finite-difference biomass step over refNu (bioNUinPore[0] / refNu)
+double fd_nu_ratio(const HostRun& r);
 std::string run_json(const HostRun& run);
 
 }  // namespace clhost

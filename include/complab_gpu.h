@@ -453,6 +453,15 @@ int cl_ca_redistribute(cl_ctx* ctx, int32_t* sweeps, int64_t* mask_changes, doub
  * has moved since the last baseline (complab.cpp:1736-1739).  cl_ade_init
  * sets the first baseline from the uploaded mask. */
 int cl_ca_update_mask(cl_ctx* ctx, int64_t* mask_changes);
+/* fdDiffusion3D (src/complab3d_processors_part2.hh:258-420), the
+ * finite-difference biomass solver (solver_type FD): one explicit step
+ * B += nu * laplacian(B) of the sessile biomass of the microbes whose bit is
+ * set in `microbes`, on the sites of x = 1 .. nx-2 whose material number
+ * exceeds 1, with no flux into sites whose material number is below 2 or
+ * out of the lattice; nu in lattice units (the reference passes
+ * bioNUinPore[0]).  The reference's step is cl_ca_update_mask, this, and
+ * cl_ca_update_mask again (complab.cpp:1716-1731). */
+int cl_fd_diffuse(cl_ctx* ctx, double nu, uint32_t microbes);
 /* the age field (read) as FP64 */
 #define CL_FIELD_CA_AGE    7
 #define CL_FIELD_CA_TOTAL  8   /* total biomass the CA last computed */

@@ -1648,3 +1648,60 @@ void orc_surrogate_forward(const cl_surrogate_net* net, const double* xin, doubl
             yout[k*wl + o] = (a[o] - net->y_ymin) / net->y_gain[o] + net->y_offset[o];
     }
 }
+
+/* fdDiffusion3D (src/complab3d_processors_part2.hh:258-420): one explicit
+ * finite-difference step of the sessile biomass of the microbes in sel on the
+ * sites of x = 1 .. nx-2 whose material number exceeds 1, reading a copy
+ * taken before the step; the boundary tests in the reference's order (the
+ * upstream side first); values below COMPLAB_THRD read as zero; a result not
+ * above COMPLAB_THRD leaves the biomass as it was; a neighbour outside the
+ * lattice reads zero. */
+void orc_fd_diffuse(const cl_config* cfg, orc_state* st, double nu, uint32_t sel) {
+    const int nx = cfg->nx, ny = cfg->ny, nz = cfg->nz, M = cfg->n_microbes;
+    const int64_t N = (int64_t)nx * ny * nz;
+    double* cp = (double*)malloc(sizeof(double) * (size_t)(M > 0 ? M : 1) * (size_t)N);
+    memcpy(cp, st->bio, sizeof(double) * (size_t)M * (size_t)N);
+    const uint8_t* mk = st->mask;
+    for (int x = 1; x <= nx - 2; ++x)
+        for (int y = 0; y < ny; ++y)
+            for (int z = 0; z < nz; ++z) {
+                const int64_t n = site(cfg, x, y, z);
+                if (mk[n] <= 1) continue;
+                int mxp = 0, mxn = 0, myp = 0, myn = 0, mzp = 0, mzn = 0;
+                if (x == 1) mxp = mk[site(cfg, x + 1, y, z)];
+                else if (x == nx - 2) mxn = mk[site(cfg, x - 1, y, z)];
+                else { mxp = mk[site(cfg, x + 1, y, z)]; mxn = mk[site(cfg, x - 1, y, z)]; }
+                if (y == 0) { if (y + 1 < ny) myp = mk[site(cfg, x, y + 1, z)]; }
+                else if (y == ny - 1) myn = mk[site(cfg, x, y - 1, z)];
+                else { myp = mk[site(cfg, x, y + 1, z)]; myn = mk[site(cfg, x, y - 1, z)]; }
+                if (z == 0) { if (z + 1 < nz) mzp = mk[site(cfg, x, y, z + 1)]; }
+                else if (z == nz - 1) mzn = mk[site(cfg, x, y, z - 1)];
+                else { mzp = mk[site(cfg, x, y, z + 1)]; mzn = mk[site(cfg, x, y, z - 1)]; }
+                for (int m = 0; m < M; ++m) {
+                    if (!((sel >> m) & 1u)) continue;
+                    const double* c = cp + (int64_t)m * N;
+#define FD_AT(xx, yy, zz) (((xx) >= 0 && (xx) < nx && (yy) >= 0 && (yy) < ny && (zz) >= 0 && (zz) < nz) ? c[site(cfg, xx, yy, zz)] : 0.0)
+                    double b0 = c[n], bxp, bxn, byp, byn, bzp, bzn;
+                    if (x == 1 || mxn < 2) { bxp = FD_AT(x + 1, y, z); bxn = b0; }
+                    else if (x == nx - 2 || mxp < 2) { bxp = b0; bxn = FD_AT(x - 1, y, z); }
+                    else { bxp = FD_AT(x + 1, y, z); bxn = FD_AT(x - 1, y, z); }
+                    if (y == 0 || myn < 2) { byp = FD_AT(x, y + 1, z); byn = b0; }
+                    else if (y == ny - 1 || myp < 2) { byp = b0; byn = FD_AT(x, y - 1, z); }
+                    else { byp = FD_AT(x, y + 1, z); byn = FD_AT(x, y - 1, z); }
+                    if (z == 0 || mzn < 2) { bzp = FD_AT(x, y, z + 1); bzn = b0; }
+                    else if (z == nz - 1 || mzp < 2) { bzp = b0; bzn = FD_AT(x, y, z - 1); }
+                    else { bzp = FD_AT(x, y, z + 1); bzn = FD_AT(x, y, z - 1); }
+#undef FD_AT
+                    if (b0 < COMPLAB_THRD) b0 = 0;
+                    if (bxp < COMPLAB_THRD) bxp = 0;
+                    if (bxn < COMPLAB_THRD) bxn = 0;
+                    if (byp < COMPLAB_THRD) byp = 0;
+                    if (byn < COMPLAB_THRD) byn = 0;
+                    if (bzp < COMPLAB_THRD) bzp = 0;
+                    if (bzn < COMPLAB_THRD) bzn = 0;
+                    const double nb = b0 + nu * ((bxp - 2 * b0 + bxn) + (byp - 2 * b0 + byn) + (bzp - 2 * b0 + bzn));
+                    if (nb > COMPLAB_THRD) st->bio[(int64_t)m * N + n] = nb;
+                }
+            }
+    free(cp);
+}

@@ -118,6 +118,8 @@ void    orc_ca_init(const cl_config* cfg, const uint8_t* mask, orc_ca* ca);
 int64_t orc_ca_update_mask(const cl_config* cfg, orc_state* st, orc_ca* ca, int serial);
 int     orc_ca_redistribute(const cl_config* cfg, orc_state* st, orc_ca* ca, int serial,
                             int32_t* sweeps, int64_t* mask_changes, double* bmax_after);
+/* fdDiffusion3D: one finite-difference step of the sessile biomass of the microbes in sel */
+void    orc_fd_diffuse(const cl_config* cfg, orc_state* st, double nu, uint32_t sel);
 
 /* ---- speciation ------------------------------------------------------------ */
 /* totals from species (calc_component_totals) */

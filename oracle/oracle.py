@@ -75,6 +75,8 @@ def lib():
         _orc.orc_ca_update_mask.argtypes = [vp, vp, vp, i]
         _orc.orc_ca_redistribute.restype = i
         _orc.orc_ca_redistribute.argtypes = [vp, vp, vp, i, vp, vp, vp]
+        _orc.orc_fd_diffuse.restype = None
+        _orc.orc_fd_diffuse.argtypes = [vp, vp, d, ctypes.c_uint32]
     return _orc
 
 
@@ -246,6 +248,10 @@ class Transport:
     def ca_update_mask(self, serial=False):
         return lib().orc_ca_update_mask(ctypes.byref(self.cfg), ctypes.byref(self.st), ctypes.byref(self.ca),
                                         1 if serial else 0)
+
+    def fd_diffuse(self, nu, microbes):
+        """fdDiffusion3D of the sessile biomass of the microbes whose bit is set."""
+        lib().orc_fd_diffuse(ctypes.byref(self.cfg), ctypes.byref(self.st), float(nu), int(microbes))
 
     def ca_redistribute(self, serial=False):
         """(status, sweeps, mask changes, biomass maximum) of one CA block."""

@@ -248,4 +248,23 @@ int ref_ca_block(int nx, int ny, int nz, int M, int half, double bmax, double fr
     return status;
 }
 
+/* fdDiffusion3D (complab3d_processors_part2.hh:258-420) on one block: the
+ * copies taken from the biomass, [B.., copies.., mask], bdryGap 1, nu */
+void ref_fd_diffuse(int nx, int ny, int nz, int M, double nu, const uint8_t* mask, double* bio) {
+    Block b(nx, ny, nz, M);
+    const size_t N = (size_t)nx * ny * nz;
+    b.each([&](plint x, plint y, plint z, size_t n) {
+        b.mask->setScalar(x, y, z, mask[n]);
+        for (int m = 0; m < M; ++m) { b.bio[m]->setScalar(x, y, z, bio[m * N + n]); b.copy[m]->setScalar(x, y, z, bio[m * N + n]); }
+    });
+    std::vector<Lat*> v(b.bio);
+    v.insert(v.end(), b.copy.begin(), b.copy.end());
+    v.push_back(b.mask);
+    fdDiffusion3D<double, CaStubD3Q7> p(nx, ny, nz, (plint)v.size(), 1, nu);
+    p.process(b.box(), v);
+    b.each([&](plint x, plint y, plint z, size_t n) {
+        for (int m = 0; m < M; ++m) bio[m * N + n] = b.bio[m]->get(x, y, z).computeDensity();
+    });
+}
+
 }  // extern "C"

@@ -22,7 +22,8 @@ sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(HERE))))
 sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(HERE)), "tests"))
 
 SUPPORTED = ["01_flow_only", "02_diffusion_only", "03_abiotic_kinetics", "04_equilibrium",
-             "05_biotic_cellular_automaton", "07_biotic_lattice_boltzmann", "08_two_microbes",
+             "05_biotic_cellular_automaton", "06_biotic_finite_difference", "07_biotic_lattice_boltzmann",
+             "08_two_microbes",
              "13_precipitation", "14_dissolution", "15_precip_and_dissolution"]
 
 

@@ -239,9 +239,8 @@ def _ref_examples():
     root = reference_root()
     return os.path.join(root, "examples") if root else None
 SUPPORTED = ["01_flow_only", "02_diffusion_only", "03_abiotic_kinetics", "04_equilibrium",
-             "05_biotic_cellular_automaton", "07_biotic_lattice_boltzmann", "08_two_microbes",
-             "13_precipitation", "14_dissolution", "15_precip_and_dissolution"]
-MOBILE_BIOMASS = ["06_biotic_finite_difference"]
+             "05_biotic_cellular_automaton", "06_biotic_finite_difference", "07_biotic_lattice_boltzmann",
+             "08_two_microbes", "13_precipitation", "14_dissolution", "15_precip_and_dissolution"]
 
 
 def _example_xml(name):
@@ -281,13 +280,26 @@ def test_reference_example_configs_parse(name):
 
 
 @pytest.mark.skipif(not driver_available(), reason="host driver not built")
-@pytest.mark.parametrize("name", MOBILE_BIOMASS)
-def test_reference_examples_with_mobile_biomass_are_refused(name):
-    """Mobile biomass (finite-difference or LBM biomass lattices) is outside
-    this library's hot path: the driver says so and exits 1."""
-    d, xml = _example_xml(name)
+def test_finite_difference_biomass_config(tmp_path):
+    """Example 06's finite-difference microbe: the driver reads it as sessile
+    biomass with the CA's mask state, reports the microbe as FD and nu / refNu
+    of its step (microbe 0's biomass over the first solute's pore
+    diffusion); without the biomass diffusion coefficients it refuses the
+    input, as the reference does (complab_functions.hh:1128)."""
+    d, xml = _example_xml("06_biotic_finite_difference")
     r = subprocess.run([DRIVER, xml, "--print-config"], cwd=d, capture_output=True, text=True)
-    assert r.returncode == 1 and "mobile biomass" in r.stderr
+    assert r.returncode == 0, r.stderr
+    c = json.loads(r.stdout)
+    assert c["fd"] == [1] and c["ca_enabled"] == 1
+    assert c["fd_nu_ratio"] == pytest.approx(3e-13 / 5e-10)
+    import shutil
+    e = tmp_path / "ex"
+    shutil.copytree(d, e)
+    x = (e / xml).read_text()
+    a0, a1 = x.index("<biomass_diffusion_coefficients>"), x.index("</biomass_diffusion_coefficients>")
+    (e / xml).write_text(x[:a0] + x[a1 + len("</biomass_diffusion_coefficients>"):])
+    r = subprocess.run([DRIVER, xml, "--print-config"], cwd=e, capture_output=True, text=True)
+    assert r.returncode == 1 and "Finite Difference" in r.stderr
 
 
 @pytest.mark.skipif(not driver_available(), reason="host driver not built")
@@ -313,7 +325,8 @@ def test_example_rate_tables_and_config_dump(name, tmp_path):
     assert (cfg.nx, cfg.ny, cfg.nz) == (c["nx"], c["ny"], c["nz"])
     mask = np.fromfile(tmp_path / "c.bin.mask", np.uint8)
     assert mask.size == cfg.nx * cfg.ny * cfg.nz
-    want_rxn = {"03_abiotic_kinetics": 1, "05_biotic_cellular_automaton": 1, "07_biotic_lattice_boltzmann": 1,
+    want_rxn = {"03_abiotic_kinetics": 1, "05_biotic_cellular_automaton": 1, "06_biotic_finite_difference": 1,
+                "07_biotic_lattice_boltzmann": 1,
                 "08_two_microbes": 2, "13_precipitation": 1, "15_precip_and_dissolution": 1}.get(name, 0)
     assert cfg.n_rxn == want_rxn
     if name == "05_biotic_cellular_automaton":

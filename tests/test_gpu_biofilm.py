@@ -135,3 +135,44 @@ def test_ca_invariants_large(gpu_lib, pkg, half):
     assert tot.max() <= BMAX + 1e-12 and bmax <= BMAX + 1e-12
     wall = np.isin(lat.mask(), [0, 1])
     assert np.all(tot[wall] == 0.0)
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_fd_diffusion_matches_oracle_bit_for_bit(gpu_lib, pkg, seed):
+    """The finite-difference biomass step on the GPU (fd_diffuse_kernel)
+    against the oracle, which the reference's own fdDiffusion3D pins
+    (test_oracle_biofilm.py): the same FP64 sums in the same order, so the
+    biomass fields are equal bit for bit, over three steps with the
+    mask update between them."""
+    nx, ny, nz = 30, 17, 13
+    rng = np.random.default_rng(seed)
+    mask = np.full((nx, ny, nz), 2, np.uint8)
+    for _ in range(12):
+        x, y, z = rng.integers(1, nx - 3), rng.integers(1, ny - 3), rng.integers(1, nz - 3)
+        mask[x:x + 2, y:y + 2, z:z + 2] = 0
+    mask[:, 0, :] = mask[:, ny - 1, :] = 1
+    mask[:, :, 0] = mask[:, :, nz - 1] = 1
+    mask[(mask == 2) & (rng.random(mask.shape) < 0.3)] = 3
+    M = 2
+    bio = rng.random((M, nx, ny, nz)) * 40.0 * (rng.random((M, nx, ny, nz)) < 0.6)
+    bio[:, mask <= 1] = 0.0
+    cfg = pkg.make_config(nx, ny, nz, solutes=[{"tau": 0.8}], microbes=M, bio_codes=(3,))
+    cfg.ca_enabled, cfg.ca_bmax, cfg.ca_thrd_frac = 1, 50.0, 0.01
+    cfg.microbe_code[0] = cfg.microbe_code[1] = 3
+    lat = pkg.Lattice(cfg)
+    lat.upload_mask(mask)
+    lat.ade_init()
+    t = o.Transport(cfg, mask.reshape(-1))
+    t.ca_init()
+    for m in range(M):
+        lat.set_field(pkg.FIELD_BIOMASS, m, bio[m])
+        t.set_biomass(m, bio[m].reshape(-1))
+    for k in range(3):
+        ch = lat.ca_update_mask()
+        assert ch == t.ca_update_mask()
+        lat.fd_diffuse(0.05, 0b11)
+        t.fd_diffuse(0.05, 0b11)
+        for m in range(M):
+            np.testing.assert_array_equal(lat.field(pkg.FIELD_BIOMASS, m).reshape(-1), t.biomass(m), err_msg=str((k, m)))
+        np.testing.assert_array_equal(lat.mask().reshape(-1), t.mask)
+    lat.close()

@@ -3,7 +3,9 @@ against the FP64 oracle replaying the same run.
 
 Examples 07 and 08 solve a microbe by LBM (the reference's planktonic
 bFree lattice): the driver carries it as one more mobile solute named after
-it (cl_config.microbe_carrier), compared as a solute field.
+it (cl_config.microbe_carrier), compared as a solute field.  Example 06
+solves its sessile microbe by finite differences (cl_fd_diffuse between two
+mask updates each step).
 
 Each folder under tests/golden/examples holds one example's CompLaB.xml and
 geometry exactly as the reference ships them (copied by make_examples.py)
@@ -46,7 +48,8 @@ pytestmark = pytest.mark.gpu
 EXAMPLES = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "examples")
 # example: transport steps (the example's own ade_max_iT)
 CASES = {"01_flow_only": 400, "02_diffusion_only": 2000, "03_abiotic_kinetics": 1500, "04_equilibrium": 600,
-         "05_biotic_cellular_automaton": 1000, "07_biotic_lattice_boltzmann": 1000, "08_two_microbes": 1000,
+         "05_biotic_cellular_automaton": 1000, "06_biotic_finite_difference": 1000,
+         "07_biotic_lattice_boltzmann": 1000, "08_two_microbes": 1000,
          "13_precipitation": 2000, "14_dissolution": 2000, "15_precip_and_dissolution": 3000}
 # Example 08 runs without flow: its LBM-solved microbe diffuses at 3e-13 m^2/s,
 # so its lattice relaxes at tau = 0.5002, and under the example's Pe = 1 flow
@@ -104,6 +107,11 @@ def replay(pkg, cj, cfg, mask, steps):
             b[mask == mat] = b0
         tr.set_biomass(m, b)
     ev = {"precip": 0, "dissol": 0, "ca_sweeps": 0, "ca_changes": 0}
+    # finite-difference microbes: the mask update, one diffusion step with
+    # nu = bioNUinPore[0] (refNu from the first solute's pore relaxation), the
+    # mask update (complab.cpp:1716-1731)
+    fd_bits = sum(1 << m for m, f in enumerate(cj.get("fd", [])) if f)
+    fd_nu = (1.0 / cfg.omega_pore[0] - 0.5) / 4.0 * cj.get("fd_nu_ratio", 0.0)
     if cfg.ca_enabled:
         tr.ca_init()
         ch = tr.ca_update_mask()
@@ -114,7 +122,12 @@ def replay(pkg, cj, cfg, mask, steps):
     for it in range(steps):
         tr.step(1)
         ca_resolve = False
-        if cfg.ca_enabled:
+        if cfg.ca_enabled and fd_bits:
+            ch = tr.ca_update_mask()
+            tr.fd_diffuse(fd_nu, fd_bits)
+            ch += tr.ca_update_mask()
+            ev["ca_changes"] += ch
+        elif cfg.ca_enabled:
             st, sw, ch, _ = tr.ca_redistribute()
             assert st == 0
             ev["ca_sweeps"] += sw

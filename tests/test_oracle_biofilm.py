@@ -4,6 +4,8 @@ orders (the reference's in-place traversal and the plan-then-gather order the
 CUDA library runs), the age wavefront of updateAgeDistance3D as a distance
 transform, and the mask reclassification of updateLocalMaskNtotalLattices3D.
 """
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -206,3 +208,42 @@ def test_serial_order_matches_the_reference_processors(pkg, half, M, n_pore):
             b = t.biomass(m) * g
             t.set_biomass(m, b)
             r.bio[m * t.N:(m + 1) * t.N] = b
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_fd_diffusion_matches_the_reference_processor(pkg, seed):
+    """The finite-difference biomass step (solver_type FD) against the
+    reference's own fdDiffusion3D, compiled from its sources and run on one
+    block: random biomass (some of it below thrd) of two microbes, one of
+    them selected, on a channel walled in y and z with cube grains, so the
+    no-flux sides, the x-planes left out and the thresholds all occur.  Equal
+    to 1e-13 (the reference stores each value as seven populations)."""
+    if o.ref_lib() is None:
+        pytest.skip("reference tree absent: oracle/_ref not built")
+    nx, ny, nz = 14, 11, 9
+    rng = np.random.default_rng(seed)
+    mask = np.full((nx, ny, nz), 2, np.uint8)
+    for _ in range(5):
+        x, y, z = rng.integers(1, nx - 3), rng.integers(1, ny - 3), rng.integers(1, nz - 3)
+        mask[x:x + 2, y:y + 2, z:z + 2] = 0
+    mask[:, 0, :] = mask[:, ny - 1, :] = 1
+    mask[:, :, 0] = mask[:, :, nz - 1] = 1
+    mask[(mask == 2) & (rng.random(mask.shape) < 0.3)] = 3
+    M = 2
+    bio = rng.random((M, nx, ny, nz)) * (rng.random((M, nx, ny, nz)) < 0.7)
+    bio[bio < 0.05] *= 1e-15                      # some values below thrd
+    bio[:, mask <= 1] = 0.0
+    cfg = pkg.make_config(nx, ny, nz, solutes=[{"tau": 0.8}], microbes=M, bio_codes=(3,))
+    t = o.Transport(cfg, mask.reshape(-1))
+    for m in range(M):
+        t.set_biomass(m, bio[m].reshape(-1))
+    nu = 0.13
+    t.fd_diffuse(nu, 0b01)
+    ref = np.ascontiguousarray(bio.reshape(-1), np.float64).copy()
+    o.ref_lib().ref_fd_diffuse(ctypes.c_int(nx), ctypes.c_int(ny), ctypes.c_int(nz), ctypes.c_int(1),
+                               ctypes.c_double(nu), np.ascontiguousarray(mask.reshape(-1)).ctypes.data_as(ctypes.c_void_p),
+                               ref.ctypes.data_as(ctypes.c_void_p))
+    N = nx * ny * nz
+    np.testing.assert_allclose(t.biomass(0), ref[:N], rtol=1e-13, atol=1e-13)
+    assert np.abs(t.biomass(0) - bio[0].reshape(-1)).max() > 1e-3       # it did diffuse
+    np.testing.assert_array_equal(t.biomass(1), bio[1].reshape(-1))      # not selected
