@@ -371,7 +371,10 @@ struct ChemSurrogate2 {
             for (int l = 0; l < kL; ++l) {
                 const int wi = width(l), wo = width(l + 1);
                 const float* W = kc.w[o] + poff(l);
-#pragma unroll
+                // outputs four at a time: unrolled whole, the two networks'
+                // code (every weight an immediate operand) overran the
+                // instruction cache (3.16 -> 2.68 ms at 256^3 this way)
+#pragma unroll 4
                 for (int q = 0; q < wo; ++q) {
                     float acc = W[wo * wi + q];
 #pragma unroll
