@@ -41,6 +41,8 @@
 #include <fstream>
 #include <string>
 #include <vector>
+#include <sstream>
+#include <map>
 
 #include "../../include/complab_gpu.h"
 #include "complab_io.h"
@@ -187,10 +189,75 @@ bool weighted_pore_mean(cl_ctx* h, const cl_config& c, const HostRun& run, doubl
     return true;
 }
 
+
+// A surrogate network file (the weights the reference compiles in with
+// surrogateModel.hh): whitespace-separated keyed lists, '#' comments:
+//   layers L   widths w0 .. wL   W0 (w1 x w0, row-major) b0 (w1) ... W{L-1} b{L-1}
+//   x_offset, x_gain (w0 each), x_ymin, y_offset, y_gain (wL each), y_ymin,
+//   optionally x_lo, x_hi (the input clamp box, w0 each)
+bool read_surrogate_net(const std::string& path, cl_surrogate_net& net, std::string& err) {
+    std::ifstream f(path);
+    if (!f) { err = "cannot open " + path; return false; }
+    std::map<std::string, std::vector<double>> kv;
+    std::string line, key;
+    while (std::getline(f, line)) {
+        const size_t h = line.find('#');
+        if (h != std::string::npos) line.resize(h);
+        std::istringstream is(line);
+        std::string tok;
+        while (is >> tok) {
+            char* end = nullptr;
+            const double v = std::strtod(tok.c_str(), &end);
+            if (end && *end == '\0' && !key.empty()) kv[key].push_back(v);
+            else key = tok;
+        }
+    }
+    auto need = [&](const std::string& k, size_t n) -> const std::vector<double>* {
+        auto it = kv.find(k);
+        if (it == kv.end() || it->second.size() != n) { err = path + ": " + k + " needs " + std::to_string(n) + " numbers"; return nullptr; }
+        return &it->second;
+    };
+    net = cl_surrogate_net{};
+    const auto* L = need("layers", 1);
+    if (!L) return false;
+    net.n_layers = (int32_t)(*L)[0];
+    if (net.n_layers < 1 || net.n_layers > CL_SRG_MAX_LAYERS) { err = path + ": 1.." + std::to_string(CL_SRG_MAX_LAYERS) + " layers"; return false; }
+    const auto* W = need("widths", (size_t)net.n_layers + 1);
+    if (!W) return false;
+    for (int l = 0; l <= net.n_layers; ++l) {
+        net.widths[l] = (int32_t)(*W)[l];
+        if (net.widths[l] < 1 || net.widths[l] > CL_SRG_MAX_WIDTH) { err = path + ": widths 1.." + std::to_string(CL_SRG_MAX_WIDTH); return false; }
+    }
+    size_t off = 0;
+    for (int l = 0; l < net.n_layers; ++l) {
+        const size_t wi = net.widths[l], wo = net.widths[l + 1];
+        const auto* w = need("W" + std::to_string(l), wi * wo);
+        const auto* b = need("b" + std::to_string(l), wo);
+        if (!w || !b) return false;
+        if (off + wi * wo + wo > 4096) { err = path + ": too many parameters"; return false; }
+        for (size_t k = 0; k < wi * wo; ++k) net.params[off++] = (*w)[k];
+        for (size_t k = 0; k < wo; ++k) net.params[off++] = (*b)[k];
+    }
+    const size_t w0 = net.widths[0], wl = net.widths[net.n_layers];
+    const auto *xo = need("x_offset", w0), *xg = need("x_gain", w0), *xy = need("x_ymin", 1);
+    const auto *yo = need("y_offset", wl), *yg = need("y_gain", wl), *yy = need("y_ymin", 1);
+    if (!xo || !xg || !xy || !yo || !yg || !yy) return false;
+    for (size_t k = 0; k < w0; ++k) {
+        net.x_offset[k] = (*xo)[k]; net.x_gain[k] = (*xg)[k];
+        net.x_lo[k] = kv.count("x_lo") && kv["x_lo"].size() == w0 ? kv["x_lo"][k] : -1e308;
+        net.x_hi[k] = kv.count("x_hi") && kv["x_hi"].size() == w0 ? kv["x_hi"][k] : 1e308;
+    }
+    for (size_t k = 0; k < wl; ++k) { net.y_offset[k] = (*yo)[k]; net.y_gain[k] = (*yg)[k]; }
+    net.x_ymin = (*xy)[0];
+    net.y_ymin = (*yy)[0];
+    return true;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
     std::string xml = "CompLaB.xml", rates, dump, restart;
+    std::vector<std::string> srg_files;
     long steps_override = -1;
     int eq_solver = -1;
     bool print_config = false, quiet = false;
@@ -200,6 +267,7 @@ int main(int argc, char** argv) {
         else if (a == "--quiet") quiet = true;
         else if (a == "--steps" && i + 1 < argc) steps_override = std::atol(argv[++i]);
         else if (a == "--rates" && i + 1 < argc) rates = argv[++i];
+        else if (a == "--surrogate" && i + 1 < argc) srg_files.push_back(argv[++i]);
         else if (a == "--dump-config" && i + 1 < argc) dump = argv[++i];
         else if (a == "--restart" && i + 1 < argc) restart = argv[++i];
         else if (a == "--eq-solver" && i + 1 < argc && (std::strcmp(argv[i + 1], "pcf") == 0 ||
@@ -208,7 +276,7 @@ int main(int argc, char** argv) {
         else if (!a.empty() && a[0] != '-') xml = a;
         else {
             std::fprintf(stderr, "usage: %s [CompLaB.xml] [--steps N] [--eq-solver newton|pcf] [--rates rates.xml] "
-                         "[--restart DIR] [--dump-config FILE] [--print-config] [--quiet]\n",
+                         "[--surrogate net.txt]... [--restart DIR] [--dump-config FILE] [--print-config] [--quiet]\n",
                          argv[0]);
             return 2;
         }
@@ -217,6 +285,27 @@ int main(int argc, char** argv) {
     std::string err;
     if (clhost::read_complab_xml(xml, run, err, rates)) { std::fprintf(stderr, "complab_b200: %s\n", err.c_str()); return 1; }
     if (eq_solver >= 0) run.cfg.eq.solver = eq_solver;
+    run.srg_files = srg_files;
+    // each surrogate organism's network: its inputs are the Fin of the first
+    // solutes in order (the shipped model reads Fin[m][0], Fin[m][1]), its
+    // first output the growth rate, further outputs the Fout of the solutes
+    std::vector<cl_surrogate_net> nets(run.cfg.n_srg);
+    if ((int)srg_files.size() < run.cfg.n_srg) {
+        std::fprintf(stderr, "complab_b200: %d surrogate organism(s) need a network each (--surrogate FILE)\n", run.cfg.n_srg);
+        return 1;
+    }
+    for (int o = 0; o < run.cfg.n_srg; ++o) {
+        if (!read_surrogate_net(srg_files[o], nets[o], err)) { std::fprintf(stderr, "complab_b200: %s\n", err.c_str()); return 1; }
+        cl_srg_organism& g = run.cfg.srg[o];
+        const int w0 = nets[o].widths[0], wl = nets[o].widths[nets[o].n_layers];
+        if (w0 > run.cfg.n_solutes || wl - 1 > run.cfg.n_solutes) {
+            std::fprintf(stderr, "complab_b200: network %s: more inputs or outputs than solutes\n", srg_files[o].c_str());
+            return 1;
+        }
+        for (int k = 0; k < w0; ++k) { g.in_kind[k] = CL_SRG_IN_FIN; g.in_index[k] = k; }
+        g.out_kind[0] = CL_SRG_OUT_GROWTH; g.out_index[0] = 0;
+        for (int q = 1; q < wl; ++q) { g.out_kind[q] = CL_SRG_OUT_FOUT; g.out_index[q] = q - 1; }
+    }
     if (print_config && dump.empty()) { std::printf("%s\n", clhost::run_json(run).c_str()); return 0; }
     if (steps_override >= 0) run.ade_max = steps_override;
     if (!print_config)
@@ -254,6 +343,8 @@ int main(int argc, char** argv) {
     ctx.h = cl_create(&c, nullptr, &st);
     if (!ctx.h) { std::fprintf(stderr, "complab_b200: cl_create failed (%d): %s\n", st, cl_last_error()); return 1; }
     cl_ctx* h = ctx.h;
+    for (int o = 0; o < c.n_srg; ++o)
+        if (!check(cl_set_surrogate(h, o, &nets[o]), "cl_set_surrogate")) return 1;
     if (!check(cl_upload_mask(h, mask.data()), "cl_upload_mask")) return 1;
     if (!restart.empty() && !clhost::restore_dynamics(h, run, restart, err)) {
         std::fprintf(stderr, "complab_b200: %s\n", err.c_str());

@@ -80,6 +80,7 @@ int read_complab_xml(const std::string& path, HostRun& run, std::string& err, co
                 enable_kinetics = !(t == "no" || t == "false" || t == "0");
             }
             if (const XmlNode* v = m->find("enable_abiotic_kinetics")) enable_abiotic = v->flag();
+            if (const XmlNode* v = m->find("enable_surrogate")) run.enable_surrogate = v->flag();
             if (const XmlNode* v = m->find("enable_fba_glpk"); v && v->flag())
                 run.notes.push_back("FBA (GLPK) reaction type is not part of this library; ignored");
             if (const XmlNode* v = m->find("enable_fba_cobrapy"); v && v->flag())
@@ -126,6 +127,30 @@ int read_complab_xml(const std::string& path, HostRun& run, std::string& err, co
                                              ": biomass_diffusion_coefficients must be defined when solver_type is Finite Difference");
                 if (m == 0 && dpo) run.D_bmass_pore0 = dpo->num();
                 run.fd.push_back(fd ? 1 : 0);
+                // the surrogate reaction type (run_surrogate3D with MetabolicConfig,
+                // complab3d_metabolic.hh:772-800): Vmax from <fba_maximum_uptake_flux>,
+                // else <maximum_uptake_flux>; Kc from <half_saturation_constants>;
+                // <biomass_molar_mass> (24.6 gDW/mol by default); kd the decay
+                const std::string rt = mb.has("reaction_type") ? lower(mb["reaction_type"].str()) : "";
+                if (run.enable_surrogate && rt.find("surrogate") != std::string::npos) {
+                    if (c.n_srg >= CL_MAX_SRG_ORG) throw std::runtime_error("more surrogate organisms than the library holds");
+                    cl_srg_organism& g = c.srg[c.n_srg];
+                    g.microbe = m;
+                    g.net = c.n_srg;
+                    const XmlNode* vm = opt(mb, {"fba_maximum_uptake_flux"});
+                    if (!vm) vm = opt(mb, {"maximum_uptake_flux"});
+                    if (!vm) throw std::runtime_error("microbe" + std::to_string(m) + ": the surrogate needs <fba_maximum_uptake_flux>");
+                    const std::vector<double> vmax = vm->nums();
+                    const std::vector<double> kc = mb.has("half_saturation_constants") ? mb["half_saturation_constants"].nums()
+                                                                                       : std::vector<double>();
+                    for (int s = 0; s < CL_MAX_SOLUTES; ++s) {
+                        g.vmax[s] = s < (int)vmax.size() ? std::fabs(vmax[s]) : 0.0;
+                        g.kc[s] = s < (int)kc.size() ? kc[s] : 0.0;
+                    }
+                    g.mw = num_or(mb, {"biomass_molar_mass"}, 24.6);
+                    g.kd = num_or(mb, {"decay_coefficient"}, 0.0);
+                    ++c.n_srg;
+                }
                 run.carried.push_back(st == "lbm" || st == "lb" || st == "lattice boltzmann" ? 1 : 0);
                 run.b0.push_back(mb["initial_densities"].nums());
                 run.microbe_names.push_back(mb.has("name_of_microbes") ? mb["name_of_microbes"].str()
@@ -491,7 +516,9 @@ std::string run_json(const HostRun& r) {
     // finite-difference microbes, and nu / refNu of their step (bioNUinPore[0])
     o << "], \"fd\": [";
     for (size_t m = 0; m < r.fd.size(); ++m) o << (m ? ", " : "") << r.fd[m];
-    o << "], \"fd_nu_ratio\": " << fd_nu_ratio(r);
+    o << "], \"fd_nu_ratio\": " << fd_nu_ratio(r) << ", \"n_srg\": " << c.n_srg << ", \"surrogate_files\": [";
+    for (size_t k = 0; k < r.srg_files.size(); ++k) o << (k ? ", " : "") << "\"" << r.srg_files[k] << "\"";
+    o << "]";
     o << ", \"microbe_names\": [";
     for (size_t m = 0; m < r.microbe_names.size(); ++m) o << (m ? ", " : "") << "\"" << r.microbe_names[m] << "\"";
     o << "], \"b0\": [";

@@ -36,6 +36,8 @@ struct HostRun {
     std::vector<double> D_bfilm_ref;                 // divisor of the biofilm relaxation (complab.cpp:725, :738)
     std::vector<int> carried;                        // per microbe: 1 if solved by LBM (a carrier solute)
     std::vector<int> fd;                             // per microbe: 1 if solved by finite differences (sessile)
+    bool enable_surrogate = false;                   // <enable_surrogate>
+    std::vector<std::string> srg_files;              // network of each surrogate organism, in order (--surrogate)
     double D_bmass_pore0 = -99.0;                    // microbe 0's biomass pore diffusion (bioNUinPore[0], complab.cpp:731-736)
     std::vector<std::vector<int>> bio_materials;    // per microbe: its biofilm material numbers
     std::vector<std::vector<double>> b0;            // per microbe: initial density per material

@@ -240,7 +240,12 @@ def _ref_examples():
     return os.path.join(root, "examples") if root else None
 SUPPORTED = ["01_flow_only", "02_diffusion_only", "03_abiotic_kinetics", "04_equilibrium",
              "05_biotic_cellular_automaton", "06_biotic_finite_difference", "07_biotic_lattice_boltzmann",
-             "08_two_microbes", "13_precipitation", "14_dissolution", "15_precip_and_dissolution"]
+             "08_two_microbes", "11_surrogate", "13_precipitation", "14_dissolution", "15_precip_and_dissolution"]
+
+
+def _net_args(d):
+    # example 11's network, which the reference compiles in, as the driver's file
+    return ["--surrogate", "shipped_network.txt"] if os.path.exists(os.path.join(d, "shipped_network.txt")) else []
 
 
 def _example_xml(name):
@@ -264,7 +269,7 @@ def test_reference_example_configs_parse(name):
     present): the driver reads each CompLaB.xml of the examples whose
     reaction types this library implements, in the reference's schema."""
     d, xml = _example_xml(name)
-    r = subprocess.run([DRIVER, xml, "--print-config"], cwd=d, capture_output=True, text=True)
+    r = subprocess.run([DRIVER, xml, "--print-config"] + _net_args(d), cwd=d, capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     c = json.loads(r.stdout)
     assert c["nx"] >= 3 and c["ny"] >= 1 and c["nz"] >= 1
@@ -313,7 +318,7 @@ def test_example_rate_tables_and_config_dump(name, tmp_path):
     from conftest import load_pkg
     pkg = load_pkg()
     d, xml = _example_xml(name)
-    args = [DRIVER, xml, "--print-config", "--dump-config", str(tmp_path / "c.bin")]
+    args = [DRIVER, xml, "--print-config", "--dump-config", str(tmp_path / "c.bin")] + _net_args(d)
     if os.path.exists(os.path.join(d, "rates.xml")):
         args[2:2] = ["--rates", "rates.xml"]
     r = subprocess.run(args, cwd=d, capture_output=True, text=True)

@@ -5,7 +5,8 @@ Examples 07 and 08 solve a microbe by LBM (the reference's planktonic
 bFree lattice): the driver carries it as one more mobile solute named after
 it (cl_config.microbe_carrier), compared as a solute field.  Example 06
 solves its sessile microbe by finite differences (cl_fd_diffuse between two
-mask updates each step).
+mask updates each step); example 11 adds the surrogate reaction type with
+the network the reference compiles in (shipped_network.txt, --surrogate).
 
 Each folder under tests/golden/examples holds one example's CompLaB.xml and
 geometry exactly as the reference ships them (copied by make_examples.py)
@@ -49,7 +50,7 @@ EXAMPLES = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "e
 # example: transport steps (the example's own ade_max_iT)
 CASES = {"01_flow_only": 400, "02_diffusion_only": 2000, "03_abiotic_kinetics": 1500, "04_equilibrium": 600,
          "05_biotic_cellular_automaton": 1000, "06_biotic_finite_difference": 1000,
-         "07_biotic_lattice_boltzmann": 1000, "08_two_microbes": 1000,
+         "07_biotic_lattice_boltzmann": 1000, "08_two_microbes": 1000, "11_surrogate": 500,
          "13_precipitation": 2000, "14_dissolution": 2000, "15_precip_and_dissolution": 3000}
 # Example 08 runs without flow: its LBM-solved microbe diffuses at 3e-13 m^2/s,
 # so its lattice relaxes at tau = 0.5002, and under the example's Pe = 1 flow
@@ -78,7 +79,29 @@ def stage(name, tmp):
 
 def driver(d, *args):
     cmd = [DRIVER, "CompLaB.xml"] + (["--rates", "rates.xml"] if os.path.exists(os.path.join(d, "rates.xml")) else [])
+    if os.path.exists(os.path.join(d, "shipped_network.txt")):
+        cmd += ["--surrogate", "shipped_network.txt"]
     return subprocess.run(cmd + list(args), cwd=d, capture_output=True, text=True)
+
+
+def load_net(pkg, path):
+    """A driver network file (--surrogate) as the library's cl_surrogate_net."""
+    kv, key = {}, None
+    for line in open(path):
+        for tok in line.split("#")[0].split():
+            try:
+                v = float(tok)
+            except ValueError:
+                key = tok
+                kv[key] = []
+                continue
+            kv[key].append(v)
+    L = int(kv["layers"][0])
+    widths = [int(w) for w in kv["widths"]]
+    W = [np.array(kv["W%d" % l]).reshape(widths[l + 1], widths[l]) for l in range(L)]
+    b = [np.array(kv["b%d" % l]) for l in range(L)]
+    return pkg.make_surrogate_net(widths, W, b, kv["x_offset"], kv["x_gain"], kv["y_offset"], kv["y_gain"],
+                                  x_ymin=kv["x_ymin"][0], y_ymin=kv["y_ymin"][0])
 
 
 def solute_switch(tr):
@@ -89,7 +112,7 @@ def solute_switch(tr):
     tr.ade[~wall & ~pore] = 3
 
 
-def replay(pkg, cj, cfg, mask, steps):
+def replay(pkg, cj, cfg, mask, steps, d=None):
     """The oracle's run of the driver's loop; returns the transport state, the
     event counts, the step the comparison stops at and the flow iterations."""
     flow = cj["Pe"] > 1e-12
@@ -99,6 +122,8 @@ def replay(pkg, cj, cfg, mask, steps):
         flow_it, _ = fl.solve(int(cj["ns_max_iT1"]), cj["ns_converge_iT1"])
         _, u = fl.macro()
     tr = o.Transport(cfg, mask, u=u)
+    if cfg.n_srg:
+        tr.set_surrogates([load_net(pkg, os.path.join(d, f)) for f in cj["surrogate_files"]])
     for m in range(cfg.n_microbes):
         if cfg.microbe_carrier[m]:
             continue                      # LBM-solved: its carrier solute's c0
@@ -163,7 +188,7 @@ def test_reference_example_against_oracle(gpu_lib, pkg, tmp_path, name):
     assert r.returncode == 0, r.stderr
     cfg = pkg.Config.from_buffer_copy(open(os.path.join(d, "run.cfg"), "rb").read())
     mask = np.fromfile(os.path.join(d, "run.cfg.mask"), np.uint8)
-    tr, ev, stop, flow_it = replay(pkg, cj, cfg, mask, steps)
+    tr, ev, stop, flow_it = replay(pkg, cj, cfg, mask, steps, d)
     r = driver(d, "--steps", str(stop), "--quiet")
     assert r.returncode == 0, r.stderr
     out = json.loads(r.stdout.strip().splitlines()[-1])
